@@ -1,0 +1,682 @@
+// Geometric multigrid kernels and driver (see mg.cuh for the method).
+#include <cmath>
+#include <cstring>
+#include "mg.cuh"
+
+namespace incrmt {
+
+namespace {
+
+constexpr int kNu1 = 2, kNu2 = 2, kCoarseSweeps = 64, kCoarsestSize = 64, kMaxLevels = 24;
+
+// ---------------------------------------------------------------------------
+// Transfer-operator index helpers (identical rules to the CPU oracle's shim).
+
+__host__ __device__ __forceinline__ int wrap_idx(int i, int m, int p, bool &ok) {
+    if (i < 0) { if (p) i += m; else ok = false; }
+    else if (i >= m) { if (p) i -= m; else ok = false; }
+    return i;
+}
+
+/** 1D prolongation weight P(f,I); mf, mc fine and coarse sizes, p periodic,
+ * k coarsened (else identity). */
+__host__ __device__ __forceinline__ double pw(int f, int I, int mf, int mc, int p, bool k) {
+    if (!k) return f == I ? 1. : 0.;
+    int d = f - 2 * I;
+    if (p) { if (d > mf / 2) d -= mf; else if (d < -mf / 2) d += mf; }
+    if (d == 0) return 1.;
+    if (d == -1) return 0.5;
+    if (d == 1) return (p || I + 1 < mc) ? 0.5 : 1.;
+    return 0.;
+}
+
+__host__ __device__ __forceinline__ int support(int I, int mf, int p, bool k, int *f) {
+    if (!k) { f[0] = I; return 1; }
+    int c = 0;
+    for (int d = -1; d <= 1; d++) {
+        bool ok = true;
+        int g = wrap_idx(2 * I + d, mf, p, ok);
+        if (ok) f[c++] = g;
+    }
+    return c;
+}
+
+inline bool can_coarsen(int m, int p) { return p ? (m % 2 == 0 && m / 2 >= 4) : m >= 5; }
+
+// ---------------------------------------------------------------------------
+// Coefficient set-up kernels.
+
+/** Edge reciprocal densities of the MAC system from the ghosted cell density
+ * (fluid_2d::set_edge_irho, fluid_2d.cc:1140-1160). */
+__global__ void k_mac_coef(const double *rho, int cm, int cn, double *ex, double *ey,
+                           float *exf, float *eyf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int ml = cm + 4;
+    if (j < cn && i <= cm) {
+        const int q = (i + 2) + ml * (j + 2);
+        double v = 0.5 / rho[q] + 0.5 / rho[q - 1];
+        ex[j * (cm + 1) + i] = v;
+        exf[j * (cm + 1) + i] = static_cast<float>(v);
+    }
+    if (j <= cn && i < cm) {
+        const int q = (i + 2) + ml * (j + 2);
+        double v = 0.5 / rho[q] + 0.5 / rho[q - ml];
+        ey[j * cm + i] = v;
+        eyf[j * cm + i] = static_cast<float>(v);
+    }
+}
+
+/** Cell reciprocal density at each FEM node, the cell below-left of the node
+ * (fluid_2d::set_corner_irho, fluid_2d.cc:1163-1170). */
+__global__ void k_fem_coef(const double *rho, int cm, int mf, int nf, double *c, float *cf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= mf || j >= nf) return;
+    const int ml = cm + 4;
+    double v = 1. / rho[(i + 1) + ml * (j + 1)];
+    c[j * mf + i] = v;
+    cf[j * mf + i] = static_cast<float>(v);
+}
+
+/** Galerkin coarse stencil A_c = P^T A P, one coarse unknown per thread. */
+template <class Op>
+__global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
+                           int cm, int cn, double *st) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= cm || J >= cn) return;
+    double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int fx[3], fy[3];
+    const int nfx = support(I, fm, px, kx, fx), nfy = support(J, fn, py, ky, fy);
+    for (int b = 0; b < nfy; b++) {
+        const double wy = pw(fy[b], J, fn, cn, py, ky);
+        for (int a = 0; a < nfx; a++) {
+            const double w = wy * pw(fx[a], I, fm, cm, px, kx);
+            if (w == 0) continue;
+            double s[9];
+            op.coef9(fx[a], fy[b], s);
+            for (int dj = -1; dj <= 1; dj++) {
+                bool oky = true;
+                const int gy = wrap_idx(fy[b] + dj, fn, py, oky);
+                if (!oky) continue;
+                for (int di = -1; di <= 1; di++) {
+                    const double av = s[3 * (dj + 1) + di + 1];
+                    if (av == 0) continue;
+                    bool okx = true;
+                    const int gx = wrap_idx(fx[a] + di, fm, px, okx);
+                    if (!okx) continue;
+                    for (int kj = -1; kj <= 1; kj++) {
+                        bool ok = true;
+                        const int Ky = wrap_idx(J + kj, cn, py, ok);
+                        if (!ok) continue;
+                        const double vy = pw(gy, Ky, fn, cn, py, ky);
+                        if (vy == 0) continue;
+                        for (int ki = -1; ki <= 1; ki++) {
+                            bool ok2 = true;
+                            const int Kx = wrap_idx(I + ki, cm, px, ok2);
+                            if (!ok2) continue;
+                            const double vx = pw(gx, Kx, fm, cm, px, kx);
+                            if (vx == 0) continue;
+                            q[3 * (kj + 1) + ki + 1] += w * av * vx * vy;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    const long N = static_cast<long>(cm) * cn;
+    const int ij = I + cm * J;
+#pragma unroll
+    for (int k = 0; k < 9; k++) st[k * N + ij] = q[k];
+}
+
+__global__ void k_cast(const double *a, float *b, long n) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x)
+        b[i] = static_cast<float>(a[i]);
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle kernels.
+
+/** One colour (pi,pj) of a Gauss-Seidel sweep: z = (b - offdiag)/diag. */
+template <class Op, class T>
+__global__ void k_smooth(Op op, T *z, const T *b, int m, int n, int pi, int pj) {
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + pi;
+    const int j = 2 * (blockIdx.y * blockDim.y + threadIdx.y) + pj;
+    if (i >= m || j >= n) return;
+    T diag;
+    const T off = op.offdiag(i, j, z, diag);
+    const int ij = i + m * j;
+    z[ij] = (b[ij] - off) / diag;
+}
+
+/** Coarse right-hand side b_c = P^T (b - A z), the fine residual formed on
+ * the fly; also clears the coarse iterate. */
+template <class Op, class T>
+__global__ void k_restrict(Op op, const T *z, const T *b, int fm, int fn, int px, int py,
+                           bool kx, bool ky, int cm, int cn, T *bc, T *zc) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= cm || J >= cn) return;
+    int fx[3], fy[3];
+    const int nfx = support(I, fm, px, kx, fx), nfy = support(J, fn, py, ky, fy);
+    T t = 0;
+    for (int bq = 0; bq < nfy; bq++) {
+        const T wy = static_cast<T>(pw(fy[bq], J, fn, cn, py, ky));
+        for (int a = 0; a < nfx; a++) {
+            const int f = fx[a] + fm * fy[bq];
+            T diag;
+            const T off = op.offdiag(fx[a], fy[bq], z, diag);
+            const T r = b[f] - off - diag * z[f];
+            t += wy * static_cast<T>(pw(fx[a], I, fm, cm, px, kx)) * r;
+        }
+    }
+    bc[I + cm * J] = t;
+    zc[I + cm * J] = 0;
+}
+
+/** Fine correction z_f += P z_c. */
+template <class T>
+__global__ void k_prolong(T *zf, int fm, int fn, int px, int py, bool kx, bool ky,
+                          const T *zc, int cm, int cn) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= fm || j >= fn) return;
+    int Is[2], Js[2], ni = 0, nj = 0;
+    if (!kx) Is[ni++] = i;
+    else {
+        const int lo = (i % 2 == 0) ? i / 2 : (i - 1) / 2;
+        Is[ni++] = lo;
+        if (i % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cm, px, ok); if (ok) Is[ni++] = hi; }
+    }
+    if (!ky) Js[nj++] = j;
+    else {
+        const int lo = (j % 2 == 0) ? j / 2 : (j - 1) / 2;
+        Js[nj++] = lo;
+        if (j % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cn, py, ok); if (ok) Js[nj++] = hi; }
+    }
+    T t = 0;
+    for (int bq = 0; bq < nj; bq++) {
+        const T wy = static_cast<T>(pw(j, Js[bq], fn, cn, py, ky));
+        for (int a = 0; a < ni; a++)
+            t += wy * static_cast<T>(pw(i, Is[a], fm, cm, px, kx)) * zc[Is[a] + cm * Js[bq]];
+    }
+    zf[i + fm * j] += t;
+}
+
+/** Coarsest-level solve: `sweeps` four-colour Gauss-Seidel sweeps by one
+ * block, with a block barrier between colours. */
+template <class Op, class T>
+__global__ void k_coarse(Op op, T *z, const T *b, int m, int n, int sweeps) {
+    const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
+    for (int s = 0; s < sweeps; s++) {
+        for (int c = 0; c < 4; c++) {
+            const int mc = (m - pis[c] + 1) / 2, nc = (n - pjs[c] + 1) / 2;
+            for (int p = threadIdx.x; p < mc * nc; p += blockDim.x) {
+                const int i = 2 * (p % mc) + pis[c], j = 2 * (p / mc) + pjs[c];
+                T diag;
+                const T off = op.offdiag(i, j, z, diag);
+                z[i + m * j] = (b[i + m * j] - off) / diag;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+/** FP64 residual r = b - A z, optionally stored in FP32, with per-block sums
+ * of r^2 in partial[blockIdx.x]. Grid-stride over the unknowns. */
+template <class Op>
+__global__ void k_resnorm(Op op, const double *z, const double *b, int m, int n, float *rf,
+                          double *partial) {
+    const long N = static_cast<long>(m) * n;
+    double acc = 0;
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int i = static_cast<int>(q % m), j = static_cast<int>(q / m);
+        double diag;
+        const double off = op.offdiag(i, j, z, diag);
+        const double r = b[q] - off - diag * z[q];
+        if (rf) rf[q] = static_cast<float>(r);
+        acc += r * r;
+    }
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+/** out = A z. */
+template <class Op>
+__global__ void k_apply(Op op, const double *z, double *out, int m, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= m || j >= n) return;
+    double diag;
+    const double off = op.offdiag(i, j, z, diag);
+    out[i + m * j] = off + diag * z[i + m * j];
+}
+
+__global__ void k_sumsq(const double *b, long N, double *partial) {
+    double acc = 0;
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x)
+        acc += b[q] * b[q];
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+/** Sums nb partials in a fixed order (one block), so results are reproducible. */
+__global__ void k_reduce(const double *partial, int nb, double *out) {
+    double acc = 0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) acc += partial[q];
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+__global__ void k_add_f32(double *z, const float *e, long N) {
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x)
+        z[q] += static_cast<double>(e[q]);
+}
+
+template <class T>
+__global__ void k_fill(T *a, long N, T v) {
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x)
+        a[q] = v;
+}
+
+/** Zeroes the right-hand side on the fixed right column (mgs_fem.cc:112). */
+__global__ void k_zero_column(double *b, int m, int n) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) b[m - 1 + m * j] = 0;
+}
+
+constexpr int kRedBlocks = 4 * kB200SMs;  // reduction grid: 4 x 148 blocks of 256
+
+inline dim3 grid2(int m, int n) { return dim3(cdiv(m, 32), cdiv(n, 8)); }
+const dim3 kBlk2(32, 8);
+
+/** Runs `sweeps` four-colour sweeps. When prof is given, each launch is
+ * bracketed by CUDA events and credited with its algorithmic bytes:
+ * (units updated) x bytes_per_unit. */
+template <class Op, class T>
+int smooth(Op op, T *z, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl,
+           Multigrid *prof = nullptr, double bytes_per_unit = 0) {
+    const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
+    for (int q = 0; q < sweeps; q++)
+        for (int c = 0; c < 4; c++) {
+            const int mc = (m - pis[c] + 1) / 2, nc = (n - pjs[c] + 1) / 2;
+            if (mc <= 0 || nc <= 0) continue;
+            if (prof) { int r = prof->prof_begin(static_cast<double>(mc) * nc * bytes_per_unit); if (r) return r; }
+            k_smooth<Op, T><<<grid2(mc, nc), kBlk2, 0, s>>>(op, z, b, m, n, pis[c], pjs[c]);
+            nl++;
+            if (prof) { int r = prof->prof_end(); if (r) return r; }
+        }
+    INCRMT_CKL("k_smooth");
+    return INCRMT_OK;
+}
+
+}  // namespace
+
+MacOp<double> Multigrid::mac64() const {
+    MacOp<double> o; o.m = m; o.n = n; o.px = px; o.py = py; o.zpr = zpr;
+    o.xxsp = xxsp; o.yysp = yysp; o.ex = ex; o.ey = ey; return o;
+}
+MacOp<float> Multigrid::mac32() const {
+    MacOp<float> o; o.m = m; o.n = n; o.px = px; o.py = py; o.zpr = zpr;
+    o.xxsp = static_cast<float>(xxsp); o.yysp = static_cast<float>(yysp); o.ex = exf; o.ey = eyf; return o;
+}
+FemOp<double> Multigrid::fem64() const {
+    FemOp<double> o; o.m = m; o.n = n; o.px = px; o.py = py; o.zpr = zpr;
+    o.fm = fm; o.fc = fc; o.hex = hex; o.hey = hey; o.c = c; return o;
+}
+FemOp<float> Multigrid::fem32() const {
+    FemOp<float> o; o.m = m; o.n = n; o.px = px; o.py = py; o.zpr = zpr;
+    o.fm = static_cast<float>(fm); o.fc = static_cast<float>(fc);
+    o.hex = static_cast<float>(hex); o.hey = static_cast<float>(hey); o.c = cf; return o;
+}
+
+int Multigrid::create(int sys_, int cm_, int cn_, double ax, double bx, double ay, double by,
+                      int px_, int py_, int zpr_) {
+    if (sys_ != INCRMT_SYS_MAC && sys_ != INCRMT_SYS_FEM) { set_error("unknown system %d", sys_); return INCRMT_ERR_BADARG; }
+    if (cm_ < 2 || cn_ < 2 || !(bx > ax) || !(by > ay)) { set_error("bad grid %dx%d", cm_, cn_); return INCRMT_ERR_BADARG; }
+    sys = sys_; cm = cm_; cn = cn_; px = px_ ? 1 : 0; py = py_ ? 1 : 0; zpr = zpr_ ? 1 : 0;
+    dx = (bx - ax) / cm; dy = (by - ay) / cn;
+    const double xsp = 1 / dx, ysp = 1 / dy;
+    xxsp = xsp * xsp; yysp = ysp * ysp;
+    if (sys == INCRMT_SYS_MAC) { m = cm; n = cn; }
+    else { m = px ? cm : cm + 1; n = py ? cn : cn + 1; }
+    if ((px && m % 2) || (py && n % 2)) {
+        set_error("a periodic direction needs an even number of unknowns (got %dx%d)", m, n);
+        return INCRMT_ERR_BADARG;
+    }
+    // Finite-element stencil constants (mgs_fem.cc:12-21).
+    const double dydx = dy / dx, dxdy = dx / dy;
+    fm = 1. / 3. * (dxdy + dydx);
+    const double fey = 1. / 3. * (-2 * dxdy + dydx), fex = 1. / 3. * (-2 * dydx + dxdy);
+    hey = 0.5 * fey; hex = 0.5 * fex;
+    fc = -1. / 6. * (dxdy + dydx);
+    INCRMT_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    INCRMT_CK(cudaEventCreate(&ev0));
+    INCRMT_CK(cudaEventCreate(&ev1));
+    const long N = static_cast<long>(m) * n;
+    if (sys == INCRMT_SYS_MAC) {
+        INCRMT_CK(cudaMalloc(&ex, sizeof(double) * (cm + 1) * cn));
+        INCRMT_CK(cudaMalloc(&ey, sizeof(double) * cm * (cn + 1)));
+        INCRMT_CK(cudaMalloc(&exf, sizeof(float) * (cm + 1) * cn));
+        INCRMT_CK(cudaMalloc(&eyf, sizeof(float) * cm * (cn + 1)));
+    } else {
+        INCRMT_CK(cudaMalloc(&c, sizeof(double) * N));
+        INCRMT_CK(cudaMalloc(&cf, sizeof(float) * N));
+    }
+    INCRMT_CK(cudaMalloc(&rho, sizeof(double) * (cm + 4) * (cn + 4)));
+    INCRMT_CK(cudaMalloc(&bbuf, sizeof(double) * N));
+    INCRMT_CK(cudaMalloc(&zbuf, sizeof(double) * N));
+    INCRMT_CK(cudaMalloc(&partial, sizeof(double) * kRedBlocks));
+    INCRMT_CK(cudaMalloc(&dnorm, sizeof(double) * 4));
+    INCRMT_CK(cudaMallocHost(&hnorm, sizeof(double) * 4));
+    return build_hierarchy();
+}
+
+int Multigrid::build_hierarchy() {
+    lev.clear();
+    MgLevel L0; L0.m = m; L0.n = n; L0.N = static_cast<long>(m) * n;
+    INCRMT_CK(cudaMalloc(&L0.zf, sizeof(float) * L0.N));
+    INCRMT_CK(cudaMalloc(&L0.bf, sizeof(float) * L0.N));
+    lev.push_back(L0);
+    int mm = m, nn = n;
+    while (static_cast<int>(lev.size()) < kMaxLevels && mm * nn > kCoarsestSize) {
+        const bool kx = can_coarsen(mm, px), ky = can_coarsen(nn, py);
+        if (!kx && !ky) break;
+        const int mc = kx ? (px ? mm / 2 : (mm + 1) / 2) : mm, nc = ky ? (py ? nn / 2 : (nn + 1) / 2) : nn;
+        lev.back().kx = kx; lev.back().ky = ky;
+        MgLevel L; L.m = mc; L.n = nc; L.N = static_cast<long>(mc) * nc;
+        INCRMT_CK(cudaMalloc(&L.z, sizeof(double) * L.N));
+        INCRMT_CK(cudaMalloc(&L.b, sizeof(double) * L.N));
+        INCRMT_CK(cudaMalloc(&L.st, sizeof(double) * 9 * L.N));
+        INCRMT_CK(cudaMalloc(&L.zf, sizeof(float) * L.N));
+        INCRMT_CK(cudaMalloc(&L.bf, sizeof(float) * L.N));
+        INCRMT_CK(cudaMalloc(&L.stf, sizeof(float) * 9 * L.N));
+        lev.push_back(L);
+        mm = mc; nn = nc;
+    }
+    return INCRMT_OK;
+}
+
+void Multigrid::destroy() {
+    for (auto &L : lev) {
+        cudaFree(L.z); cudaFree(L.b); cudaFree(L.st); cudaFree(L.zf); cudaFree(L.bf); cudaFree(L.stf);
+    }
+    lev.clear();
+    cudaFree(ex); cudaFree(ey); cudaFree(exf); cudaFree(eyf); cudaFree(c); cudaFree(cf);
+    cudaFree(rho); cudaFree(bbuf); cudaFree(zbuf); cudaFree(partial); cudaFree(dnorm);
+    if (hnorm) cudaFreeHost(hnorm);
+    for (auto e : prof_ev) cudaEventDestroy(e);
+    prof_ev.clear();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Multigrid::set_density_device(const double *d_rho) {
+    if (sys == INCRMT_SYS_MAC) {
+        k_mac_coef<<<grid2(cm + 1, cn + 1), kBlk2, 0, stream>>>(d_rho, cm, cn, ex, ey, exf, eyf);
+    } else {
+        k_fem_coef<<<grid2(m, n), kBlk2, 0, stream>>>(d_rho, cm, m, n, c, cf);
+    }
+    launches++;
+    INCRMT_CKL("coefficients");
+    int r = galerkin_all();
+    if (r == INCRMT_OK) ready = true;
+    return r;
+}
+
+int Multigrid::galerkin_all() {
+    for (size_t l = 1; l < lev.size(); l++) {
+        MgLevel &F = lev[l - 1], &C = lev[l];
+        if (l == 1) {
+            if (sys == INCRMT_SYS_MAC)
+                k_galerkin<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+            else
+                k_galerkin<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+        } else {
+            GenOp<double> g; g.m = F.m; g.n = F.n; g.px = px; g.py = py; g.N = F.N; g.st = F.st;
+            k_galerkin<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+        }
+        k_cast<<<cdiv(9 * C.N, 256) < kRedBlocks ? cdiv(9 * C.N, 256) : kRedBlocks, 256, 0, stream>>>(C.st, C.stf, 9 * C.N);
+        launches += 2;
+        INCRMT_CKL("galerkin");
+    }
+    return INCRMT_OK;
+}
+
+int Multigrid::cycle64(int l, const double *b0, double *z0) {
+    const MgLevel &L = lev[l];
+    const double *b = l == 0 ? b0 : L.b;
+    double *z = l == 0 ? z0 : L.z;
+    GenOp<double> g; g.m = L.m; g.n = L.n; g.px = px; g.py = py; g.N = L.N; g.st = L.st;
+    const bool last = l == static_cast<int>(lev.size()) - 1;
+    if (last) {
+        if (l == 0) {
+            if (sys == INCRMT_SYS_MAC) k_coarse<<<1, 256, 0, stream>>>(mac64(), z, b, L.m, L.n, kCoarseSweeps);
+            else k_coarse<<<1, 256, 0, stream>>>(fem64(), z, b, L.m, L.n, kCoarseSweeps);
+        } else k_coarse<<<1, 256, 0, stream>>>(g, z, b, L.m, L.n, kCoarseSweeps);
+        launches++;
+        INCRMT_CKL("k_coarse");
+        return INCRMT_OK;
+    }
+    const MgLevel &C = lev[l + 1];
+    int r;
+    Multigrid *pf = prof ? this : nullptr;
+    // Algorithmic bytes per updated unknown of a fine FP64 sweep: read z,b
+    // and the coefficient words, write z (3+c words; c=2 MAC, c=1 FEM).
+    const double bpu = 8.0 * (sys == INCRMT_SYS_MAC ? 5 : 4);
+    if (l == 0 && sys == INCRMT_SYS_MAC) {
+        auto op = mac64();
+        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches, pf, bpu))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, z, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+    } else if (l == 0) {
+        auto op = fem64();
+        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches, pf, bpu))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, z, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+    } else {
+        if ((r = smooth(g, z, b, L.m, L.n, kNu1, stream, launches))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, z, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+    }
+    launches++;
+    INCRMT_CKL("k_restrict");
+    if ((r = cycle64(l + 1, b0, z0))) return r;
+    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(z, L.m, L.n, px, py, L.kx, L.ky, static_cast<const double *>(C.z), C.m, C.n);
+    launches++;
+    INCRMT_CKL("k_prolong");
+    if (l == 0 && sys == INCRMT_SYS_MAC) return smooth(mac64(), z, b, L.m, L.n, kNu2, stream, launches, pf, bpu);
+    if (l == 0) return smooth(fem64(), z, b, L.m, L.n, kNu2, stream, launches, pf, bpu);
+    return smooth(g, z, b, L.m, L.n, kNu2, stream, launches);
+}
+
+int Multigrid::prof_begin(double bytes) {
+    constexpr int kMaxEvents = 4096;
+    if (prof_used + 2 > kMaxEvents) {
+        int r = prof_collect();
+        if (r) return r;
+    }
+    while (prof_used + 2 > static_cast<int>(prof_ev.size())) {
+        cudaEvent_t e;
+        INCRMT_CK(cudaEventCreate(&e));
+        prof_ev.push_back(e);
+    }
+    INCRMT_CK(cudaEventRecord(prof_ev[prof_used], stream));
+    pending_bytes = bytes;
+    prof_bytes += bytes;
+    return INCRMT_OK;
+}
+
+int Multigrid::prof_end() {
+    INCRMT_CK(cudaEventRecord(prof_ev[prof_used + 1], stream));
+    prof_used += 2;
+    prof_launches++;
+    return INCRMT_OK;
+}
+
+/** Folds the recorded event pairs into prof_ms (synchronises the stream).
+ * \return 0 (the number of pairs still pending) or an error status. */
+int Multigrid::prof_collect() {
+    if (prof_used == 0) return 0;
+    INCRMT_CK(cudaStreamSynchronize(stream));
+    for (int k = 0; k + 1 < prof_used; k += 2) {
+        float ms = 0;
+        INCRMT_CK(cudaEventElapsedTime(&ms, prof_ev[k], prof_ev[k + 1]));
+        prof_ms += ms;
+    }
+    prof_used = 0;
+    return 0;
+}
+
+int Multigrid::cycle32(int l) {
+    const MgLevel &L = lev[l];
+    const float *b = L.bf;
+    float *z = L.zf;
+    GenOp<float> g; g.m = L.m; g.n = L.n; g.px = px; g.py = py; g.N = L.N; g.st = L.stf;
+    const bool last = l == static_cast<int>(lev.size()) - 1;
+    if (last) {
+        if (l == 0) {
+            if (sys == INCRMT_SYS_MAC) k_coarse<<<1, 256, 0, stream>>>(mac32(), z, b, L.m, L.n, kCoarseSweeps);
+            else k_coarse<<<1, 256, 0, stream>>>(fem32(), z, b, L.m, L.n, kCoarseSweeps);
+        } else k_coarse<<<1, 256, 0, stream>>>(g, z, b, L.m, L.n, kCoarseSweeps);
+        launches++;
+        INCRMT_CKL("k_coarse");
+        return INCRMT_OK;
+    }
+    const MgLevel &C = lev[l + 1];
+    int r;
+    if (l == 0 && sys == INCRMT_SYS_MAC) {
+        auto op = mac32();
+        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(z), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+    } else if (l == 0) {
+        auto op = fem32();
+        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(z), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+    } else {
+        if ((r = smooth(g, z, b, L.m, L.n, kNu1, stream, launches))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, static_cast<const float *>(z), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+    }
+    launches++;
+    INCRMT_CKL("k_restrict");
+    if ((r = cycle32(l + 1))) return r;
+    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(z, L.m, L.n, px, py, L.kx, L.ky, static_cast<const float *>(C.zf), C.m, C.n);
+    launches++;
+    INCRMT_CKL("k_prolong");
+    if (l == 0 && sys == INCRMT_SYS_MAC) return smooth(mac32(), z, b, L.m, L.n, kNu2, stream, launches);
+    if (l == 0) return smooth(fem32(), z, b, L.m, L.n, kNu2, stream, launches);
+    return smooth(g, z, b, L.m, L.n, kNu2, stream, launches);
+}
+
+int Multigrid::norm2_rhs(const double *b, double *out_dev) {
+    const long N = static_cast<long>(m) * n;
+    const int nb = cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks;
+    k_sumsq<<<nb, 256, 0, stream>>>(b, N, partial);
+    k_reduce<<<1, 256, 0, stream>>>(partial, nb, out_dev);
+    launches += 2;
+    INCRMT_CKL("norm");
+    return INCRMT_OK;
+}
+
+int Multigrid::residual_norm(const double *b, const double *z, float *rf, double *out_dev) {
+    const long N = static_cast<long>(m) * n;
+    const int nb = cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks;
+    if (sys == INCRMT_SYS_MAC) k_resnorm<<<nb, 256, 0, stream>>>(mac64(), z, b, m, n, rf, partial);
+    else k_resnorm<<<nb, 256, 0, stream>>>(fem64(), z, b, m, n, rf, partial);
+    k_reduce<<<1, 256, 0, stream>>>(partial, nb, out_dev);
+    launches += 2;
+    INCRMT_CKL("residual norm");
+    return INCRMT_OK;
+}
+
+int Multigrid::fetch_norm(double *v) {
+    INCRMT_CK(cudaMemcpyAsync(hnorm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    INCRMT_CK(cudaStreamSynchronize(stream));
+    *v = hnorm[0];
+    return INCRMT_OK;
+}
+
+int Multigrid::vcycle64(const double *d_b, double *d_z) {
+    if (!ready) { set_error("density not set"); return INCRMT_ERR_BADARG; }
+    return cycle64(0, d_b, d_z);
+}
+
+int Multigrid::apply_device(const double *d_z, double *d_out) {
+    if (!ready) { set_error("density not set"); return INCRMT_ERR_BADARG; }
+    if (sys == INCRMT_SYS_MAC) k_apply<<<grid2(m, n), kBlk2, 0, stream>>>(mac64(), d_z, d_out, m, n);
+    else k_apply<<<grid2(m, n), kBlk2, 0, stream>>>(fem64(), d_z, d_out, m, n);
+    launches++;
+    INCRMT_CKL("k_apply");
+    return INCRMT_OK;
+}
+
+int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts *o,
+                            incrmt_mg_stats *st, bool time_it) {
+    if (!ready) { set_error("density not set"); return INCRMT_ERR_BADARG; }
+    const double rtol = (o && o->rel_tol > 0) ? o->rel_tol : 1e-9;
+    const int maxc = (o && o->max_vcycles > 0) ? o->max_vcycles : 200;
+    const int prec = o ? o->precision : INCRMT_PREC_FP64;
+    if (prec != INCRMT_PREC_FP64 && prec != INCRMT_PREC_MIXED) { set_error("bad precision %d", prec); return INCRMT_ERR_BADARG; }
+    const long N = static_cast<long>(m) * n;
+    if (time_it) INCRMT_CK(cudaEventRecord(ev0, stream));
+    const double *b = d_b;
+    if (sys == INCRMT_SYS_FEM && zpr) {
+        if (d_b != bbuf) INCRMT_CK(cudaMemcpyAsync(bbuf, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
+        k_zero_column<<<cdiv(n, 256), 256, 0, stream>>>(bbuf, m, n);
+        launches++;
+        INCRMT_CKL("zero column");
+        b = bbuf;
+    }
+    int r;
+    double nb2, rn2 = 0;
+    if ((r = norm2_rhs(b, dnorm))) return r;
+    if ((r = fetch_norm(&nb2))) return r;
+    const double nb = std::sqrt(nb2), tol = rtol * nb;
+    int k = 0;
+    if (nb == 0) {
+        // A zero right-hand side is solved by the current iterate's gauge:
+        // nothing to do (the solution is defined up to the null space).
+        if (st) { st->vcycles = 0; st->rel_res = 0; st->device_ms = 0; }
+        return INCRMT_OK;
+    }
+    bool conv = false, finite = true;
+    if (prec == INCRMT_PREC_MIXED) {
+        if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
+        if ((r = fetch_norm(&rn2))) return r;
+    }
+    while (k < maxc) {
+        if (prec == INCRMT_PREC_FP64) {
+            if ((r = cycle64(0, b, d_z))) return r;
+            if ((r = residual_norm(b, d_z, nullptr, dnorm))) return r;
+        } else {
+            k_fill<float><<<cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks, 256, 0, stream>>>(lev[0].zf, N, 0.f);
+            launches++;
+            if ((r = cycle32(0))) return r;
+            k_add_f32<<<cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks, 256, 0, stream>>>(d_z, lev[0].zf, N);
+            launches++;
+            INCRMT_CKL("defect correction");
+            if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
+        }
+        k++;
+        if ((r = fetch_norm(&rn2))) return r;
+        const double rn = std::sqrt(rn2);
+        if (!std::isfinite(rn)) { finite = false; break; }
+        if (rn <= tol) { conv = true; break; }
+    }
+    if (time_it) {
+        INCRMT_CK(cudaEventRecord(ev1, stream));
+        INCRMT_CK(cudaEventSynchronize(ev1));
+    }
+    if (prof && (r = prof_collect())) return r;
+    if (st) {
+        st->vcycles = k;
+        st->rel_res = nb > 0 ? std::sqrt(rn2) / nb : std::sqrt(rn2);
+        float ms = 0;
+        if (time_it) cudaEventElapsedTime(&ms, ev0, ev1);
+        st->device_ms = ms;
+    }
+    if (!finite) { set_error("non-finite residual after %d V-cycles", k); return INCRMT_ERR_NONFINITE; }
+    if (!conv && nb > 0) { set_error("V-cycle failed to converge in %d cycles", k); return INCRMT_ERR_NOCONV; }
+    return INCRMT_OK;
+}
+
+}  // namespace incrmt

@@ -1,0 +1,87 @@
+// Geometric multigrid for the MAC and FEM pressure systems on one B200.
+//
+// Same method as the CPU oracle's TGMG-API shim, so that V-cycle counts are
+// comparable: vertex-style coarsening (coarse I on fine 2I), bilinear
+// prolongation P, restriction P^T, Galerkin coarse operators P^T A P rebuilt
+// on every density change, four-colour Gauss-Seidel smoothing visited as
+// (0,0),(1,1),(1,0),(0,1) (red-black for the 5-point MAC stencil), V(2,2)
+// cycles, and a one-block Gauss-Seidel solve on the coarsest level.
+//
+// Precision. FP64 mode runs everything in double. Mixed mode keeps the outer
+// residual r = b - A z and the update z += e in FP64 and solves A e = r with
+// one FP32 V-cycle per outer iteration (FP32 copies of the fine coefficients
+// and of the Galerkin stencils).
+#pragma once
+#include <vector>
+#include "common.cuh"
+#include "mg_ops.cuh"
+
+namespace incrmt {
+
+struct MgLevel {
+    int m = 0, n = 0;
+    long N = 0;
+    bool kx = false, ky = false;  // whether the next level halves x / y
+    double *z = nullptr, *b = nullptr, *st = nullptr;  // FP64 arrays (level >= 1)
+    float *zf = nullptr, *bf = nullptr, *stf = nullptr;  // FP32 arrays (all levels)
+};
+
+class Multigrid {
+public:
+    int sys = INCRMT_SYS_MAC;
+    int cm = 0, cn = 0;           // cell grid of the simulation
+    int m = 0, n = 0;             // unknowns of the system
+    int px = 0, py = 0, zpr = 0;
+    double dx = 0, dy = 0, xxsp = 0, yysp = 0;
+    double fm = 0, fc = 0, hex = 0, hey = 0;  // FEM stencil constants
+    cudaStream_t stream = nullptr;
+    std::vector<MgLevel> lev;
+    // Fine-level coefficients: MAC ex/ey, FEM cell array c, FP64 and FP32.
+    double *ex = nullptr, *ey = nullptr, *c = nullptr;
+    float *exf = nullptr, *eyf = nullptr, *cf = nullptr;
+    double *rho = nullptr;          // device copy of a host density array
+    double *bbuf = nullptr;          // device right-hand side (host solves, FEM zpr masking)
+    double *zbuf = nullptr;          // device iterate for host solves
+    double *partial = nullptr;       // reduction partials
+    double *hnorm = nullptr;         // pinned host scalars
+    double *dnorm = nullptr;         // device scalars
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    long long launches = 0;
+    bool ready = false;              // coefficients and hierarchy built
+    // Optional timing of the fine-level smoothing launches (the dominant
+    // kernel): CUDA events around each launch on the handle's stream.
+    bool prof = false;
+    std::vector<cudaEvent_t> prof_ev;
+    int prof_used = 0;
+    double prof_ms = 0, prof_bytes = 0;
+    long long prof_launches = 0;
+    double pending_bytes = 0;
+    int prof_begin(double bytes);
+    int prof_end();
+    int prof_collect();
+
+    int create(int sys, int cm, int cn, double ax, double bx, double ay, double by,
+               int px, int py, int zpr);
+    void destroy();
+    int set_density_device(const double *d_rho);
+    int solve_device(const double *d_b, double *d_z, const incrmt_mg_opts *o,
+                     incrmt_mg_stats *st, bool time_it);
+    int vcycle64(const double *d_b, double *d_z);
+    int apply_device(const double *d_z, double *d_out);
+
+    MacOp<double> mac64() const;
+    MacOp<float> mac32() const;
+    FemOp<double> fem64() const;
+    FemOp<float> fem32() const;
+
+private:
+    int build_hierarchy();
+    int galerkin_all();
+    int cycle64(int l, const double *b0, double *z0);
+    int cycle32(int l);
+    int norm2_rhs(const double *b, double *out_dev);
+    int residual_norm(const double *b, const double *z, float *rf, double *out_dev);
+    int fetch_norm(double *v);
+};
+
+}  // namespace incrmt

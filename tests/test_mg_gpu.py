@@ -1,0 +1,144 @@
+"""GPU multigrid parity through the C ABI (libincrmt_gpu.so).
+
+For the MAC and FEM variable-density systems (mgs_mac_varying_rho,
+mgs_fem_varying_rho), the CUDA solve is compared with the oracle (the
+reference's callbacks + the clean-room TGMG shim, live when oracle/_ref is
+built, else the committed golden fixtures it produced):
+  - the residual, recomputed independently by oracle/operators.py, meets the
+    1e-9 relative tolerance;
+  - FP64: the solution agrees with the oracle's to 1e-8 relative (same
+    V-cycle algorithm, differences are rounding only), V-cycle count within 1;
+  - mixed FP32/FP64: same residual target, solution within 1e-6 relative of
+    the oracle's (both meet 1e-9 residual; the difference is bounded by the
+    conditioning), at most 3 more V-cycles;
+  - error behaviour: NaN input, V-cycle cap, warm start.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, oracle_available
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-8
+MIXED_TOL = 1e-6
+
+
+def _problem(sys_, m, zpr):
+    from incrmt_b200 import workloads
+    name = f"mg_{'mac' if sys_ == 0 else 'fem'}_{m}{'_zpr' if zpr else ''}.npz"
+    path = os.path.join(GOLDEN, name)
+    if os.path.exists(path):
+        g = np.load(path)
+        return g["rho"], g["b"], g["b_used"], g["z"], int(g["vcycles"])
+    if sys_ == 0:
+        rho, b = workloads.standalone_mac_problem(m)
+    else:
+        rho, b = workloads.standalone_fem_problem(m)
+    rho, b = rho.numpy(), b.numpy().ravel()
+    if not oracle_available():
+        return rho, b, None, None, None
+    from oracle import refsim
+    z, bu, st = refsim.mg_solve(sys_, m, m, rho, b, zpr=zpr)
+    return rho, b, bu, z, st[0]
+
+
+def _residual(sys_, m, rho, b, z, zpr):
+    from oracle import operators
+    if sys_ == 0:
+        Az = operators.mac_apply(rho, z.reshape(m, m), 2.0 / m, 2.0 / m, zpr)
+    else:
+        Az = operators.fem_apply(rho, z.reshape(m + 1, m + 1), 2.0 / m, 2.0 / m, zpr)
+    return np.linalg.norm(b - Az.ravel()) / np.linalg.norm(b)
+
+
+def _gauge(z, zpr):
+    return z if zpr else z - z.mean()
+
+
+CASES = [(0, 64, False), (1, 64, False), (1, 64, True), (0, 256, False), (1, 256, True)]
+
+
+@pytest.mark.parametrize("sys_,m,zpr", CASES)
+@pytest.mark.parametrize("prec", [0, 1])
+def test_mg_matches_oracle(gpu, sys_, m, zpr, prec):
+    from incrmt_b200 import capi
+    rho, b, b_used, z_ref, k_ref = _problem(sys_, m, zpr)
+    s = capi.MGSolver(sys_, m, m, zpr=zpr)
+    s.set_density(rho)
+    z = np.zeros(s.m_sys * s.n_sys)
+    st = s.solve(b, z, rel_tol=1e-9, precision=prec)
+    bb = b_used if b_used is not None else b
+    if sys_ == 1 and zpr:
+        bb = bb.reshape(m + 1, m + 1).copy()
+        bb[:, m] = 0
+        bb = bb.ravel()
+    assert st.rel_res <= 1e-9
+    assert _residual(sys_, m, rho, bb, z, zpr) <= 1.2e-9
+    if z_ref is None:
+        pytest.skip("no oracle solution at this size")
+    zg, zr = _gauge(z, zpr), _gauge(z_ref, zpr)
+    err = np.linalg.norm(zg - zr) / np.linalg.norm(zr)
+    if prec == 0:
+        assert err <= FP64_TOL, err
+        assert abs(st.vcycles - k_ref) <= 1, (st.vcycles, k_ref)
+    else:
+        assert err <= MIXED_TOL, err
+        assert st.vcycles <= k_ref + 3, (st.vcycles, k_ref)
+    s.close()
+
+
+def test_mg_apply_matches_numpy_operator(gpu):
+    from incrmt_b200 import capi
+    from oracle import operators
+    rng = np.random.default_rng(5)
+    m = 48
+    rho = 1 + 2 * rng.random((m + 4, m + 4))
+    for sys_, zpr in [(0, False), (0, True), (1, False), (1, True)]:
+        s = capi.MGSolver(sys_, m, m, zpr=zpr)
+        s.set_density(rho)
+        z = rng.standard_normal(s.m_sys * s.n_sys)
+        out = s.apply(z)
+        f = operators.mac_apply if sys_ == 0 else operators.fem_apply
+        ref = f(rho, z.reshape(s.n_sys, s.m_sys), 2.0 / m, 2.0 / m, zpr).ravel()
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+        s.close()
+
+
+def test_mg_large_residual_property(gpu):
+    """At 2048^2 the solve meets the tolerance by the independent residual."""
+    from incrmt_b200 import capi, workloads
+    m = 2048
+    rho, b = workloads.standalone_mac_problem(m)
+    rho, b = rho.numpy(), b.numpy().ravel()
+    for prec in (0, 1):
+        s = capi.MGSolver(0, m, m)
+        s.set_density(rho)
+        z = np.zeros(m * m)
+        st = s.solve(b, z, precision=prec)
+        assert st.vcycles <= 12
+        assert _residual(0, m, rho, b, z, False) <= 1.2e-9
+        s.close()
+
+
+def test_mg_errors_and_warm_start(gpu):
+    from incrmt_b200 import capi
+    rho, b, _, _, _ = _problem(0, 64, False)
+    s = capi.MGSolver(0, 64, 64)
+    s.set_density(rho)
+    z = np.zeros(64 * 64)
+    with pytest.raises(capi.IncrmtError) as e:
+        s.solve(b, z, rel_tol=1e-30, max_vcycles=1)
+    assert e.value.code == capi.ERR_NOCONV
+    z = np.zeros(64 * 64)
+    s.solve(b, z)
+    st = s.solve(b, z)  # warm start from the converged solution
+    assert st.vcycles == 1
+    bad = b.copy()
+    bad[100] = np.nan
+    with pytest.raises(capi.IncrmtError) as e:
+        s.solve(bad, np.zeros(64 * 64))
+    assert e.value.code == capi.ERR_NONFINITE
+    s.close()

@@ -1,0 +1,137 @@
+/* incrmt_b200: C ABI of the simulation handle, the B200 replacement of
+ * IncRMT's fluid_2d time integrator (fluid_2d.hh:131-177). Same conventions
+ * as incrmt.h: int status returns, no exit, caller-owned host buffers. The
+ * time step supports domains with walls on all four sides (the simple-spin
+ * and sediment scenarios); periodic domains are rejected with
+ * INCRMT_ERR_BADARG. */
+#ifndef INCRMT_SIM_H
+#define INCRMT_SIM_H
+
+#include "incrmt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct incrmt_sim incrmt_sim;
+
+/** Grid and domain (fluid_2d ctor arguments m, n and sim_type's
+ * ax,bx,ay,by,x_prd,y_prd; fluid_2d.cc:26-43, sim_type.hh:51-55). */
+typedef struct incrmt_grid {
+    int m, n;
+    double ax, bx, ay, by;
+    int x_prd, y_prd;
+} incrmt_grid;
+
+/** Physical and numerical parameters (fluid_2d ctor: visc, rhof, tw, pinw,
+ * ntrace; sim_type w_scale/w_force, default 3 and 20 when <= 0; fluid_2d::zpr;
+ * plus the projection tolerance and precision of this implementation). */
+typedef struct incrmt_phys {
+    double visc, rhof, tw, pinw;
+    double w_scale, w_force;
+    int ntrace;
+    int zpr;
+    int precision;       /* INCRMT_PREC_FP64 or INCRMT_PREC_MIXED for both projections */
+    double mg_rel_tol;   /* relative residual of each projection (default 1e-9 when <= 0) */
+} incrmt_phys;
+
+/** Object kinds (subclasses of object, object.hh). */
+#define INCRMT_OBJ_SIMPLE_SPIN 0  /* params: r_scale, a1, a2, piv_r, th_max, omega (object.hh:447) */
+#define INCRMT_OBJ_CIRCLE      1  /* params: cx, cy, cr, uu, vv, omega, grav (object.hh:128-138) */
+
+/** An object plus its material constants (object*, mat_const;
+ * fluid_2d::add_object, fluid_2d.cc:74-90; obj_field.hh:15-29). */
+typedef struct incrmt_object_desc {
+    int type;
+    double G, rhos, ev_trans_mult;
+    int set_velocity;
+    double params[8];
+} incrmt_object_desc;
+
+/** Field ids for get/set: 0..23 the members of struct field in order
+ * (u,v,p,rho,ux,uy,vx,vy,ud,vd,ul,vl,ur,vr,uu,vu,c0,c1,c2,c3,s11,s12,s21,s22;
+ * fields.hh:7-49); 100..115 the members of struct s_field of object k
+ * (X,Y,nX,nY,Xx,Xy,Yx,Yy,Xd,Yd,Xl,Yl,Xr,Yr,Xu,Yu; fields.hh:51-79). */
+#define INCRMT_FIELD_PHI    200  /* level set of object k */
+#define INCRMT_FIELD_STATUS 201  /* level-set status of object k (as doubles) */
+
+typedef struct incrmt_sim_stats {
+    long long steps;
+    long long vcycles_mac, vcycles_fem;   /* V-cycles summed over all projections */
+    long long solves_mac, solves_fem;
+    long long march_sweeps, extrap_sweeps;
+    long long launches;                    /* kernels issued by this handle */
+    double dt_reg, time;
+} incrmt_sim_stats;
+
+/** Creates the simulation (fluid_2d::fluid_2d, fluid_2d.cc:26-43). */
+int incrmt_create(const incrmt_grid *g, const incrmt_phys *p, incrmt_sim **out);
+
+/** Adds a solid (fluid_2d::add_object, fluid_2d.cc:74-90). */
+int incrmt_add_object(incrmt_sim *h, const incrmt_object_desc *d);
+
+/** Chooses the extra viscosity and time step and initialises every field
+ * (fluid_2d::initialize, fluid_2d.cc:101-122, without the tracer placement;
+ * see incrmt_set_tracers). dt_reg receives fluid_2d::dt_reg. */
+int incrmt_initialize(incrmt_sim *h, double ev_mult, double dt_pad, double dt_ev_pad, double *dt_reg);
+
+/** Places the ntrace passive tracers at host positions (x,y pairs);
+ * fluid_2d::init_tracers (fluid_2d.cc:1377-1386) draws them on the host. */
+int incrmt_set_tracers(incrmt_sim *h, const double *xy);
+
+/** One time step (fluid_2d::step_forward, fluid_2d.cc:298-369). */
+int incrmt_step(incrmt_sim *h, double dt);
+
+/** nsteps time steps, then waits for the device. */
+int incrmt_steps(incrmt_sim *h, double dt, int nsteps);
+
+/** Runs one step function on the current state (for parity tests): 0 tracer
+ * stage 1, 1/2 normal derivatives, 3 Godunov (tangential), 5 tangential
+ * derivatives, 6/7 half-time edge values, 8 Godunov, 9 MAC projection,
+ * 10 update_reference_map, 11 pin, 12 set_boundaries, 13 compute_stress,
+ * 14 compute_ustar, 15 finite_element_projection + copy_pressure,
+ * 17 update_velocity, 18 tracer stage 2, 19 set_rho, 20 a whole step,
+ * 21 build_band, 22 extrapolation. Edge boundary conditions (4) and
+ * copy_pressure (16) are fused into their neighbours and do nothing alone. */
+int incrmt_stage(incrmt_sim *h, int stage, double dt);
+
+/** Copies a ghosted (m+4)x(n+4) field to / from a host array (row-major). */
+int incrmt_get_field(incrmt_sim *h, int id, int k, double *host);
+int incrmt_set_field(incrmt_sim *h, int id, int k, const double *host);
+
+/** Projection arrays (m*n MAC, (m+1)*(n+1) FEM): which = 0 MAC solution
+ * (mgs_base::z of ms_mac, the warm start of the next solve), 1 FEM solution,
+ * 2 MAC right-hand side, 3 FEM right-hand side (fluid_2d::src). */
+int incrmt_get_mg(incrmt_sim *h, int which, double *host);
+int incrmt_set_mg(incrmt_sim *h, int which, const double *host);
+
+int incrmt_get_time(const incrmt_sim *h, double *t);
+int incrmt_set_time(incrmt_sim *h, double t);
+
+/** Passive tracers: ntrace records of 4 doubles (x, y, stage velocity). */
+int incrmt_get_tracers(incrmt_sim *h, double *host);
+
+/** Object-tracked points: records of 6 doubles (x, y, stage velocity, X, Y). */
+int incrmt_get_object_tracers(incrmt_sim *h, double *host, int *count);
+
+/** Tracked-point records collected so far, 5 doubles each: time, position
+ * before and after the correction onto the reference map (obj_track output,
+ * object.cc:202-219). clear=1 empties the list. */
+int incrmt_track_records(incrmt_sim *h, double *host, int cap, int *count, int clear);
+
+/** Adds a tracked-point record now (obj_track::write at frame output,
+ * object.cc:333-336). */
+int incrmt_record_track(incrmt_sim *h);
+
+int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st);
+
+/** The handle's CUDA stream (a cudaStream_t). */
+void *incrmt_sim_stream(const incrmt_sim *h);
+
+void incrmt_destroy(incrmt_sim *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

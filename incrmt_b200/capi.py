@@ -187,3 +187,197 @@ class MGSolver:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Simulation handle (include/incrmt_sim.h): the fluid_2d replacement.
+
+OBJ_SIMPLE_SPIN = 0
+OBJ_CIRCLE = 1
+FIELD_PHI = 200
+FIELD_STATUS = 201
+FIELDS = {n: k for k, n in enumerate(
+    "u v p rho ux uy vx vy ud vd ul vl ur vr uu vu c0 c1 c2 c3 s11 s12 s21 s22".split())}
+SFIELDS = {n: 100 + k for k, n in enumerate(
+    "X Y nX nY Xx Xy Yx Yy Xd Yd Xl Yl Xr Yr Xu Yu".split())}
+STAGES = {n: k for k, n in enumerate([
+    "tracers1", "normal_derivatives_velocity", "normal_derivatives_refmap",
+    "godunov_tang", "edge_boundary_conditions", "tangential_derivatives",
+    "half_time_edge_velocities", "half_time_edge_refmap", "godunov",
+    "mac_projection", "update_reference_map", "pin", "set_boundaries",
+    "compute_stress", "compute_ustar", "finite_element_projection",
+    "copy_pressure", "update_velocity", "tracers2", "set_rho", "step_forward",
+    "build_band", "extrapolate"])}
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_int), ("n", ctypes.c_int), ("ax", ctypes.c_double),
+                ("bx", ctypes.c_double), ("ay", ctypes.c_double), ("by", ctypes.c_double),
+                ("x_prd", ctypes.c_int), ("y_prd", ctypes.c_int)]
+
+
+class Phys(ctypes.Structure):
+    _fields_ = [("visc", ctypes.c_double), ("rhof", ctypes.c_double), ("tw", ctypes.c_double),
+                ("pinw", ctypes.c_double), ("w_scale", ctypes.c_double), ("w_force", ctypes.c_double),
+                ("ntrace", ctypes.c_int), ("zpr", ctypes.c_int), ("precision", ctypes.c_int),
+                ("mg_rel_tol", ctypes.c_double)]
+
+
+class ObjectDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("G", ctypes.c_double), ("rhos", ctypes.c_double),
+                ("ev_trans_mult", ctypes.c_double), ("set_velocity", ctypes.c_int),
+                ("params", ctypes.c_double * 8)]
+
+
+class SimStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("vcycles_mac", ctypes.c_longlong),
+                ("vcycles_fem", ctypes.c_longlong), ("solves_mac", ctypes.c_longlong),
+                ("solves_fem", ctypes.c_longlong), ("march_sweeps", ctypes.c_longlong),
+                ("extrap_sweeps", ctypes.c_longlong), ("launches", ctypes.c_longlong),
+                ("dt_reg", ctypes.c_double), ("time", ctypes.c_double)]
+
+
+def _sim_sigs(L):
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.incrmt_create.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(Phys), ctypes.POINTER(P)]
+    L.incrmt_add_object.argtypes = [P, ctypes.POINTER(ObjectDesc)]
+    L.incrmt_initialize.argtypes = [P, D, D, D, dp]
+    L.incrmt_set_tracers.argtypes = [P, dp]
+    L.incrmt_step.argtypes = [P, D]
+    L.incrmt_steps.argtypes = [P, D, I]
+    L.incrmt_stage.argtypes = [P, I, D]
+    L.incrmt_get_field.argtypes = [P, I, I, dp]
+    L.incrmt_set_field.argtypes = [P, I, I, dp]
+    L.incrmt_get_mg.argtypes = [P, I, dp]
+    L.incrmt_set_mg.argtypes = [P, I, dp]
+    L.incrmt_get_time.argtypes = [P, dp]
+    L.incrmt_set_time.argtypes = [P, D]
+    L.incrmt_get_tracers.argtypes = [P, dp]
+    L.incrmt_get_object_tracers.argtypes = [P, dp, ctypes.POINTER(I)]
+    L.incrmt_track_records.argtypes = [P, dp, I, ctypes.POINTER(I), I]
+    L.incrmt_record_track.argtypes = [P]
+    L.incrmt_get_stats.argtypes = [P, ctypes.POINTER(SimStats)]
+    L.incrmt_sim_stream.argtypes = [P]
+    L.incrmt_sim_stream.restype = P
+    L.incrmt_destroy.argtypes = [P]
+    L.incrmt_destroy.restype = None
+
+
+class Simulation:
+    """A fluid_2d on the GPU (fluid_2d.hh:131-177) through the C ABI."""
+
+    def __init__(self, m, n, ax=-1.0, bx=1.0, ay=-1.0, by=1.0, visc=1e-2, rhof=1.0, tw=2.5,
+                 pinw=2.5, ntrace=512, zpr=False, precision=PREC_FP64, rel_tol=1e-9):
+        L = lib()
+        if not hasattr(L, "_sim_ready"):
+            _sim_sigs(L)
+            L._sim_ready = True
+        g = Grid(m, n, ax, bx, ay, by, 0, 0)
+        p = Phys(visc, rhof, tw, pinw, 0.0, 0.0, ntrace, int(zpr), precision, rel_tol)
+        h = ctypes.c_void_p()
+        check(L.incrmt_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.m, self.n, self.ml, self.nl, self.ntrace = m, n, m + 4, n + 4, ntrace
+        self.dt_reg = None
+
+    def add_simple_spin(self, r_scale=0.8, a1=0.5, a2=0.125, piv_r=0.2, th_max=np.pi, omega=1.0,
+                        G=48.0, rhos=3.0, ev_trans_mult=1.0):
+        d = ObjectDesc(OBJ_SIMPLE_SPIN, G, rhos, ev_trans_mult, 1,
+                       (ctypes.c_double * 8)(r_scale, a1, a2, piv_r, th_max, omega, 0, 0))
+        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+
+    def add_circle(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0):
+        d = ObjectDesc(OBJ_CIRCLE, G, rhos, ev_trans_mult, 1,
+                       (ctypes.c_double * 8)(cx, cy, cr, uu, vv, omega, grav, 0))
+        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+
+    def initialize(self, ev_mult=0.8, dt_pad=0.4, dt_ev_pad=0.8):
+        dt = ctypes.c_double()
+        check(lib().incrmt_initialize(self._h, ev_mult, dt_pad, dt_ev_pad, ctypes.byref(dt)))
+        self.dt_reg = dt.value
+        return self.dt_reg
+
+    def set_tracers(self, xy):
+        xy = np.ascontiguousarray(xy, dtype=np.float64).ravel()
+        check(lib().incrmt_set_tracers(self._h, _dptr(xy)))
+
+    def step(self, dt, steps=1):
+        check(lib().incrmt_steps(self._h, dt, steps))
+
+    def stage(self, name, dt=0.0):
+        check(lib().incrmt_stage(self._h, STAGES[name], dt))
+
+    def _fid(self, name):
+        if isinstance(name, int):
+            return name
+        return FIELDS.get(name, SFIELDS.get(name, {"phi": FIELD_PHI, "status": FIELD_STATUS}.get(name)))
+
+    def get(self, name, k=0):
+        out = np.empty(self.ml * self.nl)
+        check(lib().incrmt_get_field(self._h, self._fid(name), k, _dptr(out)))
+        return out.reshape(self.nl, self.ml)
+
+    def set(self, name, arr, k=0):
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        check(lib().incrmt_set_field(self._h, self._fid(name), k, _dptr(a)))
+
+    def get_mg(self, which):
+        n = self.m * self.n if which in (0, 2) else (self.m + 1) * (self.n + 1)
+        out = np.empty(n)
+        check(lib().incrmt_get_mg(self._h, which, _dptr(out)))
+        return out
+
+    def set_mg(self, which, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        check(lib().incrmt_set_mg(self._h, which, _dptr(a)))
+
+    @property
+    def time(self):
+        t = ctypes.c_double()
+        check(lib().incrmt_get_time(self._h, ctypes.byref(t)))
+        return t.value
+
+    @time.setter
+    def time(self, t):
+        check(lib().incrmt_set_time(self._h, t))
+
+    def tracers(self):
+        out = np.empty(4 * max(self.ntrace, 1))
+        check(lib().incrmt_get_tracers(self._h, _dptr(out)))
+        return out[:4 * self.ntrace].reshape(self.ntrace, 4)
+
+    def object_tracers(self):
+        out = np.empty(6 * 64)
+        c = ctypes.c_int()
+        check(lib().incrmt_get_object_tracers(self._h, _dptr(out), ctypes.byref(c)))
+        return out[:6 * c.value].reshape(c.value, 6)
+
+    def track_records(self, clear=False):
+        c = ctypes.c_int()
+        check(lib().incrmt_track_records(self._h, None, 0, ctypes.byref(c), 0))
+        out = np.empty(5 * max(c.value, 1))
+        check(lib().incrmt_track_records(self._h, _dptr(out), c.value, ctypes.byref(c), int(clear)))
+        return out[:5 * c.value].reshape(c.value, 5)
+
+    def record_track(self):
+        check(lib().incrmt_record_track(self._h))
+
+    def stats(self):
+        s = SimStats()
+        check(lib().incrmt_get_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def stream(self):
+        return lib().incrmt_sim_stream(self._h)
+
+    def close(self):
+        if self._h:
+            lib().incrmt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

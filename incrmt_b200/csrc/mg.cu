@@ -48,10 +48,9 @@ inline bool can_coarsen(int m, int p) { return p ? (m % 2 == 0 && m / 2 >= 4) : 
 
 /** Edge reciprocal densities of the MAC system from the ghosted cell density
  * (fluid_2d::set_edge_irho, fluid_2d.cc:1140-1160). */
-__global__ void k_mac_coef(const double *rho, int cm, int cn, double *ex, double *ey,
+__global__ void k_mac_coef(const double *rho, int ml, int cm, int cn, double *ex, double *ey,
                            float *exf, float *eyf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int ml = cm + 4;
     if (j < cn && i <= cm) {
         const int q = (i + 2) + ml * (j + 2);
         double v = 0.5 / rho[q] + 0.5 / rho[q - 1];
@@ -68,10 +67,9 @@ __global__ void k_mac_coef(const double *rho, int cm, int cn, double *ex, double
 
 /** Cell reciprocal density at each FEM node, the cell below-left of the node
  * (fluid_2d::set_corner_irho, fluid_2d.cc:1163-1170). */
-__global__ void k_fem_coef(const double *rho, int cm, int mf, int nf, double *c, float *cf) {
+__global__ void k_fem_coef(const double *rho, int ml, int mf, int nf, double *c, float *cf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= mf || j >= nf) return;
-    const int ml = cm + 4;
     double v = 1. / rho[(i + 1) + ml * (j + 1)];
     c[j * mf + i] = v;
     cf[j * mf + i] = static_cast<float>(v);
@@ -332,7 +330,7 @@ FemOp<float> Multigrid::fem32() const {
 }
 
 int Multigrid::create(int sys_, int cm_, int cn_, double ax, double bx, double ay, double by,
-                      int px_, int py_, int zpr_) {
+                      int px_, int py_, int zpr_, cudaStream_t ext) {
     if (sys_ != INCRMT_SYS_MAC && sys_ != INCRMT_SYS_FEM) { set_error("unknown system %d", sys_); return INCRMT_ERR_BADARG; }
     if (cm_ < 2 || cn_ < 2 || !(bx > ax) || !(by > ay)) { set_error("bad grid %dx%d", cm_, cn_); return INCRMT_ERR_BADARG; }
     sys = sys_; cm = cm_; cn = cn_; px = px_ ? 1 : 0; py = py_ ? 1 : 0; zpr = zpr_ ? 1 : 0;
@@ -351,7 +349,8 @@ int Multigrid::create(int sys_, int cm_, int cn_, double ax, double bx, double a
     const double fey = 1. / 3. * (-2 * dxdy + dydx), fex = 1. / 3. * (-2 * dydx + dxdy);
     hey = 0.5 * fey; hex = 0.5 * fex;
     fc = -1. / 6. * (dxdy + dydx);
-    INCRMT_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    if (ext) { stream = ext; own_stream = false; }
+    else INCRMT_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     INCRMT_CK(cudaEventCreate(&ev0));
     INCRMT_CK(cudaEventCreate(&ev1));
     const long N = static_cast<long>(m) * n;
@@ -410,14 +409,16 @@ void Multigrid::destroy() {
     prof_ev.clear();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream && own_stream) cudaStreamDestroy(stream);
+    stream = nullptr;
 }
 
-int Multigrid::set_density_device(const double *d_rho) {
+int Multigrid::set_density_device(const double *d_rho, int ld) {
+    if (ld <= 0) ld = cm + 4;
     if (sys == INCRMT_SYS_MAC) {
-        k_mac_coef<<<grid2(cm + 1, cn + 1), kBlk2, 0, stream>>>(d_rho, cm, cn, ex, ey, exf, eyf);
+        k_mac_coef<<<grid2(cm + 1, cn + 1), kBlk2, 0, stream>>>(d_rho, ld, cm, cn, ex, ey, exf, eyf);
     } else {
-        k_fem_coef<<<grid2(m, n), kBlk2, 0, stream>>>(d_rho, cm, m, n, c, cf);
+        k_fem_coef<<<grid2(m, n), kBlk2, 0, stream>>>(d_rho, ld, m, n, c, cf);
     }
     launches++;
     INCRMT_CKL("coefficients");

@@ -60,10 +60,11 @@ public:
     int prof_end();
     int prof_collect();
 
+    bool own_stream = true;
     int create(int sys, int cm, int cn, double ax, double bx, double ay, double by,
-               int px, int py, int zpr);
+               int px, int py, int zpr, cudaStream_t ext = nullptr);
     void destroy();
-    int set_density_device(const double *d_rho);
+    int set_density_device(const double *d_rho, int ld = 0);
     int solve_device(const double *d_b, double *d_z, const incrmt_mg_opts *o,
                      incrmt_mg_stats *st, bool time_it);
     int vcycle64(const double *d_b, double *d_z);

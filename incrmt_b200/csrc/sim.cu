@@ -1,0 +1,804 @@
+// The simulation handle: device state of one fluid_2d, its time step
+// (fluid_2d::step_forward, fluid_2d.cc:298-369) as a sequence of kernels on
+// one stream, and the C ABI that replaces the fluid_2d interface.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <utility>
+#include <vector>
+#include "incrmt_sim.h"
+#include "mg.cuh"
+#include "step_kernels.cuh"
+#include "ls_kernels.cuh"
+#include "tracer_kernels.cuh"
+
+namespace incrmt {
+
+namespace {
+const dim3 kB2(32, 8);
+inline dim3 g2(int m, int n) { return dim3(cdiv(m, 32), cdiv(n, 8)); }
+constexpr int kLsMaxSweeps = 400;       // cap of the fixed-point sweeps of one march
+constexpr int kExtrapMaxSweeps = 1000;  // cap of the extrapolation wavefront sweeps
+constexpr int kSweepBatch = 8;          // sweeps between host checks of the change flag
+}  // namespace
+
+struct Sim {
+    GridDev g{};
+    LsGrid lg{};
+    cudaStream_t stream = nullptr;
+    FluidDev f{};
+    std::vector<double *> allocs;
+    std::vector<ObjDev> obj;
+    std::vector<SolidDev> sol;
+    std::vector<incrmt_object_desc> desc;
+    ObjDev *d_obj = nullptr;
+    SolidDev *d_sol = nullptr;
+    double *src_mac = nullptr, *z_mac = nullptr, *src_fem = nullptr, *z_fem = nullptr;
+    double *ls_a = nullptr, *ls_b = nullptr;       // march / extrapolation buffers (x)
+    double *ls_c = nullptr, *ls_d = nullptr;       // extrapolation buffers (y)
+    int *d_list = nullptr;
+    int *d_flags = nullptr;                         // [0] changed, [1] count, [2] error, [3] tracer flag
+    int *h_flags = nullptr;                         // pinned
+    double *partial = nullptr;
+    double *tm = nullptr, *otm = nullptr;          // passive and object tracers
+    int ntrace = 0, nobjtr = 0;
+    Multigrid mac, fem;
+    incrmt_mg_opts mgo{1e-9, 200, INCRMT_PREC_FP64};
+    double dt_reg = 0, time = 0;
+    double w_scale = 3, w_force = 20, tw = 2.5, pinw = 2.5;
+    bool initialized = false;
+    long long steps = 0;
+    long long vc_mac = 0, vc_fem = 0, solves_mac = 0, solves_fem = 0;
+    long long ls_sweeps = 0, ex_sweeps = 0;
+    long long launches = 0;
+    int track_count = 1;                            // obj_track step counter
+    int t_correction = 1;
+    int pre_stress_objects = 0;
+    std::vector<double> track;                      // records: time, xpre, ypre, x, y
+
+    int alloc(double **p, size_t n) {
+        INCRMT_CK(cudaMalloc(p, sizeof(double) * n));
+        INCRMT_CK(cudaMemsetAsync(*p, 0, sizeof(double) * n, stream));
+        allocs.push_back(*p);
+        return INCRMT_OK;
+    }
+    size_t cells() const { return static_cast<size_t>(g.P) * g.nl; }
+
+    int create(const incrmt_grid *gr, const incrmt_phys *ph);
+    int add_object(const incrmt_object_desc *d);
+    int initialize(double ev_mult, double dt_pad, double dt_ev_pad);
+    int step(double dt);
+    int stage(int s, double dt);
+    void destroy();
+
+    // pieces
+    int upload_objects();
+    void pre_stress_setup(double t);
+    int compute_stress();
+    int set_boundaries();
+    int set_rho();
+    int pin();
+    int build_band(int k);
+    int extrapolate(int k);
+    int mac_projection();
+    int fem_projection(double dt);
+    int update_reference_map(double dt);
+    int tracers(int stage, double dt);
+    int record_track();
+    int fetch_flags();
+};
+
+int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
+    if (gr->m < 8 || gr->n < 8 || !(gr->bx > gr->ax) || !(gr->by > gr->ay)) {
+        set_error("bad grid %dx%d", gr->m, gr->n);
+        return INCRMT_ERR_BADARG;
+    }
+    if (gr->x_prd || gr->y_prd) {
+        set_error("periodic domains are not supported by the time step (walls only)");
+        return INCRMT_ERR_BADARG;
+    }
+    INCRMT_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    g.m = gr->m; g.n = gr->n; g.ml = g.m + 4; g.nl = g.n + 4;
+    g.P = (g.ml + 31) / 32 * 32;
+    g.mf = g.m + 1; g.nf = g.n + 1;
+    g.zpr = ph->zpr ? 1 : 0;
+    g.ax = gr->ax; g.bx = gr->bx; g.ay = gr->ay; g.by = gr->by;
+    g.dx = (g.bx - g.ax) / g.m; g.dy = (g.by - g.ay) / g.n;  // fluid_2d.cc:33-34
+    g.xsp = 1 / g.dx; g.ysp = 1 / g.dy; g.xxsp = g.xsp * g.xsp; g.yysp = g.ysp * g.ysp;
+    g.visc = ph->visc; g.rhof = ph->rhof;
+    tw = ph->tw > 0 ? ph->tw : 2.5;
+    pinw = ph->pinw > 0 ? ph->pinw : 2.5;
+    g.eps = tw * (g.dx < g.dy ? g.dx : g.dy);
+    g.epsinv = 1 / g.eps;
+    g.w_scale = ph->w_scale > 0 ? ph->w_scale : 3.;   // sim_type.hh:13-16
+    g.w_force = ph->w_force > 0 ? ph->w_force : 20.;
+    if (ph->mg_rel_tol > 0) mgo.rel_tol = ph->mg_rel_tol;
+    mgo.precision = ph->precision;
+    ntrace = ph->ntrace > 0 ? ph->ntrace : 0;
+    // Level-set grid (obj_field.cc:18): ghosted grid, origin at cell (-2,-2)'s centre.
+    lg.mL = g.ml; lg.nL = g.nl; lg.P = g.P;
+    lg.axl = g.ax - 1.5 * g.dx; lg.ayl = g.ay - 1.5 * g.dy;
+    lg.dx = g.dx; lg.dy = g.dy; lg.xsp = 1 / g.dx; lg.ysp = 1 / g.dy;
+    lg.phi_up = g.eps + 4.5 * g.dx; lg.phi_down = -g.eps - 4.5 * g.dx;
+    double **fp[] = {&f.u, &f.v, &f.p, &f.rho, &f.ux, &f.uy, &f.vx, &f.vy, &f.ud, &f.vd, &f.ul, &f.vl,
+                     &f.ur, &f.vr, &f.uu, &f.vu, &f.c0, &f.c1, &f.c2, &f.c3, &f.s11, &f.s12, &f.s21, &f.s22};
+    for (double **q : fp) { int r = alloc(q, cells()); if (r) return r; }
+    int r;
+    if ((r = alloc(&src_mac, static_cast<size_t>(g.m) * g.n))) return r;
+    if ((r = alloc(&z_mac, static_cast<size_t>(g.m) * g.n))) return r;
+    if ((r = alloc(&src_fem, static_cast<size_t>(g.mf) * g.nf))) return r;
+    if ((r = alloc(&z_fem, static_cast<size_t>(g.mf) * g.nf))) return r;
+    if ((r = alloc(&ls_a, cells()))) return r;
+    if ((r = alloc(&ls_b, cells()))) return r;
+    if ((r = alloc(&ls_c, cells()))) return r;
+    if ((r = alloc(&ls_d, cells()))) return r;
+    if ((r = alloc(&partial, 4 * kB200SMs))) return r;
+    INCRMT_CK(cudaMalloc(&d_list, sizeof(int) * cells()));
+    INCRMT_CK(cudaMalloc(&d_flags, sizeof(int) * 8));
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 8, stream));
+    INCRMT_CK(cudaMallocHost(&h_flags, sizeof(int) * 8));
+    if (ntrace > 0 && (r = alloc(&tm, 4 * static_cast<size_t>(ntrace)))) return r;
+    if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, 0, g.zpr, stream))) return r;
+    if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, 0, g.zpr, stream))) return r;
+    return INCRMT_OK;
+}
+
+int Sim::add_object(const incrmt_object_desc *d) {
+    if (initialized) { set_error("objects must be added before initialize"); return INCRMT_ERR_BADARG; }
+    if (static_cast<int>(obj.size()) >= kMaxObjects) { set_error("too many objects"); return INCRMT_ERR_BADARG; }
+    if (d->type != INCRMT_OBJ_SIMPLE_SPIN && d->type != INCRMT_OBJ_CIRCLE) {
+        set_error("unknown object type %d", d->type);
+        return INCRMT_ERR_BADARG;
+    }
+    ObjDev o{};
+    o.type = d->type == INCRMT_OBJ_SIMPLE_SPIN ? OBJ_SIMPLE_SPIN : OBJ_CIRCLE;
+    o.set_velocity = d->set_velocity;
+    o.G = d->G; o.rhos = d->rhos; o.ev_trans_mult = d->ev_trans_mult;
+    o.eps = g.eps; o.pinw = pinw * g.dx;  // obj_field.cc:16
+    o.tf1 = 0.5 / g.eps; o.tf2 = 0.5 / M_PI; o.tf3 = M_PI / g.eps;
+    const double *p = d->params;
+    if (o.type == OBJ_SIMPLE_SPIN) {
+        // obj_simple_spin(r_scale,a1,a2,piv_r,th_max,omega) (object.hh:447-453)
+        const double scf = p[0] / (1 + p[1] + p[2]);
+        o.g[0] = scf * (1 - p[2]); o.g[1] = scf * p[1]; o.g[2] = 2 * scf * p[2];
+        o.g[3] = p[3]; o.g[4] = p[4]; o.g[5] = p[5];
+    } else {
+        // obj_circle(cx,cy,cr,uu,vv,omega,grav) (object.hh:128-138)
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[6];
+        o.g[4] = p[3]; o.g[5] = p[4]; o.g[6] = p[5];
+    }
+    SolidDev s{};
+    double **sp[] = {&s.X, &s.Y, &s.nX, &s.nY, &s.Xx, &s.Xy, &s.Yx, &s.Yy, &s.Xd, &s.Yd, &s.Xl, &s.Yl,
+                     &s.Xr, &s.Yr, &s.Xu, &s.Yu, &s.phi, &s.phi_tmp};
+    for (double **q : sp) { int r = alloc(q, cells()); if (r) return r; }
+    INCRMT_CK(cudaMalloc(&s.s, sizeof(int) * cells()));
+    INCRMT_CK(cudaMemsetAsync(s.s, 0, sizeof(int) * cells(), stream));
+    obj.push_back(o);
+    sol.push_back(s);
+    desc.push_back(*d);
+    return INCRMT_OK;
+}
+
+int Sim::upload_objects() {
+    if (!d_obj) {
+        INCRMT_CK(cudaMalloc(&d_obj, sizeof(ObjDev) * kMaxObjects));
+        INCRMT_CK(cudaMalloc(&d_sol, sizeof(SolidDev) * kMaxObjects));
+    }
+    if (obj.empty()) return INCRMT_OK;
+    INCRMT_CK(cudaMemcpyAsync(d_obj, obj.data(), sizeof(ObjDev) * obj.size(), cudaMemcpyHostToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(d_sol, sol.data(), sizeof(SolidDev) * sol.size(), cudaMemcpyHostToDevice, stream));
+    return INCRMT_OK;
+}
+
+/** Per-object state before a stress evaluation (object::pre_stress_setup;
+ * obj_simple_spin, object.cc:185-188). */
+void Sim::pre_stress_setup(double t) {
+    for (auto &o : obj) {
+        if (o.type == OBJ_SIMPLE_SPIN) {
+            double ang = t * o.g[5], theta = ang > 2 * M_PI ? 0 : o.g[4] * (1 - cos(ang));
+            o.cth = cos(theta);
+            o.sth = sin(theta);
+        }
+    }
+}
+
+int Sim::fetch_flags() {
+    INCRMT_CK(cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 8, cudaMemcpyDeviceToHost, stream));
+    INCRMT_CK(cudaStreamSynchronize(stream));
+    return INCRMT_OK;
+}
+
+int Sim::compute_stress() {
+    pre_stress_setup(time);
+    int r = upload_objects();
+    if (r) return r;
+    k_stress<<<g2(g.m + 1, g.n + 1), kB2, 0, stream>>>(g, f, d_obj, d_sol, static_cast<int>(obj.size()));
+    launches++;
+    INCRMT_CKL("k_stress");
+    return INCRMT_OK;
+}
+
+int Sim::set_boundaries() {
+    k_set_boundaries<<<1, 1024, 0, stream>>>(g, f);
+    launches++;
+    INCRMT_CKL("k_set_boundaries");
+    return INCRMT_OK;
+}
+
+int Sim::set_rho() {
+    k_set_rho<<<g2(g.ml, g.nl), kB2, 0, stream>>>(g, f, d_obj, d_sol, static_cast<int>(obj.size()));
+    launches++;
+    INCRMT_CKL("k_set_rho");
+    return INCRMT_OK;
+}
+
+/** levelset::build_band for object k (levelset.cc:199-335). */
+int Sim::build_band(int k) {
+    SolidDev &s = sol[k];
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, stream));
+    k_ls_scan<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.phi, s.s);
+    k_ls_newton<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.phi, s.s, s.phi_tmp, d_flags + 2);
+    k_ls_copy_interface<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, s.phi_tmp, s.phi);
+    k_ls_fim_init<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, ls_a);
+    INCRMT_CK(cudaMemcpyAsync(ls_b, ls_a, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    launches += 4;
+    INCRMT_CKL("level-set scan/newton");
+    double *cur = ls_a, *nxt = ls_b;
+    int sweeps = 0;
+    bool done = false;
+    while (!done && sweeps < kLsMaxSweeps) {
+        INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int), stream));
+        for (int b = 0; b < kSweepBatch; b++) {
+            k_ls_fim_sweep<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.phi, s.s, cur, nxt, d_flags);
+            launches++;
+            std::swap(cur, nxt);
+            sweeps++;
+        }
+        INCRMT_CKL("k_ls_fim_sweep");
+        int r = fetch_flags();
+        if (r) return r;
+        if (h_flags[2]) { set_error("level++: Newton iteration failed."); return h_flags[2]; }
+        // A batch ends with a sweep that changed nothing only if the flag,
+        // cleared at the batch start, stayed down through the whole batch.
+        done = h_flags[0] == 0;
+    }
+    ls_sweeps += sweeps;
+    if (!done) { set_error("level-set march did not settle in %d sweeps", sweeps); return INCRMT_ERR_NOCONV; }
+    k_ls_finish<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, cur, s.s, s.phi);
+    launches++;
+    INCRMT_CKL("k_ls_finish");
+    return INCRMT_OK;
+}
+
+/** obj_field::pin for every object, then set_rho (fluid_2d::pin,
+ * fluid_2d.cc:373-377). */
+int Sim::pin() {
+    int r;
+    for (size_t k = 0; k < obj.size(); k++) {
+        k_pin<<<g2(g.ml, g.nl), kB2, 0, stream>>>(g, obj[k], sol[k]);
+        launches++;
+        INCRMT_CKL("k_pin");
+        if ((r = build_band(static_cast<int>(k)))) return r;
+    }
+    return set_rho();
+}
+
+/** levelset::extrapolate_fields for object k (traverse.hh:235-260). */
+int Sim::extrapolate(int k) {
+    SolidDev &s = sol[k];
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, stream));
+    k_ls_collect_outside<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, d_list, d_flags + 1);
+    launches++;
+    INCRMT_CKL("collect");
+    int r = fetch_flags();
+    if (r) return r;
+    const int count = h_flags[1];
+    if (count == 0) return INCRMT_OK;
+    INCRMT_CK(cudaMemcpyAsync(ls_a, s.nX, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(ls_c, s.nY, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(ls_b, s.nX, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(ls_d, s.nY, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    double *cx = ls_a, *cy = ls_c, *tx = ls_b, *ty = ls_d;
+    int sweeps = 0;
+    bool done = false;
+    while (!done && sweeps < kExtrapMaxSweeps) {
+        INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int), stream));
+        for (int b = 0; b < kSweepBatch; b++) {
+            k_ls_extrap_sweep<<<cdiv(count, 128), 128, 0, stream>>>(lg, s.s, s.phi, s.nX, s.nY, d_list, d_flags + 1,
+                                                                   cx, cy, tx, ty, d_flags, d_flags + 2);
+            launches++;
+            std::swap(cx, tx);
+            std::swap(cy, ty);
+            sweeps++;
+        }
+        INCRMT_CKL("k_ls_extrap_sweep");
+        if ((r = fetch_flags())) return r;
+        if (h_flags[2]) { set_error("singular extrapolation fit"); return h_flags[2]; }
+        done = h_flags[0] == 0;
+    }
+    ex_sweeps += sweeps;
+    if (!done) { set_error("extrapolation did not settle in %d sweeps", sweeps); return INCRMT_ERR_NOCONV; }
+    // Only the listed points changed; copy the whole iterate back.
+    INCRMT_CK(cudaMemcpyAsync(s.nX, cx, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(s.nY, cy, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    return INCRMT_OK;
+}
+
+/** fluid_2d::update_reference_map (fluid_2d.cc:1242-1273). */
+int Sim::update_reference_map(double dt) {
+    for (size_t k = 0; k < obj.size(); k++) {
+        k_refmap_update<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, sol[k], dt);
+        launches++;
+        INCRMT_CKL("k_refmap_update");
+    }
+    int r;
+    for (size_t k = 0; k < obj.size(); k++)
+        if ((r = extrapolate(static_cast<int>(k)))) return r;
+    for (size_t k = 0; k < obj.size(); k++) {
+        k_refmap_half<<<g2(g.m, g.n), kB2, 0, stream>>>(g, sol[k]);
+        launches++;
+        INCRMT_CKL("k_refmap_half");
+    }
+    return INCRMT_OK;
+}
+
+/** fluid_2d::mac_projection (fluid_2d.cc:1175-1236). */
+int Sim::mac_projection() {
+    k_mac_source<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, src_mac);
+    launches++;
+    INCRMT_CKL("k_mac_source");
+    int r = mac.set_density_device(f.rho, g.P);
+    if (r) return r;
+    incrmt_mg_stats st{};
+    long long l0 = mac.launches;
+    r = mac.solve_device(src_mac, z_mac, &mgo, &st, false);
+    launches += mac.launches - l0;
+    vc_mac += st.vcycles;
+    solves_mac++;
+    if (r) return r;
+    k_mac_correct<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, z_mac, mac.ex, mac.ey);
+    launches++;
+    INCRMT_CKL("k_mac_correct");
+    return INCRMT_OK;
+}
+
+/** fluid_2d::finite_element_projection + copy_pressure
+ * (fluid_2d.cc:1297-1328). */
+int Sim::fem_projection(double dt) {
+    k_fem_source<<<g2(g.mf, g.nf), kB2, 0, stream>>>(g, f, src_fem, dt);
+    launches++;
+    INCRMT_CKL("k_fem_source");
+    int r = fem.set_density_device(f.rho, g.P);
+    if (r) return r;
+    incrmt_mg_stats st{};
+    long long l0 = fem.launches;
+    r = fem.solve_device(src_fem, z_fem, &mgo, &st, false);
+    launches += fem.launches - l0;
+    vc_fem += st.vcycles;
+    solves_fem++;
+    if (r) return r;
+    const int nb = 2 * kB200SMs;
+    k_pressure_sum<<<nb, 256, 0, stream>>>(g, z_fem, partial);
+    k_reduce_partials<<<1, 256, 0, stream>>>(partial, nb, partial + nb);
+    k_copy_pressure<<<g2(g.m + 1, g.n + 1), kB2, 0, stream>>>(g, f, z_fem, partial + nb);
+    launches += 3;
+    INCRMT_CKL("copy_pressure");
+    return INCRMT_OK;
+}
+
+int Sim::tracers(int st, double dt) {
+    Field2 vel{f.u, f.v};
+    if (ntrace > 0) {
+        k_tracers<<<cdiv(ntrace, 128), 128, 0, stream>>>(g, vel, tm, ntrace, 4, st, dt, 1, d_flags + 3);
+        launches++;
+    }
+    if (nobjtr > 0) {
+        k_tracers<<<cdiv(nobjtr, 128), 128, 0, stream>>>(g, vel, otm, nobjtr, 6, st, dt, 0, d_flags + 3);
+        launches++;
+    }
+    INCRMT_CKL("k_tracers");
+    if (st == 2 && nobjtr > 0) {
+        // obj_track::update_tracers (object.cc:358-366): a record every 10 steps.
+        if (track_count == 10) return record_track();
+        track_count++;
+    }
+    return INCRMT_OK;
+}
+
+/** obj_track::file_output / obj_simple_spin::file_output (object.cc:202-219,
+ * 339-347): the point before and after its correction onto the reference
+ * map, stored with the time; the host writes track.dat from these. */
+int Sim::record_track() {
+    double pre[2];
+    INCRMT_CK(cudaMemcpyAsync(pre, otm, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+    if (t_correction) {
+        Field2 rm{sol[0].X, sol[0].Y};
+        INCRMT_CK(cudaMemsetAsync(d_flags + 4, 0, sizeof(int), stream));
+        k_correct_tracers<<<1, 32, 0, stream>>>(g, rm, otm, nobjtr, d_flags + 4);
+        launches++;
+        INCRMT_CKL("k_correct_tracers");
+    }
+    double post[2];
+    INCRMT_CK(cudaMemcpyAsync(post, otm, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+    int r = fetch_flags();
+    if (r) return r;
+    if (h_flags[4]) t_correction = 0;
+    track.push_back(time);
+    track.push_back(pre[0]); track.push_back(pre[1]);
+    track.push_back(post[0]); track.push_back(post[1]);
+    track_count = 1;
+    return INCRMT_OK;
+}
+
+int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
+    if (initialized) { set_error("already initialized"); return INCRMT_ERR_BADARG; }
+    // fluid_2d::choose_ev_and_dt (fluid_2d.cc:152-192) and obj_field::set_ex_visc
+    // (obj_field.cc:35-49).
+    const double hmax = g.dx > g.dy ? g.dx : g.dy, hmin = g.dx > g.dy ? g.dy : g.dx;
+    double sws_max = 0, ex_visc_max = 0, rdev_min = 1.7976931348623157e308;
+    for (auto &o : obj) {
+        const double tfac = ev_mult * hmax, sws = sqrt(o.G / o.rhos);
+        if (sws > sws_max) sws_max = sws;
+        o.ex_visc = tfac * o.rhos * sws;
+        if (o.ex_visc > ex_visc_max) ex_visc_max = o.ex_visc;
+        const double r = o.rhos / (o.ex_visc * (o.ev_trans_mult + 1));
+        if (r < rdev_min) rdev_min = r;
+    }
+    const double dt0 = hmin / sws_max * dt_pad, dt1 = 0.5 * rdev_min / (g.xxsp + g.yysp) * dt_ev_pad,
+                 dt2 = 0.5 * g.rhof / (g.visc * (g.xxsp + g.yysp)) * dt_pad;
+    if (dt0 < dt1) dt_reg = dt0 < dt2 ? dt0 : dt2;
+    else dt_reg = dt1 < dt2 ? dt1 : dt2;
+    // object::start (obj_simple_spin::start_extra, object.cc:152-165).
+    for (auto &o : obj) {
+        if (o.type == OBJ_SIMPLE_SPIN) {
+            double t = o.g[3] + o.eps;
+            o.g[6] = t * t;
+            o.g[7] = 0.1 / (dt_reg * dt_reg);
+        }
+    }
+    // Object tracers: obj_simple_spin tracks one point at 0.9*r_scale on the
+    // x axis (object.hh:454-457).
+    nobjtr = 0;
+    if (!obj.empty() && obj[0].type == OBJ_SIMPLE_SPIN) {
+        nobjtr = 1;
+        int r = alloc(&otm, 6);
+        if (r) return r;
+        double h[6] = {0.9 * desc[0].params[0], 0, 0, 0, 0.9 * desc[0].params[0], 0};
+        INCRMT_CK(cudaMemcpyAsync(otm, h, sizeof(h), cudaMemcpyHostToDevice, stream));
+        INCRMT_CK(cudaStreamSynchronize(stream));
+    }
+    int r = upload_objects();
+    if (r) return r;
+    // fluid_2d::init_fields (fluid_2d.cc:195-254).
+    for (size_t k = 0; k < obj.size(); k++) {
+        k_init_object<<<g2(g.ml, g.nl), kB2, 0, stream>>>(g, obj[k], sol[k]);
+        launches++;
+        INCRMT_CKL("k_init_object");
+        if ((r = build_band(static_cast<int>(k)))) return r;
+    }
+    k_init_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, static_cast<int>(obj.size()));
+    launches++;
+    INCRMT_CKL("k_init_velocity");
+    if ((r = set_boundaries())) return r;
+    if ((r = compute_stress())) return r;
+    if ((r = set_rho())) return r;
+    initialized = true;
+    INCRMT_CK(cudaStreamSynchronize(stream));
+    return INCRMT_OK;
+}
+
+/** fluid_2d::step_forward (fluid_2d.cc:298-369). */
+int Sim::step(double dt) {
+    if (!initialized) { set_error("not initialized"); return INCRMT_ERR_BADARG; }
+    const int no = static_cast<int>(obj.size());
+    const double ntime = time + dt;
+    int r;
+    if ((r = tracers(1, dt))) return r;
+    k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
+    k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+    k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f);
+    k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
+    k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+    launches += 5;
+    INCRMT_CKL("advection");
+    time += 0.5 * dt;
+    if ((r = mac_projection())) return r;
+    if ((r = update_reference_map(dt))) return r;
+    if ((r = pin())) return r;
+    if ((r = set_boundaries())) return r;
+    if ((r = compute_stress())) return r;
+    k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
+    launches++;
+    INCRMT_CKL("k_ustar");
+    time = ntime;
+    if ((r = fem_projection(dt))) return r;
+    k_update_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
+    launches++;
+    INCRMT_CKL("k_update_velocity");
+    if ((r = pin())) return r;
+    if ((r = set_boundaries())) return r;
+    if ((r = compute_stress())) return r;
+    if ((r = tracers(2, dt))) return r;
+    steps++;
+    return INCRMT_OK;
+}
+
+/** Runs one reference step function on the current state (same numbering as
+ * the oracle's ref_stage). */
+int Sim::stage(int s, double dt) {
+    const int no = static_cast<int>(obj.size());
+    switch (s) {
+        case 0: return tracers(1, dt);
+        case 1:
+        case 2: k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt); break;
+        case 3: k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no); break;
+        case 4: break;  // fused into the Godunov kernels
+        case 5: k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f); break;
+        case 6:
+        case 7: k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt); break;
+        case 8: k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no); break;
+        case 9: return mac_projection();
+        case 10: return update_reference_map(dt);
+        case 11: return pin();
+        case 12: return set_boundaries();
+        case 13: return compute_stress();
+        case 14: k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt); break;
+        case 15: return fem_projection(dt);
+        case 16: return INCRMT_OK;  // fused into fem_projection
+        case 17: k_update_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt); break;
+        case 18: return tracers(2, dt);
+        case 19: return set_rho();
+        case 20: return step(dt);
+        case 21: for (int k = 0; k < no; k++) { int r = build_band(k); if (r) return r; } return INCRMT_OK;
+        case 22: for (int k = 0; k < no; k++) { int r = extrapolate(k); if (r) return r; } return INCRMT_OK;
+        default: set_error("unknown stage %d", s); return INCRMT_ERR_BADARG;
+    }
+    launches++;
+    INCRMT_CKL("stage");
+    return INCRMT_OK;
+}
+
+void Sim::destroy() {
+    if (stream) cudaStreamSynchronize(stream);
+    mac.destroy();
+    fem.destroy();
+    for (double *p : allocs) cudaFree(p);
+    allocs.clear();
+    for (auto &s : sol) cudaFree(s.s);
+    cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_list); cudaFree(d_flags);
+    if (h_flags) cudaFreeHost(h_flags);
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+}
+
+}  // namespace incrmt
+
+struct incrmt_sim {
+    incrmt::Sim s;
+};
+
+using incrmt::set_error;
+
+namespace {
+
+/** Device array of field id (include/incrmt_sim.h) for object k. */
+double *field_ptr(incrmt::Sim &S, int id, int k) {
+    incrmt::FluidDev &f = S.f;
+    double *fl[] = {f.u, f.v, f.p, f.rho, f.ux, f.uy, f.vx, f.vy, f.ud, f.vd, f.ul, f.vl,
+                    f.ur, f.vr, f.uu, f.vu, f.c0, f.c1, f.c2, f.c3, f.s11, f.s12, f.s21, f.s22};
+    if (id >= 0 && id < 24) return fl[id];
+    if (k < 0 || k >= static_cast<int>(S.sol.size())) return nullptr;
+    incrmt::SolidDev &s = S.sol[k];
+    double *sl[] = {s.X, s.Y, s.nX, s.nY, s.Xx, s.Xy, s.Yx, s.Yy, s.Xd, s.Yd, s.Xl, s.Yl, s.Xr, s.Yr, s.Xu, s.Yu};
+    if (id >= 100 && id < 116) return sl[id - 100];
+    if (id == INCRMT_FIELD_PHI) return s.phi;
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int incrmt_create(const incrmt_grid *g, const incrmt_phys *p, incrmt_sim **out) {
+    if (!g || !p || !out) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    *out = nullptr;
+    incrmt_sim *h = new (std::nothrow) incrmt_sim;
+    if (!h) { set_error("host allocation failed"); return INCRMT_ERR_OOM; }
+    int r = h->s.create(g, p);
+    if (r) { h->s.destroy(); delete h; return r; }
+    *out = h;
+    return INCRMT_OK;
+}
+
+int incrmt_add_object(incrmt_sim *h, const incrmt_object_desc *d) {
+    if (!h || !d) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    return h->s.add_object(d);
+}
+
+int incrmt_initialize(incrmt_sim *h, double ev_mult, double dt_pad, double dt_ev_pad, double *dt_reg) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    int r = h->s.initialize(ev_mult, dt_pad, dt_ev_pad);
+    if (dt_reg) *dt_reg = h->s.dt_reg;
+    return r;
+}
+
+int incrmt_set_tracers(incrmt_sim *h, const double *xy) {
+    if (!h || !xy) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    if (S.ntrace == 0) return INCRMT_OK;
+    std::vector<double> t(4 * static_cast<size_t>(S.ntrace), 0.0);
+    for (int k = 0; k < S.ntrace; k++) { t[4 * k] = xy[2 * k]; t[4 * k + 1] = xy[2 * k + 1]; }
+    INCRMT_CK(cudaMemcpyAsync(S.tm, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_step(incrmt_sim *h, double dt) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    return h->s.step(dt);
+}
+
+int incrmt_steps(incrmt_sim *h, double dt, int nsteps) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    for (int k = 0; k < nsteps; k++) { int r = h->s.step(dt); if (r) return r; }
+    INCRMT_CK(cudaStreamSynchronize(h->s.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_stage(incrmt_sim *h, int stage, double dt) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    int r = h->s.stage(stage, dt);
+    if (r) return r;
+    INCRMT_CK(cudaStreamSynchronize(h->s.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_get_field(incrmt_sim *h, int id, int k, double *host) {
+    if (!h || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    const size_t w = S.g.ml, rows = S.g.nl;
+    if (id == INCRMT_FIELD_STATUS) {
+        if (k < 0 || k >= static_cast<int>(S.sol.size())) { set_error("bad object"); return INCRMT_ERR_BADARG; }
+        std::vector<int> tmp(w * rows);
+        INCRMT_CK(cudaMemcpy2DAsync(tmp.data(), w * sizeof(int), S.sol[k].s, S.g.P * sizeof(int), w * sizeof(int),
+                                    rows, cudaMemcpyDeviceToHost, S.stream));
+        INCRMT_CK(cudaStreamSynchronize(S.stream));
+        for (size_t q = 0; q < w * rows; q++) host[q] = tmp[q];
+        return INCRMT_OK;
+    }
+    double *p = field_ptr(S, id, k);
+    if (!p) { set_error("bad field id %d", id); return INCRMT_ERR_BADARG; }
+    INCRMT_CK(cudaMemcpy2DAsync(host, w * sizeof(double), p, S.g.P * sizeof(double), w * sizeof(double), rows,
+                                cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_set_field(incrmt_sim *h, int id, int k, const double *host) {
+    if (!h || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    const size_t w = S.g.ml, rows = S.g.nl;
+    if (id == INCRMT_FIELD_STATUS) {
+        if (k < 0 || k >= static_cast<int>(S.sol.size())) { set_error("bad object"); return INCRMT_ERR_BADARG; }
+        std::vector<int> tmp(w * rows);
+        for (size_t q = 0; q < w * rows; q++) tmp[q] = static_cast<int>(host[q]);
+        INCRMT_CK(cudaMemcpy2DAsync(S.sol[k].s, S.g.P * sizeof(int), tmp.data(), w * sizeof(int), w * sizeof(int),
+                                    rows, cudaMemcpyHostToDevice, S.stream));
+        INCRMT_CK(cudaStreamSynchronize(S.stream));
+        return INCRMT_OK;
+    }
+    double *p = field_ptr(S, id, k);
+    if (!p) { set_error("bad field id %d", id); return INCRMT_ERR_BADARG; }
+    INCRMT_CK(cudaMemcpy2DAsync(p, S.g.P * sizeof(double), host, w * sizeof(double), w * sizeof(double), rows,
+                                cudaMemcpyHostToDevice, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+namespace {
+double *mg_ptr(incrmt::Sim &S, int which, size_t &n) {
+    const size_t nm = static_cast<size_t>(S.g.m) * S.g.n, nf = static_cast<size_t>(S.g.mf) * S.g.nf;
+    switch (which) {
+        case 0: n = nm; return S.z_mac;
+        case 1: n = nf; return S.z_fem;
+        case 2: n = nm; return S.src_mac;
+        case 3: n = nf; return S.src_fem;
+    }
+    n = 0;
+    return nullptr;
+}
+}  // namespace
+
+int incrmt_get_mg(incrmt_sim *h, int which, double *host) {
+    if (!h || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    size_t n;
+    double *p = mg_ptr(h->s, which, n);
+    if (!p) { set_error("bad array %d", which); return INCRMT_ERR_BADARG; }
+    INCRMT_CK(cudaMemcpyAsync(host, p, sizeof(double) * n, cudaMemcpyDeviceToHost, h->s.stream));
+    INCRMT_CK(cudaStreamSynchronize(h->s.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_set_mg(incrmt_sim *h, int which, const double *host) {
+    if (!h || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    size_t n;
+    double *p = mg_ptr(h->s, which, n);
+    if (!p) { set_error("bad array %d", which); return INCRMT_ERR_BADARG; }
+    INCRMT_CK(cudaMemcpyAsync(p, host, sizeof(double) * n, cudaMemcpyHostToDevice, h->s.stream));
+    INCRMT_CK(cudaStreamSynchronize(h->s.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_get_time(const incrmt_sim *h, double *t) {
+    if (!h || !t) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    *t = h->s.time;
+    return INCRMT_OK;
+}
+
+int incrmt_set_time(incrmt_sim *h, double t) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    h->s.time = t;
+    return INCRMT_OK;
+}
+
+int incrmt_get_tracers(incrmt_sim *h, double *host) {
+    if (!h || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    if (S.ntrace > 0)
+        INCRMT_CK(cudaMemcpyAsync(host, S.tm, sizeof(double) * 4 * S.ntrace, cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_get_object_tracers(incrmt_sim *h, double *host, int *count) {
+    if (!h || !count) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    *count = S.nobjtr;
+    if (host && S.nobjtr > 0)
+        INCRMT_CK(cudaMemcpyAsync(host, S.otm, sizeof(double) * 6 * S.nobjtr, cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_track_records(incrmt_sim *h, double *host, int cap, int *count, int clear) {
+    if (!h || !count) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    const int n = static_cast<int>(S.track.size() / 5);
+    *count = n;
+    if (host) memcpy(host, S.track.data(), sizeof(double) * 5 * (n < cap ? n : cap));
+    if (clear) S.track.clear();
+    return INCRMT_OK;
+}
+
+int incrmt_record_track(incrmt_sim *h) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    if (h->s.nobjtr == 0) return INCRMT_OK;
+    return h->s.record_track();
+}
+
+int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
+    if (!h || !st) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    const incrmt::Sim &S = h->s;
+    st->steps = S.steps;
+    st->vcycles_mac = S.vc_mac;
+    st->vcycles_fem = S.vc_fem;
+    st->solves_mac = S.solves_mac;
+    st->solves_fem = S.solves_fem;
+    st->march_sweeps = S.ls_sweeps;
+    st->extrap_sweeps = S.ex_sweeps;
+    st->launches = S.launches;
+    st->dt_reg = S.dt_reg;
+    st->time = S.time;
+    return INCRMT_OK;
+}
+
+void *incrmt_sim_stream(const incrmt_sim *h) { return h ? static_cast<void *>(h->s.stream) : nullptr; }
+
+void incrmt_destroy(incrmt_sim *h) {
+    if (!h) return;
+    h->s.destroy();
+    delete h;
+}
+
+}  // extern "C"

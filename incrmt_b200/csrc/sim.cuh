@@ -1,0 +1,124 @@
+// Device state and per-point helpers of the time-step kernels.
+//
+// Layout in HBM: structure of arrays, FP64, one array per field of the
+// reference's struct field / struct s_field (fields.hh:7-79), each covering
+// the ghosted (m+4) x (n+4) grid with a row pitch P (>= m+4, a multiple of 32
+// doubles = 256 B so rows start aligned). Cell (i,j), -2 <= i < m+2,
+// -2 <= j < n+2, lives at (j+2)*P + (i+2). The level-set status of each
+// object is an int array with the same layout. The reference's dead r0..r3
+// temporaries (written at fluid_2d.cc:968-971, never read) are not stored.
+#pragma once
+#include <cuda_runtime.h>
+#include <cmath>
+#include "common.cuh"
+
+namespace incrmt {
+
+constexpr int kMaxObjects = 64;
+
+/** Object geometry / forcing kinds (the object subclasses of object.hh). */
+enum ObjType : int {
+    OBJ_SIMPLE_SPIN = 0,  // obj_simple_spin (object.hh:422-467, object.cc:152-219)
+    OBJ_CIRCLE = 1,       // obj_circle (object.hh:128-138, object.cc:22-34)
+};
+
+/** Device description of one solid: material constants (mat_const,
+ * obj_field.hh:15-29), transition-function constants (obj_field.cc:14-20),
+ * geometry parameters and the per-step state of pre_stress_setup. */
+struct ObjDev {
+    int type;
+    int set_velocity;
+    double G, rhos, ev_trans_mult;
+    double eps, pinw, ex_visc;
+    double tf1, tf2, tf3;
+    // Geometry: simple spin {c0, c1, c2, piv_r, th_max, omega, piv_thresh,
+    // K_stiff}; circle {cx, cy, cr, grav, uu, vv, omega}.
+    double g[10];
+    // Per-step state set on the host before each stress evaluation.
+    double cth, sth;
+};
+
+/** Smoothed Heaviside inside the solid or blur zone (obj_field.hh:110-112). */
+__device__ __forceinline__ double trans_func_in(const ObjDev &o, double x) {
+    return x < -o.eps ? 1 : 0.5 - x * o.tf1 - o.tf2 * sin(o.tf3 * x);
+}
+__device__ __forceinline__ double trans_func(const ObjDev &o, double x) {
+    return x > o.eps ? 0 : trans_func_in(o, x);
+}
+/** eps times the transition derivative (obj_field.hh:118-120). */
+__device__ __forceinline__ double tderiv_func_in(const ObjDev &o, double x) {
+    return x < -o.eps ? 0 : 0.5 * (1 + cos(M_PI * x / o.eps));
+}
+__device__ __forceinline__ double coll_func(const ObjDev &o, double x) {
+    return x > o.eps ? 0 : 0.5 - x * o.tf1;
+}
+
+/** Level-set function of the object at reference-map position (X,Y). */
+__device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
+    if (o.type == OBJ_SIMPLE_SPIN) {  // object.cc:177-180
+        double th = atan2(Y, X), c = cos(3 * th);
+        return sqrt(X * X + Y * Y) - o.g[0] - c * (o.g[1] + o.g[2] * c);
+    }
+    return sqrt(X * X + Y * Y) - o.g[2];  // obj_circle::phi, object.cc:22-24
+}
+
+/** Initial reference map (object::transform / obj_standard::transform). */
+__device__ __forceinline__ void obj_transform(const ObjDev &o, double x, double y, double &X, double &Y) {
+    if (o.type == OBJ_CIRCLE) { X = x - o.g[0]; Y = y - o.g[1]; }
+    else { X = x; Y = y; }
+}
+
+/** Initial solid velocity (object::velocity / obj_standard::velocity,
+ * object.cc:13-16). */
+__device__ __forceinline__ void obj_velocity(const ObjDev &o, double X, double Y, double &u, double &v) {
+    if (o.type == OBJ_CIRCLE) { u = o.g[4] - o.g[6] * Y; v = o.g[5] + o.g[6] * X; }
+    else { u = 0; v = 0; }
+}
+
+/** Extra accelerations (object::accel overrides): the simple spinner's
+ * rotating pivot (object.cc:189-197) and the circle's gravity
+ * (object.cc:31-34). */
+__device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, double X, double Y,
+                                          double phiv, double &ax, double &ay) {
+    if (o.type == OBJ_SIMPLE_SPIN) {
+        double rsq = x * x + y * y;
+        if (rsq < o.g[6]) {
+            double rx = X * o.cth - Y * o.sth, ry = X * o.sth + Y * o.cth,
+                   K = o.g[7] * trans_func_in(o, sqrt(rsq) - o.g[3]);
+            ax -= K * (x - rx);
+            ay -= K * (y - ry);
+        }
+    } else {
+        ay -= o.g[3] * trans_func_in(o, phiv);
+    }
+}
+
+/** Grid constants (fluid_2d.hh:32-99). */
+struct GridDev {
+    int m, n, ml, nl, P;
+    int mf, nf;  // FEM nodes
+    int zpr;
+    double ax, bx, ay, by, dx, dy, xsp, ysp, xxsp, yysp;
+    double visc, rhof, eps, epsinv, w_scale, w_force;
+    __device__ __forceinline__ int idx(int i, int j) const { return (j + 2) * P + (i + 2); }
+};
+
+/** Fluid fields (struct field, fields.hh:7-49). */
+struct FluidDev {
+    double *u, *v, *p, *rho;
+    double *ux, *uy, *vx, *vy;
+    double *ud, *vd, *ul, *vl, *ur, *vr, *uu, *vu;
+    double *c0, *c1, *c2, *c3;
+    double *s11, *s12, *s21, *s22;
+};
+
+/** Fields of one solid (struct s_field, fields.hh:51-79, plus the level set). */
+struct SolidDev {
+    double *X, *Y, *nX, *nY;
+    double *Xx, *Xy, *Yx, *Yy;
+    double *Xd, *Yd, *Xl, *Yl, *Xr, *Yr, *Xu, *Yu;
+    double *phi, *phi_tmp;
+    int *s;
+};
+
+}  // namespace incrmt

@@ -1,7 +1,14 @@
 """Benchmark of incrmt_b200 on one node; prints ONE JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mac4096] [--precision fp64|mixed]
+                    [--workload sspin1024|mac4096] [--precision fp64|mixed]
+
+Workload "sspin1024" (default): the ftest simple-spin scenario (three-pronged
+neo-Hookean rotor in a walled [-1,1]^2 box, ftest.cc:116-143) on a 1024 x 1024
+grid. One step = fluid_2d::step_forward (fluid_2d.cc:298-369) with the step
+size solve(2*pi,120) uses; the state starts from the scenario's own
+initialisation. Every field array is 8.4 MB (the ~60 arrays together exceed
+the 126 MB L2), and each step streams them, so no flush is added.
 
 Workload "mac4096": the standalone variable-density MAC pressure solve on a
 4096 x 4096 cell grid (8 seeded circles at density ratio 3, right-hand side
@@ -149,11 +156,46 @@ def cpu_reference_mac(m, steps, warmup, seed=3):
     return steps / dt, dt, float(np.mean(vc)) if vc else 0.0
 
 
+def cpu_reference_sspin(m, steps, warmup):
+    """The reference's own step on the host cores: oracle/_ref/ref_run."""
+    from oracle import refsim
+    if not refsim.available():
+        refsim.build()
+    with tempfile.TemporaryDirectory() as td:
+        out = subprocess.run([refsim.RUN, str(m), str(steps), str(warmup), os.path.join(td, "sspin")],
+                             capture_output=True, text=True, check=True).stdout
+    last = [l for l in out.splitlines() if l and not l.startswith("#")][-1].split()
+    nsteps, secs, vm, vf, threads = int(last[0]), float(last[1]), int(last[2]), int(last[3]), int(last[4])
+    return nsteps / secs, secs, (vm + vf) / (2.0 * nsteps), threads
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
     threads = os.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    if args.workload == "sspin1024":
+        m = 1024
+        try:
+            sps, dt, vc, thr = cpu_reference_sspin(m, args.steps, args.warmup)
+        except Exception as e:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"}))
+            return
+        line = {
+            "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"simple-spin {m}x{m} fluid_2d::step_forward, dt of solve(2pi,120)",
+                       "flush": "working set larger than L2"},
+            "vcycles_per_projection": vc,
+            "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
+                             "sample": f"{args.steps} steps after {args.warmup} warm-up steps at {m}x{m}, "
+                                       f"reference sources + TGMG-API shim, OMP threads = {thr}"},
+            "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
     m = 4096
     try:
         sps, dt, vc = cpu_reference_mac(m, args.steps, args.warmup)
@@ -178,9 +220,100 @@ def run_reference(args, ws, rank):
 # ---------------------------------------------------------------------------
 # GPU path
 
+def run_ours_sspin(args, ws, rank, local, dist):
+    """Simple-spin steps on the GPU through the simulation C ABI."""
+    import torch
+    from incrmt_b200 import capi
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    m = 1024
+    prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    sim = capi.Simulation(m, m, ntrace=512, precision=prec)
+    sim.add_simple_spin()
+    dt_reg = sim.initialize()
+    rng = np.random.default_rng(1 + rank)
+    sim.set_tracers(rng.uniform(-1, 1, size=(512, 2)))
+    interval = 2 * np.pi / 120
+    l = int(interval / dt_reg) + 1
+    dt = interval / l
+    ext = torch.cuda.ExternalStream(sim.stream(), device=dev)
+    sim.step(dt, args.warmup)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    torch.cuda.synchronize()
+    st0 = sim.stats()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        sim.step(dt, args.steps)
+        e1.record(ext)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st1 = sim.stats()
+    _barrier(dist)
+    torch.cuda.synchronize()
+    ms_max = _max_over_ranks(dist, ms)
+    value = ws * args.steps / (ms_max / 1e3)
+    vc = ((st1.vcycles_mac - st0.vcycles_mac) + (st1.vcycles_fem - st0.vcycles_fem)) / (2.0 * args.steps)
+
+    # End to end through the C ABI as fluid_2d::solve drives it: the steps of
+    # one frame, then the frame's fields copied to host buffers (p, u, v for
+    # the vorticity, X, Y, phi; fluid_2d::write_files, fluid_2d_io.cc:60-102).
+    frame_fields = ["p", "u", "v", "X", "Y", "phi"]
+    _barrier(dist)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.step(dt, args.steps)
+    host = [sim.get(f) for f in frame_fields]
+    e2e_s = time.perf_counter() - t0
+    e2e_s = _max_over_ranks(dist, e2e_s)
+    e2e = ws * args.steps / e2e_s
+    d2h = sum(h.nbytes for h in host)
+
+    if rank != 0:
+        return
+    cpu = None
+    if ws == 1 and not args.no_cpu_baseline:
+        try:
+            sps, dts, vcr, thr = cpu_reference_sspin(m, 4, 1)
+            cpu = {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
+                   "sample": f"4 steps after 1 warm-up step at {m}x{m} (reference sources + "
+                             f"TGMG-API shim), OMP threads = {thr}"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == capi.PREC_FP64 else "f64 state, f32 V-cycles in f64 defect correction",
+        "data": "synthetic",
+        "config": {"workload": f"simple-spin {m}x{m} fluid_2d::step_forward, dt of solve(2pi,120)",
+                   "precision": args.precision, "flush": "working set larger than L2",
+                   "parallelism": f"replicas x{ws}"},
+        "vcycles_per_projection": vc,
+        "march_sweeps_per_step": (st1.march_sweeps - st0.march_sweeps) / args.steps,
+        "extrap_sweeps_per_step": (st1.extrap_sweeps - st0.extrap_sweeps) / args.steps,
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(d2h / args.steps),
+                "note": "one frame of fields (p,u,v,X,Y,phi) copied to host per timed run"},
+        "gpu_launches": int(st1.launches - st0.launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    sim.close()
+
+
 def run_ours(args, ws, rank, local, dist):
     import torch
     from incrmt_b200 import capi, workloads
+    if args.workload == "sspin1024":
+        return run_ours_sspin(args, ws, rank, local, dist)
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -291,10 +424,10 @@ def run_ours(args, ws, rank, local, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mac4096", choices=["mac4096"])
+    ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -106,6 +106,8 @@ int incrmt_get_mg(incrmt_sim *h, int which, double *host);
 int incrmt_set_mg(incrmt_sim *h, int which, const double *host);
 
 int incrmt_get_time(const incrmt_sim *h, double *t);
+/** Sets the simulation time; also re-evaluates the objects' time-dependent
+ * state (object::pre_stress_setup) at that time. */
 int incrmt_set_time(incrmt_sim *h, double t);
 
 /** Passive tracers: ntrace records of 4 doubles (x, y, stage velocity). */

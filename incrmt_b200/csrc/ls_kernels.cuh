@@ -26,6 +26,7 @@
 // that stops when no value changes; the dependency depth is ~65 for the
 // ~7-cell-wide band, independent of the grid size.
 #pragma once
+#include <cooperative_groups.h>
 #include "sim.cuh"
 
 namespace incrmt {
@@ -506,10 +507,9 @@ __global__ void k_ls_fim_sweep(LsGrid g, const double *phi, const int *s, const 
     if (v != old) atomicExch(changed, 1);
 }
 
-/** Final statuses and clean-up (heap::march acceptance, levelset::clean,
+/** Final values and clean-up (heap::march acceptance, levelset::clean,
  * levelset.cc:408-413): far points whose value fell inside the band limit are
- * accepted (5 / 2), those reached but beyond it are trial (6 / 1), and every
- * point outside the band is set to the band limit. */
+ * accepted (5 / 2); every point outside the band is set to the band limit. */
 __global__ void k_ls_finish(LsGrid g, const double *cur, int *s, double *phi) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
@@ -517,11 +517,31 @@ __global__ void k_ls_finish(LsGrid g, const double *cur, int *s, double *phi) {
     const double v = cur[ij];
     if (st == 7) {
         if (v < g.phi_up) { s[ij] = 5; phi[ij] = v; }
-        else { s[ij] = v < kUnset ? 6 : 7; phi[ij] = g.phi_up; }
+        else phi[ij] = g.phi_up;
     } else if (st == 0) {
         if (v > g.phi_down) { s[ij] = 2; phi[ij] = v; }
-        else { s[ij] = v > -kUnset ? 1 : 0; phi[ij] = g.phi_down; }
+        else phi[ij] = g.phi_down;
     }
+}
+
+/** Trial statuses (heap::check_gridpoint / update, heap.cc:38-44,159-167):
+ * a far point next to an interface or accepted point of its side was put on
+ * the heap and, not being accepted, stays trial (6 / 1). */
+__global__ void k_ls_trial(LsGrid g, const int *s, int *s_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.mL || j >= g.nL) return;
+    const int ij = j * g.P + i, st = s[ij];
+    int out = st;
+    if (st == 7 || st == 0) {
+        const int lo = st == 7 ? 4 : 2, hi = st == 7 ? 5 : 3;
+        bool nb = false;
+        if (i > 0) nb |= s[ij - 1] >= lo && s[ij - 1] <= hi;
+        if (i < g.mL - 1) nb |= s[ij + 1] >= lo && s[ij + 1] <= hi;
+        if (j > 0) nb |= s[ij - g.P] >= lo && s[ij - g.P] <= hi;
+        if (j < g.nL - 1) nb |= s[ij + g.P] >= lo && s[ij + g.P] <= hi;
+        if (nb) out = st == 7 ? 6 : 1;
+    }
+    s_out[ij] = out;
 }
 
 /** Weighted least-squares extrapolation of (nX,nY) at one band point outside
@@ -593,6 +613,119 @@ __global__ void k_ls_collect_outside(LsGrid g, const int *s, int *list, int *cou
     if (i >= g.mL || j >= g.nL) return;
     const int ij = j * g.P + i, st = s[ij];
     if (st == 4 || st == 5) list[atomicAdd(count, 1)] = ij;
+}
+
+}  // namespace incrmt
+
+namespace incrmt {
+
+/** Marks the points next to the interface (status 3 or 4) as 1 in mark. */
+__global__ void k_ls_mark_interface(LsGrid g, const int *s, int *mark) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.mL || j >= g.nL) return;
+    const int ij = j * g.P + i, st = s[ij];
+    mark[ij] = (st == 3 || st == 4) ? 1 : 0;
+}
+
+/** One direction of a separable dilation by radius R (max over a window). */
+template <bool ALONG_X>
+__global__ void k_ls_dilate(LsGrid g, const int *in, int *out, int R) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.mL || j >= g.nL) return;
+    int v = 0;
+    if (ALONG_X) {
+        const int lo = i - R < 0 ? 0 : i - R, hi = i + R >= g.mL ? g.mL - 1 : i + R;
+        for (int a = lo; a <= hi && !v; a++) v = in[j * g.P + a];
+    } else {
+        const int lo = j - R < 0 ? 0 : j - R, hi = j + R >= g.nL ? g.nL - 1 : j + R;
+        for (int b = lo; b <= hi && !v; b++) v = in[b * g.P + i];
+    }
+    out[j * g.P + i] = v;
+}
+
+/** Lists the far points (status 0 or 7) inside the dilated interface region:
+ * the only points the march can reach within the band limit. */
+__global__ void k_ls_collect_candidates(LsGrid g, const int *s, const int *near, int *list, int *count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.mL || j >= g.nL) return;
+    const int ij = j * g.P + i, st = s[ij];
+    if ((st == 0 || st == 7) && near[ij]) list[atomicAdd(count, 1)] = ij;
+}
+
+/** All sweeps of the march fixed point in one cooperative launch: every
+ * sweep evaluates the stencil at the listed candidates (Jacobi, reading cur,
+ * writing nxt), a grid barrier follows, and the loop ends after the first
+ * sweep that changed nothing. flags[0..2] rotate as per-sweep change flags;
+ * flags[3] receives the number of sweeps and flags[4] 1 if converged. */
+__global__ void k_ls_fim_coop(LsGrid g, const double *phi, const int *s, double *a, double *b, const int *list,
+                              const int *countp, int *flags, int max_sweeps) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const int count = *countp;
+    double *cur = a, *nxt = b;
+    int it = 0;
+    bool done = false;
+    for (; it < max_sweeps; it++) {
+        if (tid == 0) flags[(it + 1) % 3] = 0;
+        bool ch = false;
+        for (int t = tid; t < count; t += nth) {
+            const int ij = list[t], i = ij % g.P, j = ij / g.P, st = s[ij];
+            const double old = cur[ij];
+            double v = old;
+            if (st == 7) {
+                March<true> mr(g, phi, s, cur, old);
+                if (any_in(mr, i, j)) v = mr.calc(i, j);
+            } else {
+                March<false> mr(g, phi, s, cur, old);
+                if (any_in(mr, i, j)) v = mr.calc(i, j);
+            }
+            nxt[ij] = v;
+            if (v != old) ch = true;
+        }
+        if (ch) atomicExch(&flags[it % 3], 1);
+        grid.sync();
+        const int c = atomicAdd(&flags[it % 3], 0);
+        double *t = cur; cur = nxt; nxt = t;
+        if (!c) { done = true; break; }
+    }
+    if (tid == 0) { flags[3] = done ? it + 1 : it; flags[4] = done ? 1 : 0; }
+}
+
+/** All sweeps of the extrapolation wavefront in one cooperative launch (same
+ * scheme as k_ls_fim_coop); flags[5] is raised for a singular fit. */
+__global__ void k_ls_extrap_coop(LsGrid g, const int *s, const double *phi, const double *nX, const double *nY,
+                                 const int *list, const int *countp, double *ax_, double *ay_, double *bx_,
+                                 double *by_, int *flags, int max_sweeps) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const int count = *countp;
+    double *cx = ax_, *cy = ay_, *tx = bx_, *ty = by_;
+    int it = 0;
+    bool done = false;
+    for (; it < max_sweeps; it++) {
+        if (tid == 0) flags[(it + 1) % 3] = 0;
+        bool ch = false;
+        for (int t = tid; t < count; t += nth) {
+            const int ij = list[t], i = ij % g.P, j = ij / g.P;
+            double ox, oy;
+            if (!ls_extrap_point(g, s, phi, nX, nY, cx, cy, i, j, ox, oy)) {
+                atomicExch(&flags[5], INCRMT_ERR_EXTRAP_SINGULAR);
+                ox = cx[ij]; oy = cy[ij];
+            }
+            if (ox != cx[ij] || oy != cy[ij]) ch = true;
+            tx[ij] = ox;
+            ty[ij] = oy;
+        }
+        if (ch) atomicExch(&flags[it % 3], 1);
+        grid.sync();
+        const int c = atomicAdd(&flags[it % 3], 0);
+        double *t1 = cx; cx = tx; tx = t1;
+        double *t2 = cy; cy = ty; ty = t2;
+        if (!c) { done = true; break; }
+    }
+    if (tid == 0) { flags[3] = done ? it + 1 : it; flags[4] = done ? 1 : 0; }
 }
 
 }  // namespace incrmt

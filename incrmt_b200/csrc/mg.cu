@@ -218,6 +218,109 @@ __global__ void k_coarse(Op op, T *z, const T *b, int m, int n, int sweeps) {
     }
 }
 
+/** Levels handled by the one-block tail kernel. */
+constexpr int kTailMaxLevels = 12;
+constexpr int kTailMaxSize = 4096;  // unknowns of the first tail level at most
+
+template <class T>
+struct TailLevels {
+    int first, count, px, py;
+    int m[kTailMaxLevels], n[kTailMaxLevels];
+    long N[kTailMaxLevels];
+    bool kx[kTailMaxLevels], ky[kTailMaxLevels];
+    T *z[kTailMaxLevels];
+    T *b[kTailMaxLevels];
+    const T *st[kTailMaxLevels];
+};
+
+template <class T>
+__device__ __forceinline__ GenOp<T> tail_op(const TailLevels<T> &L, int l) {
+    GenOp<T> g; g.m = L.m[l]; g.n = L.n[l]; g.px = L.px; g.py = L.py; g.N = L.N[l]; g.st = L.st[l];
+    return g;
+}
+
+template <class T>
+__device__ void tail_smooth(const TailLevels<T> &L, int l, int sweeps) {
+    const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
+    const GenOp<T> op = tail_op(L, l);
+    const int m = L.m[l], n = L.n[l];
+    T *z = L.z[l];
+    const T *b = L.b[l];
+    for (int s = 0; s < sweeps; s++)
+        for (int c = 0; c < 4; c++) {
+            const int mc = (m - pis[c] + 1) / 2, nc = (n - pjs[c] + 1) / 2;
+            for (int p = threadIdx.x; p < mc * nc; p += blockDim.x) {
+                const int i = 2 * (p % mc) + pis[c], j = 2 * (p / mc) + pjs[c];
+                T diag;
+                const T off = op.offdiag(i, j, z, diag);
+                z[i + m * j] = (b[i + m * j] - off) / diag;
+            }
+            __syncthreads();
+        }
+}
+
+/** The V-cycle below (and including) level L.first in one block: smoothing,
+ * restriction and prolongation of every tail level with block barriers
+ * between phases, and the coarsest solve. The levels are small enough to sit
+ * in L2, so the cost is the barriers rather than launches. */
+template <class T>
+__global__ void __launch_bounds__(1024) k_tail(TailLevels<T> L, int nu1, int nu2, int coarse_sweeps) {
+    const int last = L.count - 1;
+    for (int l = 0; l < last; l++) {
+        tail_smooth(L, l, nu1);
+        const GenOp<T> op = tail_op(L, l);
+        const int fm = L.m[l], fn = L.n[l], cm = L.m[l + 1], cn = L.n[l + 1];
+        for (int q = threadIdx.x; q < cm * cn; q += blockDim.x) {
+            const int I = q % cm, J = q / cm;
+            int fx[3], fy[3];
+            const int nfx = support(I, fm, L.px, L.kx[l], fx), nfy = support(J, fn, L.py, L.ky[l], fy);
+            T t = 0;
+            for (int bq = 0; bq < nfy; bq++) {
+                const T wy = static_cast<T>(pw(fy[bq], J, fn, cn, L.py, L.ky[l]));
+                for (int a = 0; a < nfx; a++) {
+                    const int f = fx[a] + fm * fy[bq];
+                    T diag;
+                    const T off = op.offdiag(fx[a], fy[bq], L.z[l], diag);
+                    const T r = L.b[l][f] - off - diag * L.z[l][f];
+                    t += wy * static_cast<T>(pw(fx[a], I, fm, cm, L.px, L.kx[l])) * r;
+                }
+            }
+            L.b[l + 1][q] = t;
+            L.z[l + 1][q] = 0;
+        }
+        __syncthreads();
+    }
+    tail_smooth(L, last, coarse_sweeps);
+    for (int l = last - 1; l >= 0; l--) {
+        const int fm = L.m[l], fn = L.n[l], cm = L.m[l + 1], cn = L.n[l + 1];
+        for (int q = threadIdx.x; q < fm * fn; q += blockDim.x) {
+            const int i = q % fm, j = q / fm;
+            int Is[2], Js[2], ni = 0, nj = 0;
+            if (!L.kx[l]) Is[ni++] = i;
+            else {
+                const int lo = (i % 2 == 0) ? i / 2 : (i - 1) / 2;
+                Is[ni++] = lo;
+                if (i % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cm, L.px, ok); if (ok) Is[ni++] = hi; }
+            }
+            if (!L.ky[l]) Js[nj++] = j;
+            else {
+                const int lo = (j % 2 == 0) ? j / 2 : (j - 1) / 2;
+                Js[nj++] = lo;
+                if (j % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cn, L.py, ok); if (ok) Js[nj++] = hi; }
+            }
+            T t = 0;
+            for (int bq = 0; bq < nj; bq++) {
+                const T wy = static_cast<T>(pw(j, Js[bq], fn, cn, L.py, L.ky[l]));
+                for (int a = 0; a < ni; a++)
+                    t += wy * static_cast<T>(pw(i, Is[a], fm, cm, L.px, L.kx[l])) * L.z[l + 1][Is[a] + cm * Js[bq]];
+            }
+            L.z[l][q] += t;
+        }
+        __syncthreads();
+        tail_smooth(L, l, nu2);
+    }
+}
+
 /** FP64 residual r = b - A z, optionally stored in FP32, with per-block sums
  * of r^2 in partial[blockIdx.x]. Grid-stride over the unknowns. */
 template <class Op>
@@ -394,6 +497,10 @@ int Multigrid::build_hierarchy() {
         lev.push_back(L);
         mm = mc; nn = nc;
     }
+    // First level small enough for the one-block tail kernel (never level 0).
+    tail_level = -1;
+    for (int l = 1; l < static_cast<int>(lev.size()); l++)
+        if (lev[l].N <= kTailMaxSize && static_cast<int>(lev.size()) - l <= kTailMaxLevels) { tail_level = l; break; }
     return INCRMT_OK;
 }
 
@@ -405,6 +512,7 @@ void Multigrid::destroy() {
     cudaFree(ex); cudaFree(ey); cudaFree(exf); cudaFree(eyf); cudaFree(c); cudaFree(cf);
     cudaFree(rho); cudaFree(bbuf); cudaFree(zbuf); cudaFree(partial); cudaFree(dnorm);
     if (hnorm) cudaFreeHost(hnorm);
+    if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
     for (auto e : prof_ev) cudaEventDestroy(e);
     prof_ev.clear();
     if (ev0) cudaEventDestroy(ev0);
@@ -447,6 +555,7 @@ int Multigrid::galerkin_all() {
 }
 
 int Multigrid::cycle64(int l, const double *b0, double *z0) {
+    if (l > 0 && l == tail_level) return tail64();
     const MgLevel &L = lev[l];
     const double *b = l == 0 ? b0 : L.b;
     double *z = l == 0 ? z0 : L.z;
@@ -529,6 +638,7 @@ int Multigrid::prof_collect() {
 }
 
 int Multigrid::cycle32(int l) {
+    if (l > 0 && l == tail_level) return tail32();
     const MgLevel &L = lev[l];
     const float *b = L.bf;
     float *z = L.zf;
@@ -568,6 +678,34 @@ int Multigrid::cycle32(int l) {
     return smooth(g, z, b, L.m, L.n, kNu2, stream, launches);
 }
 
+int Multigrid::tail64() {
+    TailLevels<double> T{};
+    T.first = tail_level; T.count = static_cast<int>(lev.size()) - tail_level; T.px = px; T.py = py;
+    for (int k = 0; k < T.count; k++) {
+        const MgLevel &L = lev[tail_level + k];
+        T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
+        T.z[k] = L.z; T.b[k] = L.b; T.st[k] = L.st;
+    }
+    k_tail<double><<<1, 1024, 0, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
+    launches++;
+    INCRMT_CKL("k_tail");
+    return INCRMT_OK;
+}
+
+int Multigrid::tail32() {
+    TailLevels<float> T{};
+    T.first = tail_level; T.count = static_cast<int>(lev.size()) - tail_level; T.px = px; T.py = py;
+    for (int k = 0; k < T.count; k++) {
+        const MgLevel &L = lev[tail_level + k];
+        T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
+        T.z[k] = L.zf; T.b[k] = L.bf; T.st[k] = L.stf;
+    }
+    k_tail<float><<<1, 1024, 0, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
+    launches++;
+    INCRMT_CKL("k_tail");
+    return INCRMT_OK;
+}
+
 int Multigrid::norm2_rhs(const double *b, double *out_dev) {
     const long N = static_cast<long>(m) * n;
     const int nb = cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks;
@@ -593,6 +731,29 @@ int Multigrid::fetch_norm(double *v) {
     INCRMT_CK(cudaMemcpyAsync(hnorm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, stream));
     INCRMT_CK(cudaStreamSynchronize(stream));
     *v = hnorm[0];
+    return INCRMT_OK;
+}
+
+/** One V-cycle (FP64, or one FP32 defect-correction step in mixed mode),
+ * the FP64 residual norm of the new iterate, and its copy to hnorm[0]. */
+int Multigrid::vcycle_and_norm(int prec, const double *b, double *d_z, long N) {
+    int r;
+    const long long l0 = launches;
+    if (prec == INCRMT_PREC_FP64) {
+        if ((r = cycle64(0, b, d_z))) return r;
+        if ((r = residual_norm(b, d_z, nullptr, dnorm))) return r;
+    } else {
+        const int nbk = cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks;
+        k_fill<float><<<nbk, 256, 0, stream>>>(lev[0].zf, N, 0.f);
+        launches++;
+        if ((r = cycle32(0))) return r;
+        k_add_f32<<<nbk, 256, 0, stream>>>(d_z, lev[0].zf, N);
+        launches++;
+        INCRMT_CKL("defect correction");
+        if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
+    }
+    INCRMT_CK(cudaMemcpyAsync(hnorm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    graph_launches = launches - l0;
     return INCRMT_OK;
 }
 
@@ -644,21 +805,34 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
         if ((r = fetch_norm(&rn2))) return r;
     }
+    // One V-cycle, its residual norm and the read-back of that norm, captured
+    // once into a CUDA graph per (precision, b, z) and replayed per cycle.
+    const bool use_graph = !prof;
+    if (use_graph && (!gexec || gkey_prec != prec || gkey_b != b || gkey_z != d_z)) {
+        if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+        cudaGraph_t graph;
+        INCRMT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int rc = vcycle_and_norm(prec, b, d_z, N);
+        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+        if (rc) return rc;
+        if (ce != cudaSuccess) return cuda_status(ce, "capture", __FILE__, __LINE__);
+        ce = cudaGraphInstantiate(&gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) { gexec = nullptr; return cuda_status(ce, "instantiate", __FILE__, __LINE__); }
+        gkey_prec = prec; gkey_b = b; gkey_z = d_z;
+    }
     while (k < maxc) {
-        if (prec == INCRMT_PREC_FP64) {
-            if ((r = cycle64(0, b, d_z))) return r;
-            if ((r = residual_norm(b, d_z, nullptr, dnorm))) return r;
+        if (use_graph) {
+            INCRMT_CK(cudaGraphLaunch(gexec, stream));
+            launches += graph_launches;
+            INCRMT_CK(cudaStreamSynchronize(stream));
+            rn2 = hnorm[0];
         } else {
-            k_fill<float><<<cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks, 256, 0, stream>>>(lev[0].zf, N, 0.f);
-            launches++;
-            if ((r = cycle32(0))) return r;
-            k_add_f32<<<cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks, 256, 0, stream>>>(d_z, lev[0].zf, N);
-            launches++;
-            INCRMT_CKL("defect correction");
-            if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
+            if ((r = vcycle_and_norm(prec, b, d_z, N))) return r;
+            INCRMT_CK(cudaStreamSynchronize(stream));
+            rn2 = hnorm[0];
         }
         k++;
-        if ((r = fetch_norm(&rn2))) return r;
         const double rn = std::sqrt(rn2);
         if (!std::isfinite(rn)) { finite = false; break; }
         if (rn <= tol) { conv = true; break; }

@@ -48,6 +48,12 @@ public:
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
     bool ready = false;              // coefficients and hierarchy built
+    int tail_level = -1;             // first level run by the one-block tail kernel
+    cudaGraphExec_t gexec = nullptr; // captured V-cycle + norm
+    int gkey_prec = -1;
+    const double *gkey_b = nullptr;
+    const double *gkey_z = nullptr;
+    long long graph_launches = 0;    // kernels in the captured graph
     // Optional timing of the fine-level smoothing launches (the dominant
     // kernel): CUDA events around each launch on the handle's stream.
     bool prof = false;
@@ -80,6 +86,9 @@ private:
     int galerkin_all();
     int cycle64(int l, const double *b0, double *z0);
     int cycle32(int l);
+    int tail64();
+    int vcycle_and_norm(int prec, const double *b, double *d_z, long N);
+    int tail32();
     int norm2_rhs(const double *b, double *out_dev);
     int residual_norm(const double *b, const double *z, float *rf, double *out_dev);
     int fetch_norm(double *v);

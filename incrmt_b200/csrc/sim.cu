@@ -20,7 +20,6 @@ const dim3 kB2(32, 8);
 inline dim3 g2(int m, int n) { return dim3(cdiv(m, 32), cdiv(n, 8)); }
 constexpr int kLsMaxSweeps = 400;       // cap of the fixed-point sweeps of one march
 constexpr int kExtrapMaxSweeps = 1000;  // cap of the extrapolation wavefront sweeps
-constexpr int kSweepBatch = 8;          // sweeps between host checks of the change flag
 }  // namespace
 
 struct Sim {
@@ -37,8 +36,10 @@ struct Sim {
     double *src_mac = nullptr, *z_mac = nullptr, *src_fem = nullptr, *z_fem = nullptr;
     double *ls_a = nullptr, *ls_b = nullptr;       // march / extrapolation buffers (x)
     double *ls_c = nullptr, *ls_d = nullptr;       // extrapolation buffers (y)
-    int *d_list = nullptr;
-    int *d_flags = nullptr;                         // [0] changed, [1] count, [2] error, [3] tracer flag
+    int *d_list = nullptr, *d_ia = nullptr, *d_ib = nullptr;
+    int coop_blocks_fim = 0, coop_blocks_ext = 0;   // co-resident grid sizes
+    int *d_flags = nullptr;  // [0..2] sweep change flags, [3] sweeps, [4] converged, [5] fit error,
+                           // [6] Newton error, [7] list length, [8] tracer remaps, [9] correction failure
     int *h_flags = nullptr;                         // pinned
     double *partial = nullptr;
     double *tm = nullptr, *otm = nullptr;          // passive and object tracers
@@ -135,9 +136,20 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     if ((r = alloc(&ls_d, cells()))) return r;
     if ((r = alloc(&partial, 4 * kB200SMs))) return r;
     INCRMT_CK(cudaMalloc(&d_list, sizeof(int) * cells()));
-    INCRMT_CK(cudaMalloc(&d_flags, sizeof(int) * 8));
-    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 8, stream));
-    INCRMT_CK(cudaMallocHost(&h_flags, sizeof(int) * 8));
+    INCRMT_CK(cudaMalloc(&d_ia, sizeof(int) * cells()));
+    INCRMT_CK(cudaMalloc(&d_ib, sizeof(int) * cells()));
+    {
+        int dev = 0, sms = 0, nb = 0;
+        INCRMT_CK(cudaGetDevice(&dev));
+        INCRMT_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_fim_coop, 256, 0));
+        coop_blocks_fim = sms * (nb > 0 ? nb : 1);
+        INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_extrap_coop, 256, 0));
+        coop_blocks_ext = sms * (nb > 0 ? nb : 1);
+    }
+    INCRMT_CK(cudaMalloc(&d_flags, sizeof(int) * 16));
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 16, stream));
+    INCRMT_CK(cudaMallocHost(&h_flags, sizeof(int) * 16));
     if (ntrace > 0 && (r = alloc(&tm, 4 * static_cast<size_t>(ntrace)))) return r;
     if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, 0, g.zpr, stream))) return r;
     if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, 0, g.zpr, stream))) return r;
@@ -204,7 +216,7 @@ void Sim::pre_stress_setup(double t) {
 }
 
 int Sim::fetch_flags() {
-    INCRMT_CK(cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 8, cudaMemcpyDeviceToHost, stream));
+    INCRMT_CK(cudaMemcpyAsync(h_flags, d_flags, sizeof(int) * 16, cudaMemcpyDeviceToHost, stream));
     INCRMT_CK(cudaStreamSynchronize(stream));
     return INCRMT_OK;
 }
@@ -236,37 +248,39 @@ int Sim::set_rho() {
 /** levelset::build_band for object k (levelset.cc:199-335). */
 int Sim::build_band(int k) {
     SolidDev &s = sol[k];
-    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, stream));
-    k_ls_scan<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.phi, s.s);
-    k_ls_newton<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.phi, s.s, s.phi_tmp, d_flags + 2);
-    k_ls_copy_interface<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, s.phi_tmp, s.phi);
-    k_ls_fim_init<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, ls_a);
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 8, stream));
+    const dim3 gg = g2(lg.mL, lg.nL);
+    k_ls_scan<<<gg, kB2, 0, stream>>>(lg, s.phi, s.s);
+    k_ls_newton<<<gg, kB2, 0, stream>>>(lg, s.phi, s.s, s.phi_tmp, d_flags + 6);
+    k_ls_copy_interface<<<gg, kB2, 0, stream>>>(lg, s.s, s.phi_tmp, s.phi);
+    // Candidates: far points within the band radius of the interface.
+    const int R = static_cast<int>(std::ceil((lg.phi_up) / (g.dx < g.dy ? g.dx : g.dy))) + 2;
+    k_ls_mark_interface<<<gg, kB2, 0, stream>>>(lg, s.s, d_ia);
+    k_ls_dilate<true><<<gg, kB2, 0, stream>>>(lg, d_ia, d_ib, R);
+    k_ls_dilate<false><<<gg, kB2, 0, stream>>>(lg, d_ib, d_ia, R);
+    k_ls_collect_candidates<<<gg, kB2, 0, stream>>>(lg, s.s, d_ia, d_list, d_flags + 7);
+    k_ls_fim_init<<<gg, kB2, 0, stream>>>(lg, s.s, ls_a);
+    launches += 8;
+    INCRMT_CKL("level-set scan/newton/candidates");
     INCRMT_CK(cudaMemcpyAsync(ls_b, ls_a, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    launches += 4;
-    INCRMT_CKL("level-set scan/newton");
-    double *cur = ls_a, *nxt = ls_b;
-    int sweeps = 0;
-    bool done = false;
-    while (!done && sweeps < kLsMaxSweeps) {
-        INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int), stream));
-        for (int b = 0; b < kSweepBatch; b++) {
-            k_ls_fim_sweep<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.phi, s.s, cur, nxt, d_flags);
-            launches++;
-            std::swap(cur, nxt);
-            sweeps++;
-        }
-        INCRMT_CKL("k_ls_fim_sweep");
-        int r = fetch_flags();
-        if (r) return r;
-        if (h_flags[2]) { set_error("level++: Newton iteration failed."); return h_flags[2]; }
-        // A batch ends with a sweep that changed nothing only if the flag,
-        // cleared at the batch start, stayed down through the whole batch.
-        done = h_flags[0] == 0;
-    }
-    ls_sweeps += sweeps;
-    if (!done) { set_error("level-set march did not settle in %d sweeps", sweeps); return INCRMT_ERR_NOCONV; }
-    k_ls_finish<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, cur, s.s, s.phi);
+    int maxs = kLsMaxSweeps;
+    const int *countp = d_flags + 7;
+    double *pa = ls_a, *pb = ls_b;
+    const double *phic = s.phi;
+    const int *sc = s.s;
+    void *args[] = {&lg, &phic, &sc, &pa, &pb, &d_list, &countp, &d_flags, &maxs};
+    INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_fim_coop), dim3(coop_blocks_fim), dim3(256),
+                                          args, 0, stream));
     launches++;
+    int r = fetch_flags();
+    if (r) return r;
+    if (h_flags[6]) { set_error("level++: Newton iteration failed."); return h_flags[6]; }
+    ls_sweeps += h_flags[3];
+    if (!h_flags[4]) { set_error("level-set march did not settle in %d sweeps", h_flags[3]); return INCRMT_ERR_NOCONV; }
+    k_ls_finish<<<gg, kB2, 0, stream>>>(lg, ls_a, s.s, s.phi);
+    k_ls_trial<<<gg, kB2, 0, stream>>>(lg, s.s, d_ia);
+    INCRMT_CK(cudaMemcpyAsync(s.s, d_ia, sizeof(int) * cells(), cudaMemcpyDeviceToDevice, stream));
+    launches += 2;
     INCRMT_CKL("k_ls_finish");
     return INCRMT_OK;
 }
@@ -287,41 +301,30 @@ int Sim::pin() {
 /** levelset::extrapolate_fields for object k (traverse.hh:235-260). */
 int Sim::extrapolate(int k) {
     SolidDev &s = sol[k];
-    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, stream));
-    k_ls_collect_outside<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, d_list, d_flags + 1);
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 8, stream));
+    k_ls_collect_outside<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, d_list, d_flags + 7);
     launches++;
     INCRMT_CKL("collect");
-    int r = fetch_flags();
-    if (r) return r;
-    const int count = h_flags[1];
-    if (count == 0) return INCRMT_OK;
     INCRMT_CK(cudaMemcpyAsync(ls_a, s.nX, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
     INCRMT_CK(cudaMemcpyAsync(ls_c, s.nY, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
     INCRMT_CK(cudaMemcpyAsync(ls_b, s.nX, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
     INCRMT_CK(cudaMemcpyAsync(ls_d, s.nY, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    double *cx = ls_a, *cy = ls_c, *tx = ls_b, *ty = ls_d;
-    int sweeps = 0;
-    bool done = false;
-    while (!done && sweeps < kExtrapMaxSweeps) {
-        INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int), stream));
-        for (int b = 0; b < kSweepBatch; b++) {
-            k_ls_extrap_sweep<<<cdiv(count, 128), 128, 0, stream>>>(lg, s.s, s.phi, s.nX, s.nY, d_list, d_flags + 1,
-                                                                   cx, cy, tx, ty, d_flags, d_flags + 2);
-            launches++;
-            std::swap(cx, tx);
-            std::swap(cy, ty);
-            sweeps++;
-        }
-        INCRMT_CKL("k_ls_extrap_sweep");
-        if ((r = fetch_flags())) return r;
-        if (h_flags[2]) { set_error("singular extrapolation fit"); return h_flags[2]; }
-        done = h_flags[0] == 0;
-    }
-    ex_sweeps += sweeps;
-    if (!done) { set_error("extrapolation did not settle in %d sweeps", sweeps); return INCRMT_ERR_NOCONV; }
-    // Only the listed points changed; copy the whole iterate back.
-    INCRMT_CK(cudaMemcpyAsync(s.nX, cx, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    INCRMT_CK(cudaMemcpyAsync(s.nY, cy, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    int maxs = kExtrapMaxSweeps;
+    const int *countp = d_flags + 7;
+    const int *sc = s.s;
+    const double *phic = s.phi, *nXc = s.nX, *nYc = s.nY;
+    void *args[] = {&lg, &sc, &phic, &nXc, &nYc, &d_list, &countp, &ls_a, &ls_c, &ls_b, &ls_d, &d_flags, &maxs};
+    INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_extrap_coop), dim3(coop_blocks_ext),
+                                          dim3(256), args, 0, stream));
+    launches++;
+    int r = fetch_flags();
+    if (r) return r;
+    if (h_flags[5]) { set_error("singular extrapolation fit"); return h_flags[5]; }
+    ex_sweeps += h_flags[3];
+    if (!h_flags[4]) { set_error("extrapolation did not settle in %d sweeps", h_flags[3]); return INCRMT_ERR_NOCONV; }
+    // After the last sweep both buffers hold the same values.
+    INCRMT_CK(cudaMemcpyAsync(s.nX, ls_a, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(s.nY, ls_c, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
     return INCRMT_OK;
 }
 
@@ -390,11 +393,11 @@ int Sim::fem_projection(double dt) {
 int Sim::tracers(int st, double dt) {
     Field2 vel{f.u, f.v};
     if (ntrace > 0) {
-        k_tracers<<<cdiv(ntrace, 128), 128, 0, stream>>>(g, vel, tm, ntrace, 4, st, dt, 1, d_flags + 3);
+        k_tracers<<<cdiv(ntrace, 128), 128, 0, stream>>>(g, vel, tm, ntrace, 4, st, dt, 1, d_flags + 8);
         launches++;
     }
     if (nobjtr > 0) {
-        k_tracers<<<cdiv(nobjtr, 128), 128, 0, stream>>>(g, vel, otm, nobjtr, 6, st, dt, 0, d_flags + 3);
+        k_tracers<<<cdiv(nobjtr, 128), 128, 0, stream>>>(g, vel, otm, nobjtr, 6, st, dt, 0, d_flags + 8);
         launches++;
     }
     INCRMT_CKL("k_tracers");
@@ -414,8 +417,8 @@ int Sim::record_track() {
     INCRMT_CK(cudaMemcpyAsync(pre, otm, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
     if (t_correction) {
         Field2 rm{sol[0].X, sol[0].Y};
-        INCRMT_CK(cudaMemsetAsync(d_flags + 4, 0, sizeof(int), stream));
-        k_correct_tracers<<<1, 32, 0, stream>>>(g, rm, otm, nobjtr, d_flags + 4);
+        INCRMT_CK(cudaMemsetAsync(d_flags + 9, 0, sizeof(int), stream));
+        k_correct_tracers<<<1, 32, 0, stream>>>(g, rm, otm, nobjtr, d_flags + 9);
         launches++;
         INCRMT_CKL("k_correct_tracers");
     }
@@ -423,7 +426,7 @@ int Sim::record_track() {
     INCRMT_CK(cudaMemcpyAsync(post, otm, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
     int r = fetch_flags();
     if (r) return r;
-    if (h_flags[4]) t_correction = 0;
+    if (h_flags[9]) t_correction = 0;
     track.push_back(time);
     track.push_back(pre[0]); track.push_back(pre[1]);
     track.push_back(post[0]); track.push_back(post[1]);
@@ -566,7 +569,7 @@ void Sim::destroy() {
     for (double *p : allocs) cudaFree(p);
     allocs.clear();
     for (auto &s : sol) cudaFree(s.s);
-    cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_list); cudaFree(d_flags);
+    cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_list); cudaFree(d_ia); cudaFree(d_ib); cudaFree(d_flags);
     if (h_flags) cudaFreeHost(h_flags);
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
@@ -739,7 +742,10 @@ int incrmt_get_time(const incrmt_sim *h, double *t) {
 int incrmt_set_time(incrmt_sim *h, double t) {
     if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
     h->s.time = t;
-    return INCRMT_OK;
+    // The per-object state of the last stress evaluation follows the clock
+    // (object::pre_stress_setup is called at every compute_stress).
+    h->s.pre_stress_setup(t);
+    return h->s.upload_objects();
 }
 
 int incrmt_get_tracers(incrmt_sim *h, double *host) {

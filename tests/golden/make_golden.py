@@ -34,6 +34,28 @@ def mg_cases():
     return cases
 
 
+def sspin_cases():
+    """Simple-spin end states after a few steps from the scenario's own
+    initialisation (ftest.cc:116-143), interior cells only."""
+    out = []
+    for m, steps in [(64, 20), (128, 50)]:
+        r = refsim.RefSim(m, ntrace=16)
+        tr0 = r.tracers()[:, :2].copy()
+        dt, _ = refsim.frame_dt(r.scalars()["dt_reg"])
+        r.step(dt, steps)
+        d = {f: r.get(f)[2:-2, 2:-2] for f in ["u", "v", "p", "X", "Y", "phi"]}
+        d["tracers0"] = tr0
+        d["tracers"] = r.tracers()[:, :2]
+        d["objtr"] = r.obj_tracers()[:, :2]
+        name = f"sspin_{m}_{steps}.npz"
+        np.savez_compressed(os.path.join(OUT, name), **d)
+        r.close()
+        out.append(name)
+    return out
+
+
 if __name__ == "__main__":
     for name, st in mg_cases():
         print(name, st)
+    for name in sspin_cases():
+        print(name)

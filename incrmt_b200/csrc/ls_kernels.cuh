@@ -683,9 +683,11 @@ __global__ void k_ls_fim_coop(LsGrid g, const double *phi, const int *s, double 
             nxt[ij] = v;
             if (v != old) ch = true;
         }
-        if (ch) atomicExch(&flags[it % 3], 1);
+        // One store per block; the flag is read once per thread after the
+        // barrier with a volatile load (no atomics on a single address).
+        if (__syncthreads_or(ch) && threadIdx.x == 0) flags[it % 3] = 1;
         grid.sync();
-        const int c = atomicAdd(&flags[it % 3], 0);
+        const int c = *reinterpret_cast<volatile int *>(&flags[it % 3]);
         double *t = cur; cur = nxt; nxt = t;
         if (!c) { done = true; break; }
     }
@@ -718,9 +720,9 @@ __global__ void k_ls_extrap_coop(LsGrid g, const int *s, const double *phi, cons
             tx[ij] = ox;
             ty[ij] = oy;
         }
-        if (ch) atomicExch(&flags[it % 3], 1);
+        if (__syncthreads_or(ch) && threadIdx.x == 0) flags[it % 3] = 1;
         grid.sync();
-        const int c = atomicAdd(&flags[it % 3], 0);
+        const int c = *reinterpret_cast<volatile int *>(&flags[it % 3]);
         double *t1 = cx; cx = tx; tx = t1;
         double *t2 = cy; cy = ty; ty = t2;
         if (!c) { done = true; break; }

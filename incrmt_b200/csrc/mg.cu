@@ -75,12 +75,55 @@ __global__ void k_fem_coef(const double *rho, int ml, int mf, int nf, double *c,
     cf[j * mf + i] = static_cast<float>(v);
 }
 
+/** 1D prolongation weight of fine offset t (fine 2I+t) to coarse offset k
+ * (coarse I+k) away from any boundary: 1 on the coarse point, 1/2 next to it. */
+__host__ __device__ constexpr double pw_int(int t, int k) {
+    return (t - 2 * k == 0) ? 1.0 : ((t - 2 * k == 1 || t - 2 * k == -1) ? 0.5 : 0.0);
+}
+
+/** Galerkin product at an interior coarse unknown, fully unrolled so the 81
+ * fine stencil entries stay in registers. */
+template <class Op>
+__device__ __forceinline__ void galerkin_interior(const Op &op, int I, int J, double q[9]) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) q[k] = 0;
+#pragma unroll
+    for (int ty = -1; ty <= 1; ty++) {
+#pragma unroll
+        for (int tx = -1; tx <= 1; tx++) {
+            double a[9];
+            op.coef9(2 * I + tx, 2 * J + ty, a);
+            const double w = pw_int(tx, 0) * pw_int(ty, 0);
+#pragma unroll
+            for (int dj = -1; dj <= 1; dj++)
+#pragma unroll
+                for (int di = -1; di <= 1; di++)
+#pragma unroll
+                    for (int kj = -1; kj <= 1; kj++)
+#pragma unroll
+                        for (int ki = -1; ki <= 1; ki++) {
+                            const double v = pw_int(tx + di, ki) * pw_int(ty + dj, kj);
+                            if (v != 0.0) q[3 * (kj + 1) + ki + 1] += w * a[3 * (dj + 1) + di + 1] * v;
+                        }
+        }
+    }
+}
+
 /** Galerkin coarse stencil A_c = P^T A P, one coarse unknown per thread. */
 template <class Op>
 __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
                            int cm, int cn, double *st) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
     if (I >= cm || J >= cn) return;
+    const long N = static_cast<long>(cm) * cn;
+    const int ij = I + cm * J;
+    if (kx && ky && I >= 1 && J >= 1 && I <= cm - 2 && J <= cn - 2 && 2 * I + 2 <= fm - 1 && 2 * J + 2 <= fn - 1) {
+        double q[9];
+        galerkin_interior(op, I, J, q);
+#pragma unroll
+        for (int k = 0; k < 9; k++) st[k * N + ij] = q[k];
+        return;
+    }
     double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int fx[3], fy[3];
     const int nfx = support(I, fm, px, kx, fx), nfy = support(J, fn, py, ky, fy);
@@ -120,8 +163,6 @@ __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool 
             }
         }
     }
-    const long N = static_cast<long>(cm) * cn;
-    const int ij = I + cm * J;
 #pragma unroll
     for (int k = 0; k < 9; k++) st[k * N + ij] = q[k];
 }
@@ -221,10 +262,13 @@ __global__ void k_coarse(Op op, T *z, const T *b, int m, int n, int sweeps) {
 /** Levels handled by the one-block tail kernel. */
 constexpr int kTailMaxLevels = 12;
 constexpr int kTailMaxSize = 4096;  // unknowns of the first tail level at most
+constexpr size_t kTailSmemBudget = 160 * 1024;  // shared memory for the smallest tail levels
 
 template <class T>
 struct TailLevels {
     int first, count, px, py;
+    int smem_from;                 // levels >= smem_from live in shared memory
+    long smem_off[kTailMaxLevels]; // element offsets of st, then z, then b
     int m[kTailMaxLevels], n[kTailMaxLevels];
     long N[kTailMaxLevels];
     bool kx[kTailMaxLevels], ky[kTailMaxLevels];
@@ -264,7 +308,21 @@ __device__ void tail_smooth(const TailLevels<T> &L, int l, int sweeps) {
  * between phases, and the coarsest solve. The levels are small enough to sit
  * in L2, so the cost is the barriers rather than launches. */
 template <class T>
-__global__ void __launch_bounds__(1024) k_tail(TailLevels<T> L, int nu1, int nu2, int coarse_sweeps) {
+__global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu2, int coarse_sweeps) {
+    // The smallest levels are moved into shared memory: stencils copied in,
+    // iterate and right-hand side written there by the restriction.
+    extern __shared__ __align__(16) unsigned char tail_smem[];
+    T *sbase = reinterpret_cast<T *>(tail_smem);
+    TailLevels<T> L = Lp;
+    for (int l = L.smem_from; l < L.count; l++) {
+        T *st = sbase + L.smem_off[l];
+        const long n9 = 9 * L.N[l];
+        for (long q = threadIdx.x; q < n9; q += blockDim.x) st[q] = L.st[l][q];
+        L.st[l] = st;
+        L.z[l] = st + n9;
+        L.b[l] = st + n9 + L.N[l];
+    }
+    __syncthreads();
     const int last = L.count - 1;
     for (int l = 0; l < last; l++) {
         tail_smooth(L, l, nu1);
@@ -497,6 +555,10 @@ int Multigrid::build_hierarchy() {
         lev.push_back(L);
         mm = mc; nn = nc;
     }
+    INCRMT_CK(cudaFuncSetAttribute(k_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kTailSmemBudget)));
+    INCRMT_CK(cudaFuncSetAttribute(k_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kTailSmemBudget)));
     // First level small enough for the one-block tail kernel (never level 0).
     tail_level = -1;
     for (int l = 1; l < static_cast<int>(lev.size()); l++)
@@ -678,6 +740,24 @@ int Multigrid::cycle32(int l) {
     return smooth(g, z, b, L.m, L.n, kNu2, stream, launches);
 }
 
+/** Shared-memory layout of the tail: the coarsest levels, from the bottom
+ * up, while their stencils, iterates and right-hand sides fit in the budget.
+ * \return the dynamic shared memory in bytes. */
+template <class T>
+size_t tail_layout(TailLevels<T> &L, size_t budget) {
+    long off = 0;
+    L.smem_from = L.count;
+    for (int k = L.count - 1; k >= 1; k--) {
+        const long need = 11 * L.N[k];
+        if (static_cast<size_t>(off + need) * sizeof(T) > budget) break;
+        L.smem_from = k;
+        off += need;
+    }
+    long o = 0;
+    for (int k = L.smem_from; k < L.count; k++) { L.smem_off[k] = o; o += 11 * L.N[k]; }
+    return static_cast<size_t>(o) * sizeof(T);
+}
+
 int Multigrid::tail64() {
     TailLevels<double> T{};
     T.first = tail_level; T.count = static_cast<int>(lev.size()) - tail_level; T.px = px; T.py = py;
@@ -686,7 +766,8 @@ int Multigrid::tail64() {
         T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
         T.z[k] = L.z; T.b[k] = L.b; T.st[k] = L.st;
     }
-    k_tail<double><<<1, 1024, 0, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
+    const size_t sm = tail_layout(T, kTailSmemBudget);
+    k_tail<double><<<1, 1024, sm, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
     launches++;
     INCRMT_CKL("k_tail");
     return INCRMT_OK;
@@ -700,7 +781,8 @@ int Multigrid::tail32() {
         T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
         T.z[k] = L.zf; T.b[k] = L.bf; T.st[k] = L.stf;
     }
-    k_tail<float><<<1, 1024, 0, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
+    const size_t sm = tail_layout(T, kTailSmemBudget);
+    k_tail<float><<<1, 1024, sm, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
     launches++;
     INCRMT_CKL("k_tail");
     return INCRMT_OK;

@@ -188,6 +188,53 @@ __global__ void k_smooth(Op op, T *z, const T *b, int m, int n, int pi, int pj) 
     z[ij] = (b[ij] - off) / diag;
 }
 
+/** Tile-fused Gauss-Seidel: SWEEPS complete four-colour sweeps in one launch
+ * for a non-periodic grid. The block stages its TW x TH tile of the iterate
+ * plus a halo of 4*SWEEPS cells in shared memory and runs the colour phases
+ * there, phase p updating the tile grown by 4*SWEEPS-1-p cells, so that every
+ * value a later phase reads is already final; the tile is then written back.
+ * Each point sees exactly the neighbour values of the one-launch-per-colour
+ * schedule, so the result is identical to it. Coefficients and the right-hand
+ * side are read from global memory (L1/L2). */
+template <class Op, class T, int SWEEPS, int TW, int TH>
+__global__ void __launch_bounds__(256) k_smooth_tile(Op op, T *z, const T *b, int m, int n) {
+    constexpr int H = 4 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H;
+    __shared__ T zs[LW * LH];
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    const int gx0 = x0 - H, gy0 = y0 - H;
+    for (int t = threadIdx.x; t < LW * LH; t += blockDim.x) {
+        const int li = t % LW, lj = t / LW, i = gx0 + li, j = gy0 + lj;
+        if (i >= 0 && i < m && j >= 0 && j < n) zs[t] = z[i + static_cast<long>(m) * j];
+    }
+    __syncthreads();
+    const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
+    constexpr int P = 4 * SWEEPS;
+#pragma unroll 1
+    for (int p = 0; p < P; p++) {
+        const int e = P - 1 - p, c = p & 3;
+        int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
+        if (ilo < 0) ilo = 0;
+        if (jlo < 0) jlo = 0;
+        if (ihi > m - 1) ihi = m - 1;
+        if (jhi > n - 1) jhi = n - 1;
+        // first index of the colour's parity at or above the low bound
+        const int i0 = ilo + ((ilo & 1) != pis[c]), j0 = jlo + ((jlo & 1) != pjs[c]);
+        const int ni = i0 <= ihi ? (ihi - i0) / 2 + 1 : 0, nj = j0 <= jhi ? (jhi - j0) / 2 + 1 : 0;
+        for (int t = threadIdx.x; t < ni * nj; t += blockDim.x) {
+            const int i = i0 + 2 * (t % ni), j = j0 + 2 * (t / ni);
+            const int lz = (i - gx0) + LW * (j - gy0);
+            T diag;
+            const T off = op.offdiag_s(i, j, zs, lz, LW, diag);
+            zs[lz] = (b[i + static_cast<long>(m) * j] - off) / diag;
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < TW * TH; t += blockDim.x) {
+        const int i = x0 + t % TW, j = y0 + t / TW;
+        if (i < m && j < n) z[i + static_cast<long>(m) * j] = zs[(i - gx0) + LW * (j - gy0)];
+    }
+}
+
 /** Coarse right-hand side b_c = P^T (b - A z), the fine residual formed on
  * the fly; also clears the coarse iterate. */
 template <class Op, class T>
@@ -283,6 +330,11 @@ __device__ __forceinline__ GenOp<T> tail_op(const TailLevels<T> &L, int l) {
     return g;
 }
 
+/** Smoothing of one tail level. Levels of at most kWarpLevel unknowns are
+ * swept by the first warp alone with warp barriers (a block barrier per
+ * colour phase would dominate there); the block waits once at the end. */
+constexpr int kWarpLevel = 256;
+
 template <class T>
 __device__ void tail_smooth(const TailLevels<T> &L, int l, int sweeps) {
     const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
@@ -290,17 +342,22 @@ __device__ void tail_smooth(const TailLevels<T> &L, int l, int sweeps) {
     const int m = L.m[l], n = L.n[l];
     T *z = L.z[l];
     const T *b = L.b[l];
+    const bool warp_only = m * n <= kWarpLevel;
+    if (warp_only && threadIdx.x >= 32) { __syncthreads(); return; }
+    const int nth = warp_only ? 32 : blockDim.x;
     for (int s = 0; s < sweeps; s++)
         for (int c = 0; c < 4; c++) {
             const int mc = (m - pis[c] + 1) / 2, nc = (n - pjs[c] + 1) / 2;
-            for (int p = threadIdx.x; p < mc * nc; p += blockDim.x) {
+            for (int p = threadIdx.x; p < mc * nc; p += nth) {
                 const int i = 2 * (p % mc) + pis[c], j = 2 * (p / mc) + pjs[c];
                 T diag;
                 const T off = op.offdiag(i, j, z, diag);
                 z[i + m * j] = (b[i + m * j] - off) / diag;
             }
-            __syncthreads();
+            if (warp_only) __syncwarp();
+            else __syncthreads();
         }
+    if (warp_only) __syncthreads();
 }
 
 /** The V-cycle below (and including) level L.first in one block: smoothing,
@@ -456,6 +513,16 @@ const dim3 kBlk2(32, 8);
 template <class Op, class T>
 int smooth(Op op, T *z, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl,
            Multigrid *prof = nullptr, double bytes_per_unit = 0) {
+    if (!op.px && !op.py && sweeps == 2) {
+        // Two sweeps per launch with shared-memory tiles (identical results).
+        constexpr int TW = 64, TH = 32;
+        if (prof) { int r = prof->prof_begin(static_cast<double>(m) * n * 2 * bytes_per_unit); if (r) return r; }
+        k_smooth_tile<Op, T, 2, TW, TH><<<dim3(cdiv(m, TW), cdiv(n, TH)), 256, 0, s>>>(op, z, b, m, n);
+        nl++;
+        if (prof) { int r = prof->prof_end(); if (r) return r; }
+        INCRMT_CKL("k_smooth_tile");
+        return INCRMT_OK;
+    }
     const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
     for (int q = 0; q < sweeps; q++)
         for (int c = 0; c < 4; c++) {

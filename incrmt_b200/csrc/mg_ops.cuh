@@ -41,6 +41,22 @@ struct MacOp {
         return xxsp * sx + yysp * sy;
     }
 
+    /** offdiag with the iterate in a shared-memory tile (lz: local index of
+     * (i,j), ldz: tile row stride); for non-periodic grids. */
+    __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
+        const T el = ex[j * (m + 1) + i], er = ex[j * (m + 1) + i + 1];
+        const T ed = ey[j * m + i], eu = ey[(j + 1) * m + i];
+        const bool l = i > 0, r = i < m - 1, d = j > 0, u = j < n - 1;
+        T sx = 0, sy = 0;
+        if (l) sx = el * zs[lz - 1];
+        if (r) sx += er * zs[lz + 1];
+        if (d) sy = ed * zs[lz - ldz];
+        if (u) sy += eu * zs[lz + ldz];
+        diag = -xxsp * ((l ? el : T(0)) + (i < m - 1 ? er : (zpr ? 2 * er : T(0))))
+               - yysp * ((d ? ed : T(0)) + (u ? eu : T(0)));
+        return xxsp * sx + yysp * sy;
+    }
+
     __device__ __forceinline__ void coef9(int i, int j, T a[9]) const {
         T diag;
         const T el = ex[j * (m + 1) + i], er = ex[j * (m + 1) + i + 1];
@@ -100,6 +116,37 @@ struct FemOp {
         a[5] = r ? ((d ? cdr : T(0)) + (u ? cur : T(0))) * hex : T(0);
     }
 
+    __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
+        const int ij = i + m * j;
+        if (i > 0 && i < m - 1 && j > 0 && j < n - 1) {
+            const T cdl = c[ij], cdr = c[ij + 1], cul = c[ij + m], cur = c[ij + m + 1];
+            diag = fm * ((cul + cdl) + (cur + cdr));
+            const T *w = zs + lz;
+            return cul * (w[-1] * hex + w[ldz - 1] * fc + w[ldz] * hey)
+                 + cdl * (w[-1] * hex + w[-ldz - 1] * fc + w[-ldz] * hey)
+                 + cur * (w[1] * hex + w[ldz + 1] * fc + w[ldz] * hey)
+                 + cdr * (w[1] * hex + w[-ldz + 1] * fc + w[-ldz] * hey);
+        }
+        T a[9];
+        coef9(i, j, a);
+        diag = a[4];
+        const bool l = i > 0, r = i < m - 1, d = j > 0, u = j < n - 1;
+        T t = 0;
+        if (d) {
+            if (l) t += a[0] * zs[lz - ldz - 1];
+            t += a[1] * zs[lz - ldz];
+            if (r) t += a[2] * zs[lz - ldz + 1];
+        }
+        if (l) t += a[3] * zs[lz - 1];
+        if (r) t += a[5] * zs[lz + 1];
+        if (u) {
+            if (l) t += a[6] * zs[lz + ldz - 1];
+            t += a[7] * zs[lz + ldz];
+            if (r) t += a[8] * zs[lz + ldz + 1];
+        }
+        return t;
+    }
+
     __device__ __forceinline__ T offdiag(int i, int j, const T *z, T &diag) const {
         const int ij = i + m * j;
         if (i > 0 && i < m - 1 && j > 0 && j < n - 1) {
@@ -147,6 +194,26 @@ struct GenOp {
         const int ij = i + m * j;
 #pragma unroll
         for (int k = 0; k < 9; k++) a[k] = st[k * N + ij];
+    }
+
+    __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
+        const int ij = i + m * j;
+        const bool l = i > 0, r = i < m - 1, d = j > 0, u = j < n - 1;
+        diag = st[4 * N + ij];
+        T t = 0;
+        if (d) {
+            if (l) t += st[ij] * zs[lz - ldz - 1];
+            t += st[N + ij] * zs[lz - ldz];
+            if (r) t += st[2 * N + ij] * zs[lz - ldz + 1];
+        }
+        if (l) t += st[3 * N + ij] * zs[lz - 1];
+        if (r) t += st[5 * N + ij] * zs[lz + 1];
+        if (u) {
+            if (l) t += st[6 * N + ij] * zs[lz + ldz - 1];
+            t += st[7 * N + ij] * zs[lz + ldz];
+            if (r) t += st[8 * N + ij] * zs[lz + ldz + 1];
+        }
+        return t;
     }
 
     __device__ __forceinline__ T offdiag(int i, int j, const T *z, T &diag) const {

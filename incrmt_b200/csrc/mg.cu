@@ -513,9 +513,10 @@ const dim3 kBlk2(32, 8);
 template <class Op, class T>
 int smooth(Op op, T *z, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl,
            Multigrid *prof = nullptr, double bytes_per_unit = 0) {
-    if (!op.px && !op.py && sweeps == 2) {
-        // Two sweeps per launch with shared-memory tiles (identical results).
-        constexpr int TW = 64, TH = 32;
+    constexpr int TW = 64, TH = 32;
+    if (!op.px && !op.py && sweeps == 2 && cdiv(m, TW) * cdiv(n, TH) >= 2 * kB200SMs) {
+        // Two sweeps per launch with shared-memory tiles (identical results),
+        // on grids large enough to fill the GPU with tiles.
         if (prof) { int r = prof->prof_begin(static_cast<double>(m) * n * 2 * bytes_per_unit); if (r) return r; }
         k_smooth_tile<Op, T, 2, TW, TH><<<dim3(cdiv(m, TW), cdiv(n, TH)), 256, 0, s>>>(op, z, b, m, n);
         nl++;

@@ -306,6 +306,121 @@ __global__ void k_coarse(Op op, T *z, const T *b, int m, int n, int sweeps) {
     }
 }
 
+/** Coarse levels with at most this many unknowns are solved exactly. */
+constexpr int kDirectMax = 96;
+
+/** Dense inverse of the coarsest Galerkin operator, one block, Gauss-Jordan
+ * with partial pivoting on [A | I] in shared memory. The singular
+ * pure-Neumann operator (zero row sums) is regularised by c e e^T, c the
+ * mean |diagonal| / N, which gives the zero-mean solution of a compatible
+ * system. Writes the FP64 inverse and an FP32 copy. */
+__global__ void k_coarse_inverse(const double *st, int m, int n, int px, int py, double *ginv, float *ginvf) {
+    extern __shared__ __align__(16) double gj[];
+    const int N = m * n, W = 2 * N;
+    double *a = gj, *f = gj + static_cast<long>(N) * W;
+    __shared__ double red[32];
+    __shared__ int piv;
+    __shared__ bool singular;
+    __shared__ double creg;
+    for (int q = threadIdx.x; q < N * W; q += blockDim.x) a[q] = 0;
+    __syncthreads();
+    double rsmax = 0, dsum = 0;
+    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        const int i = r % m, j = r / m;
+        double rs = 0;
+        for (int dj = -1; dj <= 1; dj++) {
+            bool oky = true;
+            const int jj = wrap_idx(j + dj, n, py, oky);
+            if (!oky) continue;
+            for (int di = -1; di <= 1; di++) {
+                bool okx = true;
+                const int ii = wrap_idx(i + di, m, px, okx);
+                if (!okx) continue;
+                const double v = st[(3 * (dj + 1) + di + 1) * static_cast<long>(N) + r];
+                a[static_cast<long>(r) * W + ii + m * jj] += v;
+                rs += v;
+            }
+        }
+        rsmax = fmax(rsmax, fabs(rs));
+        dsum += fabs(st[4 * static_cast<long>(N) + r]);
+        a[static_cast<long>(r) * W + N + r] = 1;
+    }
+    // block max / sum (1024 threads = 32 warps)
+    for (int o = 16; o > 0; o >>= 1) {
+        rsmax = fmax(rsmax, __shfl_down_sync(0xffffffffu, rsmax, o));
+        dsum += __shfl_down_sync(0xffffffffu, dsum, o);
+    }
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    if (lane == 0) red[wp] = rsmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) mx = fmax(mx, red[w]);
+        creg = mx;
+    }
+    __syncthreads();
+    if (lane == 0) red[wp] = dsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sm = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) sm += red[w];
+        singular = creg <= 1e-10 * sm / N;
+        creg = sm / N / N;
+    }
+    __syncthreads();
+    if (singular)
+        for (int q = threadIdx.x; q < N * N; q += blockDim.x) a[static_cast<long>(q / N) * W + q % N] += creg;
+    __syncthreads();
+    for (int k = 0; k < N; k++) {
+        if (threadIdx.x == 0) {
+            int p = k;
+            for (int r = k + 1; r < N; r++)
+                if (fabs(a[static_cast<long>(r) * W + k]) > fabs(a[static_cast<long>(p) * W + k])) p = r;
+            piv = p;
+        }
+        __syncthreads();
+        const int p = piv;
+        if (p != k)
+            for (int q = threadIdx.x; q < W; q += blockDim.x) {
+                const double t = a[static_cast<long>(k) * W + q];
+                a[static_cast<long>(k) * W + q] = a[static_cast<long>(p) * W + q];
+                a[static_cast<long>(p) * W + q] = t;
+            }
+        __syncthreads();
+        const double iv = 1.0 / a[static_cast<long>(k) * W + k];
+        __syncthreads();
+        for (int q = threadIdx.x; q < W; q += blockDim.x) a[static_cast<long>(k) * W + q] *= iv;
+        for (int r = threadIdx.x; r < N; r += blockDim.x) f[r] = a[static_cast<long>(r) * W + k];
+        __syncthreads();
+        for (long q = threadIdx.x; q < static_cast<long>(N) * W; q += blockDim.x) {
+            const int r = static_cast<int>(q / W);
+            if (r == k || f[r] == 0) continue;
+            a[q] -= f[r] * a[static_cast<long>(k) * W + q % W];
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < N * N; q += blockDim.x) {
+        const double v = a[static_cast<long>(q / N) * W + N + q % N];
+        ginv[q] = v;
+        ginvf[q] = static_cast<float>(v);
+    }
+}
+
+/** Coarsest solve by the dense inverse: z = G b. */
+template <class T>
+__device__ __forceinline__ void coarse_direct(const T *G, const T *b, T *z, int N) {
+    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        T t = 0;
+        for (int q = 0; q < N; q++) t += G[static_cast<long>(r) * N + q] * b[q];
+        z[r] = t;
+    }
+}
+
+template <class T>
+__global__ void k_coarse_direct(const T *G, const T *b, T *z, int N) {
+    coarse_direct(G, b, z, N);
+}
+
 /** Levels handled by the one-block tail kernel. */
 constexpr int kTailMaxLevels = 12;
 constexpr int kTailMaxSize = 4096;  // unknowns of the first tail level at most
@@ -315,6 +430,7 @@ template <class T>
 struct TailLevels {
     int first, count, px, py;
     int smem_from;                 // levels >= smem_from live in shared memory
+    const T *ginv;                 // dense inverse of the coarsest level, or null
     long smem_off[kTailMaxLevels]; // element offsets of st, then z, then b
     int m[kTailMaxLevels], n[kTailMaxLevels];
     long N[kTailMaxLevels];
@@ -405,7 +521,12 @@ __global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu
         }
         __syncthreads();
     }
-    tail_smooth(L, last, coarse_sweeps);
+    if (L.ginv) {
+        coarse_direct(L.ginv, L.b[last], L.z[last], static_cast<int>(L.N[last]));
+        __syncthreads();
+    } else {
+        tail_smooth(L, last, coarse_sweeps);
+    }
     for (int l = last - 1; l >= 0; l--) {
         const int fm = L.m[l], fn = L.n[l], cm = L.m[l + 1], cn = L.n[l + 1];
         for (int q = threadIdx.x; q < fm * fn; q += blockDim.x) {
@@ -623,6 +744,13 @@ int Multigrid::build_hierarchy() {
         lev.push_back(L);
         mm = mc; nn = nc;
     }
+    if (lev.size() > 1 && lev.back().N <= kDirectMax) {
+        const long N = lev.back().N;
+        INCRMT_CK(cudaMalloc(&ginv, sizeof(double) * N * N));
+        INCRMT_CK(cudaMalloc(&ginvf, sizeof(float) * N * N));
+        INCRMT_CK(cudaFuncSetAttribute(k_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(sizeof(double) * (2 * N * N + N))));
+    }
     INCRMT_CK(cudaFuncSetAttribute(k_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTailSmemBudget)));
     INCRMT_CK(cudaFuncSetAttribute(k_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -641,6 +769,7 @@ void Multigrid::destroy() {
     lev.clear();
     cudaFree(ex); cudaFree(ey); cudaFree(exf); cudaFree(eyf); cudaFree(c); cudaFree(cf);
     cudaFree(rho); cudaFree(bbuf); cudaFree(zbuf); cudaFree(partial); cudaFree(dnorm);
+    cudaFree(ginv); cudaFree(ginvf); ginv = nullptr; ginvf = nullptr;
     if (hnorm) cudaFreeHost(hnorm);
     if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
     for (auto e : prof_ev) cudaEventDestroy(e);
@@ -681,6 +810,13 @@ int Multigrid::galerkin_all() {
         launches += 2;
         INCRMT_CKL("galerkin");
     }
+    if (ginv) {
+        const MgLevel &C = lev.back();
+        const size_t sm = sizeof(double) * (2 * C.N * C.N + C.N);
+        k_coarse_inverse<<<1, 1024, sm, stream>>>(C.st, C.m, C.n, px, py, ginv, ginvf);
+        launches++;
+        INCRMT_CKL("k_coarse_inverse");
+    }
     return INCRMT_OK;
 }
 
@@ -695,7 +831,8 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
         if (l == 0) {
             if (sys == INCRMT_SYS_MAC) k_coarse<<<1, 256, 0, stream>>>(mac64(), z, b, L.m, L.n, kCoarseSweeps);
             else k_coarse<<<1, 256, 0, stream>>>(fem64(), z, b, L.m, L.n, kCoarseSweeps);
-        } else k_coarse<<<1, 256, 0, stream>>>(g, z, b, L.m, L.n, kCoarseSweeps);
+        } else if (ginv) k_coarse_direct<double><<<1, 256, 0, stream>>>(ginv, b, z, static_cast<int>(L.N));
+        else k_coarse<<<1, 256, 0, stream>>>(g, z, b, L.m, L.n, kCoarseSweeps);
         launches++;
         INCRMT_CKL("k_coarse");
         return INCRMT_OK;
@@ -778,7 +915,8 @@ int Multigrid::cycle32(int l) {
         if (l == 0) {
             if (sys == INCRMT_SYS_MAC) k_coarse<<<1, 256, 0, stream>>>(mac32(), z, b, L.m, L.n, kCoarseSweeps);
             else k_coarse<<<1, 256, 0, stream>>>(fem32(), z, b, L.m, L.n, kCoarseSweeps);
-        } else k_coarse<<<1, 256, 0, stream>>>(g, z, b, L.m, L.n, kCoarseSweeps);
+        } else if (ginvf) k_coarse_direct<float><<<1, 256, 0, stream>>>(ginvf, b, z, static_cast<int>(L.N));
+        else k_coarse<<<1, 256, 0, stream>>>(g, z, b, L.m, L.n, kCoarseSweeps);
         launches++;
         INCRMT_CKL("k_coarse");
         return INCRMT_OK;
@@ -834,6 +972,7 @@ int Multigrid::tail64() {
         T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
         T.z[k] = L.z; T.b[k] = L.b; T.st[k] = L.st;
     }
+    T.ginv = ginv;
     const size_t sm = tail_layout(T, kTailSmemBudget);
     k_tail<double><<<1, 1024, sm, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
     launches++;
@@ -849,6 +988,7 @@ int Multigrid::tail32() {
         T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
         T.z[k] = L.zf; T.b[k] = L.bf; T.st[k] = L.stf;
     }
+    T.ginv = ginvf;
     const size_t sm = tail_layout(T, kTailSmemBudget);
     k_tail<float><<<1, 1024, sm, stream>>>(T, kNu1, kNu2, kCoarseSweeps);
     launches++;

@@ -43,6 +43,8 @@ public:
     double *bbuf = nullptr;          // device right-hand side (host solves, FEM zpr masking)
     double *zbuf = nullptr;          // device iterate for host solves
     double *partial = nullptr;       // reduction partials
+    double *ginv = nullptr;          // dense inverse of the coarsest level (FP64)
+    float *ginvf = nullptr;          // and its FP32 copy
     double *hnorm = nullptr;         // pinned host scalars
     double *dnorm = nullptr;         // device scalars
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

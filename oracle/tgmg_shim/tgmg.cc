@@ -174,7 +174,7 @@ inline bool tgmg_can_coarsen(int m,bool p) {
 
 template<class S,class V,class M>
 tgmg<S,V,M>::tgmg(S &s_,V *b_,V *z_) : tgmg_base<S,V,M>(s_,b_,z_),
-    nlev(1), rf(new V[s_.mn]), last_vcycles(0), last_rel_res(0) {
+    nlev(1), rf(new V[s_.mn]), last_vcycles(0), last_rel_res(0), ginv(NULL) {
     int m=this->m,n=this->n;
     bool xp=this->x_prd,yp=this->y_prd;
     while(nlev<tgmg_max_levels&&m*n>tgmg_coarsest_size) {
@@ -192,6 +192,59 @@ template<class S,class V,class M>
 tgmg<S,V,M>::~tgmg() {
     for(int l=nlev-1;l>=1;l--) {delete lb[l];delete lev[l];}
     delete [] rf;
+    if(ginv!=NULL) delete [] ginv;
+}
+
+/** Dense inverse of the coarsest operator by Gauss-Jordan elimination with
+ * partial pivoting; the singular Neumann operator is regularised by
+ * c e e^T first. */
+template<class S,class V,class M>
+void tgmg<S,V,M>::coarse_inverse() {
+    tgmg_level<V,M> &c=*lev[nlev-1];
+    const int N=c.mn,W=2*N;
+    if(ginv==NULL) ginv=new double[N*N];
+    double *a=new double[N*W];
+    for(int k=0;k<N*W;k++) a[k]=0;
+    double rsmax=0,dsum=0;
+    for(int r=0;r<N;r++) {
+        int i=r%c.m,j=r/c.m;
+        double rs=0;
+        for(int dj=-1;dj<=1;dj++) {
+            bool oky=true;
+            int jj=tgmg_wrap(j+dj,c.n,c.y_prd,oky);
+            if(!oky) continue;
+            for(int di=-1;di<=1;di++) {
+                bool okx=true;
+                int ii=tgmg_wrap(i+di,c.m,c.x_prd,okx);
+                if(!okx) continue;
+                double v=c.st[9*r+3*(dj+1)+di+1];
+                a[r*W+ii+c.m*jj]+=v;
+                rs+=v;
+            }
+        }
+        if(fabs(rs)>rsmax) rsmax=fabs(rs);
+        dsum+=fabs(c.st[9*r+4]);
+        a[r*W+N+r]=1;
+    }
+    if(rsmax<=1e-10*dsum/N) {
+        const double cc=dsum/N/N;
+        for(int r=0;r<N;r++) for(int q=0;q<N;q++) a[r*W+q]+=cc;
+    }
+    for(int k=0;k<N;k++) {
+        int p=k;
+        for(int r=k+1;r<N;r++) if(fabs(a[r*W+k])>fabs(a[p*W+k])) p=r;
+        if(p!=k) for(int q=0;q<W;q++) {double t=a[k*W+q];a[k*W+q]=a[p*W+q];a[p*W+q]=t;}
+        const double iv=1.0/a[k*W+k];
+        for(int q=0;q<W;q++) a[k*W+q]*=iv;
+        for(int r=0;r<N;r++) {
+            if(r==k) continue;
+            const double f=a[r*W+k];
+            if(f==0) continue;
+            for(int q=0;q<W;q++) a[r*W+q]-=f*a[k*W+q];
+        }
+    }
+    for(int r=0;r<N;r++) for(int q=0;q<N;q++) ginv[r*N+q]=a[r*W+N+q];
+    delete [] a;
 }
 
 /** Rebuilds every coarse operator by the Galerkin product P^T A P. */
@@ -204,6 +257,7 @@ void tgmg<S,V,M>::setup() {
             galerkin(f,f.m,f.n,f.x_prd,f.y_prd,*lev[l],cx[l-1],cy[l-1]);
         }
     }
+    if(nlev>1&&lev[nlev-1]->mn<=tgmg_direct_max) coarse_inverse();
 }
 
 template<class S,class V,class M>
@@ -323,7 +377,15 @@ template<class S,class V,class M>
 void tgmg<S,V,M>::cycle(int l) {
     if(l==nlev-1) {
         if(l==0) this->smooth(tgmg_coarse_sweeps);
-        else lb[l]->smooth(tgmg_coarse_sweeps);
+        else if(ginv!=NULL) {
+            tgmg_level<V,M> &c=*lev[l];
+            const int N=c.mn;
+            for(int r=0;r<N;r++) {
+                double t=0;
+                for(int q=0;q<N;q++) t+=ginv[r*N+q]*c.b[q];
+                c.z[r]=t;
+            }
+        } else lb[l]->smooth(tgmg_coarse_sweeps);
         return;
     }
     tgmg_level<V,M> &c=*lev[l+1];

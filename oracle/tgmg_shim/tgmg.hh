@@ -22,7 +22,10 @@
  * which is red-black ordering for a 5-point stencil and race-free for a
  * 9-point one. A V-cycle does tgmg_nu1 sweeps, restricts the residual,
  * recurses with a zero coarse guess, prolongs the correction and does
- * tgmg_nu2 sweeps; the coarsest level does tgmg_coarse_sweeps sweeps. A solve
+ * tgmg_nu2 sweeps; the coarsest level is solved exactly with a dense inverse
+ * built at setup: A^-1, or (A + c e e^T)^-1 with c the mean diagonal / N when
+ * A is the singular pure-Neumann operator (zero row sums, null space the
+ * constants), which yields the solution of zero mean. A solve
  * runs V-cycles until ||b-Az||_2 <= max(rtol*||b||_2, acc). */
 #ifndef TGMG_HH
 #define TGMG_HH
@@ -115,6 +118,9 @@ class tgmg : public tgmg_base<S,V,M> {
         int last_vcycles;
         /** Residual norm ratio ||b-Az||/||b|| reached by the most recent solve. */
         double last_rel_res;
+        /** Dense inverse of the coarsest operator (regularised when singular),
+         * or NULL when the coarsest level is solved by sweeps. */
+        double *ginv;
         tgmg(S &s_,V *b_,V *z_);
         ~tgmg();
         void setup();
@@ -133,6 +139,7 @@ class tgmg : public tgmg_base<S,V,M> {
         void galerkin(T &fs,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
         void restrict_to(V *r,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
         void prolong_add(V *zf,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
+        void coarse_inverse();
 };
 
 #endif

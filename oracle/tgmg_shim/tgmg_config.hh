@@ -22,8 +22,12 @@
 const int tgmg_nu1=2;
 /** Gauss-Seidel sweeps after the coarse-grid correction. */
 const int tgmg_nu2=2;
-/** Gauss-Seidel sweeps used as the solve on the coarsest level. */
+/** Gauss-Seidel sweeps used as the solve on the coarsest level when that
+ * level is the finest one (a grid too small to coarsen). */
 const int tgmg_coarse_sweeps=64;
+/** Coarse levels with at most this many unknowns are solved exactly, by a
+ * dense inverse built at setup. */
+const int tgmg_direct_max=96;
 /** Coarsening stops once a level has at most this many unknowns. */
 const int tgmg_coarsest_size=64;
 /** Maximum number of levels in a hierarchy. */

@@ -748,8 +748,9 @@ int Multigrid::build_hierarchy() {
         const long N = lev.back().N;
         INCRMT_CK(cudaMalloc(&ginv, sizeof(double) * N * N));
         INCRMT_CK(cudaMalloc(&ginvf, sizeof(float) * N * N));
+        // The attribute is per kernel, shared by every solver: set the maximum.
         INCRMT_CK(cudaFuncSetAttribute(k_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(sizeof(double) * (2 * N * N + N))));
+                                       static_cast<int>(sizeof(double) * (2 * kDirectMax * kDirectMax + kDirectMax))));
     }
     INCRMT_CK(cudaFuncSetAttribute(k_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTailSmemBudget)));

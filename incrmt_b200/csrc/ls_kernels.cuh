@@ -652,18 +652,38 @@ __global__ void k_ls_collect_candidates(LsGrid g, const int *s, const int *near,
     if ((st == 0 || st == 7) && near[ij]) list[atomicAdd(count, 1)] = ij;
 }
 
+/** Whether any point the stencil of (i,j) reads (up to two cells along
+ * each axis) changed in the previous sweep. */
+__device__ __forceinline__ bool stencil_changed(const LsGrid &g, const unsigned char *chg, int i, int j) {
+    const int P = g.P, ij = j * P + i;
+    if (chg[ij]) return true;
+    for (int d = 1; d <= 2; d++) {
+        if (i - d >= 0 && chg[ij - d]) return true;
+        if (i + d < g.mL && chg[ij + d]) return true;
+        if (j - d >= 0 && chg[ij - d * P]) return true;
+        if (j + d < g.nL && chg[ij + d * P]) return true;
+    }
+    return false;
+}
+
 /** All sweeps of the march fixed point in one cooperative launch: every
  * sweep evaluates the stencil at the listed candidates (Jacobi, reading cur,
  * writing nxt), a grid barrier follows, and the loop ends after the first
- * sweep that changed nothing. flags[0..2] rotate as per-sweep change flags;
- * flags[3] receives the number of sweeps and flags[4] 1 if converged. */
+ * sweep that changed nothing. A candidate whose stencil inputs did not change
+ * in the previous sweep keeps its value (its stencil would return it again),
+ * so later sweeps only touch the moving front; chg_a/chg_b are per-point
+ * change marks of the previous and the current sweep (cleared by the caller).
+ * flags[0..2] rotate as per-sweep change flags; flags[3] receives the number
+ * of sweeps and flags[4] 1 if converged. */
 __global__ void k_ls_fim_coop(LsGrid g, const double *phi, const int *s, double *a, double *b, const int *list,
-                              const int *countp, int *flags, int max_sweeps) {
+                              const int *countp, int *flags, int max_sweeps, unsigned char *chg_a,
+                              unsigned char *chg_b) {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     const int count = *countp;
     double *cur = a, *nxt = b;
+    unsigned char *cprev = chg_a, *cnow = chg_b;
     int it = 0;
     bool done = false;
     for (; it < max_sweeps; it++) {
@@ -673,22 +693,25 @@ __global__ void k_ls_fim_coop(LsGrid g, const double *phi, const int *s, double 
             const int ij = list[t], i = ij % g.P, j = ij / g.P, st = s[ij];
             const double old = cur[ij];
             double v = old;
-            if (st == 7) {
-                March<true> mr(g, phi, s, cur, old);
-                if (any_in(mr, i, j)) v = mr.calc(i, j);
-            } else {
-                March<false> mr(g, phi, s, cur, old);
-                if (any_in(mr, i, j)) v = mr.calc(i, j);
+            if (it == 0 || stencil_changed(g, cprev, i, j)) {
+                if (st == 7) {
+                    March<true> mr(g, phi, s, cur, old);
+                    if (any_in(mr, i, j)) v = mr.calc(i, j);
+                } else {
+                    March<false> mr(g, phi, s, cur, old);
+                    if (any_in(mr, i, j)) v = mr.calc(i, j);
+                }
             }
             nxt[ij] = v;
-            if (v != old) ch = true;
+            const bool c = v != old;
+            cnow[ij] = c;
+            if (c) ch = true;
         }
-        // One store per block; the flag is read once per thread after the
-        // barrier with a volatile load (no atomics on a single address).
         if (__syncthreads_or(ch) && threadIdx.x == 0) flags[it % 3] = 1;
         grid.sync();
         const int c = *reinterpret_cast<volatile int *>(&flags[it % 3]);
         double *t = cur; cur = nxt; nxt = t;
+        unsigned char *u = cprev; cprev = cnow; cnow = u;
         if (!c) { done = true; break; }
     }
     if (tid == 0) { flags[3] = done ? it + 1 : it; flags[4] = done ? 1 : 0; }

@@ -423,7 +423,7 @@ __global__ void k_coarse_direct(const T *G, const T *b, T *z, int N) {
 
 /** Levels handled by the one-block tail kernel. */
 constexpr int kTailMaxLevels = 12;
-constexpr int kTailMaxSize = 4096;  // unknowns of the first tail level at most
+constexpr int kTailMaxSize = 1024;  // unknowns of the first tail level at most
 constexpr size_t kTailSmemBudget = 160 * 1024;  // shared memory for the smallest tail levels
 
 template <class T>
@@ -634,12 +634,17 @@ const dim3 kBlk2(32, 8);
 template <class Op, class T>
 int smooth(Op op, T *z, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl,
            Multigrid *prof = nullptr, double bytes_per_unit = 0) {
-    constexpr int TW = 64, TH = 32;
-    if (!op.px && !op.py && sweeps == 2 && cdiv(m, TW) * cdiv(n, TH) >= 2 * kB200SMs) {
-        // Two sweeps per launch with shared-memory tiles (identical results),
-        // on grids large enough to fill the GPU with tiles.
+    if (!op.px && !op.py && sweeps == 2) {
+        // Two sweeps per launch with shared-memory tiles (identical results);
+        // the largest tile that still gives every SM work, else the smallest.
+        const dim3 b64(cdiv(m, 64), cdiv(n, 32)), b32(cdiv(m, 32), cdiv(n, 16)), b16(cdiv(m, 16), cdiv(n, 16));
         if (prof) { int r = prof->prof_begin(static_cast<double>(m) * n * 2 * bytes_per_unit); if (r) return r; }
-        k_smooth_tile<Op, T, 2, TW, TH><<<dim3(cdiv(m, TW), cdiv(n, TH)), 256, 0, s>>>(op, z, b, m, n);
+        if (static_cast<int>(b64.x * b64.y) >= 2 * kB200SMs)
+            k_smooth_tile<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, b, m, n);
+        else if (static_cast<int>(b32.x * b32.y) >= kB200SMs)
+            k_smooth_tile<Op, T, 2, 32, 16><<<b32, 256, 0, s>>>(op, z, b, m, n);
+        else
+            k_smooth_tile<Op, T, 2, 16, 16><<<b16, 256, 0, s>>>(op, z, b, m, n);
         nl++;
         if (prof) { int r = prof->prof_end(); if (r) return r; }
         INCRMT_CKL("k_smooth_tile");

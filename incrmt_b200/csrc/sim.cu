@@ -37,6 +37,7 @@ struct Sim {
     double *ls_a = nullptr, *ls_b = nullptr;       // march / extrapolation buffers (x)
     double *ls_c = nullptr, *ls_d = nullptr;       // extrapolation buffers (y)
     int *d_list = nullptr, *d_ia = nullptr, *d_ib = nullptr;
+    unsigned char *d_chg = nullptr;                 // change marks of the march sweeps (2 x cells)
     int coop_blocks_fim = 0, coop_blocks_ext = 0;   // co-resident grid sizes
     int *d_flags = nullptr;  // [0..2] sweep change flags, [3] sweeps, [4] converged, [5] fit error,
                            // [6] Newton error, [7] list length, [8] tracer remaps, [9] correction failure
@@ -138,6 +139,7 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     INCRMT_CK(cudaMalloc(&d_list, sizeof(int) * cells()));
     INCRMT_CK(cudaMalloc(&d_ia, sizeof(int) * cells()));
     INCRMT_CK(cudaMalloc(&d_ib, sizeof(int) * cells()));
+    INCRMT_CK(cudaMalloc(&d_chg, 2 * cells()));
     {
         int dev = 0, sms = 0, nb = 0;
         INCRMT_CK(cudaGetDevice(&dev));
@@ -268,7 +270,9 @@ int Sim::build_band(int k) {
     double *pa = ls_a, *pb = ls_b;
     const double *phic = s.phi;
     const int *sc = s.s;
-    void *args[] = {&lg, &phic, &sc, &pa, &pb, &d_list, &countp, &d_flags, &maxs};
+    INCRMT_CK(cudaMemsetAsync(d_chg, 0, 2 * cells(), stream));
+    unsigned char *ca = d_chg, *cb = d_chg + cells();
+    void *args[] = {&lg, &phic, &sc, &pa, &pb, &d_list, &countp, &d_flags, &maxs, &ca, &cb};
     INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_fim_coop), dim3(coop_blocks_fim), dim3(256),
                                           args, 0, stream));
     launches++;
@@ -569,7 +573,7 @@ void Sim::destroy() {
     for (double *p : allocs) cudaFree(p);
     allocs.clear();
     for (auto &s : sol) cudaFree(s.s);
-    cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_list); cudaFree(d_ia); cudaFree(d_ib); cudaFree(d_flags);
+    cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_list); cudaFree(d_ia); cudaFree(d_ib); cudaFree(d_chg); cudaFree(d_flags);
     if (h_flags) cudaFreeHost(h_flags);
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;

@@ -81,32 +81,39 @@ __host__ __device__ constexpr double pw_int(int t, int k) {
     return (t - 2 * k == 0) ? 1.0 : ((t - 2 * k == 1 || t - 2 * k == -1) ? 0.5 : 0.0);
 }
 
-/** Galerkin product at an interior coarse unknown, fully unrolled so the 81
- * fine stencil entries stay in registers. */
+/** Galerkin product at an interior coarse unknown, compactly: each of the
+ * 81 products (fine point 2I+t, stencil entry d) lands on the coarse
+ * neighbours k with |t+d-2k| <= 1, at most four, with weights 1 or 1/2. The
+ * nine accumulators live in the thread's slice of shared memory (q). */
 template <class Op>
-__device__ __forceinline__ void galerkin_interior(const Op &op, int I, int J, double q[9]) {
-#pragma unroll
+__device__ __forceinline__ void galerkin_interior(const Op &op, int I, int J, double *q) {
     for (int k = 0; k < 9; k++) q[k] = 0;
-#pragma unroll
-    for (int ty = -1; ty <= 1; ty++) {
-#pragma unroll
+    for (int ty = -1; ty <= 1; ty++)
         for (int tx = -1; tx <= 1; tx++) {
             double a[9];
             op.coef9(2 * I + tx, 2 * J + ty, a);
-            const double w = pw_int(tx, 0) * pw_int(ty, 0);
-#pragma unroll
-            for (int dj = -1; dj <= 1; dj++)
-#pragma unroll
-                for (int di = -1; di <= 1; di++)
-#pragma unroll
-                    for (int kj = -1; kj <= 1; kj++)
-#pragma unroll
-                        for (int ki = -1; ki <= 1; ki++) {
-                            const double v = pw_int(tx + di, ki) * pw_int(ty + dj, kj);
-                            if (v != 0.0) q[3 * (kj + 1) + ki + 1] += w * a[3 * (dj + 1) + di + 1] * v;
+            const double w = (tx == 0 ? 1.0 : 0.5) * (ty == 0 ? 1.0 : 0.5);
+            for (int dj = -1; dj <= 1; dj++) {
+                const int sy = ty + dj;
+                const int ky0 = sy <= 0 ? -1 : 0, ky1 = sy >= 0 ? 1 : 0;
+                for (int di = -1; di <= 1; di++) {
+                    const double av = a[3 * (dj + 1) + di + 1];
+                    if (av == 0) continue;
+                    const int sx = tx + di;
+                    const int kx0 = sx <= 0 ? -1 : 0, kx1 = sx >= 0 ? 1 : 0;
+                    for (int kj = ky0; kj <= ky1; kj++) {
+                        const int ey = sy - 2 * kj;
+                        if (ey < -1 || ey > 1) continue;
+                        const double vy = ey == 0 ? 1.0 : 0.5;
+                        for (int ki = kx0; ki <= kx1; ki++) {
+                            const int ex = sx - 2 * ki;
+                            if (ex < -1 || ex > 1) continue;
+                            q[3 * (kj + 1) + ki + 1] += w * av * vy * (ex == 0 ? 1.0 : 0.5);
                         }
+                    }
+                }
+            }
         }
-    }
 }
 
 /** Galerkin coarse stencil A_c = P^T A P, one coarse unknown per thread. */
@@ -118,9 +125,9 @@ __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool 
     const long N = static_cast<long>(cm) * cn;
     const int ij = I + cm * J;
     if (kx && ky && I >= 1 && J >= 1 && I <= cm - 2 && J <= cn - 2 && 2 * I + 2 <= fm - 1 && 2 * J + 2 <= fn - 1) {
-        double q[9];
+        __shared__ double qs[9 * 256];
+        double *q = qs + 9 * (threadIdx.x + blockDim.x * threadIdx.y);
         galerkin_interior(op, I, J, q);
-#pragma unroll
         for (int k = 0; k < 9; k++) st[k * N + ij] = q[k];
         return;
     }
@@ -372,11 +379,20 @@ __global__ void k_coarse_inverse(const double *st, int m, int n, int px, int py,
         for (int q = threadIdx.x; q < N * N; q += blockDim.x) a[static_cast<long>(q / N) * W + q % N] += creg;
     __syncthreads();
     for (int k = 0; k < N; k++) {
-        if (threadIdx.x == 0) {
-            int p = k;
-            for (int r = k + 1; r < N; r++)
-                if (fabs(a[static_cast<long>(r) * W + k]) > fabs(a[static_cast<long>(p) * W + k])) p = r;
-            piv = p;
+        if (threadIdx.x < 32) {
+            // warp argmax of |a(r,k)|, r >= k; ties go to the lower row
+            int p = -1;
+            double best = -1;
+            for (int r = k + threadIdx.x; r < N; r += 32) {
+                const double v = fabs(a[static_cast<long>(r) * W + k]);
+                if (v > best) { best = v; p = r; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_down_sync(0xffffffffu, best, o);
+                const int op_ = __shfl_down_sync(0xffffffffu, p, o);
+                if (ob > best || (ob == best && op_ >= 0 && (p < 0 || op_ < p))) { best = ob; p = op_; }
+            }
+            if (threadIdx.x == 0) piv = p;
         }
         __syncthreads();
         const int p = piv;

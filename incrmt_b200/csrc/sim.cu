@@ -144,10 +144,16 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
         int dev = 0, sms = 0, nb = 0;
         INCRMT_CK(cudaGetDevice(&dev));
         INCRMT_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        // One block per SM: the grid barrier of the cooperative sweeps costs
+        // more with more blocks, and the candidate lists are ~1e4-1e5 points.
         INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_fim_coop, 256, 0));
-        coop_blocks_fim = sms * (nb > 0 ? nb : 1);
+        coop_blocks_fim = sms * (nb > 0 ? 1 : 0);
         INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_extrap_coop, 256, 0));
-        coop_blocks_ext = sms * (nb > 0 ? nb : 1);
+        coop_blocks_ext = sms * (nb > 0 ? 1 : 0);
+        if (coop_blocks_fim == 0 || coop_blocks_ext == 0) {
+            set_error("level-set kernels cannot be co-resident");
+            return INCRMT_ERR_CUDA;
+        }
     }
     INCRMT_CK(cudaMalloc(&d_flags, sizeof(int) * 16));
     INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 16, stream));

@@ -258,6 +258,13 @@ def run_ours_sspin(args, ws, rank, local, dist):
     value = ws * args.steps / (ms_max / 1e3)
     vc = ((st1.vcycles_mac - st0.vcycles_mac) + (st1.vcycles_fem - st0.vcycles_fem)) / (2.0 * args.steps)
 
+    # Phase breakdown of a few extra steps, timed by CUDA events on the stream
+    # (outside the timed region).
+    sim.set_profiling(True)
+    sim.step(dt, min(args.steps, 10))
+    phases = {k: v / min(args.steps, 10) for k, v in sim.profile().items()}
+    sim.set_profiling(False)
+
     # End to end through the C ABI as fluid_2d::solve drives it: the steps of
     # one frame, then the frame's fields copied to host buffers (p, u, v for
     # the vorticity, X, Y, phi; fluid_2d::write_files, fluid_2d_io.cc:60-102).
@@ -295,6 +302,7 @@ def run_ours_sspin(args, ws, rank, local, dist):
                    "precision": args.precision, "flush": "working set larger than L2",
                    "parallelism": f"replicas x{ws}"},
         "vcycles_per_projection": vc,
+        "phase_ms_per_step": phases,
         "march_sweeps_per_step": (st1.march_sweeps - st0.march_sweeps) / args.steps,
         "extrap_sweeps_per_step": (st1.extrap_sweeps - st0.extrap_sweeps) / args.steps,
         "roofline": None,

@@ -127,6 +127,26 @@ int incrmt_record_track(incrmt_sim *h);
 
 int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st);
 
+/** Phases of a step timed by the profiler (device milliseconds). */
+#define INCRMT_PHASE_TRACERS   0  /* tracer stages */
+#define INCRMT_PHASE_ADVECTION 1  /* normal derivatives, Godunov, half-time edge values */
+#define INCRMT_PHASE_MAC       2  /* MAC source, V-cycles, correction */
+#define INCRMT_PHASE_REFMAP    3  /* reference-map update (without the extrapolation) */
+#define INCRMT_PHASE_EXTRAP    4  /* reference-map extrapolation */
+#define INCRMT_PHASE_PIN       5  /* pinning, band rebuild, density */
+#define INCRMT_PHASE_STRESS    6  /* boundaries, stress, u*, velocity update */
+#define INCRMT_PHASE_FEM       7  /* FEM source, V-cycles, pressure copy */
+#define INCRMT_PHASE_MG_SETUP  8  /* coefficients and Galerkin hierarchy of both projections */
+#define INCRMT_PHASES          9
+
+/** Turns phase timing on or off (CUDA events on the handle's stream; no
+ * reference counterpart) and clears the accumulated times. */
+int incrmt_sim_set_profiling(incrmt_sim *h, int on);
+
+/** Accumulated device time per phase since profiling was turned on
+ * (INCRMT_PHASES doubles, milliseconds). */
+int incrmt_sim_profile(incrmt_sim *h, double *ms);
+
 /** The handle's CUDA stream (a cudaStream_t). */
 void *incrmt_sim_stream(const incrmt_sim *h);
 

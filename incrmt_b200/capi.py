@@ -258,6 +258,8 @@ def _sim_sigs(L):
     L.incrmt_track_records.argtypes = [P, dp, I, ctypes.POINTER(I), I]
     L.incrmt_record_track.argtypes = [P]
     L.incrmt_get_stats.argtypes = [P, ctypes.POINTER(SimStats)]
+    L.incrmt_sim_set_profiling.argtypes = [P, I]
+    L.incrmt_sim_profile.argtypes = [P, dp]
     L.incrmt_sim_stream.argtypes = [P]
     L.incrmt_sim_stream.restype = P
     L.incrmt_destroy.argtypes = [P]
@@ -367,6 +369,18 @@ class Simulation:
         s = SimStats()
         check(lib().incrmt_get_stats(self._h, ctypes.byref(s)))
         return s
+
+    PHASES = ["tracers", "advection", "mac", "refmap", "extrapolation", "pin_and_band", "stress",
+              "fem", "mg_setup"]
+
+    def set_profiling(self, on=True):
+        check(lib().incrmt_sim_set_profiling(self._h, int(on)))
+
+    def profile(self):
+        """Device ms per step phase since profiling was turned on."""
+        out = np.zeros(len(self.PHASES))
+        check(lib().incrmt_sim_profile(self._h, _dptr(out)))
+        return dict(zip(self.PHASES, out.tolist()))
 
     def stream(self):
         return lib().incrmt_sim_stream(self._h)

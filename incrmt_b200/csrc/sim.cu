@@ -58,6 +58,49 @@ struct Sim {
     int t_correction = 1;
     int pre_stress_objects = 0;
     std::vector<double> track;                      // records: time, xpre, ypre, x, y
+    // Optional phase timing: CUDA events on the stream at phase boundaries.
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_phase;                      // phase of each recorded (start,end) pair
+    int ev_used = 0;
+    double phase_ms[INCRMT_PHASES] = {0};
+    long long phase_n[INCRMT_PHASES] = {0};
+    int cur_phase = -1;
+    int phase_begin(int ph) {
+        if (!prof) return INCRMT_OK;
+        if (ev_used + 2 > static_cast<int>(ev_pool.size())) {
+            if (ev_used + 2 > 8192) { int r = phase_collect(); if (r) return r; }
+            while (ev_used + 2 > static_cast<int>(ev_pool.size())) {
+                cudaEvent_t e;
+                INCRMT_CK(cudaEventCreate(&e));
+                ev_pool.push_back(e);
+            }
+        }
+        INCRMT_CK(cudaEventRecord(ev_pool[ev_used], stream));
+        cur_phase = ph;
+        return INCRMT_OK;
+    }
+    int phase_end() {
+        if (!prof || cur_phase < 0) return INCRMT_OK;
+        INCRMT_CK(cudaEventRecord(ev_pool[ev_used + 1], stream));
+        if (static_cast<int>(ev_phase.size()) <= ev_used / 2) ev_phase.resize(ev_used / 2 + 1);
+        ev_phase[ev_used / 2] = cur_phase;
+        ev_used += 2;
+        cur_phase = -1;
+        return INCRMT_OK;
+    }
+    int phase_collect() {
+        if (ev_used == 0) return INCRMT_OK;
+        INCRMT_CK(cudaStreamSynchronize(stream));
+        for (int k = 0; k + 1 < ev_used; k += 2) {
+            float ms = 0;
+            INCRMT_CK(cudaEventElapsedTime(&ms, ev_pool[k], ev_pool[k + 1]));
+            phase_ms[ev_phase[k / 2]] += ms;
+            phase_n[ev_phase[k / 2]]++;
+        }
+        ev_used = 0;
+        return INCRMT_OK;
+    }
 
     int alloc(double **p, size_t n) {
         INCRMT_CK(cudaMalloc(p, sizeof(double) * n));
@@ -345,9 +388,13 @@ int Sim::update_reference_map(double dt) {
         launches++;
         INCRMT_CKL("k_refmap_update");
     }
-    int r;
+    int r, outer = cur_phase;
+    if ((r = phase_end())) return r;
+    if ((r = phase_begin(INCRMT_PHASE_EXTRAP))) return r;
     for (size_t k = 0; k < obj.size(); k++)
         if ((r = extrapolate(static_cast<int>(k)))) return r;
+    if ((r = phase_end())) return r;
+    if ((r = phase_begin(outer))) return r;
     for (size_t k = 0; k < obj.size(); k++) {
         k_refmap_half<<<g2(g.m, g.n), kB2, 0, stream>>>(g, sol[k]);
         launches++;
@@ -361,8 +408,13 @@ int Sim::mac_projection() {
     k_mac_source<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, src_mac);
     launches++;
     INCRMT_CKL("k_mac_source");
-    int r = mac.set_density_device(f.rho, g.P);
+    int outer = cur_phase, r;
+    if ((r = phase_end())) return r;
+    if ((r = phase_begin(INCRMT_PHASE_MG_SETUP))) return r;
+    r = mac.set_density_device(f.rho, g.P);
     if (r) return r;
+    if ((r = phase_end())) return r;
+    if ((r = phase_begin(outer))) return r;
     incrmt_mg_stats st{};
     long long l0 = mac.launches;
     r = mac.solve_device(src_mac, z_mac, &mgo, &st, false);
@@ -382,8 +434,13 @@ int Sim::fem_projection(double dt) {
     k_fem_source<<<g2(g.mf, g.nf), kB2, 0, stream>>>(g, f, src_fem, dt);
     launches++;
     INCRMT_CKL("k_fem_source");
-    int r = fem.set_density_device(f.rho, g.P);
+    int outer = cur_phase, r;
+    if ((r = phase_end())) return r;
+    if ((r = phase_begin(INCRMT_PHASE_MG_SETUP))) return r;
+    r = fem.set_density_device(f.rho, g.P);
     if (r) return r;
+    if ((r = phase_end())) return r;
+    if ((r = phase_begin(outer))) return r;
     incrmt_mg_stats st{};
     long long l0 = fem.launches;
     r = fem.solve_device(src_fem, z_fem, &mgo, &st, false);
@@ -507,32 +564,42 @@ int Sim::step(double dt) {
     const int no = static_cast<int>(obj.size());
     const double ntime = time + dt;
     int r;
-    if ((r = tracers(1, dt))) return r;
-    k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
-    k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
-    k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f);
-    k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
-    k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
-    launches += 5;
-    INCRMT_CKL("advection");
+#define INCRMT_PHASE(ph, ...) do { if ((r = phase_begin(ph))) return r; __VA_ARGS__; if ((r = phase_end())) return r; } while (0)
+    INCRMT_PHASE(INCRMT_PHASE_TRACERS, if ((r = tracers(1, dt))) return r);
+    INCRMT_PHASE(INCRMT_PHASE_ADVECTION, {
+        k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
+        k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+        k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f);
+        k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
+        k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+        launches += 5;
+        INCRMT_CKL("advection");
+    });
     time += 0.5 * dt;
-    if ((r = mac_projection())) return r;
-    if ((r = update_reference_map(dt))) return r;
-    if ((r = pin())) return r;
-    if ((r = set_boundaries())) return r;
-    if ((r = compute_stress())) return r;
-    k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
-    launches++;
-    INCRMT_CKL("k_ustar");
+    INCRMT_PHASE(INCRMT_PHASE_MAC, if ((r = mac_projection())) return r);
+    INCRMT_PHASE(INCRMT_PHASE_REFMAP, if ((r = update_reference_map(dt))) return r);
+    INCRMT_PHASE(INCRMT_PHASE_PIN, if ((r = pin())) return r);
+    INCRMT_PHASE(INCRMT_PHASE_STRESS, {
+        if ((r = set_boundaries())) return r;
+        if ((r = compute_stress())) return r;
+        k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
+        launches++;
+        INCRMT_CKL("k_ustar");
+    });
     time = ntime;
-    if ((r = fem_projection(dt))) return r;
-    k_update_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
-    launches++;
-    INCRMT_CKL("k_update_velocity");
-    if ((r = pin())) return r;
-    if ((r = set_boundaries())) return r;
-    if ((r = compute_stress())) return r;
-    if ((r = tracers(2, dt))) return r;
+    INCRMT_PHASE(INCRMT_PHASE_FEM, if ((r = fem_projection(dt))) return r);
+    INCRMT_PHASE(INCRMT_PHASE_STRESS, {
+        k_update_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
+        launches++;
+        INCRMT_CKL("k_update_velocity");
+    });
+    INCRMT_PHASE(INCRMT_PHASE_PIN, if ((r = pin())) return r);
+    INCRMT_PHASE(INCRMT_PHASE_STRESS, {
+        if ((r = set_boundaries())) return r;
+        if ((r = compute_stress())) return r;
+    });
+    INCRMT_PHASE(INCRMT_PHASE_TRACERS, if ((r = tracers(2, dt))) return r);
+#undef INCRMT_PHASE
     steps++;
     return INCRMT_OK;
 }
@@ -581,6 +648,8 @@ void Sim::destroy() {
     for (auto &s : sol) cudaFree(s.s);
     cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_list); cudaFree(d_ia); cudaFree(d_ib); cudaFree(d_chg); cudaFree(d_flags);
     if (h_flags) cudaFreeHost(h_flags);
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    ev_pool.clear();
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }
@@ -806,6 +875,24 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;
     st->time = S.time;
+    return INCRMT_OK;
+}
+
+int incrmt_sim_set_profiling(incrmt_sim *h, int on) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    int r = S.phase_collect();
+    if (r) return r;
+    S.prof = on != 0;
+    for (int k = 0; k < INCRMT_PHASES; k++) { S.phase_ms[k] = 0; S.phase_n[k] = 0; }
+    return INCRMT_OK;
+}
+
+int incrmt_sim_profile(incrmt_sim *h, double *ms) {
+    if (!h || !ms) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    int r = h->s.phase_collect();
+    if (r) return r;
+    for (int k = 0; k < INCRMT_PHASES; k++) ms[k] = h->s.phase_ms[k];
     return INCRMT_OK;
 }
 

@@ -7,7 +7,7 @@ namespace incrmt {
 
 namespace {
 
-constexpr int kNu1 = 2, kNu2 = 2, kCoarseSweeps = 64, kCoarsestSize = 64, kMaxLevels = 24;
+constexpr int kNu1 = 2, kNu2 = 2, kCoarseSweeps = 64, kCoarsestSize = 16, kMaxLevels = 24;
 
 // ---------------------------------------------------------------------------
 // Transfer-operator index helpers (identical rules to the CPU oracle's shim).
@@ -75,65 +75,20 @@ __global__ void k_fem_coef(const double *rho, int ml, int mf, int nf, double *c,
     cf[j * mf + i] = static_cast<float>(v);
 }
 
-/** 1D prolongation weight of fine offset t (fine 2I+t) to coarse offset k
- * (coarse I+k) away from any boundary: 1 on the coarse point, 1/2 next to it. */
-__host__ __device__ constexpr double pw_int(int t, int k) {
-    return (t - 2 * k == 0) ? 1.0 : ((t - 2 * k == 1 || t - 2 * k == -1) ? 0.5 : 0.0);
-}
 
-/** Galerkin product at an interior coarse unknown, compactly: each of the
- * 81 products (fine point 2I+t, stencil entry d) lands on the coarse
- * neighbours k with |t+d-2k| <= 1, at most four, with weights 1 or 1/2. The
- * nine accumulators live in the thread's slice of shared memory (q). */
+/** One entry (target offset ki,kj) of the Galerkin coarse stencil
+ * A_c = P^T A P at coarse unknown (I,J), by one thread: the sum over the
+ * fine support points f of (I,J) and their stencil entries of
+ * P(f,I,J) * A(f,g) * P(g,(I+ki,J+kj)). */
 template <class Op>
-__device__ __forceinline__ void galerkin_interior(const Op &op, int I, int J, double *q) {
-    for (int k = 0; k < 9; k++) q[k] = 0;
-    for (int ty = -1; ty <= 1; ty++)
-        for (int tx = -1; tx <= 1; tx++) {
-            double a[9];
-            op.coef9(2 * I + tx, 2 * J + ty, a);
-            const double w = (tx == 0 ? 1.0 : 0.5) * (ty == 0 ? 1.0 : 0.5);
-            for (int dj = -1; dj <= 1; dj++) {
-                const int sy = ty + dj;
-                const int ky0 = sy <= 0 ? -1 : 0, ky1 = sy >= 0 ? 1 : 0;
-                for (int di = -1; di <= 1; di++) {
-                    const double av = a[3 * (dj + 1) + di + 1];
-                    if (av == 0) continue;
-                    const int sx = tx + di;
-                    const int kx0 = sx <= 0 ? -1 : 0, kx1 = sx >= 0 ? 1 : 0;
-                    for (int kj = ky0; kj <= ky1; kj++) {
-                        const int ey = sy - 2 * kj;
-                        if (ey < -1 || ey > 1) continue;
-                        const double vy = ey == 0 ? 1.0 : 0.5;
-                        for (int ki = kx0; ki <= kx1; ki++) {
-                            const int ex = sx - 2 * ki;
-                            if (ex < -1 || ex > 1) continue;
-                            q[3 * (kj + 1) + ki + 1] += w * av * vy * (ex == 0 ? 1.0 : 0.5);
-                        }
-                    }
-                }
-            }
-        }
-}
-
-/** Galerkin coarse stencil A_c = P^T A P, one coarse unknown per thread. */
-template <class Op>
-__global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
-                           int cm, int cn, double *st) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
-    if (I >= cm || J >= cn) return;
-    const long N = static_cast<long>(cm) * cn;
-    const int ij = I + cm * J;
-    if (kx && ky && I >= 1 && J >= 1 && I <= cm - 2 && J <= cn - 2 && 2 * I + 2 <= fm - 1 && 2 * J + 2 <= fn - 1) {
-        __shared__ double qs[9 * 256];
-        double *q = qs + 9 * (threadIdx.x + blockDim.x * threadIdx.y);
-        galerkin_interior(op, I, J, q);
-        for (int k = 0; k < 9; k++) st[k * N + ij] = q[k];
-        return;
-    }
-    double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+__device__ __forceinline__ double galerkin_entry(const Op &op, int fm, int fn, int px, int py, bool kx, bool ky,
+                                                 int cm, int cn, int I, int J, int ki, int kj) {
+    bool okt = true;
+    const int Kx = wrap_idx(I + ki, cm, px, okt), Ky = wrap_idx(J + kj, cn, py, okt);
+    if (!okt) return 0;
     int fx[3], fy[3];
     const int nfx = support(I, fm, px, kx, fx), nfy = support(J, fn, py, ky, fy);
+    double q = 0;
     for (int b = 0; b < nfy; b++) {
         const double wy = pw(fy[b], J, fn, cn, py, ky);
         for (int a = 0; a < nfx; a++) {
@@ -145,33 +100,34 @@ __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool 
                 bool oky = true;
                 const int gy = wrap_idx(fy[b] + dj, fn, py, oky);
                 if (!oky) continue;
+                const double vy = pw(gy, Ky, fn, cn, py, ky);
+                if (vy == 0) continue;
                 for (int di = -1; di <= 1; di++) {
                     const double av = s[3 * (dj + 1) + di + 1];
                     if (av == 0) continue;
                     bool okx = true;
                     const int gx = wrap_idx(fx[a] + di, fm, px, okx);
                     if (!okx) continue;
-                    for (int kj = -1; kj <= 1; kj++) {
-                        bool ok = true;
-                        const int Ky = wrap_idx(J + kj, cn, py, ok);
-                        if (!ok) continue;
-                        const double vy = pw(gy, Ky, fn, cn, py, ky);
-                        if (vy == 0) continue;
-                        for (int ki = -1; ki <= 1; ki++) {
-                            bool ok2 = true;
-                            const int Kx = wrap_idx(I + ki, cm, px, ok2);
-                            if (!ok2) continue;
-                            const double vx = pw(gx, Kx, fm, cm, px, kx);
-                            if (vx == 0) continue;
-                            q[3 * (kj + 1) + ki + 1] += w * av * vx * vy;
-                        }
-                    }
+                    const double vx = pw(gx, Kx, fm, cm, px, kx);
+                    if (vx != 0) q += w * av * vx * vy;
                 }
             }
         }
     }
-#pragma unroll
-    for (int k = 0; k < 9; k++) st[k * N + ij] = q[k];
+    return q;
+}
+
+/** Galerkin coarse stencil A_c = P^T A P: one thread per coarse unknown and
+ * stencil entry (blockIdx.z = entry), so that the boundary rows, whose
+ * weights need the general index rules, cost no more than the others. */
+template <class Op>
+__global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
+                           int cm, int cn, double *st) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= cm || J >= cn) return;
+    const int e = blockIdx.z, ki = e % 3 - 1, kj = e / 3 - 1;
+    const long N = static_cast<long>(cm) * cn;
+    st[e * N + I + static_cast<long>(cm) * J] = galerkin_entry(op, fm, fn, px, py, kx, ky, cm, cn, I, J, ki, kj);
 }
 
 __global__ void k_cast(const double *a, float *b, long n) {
@@ -821,12 +777,12 @@ int Multigrid::galerkin_all() {
         MgLevel &F = lev[l - 1], &C = lev[l];
         if (l == 1) {
             if (sys == INCRMT_SYS_MAC)
-                k_galerkin<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+                k_galerkin<<<dim3(cdiv(C.m, 32), cdiv(C.n, 8), 9), kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
             else
-                k_galerkin<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+                k_galerkin<<<dim3(cdiv(C.m, 32), cdiv(C.n, 8), 9), kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
         } else {
             GenOp<double> g; g.m = F.m; g.n = F.n; g.px = px; g.py = py; g.N = F.N; g.st = F.st;
-            k_galerkin<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+            k_galerkin<<<dim3(cdiv(C.m, 32), cdiv(C.n, 8), 9), kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
         }
         k_cast<<<cdiv(9 * C.N, 256) < kRedBlocks ? cdiv(9 * C.N, 256) : kRedBlocks, 256, 0, stream>>>(C.st, C.stf, 9 * C.N);
         launches += 2;

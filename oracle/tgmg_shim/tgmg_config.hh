@@ -29,7 +29,7 @@ const int tgmg_coarse_sweeps=64;
  * dense inverse built at setup. */
 const int tgmg_direct_max=96;
 /** Coarsening stops once a level has at most this many unknowns. */
-const int tgmg_coarsest_size=64;
+const int tgmg_coarsest_size=16;
 /** Maximum number of levels in a hierarchy. */
 const int tgmg_max_levels=24;
 /** Maximum number of V-cycles in one solve before reporting failure. */

@@ -555,6 +555,48 @@ __device__ bool ls_extrap_point(const LsGrid &g, const int *s, const double *phi
     const int P = g.P, ij = j * P + i;
     const double pp = phi[ij];
     double sw, sx, sy, sxx, sxy, syy, det, acc[6];
+    if (i >= 3 && j >= 3 && i + 3 < g.mL && j + 3 < g.nL) {
+        // The radius-3 window lies inside the grid: unrolled, so the status
+        // and phi loads of all 49 points issue together. Same sums, same order.
+        sw = sx = sy = sxx = sxy = syy = 0;
+#pragma unroll
+        for (int k = 0; k < 6; k++) acc[k] = 0;
+#pragma unroll
+        for (int dj = -3; dj <= 3; dj++) {
+            int sq[7];
+            double w[7];
+#pragma unroll
+            for (int di = -3; di <= 3; di++) {
+                const int q = ij + dj * P + di;
+                sq[di + 3] = s[q];
+                w[di + 3] = phi[q];
+            }
+#pragma unroll
+            for (int di = -3; di <= 3; di++) {
+                const int q = ij + dj * P + di, st = sq[di + 3];
+                if (st < 2 || st > 5 || !(w[di + 3] < pp)) continue;
+                const double ww = pp - w[di + 3];
+                sw += ww;
+                sx += di * ww;
+                sy += dj * ww;
+                sxx += di * di * ww;
+                sxy += di * dj * ww;
+                syy += dj * dj * ww;
+                const double vx = st <= 3 ? nX[q] : cx[q], vy = st <= 3 ? nY[q] : cy[q];
+                acc[0] += ww * vx; acc[1] += ww * di * vx; acc[2] += ww * dj * vx;
+                acc[3] += ww * vy; acc[4] += ww * di * vy; acc[5] += ww * dj * vy;
+            }
+        }
+        det = sw * (sxy * sxy - sxx * syy) + sx * sx * syy - 2 * sx * sxy * sy + sy * sy * sxx;
+        if (!(fabs(det) < 1e-10)) {
+            det = 1 / det;
+            const double al = (sxy * sxy - sxx * syy) * det, be = (sx * syy - sxy * sy) * det,
+                         ga = (sxx * sy - sxy * sx) * det;
+            ox = acc[0] * al + acc[1] * be + acc[2] * ga;
+            oy = acc[3] * al + acc[4] * be + acc[5] * ga;
+            return true;
+        }
+    }
     int r = 3;
     do {
         const int ilo = i <= r ? -i : -r, ihi = i + r >= g.mL ? g.mL - 1 - i : r;

@@ -120,6 +120,34 @@ __device__ __forceinline__ double galerkin_entry(const Op &op, int fm, int fn, i
 /** Galerkin coarse stencil A_c = P^T A P: one thread per coarse unknown and
  * stencil entry (blockIdx.z = entry), so that the boundary rows, whose
  * weights need the general index rules, cost no more than the others. */
+/** The same entry at an interior coarse unknown, where every weight is the
+ * standard 1 (on a coarse point) or 1/2 (next to it): only the fine points
+ * 2I+t and stencil offsets d with |t+d-2k| <= 1 contribute. */
+template <class Op>
+__device__ __forceinline__ double galerkin_entry_interior(const Op &op, int I, int J, int ki, int kj) {
+    double q = 0;
+    for (int ty = -1; ty <= 1; ty++) {
+        const double wy = ty == 0 ? 1.0 : 0.5;
+        for (int tx = -1; tx <= 1; tx++) {
+            // offsets d reaching the target: |t+d-2k| <= 1 and |d| <= 1
+            const int dxlo = max(-1, 2 * ki - 1 - tx), dxhi = min(1, 2 * ki + 1 - tx);
+            const int dylo = max(-1, 2 * kj - 1 - ty), dyhi = min(1, 2 * kj + 1 - ty);
+            if (dxlo > dxhi || dylo > dyhi) continue;
+            double a[9];
+            op.coef9(2 * I + tx, 2 * J + ty, a);
+            const double w = wy * (tx == 0 ? 1.0 : 0.5);
+            for (int dj = dylo; dj <= dyhi; dj++) {
+                const double vy = (ty + dj - 2 * kj) == 0 ? 1.0 : 0.5;
+                for (int di = dxlo; di <= dxhi; di++) {
+                    const double vx = (tx + di - 2 * ki) == 0 ? 1.0 : 0.5;
+                    q += w * a[3 * (dj + 1) + di + 1] * vx * vy;
+                }
+            }
+        }
+    }
+    return q;
+}
+
 template <class Op>
 __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
                            int cm, int cn, double *st) {
@@ -127,7 +155,11 @@ __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool 
     if (I >= cm || J >= cn) return;
     const int e = blockIdx.z, ki = e % 3 - 1, kj = e / 3 - 1;
     const long N = static_cast<long>(cm) * cn;
-    st[e * N + I + static_cast<long>(cm) * J] = galerkin_entry(op, fm, fn, px, py, kx, ky, cm, cn, I, J, ki, kj);
+    const bool interior = kx && ky && I >= 1 && J >= 1 && I <= cm - 2 && J <= cn - 2 &&
+                          2 * I + 2 <= fm - 1 && 2 * J + 2 <= fn - 1;
+    st[e * N + I + static_cast<long>(cm) * J] =
+        interior ? galerkin_entry_interior(op, I, J, ki, kj)
+                 : galerkin_entry(op, fm, fn, px, py, kx, ky, cm, cn, I, J, ki, kj);
 }
 
 __global__ void k_cast(const double *a, float *b, long n) {

@@ -109,6 +109,23 @@ long long incrmt_mg_launches(const incrmt_mg *h);
 
 void incrmt_mg_destroy(incrmt_mg *h);
 
+/** Allocation-free out = A z for the MAC (sys 0) or FEM (sys 1) system of a
+ * non-periodic m x n cell grid built from the ghosted density, all pointers
+ * device pointers, work issued on `stream` (a cudaStream_t, 0 = default) and
+ * not waited for. It has no counterpart in the reference. It is for callers
+ * that cannot allocate device memory (a framework arena that forbids
+ * cudaMalloc, a real-time loop that must not take allocation locks): it calls
+ * no allocator, and its only scratch, the edge or cell reciprocal densities,
+ * lives in a ~1 MB array compiled into the library (held by every GPU that
+ * loads the library until exit). Grids larger than 256 x 256 cells are
+ * rejected with INCRMT_ERR_BADARG. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture. All calls share the array, so calls that overlap on the
+ * GPU (other streams, other host threads) race; each call writes every
+ * scratch word it reads. */
+int incrmt_mg_apply_noalloc(int sys, int m, int n, double ax, double bx, double ay, double by,
+                            int zpr, const double *d_rho, const double *d_z, double *d_out, void *stream);
+
 /** Last error message of the calling thread (empty if none). */
 const char *incrmt_last_error(void);
 

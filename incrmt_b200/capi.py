@@ -86,6 +86,7 @@ def lib():
     L.incrmt_mg_launches.restype = ctypes.c_longlong
     L.incrmt_mg_destroy.argtypes = [P]
     L.incrmt_mg_destroy.restype = None
+    L.incrmt_mg_apply_noalloc.argtypes = [I, I, I, D, D, D, D, I, P, P, P, P]
     _lib = L
     return L
 
@@ -98,6 +99,15 @@ def check(code):
 
 def _dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def mg_apply_noalloc(sys, m, n, rho_ptr, z_ptr, out_ptr, ax=-1.0, bx=1.0, ay=-1.0, by=1.0,
+                     zpr=False, stream=0):
+    """out = A z with device pointers and no device allocation
+    (incrmt_mg_apply_noalloc); returns once the work is queued on `stream`."""
+    check(lib().incrmt_mg_apply_noalloc(sys, m, n, ax, bx, ay, by, int(zpr), ctypes.c_void_p(rho_ptr),
+                                        ctypes.c_void_p(z_ptr), ctypes.c_void_p(out_ptr),
+                                        ctypes.c_void_p(stream)))
 
 
 class MGSolver:

@@ -38,6 +38,10 @@ typedef struct incrmt_phys {
 /** Object kinds (subclasses of object, object.hh). */
 #define INCRMT_OBJ_SIMPLE_SPIN 0  /* params: r_scale, a1, a2, piv_r, th_max, omega (object.hh:447) */
 #define INCRMT_OBJ_CIRCLE      1  /* params: cx, cy, cr, uu, vv, omega, grav (object.hh:128-138) */
+#define INCRMT_OBJ_ROUNDED_ROD 2  /* params: cx, cy, cr, cl, grav (object.hh:218-241) */
+#define INCRMT_OBJ_ELLIPSE     3  /* params: cx, cy, a, b, theta, grav: an ellipse with semi-axes a, b
+                                     rotated by theta, falling under grav like obj_circle; it has no
+                                     counterpart in the reference */
 
 /** An object plus its material constants (object*, mat_const;
  * fluid_2d::add_object, fluid_2d.cc:74-90; obj_field.hh:15-29). */
@@ -125,6 +129,21 @@ int incrmt_track_records(incrmt_sim *h, double *host, int cap, int *count, int c
  * object.cc:333-336). */
 int incrmt_record_track(incrmt_sim *h);
 
+/** Bounding box of the solids for cropped output (obj_field::bound,
+ * obj_field.cc:102-106, as fluid_2d::write_files uses it, fluid_2d_io.cc:74-79):
+ * box = {li, ui, lj, uj} in ghosted indices, starting from {ml, 0, nl, 0} and
+ * extended to every point whose level-set status is below 4 in any object. */
+int incrmt_solid_bound(incrmt_sim *h, int box[4]);
+
+/** One output frame as fluid_2d::output writes it (fluid_2d_io.cc:123-179),
+ * assembled on the GPU: mode is the reference's field code (0 u, 1 v, 2 speed,
+ * 3 p, 4 vorticity, 5 rho, 6 X, 7 Y, 8 phi, 9 volume change, 10 c0, 11 c1,
+ * 12 divergence), box = {li, ui, lj, uj} the ghosted index box [li,ui)x[lj,uj).
+ * host receives (uj-lj+1) x (ui-li+1) floats: row 0 = [ui-li, x coordinates],
+ * then one row per j = [y, values], the gnuplot binary matrix layout. Modes
+ * 4, 9 and 12 read the points below and to the left, so they need li, lj >= 1. */
+int incrmt_frame(incrmt_sim *h, int mode, const int box[4], float *host);
+
 int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st);
 
 /** Phases of a step timed by the profiler (device milliseconds). */
@@ -139,9 +158,17 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st);
 #define INCRMT_PHASE_MG_SETUP  8  /* coefficients and Galerkin hierarchy of both projections */
 #define INCRMT_PHASES          9
 
-/** Turns phase timing on or off (CUDA events on the handle's stream; no
- * reference counterpart) and clears the accumulated times. */
+/** Turns timing on or off (CUDA events on the handle's stream; no reference
+ * counterpart) and clears the accumulated times: bit 0 times the phases,
+ * bit 1 times every fine-level smoothing launch of both projections (their
+ * V-cycles then run without CUDA graphs). */
 int incrmt_sim_set_profiling(incrmt_sim *h, int on);
+
+/** Fine-level smoothing launches of the MAC (which = INCRMT_SYS_MAC) or FEM
+ * projection timed since bit 1 of the profiling flags was set: total device
+ * milliseconds, algorithmic bytes (updated unknowns x (3+c) x 8, c = 2 MAC,
+ * 1 FEM) and launches. */
+int incrmt_sim_mg_profile(incrmt_sim *h, int which, double *ms, double *bytes, long long *launches);
 
 /** Accumulated device time per phase since profiling was turned on
  * (INCRMT_PHASES doubles, milliseconds). */

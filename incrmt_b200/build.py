@@ -1,6 +1,7 @@
 """In-tree build of libincrmt_gpu.so for sm_100a with nvcc.
 
-Usage: python -m incrmt_b200.build   (or incrmt_b200.build.build())
+Usage: python -m incrmt_b200.build   (or incrmt_b200.build.build(), and
+build_host() for the C++ host programs in incrmt_b200/host)
 The library lands next to this file so it travels with the repository
 snapshot; nothing is installed into site-packages.
 """
@@ -46,6 +47,15 @@ def build(force=False, verbose=False):
     return LIB
 
 
+def build_host(verbose=False):
+    """Builds the C++ host programs (incrmt_b200/host: ftest_gpu) over the library."""
+    build(verbose=verbose)
+    out = None if verbose else subprocess.DEVNULL
+    subprocess.run(["make", "-C", os.path.join(HERE, "host")], check=True, stdout=out)
+    return os.path.join(HERE, "host", "ftest_gpu")
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
+    build_host(verbose=True)
     print(LIB)

@@ -204,6 +204,8 @@ class MGSolver:
 
 OBJ_SIMPLE_SPIN = 0
 OBJ_CIRCLE = 1
+OBJ_ROUNDED_ROD = 2
+OBJ_ELLIPSE = 3
 FIELD_PHI = 200
 FIELD_STATUS = 201
 FIELDS = {n: k for k, n in enumerate(
@@ -270,6 +272,9 @@ def _sim_sigs(L):
     L.incrmt_get_stats.argtypes = [P, ctypes.POINTER(SimStats)]
     L.incrmt_sim_set_profiling.argtypes = [P, I]
     L.incrmt_sim_profile.argtypes = [P, dp]
+    L.incrmt_sim_mg_profile.argtypes = [P, I, dp, dp, ctypes.POINTER(ctypes.c_longlong)]
+    L.incrmt_solid_bound.argtypes = [P, ctypes.POINTER(I)]
+    L.incrmt_frame.argtypes = [P, I, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_float)]
     L.incrmt_sim_stream.argtypes = [P]
     L.incrmt_sim_stream.restype = P
     L.incrmt_destroy.argtypes = [P]
@@ -302,6 +307,16 @@ class Simulation:
     def add_circle(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_CIRCLE, G, rhos, ev_trans_mult, 1,
                        (ctypes.c_double * 8)(cx, cy, cr, uu, vv, omega, grav, 0))
+        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+
+    def add_rounded_rod(self, cx, cy, cr, cl, G, rhos, grav=0.0, ev_trans_mult=1.0):
+        d = ObjectDesc(OBJ_ROUNDED_ROD, G, rhos, ev_trans_mult, 1,
+                       (ctypes.c_double * 8)(cx, cy, cr, cl, grav, 0, 0, 0))
+        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+
+    def add_ellipse(self, cx, cy, a, b, theta, G, rhos, grav=0.0, ev_trans_mult=1.0):
+        d = ObjectDesc(OBJ_ELLIPSE, G, rhos, ev_trans_mult, 1,
+                       (ctypes.c_double * 8)(cx, cy, a, b, theta, grav, 0, 0))
         check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
 
     def initialize(self, ev_mult=0.8, dt_pad=0.4, dt_ev_pad=0.8):
@@ -383,14 +398,39 @@ class Simulation:
     PHASES = ["tracers", "advection", "mac", "refmap", "extrapolation", "pin_and_band", "stress",
               "fem", "mg_setup"]
 
-    def set_profiling(self, on=True):
-        check(lib().incrmt_sim_set_profiling(self._h, int(on)))
+    def set_profiling(self, on=True, smoothers=False):
+        """Phase timing (on) and per-launch timing of the projections'
+        fine-level smoothing (smoothers; V-cycles then run without graphs)."""
+        check(lib().incrmt_sim_set_profiling(self._h, (1 if on else 0) | (2 if smoothers else 0)))
 
     def profile(self):
         """Device ms per step phase since profiling was turned on."""
         out = np.zeros(len(self.PHASES))
         check(lib().incrmt_sim_profile(self._h, _dptr(out)))
         return dict(zip(self.PHASES, out.tolist()))
+
+    def solid_bound(self):
+        """Ghosted index box [li, ui, lj, uj] of all points with level-set
+        status below 4 (obj_field::bound)."""
+        b = (ctypes.c_int * 4)()
+        check(lib().incrmt_solid_bound(self._h, b))
+        return list(b)
+
+    def frame(self, mode, box):
+        """Output frame of field code `mode` over the ghosted box as the
+        float32 gnuplot matrix fluid_2d::output writes."""
+        b = (ctypes.c_int * 4)(*box)
+        si, sj = box[1] - box[0], box[3] - box[2]
+        out = np.empty((sj + 1, si + 1), dtype=np.float32)
+        check(lib().incrmt_frame(self._h, mode, b, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def smoother_profile(self, which):
+        """(ms, algorithmic bytes, launches) of the fine-level smoothing of
+        projection `which` (SYS_MAC or SYS_FEM) since profiling was set."""
+        ms, by, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+        check(lib().incrmt_sim_mg_profile(self._h, which, ctypes.byref(ms), ctypes.byref(by), ctypes.byref(n)))
+        return ms.value, by.value, n.value
 
     def stream(self):
         return lib().incrmt_sim_stream(self._h)

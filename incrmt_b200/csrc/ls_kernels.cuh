@@ -37,14 +37,31 @@ struct LsGrid {
     double phi_up, phi_down;
 };
 
+/** Level-set arrays of one object. The batched kernels below take an array
+ * of these and treat blockIdx.z as the object index; the cooperative ones
+ * take a combined point list whose entries carry their object index, so
+ * every object's band is rebuilt (or extrapolated) in the same launches. */
+struct LsObj {
+    double *phi;             // level set (ghosted grid, pitch P)
+    int *s;                  // status
+    double *phi_new;         // Newton distances of the interface points
+    double *a, *b;           // march values, or extrapolated X (ping-pong)
+    double *c, *d;           // extrapolated Y (ping-pong)
+    unsigned char *ca, *cb;  // change marks of the previous / current sweep
+    int *ia, *ib;            // dilation masks; trial statuses
+    double *nX, *nY;         // reference map being extrapolated
+};
+
 // Status values (levelset.cc:211-263, heap.cc): 0/7 far negative/positive,
 // 1/6 trial, 2/5 accepted by the march, 3/4 next to the interface.
 
 /** Sign classification (levelset.cc:209-263): s=4 for phi>0 with a 4-neighbour
  * phi<=0, s=3 for phi<=0 with a neighbour phi>0, else 7 / 0. */
-__global__ void k_ls_scan(LsGrid g, const double *phi, int *s) {
+__global__ void k_ls_scan(LsGrid g, const LsObj *ob) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
+    const double *phi = ob[blockIdx.z].phi;
+    int *s = ob[blockIdx.z].s;
     const int ij = j * g.P + i;
     const bool pos = phi[ij] > 0;
     bool diff = false;
@@ -178,9 +195,12 @@ __device__ __forceinline__ double int_abs(double v) {
  * integer abs the loop ends after eight steps whose |phi| < 1 and the
  * closeness test is |x0-x| < 1, exactly as the reference runs. Writes the
  * signed distance to phi_new; sets *err on a failure (levelset.cc:275). */
-__global__ void k_ls_newton(LsGrid g, const double *phi, const int *s, double *phi_new, int *err) {
+__global__ void k_ls_newton(LsGrid g, const LsObj *ob, int *err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
+    const double *phi = ob[blockIdx.z].phi;
+    const int *s = ob[blockIdx.z].s;
+    double *phi_new = ob[blockIdx.z].phi_new;
     const int ij = j * g.P + i, st = s[ij];
     if (st != 3 && st != 4) return;
     const double dyy = g.dy / static_cast<double>(g.mL), step_limit = sqrt(g.dx * g.dx + g.dy * g.dy);
@@ -210,11 +230,12 @@ __global__ void k_ls_newton(LsGrid g, const double *phi, const int *s, double *p
     phi_new[ij] = st == 4 ? d : -d;
 }
 
-__global__ void k_ls_copy_interface(LsGrid g, const int *s, const double *phi_new, double *phi) {
+__global__ void k_ls_copy_interface(LsGrid g, const LsObj *ob) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
+    const LsObj &o = ob[blockIdx.z];
     const int ij = j * g.P + i;
-    if (s[ij] == 3 || s[ij] == 4) phi[ij] = phi_new[ij];
+    if (o.s[ij] == 3 || o.s[ij] == 4) o.phi[ij] = o.phi_new[ij];
 }
 
 /** Marching direction: positive side (dir_positive) or negative side
@@ -476,43 +497,30 @@ __device__ __forceinline__ bool any_in(const March<POS> &mr, int i, int j) {
 
 constexpr double kUnset = 1e300;
 
-/** Initialises the march buffers: +/-kUnset for this side's far points. */
-__global__ void k_ls_fim_init(LsGrid g, const int *s, double *cur) {
+/** Initialises both march buffers (+/-kUnset for this side's far points)
+ * and clears both change marks. */
+__global__ void k_ls_fim_init(LsGrid g, const LsObj *ob) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
-    const int ij = j * g.P + i, st = s[ij];
-    cur[ij] = st == 7 ? kUnset : (st == 0 ? -kUnset : 0.0);
-}
-
-/** One Jacobi sweep of both marches: every far point of either side that
- * touches an "in" neighbour gets the stencil value; *changed is raised when
- * any value moves. Points beyond the band limit keep moving only while they
- * can still fall below it. */
-__global__ void k_ls_fim_sweep(LsGrid g, const double *phi, const int *s, const double *cur, double *nxt,
-                               int *changed) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
-    const int ij = j * g.P + i, st = s[ij];
-    double old = cur[ij], v = old;
-    if (st == 7) {
-        March<true> mr(g, phi, s, cur, old);
-        if (any_in(mr, i, j)) v = mr.calc(i, j);
-    } else if (st == 0) {
-        March<false> mr(g, phi, s, cur, old);
-        if (any_in(mr, i, j)) v = mr.calc(i, j);
-    } else {
-        return;
-    }
-    nxt[ij] = v;
-    if (v != old) atomicExch(changed, 1);
+    const LsObj &o = ob[blockIdx.z];
+    const int ij = j * g.P + i, st = o.s[ij];
+    const double v = st == 7 ? kUnset : (st == 0 ? -kUnset : 0.0);
+    o.a[ij] = v;
+    o.b[ij] = v;
+    o.ca[ij] = 0;
+    o.cb[ij] = 0;
 }
 
 /** Final values and clean-up (heap::march acceptance, levelset::clean,
  * levelset.cc:408-413): far points whose value fell inside the band limit are
  * accepted (5 / 2); every point outside the band is set to the band limit. */
-__global__ void k_ls_finish(LsGrid g, const double *cur, int *s, double *phi) {
+__global__ void k_ls_finish(LsGrid g, const LsObj *ob) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
+    // After the last (unchanging) sweep both buffers hold the final values.
+    const double *cur = ob[blockIdx.z].a;
+    int *s = ob[blockIdx.z].s;
+    double *phi = ob[blockIdx.z].phi;
     const int ij = j * g.P + i, st = s[ij];
     const double v = cur[ij];
     if (st == 7) {
@@ -527,9 +535,11 @@ __global__ void k_ls_finish(LsGrid g, const double *cur, int *s, double *phi) {
 /** Trial statuses (heap::check_gridpoint / update, heap.cc:38-44,159-167):
  * a far point next to an interface or accepted point of its side was put on
  * the heap and, not being accepted, stays trial (6 / 1). */
-__global__ void k_ls_trial(LsGrid g, const int *s, int *s_out) {
+__global__ void k_ls_trial(LsGrid g, const LsObj *ob) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
+    const int *s = ob[blockIdx.z].s;
+    int *s_out = ob[blockIdx.z].ia;
     const int ij = j * g.P + i, st = s[ij];
     int out = st;
     if (st == 7 || st == 0) {
@@ -542,6 +552,14 @@ __global__ void k_ls_trial(LsGrid g, const int *s, int *s_out) {
         if (nb) out = st == 7 ? 6 : 1;
     }
     s_out[ij] = out;
+}
+
+/** Copies the trial statuses back into the status array. */
+__global__ void k_ls_store_status(LsGrid g, const LsObj *ob) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.mL || j >= g.nL) return;
+    const int ij = j * g.P + i;
+    ob[blockIdx.z].s[ij] = ob[blockIdx.z].ia[ij];
 }
 
 /** Weighted least-squares extrapolation of (nX,nY) at one band point outside
@@ -631,30 +649,46 @@ __device__ bool ls_extrap_point(const LsGrid &g, const int *s, const double *phi
     return true;
 }
 
-/** One wavefront (Jacobi) sweep of the extrapolation over the listed band
- * points outside the solid: reads (cx,cy), writes (tx,ty). */
-__global__ void k_ls_extrap_sweep(LsGrid g, const int *s, const double *phi, const double *nX, const double *nY,
-                                  const int *list, const int *count, const double *cx, const double *cy,
-                                  double *tx, double *ty, int *changed, int *err) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= *count) return;
-    const int ij = list[t], i = ij % g.P, j = ij / g.P;
-    double ox, oy;
-    if (!ls_extrap_point(g, s, phi, nX, nY, cx, cy, i, j, ox, oy)) {
-        atomicExch(err, INCRMT_ERR_EXTRAP_SINGULAR);
-        ox = cx[ij]; oy = cy[ij];
-    }
-    if (ox != cx[ij] || oy != cy[ij]) atomicExch(changed, 1);
-    tx[ij] = ox;
-    ty[ij] = oy;
+/** Appends (ij, object) to the combined point list if it has room;
+ * flags an overflow otherwise (the list is sized for every point of every
+ * object, so this only guards the bound). */
+__device__ __forceinline__ void ls_list_push(int *list, int *list_k, int *count, int cap, int *overflow, int ij,
+                                             int k) {
+    const int t = atomicAdd(count, 1);
+    if (t < cap) { list[t] = ij; list_k[t] = k; }
+    else atomicExch(overflow, 1);
 }
 
-/** Lists the band points outside the solid (status 4 or 5). */
-__global__ void k_ls_collect_outside(LsGrid g, const int *s, int *list, int *count) {
+/** Lists the band points outside each solid (status 4 or 5). */
+__global__ void k_ls_collect_outside(LsGrid g, const LsObj *ob, int *list, int *list_k, int *count, int cap,
+                                     int *overflow) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
-    const int ij = j * g.P + i, st = s[ij];
-    if (st == 4 || st == 5) list[atomicAdd(count, 1)] = ij;
+    const int ij = j * g.P + i, st = ob[blockIdx.z].s[ij];
+    if (st == 4 || st == 5) ls_list_push(list, list_k, count, cap, overflow, ij, blockIdx.z);
+}
+
+/** Starts the extrapolation: both buffers of every listed point hold its
+ * current reference map. Only listed points are ever read as iterates. */
+__global__ void k_ls_extrap_init(const LsObj *ob, const int *list, const int *list_k, const int *countp, int cap) {
+    const int count = min(*countp, cap);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const LsObj &o = ob[list_k[t]];
+        const int ij = list[t];
+        o.a[ij] = o.b[ij] = o.nX[ij];
+        o.c[ij] = o.d[ij] = o.nY[ij];
+    }
+}
+
+/** Stores the extrapolated values of the listed points into nX, nY. */
+__global__ void k_ls_extrap_store(const LsObj *ob, const int *list, const int *list_k, const int *countp, int cap) {
+    const int count = min(*countp, cap);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const LsObj &o = ob[list_k[t]];
+        const int ij = list[t];
+        o.nX[ij] = o.a[ij];
+        o.nY[ij] = o.c[ij];
+    }
 }
 
 }  // namespace incrmt
@@ -662,18 +696,21 @@ __global__ void k_ls_collect_outside(LsGrid g, const int *s, int *list, int *cou
 namespace incrmt {
 
 /** Marks the points next to the interface (status 3 or 4) as 1 in mark. */
-__global__ void k_ls_mark_interface(LsGrid g, const int *s, int *mark) {
+__global__ void k_ls_mark_interface(LsGrid g, const LsObj *ob) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
-    const int ij = j * g.P + i, st = s[ij];
-    mark[ij] = (st == 3 || st == 4) ? 1 : 0;
+    const int ij = j * g.P + i, st = ob[blockIdx.z].s[ij];
+    ob[blockIdx.z].ia[ij] = (st == 3 || st == 4) ? 1 : 0;
 }
 
-/** One direction of a separable dilation by radius R (max over a window). */
+/** One direction of a separable dilation by radius R (max over a window):
+ * along x from ia into ib, along y from ib back into ia. */
 template <bool ALONG_X>
-__global__ void k_ls_dilate(LsGrid g, const int *in, int *out, int R) {
+__global__ void k_ls_dilate(LsGrid g, const LsObj *ob, int R) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
+    const int *in = ALONG_X ? ob[blockIdx.z].ia : ob[blockIdx.z].ib;
+    int *out = ALONG_X ? ob[blockIdx.z].ib : ob[blockIdx.z].ia;
     int v = 0;
     if (ALONG_X) {
         const int lo = i - R < 0 ? 0 : i - R, hi = i + R >= g.mL ? g.mL - 1 : i + R;
@@ -687,11 +724,13 @@ __global__ void k_ls_dilate(LsGrid g, const int *in, int *out, int R) {
 
 /** Lists the far points (status 0 or 7) inside the dilated interface region:
  * the only points the march can reach within the band limit. */
-__global__ void k_ls_collect_candidates(LsGrid g, const int *s, const int *near, int *list, int *count) {
+__global__ void k_ls_collect_candidates(LsGrid g, const LsObj *ob, int *list, int *list_k, int *count, int cap,
+                                        int *overflow) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.mL || j >= g.nL) return;
-    const int ij = j * g.P + i, st = s[ij];
-    if ((st == 0 || st == 7) && near[ij]) list[atomicAdd(count, 1)] = ij;
+    const LsObj &o = ob[blockIdx.z];
+    const int ij = j * g.P + i, st = o.s[ij];
+    if ((st == 0 || st == 7) && o.ia[ij]) ls_list_push(list, list_k, count, cap, overflow, ij, blockIdx.z);
 }
 
 /** Whether any point the stencil of (i,j) reads (up to two cells along
@@ -713,34 +752,39 @@ __device__ __forceinline__ bool stencil_changed(const LsGrid &g, const unsigned 
  * writing nxt), a grid barrier follows, and the loop ends after the first
  * sweep that changed nothing. A candidate whose stencil inputs did not change
  * in the previous sweep keeps its value (its stencil would return it again),
- * so later sweeps only touch the moving front; chg_a/chg_b are per-point
- * change marks of the previous and the current sweep (cleared by the caller).
+ * so later sweeps only touch the moving front; each object's ca/cb are
+ * per-point change marks of the previous and the current sweep (cleared by
+ * k_ls_fim_init) and a/b its values, swapped every sweep. The list holds the
+ * candidates of every object, so all bands settle in the same launch.
  * flags[0..2] rotate as per-sweep change flags; flags[3] receives the number
  * of sweeps and flags[4] 1 if converged. */
-__global__ void k_ls_fim_coop(LsGrid g, const double *phi, const int *s, double *a, double *b, const int *list,
-                              const int *countp, int *flags, int max_sweeps, unsigned char *chg_a,
-                              unsigned char *chg_b) {
+__global__ void k_ls_fim_coop(LsGrid g, const LsObj *ob, const int *list, const int *list_k, const int *countp,
+                              int cap, int *flags, int max_sweeps) {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    const int count = *countp;
-    double *cur = a, *nxt = b;
-    unsigned char *cprev = chg_a, *cnow = chg_b;
+    const int count = min(*countp, cap);
     int it = 0;
     bool done = false;
     for (; it < max_sweeps; it++) {
         if (tid == 0) flags[(it + 1) % 3] = 0;
+        const bool odd = it & 1;
         bool ch = false;
         for (int t = tid; t < count; t += nth) {
-            const int ij = list[t], i = ij % g.P, j = ij / g.P, st = s[ij];
+            const LsObj &o = ob[list_k[t]];
+            const double *cur = odd ? o.b : o.a;
+            double *nxt = odd ? o.a : o.b;
+            const unsigned char *cprev = odd ? o.cb : o.ca;
+            unsigned char *cnow = odd ? o.ca : o.cb;
+            const int ij = list[t], i = ij % g.P, j = ij / g.P, st = o.s[ij];
             const double old = cur[ij];
             double v = old;
             if (it == 0 || stencil_changed(g, cprev, i, j)) {
                 if (st == 7) {
-                    March<true> mr(g, phi, s, cur, old);
+                    March<true> mr(g, o.phi, o.s, cur, old);
                     if (any_in(mr, i, j)) v = mr.calc(i, j);
                 } else {
-                    March<false> mr(g, phi, s, cur, old);
+                    March<false> mr(g, o.phi, o.s, cur, old);
                     if (any_in(mr, i, j)) v = mr.calc(i, j);
                 }
             }
@@ -752,8 +796,6 @@ __global__ void k_ls_fim_coop(LsGrid g, const double *phi, const int *s, double 
         if (__syncthreads_or(ch) && threadIdx.x == 0) flags[it % 3] = 1;
         grid.sync();
         const int c = *reinterpret_cast<volatile int *>(&flags[it % 3]);
-        double *t = cur; cur = nxt; nxt = t;
-        unsigned char *u = cprev; cprev = cnow; cnow = u;
         if (!c) { done = true; break; }
     }
     if (tid == 0) { flags[3] = done ? it + 1 : it; flags[4] = done ? 1 : 0; }
@@ -761,23 +803,25 @@ __global__ void k_ls_fim_coop(LsGrid g, const double *phi, const int *s, double 
 
 /** All sweeps of the extrapolation wavefront in one cooperative launch (same
  * scheme as k_ls_fim_coop); flags[5] is raised for a singular fit. */
-__global__ void k_ls_extrap_coop(LsGrid g, const int *s, const double *phi, const double *nX, const double *nY,
-                                 const int *list, const int *countp, double *ax_, double *ay_, double *bx_,
-                                 double *by_, int *flags, int max_sweeps) {
+__global__ void k_ls_extrap_coop(LsGrid g, const LsObj *ob, const int *list, const int *list_k,
+                                 const int *countp, int cap, int *flags, int max_sweeps) {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    const int count = *countp;
-    double *cx = ax_, *cy = ay_, *tx = bx_, *ty = by_;
+    const int count = min(*countp, cap);
     int it = 0;
     bool done = false;
     for (; it < max_sweeps; it++) {
         if (tid == 0) flags[(it + 1) % 3] = 0;
+        const bool odd = it & 1;
         bool ch = false;
         for (int t = tid; t < count; t += nth) {
+            const LsObj &o = ob[list_k[t]];
+            const double *cx = odd ? o.b : o.a, *cy = odd ? o.d : o.c;
+            double *tx = odd ? o.a : o.b, *ty = odd ? o.c : o.d;
             const int ij = list[t], i = ij % g.P, j = ij / g.P;
             double ox, oy;
-            if (!ls_extrap_point(g, s, phi, nX, nY, cx, cy, i, j, ox, oy)) {
+            if (!ls_extrap_point(g, o.s, o.phi, o.nX, o.nY, cx, cy, i, j, ox, oy)) {
                 atomicExch(&flags[5], INCRMT_ERR_EXTRAP_SINGULAR);
                 ox = cx[ij]; oy = cy[ij];
             }
@@ -788,8 +832,6 @@ __global__ void k_ls_extrap_coop(LsGrid g, const int *s, const double *phi, cons
         if (__syncthreads_or(ch) && threadIdx.x == 0) flags[it % 3] = 1;
         grid.sync();
         const int c = *reinterpret_cast<volatile int *>(&flags[it % 3]);
-        double *t1 = cx; cx = tx; tx = t1;
-        double *t2 = cy; cy = ty; ty = t2;
         if (!c) { done = true; break; }
     }
     if (tid == 0) { flags[3] = done ? it + 1 : it; flags[4] = done ? 1 : 0; }

@@ -22,6 +22,8 @@ namespace incrmt {
  * 0.5/rho+0.5/rho of the two adjacent cells (fluid_2d.cc:1140-1160). */
 template <class T>
 struct MacOp {
+    /** Five-point stencil: red-black ordering equals the four-colour one. */
+    static constexpr bool kFivePoint = true;
     int m, n, px, py, zpr;
     T xxsp, yysp;
     const T *ex, *ey;
@@ -77,6 +79,7 @@ struct MacOp {
  * node whose off-diagonal entries vanish (mgs_fem.cc:19-20). */
 template <class T>
 struct FemOp {
+    static constexpr bool kFivePoint = false;
     int m, n, px, py, zpr;
     T fm, fc, hex, hey;
     const T *c;
@@ -186,6 +189,7 @@ struct FemOp {
  * arrays, entry k of unknown ij at st[k*N+ij]. */
 template <class T>
 struct GenOp {
+    static constexpr bool kFivePoint = false;
     int m, n, px, py;
     long N;
     const T *st;

@@ -12,6 +12,7 @@
 #include "step_kernels.cuh"
 #include "ls_kernels.cuh"
 #include "tracer_kernels.cuh"
+#include "frame_kernels.cuh"
 
 namespace incrmt {
 
@@ -34,10 +35,11 @@ struct Sim {
     ObjDev *d_obj = nullptr;
     SolidDev *d_sol = nullptr;
     double *src_mac = nullptr, *z_mac = nullptr, *src_fem = nullptr, *z_fem = nullptr;
-    double *ls_a = nullptr, *ls_b = nullptr;       // march / extrapolation buffers (x)
-    double *ls_c = nullptr, *ls_d = nullptr;       // extrapolation buffers (y)
-    int *d_list = nullptr, *d_ia = nullptr, *d_ib = nullptr;
-    unsigned char *d_chg = nullptr;                 // change marks of the march sweeps (2 x cells)
+    std::vector<LsObj> lso;                         // level-set working arrays per object
+    LsObj *d_lso = nullptr;
+    int *d_list = nullptr, *d_list_k = nullptr;     // combined point list of all objects
+    int list_cap = 0;
+    std::vector<void *> raw_allocs;                 // non-double per-object arrays
     int coop_blocks_fim = 0, coop_blocks_ext = 0;   // co-resident grid sizes
     int *d_flags = nullptr;  // [0..2] sweep change flags, [3] sweeps, [4] converged, [5] fit error,
                            // [6] Newton error, [7] list length, [8] tracer remaps, [9] correction failure
@@ -58,6 +60,9 @@ struct Sim {
     int t_correction = 1;
     int pre_stress_objects = 0;
     std::vector<double> track;                      // records: time, xpre, ypre, x, y
+    float *d_frame = nullptr;                       // output frame staging (grown on demand)
+    size_t frame_cap = 0;
+    int *d_box = nullptr;                           // solid bounding box reduction
     // Optional phase timing: CUDA events on the stream at phase boundaries.
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -124,8 +129,8 @@ struct Sim {
     int set_boundaries();
     int set_rho();
     int pin();
-    int build_band(int k);
-    int extrapolate(int k);
+    int build_bands();
+    int extrapolate_all();
     int mac_projection();
     int fem_projection(double dt);
     int update_reference_map(double dt);
@@ -174,15 +179,8 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     if ((r = alloc(&z_mac, static_cast<size_t>(g.m) * g.n))) return r;
     if ((r = alloc(&src_fem, static_cast<size_t>(g.mf) * g.nf))) return r;
     if ((r = alloc(&z_fem, static_cast<size_t>(g.mf) * g.nf))) return r;
-    if ((r = alloc(&ls_a, cells()))) return r;
-    if ((r = alloc(&ls_b, cells()))) return r;
-    if ((r = alloc(&ls_c, cells()))) return r;
-    if ((r = alloc(&ls_d, cells()))) return r;
     if ((r = alloc(&partial, 4 * kB200SMs))) return r;
-    INCRMT_CK(cudaMalloc(&d_list, sizeof(int) * cells()));
-    INCRMT_CK(cudaMalloc(&d_ia, sizeof(int) * cells()));
-    INCRMT_CK(cudaMalloc(&d_ib, sizeof(int) * cells()));
-    INCRMT_CK(cudaMalloc(&d_chg, 2 * cells()));
+    INCRMT_CK(cudaMalloc(&d_lso, sizeof(LsObj) * kMaxObjects));
     {
         int dev = 0, sms = 0, nb = 0;
         INCRMT_CK(cudaGetDevice(&dev));
@@ -210,12 +208,15 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
 int Sim::add_object(const incrmt_object_desc *d) {
     if (initialized) { set_error("objects must be added before initialize"); return INCRMT_ERR_BADARG; }
     if (static_cast<int>(obj.size()) >= kMaxObjects) { set_error("too many objects"); return INCRMT_ERR_BADARG; }
-    if (d->type != INCRMT_OBJ_SIMPLE_SPIN && d->type != INCRMT_OBJ_CIRCLE) {
+    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_ELLIPSE) {
         set_error("unknown object type %d", d->type);
         return INCRMT_ERR_BADARG;
     }
     ObjDev o{};
-    o.type = d->type == INCRMT_OBJ_SIMPLE_SPIN ? OBJ_SIMPLE_SPIN : OBJ_CIRCLE;
+    o.type = d->type == INCRMT_OBJ_SIMPLE_SPIN ? OBJ_SIMPLE_SPIN
+             : d->type == INCRMT_OBJ_CIRCLE   ? OBJ_CIRCLE
+             : d->type == INCRMT_OBJ_ROUNDED_ROD ? OBJ_ROUNDED_ROD
+                                                 : OBJ_ELLIPSE;
     o.set_velocity = d->set_velocity;
     o.G = d->G; o.rhos = d->rhos; o.ev_trans_mult = d->ev_trans_mult;
     o.eps = g.eps; o.pinw = pinw * g.dx;  // obj_field.cc:16
@@ -226,10 +227,19 @@ int Sim::add_object(const incrmt_object_desc *d) {
         const double scf = p[0] / (1 + p[1] + p[2]);
         o.g[0] = scf * (1 - p[2]); o.g[1] = scf * p[1]; o.g[2] = 2 * scf * p[2];
         o.g[3] = p[3]; o.g[4] = p[4]; o.g[5] = p[5];
-    } else {
+    } else if (o.type == OBJ_CIRCLE) {
         // obj_circle(cx,cy,cr,uu,vv,omega,grav) (object.hh:128-138)
         o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[6];
         o.g[4] = p[3]; o.g[5] = p[4]; o.g[6] = p[5];
+    } else if (o.type == OBJ_ROUNDED_ROD) {
+        // obj_rounded_rod(cx,cy,cr,cl,grav) (object.hh:229-230); at rest initially
+        if (!(p[2] > 0) || !(p[3] >= 0)) { set_error("rounded rod needs cr > 0, cl >= 0"); return INCRMT_ERR_BADARG; }
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[4]; o.g[7] = p[3];
+    } else {
+        // ellipse (cx,cy,a,b,theta,grav); at rest initially
+        if (!(p[2] > 0) || !(p[3] > 0)) { set_error("ellipse needs positive semi-axes"); return INCRMT_ERR_BADARG; }
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[5]; o.g[7] = p[3];
+        o.g[8] = cos(p[4]); o.g[9] = sin(p[4]);
     }
     SolidDev s{};
     double **sp[] = {&s.X, &s.Y, &s.nX, &s.nY, &s.Xx, &s.Xy, &s.Yx, &s.Yy, &s.Xd, &s.Yd, &s.Xl, &s.Yl,
@@ -237,6 +247,18 @@ int Sim::add_object(const incrmt_object_desc *d) {
     for (double **q : sp) { int r = alloc(q, cells()); if (r) return r; }
     INCRMT_CK(cudaMalloc(&s.s, sizeof(int) * cells()));
     INCRMT_CK(cudaMemsetAsync(s.s, 0, sizeof(int) * cells(), stream));
+    LsObj l{};
+    l.phi = s.phi; l.s = s.s; l.phi_new = s.phi_tmp; l.nX = s.nX; l.nY = s.nY;
+    for (double **q : {&l.a, &l.b, &l.c, &l.d}) { int r = alloc(q, cells()); if (r) return r; }
+    void *raw = nullptr;
+    INCRMT_CK(cudaMalloc(&raw, 2 * cells() + 2 * sizeof(int) * cells()));
+    raw_allocs.push_back(raw);
+    INCRMT_CK(cudaMemsetAsync(raw, 0, 2 * cells() + 2 * sizeof(int) * cells(), stream));
+    l.ia = static_cast<int *>(raw);
+    l.ib = l.ia + cells();
+    l.ca = reinterpret_cast<unsigned char *>(l.ib + cells());
+    l.cb = l.ca + cells();
+    lso.push_back(l);
     obj.push_back(o);
     sol.push_back(s);
     desc.push_back(*d);
@@ -251,6 +273,19 @@ int Sim::upload_objects() {
     if (obj.empty()) return INCRMT_OK;
     INCRMT_CK(cudaMemcpyAsync(d_obj, obj.data(), sizeof(ObjDev) * obj.size(), cudaMemcpyHostToDevice, stream));
     INCRMT_CK(cudaMemcpyAsync(d_sol, sol.data(), sizeof(SolidDev) * sol.size(), cudaMemcpyHostToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(d_lso, lso.data(), sizeof(LsObj) * lso.size(), cudaMemcpyHostToDevice, stream));
+    // Room for every point of every object in the combined level-set list.
+    const size_t need = cells() * obj.size();
+    if (need > static_cast<size_t>(list_cap)) {
+        if (need > 0x7fffffffu) { set_error("level-set point list too large"); return INCRMT_ERR_BADARG; }
+        cudaFree(d_list);
+        cudaFree(d_list_k);
+        d_list = d_list_k = nullptr;
+        list_cap = 0;
+        INCRMT_CK(cudaMalloc(&d_list, sizeof(int) * need));
+        INCRMT_CK(cudaMalloc(&d_list_k, sizeof(int) * need));
+        list_cap = static_cast<int>(need);
+    }
     return INCRMT_OK;
 }
 
@@ -297,43 +332,44 @@ int Sim::set_rho() {
 }
 
 /** levelset::build_band for object k (levelset.cc:199-335). */
-int Sim::build_band(int k) {
-    SolidDev &s = sol[k];
-    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 8, stream));
-    const dim3 gg = g2(lg.mL, lg.nL);
-    k_ls_scan<<<gg, kB2, 0, stream>>>(lg, s.phi, s.s);
-    k_ls_newton<<<gg, kB2, 0, stream>>>(lg, s.phi, s.s, s.phi_tmp, d_flags + 6);
-    k_ls_copy_interface<<<gg, kB2, 0, stream>>>(lg, s.s, s.phi_tmp, s.phi);
+/** levelset::build_band for every object (levelset.cc:199-335): each kernel
+ * runs over all objects at once (blockIdx.z), and one cooperative launch
+ * settles every object's march, the objects being independent. */
+int Sim::build_bands() {
+    const int no = static_cast<int>(obj.size());
+    if (no == 0) return INCRMT_OK;
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 11, stream));
+    const dim3 gg(cdiv(lg.mL, 32), cdiv(lg.nL, 8), no);
+    k_ls_scan<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    k_ls_newton<<<gg, kB2, 0, stream>>>(lg, d_lso, d_flags + 6);
+    k_ls_copy_interface<<<gg, kB2, 0, stream>>>(lg, d_lso);
     // Candidates: far points within the band radius of the interface.
     const int R = static_cast<int>(std::ceil((lg.phi_up) / (g.dx < g.dy ? g.dx : g.dy))) + 2;
-    k_ls_mark_interface<<<gg, kB2, 0, stream>>>(lg, s.s, d_ia);
-    k_ls_dilate<true><<<gg, kB2, 0, stream>>>(lg, d_ia, d_ib, R);
-    k_ls_dilate<false><<<gg, kB2, 0, stream>>>(lg, d_ib, d_ia, R);
-    k_ls_collect_candidates<<<gg, kB2, 0, stream>>>(lg, s.s, d_ia, d_list, d_flags + 7);
-    k_ls_fim_init<<<gg, kB2, 0, stream>>>(lg, s.s, ls_a);
+    k_ls_mark_interface<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    k_ls_dilate<true><<<gg, kB2, 0, stream>>>(lg, d_lso, R);
+    k_ls_dilate<false><<<gg, kB2, 0, stream>>>(lg, d_lso, R);
+    k_ls_collect_candidates<<<gg, kB2, 0, stream>>>(lg, d_lso, d_list, d_list_k, d_flags + 7, list_cap,
+                                                    d_flags + 10);
+    k_ls_fim_init<<<gg, kB2, 0, stream>>>(lg, d_lso);
     launches += 8;
     INCRMT_CKL("level-set scan/newton/candidates");
-    INCRMT_CK(cudaMemcpyAsync(ls_b, ls_a, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    int maxs = kLsMaxSweeps;
+    int maxs = kLsMaxSweeps, cap = list_cap;
     const int *countp = d_flags + 7;
-    double *pa = ls_a, *pb = ls_b;
-    const double *phic = s.phi;
-    const int *sc = s.s;
-    INCRMT_CK(cudaMemsetAsync(d_chg, 0, 2 * cells(), stream));
-    unsigned char *ca = d_chg, *cb = d_chg + cells();
-    void *args[] = {&lg, &phic, &sc, &pa, &pb, &d_list, &countp, &d_flags, &maxs, &ca, &cb};
+    const LsObj *ob = d_lso;
+    void *args[] = {&lg, &ob, &d_list, &d_list_k, &countp, &cap, &d_flags, &maxs};
     INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_fim_coop), dim3(coop_blocks_fim), dim3(256),
                                           args, 0, stream));
     launches++;
     int r = fetch_flags();
     if (r) return r;
     if (h_flags[6]) { set_error("level++: Newton iteration failed."); return h_flags[6]; }
+    if (h_flags[10]) { set_error("level-set candidate list overflow"); return INCRMT_ERR_BADARG; }
     ls_sweeps += h_flags[3];
     if (!h_flags[4]) { set_error("level-set march did not settle in %d sweeps", h_flags[3]); return INCRMT_ERR_NOCONV; }
-    k_ls_finish<<<gg, kB2, 0, stream>>>(lg, ls_a, s.s, s.phi);
-    k_ls_trial<<<gg, kB2, 0, stream>>>(lg, s.s, d_ia);
-    INCRMT_CK(cudaMemcpyAsync(s.s, d_ia, sizeof(int) * cells(), cudaMemcpyDeviceToDevice, stream));
-    launches += 2;
+    k_ls_finish<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    k_ls_trial<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    k_ls_store_status<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    launches += 3;
     INCRMT_CKL("k_ls_finish");
     return INCRMT_OK;
 }
@@ -342,42 +378,43 @@ int Sim::build_band(int k) {
  * fluid_2d.cc:373-377). */
 int Sim::pin() {
     int r;
-    for (size_t k = 0; k < obj.size(); k++) {
-        k_pin<<<g2(g.ml, g.nl), kB2, 0, stream>>>(g, obj[k], sol[k]);
+    if (!obj.empty()) {
+        k_pin<<<dim3(cdiv(g.ml, 32), cdiv(g.nl, 8), obj.size()), kB2, 0, stream>>>(g, d_obj, d_sol);
         launches++;
         INCRMT_CKL("k_pin");
-        if ((r = build_band(static_cast<int>(k)))) return r;
     }
+    if ((r = build_bands())) return r;
     return set_rho();
 }
 
-/** levelset::extrapolate_fields for object k (traverse.hh:235-260). */
-int Sim::extrapolate(int k) {
-    SolidDev &s = sol[k];
-    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 8, stream));
-    k_ls_collect_outside<<<g2(lg.mL, lg.nL), kB2, 0, stream>>>(lg, s.s, d_list, d_flags + 7);
-    launches++;
+/** levelset::extrapolate_fields for every object (traverse.hh:235-260),
+ * the objects' wavefronts settling together in one cooperative launch. */
+int Sim::extrapolate_all() {
+    const int no = static_cast<int>(obj.size());
+    if (no == 0) return INCRMT_OK;
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 11, stream));
+    k_ls_collect_outside<<<dim3(cdiv(lg.mL, 32), cdiv(lg.nL, 8), no), kB2, 0, stream>>>(
+        lg, d_lso, d_list, d_list_k, d_flags + 7, list_cap, d_flags + 10);
+    k_ls_extrap_init<<<4 * kB200SMs, 256, 0, stream>>>(d_lso, d_list, d_list_k, d_flags + 7, list_cap);
+    launches += 2;
     INCRMT_CKL("collect");
-    INCRMT_CK(cudaMemcpyAsync(ls_a, s.nX, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    INCRMT_CK(cudaMemcpyAsync(ls_c, s.nY, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    INCRMT_CK(cudaMemcpyAsync(ls_b, s.nX, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    INCRMT_CK(cudaMemcpyAsync(ls_d, s.nY, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    int maxs = kExtrapMaxSweeps;
+    int maxs = kExtrapMaxSweeps, cap = list_cap;
     const int *countp = d_flags + 7;
-    const int *sc = s.s;
-    const double *phic = s.phi, *nXc = s.nX, *nYc = s.nY;
-    void *args[] = {&lg, &sc, &phic, &nXc, &nYc, &d_list, &countp, &ls_a, &ls_c, &ls_b, &ls_d, &d_flags, &maxs};
+    const LsObj *ob = d_lso;
+    void *args[] = {&lg, &ob, &d_list, &d_list_k, &countp, &cap, &d_flags, &maxs};
     INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_extrap_coop), dim3(coop_blocks_ext),
                                           dim3(256), args, 0, stream));
     launches++;
     int r = fetch_flags();
     if (r) return r;
     if (h_flags[5]) { set_error("singular extrapolation fit"); return h_flags[5]; }
+    if (h_flags[10]) { set_error("extrapolation list overflow"); return INCRMT_ERR_BADARG; }
     ex_sweeps += h_flags[3];
     if (!h_flags[4]) { set_error("extrapolation did not settle in %d sweeps", h_flags[3]); return INCRMT_ERR_NOCONV; }
     // After the last sweep both buffers hold the same values.
-    INCRMT_CK(cudaMemcpyAsync(s.nX, ls_a, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
-    INCRMT_CK(cudaMemcpyAsync(s.nY, ls_c, sizeof(double) * cells(), cudaMemcpyDeviceToDevice, stream));
+    k_ls_extrap_store<<<4 * kB200SMs, 256, 0, stream>>>(d_lso, d_list, d_list_k, d_flags + 7, list_cap);
+    launches++;
+    INCRMT_CKL("k_ls_extrap_store");
     return INCRMT_OK;
 }
 
@@ -391,8 +428,7 @@ int Sim::update_reference_map(double dt) {
     int r, outer = cur_phase;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(INCRMT_PHASE_EXTRAP))) return r;
-    for (size_t k = 0; k < obj.size(); k++)
-        if ((r = extrapolate(static_cast<int>(k)))) return r;
+    if ((r = extrapolate_all())) return r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(outer))) return r;
     for (size_t k = 0; k < obj.size(); k++) {
@@ -541,12 +577,12 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
     int r = upload_objects();
     if (r) return r;
     // fluid_2d::init_fields (fluid_2d.cc:195-254).
-    for (size_t k = 0; k < obj.size(); k++) {
-        k_init_object<<<g2(g.ml, g.nl), kB2, 0, stream>>>(g, obj[k], sol[k]);
+    if (!obj.empty()) {
+        k_init_object<<<dim3(cdiv(g.ml, 32), cdiv(g.nl, 8), obj.size()), kB2, 0, stream>>>(g, d_obj, d_sol);
         launches++;
         INCRMT_CKL("k_init_object");
-        if ((r = build_band(static_cast<int>(k)))) return r;
     }
+    if ((r = build_bands())) return r;
     k_init_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, static_cast<int>(obj.size()));
     launches++;
     INCRMT_CKL("k_init_velocity");
@@ -630,8 +666,8 @@ int Sim::stage(int s, double dt) {
         case 18: return tracers(2, dt);
         case 19: return set_rho();
         case 20: return step(dt);
-        case 21: for (int k = 0; k < no; k++) { int r = build_band(k); if (r) return r; } return INCRMT_OK;
-        case 22: for (int k = 0; k < no; k++) { int r = extrapolate(k); if (r) return r; } return INCRMT_OK;
+        case 21: return build_bands();
+        case 22: return extrapolate_all();
         default: set_error("unknown stage %d", s); return INCRMT_ERR_BADARG;
     }
     launches++;
@@ -646,7 +682,13 @@ void Sim::destroy() {
     for (double *p : allocs) cudaFree(p);
     allocs.clear();
     for (auto &s : sol) cudaFree(s.s);
-    cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_list); cudaFree(d_ia); cudaFree(d_ib); cudaFree(d_chg); cudaFree(d_flags);
+    cudaFree(d_frame); cudaFree(d_box);
+    d_frame = nullptr; d_box = nullptr; frame_cap = 0;
+    for (void *p : raw_allocs) cudaFree(p);
+    raw_allocs.clear();
+    lso.clear();
+    cudaFree(d_obj); cudaFree(d_sol); cudaFree(d_lso); cudaFree(d_list); cudaFree(d_list_k); cudaFree(d_flags);
+    d_obj = nullptr; d_sol = nullptr; d_lso = nullptr; d_list = d_list_k = nullptr; d_flags = nullptr; list_cap = 0;
     if (h_flags) cudaFreeHost(h_flags);
     for (auto e : ev_pool) cudaEventDestroy(e);
     ev_pool.clear();
@@ -883,8 +925,25 @@ int incrmt_sim_set_profiling(incrmt_sim *h, int on) {
     incrmt::Sim &S = h->s;
     int r = S.phase_collect();
     if (r) return r;
-    S.prof = on != 0;
+    S.prof = (on & 1) != 0;
     for (int k = 0; k < INCRMT_PHASES; k++) { S.phase_ms[k] = 0; S.phase_n[k] = 0; }
+    for (incrmt::Multigrid *mg : {&S.mac, &S.fem}) {
+        r = mg->prof_collect();
+        if (r) return r;
+        mg->prof = (on & 2) != 0;
+        mg->prof_ms = 0; mg->prof_bytes = 0; mg->prof_launches = 0;
+    }
+    return INCRMT_OK;
+}
+
+int incrmt_sim_mg_profile(incrmt_sim *h, int which, double *ms, double *bytes, long long *launches) {
+    if (!h || (which != INCRMT_SYS_MAC && which != INCRMT_SYS_FEM)) { set_error("bad argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Multigrid &mg = which == INCRMT_SYS_MAC ? h->s.mac : h->s.fem;
+    int r = mg.prof_collect();
+    if (r) return r;
+    if (ms) *ms = mg.prof_ms;
+    if (bytes) *bytes = mg.prof_bytes;
+    if (launches) *launches = mg.prof_launches;
     return INCRMT_OK;
 }
 
@@ -905,3 +964,50 @@ void incrmt_destroy(incrmt_sim *h) {
 }
 
 }  // extern "C"
+
+int incrmt_solid_bound(incrmt_sim *h, int box[4]) {
+    if (!h || !box) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    const int nobj = static_cast<int>(S.sol.size());
+    int init[4] = {S.g.ml, 0, S.g.nl, 0};
+    if (nobj == 0) { std::memcpy(box, init, sizeof(init)); return INCRMT_OK; }
+    if (!S.d_box) INCRMT_CK(cudaMalloc(&S.d_box, 4 * sizeof(int)));
+    INCRMT_CK(cudaMemcpyAsync(S.d_box, init, sizeof(init), cudaMemcpyHostToDevice, S.stream));
+    incrmt::k_solid_bound<<<incrmt::g2(S.g.ml, S.g.nl), dim3(32, 8), 0, S.stream>>>(S.g, S.d_sol, nobj, S.d_box);
+    S.launches++;
+    INCRMT_CKL("k_solid_bound");
+    INCRMT_CK(cudaMemcpyAsync(box, S.d_box, 4 * sizeof(int), cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_frame(incrmt_sim *h, int mode, const int box[4], float *host) {
+    if (!h || !box || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    const int nobj = static_cast<int>(S.sol.size());
+    const int li = box[0], ui = box[1], lj = box[2], uj = box[3], si = ui - li, sj = uj - lj;
+    if (mode < 0 || mode > 12) { set_error("bad output mode %d", mode); return INCRMT_ERR_BADARG; }
+    if (mode >= 6 && mode <= 9 && nobj == 0) { set_error("output mode %d needs a solid", mode); return INCRMT_ERR_BADARG; }
+    const bool stencil = mode == 4 || mode == 9 || mode == 12;
+    if (si <= 0 || sj <= 0 || li < (stencil ? 1 : 0) || lj < (stencil ? 1 : 0) || ui > S.g.ml || uj > S.g.nl) {
+        set_error("bad output box [%d,%d)x[%d,%d) for mode %d", li, ui, lj, uj, mode);
+        return INCRMT_ERR_BADARG;
+    }
+    const size_t need = static_cast<size_t>(si + 1) * (sj + 1);
+    if (need > S.frame_cap) {
+        cudaFree(S.d_frame);
+        S.d_frame = nullptr;
+        S.frame_cap = 0;
+        INCRMT_CK(cudaMalloc(&S.d_frame, need * sizeof(float)));
+        S.frame_cap = need;
+    }
+    const double off = incrmt::frame_corner_mode(mode) ? 2.0 : 1.5;
+    const double lx = S.g.ax + S.g.dx * (li - off), ly = S.g.ay + S.g.dy * (lj - off);
+    incrmt::k_frame<<<incrmt::g2(si + 1, sj + 1), dim3(32, 8), 0, S.stream>>>(S.g, S.f, S.d_sol, nobj, mode, li, lj,
+                                                                             si, sj, lx, ly, S.d_frame);
+    S.launches++;
+    INCRMT_CKL("k_frame");
+    INCRMT_CK(cudaMemcpyAsync(host, S.d_frame, need * sizeof(float), cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}

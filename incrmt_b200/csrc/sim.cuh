@@ -20,6 +20,8 @@ constexpr int kMaxObjects = 64;
 enum ObjType : int {
     OBJ_SIMPLE_SPIN = 0,  // obj_simple_spin (object.hh:422-467, object.cc:152-219)
     OBJ_CIRCLE = 1,       // obj_circle (object.hh:128-138, object.cc:22-34)
+    OBJ_ROUNDED_ROD = 2,  // obj_rounded_rod (object.hh:218-241, object.cc:75-78, 275-278)
+    OBJ_ELLIPSE = 3,      // rotated ellipse under gravity (no reference counterpart)
 };
 
 /** Device description of one solid: material constants (mat_const,
@@ -32,7 +34,9 @@ struct ObjDev {
     double eps, pinw, ex_visc;
     double tf1, tf2, tf3;
     // Geometry: simple spin {c0, c1, c2, piv_r, th_max, omega, piv_thresh,
-    // K_stiff}; circle {cx, cy, cr, grav, uu, vv, omega}.
+    // K_stiff}; circle {cx, cy, cr, grav, uu, vv, omega}; rounded rod
+    // {cx, cy, cr, grav, 0, 0, 0, cl}; ellipse {cx, cy, a, grav, 0, 0, 0, b,
+    // cos theta, sin theta}.
     double g[10];
     // Per-step state set on the host before each stress evaluation.
     double cth, sth;
@@ -59,25 +63,41 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
         double th = atan2(Y, X), c = cos(3 * th);
         return sqrt(X * X + Y * Y) - o.g[0] - c * (o.g[1] + o.g[2] * c);
     }
+    if (o.type == OBJ_ROUNDED_ROD) {  // obj_rounded_rod::phi, object.cc:275-278
+        double fY = fabs(Y) - o.g[7];
+        return (fY < 0 ? fabs(X) : sqrt(fY * fY + X * X)) - o.g[2];
+    }
+    if (o.type == OBJ_ELLIPSE) {
+        // Semi-axes a=g[2], b=g[7] at angle th (g[8]=cos th, g[9]=sin th).
+        // With r = |(X'/a, Y'/b)| in the body frame, (r-1)/|grad r| is the
+        // signed distance to first order in the distance, which is all the
+        // pinning band uses; the band rebuild makes it exact.
+        const double xb = o.g[8] * X + o.g[9] * Y, yb = -o.g[9] * X + o.g[8] * Y;
+        const double ia = 1 / o.g[2], ib = 1 / o.g[7];
+        const double r = sqrt(xb * xb * ia * ia + yb * yb * ib * ib);
+        const double gr = sqrt(xb * xb * ia * ia * ia * ia + yb * yb * ib * ib * ib * ib);
+        if (gr == 0) return -fmin(o.g[2], o.g[7]);
+        return (r - 1) * r / gr;
+    }
     return sqrt(X * X + Y * Y) - o.g[2];  // obj_circle::phi, object.cc:22-24
 }
 
 /** Initial reference map (object::transform / obj_standard::transform). */
 __device__ __forceinline__ void obj_transform(const ObjDev &o, double x, double y, double &X, double &Y) {
-    if (o.type == OBJ_CIRCLE) { X = x - o.g[0]; Y = y - o.g[1]; }
+    if (o.type != OBJ_SIMPLE_SPIN) { X = x - o.g[0]; Y = y - o.g[1]; }
     else { X = x; Y = y; }
 }
 
 /** Initial solid velocity (object::velocity / obj_standard::velocity,
  * object.cc:13-16). */
 __device__ __forceinline__ void obj_velocity(const ObjDev &o, double X, double Y, double &u, double &v) {
-    if (o.type == OBJ_CIRCLE) { u = o.g[4] - o.g[6] * Y; v = o.g[5] + o.g[6] * X; }
+    if (o.type != OBJ_SIMPLE_SPIN) { u = o.g[4] - o.g[6] * Y; v = o.g[5] + o.g[6] * X; }
     else { u = 0; v = 0; }
 }
 
 /** Extra accelerations (object::accel overrides): the simple spinner's
- * rotating pivot (object.cc:189-197) and the circle's gravity
- * (object.cc:31-34). */
+ * rotating pivot (object.cc:189-197) and the gravity of the circle, the
+ * rounded rod and the ellipse (object.cc:31-34, 75-78). */
 __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, double X, double Y,
                                           double phiv, double &ax, double &ay) {
     if (o.type == OBJ_SIMPLE_SPIN) {

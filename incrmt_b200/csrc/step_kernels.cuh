@@ -532,20 +532,25 @@ __global__ void k_update_velocity(GridDev g, FluidDev f, const SolidDev *sol, in
 }
 
 /** Pins the level set to the reference map within the pinning width, over
- * the whole ghosted grid (obj_field::pin, obj_field.cc:92-97). */
-__global__ void k_pin(GridDev g, ObjDev o, SolidDev s) {
+ * the whole ghosted grid (obj_field::pin, obj_field.cc:92-97); object
+ * blockIdx.z. */
+__global__ void k_pin(GridDev g, const ObjDev *obj, const SolidDev *sol) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - 2, j = blockIdx.y * blockDim.y + threadIdx.y - 2;
     if (i >= g.m + 2 || j >= g.n + 2) return;
+    const ObjDev &o = obj[blockIdx.z];
+    const SolidDev &s = sol[blockIdx.z];
     const int q = g.idx(i, j);
     const double p = s.phi[q];
     if (p < o.pinw && p > -o.pinw) s.phi[q] = obj_phi(o, s.X[q], s.Y[q]);
 }
 
-/** Initial reference map and level set of one object over the ghosted grid
- * (obj_field::init via fluid_2d::init_fields, fluid_2d.cc:198-205). */
-__global__ void k_init_object(GridDev g, ObjDev o, SolidDev s) {
+/** Initial reference map and level set of object blockIdx.z over the
+ * ghosted grid (obj_field::init via fluid_2d::init_fields, fluid_2d.cc:198-205). */
+__global__ void k_init_object(GridDev g, const ObjDev *obj, const SolidDev *sol) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - 2, j = blockIdx.y * blockDim.y + threadIdx.y - 2;
     if (i >= g.m + 2 || j >= g.n + 2) return;
+    const ObjDev &o = obj[blockIdx.z];
+    const SolidDev &s = sol[blockIdx.z];
     const int q = g.idx(i, j);
     double X, Y;
     obj_transform(o, g.ax + g.dx * (0.5 + i), g.ay + g.dy * (0.5 + j), X, Y);

@@ -1,0 +1,158 @@
+/* Host-side classes with the names, constructor arguments, call sequence,
+ * stdout lines and output files of IncRMT's simulation classes (fluid_2d,
+ * sim_type, mat_const and the object types; fluid_2d.hh:29-178,
+ * sim_type.hh:22-81, obj_field.hh:15-29, object.hh), driving the GPU through
+ * the C ABI of libincrmt_gpu.so. A program written against the reference's
+ * fluid_2d (such as its ftest driver) builds against these classes unchanged
+ * for the scenarios they cover: walled domains with simple-spin rotors and
+ * circles. Errors from the library print the library's message to stderr and
+ * exit with status 1, the reference's own convention (mgs_mac.cc:31-34). */
+#ifndef INCRMT_HOST_HH
+#define INCRMT_HOST_HH
+
+#include <cstdio>
+#include <vector>
+
+#include "incrmt.h"
+#include "incrmt_sim.h"
+
+class fluid_2d;
+
+/** Default size of the boundary repulsion region, in multiples of eps
+ * (sim_type.hh:14). */
+const double w_scale_default = 3.;
+/** Default boundary repulsion force (sim_type.hh:17). */
+const double w_force_default = 20.;
+
+/** Simulation geometry and boundary periodicity (sim_type.hh:22-81). */
+struct sim_type {
+    const double ax, bx, ay, by;
+    const double w_scale, w_force;
+    const bool x_prd, y_prd;
+    sim_type() : ax(-1), bx(1), ay(-1), by(1), w_scale(w_scale_default), w_force(w_force_default),
+                 x_prd(true), y_prd(true) {}
+    sim_type(double ax_, double bx_, double ay_, double by_, bool x_prd_, bool y_prd_)
+        : ax(ax_), bx(bx_), ay(ay_), by(by_), w_scale(w_scale_default), w_force(w_force_default),
+          x_prd(x_prd_), y_prd(y_prd_) {}
+    sim_type(double ax_, double bx_, double ay_, double by_, bool x_prd_, bool y_prd_, double w_scale_,
+             double w_force_)
+        : ax(ax_), bx(bx_), ay(ay_), by(by_), w_scale(w_scale_), w_force(w_force_), x_prd(x_prd_), y_prd(y_prd_) {}
+    virtual ~sim_type() {}
+};
+
+/** Material constants of a solid (obj_field.hh:15-29). */
+struct mat_const {
+    double G, rhos, ev_trans_mult;
+    bool set_velocity;
+    mat_const(double G_, double rhos_, double ev_trans_mult_, bool set_velocity_ = true)
+        : G(G_), rhos(rhos_), ev_trans_mult(ev_trans_mult_), set_velocity(set_velocity_) {}
+};
+
+/** A solid's geometry and forcing, described to the GPU as a plain record. */
+struct object {
+    virtual ~object() {}
+    /** Fills the type and geometry fields of the library's object record. */
+    virtual void describe(incrmt_object_desc &d) const = 0;
+    /** Called by fluid_2d::initialize after the time step is chosen
+     * (object::start, fluid_2d.cc:114-115). */
+    virtual void start(fluid_2d &f) {}
+    /** Called with each tracked-point record the library collected
+     * (time, position before and after its correction). */
+    virtual void track_record(const double *rec) {}
+    /** Flushes per-object output at a frame (object::write, fluid_2d_io.cc:107). */
+    virtual void write(int k, double time) {}
+};
+
+/** Three-pronged rotor pinned at its centre, spun by a stiff anchor
+ * (object.hh:418-470). Writes <filename>.odr/track.dat: records of four
+ * doubles (time, x, y, unwrapped angle) for the tracked point
+ * (obj_simple_spin::file_output, object.cc:202-219). */
+struct obj_simple_spin : public object {
+    const double r_scale, a1, a2, piv_r, th_max, omega;
+    const char *filename;
+    FILE *fp;
+    int prev_q, wind;
+    double K_stiff;
+    obj_simple_spin(double r_scale_, double a1_, double a2_, double piv_r_, double th_max_, double omega_,
+                    const char *filename_)
+        : r_scale(r_scale_), a1(a1_), a2(a2_), piv_r(piv_r_), th_max(th_max_), omega(omega_),
+          filename(filename_), fp(nullptr), prev_q(0), wind(0), K_stiff(0) {}
+    ~obj_simple_spin();
+    void describe(incrmt_object_desc &d) const override;
+    void start(fluid_2d &f) override;
+    void track_record(const double *rec) override;
+    void write(int k, double time) override;
+};
+
+/** Circle of radius cr centred at (cx, cy) with an initial velocity and
+ * spin and a downward acceleration grav (object.hh:124-137). */
+struct obj_circle : public object {
+    const double cx, cy, cr, uu, vv, omega, grav;
+    obj_circle(double cx_, double cy_, double cr_, double grav_ = 0)
+        : cx(cx_), cy(cy_), cr(cr_), uu(0), vv(0), omega(0), grav(grav_) {}
+    obj_circle(double cx_, double cy_, double cr_, double uu_, double vv_, double omega_, double grav_ = 0)
+        : cx(cx_), cy(cy_), cr(cr_), uu(uu_), vv(vv_), omega(omega_), grav(grav_) {}
+    void describe(incrmt_object_desc &d) const override;
+};
+
+/** The fluid-structure simulation (fluid_2d.hh:29-178): same constructor,
+ * add_object / initialize / solve / step_forward / write_files sequence and
+ * output directory layout. The state lives on the GPU. */
+class fluid_2d {
+    public:
+        const int m, n, ml, nl;
+        const bool x_prd, y_prd;
+        const double ax, bx, ay, by, dx, dy, xsp, ysp;
+        const double visc, rhof, tw, pinw, eps;
+        const int ntrace;
+        const unsigned int fflags;
+        const char *filename;
+        /** Time step limit chosen by initialize (fluid_2d.hh:107). */
+        double dt_reg;
+        /** Simulation time (fluid_2d.hh:105), updated after every step. */
+        double time;
+        /** Frames written so far by solve (fluid_2d.hh:83). */
+        int f_num;
+        /** Right-edge zero-pressure condition (fluid_2d.hh:117-121). */
+        bool zpr;
+        /** Precision of the projections' V-cycles: INCRMT_PREC_FP64 (the
+         * reference's) or INCRMT_PREC_MIXED; set before initialize. */
+        int precision;
+        fluid_2d(int m_, int n_, sim_type &sim_t_, double visc_, double rhof_, double tw_, double pinw_,
+                 int ntrace_, unsigned int fflags_, const char *filename_);
+        ~fluid_2d();
+        void add_object(object *o, mat_const &mc);
+        void initialize(double ev_mult, double dt_pad, double dt_ev_pad);
+        void solve(double duration, int frames);
+        void step_forward(double dt);
+        void write_files(int sn);
+        void save_header(double duration, int frames);
+        /** Steps of size adt <= dt_reg that cover interval (fluid_2d.hh:173-177). */
+        inline int timestep_select(double interval, double &adt) {
+            int l = static_cast<int>(interval / dt_reg) + 1;
+            adt = interval / l;
+            return l;
+        }
+        /** The library handle, for callers that need the rest of the C ABI. */
+        incrmt_sim *handle() { return h; }
+    private:
+        sim_type &sim_t;
+        incrmt_sim *h;
+        std::vector<object *> olist;
+        std::vector<double> rhos;
+        std::vector<float> fbuf;
+        std::vector<double> dbuf;
+        bool const_rho;
+        bool created;
+        void create();
+        void output(const char *prefix, int mode, int sn);
+        void output(const char *prefix, int mode, int sn, const int box[4]);
+        void output_tracers(int sn);
+        void init_tracers();
+        void drain_track_records();
+};
+
+/** Prints the library's last error and exits when r is not INCRMT_OK. */
+void incrmt_check(int r, const char *what);
+
+#endif

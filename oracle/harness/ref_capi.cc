@@ -68,6 +68,36 @@ ref_sim* make_sspin(int m,int ntrace,const char *base) {
     return r;
 }
 
+/** A walled (or periodic) domain with any number of circles (type 1:
+ * obj_circle(cx,cy,cr,uu,vv,omega,grav), object.hh:128-138) and rounded rods
+ * (type 2: obj_rounded_rod(cx,cy,cr,cl,grav), object.hh:229-230); mats holds
+ * G and rhos per object. Output directory <base>.odr. */
+ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double visc,double rhof,
+                    int ntrace,int nobj,const int *types,const double *params,const double *mats,
+                    const char *base) {
+    ref_sim *r=new ref_sim;
+    r->fa=new char[strlen(base)+1];
+    strcpy(r->fa,base);
+    r->fout=new char[strlen(base)+8];
+    sprintf(r->fout,"%s.odr",base);
+    mkdir(r->fout,S_IRWXU|S_IRWXG|S_IROTH|S_IXOTH);
+    const double tw=2.5,pinw=2.5;
+    const unsigned int fflags=8|16|64|128|256|512;
+    for(int k=0;k<nobj;k++) {
+        const double *p=params+8*k;
+        if(types[k]==1) r->obj.push_back(new obj_circle(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
+        else r->obj.push_back(new obj_rounded_rod(p[0],p[1],p[2],p[3],p[4]));
+    }
+    r->st=new sim_type(geom[0],geom[1],geom[2],geom[3],x_prd!=0,y_prd!=0);
+    r->f=new fluid_2d(m,n,*r->st,visc,rhof,tw,pinw,ntrace,fflags,r->fout);
+    for(int k=0;k<nobj;k++) {
+        mat_const mc(mats[2*k],mats[2*k+1],1,true);
+        r->f->add_object(r->obj[k],mc);
+    }
+    r->f->initialize(0.8,0.4,0.8);
+    return r;
+}
+
 /** Address of field number id (0..23, in the member order of struct field,
  * fields.hh:7-49) at grid index ij of the full (ghosted) array. */
 inline double& fld(fluid_2d &f,int id,int ij) {
@@ -87,6 +117,12 @@ extern "C" {
 /** Creates the simple-spin simulation. \return an opaque handle. */
 void* ref_sspin_create(int m,int ntrace,const char *base) {
     return make_sspin(m,ntrace,base);
+}
+
+void* ref_multi_create(int m,int n,const double *geom,int x_prd,int y_prd,double visc,double rhof,
+                       int ntrace,int nobj,const int *types,const double *params,const double *mats,
+                       const char *base) {
+    return make_multi(m,n,geom,x_prd,y_prd,visc,rhof,ntrace,nobj,types,params,mats,base);
 }
 
 void ref_destroy(void *h) {
@@ -265,6 +301,12 @@ int ref_stage(void *h,int stage,double dt) {
 void ref_steps(void *h,int steps,double dt) {
     fluid_2d &f=*static_cast<ref_sim*>(h)->f;
     for(int s=0;s<steps;s++) f.step_forward(dt);
+}
+
+/** fluid_2d::solve (fluid_2d.cc:254-295): frames of output written by the
+ * reference's own writers into the simulation's output directory. */
+void ref_solve(void *h,double duration,int frames) {
+    static_cast<ref_sim*>(h)->f->solve(duration,frames);
 }
 
 /** Standalone variable-density solve of the reference's MAC (sys=0,

@@ -17,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libincrmt_ref.so")
 RUN = os.path.join(HERE, "_ref", "ref_run")
+FTEST = os.path.join(HERE, "_ref", "ref_ftest")
 
 FIELD = {n: k for k, n in enumerate(
     "u v p rho ux uy vx vy ud vd ul vl ur vr uu vu c0 c1 c2 c3 s11 s12 s21 s22".split())}
@@ -59,6 +60,8 @@ def lib():
     L.ref_sspin_create.argtypes = [I, I, ctypes.c_char_p]
     L.ref_sspin_create.restype = P
     L.ref_destroy.argtypes = [P]
+    L.ref_multi_create.argtypes = [I, I, dp, I, I, D, D, I, I, ip, dp, dp, ctypes.c_char_p]
+    L.ref_multi_create.restype = P
     L.ref_dims.argtypes = [P, ip]
     L.ref_scalars.argtypes = [P, dp]
     L.ref_set_time.argtypes = [P, D]
@@ -109,15 +112,34 @@ def mg_apply(sys, m, n, rho, z, ax=-1., bx=1., ay=-1., by=1., x_prd=False, y_prd
 
 
 class RefSim:
-    """A reference fluid_2d simulation (currently the simple-spin scenario)."""
+    """A reference fluid_2d simulation: the simple-spin scenario, or with
+    `objects` a domain of circles and rounded rods.
 
-    def __init__(self, m, ntrace=512, workdir=None):
+    objects: list of ("circle", (cx, cy, cr, uu, vv, omega, grav), G, rhos) or
+    ("rod", (cx, cy, cr, cl, grav), G, rhos); geom = (ax, bx, ay, by)."""
+
+    def __init__(self, m, ntrace=512, workdir=None, n=None, objects=None, geom=(-1., 1., -1., 1.),
+                 visc=1e-2, rhof=1.0, periodic=(False, False)):
         self._tmp = None
         if workdir is None:
             self._tmp = tempfile.TemporaryDirectory()
             workdir = self._tmp.name
-        base = os.path.join(workdir, f"sspin_{m}").encode()
-        self.h = lib().ref_sspin_create(m, ntrace, base)
+        if objects is None:
+            base = os.path.join(workdir, f"sspin_{m}").encode()
+            self.h = lib().ref_sspin_create(m, ntrace, base)
+        else:
+            n = m if n is None else n
+            k = len(objects)
+            types = (ctypes.c_int * k)(*[1 if o[0] == "circle" else 2 for o in objects])
+            params = np.zeros((k, 8))
+            mats = np.zeros((k, 2))
+            for q, (kind, p, G, rhos) in enumerate(objects):
+                params[q, :len(p)] = p
+                mats[q] = (G, rhos)
+            g = np.array(geom, dtype=np.float64)
+            base = os.path.join(workdir, f"multi_{m}").encode()
+            self.h = lib().ref_multi_create(m, n, _dp(g), int(periodic[0]), int(periodic[1]), visc, rhof,
+                                            ntrace, k, types, _dp(params), _dp(mats), base)
         d = (ctypes.c_int * 7)()
         lib().ref_dims(self.h, d)
         self.m, self.n, self.ml, self.nl, self.n_obj, self.m_fem, self.n_fem = list(d)

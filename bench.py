@@ -1,7 +1,7 @@
 """Benchmark of incrmt_b200 on one node; prints ONE JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sspin1024|mac4096] [--precision fp64|mixed]
+                    [--workload sspin1024|mac4096|sed1024] [--precision fp64|mixed]
 
 Workload "sspin1024" (default): the ftest simple-spin scenario (three-pronged
 neo-Hookean rotor in a walled [-1,1]^2 box, ftest.cc:116-143) on a 1024 x 1024
@@ -17,6 +17,16 @@ one projection as the reference performs it: rebuild the coefficients and
 the multigrid hierarchy from the density (mgs_mac.cc:62-63), then V-cycles
 from a zero guess until ||b-Az||_2 <= 1e-9 ||b||_2. Every array is larger
 than the 126 MB L2, so no flush is needed between steps.
+
+The timed region is bracketed by cudaProfilerStart/Stop, so
+`ncu --profile-from-start off` lists exactly the timed launches.
+
+Workload "sed1024": the sediment configuration, 32 seeded bodies
+(alternately circles and ellipses, size 0.03-0.06, density 1.5-3, G 1,
+gravity (rho_s-1)/rho_s) settling in the walled [-0.75,0.75]x[-1.5,1.5] box of
+the reference's sediment driver on a 1024 x 2048 grid; one step =
+fluid_2d::step_forward. The reference arm runs the same bodies with each
+ellipse replaced by a rounded rod, the reference having no ellipse.
 
 Multi-GPU: the path does not shard; N ranks run N independent replicas
 (weak scaling), timed on the device as the maximum over ranks.
@@ -169,11 +179,59 @@ def cpu_reference_sspin(m, steps, warmup):
     return nsteps / secs, secs, (vm + vf) / (2.0 * nsteps), threads
 
 
+def _sed_reference_objects(seed=11):
+    """The sediment bodies as reference objects: circles as obj_circle, each
+    ellipse as the nearest reference shape, a rounded rod (obj_rounded_rod)
+    with the minor semi-axis as radius and the axis difference as half-length."""
+    from incrmt_b200 import workloads
+    objs = []
+    for o in workloads.sediment_bodies(seed=seed):
+        if o["kind"] == "circle":
+            objs.append(("circle", (o["cx"], o["cy"], o["r"], 0, 0, 0, o["grav"]), 1.0, o["rhos"]))
+        else:
+            objs.append(("rod", (o["cx"], o["cy"], o["b"], o["r"] - o["b"], o["grav"]), 1.0, o["rhos"]))
+    return objs
+
+
+def cpu_reference_sed(steps, warmup):
+    """The reference's own step on the sediment workload (oracle/_ref)."""
+    from oracle import refsim
+    if not refsim.available():
+        refsim.build()
+    r = refsim.RefSim(SED_M, ntrace=512, n=2 * SED_M, objects=_sed_reference_objects(), geom=SED_BOX, visc=2e-3)
+    dt_reg = r.scalars()["dt_reg"]
+    dt = 0.1 / (int(0.1 / dt_reg) + 1)
+    r.step(dt, warmup)
+    t0 = time.perf_counter()
+    r.step(dt, steps)
+    secs = time.perf_counter() - t0
+    r.close()
+    return steps / secs, secs, None, int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
     threads = os.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    if args.workload == "sed1024":
+        nref = max(1, min(args.steps, 3))
+        try:
+            sps, dt, _, thr = cpu_reference_sed(nref, min(args.warmup, 1))
+        except Exception as e:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"}))
+            return
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s",
+            "n_gpus": args.gpus, "steps": nref, "warmup": min(args.warmup, 1),
+            "ms_per_step": 1e3 * dt / nref, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"sediment {SED_M}x{2 * SED_M}, 32 bodies, ellipses as rounded rods",
+                       "flush": "working set larger than L2"},
+            "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
+                             "sample": f"{nref} steps (a step takes seconds on the host)"},
+            "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
     if args.workload == "sspin1024":
         m = 1024
         try:
@@ -197,21 +255,23 @@ def run_reference(args, ws, rank):
         print(json.dumps(line))
         return
     m = 4096
+    # A 4096^2 solve takes seconds on the host: time at most 8 of them.
+    nref = max(1, min(args.steps, 8))
     try:
-        sps, dt, vc = cpu_reference_mac(m, args.steps, args.warmup)
+        sps, dt, vc = cpu_reference_mac(m, nref, min(args.warmup, 1))
     except Exception as e:  # the reference could not be built here
         print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"}))
         return
     line = {
         "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * dt / max(args.steps, 1), "higher_is_better": True,
+        "ms_per_step": 1e3 * dt / nref, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"standalone MAC solve {m}x{m} (8 circles rho 3, 64 blobs), 1e-9",
                    "flush": "inputs larger than L2"},
         "vcycles_per_projection": vc,
         "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": threads, "kind": "reference",
-                         "sample": f"{args.steps} full solves at {m}x{m}"},
+                         "sample": f"{nref} full solves at {m}x{m} after {min(args.warmup, 1)} warm-up"},
         "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -220,21 +280,49 @@ def run_reference(args, ws, rank):
 # ---------------------------------------------------------------------------
 # GPU path
 
+SED_M = 1024
+SED_BOX = (-0.75, 0.75, -1.5, 1.5)
+
+
+def _make_sim(workload, rank, prec):
+    """The simulation of a step workload and its frame interval:
+    sspin1024 (ftest simple-spin, solve(2pi,120) frames) or sed1024 (32
+    seeded circles and ellipses settling in the sediment box at 1024 x 2048,
+    frame interval 0.1 as sediment.cc's 1600 frames over T=160)."""
+    from incrmt_b200 import capi, workloads
+    if workload == "sspin1024":
+        m = 1024
+        sim = capi.Simulation(m, m, ntrace=512, precision=prec)
+        sim.add_simple_spin()
+        sim.initialize()
+        rng = np.random.default_rng(1 + rank)
+        sim.set_tracers(rng.uniform(-1, 1, size=(512, 2)))
+        return sim, 2 * np.pi / 120, f"simple-spin {m}x{m} fluid_2d::step_forward, dt of solve(2pi,120)"
+    m, n = SED_M, 2 * SED_M
+    ax, bx, ay, by = SED_BOX
+    sim = capi.Simulation(m, n, ax=ax, bx=bx, ay=ay, by=by, visc=2e-3, ntrace=512, precision=prec)
+    for o in workloads.sediment_bodies(seed=11 + rank):
+        if o["kind"] == "circle":
+            sim.add_circle(o["cx"], o["cy"], o["r"], 1.0, o["rhos"], grav=o["grav"])
+        else:
+            sim.add_ellipse(o["cx"], o["cy"], o["r"], o["b"], o["theta"], 1.0, o["rhos"], grav=o["grav"])
+    sim.initialize()
+    rng = np.random.default_rng(1 + rank)
+    sim.set_tracers(np.stack([rng.uniform(ax, bx, 512), rng.uniform(ay, by, 512)], axis=1))
+    return sim, 0.1, (f"sediment {m}x{n}: 32 seeded circles and ellipses (r 0.03-0.06, rho 1.5-3, G 1) "
+                      f"settling, fluid_2d::step_forward, dt of 0.1 frames")
+
+
 def run_ours_sspin(args, ws, rank, local, dist):
-    """Simple-spin steps on the GPU through the simulation C ABI."""
+    """Simulation steps on the GPU through the simulation C ABI."""
     import torch
     from incrmt_b200 import capi
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    m = 1024
     prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
-    sim = capi.Simulation(m, m, ntrace=512, precision=prec)
-    sim.add_simple_spin()
-    dt_reg = sim.initialize()
-    rng = np.random.default_rng(1 + rank)
-    sim.set_tracers(rng.uniform(-1, 1, size=(512, 2)))
-    interval = 2 * np.pi / 120
+    sim, interval, wl = _make_sim(args.workload, rank, prec)
+    dt_reg = sim.dt_reg
     l = int(interval / dt_reg) + 1
     dt = interval / l
     ext = torch.cuda.ExternalStream(sim.stream(), device=dev)
@@ -246,10 +334,12 @@ def run_ours_sspin(args, ws, rank, local, dist):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        torch.cuda.cudart().cudaProfilerStart()
         e0.record(ext)
         sim.step(dt, args.steps)
         e1.record(ext)
         torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
     ms = e0.elapsed_time(e1)
     st1 = sim.stats()
     _barrier(dist)
@@ -284,10 +374,15 @@ def run_ours_sspin(args, ws, rank, local, dist):
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
         try:
-            sps, dts, vcr, thr = cpu_reference_sspin(m, 4, 1)
-            cpu = {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
-                   "sample": f"4 steps after 1 warm-up step at {m}x{m} (reference sources + "
-                             f"TGMG-API shim), OMP threads = {thr}"}
+            if args.workload == "sspin1024":
+                sps, dts, vcr, thr = cpu_reference_sspin(1024, 40, 2)
+                sample = (f"40 steps after 2 warm-up steps at 1024x1024 (reference sources + "
+                          f"TGMG-API shim), OMP threads = {thr}")
+            else:
+                sps, dts, vcr, thr = cpu_reference_sed(2, 0)
+                sample = (f"2 steps of the sediment workload with each ellipse replaced by a "
+                          f"rounded rod (the reference has no ellipse), OMP threads = {thr}")
+            cpu = {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference", "sample": sample}
         except Exception as e:
             cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
@@ -298,8 +393,7 @@ def run_ours_sspin(args, ws, rank, local, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == capi.PREC_FP64 else "f64 state, f32 V-cycles in f64 defect correction",
         "data": "synthetic",
-        "config": {"workload": f"simple-spin {m}x{m} fluid_2d::step_forward, dt of solve(2pi,120)",
-                   "precision": args.precision, "flush": "working set larger than L2",
+        "config": {"workload": wl, "precision": args.precision, "flush": "working set larger than L2",
                    "parallelism": f"replicas x{ws}"},
         "vcycles_per_projection": vc,
         "phase_ms_per_step": phases,
@@ -320,7 +414,7 @@ def run_ours_sspin(args, ws, rank, local, dist):
 def run_ours(args, ws, rank, local, dist):
     import torch
     from incrmt_b200 import capi, workloads
-    if args.workload == "sspin1024":
+    if args.workload in ("sspin1024", "sed1024"):
         return run_ours_sspin(args, ws, rank, local, dist)
 
     dev = torch.device("cuda", local)
@@ -353,11 +447,13 @@ def run_ours(args, ws, rank, local, dist):
     e1 = torch.cuda.Event(enable_timing=True)
     vcs = []
     with ClockSampler(local) as clk:
+        torch.cuda.cudart().cudaProfilerStart()
         e0.record(ext)
         for _ in range(args.steps):
             vcs.append(step())
         e1.record(ext)
         torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
     ms = e0.elapsed_time(e1)
     launches = s.launches() - l0
     kms, kbytes, klaunch = s.profile()
@@ -396,9 +492,9 @@ def run_ours(args, ws, rank, local, dist):
     if ws == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count()
-            sps, dt, _ = cpu_reference_mac(m, 2, 0)
+            sps, dt, _ = cpu_reference_mac(m, 4, 0)
             cpu = {"value": sps, "unit": "steps/s", "cores": threads, "kind": "reference",
-                   "sample": f"2 full {m}x{m} solves (reference callbacks + TGMG-API shim), "
+                   "sample": f"4 full {m}x{m} solves (reference callbacks + TGMG-API shim), "
                              f"OMP threads = {threads}"}
         except Exception as e:
             cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "reference",
@@ -432,10 +528,10 @@ def run_ours(args, ws, rank, local, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096"])
+    ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096", "sed1024"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

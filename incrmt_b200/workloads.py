@@ -122,3 +122,36 @@ def standalone_fem_problem(m, n=None, seed=5, device="cpu"):
     rho = circle_density(m, n, circ, device=device)
     src = blob_divergence(m + 1, n + 1, seed, device=device)
     return rho, src
+
+
+def sediment_bodies(seed=11, count=32, box=(-0.75, 0.75, -1.5, 1.5), rmin=0.03, rmax=0.06,
+                    rho_min=1.5, rho_max=3.0, gap=0.02):
+    """Seeded solids for the sediment configuration: `count` bodies in the
+    walled box of the reference's sediment driver (sediment.cc:22,124),
+    alternately circles and ellipses, sizes rmin-rmax, densities
+    rho_min-rho_max, each falling with gravity (rho_s-1)/rho_s
+    (sediment.cc:98). Placement is rejection-sampled so that bounding circles
+    keep `gap` from each other and from the walls (as sediment.cc:91-121
+    rejects overlaps). Returns a list of dicts: kind ('circle'|'ellipse'),
+    cx, cy, r (circle radius / ellipse major semi-axis), b (minor semi-axis),
+    theta, rhos, grav."""
+    rng = np.random.default_rng(seed)
+    ax, bx, ay, by = box
+    out = []
+    tries = 0
+    while len(out) < count:
+        tries += 1
+        if tries > 1000000:
+            raise RuntimeError("could not place the bodies")
+        r = rng.uniform(rmin, rmax)
+        x = rng.uniform(ax + r + gap, bx - r - gap)
+        y = rng.uniform(ay + r + gap, by - r - gap)
+        if any(math.hypot(x - o["cx"], y - o["cy"]) <= r + o["r"] + gap for o in out):
+            continue
+        rhos = rng.uniform(rho_min, rho_max)
+        kind = "circle" if len(out) % 2 == 0 else "ellipse"
+        bsemi = r if kind == "circle" else r * rng.uniform(0.5, 0.8)
+        theta = 0.0 if kind == "circle" else rng.uniform(0, math.pi)
+        out.append(dict(kind=kind, cx=x, cy=y, r=r, b=bsemi, theta=theta, rhos=rhos,
+                        grav=(rhos - 1) / rhos))
+    return out

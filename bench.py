@@ -1,7 +1,7 @@
 """Benchmark of incrmt_b200 on one node; prints ONE JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sspin1024|mac4096|sed1024] [--precision fp64|mixed]
+                    [--workload sspin1024|mac4096|sed1024|flag2048] [--precision fp64|mixed]
 
 Workload "sspin1024" (default): the ftest simple-spin scenario (three-pronged
 neo-Hookean rotor in a walled [-1,1]^2 box, ftest.cc:116-143) on a 1024 x 1024
@@ -27,6 +27,11 @@ gravity (rho_s-1)/rho_s) settling in the walled [-0.75,0.75]x[-1.5,1.5] box of
 the reference's sediment driver on a 1024 x 2048 grid; one step =
 fluid_2d::step_forward. The reference arm runs the same bodies with each
 ellipse replaced by a rounded rod, the reference having no ellipse.
+
+Workload "flag2048": the flag scenario (ftest.cc:335-378; y-periodic channel,
+uniform inflow, zero-pressure outlet, FEM projection with its fixed column) on
+3456 x 1152 square cells of [-1,5]x[-1,1] (about 2048^2 cells), mass ratio 1,
+bending rigidity 0.1, Re 100, aspect ratio 10.
 
 Multi-GPU: the path does not shard; N ranks run N independent replicas
 (weak scaling), timed on the device as the maximum over ranks.
@@ -108,6 +113,33 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
                 "samples": len(rows)}
+
+
+def _traffic(key):
+    """DRAM bytes per launch of a roofline kernel from the committed ncu
+    summary (profiles/traffic.json: dram__bytes_read.sum + dram__bytes_write.sum
+    of one captured launch), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f).get(key)
+
+
+def _roofline(key, ms, nbytes, launches, kernel, rule):
+    """Roofline object of a kernel timed live with CUDA events: achieved =
+    algorithmic bytes / device time, against the measured copy bandwidth."""
+    if not launches or ms <= 0:
+        return None
+    peak, peak_kind = _peaks()
+    achieved = (nbytes / (ms / 1e3)) / 1e9
+    t = _traffic(key)
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": t["bytes_per_launch"] if t else None,
+            "traffic_source": t["source"] if t else None,
+            "algorithmic_bytes_per_launch": nbytes / launches,
+            "avg_launch_us": 1e3 * ms / launches, "launches": launches, "bytes_rule": rule}
 
 
 def _dist():
@@ -209,15 +241,36 @@ def cpu_reference_sed(steps, warmup):
     return steps / secs, secs, None, int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
 
 
+def cpu_reference_flag(steps, warmup):
+    """The reference's own step on the flag workload (oracle/_ref)."""
+    from oracle import refsim
+    if not refsim.available():
+        refsim.build()
+    w = 0.1
+    flag = ("flag", (0.0, 0.0, 1.0, w, 0.25 * w, 0.0, 17), 4 * 0.1 / w ** 3, 1.0 / w)
+    r = refsim.RefSim(3 * FLAG_N, ntrace=0, n=FLAG_N, objects=[flag], geom=(-1.0, 5.0, -1.0, 1.0), visc=0.01,
+                      flow_u=1.0)
+    dt_reg = r.scalars()["dt_reg"]
+    iv = 30.0 / 900
+    dt = iv / (int(iv / dt_reg) + 1)
+    r.step(dt, warmup)
+    t0 = time.perf_counter()
+    r.step(dt, steps)
+    secs = time.perf_counter() - t0
+    r.close()
+    return steps / secs, secs, None, int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
     threads = os.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    if args.workload == "sed1024":
+    if args.workload in ("sed1024", "flag2048"):
         nref = max(1, min(args.steps, 3))
         try:
-            sps, dt, _, thr = cpu_reference_sed(nref, min(args.warmup, 1))
+            fn = cpu_reference_sed if args.workload == "sed1024" else cpu_reference_flag
+            sps, dt, _, thr = fn(nref, min(args.warmup, 1))
         except Exception as e:
             print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"}))
             return
@@ -226,7 +279,9 @@ def run_reference(args, ws, rank):
             "n_gpus": args.gpus, "steps": nref, "warmup": min(args.warmup, 1),
             "ms_per_step": 1e3 * dt / nref, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"sediment {SED_M}x{2 * SED_M}, 32 bodies, ellipses as rounded rods",
+            "config": {"workload": (f"sediment {SED_M}x{2 * SED_M}, 32 bodies, ellipses as rounded rods"
+                                    if args.workload == "sed1024" else
+                                    f"flag {3 * FLAG_N}x{FLAG_N} (mu 1, k_B 0.1, Re 100, ar 10)"),
                        "flush": "working set larger than L2"},
             "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
                              "sample": f"{nref} steps (a step takes seconds on the host)"},
@@ -282,6 +337,7 @@ def run_reference(args, ws, rank):
 
 SED_M = 1024
 SED_BOX = (-0.75, 0.75, -1.5, 1.5)
+FLAG_N = 1152
 
 
 def _make_sim(workload, rank, prec):
@@ -298,6 +354,21 @@ def _make_sim(workload, rank, prec):
         rng = np.random.default_rng(1 + rank)
         sim.set_tracers(rng.uniform(-1, 1, size=(512, 2)))
         return sim, 2 * np.pi / 120, f"simple-spin {m}x{m} fluid_2d::step_forward, dt of solve(2pi,120)"
+    if workload == "flag2048":
+        # The flag scenario (ftest.cc:335-378) on 3456 x 1152 square cells of
+        # [-1,5]x[-1,1] (about 2048^2 cells; 1152 = 9 x 2^7 lets the periodic
+        # direction halve seven times); mass ratio 1, bending rigidity 0.1,
+        # Re 100, aspect ratio 10.
+        n = FLAG_N
+        m = 3 * n
+        mu, k_B, Re, ar = 1.0, 0.1, 100.0, 10.0
+        w = 1.0 / ar
+        sim = capi.Simulation(m, n, ax=-1.0, bx=5.0, ay=-1.0, by=1.0, visc=1.0 / Re, ntrace=0,
+                              precision=prec, y_prd=True, horiz_flow=1.0)
+        sim.add_flag(0.0, 0.0, 1.0, w, 0.25 * w, 4 * k_B / w ** 3, mu / w, ntrace=17)
+        sim.initialize()
+        return sim, 30.0 / 900, (f"flag {m}x{n} on [-1,5]x[-1,1] (mu 1, k_B 0.1, Re 100, ar 10), FEM with "
+                                 f"zero-pressure outlet, y-periodic; fluid_2d::step_forward, dt of 900 frames over T=30")
     m, n = SED_M, 2 * SED_M
     ax, bx, ay, by = SED_BOX
     sim = capi.Simulation(m, n, ax=ax, bx=bx, ay=ay, by=by, visc=2e-3, ntrace=512, precision=prec)
@@ -353,6 +424,15 @@ def run_ours_sspin(args, ws, rank, local, dist):
     sim.set_profiling(True)
     sim.step(dt, min(args.steps, 10))
     phases = {k: v / min(args.steps, 10) for k, v in sim.profile().items()}
+    # Roofline of the projections' fine-level smoothing (the HBM-bound kernel
+    # with the largest time share): every launch bracketed by CUDA events on
+    # the simulation stream over a few more steps.
+    sim.set_profiling(False, smoothers=True)
+    sim.step(dt, min(args.steps, 10))
+    sm_ms, sm_bytes, sm_launch = 0.0, 0.0, 0
+    for which in (capi.SYS_MAC, capi.SYS_FEM):
+        a, b, c = sim.smoother_profile(which)
+        sm_ms, sm_bytes, sm_launch = sm_ms + a, sm_bytes + b, sm_launch + c
     sim.set_profiling(False)
 
     # End to end through the C ABI as fluid_2d::solve drives it: the steps of
@@ -378,6 +458,9 @@ def run_ours_sspin(args, ws, rank, local, dist):
                 sps, dts, vcr, thr = cpu_reference_sspin(1024, 40, 2)
                 sample = (f"40 steps after 2 warm-up steps at 1024x1024 (reference sources + "
                           f"TGMG-API shim), OMP threads = {thr}")
+            elif args.workload == "flag2048":
+                sps, dts, vcr, thr = cpu_reference_flag(2, 0)
+                sample = f"2 steps of the flag workload (reference sources + TGMG-API shim), OMP threads = {thr}"
             else:
                 sps, dts, vcr, thr = cpu_reference_sed(2, 0)
                 sample = (f"2 steps of the sediment workload with each ellipse replaced by a "
@@ -386,7 +469,6 @@ def run_ours_sspin(args, ws, rank, local, dist):
         except Exception as e:
             cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
-    peak, peak_kind = _peaks()
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -398,8 +480,12 @@ def run_ours_sspin(args, ws, rank, local, dist):
         "vcycles_per_projection": vc,
         "phase_ms_per_step": phases,
         "march_sweeps_per_step": (st1.march_sweeps - st0.march_sweeps) / args.steps,
+        "march_monotone_rebuilds": int(st1.march_monotone - st0.march_monotone),
         "extrap_sweeps_per_step": (st1.extrap_sweeps - st0.extrap_sweeps) / args.steps,
-        "roofline": None,
+        "roofline": _roofline(f"{args.workload}_smooth", sm_ms, sm_bytes, sm_launch,
+                              "k_smooth_rb / k_smooth_tile on the fine level of the MAC and FEM projections "
+                              "(two Gauss-Seidel sweeps per launch)",
+                              "updated unknowns x 2 sweeps x (3+c) x 8 B; c=2 MAC, 1 FEM"),
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(d2h / args.steps),
@@ -414,7 +500,7 @@ def run_ours_sspin(args, ws, rank, local, dist):
 def run_ours(args, ws, rank, local, dist):
     import torch
     from incrmt_b200 import capi, workloads
-    if args.workload in ("sspin1024", "sed1024"):
+    if args.workload in ("sspin1024", "sed1024", "flag2048"):
         return run_ours_sspin(args, ws, rank, local, dist)
 
     dev = torch.device("cuda", local)
@@ -486,8 +572,6 @@ def run_ours(args, ws, rank, local, dist):
 
     if rank != 0:
         return
-    peak, peak_kind = _peaks()
-    achieved = (kbytes / (kms / 1e3)) / 1e9 if kms > 0 else None
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
         try:
@@ -509,11 +593,9 @@ def run_ours(args, ws, rank, local, dist):
                                f"setup + V-cycles to 1e-9 from zero", "precision": args.precision,
                    "flush": "inputs larger than L2 (each array 134 MB)", "parallelism": f"replicas x{ws}"},
         "vcycles_per_projection": float(np.mean(vcs)),
-        "roofline": {"bound": "hbm", "kernel": "k_smooth (fine-level Gauss-Seidel colour sweep)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-                     "traffic": None, "launches": klaunch,
-                     "bytes_rule": "updated unknowns x (3+c) x 8 B, c=2 (MAC)"},
+        "roofline": _roofline("mac4096_smooth", kms, kbytes, klaunch,
+                              "k_smooth_rb (fine-level red-black Gauss-Seidel, two sweeps per launch)",
+                              "updated unknowns x 2 sweeps x (3+c) x 8 B, c=2 (MAC)"),
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "steps/s",
                 "h2d_bytes_per_step": int(rho_h.numel() * 8 + 2 * b_h.numel() * 8),
@@ -531,7 +613,7 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096", "sed1024"])
+    ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096", "sed1024", "flag2048"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -25,7 +25,11 @@ typedef struct incrmt_grid {
 
 /** Physical and numerical parameters (fluid_2d ctor: visc, rhof, tw, pinw,
  * ntrace; sim_type w_scale/w_force, default 3 and 20 when <= 0; fluid_2d::zpr;
- * plus the projection tolerance and precision of this implementation). */
+ * plus the projection tolerance and precision of this implementation).
+ * horiz_flow selects sim_horiz_flow (sim_type.hh:117-141, sim_type.cc:51-64):
+ * a uniform inflow of speed flow_u through the left edge (its two ghost
+ * columns hold (flow_u, 0)), the zero-pressure right edge (zpr is set) and
+ * the fluid initialised to (flow_u, 0). */
 typedef struct incrmt_phys {
     double visc, rhof, tw, pinw;
     double w_scale, w_force;
@@ -33,6 +37,8 @@ typedef struct incrmt_phys {
     int zpr;
     int precision;       /* INCRMT_PREC_FP64 or INCRMT_PREC_MIXED for both projections */
     double mg_rel_tol;   /* relative residual of each projection (default 1e-9 when <= 0) */
+    int horiz_flow;      /* 1: sim_horiz_flow boundary and initial conditions */
+    double flow_u;       /* its inflow speed U */
 } incrmt_phys;
 
 /** Object kinds (subclasses of object, object.hh). */
@@ -42,6 +48,9 @@ typedef struct incrmt_phys {
 #define INCRMT_OBJ_ELLIPSE     3  /* params: cx, cy, a, b, theta, grav: an ellipse with semi-axes a, b
                                      rotated by theta, falling under grav like obj_circle; it has no
                                      counterpart in the reference */
+#define INCRMT_OBJ_FLAG        4  /* params: cx, cy, flag_l, flag_w, flag_a, perturb_v, ntrace: a flag
+                                     anchored at its leading end (obj_flag, object.hh:471-505,
+                                     object.cc:420-496), tracking ntrace points along its length */
 
 /** An object plus its material constants (object*, mat_const;
  * fluid_2d::add_object, fluid_2d.cc:74-90; obj_field.hh:15-29). */
@@ -66,6 +75,7 @@ typedef struct incrmt_sim_stats {
     long long march_sweeps, extrap_sweeps;
     long long launches;                    /* kernels issued by this handle */
     double dt_reg, time;
+    long long march_monotone;              /* band rebuilds that needed the monotone march sweeps */
 } incrmt_sim_stats;
 
 /** Creates the simulation (fluid_2d::fluid_2d, fluid_2d.cc:26-43). */
@@ -120,9 +130,11 @@ int incrmt_get_tracers(incrmt_sim *h, double *host);
 /** Object-tracked points: records of 6 doubles (x, y, stage velocity, X, Y). */
 int incrmt_get_object_tracers(incrmt_sim *h, double *host, int *count);
 
-/** Tracked-point records collected so far, 5 doubles each: time, position
- * before and after the correction onto the reference map (obj_track output,
- * object.cc:202-219). clear=1 empties the list. */
+/** Tracked-point records collected so far, 1 + 4*K doubles each for the K
+ * object tracers of incrmt_get_object_tracers: the time, then for every
+ * tracer its position before and after the correction onto the reference map
+ * (obj_track::file_output, object.cc:202-219, 339-347). clear=1 empties the
+ * list. */
 int incrmt_track_records(incrmt_sim *h, double *host, int cap, int *count, int clear);
 
 /** Adds a tracked-point record now (obj_track::write at frame output,

@@ -206,6 +206,7 @@ OBJ_SIMPLE_SPIN = 0
 OBJ_CIRCLE = 1
 OBJ_ROUNDED_ROD = 2
 OBJ_ELLIPSE = 3
+OBJ_FLAG = 4
 FIELD_PHI = 200
 FIELD_STATUS = 201
 FIELDS = {n: k for k, n in enumerate(
@@ -232,7 +233,7 @@ class Phys(ctypes.Structure):
     _fields_ = [("visc", ctypes.c_double), ("rhof", ctypes.c_double), ("tw", ctypes.c_double),
                 ("pinw", ctypes.c_double), ("w_scale", ctypes.c_double), ("w_force", ctypes.c_double),
                 ("ntrace", ctypes.c_int), ("zpr", ctypes.c_int), ("precision", ctypes.c_int),
-                ("mg_rel_tol", ctypes.c_double)]
+                ("mg_rel_tol", ctypes.c_double), ("horiz_flow", ctypes.c_int), ("flow_u", ctypes.c_double)]
 
 
 class ObjectDesc(ctypes.Structure):
@@ -246,7 +247,8 @@ class SimStats(ctypes.Structure):
                 ("vcycles_fem", ctypes.c_longlong), ("solves_mac", ctypes.c_longlong),
                 ("solves_fem", ctypes.c_longlong), ("march_sweeps", ctypes.c_longlong),
                 ("extrap_sweeps", ctypes.c_longlong), ("launches", ctypes.c_longlong),
-                ("dt_reg", ctypes.c_double), ("time", ctypes.c_double)]
+                ("dt_reg", ctypes.c_double), ("time", ctypes.c_double),
+                ("march_monotone", ctypes.c_longlong)]
 
 
 def _sim_sigs(L):
@@ -285,13 +287,17 @@ class Simulation:
     """A fluid_2d on the GPU (fluid_2d.hh:131-177) through the C ABI."""
 
     def __init__(self, m, n, ax=-1.0, bx=1.0, ay=-1.0, by=1.0, visc=1e-2, rhof=1.0, tw=2.5,
-                 pinw=2.5, ntrace=512, zpr=False, precision=PREC_FP64, rel_tol=1e-9):
+                 pinw=2.5, ntrace=512, zpr=False, precision=PREC_FP64, rel_tol=1e-9, y_prd=False,
+                 horiz_flow=None):
+        """horiz_flow=U selects sim_horiz_flow: inflow of speed U at the left
+        edge, zero pressure at the right, fluid starting at (U, 0)."""
         L = lib()
         if not hasattr(L, "_sim_ready"):
             _sim_sigs(L)
             L._sim_ready = True
-        g = Grid(m, n, ax, bx, ay, by, 0, 0)
-        p = Phys(visc, rhof, tw, pinw, 0.0, 0.0, ntrace, int(zpr), precision, rel_tol)
+        g = Grid(m, n, ax, bx, ay, by, 0, int(y_prd))
+        p = Phys(visc, rhof, tw, pinw, 0.0, 0.0, ntrace, int(zpr), precision, rel_tol,
+                 int(horiz_flow is not None), float(horiz_flow or 0.0))
         h = ctypes.c_void_p()
         check(L.incrmt_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -317,6 +323,11 @@ class Simulation:
     def add_ellipse(self, cx, cy, a, b, theta, G, rhos, grav=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_ELLIPSE, G, rhos, ev_trans_mult, 1,
                        (ctypes.c_double * 8)(cx, cy, a, b, theta, grav, 0, 0))
+        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+
+    def add_flag(self, cx, cy, flag_l, flag_w, flag_a, G, rhos, perturb_v=0.0, ntrace=17, ev_trans_mult=1.0):
+        d = ObjectDesc(OBJ_FLAG, G, rhos, ev_trans_mult, 1,
+                       (ctypes.c_double * 8)(cx, cy, flag_l, flag_w, flag_a, perturb_v, ntrace, 0))
         check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
 
     def initialize(self, ev_mult=0.8, dt_pad=0.4, dt_ev_pad=0.8):
@@ -375,17 +386,21 @@ class Simulation:
         return out[:4 * self.ntrace].reshape(self.ntrace, 4)
 
     def object_tracers(self):
-        out = np.empty(6 * 64)
         c = ctypes.c_int()
+        check(lib().incrmt_get_object_tracers(self._h, None, ctypes.byref(c)))
+        out = np.empty(6 * max(c.value, 1))
         check(lib().incrmt_get_object_tracers(self._h, _dptr(out), ctypes.byref(c)))
         return out[:6 * c.value].reshape(c.value, 6)
 
     def track_records(self, clear=False):
+        """Records of 1 + 4*K doubles: time, then (x, y) before and after the
+        correction for each of the K object tracers."""
+        rec = 1 + 4 * len(self.object_tracers())
         c = ctypes.c_int()
         check(lib().incrmt_track_records(self._h, None, 0, ctypes.byref(c), 0))
-        out = np.empty(5 * max(c.value, 1))
+        out = np.empty(rec * max(c.value, 1))
         check(lib().incrmt_track_records(self._h, _dptr(out), c.value, ctypes.byref(c), int(clear)))
-        return out[:5 * c.value].reshape(c.value, 5)
+        return out[:rec * c.value].reshape(c.value, rec)
 
     def record_track(self):
         check(lib().incrmt_record_track(self._h))

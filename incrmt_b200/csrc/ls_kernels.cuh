@@ -769,6 +769,12 @@ __global__ void k_ls_fim_coop(LsGrid g, const LsObj *ob, const int *list, const 
     for (; it < max_sweeps; it++) {
         if (tid == 0) flags[(it + 1) % 3] = 0;
         const bool odd = it & 1;
+        // Where the second-order stencil is not monotone, the plain sweeps can
+        // cycle between two states instead of settling (seen on thin solids at
+        // fine grids). After half the sweep budget each value may then only
+        // move towards the interface, which settles; flags[12] records it.
+        const bool monotone = it >= max_sweeps / 2;
+        if (monotone && tid == 0) flags[12] = 1;
         bool ch = false;
         for (int t = tid; t < count; t += nth) {
             const LsObj &o = ob[list_k[t]];
@@ -783,9 +789,11 @@ __global__ void k_ls_fim_coop(LsGrid g, const LsObj *ob, const int *list, const 
                 if (st == 7) {
                     March<true> mr(g, o.phi, o.s, cur, old);
                     if (any_in(mr, i, j)) v = mr.calc(i, j);
+                    if (monotone && v > old) v = old;
                 } else {
                     March<false> mr(g, o.phi, o.s, cur, old);
                     if (any_in(mr, i, j)) v = mr.calc(i, j);
+                    if (monotone && v < old) v = old;
                 }
             }
             nxt[ij] = v;

@@ -55,8 +55,11 @@ struct Sim {
     long long steps = 0;
     long long vc_mac = 0, vc_fem = 0, solves_mac = 0, solves_fem = 0;
     long long ls_sweeps = 0, ex_sweeps = 0;
+    long long ls_monotone = 0;                      // band rebuilds that needed the monotone sweeps
     long long launches = 0;
     int track_count = 1;                            // obj_track step counter
+    int track_every = 10;                           // steps between its records
+    int trk = -1;                                   // object whose points are tracked
     int t_correction = 1;
     int pre_stress_objects = 0;
     std::vector<double> track;                      // records: time, xpre, ypre, x, y
@@ -130,6 +133,7 @@ struct Sim {
     int set_rho();
     int pin();
     int build_bands();
+    int godunov(bool tang);
     int extrapolate_all();
     int mac_projection();
     int fem_projection(double dt);
@@ -144,15 +148,22 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
         set_error("bad grid %dx%d", gr->m, gr->n);
         return INCRMT_ERR_BADARG;
     }
-    if (gr->x_prd || gr->y_prd) {
-        set_error("periodic domains are not supported by the time step (walls only)");
+    if (gr->x_prd) {
+        set_error("x-periodic domains are not supported by the time step (walls or inflow in x)");
+        return INCRMT_ERR_BADARG;
+    }
+    if (gr->y_prd && (gr->n & 1)) {
+        set_error("a y-periodic grid needs an even n (multigrid coarsening)");
         return INCRMT_ERR_BADARG;
     }
     INCRMT_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     g.m = gr->m; g.n = gr->n; g.ml = g.m + 4; g.nl = g.n + 4;
     g.P = (g.ml + 31) / 32 * 32;
-    g.mf = g.m + 1; g.nf = g.n + 1;
-    g.zpr = ph->zpr ? 1 : 0;
+    g.yp = gr->y_prd ? 1 : 0;
+    g.mf = g.m + 1; g.nf = g.yp ? g.n : g.n + 1;  // m_fem, n_fem (fluid_2d.cc:30-31)
+    g.hflow = ph->horiz_flow ? 1 : 0;
+    g.flow_u = ph->flow_u;
+    g.zpr = (ph->zpr || g.hflow) ? 1 : 0;  // sim_horiz_flow::start sets zpr (sim_type.cc:59-64)
     g.ax = gr->ax; g.bx = gr->bx; g.ay = gr->ay; g.by = gr->by;
     g.dx = (g.bx - g.ax) / g.m; g.dy = (g.by - g.ay) / g.n;  // fluid_2d.cc:33-34
     g.xsp = 1 / g.dx; g.ysp = 1 / g.dy; g.xxsp = g.xsp * g.xsp; g.yysp = g.ysp * g.ysp;
@@ -200,23 +211,24 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 16, stream));
     INCRMT_CK(cudaMallocHost(&h_flags, sizeof(int) * 16));
     if (ntrace > 0 && (r = alloc(&tm, 4 * static_cast<size_t>(ntrace)))) return r;
-    if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, 0, g.zpr, stream))) return r;
-    if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, 0, g.zpr, stream))) return r;
+    if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, g.yp, g.zpr, stream))) return r;
+    if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, g.yp, g.zpr, stream))) return r;
     return INCRMT_OK;
 }
 
 int Sim::add_object(const incrmt_object_desc *d) {
     if (initialized) { set_error("objects must be added before initialize"); return INCRMT_ERR_BADARG; }
     if (static_cast<int>(obj.size()) >= kMaxObjects) { set_error("too many objects"); return INCRMT_ERR_BADARG; }
-    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_ELLIPSE) {
+    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_FLAG) {
         set_error("unknown object type %d", d->type);
         return INCRMT_ERR_BADARG;
     }
     ObjDev o{};
-    o.type = d->type == INCRMT_OBJ_SIMPLE_SPIN ? OBJ_SIMPLE_SPIN
-             : d->type == INCRMT_OBJ_CIRCLE   ? OBJ_CIRCLE
+    o.type = d->type == INCRMT_OBJ_SIMPLE_SPIN   ? OBJ_SIMPLE_SPIN
+             : d->type == INCRMT_OBJ_CIRCLE      ? OBJ_CIRCLE
              : d->type == INCRMT_OBJ_ROUNDED_ROD ? OBJ_ROUNDED_ROD
-                                                 : OBJ_ELLIPSE;
+             : d->type == INCRMT_OBJ_ELLIPSE     ? OBJ_ELLIPSE
+                                                 : OBJ_FLAG;
     o.set_velocity = d->set_velocity;
     o.G = d->G; o.rhos = d->rhos; o.ev_trans_mult = d->ev_trans_mult;
     o.eps = g.eps; o.pinw = pinw * g.dx;  // obj_field.cc:16
@@ -235,6 +247,15 @@ int Sim::add_object(const incrmt_object_desc *d) {
         // obj_rounded_rod(cx,cy,cr,cl,grav) (object.hh:229-230); at rest initially
         if (!(p[2] > 0) || !(p[3] >= 0)) { set_error("rounded rod needs cr > 0, cl >= 0"); return INCRMT_ERR_BADARG; }
         o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[4]; o.g[7] = p[3];
+    } else if (o.type == OBJ_FLAG) {
+        // obj_flag(cx,cy,flag_l,flag_w,flag_a,perturb_v,ntrace) (object.cc:420-441)
+        if (!(p[2] > 0) || !(p[3] > 0) || !(p[4] >= 0)) { set_error("flag needs positive length and width"); return INCRMT_ERR_BADARG; }
+        if (p[4] >= 0.5 * p[3]) {
+            set_error("flag_a should be smaller than 0.5*flag_w to avoid cutting off its influence");
+            return INCRMT_ERR_BADARG;
+        }
+        if (!(p[6] >= 1) || p[6] > 4096) { set_error("flag needs 1..4096 tracked points"); return INCRMT_ERR_BADARG; }
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[7] = p[3]; o.g[8] = p[4]; o.g[9] = p[5];
     } else {
         // ellipse (cx,cy,a,b,theta,grav); at rest initially
         if (!(p[2] > 0) || !(p[3] > 0)) { set_error("ellipse needs positive semi-axes"); return INCRMT_ERR_BADARG; }
@@ -338,7 +359,7 @@ int Sim::set_rho() {
 int Sim::build_bands() {
     const int no = static_cast<int>(obj.size());
     if (no == 0) return INCRMT_OK;
-    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 11, stream));
+    INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 13, stream));
     const dim3 gg(cdiv(lg.mL, 32), cdiv(lg.nL, 8), no);
     k_ls_scan<<<gg, kB2, 0, stream>>>(lg, d_lso);
     k_ls_newton<<<gg, kB2, 0, stream>>>(lg, d_lso, d_flags + 6);
@@ -365,6 +386,7 @@ int Sim::build_bands() {
     if (h_flags[6]) { set_error("level++: Newton iteration failed."); return h_flags[6]; }
     if (h_flags[10]) { set_error("level-set candidate list overflow"); return INCRMT_ERR_BADARG; }
     ls_sweeps += h_flags[3];
+    if (h_flags[12]) ls_monotone++;
     if (!h_flags[4]) { set_error("level-set march did not settle in %d sweeps", h_flags[3]); return INCRMT_ERR_NOCONV; }
     k_ls_finish<<<gg, kB2, 0, stream>>>(lg, d_lso);
     k_ls_trial<<<gg, kB2, 0, stream>>>(lg, d_lso);
@@ -467,8 +489,9 @@ int Sim::mac_projection() {
 /** fluid_2d::finite_element_projection + copy_pressure
  * (fluid_2d.cc:1297-1328). */
 int Sim::fem_projection(double dt) {
+    k_fem_ghosts<<<1, 1024, 0, stream>>>(g, f);
     k_fem_source<<<g2(g.mf, g.nf), kB2, 0, stream>>>(g, f, src_fem, dt);
-    launches++;
+    launches += 2;
     INCRMT_CKL("k_fem_source");
     int outer = cur_phase, r;
     if ((r = phase_end())) return r;
@@ -506,7 +529,7 @@ int Sim::tracers(int st, double dt) {
     INCRMT_CKL("k_tracers");
     if (st == 2 && nobjtr > 0) {
         // obj_track::update_tracers (object.cc:358-366): a record every 10 steps.
-        if (track_count == 10) return record_track();
+        if (track_count == track_every) return record_track();
         track_count++;
     }
     return INCRMT_OK;
@@ -516,23 +539,24 @@ int Sim::tracers(int st, double dt) {
  * 339-347): the point before and after its correction onto the reference
  * map, stored with the time; the host writes track.dat from these. */
 int Sim::record_track() {
-    double pre[2];
-    INCRMT_CK(cudaMemcpyAsync(pre, otm, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+    std::vector<double> pre(6 * static_cast<size_t>(nobjtr)), post(pre.size());
+    INCRMT_CK(cudaMemcpyAsync(pre.data(), otm, sizeof(double) * pre.size(), cudaMemcpyDeviceToHost, stream));
     if (t_correction) {
-        Field2 rm{sol[0].X, sol[0].Y};
+        Field2 rm{sol[trk].X, sol[trk].Y};
         INCRMT_CK(cudaMemsetAsync(d_flags + 9, 0, sizeof(int), stream));
-        k_correct_tracers<<<1, 32, 0, stream>>>(g, rm, otm, nobjtr, d_flags + 9);
+        k_correct_tracers<<<cdiv(nobjtr, 128), 128, 0, stream>>>(g, rm, otm, nobjtr, d_flags + 9);
         launches++;
         INCRMT_CKL("k_correct_tracers");
     }
-    double post[2];
-    INCRMT_CK(cudaMemcpyAsync(post, otm, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+    INCRMT_CK(cudaMemcpyAsync(post.data(), otm, sizeof(double) * post.size(), cudaMemcpyDeviceToHost, stream));
     int r = fetch_flags();
     if (r) return r;
     if (h_flags[9]) t_correction = 0;
     track.push_back(time);
-    track.push_back(pre[0]); track.push_back(pre[1]);
-    track.push_back(post[0]); track.push_back(post[1]);
+    for (int k = 0; k < nobjtr; k++) {
+        track.push_back(pre[6 * k]); track.push_back(pre[6 * k + 1]);
+        track.push_back(post[6 * k]); track.push_back(post[6 * k + 1]);
+    }
     track_count = 1;
     return INCRMT_OK;
 }
@@ -555,23 +579,48 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
                  dt2 = 0.5 * g.rhof / (g.visc * (g.xxsp + g.yysp)) * dt_pad;
     if (dt0 < dt1) dt_reg = dt0 < dt2 ? dt0 : dt2;
     else dt_reg = dt1 < dt2 ? dt1 : dt2;
-    // object::start (obj_simple_spin::start_extra, object.cc:152-165).
+    // object::start (obj_simple_spin::start_extra, object.cc:152-165;
+    // obj_flag::start_extra, object.cc:455-469).
     for (auto &o : obj) {
         if (o.type == OBJ_SIMPLE_SPIN) {
             double t = o.g[3] + o.eps;
             o.g[6] = t * t;
             o.g[7] = 0.1 / (dt_reg * dt_reg);
+        } else if (o.type == OBJ_FLAG) {
+            double t = o.g[8] + o.eps;
+            o.g[10] = t * t;
+            o.g[11] = 0.01 / (dt_reg * dt_reg);
         }
     }
-    // Object tracers: obj_simple_spin tracks one point at 0.9*r_scale on the
-    // x axis (object.hh:454-457).
+    // Object tracers (obj_track) of the first tracking object: the simple
+    // spinner's point at 0.9*r_scale on the x axis, recorded every 10 steps
+    // (object.hh:444-453), or the flag's points evenly spaced along its
+    // length from the tail, recorded every 100 steps (object.cc:427-434).
     nobjtr = 0;
-    if (!obj.empty() && obj[0].type == OBJ_SIMPLE_SPIN) {
-        nobjtr = 1;
-        int r = alloc(&otm, 6);
+    trk = -1;
+    for (size_t k = 0; k < obj.size() && trk < 0; k++)
+        if (obj[k].type == OBJ_SIMPLE_SPIN || obj[k].type == OBJ_FLAG) trk = static_cast<int>(k);
+    if (trk >= 0) {
+        const ObjDev &o = obj[trk];
+        std::vector<double> h;
+        if (o.type == OBJ_SIMPLE_SPIN) {
+            const double x = 0.9 * desc[trk].params[0];
+            h = {x, 0, 0, 0, x, 0};
+            track_every = 10;
+        } else {
+            const int nt = static_cast<int>(desc[trk].params[6]);
+            const double step = nt == 1 ? 0. : o.g[2] / (nt - 1);
+            double ex = o.g[2];
+            for (int k = 0; k < nt; k++, ex -= step) {
+                const double t[6] = {ex, 0, 0, 0, ex - o.g[0], 0 - o.g[1]};
+                h.insert(h.end(), t, t + 6);
+            }
+            track_every = 100;
+        }
+        nobjtr = static_cast<int>(h.size() / 6);
+        int r = alloc(&otm, h.size());
         if (r) return r;
-        double h[6] = {0.9 * desc[0].params[0], 0, 0, 0, 0.9 * desc[0].params[0], 0};
-        INCRMT_CK(cudaMemcpyAsync(otm, h, sizeof(h), cudaMemcpyHostToDevice, stream));
+        INCRMT_CK(cudaMemcpyAsync(otm, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, stream));
         INCRMT_CK(cudaStreamSynchronize(stream));
     }
     int r = upload_objects();
@@ -594,6 +643,21 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
     return INCRMT_OK;
 }
 
+/** godunov_upwinding_set<tang> followed by edge_boundary_conditions
+ * (fluid_2d.cc:1112-1121, 689-777). */
+int Sim::godunov(bool tang) {
+    const int no = static_cast<int>(obj.size());
+    if (tang) k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+    else k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+    launches++;
+    if (g.yp) {
+        k_wrap_edges_y<<<cdiv(g.m, 256), 256, 0, stream>>>(g, f);
+        launches++;
+    }
+    INCRMT_CKL("k_godunov");
+    return INCRMT_OK;
+}
+
 /** fluid_2d::step_forward (fluid_2d.cc:298-369). */
 int Sim::step(double dt) {
     if (!initialized) { set_error("not initialized"); return INCRMT_ERR_BADARG; }
@@ -604,11 +668,11 @@ int Sim::step(double dt) {
     INCRMT_PHASE(INCRMT_PHASE_TRACERS, if ((r = tracers(1, dt))) return r);
     INCRMT_PHASE(INCRMT_PHASE_ADVECTION, {
         k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
-        k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+        if ((r = godunov(true))) return r;
         k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f);
         k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
-        k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
-        launches += 5;
+        if ((r = godunov(false))) return r;
+        launches += 3;
         INCRMT_CKL("advection");
     });
     time += 0.5 * dt;
@@ -648,12 +712,12 @@ int Sim::stage(int s, double dt) {
         case 0: return tracers(1, dt);
         case 1:
         case 2: k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt); break;
-        case 3: k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no); break;
+        case 3: return godunov(true);
         case 4: break;  // fused into the Godunov kernels
         case 5: k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f); break;
         case 6:
         case 7: k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt); break;
-        case 8: k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no); break;
+        case 8: return godunov(false);
         case 9: return mac_projection();
         case 10: return update_reference_map(dt);
         case 11: return pin();
@@ -891,9 +955,10 @@ int incrmt_get_object_tracers(incrmt_sim *h, double *host, int *count) {
 int incrmt_track_records(incrmt_sim *h, double *host, int cap, int *count, int clear) {
     if (!h || !count) { set_error("null argument"); return INCRMT_ERR_BADARG; }
     incrmt::Sim &S = h->s;
-    const int n = static_cast<int>(S.track.size() / 5);
+    const size_t rec = 1 + 4 * static_cast<size_t>(S.nobjtr);
+    const int n = static_cast<int>(S.track.size() / rec);
     *count = n;
-    if (host) memcpy(host, S.track.data(), sizeof(double) * 5 * (n < cap ? n : cap));
+    if (host) memcpy(host, S.track.data(), sizeof(double) * rec * (n < cap ? n : cap));
     if (clear) S.track.clear();
     return INCRMT_OK;
 }
@@ -913,6 +978,7 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
     st->solves_mac = S.solves_mac;
     st->solves_fem = S.solves_fem;
     st->march_sweeps = S.ls_sweeps;
+    st->march_monotone = S.ls_monotone;
     st->extrap_sweeps = S.ex_sweeps;
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;

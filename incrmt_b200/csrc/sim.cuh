@@ -22,6 +22,7 @@ enum ObjType : int {
     OBJ_CIRCLE = 1,       // obj_circle (object.hh:128-138, object.cc:22-34)
     OBJ_ROUNDED_ROD = 2,  // obj_rounded_rod (object.hh:218-241, object.cc:75-78, 275-278)
     OBJ_ELLIPSE = 3,      // rotated ellipse under gravity (no reference counterpart)
+    OBJ_FLAG = 4,         // obj_flag (object.hh:471-505, object.cc:420-496)
 };
 
 /** Device description of one solid: material constants (mat_const,
@@ -36,8 +37,9 @@ struct ObjDev {
     // Geometry: simple spin {c0, c1, c2, piv_r, th_max, omega, piv_thresh,
     // K_stiff}; circle {cx, cy, cr, grav, uu, vv, omega}; rounded rod
     // {cx, cy, cr, grav, 0, 0, 0, cl}; ellipse {cx, cy, a, grav, 0, 0, 0, b,
-    // cos theta, sin theta}.
-    double g[10];
+    // cos theta, sin theta}; flag {cx, cy, flag_l, 0, 0, 0, 0, flag_w, flag_a,
+    // perturb_v, flag_thresh, K_stiff}.
+    double g[12];
     // Per-step state set on the host before each stress evaluation.
     double cth, sth;
 };
@@ -67,6 +69,10 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
         double fY = fabs(Y) - o.g[7];
         return (fY < 0 ? fabs(X) : sqrt(fY * fY + X * X)) - o.g[2];
     }
+    if (o.type == OBJ_FLAG) {  // obj_flag::phi, object.cc:446-449
+        const double L = o.g[2];
+        return (X < 0 ? sqrt(X * X + Y * Y) : (X > L ? sqrt((X - L) * (X - L) + Y * Y) : fabs(Y))) - 0.5 * o.g[7];
+    }
     if (o.type == OBJ_ELLIPSE) {
         // Semi-axes a=g[2], b=g[7] at angle th (g[8]=cos th, g[9]=sin th).
         // With r = |(X'/a, Y'/b)| in the body frame, (r-1)/|grad r| is the
@@ -91,13 +97,19 @@ __device__ __forceinline__ void obj_transform(const ObjDev &o, double x, double 
 /** Initial solid velocity (object::velocity / obj_standard::velocity,
  * object.cc:13-16). */
 __device__ __forceinline__ void obj_velocity(const ObjDev &o, double X, double Y, double &u, double &v) {
-    if (o.type != OBJ_SIMPLE_SPIN) { u = o.g[4] - o.g[6] * Y; v = o.g[5] + o.g[6] * X; }
+    if (o.type == OBJ_FLAG) {  // obj_flag::velocity, object.cc:489-496
+        X -= o.g[2];
+        const double rsq = X * X + Y * Y;
+        u = 0;
+        v = rsq < o.g[10] ? o.g[9] * trans_func_in(o, sqrt(rsq) - o.g[8]) : 0.;
+    } else if (o.type != OBJ_SIMPLE_SPIN) { u = o.g[4] - o.g[6] * Y; v = o.g[5] + o.g[6] * X; }
     else { u = 0; v = 0; }
 }
 
 /** Extra accelerations (object::accel overrides): the simple spinner's
- * rotating pivot (object.cc:189-197) and the gravity of the circle, the
- * rounded rod and the ellipse (object.cc:31-34, 75-78). */
+ * rotating pivot (object.cc:189-197), the flag's anchor (object.cc:476-484)
+ * and the gravity of the circle, the rounded rod and the ellipse
+ * (object.cc:31-34, 75-78). */
 __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, double X, double Y,
                                           double phiv, double &ax, double &ay) {
     if (o.type == OBJ_SIMPLE_SPIN) {
@@ -107,6 +119,13 @@ __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, d
                    K = o.g[7] * trans_func_in(o, sqrt(rsq) - o.g[3]);
             ax -= K * (x - rx);
             ay -= K * (y - ry);
+        }
+    } else if (o.type == OBJ_FLAG) {  // obj_flag::accel, object.cc:476-484
+        const double delx = x - o.g[0], dely = y - o.g[1], rsq = delx * delx + dely * dely;
+        if (rsq < o.g[10]) {
+            const double K = o.g[11] * trans_func_in(o, sqrt(rsq) - o.g[8]);
+            ax -= K * (x - X);
+            ay -= K * (y - Y);
         }
     } else {
         ay -= o.g[3] * trans_func_in(o, phiv);
@@ -118,6 +137,9 @@ struct GridDev {
     int m, n, ml, nl, P;
     int mf, nf;  // FEM nodes
     int zpr;
+    int yp;         // y-periodic (sim_type::y_prd)
+    int hflow;      // sim_horiz_flow inflow at the left edge
+    double flow_u;  // its speed
     double ax, bx, ay, by, dx, dy, xsp, ysp, xxsp, yysp;
     double visc, rhof, eps, epsinv, w_scale, w_force;
     __device__ __forceinline__ int idx(int i, int j) const { return (j + 2) * P + (i + 2); }

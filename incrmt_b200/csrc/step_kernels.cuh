@@ -1,7 +1,8 @@
 // Time-step kernels of fluid_2d::step_forward (fluid_2d.cc:298-369) for
-// grids that are non-periodic in both directions. One thread per cell or
-// edge; every kernel reads the fields it needs straight from HBM (SoA,
-// coalesced along x) and writes each output once.
+// grids with walls in x (optionally the zero-pressure right edge and the
+// horizontal inflow of sim_horiz_flow) and walls or periodicity in y. One
+// thread per cell or edge; every kernel reads the fields it needs straight
+// from HBM (SoA, coalesced along x) and writes each output once.
 #pragma once
 #include "sim.cuh"
 
@@ -97,22 +98,29 @@ __global__ void k_godunov(GridDev g, FluidDev f, const SolidDev *sol, int nobj) 
             }
         }
     }
-    if (j < g.n - 1) {
-        const int t = q + P;
+    if (j < g.n - 1 || g.yp) {
+        // With y periodicity the top edge of the last row is the bottom edge
+        // of row 0. The reference selects it in edge_boundary_conditions with
+        // godunov_set_du<true> on the ghost row -1, which holds row n-1's
+        // fluid edge values but the (never written) ghost solid values
+        // (fluid_2d.cc:760-768); qs is that row for the solids.
+        const bool wrap = j == g.n - 1;
+        const bool tg = tang || wrap;
+        const int t = wrap ? q - (g.n - 1) * P : q + P, qs = wrap ? t - P : q;
         const double fvu = f.vu[q], ftvd = f.vd[t];
         if (fvu + ftvd > 0 && fvu > 0) {
             f.vd[t] = fvu;
             f.ud[t] = f.uu[q];
-            for (int k = 0; k < nobj; k++) { sol[k].Xd[t] = sol[k].Xu[q]; sol[k].Yd[t] = sol[k].Yu[q]; }
+            for (int k = 0; k < nobj; k++) { sol[k].Xd[t] = sol[k].Xu[qs]; sol[k].Yd[t] = sol[k].Yu[qs]; }
         } else if (fvu + ftvd < 0 && ftvd < 0) {
-            if (tang) f.vu[q] = ftvd;
+            if (tg) f.vu[q] = ftvd;
         } else {
-            if (tang) f.vu[q] = 0.5 * (fvu + ftvd);
+            if (tg) f.vu[q] = 0.5 * (fvu + ftvd);
             f.vd[t] = 0;
             f.ud[t] = 0.5 * (f.uu[q] + f.ud[t]);
             for (int k = 0; k < nobj; k++) {
-                sol[k].Xd[t] = 0.5 * (sol[k].Xu[q] + sol[k].Xd[t]);
-                sol[k].Yd[t] = 0.5 * (sol[k].Yu[q] + sol[k].Yd[t]);
+                sol[k].Xd[t] = 0.5 * (sol[k].Xu[qs] + sol[k].Xd[t]);
+                sol[k].Yd[t] = 0.5 * (sol[k].Yu[qs] + sol[k].Yd[t]);
             }
         }
     }
@@ -125,8 +133,23 @@ __global__ void k_godunov(GridDev g, FluidDev f, const SolidDev *sol, int nobj) 
         if (g.zpr) { f.ul[q + 1] = f.ur[q]; f.vl[q + 1] = f.vr[q]; }
         else { f.ul[q + 1] = 0; f.vl[q + 1] = 0; f.ur[q] = 0; }
     }
-    if (j == 0) { f.ud[q] = 0; f.vd[q] = 0; f.vu[q - P] = 0; }
-    if (j == g.n - 1) { f.ud[q + P] = 0; f.vd[q + P] = 0; f.vu[q] = 0; }
+    if (!g.yp) {
+        if (j == 0) { f.ud[q] = 0; f.vd[q] = 0; f.vu[q - P] = 0; }
+        if (j == g.n - 1) { f.ud[q + P] = 0; f.vd[q + P] = 0; f.vu[q] = 0; }
+    }
+}
+
+/** Ghost rows of the edge values under y periodicity, after k_godunov
+ * (fluid_2d::edge_boundary_conditions, fluid_2d.cc:760-768): row -1 takes
+ * row n-1's top values, row n row 0's bottom values. */
+__global__ void k_wrap_edges_y(GridDev g, FluidDev f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.m) return;
+    const int q0 = g.idx(i, 0), qt = g.idx(i, g.n - 1);
+    f.vu[q0 - g.P] = f.vu[qt];
+    f.uu[q0 - g.P] = f.uu[qt];
+    f.vd[qt + g.P] = f.vd[q0];
+    f.ud[qt + g.P] = f.ud[q0];
 }
 
 /** compute_tangential_stability_derivatives (fluid_2d.cc:953-975), without
@@ -238,6 +261,10 @@ __global__ void k_mac_correct(GridDev g, FluidDev f, const double *z, const doub
     if (i >= g.m || j >= g.n) return;
     const int q = g.idx(i, j), ij = j * g.m + i;
     if (j > 0) f.vd[q] -= ey[j * g.m + i] * (z[ij] - z[ij - g.m]) * g.ysp;
+    else if (g.yp) {
+        f.vd[q] -= ey[i] * (z[ij] - z[ij + (g.n - 1) * g.m]) * g.ysp;
+        f.vd[q + g.n * g.P] = f.vd[q];
+    }
     if (i > 0) f.ul[q] -= ex[j * (g.m + 1) + i] * (z[ij] - z[ij - 1]) * g.xsp;
 }
 
@@ -281,14 +308,16 @@ __global__ void k_set_rho(GridDev g, FluidDev f, const ObjDev *obj, const SolidD
     f.rho[q] = sfrac >= 1 ? rho / sfrac : (1 - sfrac) * g.rhof + rho;
 }
 
-/** Ghost velocities for walls (fluid_2d::set_boundaries, fluid_2d.cc:698-721):
- * one block; first the left/right ghosts of every row, then the bottom/top
- * ghost rows including the corners. */
+/** Ghost velocities (fluid_2d::set_boundaries, fluid_2d.cc:689-725): one
+ * block; first the left/right ghosts of every row (walls, or linear
+ * extrapolation at a zero-pressure right edge), then the bottom/top ghost
+ * rows including the corners (walls or periodic), then the inflow of
+ * sim_horiz_flow::boundary (sim_type.cc:51-56) on the two left ghost columns. */
 __global__ void k_set_boundaries(GridDev g, FluidDev f) {
     const int P = g.P;
+    double *u = f.u, *v = f.v;
     for (int j = threadIdx.x; j < g.n; j += blockDim.x) {
         const int q = g.idx(0, j);
-        double *u = f.u, *v = f.v;
         u[q - 2] = -u[q + 1]; v[q - 2] = -v[q + 1];
         u[q - 1] = -u[q]; v[q - 1] = -v[q];
         const int r = q + g.m;
@@ -304,11 +333,24 @@ __global__ void k_set_boundaries(GridDev g, FluidDev f) {
     const int G = g.n * P;
     for (int i = threadIdx.x - 2; i < g.m + 2; i += blockDim.x) {
         const int q = g.idx(i, 0);
-        double *u = f.u, *v = f.v;
-        u[q - 2 * P] = -u[q + P]; v[q - 2 * P] = -v[q + P];
-        u[q - P] = -u[q]; v[q - P] = -v[q];
-        u[q + G] = -u[q + G - P]; v[q + G] = -v[q + G - P];
-        u[q + G + P] = -u[q + G - 2 * P]; v[q + G + P] = -v[q + G - 2 * P];
+        if (g.yp) {
+            u[q - 2 * P] = u[q + G - 2 * P]; v[q - 2 * P] = v[q + G - 2 * P];
+            u[q - P] = u[q + G - P]; v[q - P] = v[q + G - P];
+            u[q + G] = u[q]; v[q + G] = v[q];
+            u[q + G + P] = u[q + P]; v[q + G + P] = v[q + P];
+        } else {
+            u[q - 2 * P] = -u[q + P]; v[q - 2 * P] = -v[q + P];
+            u[q - P] = -u[q]; v[q - P] = -v[q];
+            u[q + G] = -u[q + G - P]; v[q + G] = -v[q + G - P];
+            u[q + G + P] = -u[q + G - 2 * P]; v[q + G + P] = -v[q + G - 2 * P];
+        }
+    }
+    if (!g.hflow) return;
+    __syncthreads();
+    for (int j = threadIdx.x - 2; j < g.n + 2; j += blockDim.x) {
+        const int q = g.idx(0, j);
+        u[q - 1] = u[q - 2] = g.flow_u;
+        v[q - 1] = v[q - 2] = 0;
     }
 }
 
@@ -457,8 +499,10 @@ __global__ void k_ustar(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev
 }
 
 /** u* at cell (i,j) for the FEM source, with the ghost values that
- * fem_source_term_conditions sets for walls (fluid_2d.cc:847-871). */
+ * fem_source_term_conditions sets for walls, the zero-pressure edge and y
+ * periodicity (fluid_2d.cc:837-871). */
 __device__ __forceinline__ void ustar_bc(const GridDev &g, const FluidDev &f, int i, int j, double &c0, double &c1) {
+    if (j < 0 && g.yp) j = g.n - 1;  // ghost row -1 copies row n-1 (fluid_2d.cc:861-865)
     if (j < 0 || j >= g.n || i >= g.m) { c0 = 0; c1 = 0; return; }
     const int q = g.idx(i, j);
     if (i < 0) {
@@ -467,6 +511,34 @@ __device__ __forceinline__ void ustar_bc(const GridDev &g, const FluidDev &f, in
     }
     c0 = f.c0[q];
     c1 = f.c1[q];
+}
+
+/** The ghost values of u* that fem_source_term_conditions stores
+ * (fluid_2d.cc:837-871), written back into c0/c1 so that the state matches
+ * the reference's: left ghost column u (zero-pressure edge) or 0, right ghost
+ * column 0, then the bottom ghost row copying row n-1 (y periodic) or the
+ * bottom and top ghost rows 0. One block; k_fem_source computes the same
+ * values on the fly (ustar_bc). */
+__global__ void k_fem_ghosts(GridDev g, FluidDev f) {
+    for (int j = threadIdx.x; j < g.n; j += blockDim.x) {
+        const int q = g.idx(0, j), r = g.idx(g.m, j);
+        f.c0[q - 1] = g.zpr ? f.u[q - 1] : 0.;
+        f.c1[q - 1] = g.zpr ? f.v[q - 1] : 0.;
+        f.c0[r] = 0;
+        f.c1[r] = 0;
+    }
+    __syncthreads();
+    const int G = g.n * g.P;
+    for (int i = threadIdx.x - 1; i <= g.m; i += blockDim.x) {
+        const int q = g.idx(i, 0);
+        if (g.yp) {
+            f.c0[q - g.P] = f.c0[q + G - g.P];
+            f.c1[q - g.P] = f.c1[q + G - g.P];
+        } else {
+            f.c0[q - g.P] = f.c0[q + G] = 0;
+            f.c1[q - g.P] = f.c1[q + G] = 0;
+        }
+    }
 }
 
 /** FEM source at the (m+1) x (n+1) corners (finite_element_projection,
@@ -492,7 +564,7 @@ __global__ void k_pressure_sum(GridDev g, const double *z, double *partial) {
          t += static_cast<long>(gridDim.x) * blockDim.x) {
         const int i = static_cast<int>(t % g.mf), j = static_cast<int>(t / g.mf);
         double w = (i == 0 || i == g.mf - 1) ? 0.5 : 1.0;
-        if (j == 0 || j == g.nf - 1) w *= 0.5;
+        if (!g.yp && (j == 0 || j == g.nf - 1)) w *= 0.5;
         acc += w * z[t];
     }
     acc = block_sum_256(acc);
@@ -513,7 +585,8 @@ __global__ void k_copy_pressure(GridDev g, FluidDev f, const double *z, const do
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i > g.m || j > g.n) return;
     const double pavg = g.zpr ? 0. : psum[0] * (1. / (static_cast<double>(g.m) * g.n));
-    f.p[g.idx(i, j)] = z[j * g.mf + i] - pavg;
+    const int jz = g.yp && j == g.n ? 0 : j;  // the last row repeats row 0 (fluid_2d.cc:1323)
+    f.p[g.idx(i, j)] = z[jz * g.mf + i] - pavg;
 }
 
 /** End-of-step velocity and reference map (update_velocity,
@@ -559,8 +632,8 @@ __global__ void k_init_object(GridDev g, const ObjDev *obj, const SolidDev *sol)
     s.phi[q] = obj_phi(o, X, Y);
 }
 
-/** Initial velocity from the solids' momenta (fluid_2d::init_fields,
- * fluid_2d.cc:213-239); the fluid starts at rest (base sim_type::velocity). */
+/** Initial velocity from the solids' momenta and the scenario's fluid
+ * velocity (fluid_2d::init_fields, fluid_2d.cc:213-239). */
 __global__ void k_init_velocity(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, int nobj) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.m || j >= g.n) return;
@@ -579,8 +652,10 @@ __global__ void k_init_velocity(GridDev g, FluidDev f, const ObjDev *obj, const 
         f.u[q] = mu / rho;
         f.v[q] = mv / rho;
     } else {
+        // sim_type::velocity: at rest, or (U, 0) for sim_horiz_flow (sim_type.hh:132-135)
+        const double uf = g.hflow ? g.flow_u : 0.;
         double irho = 1 / ((1 - sfrac) * g.rhof + rho);
-        f.u[q] = ((1 - sfrac) * g.rhof * 0. + mu) * irho;
+        f.u[q] = ((1 - sfrac) * g.rhof * uf + mu) * irho;
         f.v[q] = ((1 - sfrac) * g.rhof * 0. + mv) * irho;
     }
 }

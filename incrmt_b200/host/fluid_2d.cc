@@ -79,6 +79,40 @@ void obj_simple_spin::write(int k, double time) {
     if (fp != nullptr) fflush(fp);
 }
 
+obj_flag::~obj_flag() {
+    if (fp != nullptr) fclose(fp);
+}
+
+void obj_flag::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_FLAG;
+    const double p[8] = {cx, cy, flag_l, flag_w, flag_a, perturb_v, static_cast<double>(ntrace), 0};
+    memcpy(d.params, p, sizeof(p));
+}
+
+/** obj_flag::start_extra (object.cc:455-469). */
+void obj_flag::start(fluid_2d &f) {
+    std::vector<char> fn(strlen(filename) + 16);
+    snprintf(fn.data(), fn.size(), "%s.odr/track.dat", filename);
+    fp = open_or_die(fn.data(), "wb");
+    printf("# Anchoring K_stiff       : %g (1/T^2)\n", 0.01 / (f.dt_reg * f.dt_reg));
+}
+
+/** obj_track::file_output (object.cc:344-351): time and the corrected
+ * positions of the tracked points. */
+void obj_flag::track_record(const double *rec) {
+    std::vector<double> out(1 + 2 * static_cast<size_t>(ntrace));
+    out[0] = rec[0];
+    for (int k = 0; k < ntrace; k++) {
+        out[1 + 2 * k] = rec[1 + 4 * k + 2];
+        out[2 + 2 * k] = rec[1 + 4 * k + 3];
+    }
+    fwrite(out.data(), sizeof(double), out.size(), fp);
+}
+
+void obj_flag::write(int k, double time) {
+    if (fp != nullptr) fflush(fp);
+}
+
 void obj_circle::describe(incrmt_object_desc &d) const {
     d.type = INCRMT_OBJ_CIRCLE;
     const double p[8] = {cx, cy, cr, uu, vv, omega, grav, 0};
@@ -106,7 +140,10 @@ fluid_2d::~fluid_2d() {
 void fluid_2d::create() {
     if (created) return;
     incrmt_grid g = {m, n, ax, bx, ay, by, x_prd, y_prd};
-    incrmt_phys p = {visc, rhof, tw, pinw, sim_t.w_scale, sim_t.w_force, ntrace, zpr ? 1 : 0, precision, 1e-9};
+    const double U = sim_t.flow_speed();
+    if (U != 0) zpr = true;  // sim_horiz_flow::start (sim_type.cc:59-64)
+    incrmt_phys p = {visc, rhof, tw, pinw, sim_t.w_scale, sim_t.w_force, ntrace, zpr ? 1 : 0, precision, 1e-9,
+                     U != 0 ? 1 : 0, U};
     incrmt_check(incrmt_create(&g, &p, &h), "incrmt_create");
     created = true;
 }
@@ -232,10 +269,16 @@ void fluid_2d::drain_track_records() {
     int count = 0;
     incrmt_check(incrmt_track_records(h, nullptr, 0, &count, 0), "incrmt_track_records");
     if (count == 0) return;
-    dbuf.resize(5 * static_cast<size_t>(count));
+    object *trk = nullptr;
+    for (object *o : olist)
+        if (o->tracks()) { trk = o; break; }
+    int ntr = 0;
+    incrmt_check(incrmt_get_object_tracers(h, nullptr, &ntr), "incrmt_get_object_tracers");
+    const size_t rec = 1 + 4 * static_cast<size_t>(ntr);
+    dbuf.resize(rec * count);
     incrmt_check(incrmt_track_records(h, dbuf.data(), count, &count, 1), "incrmt_track_records");
-    for (int r = 0; r < count; r++)
-        for (object *o : olist) o->track_record(dbuf.data() + 5 * r);
+    if (trk != nullptr)
+        for (int r = 0; r < count; r++) trk->track_record(dbuf.data() + rec * r);
 }
 
 /** fluid_2d::write_files (fluid_2d_io.cc:60-110). */

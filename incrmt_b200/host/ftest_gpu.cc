@@ -6,13 +6,19 @@
  *             [-d <duration>] [-n <frames>] [-mixed]
  *   ftest_gpu circles <grid resolution> <count> <seed>
  *             [-d <duration>] [-n <frames>] [-mixed]
+ *   ftest_gpu flag <mu> <k_B> <Re> <ar> [<perturb_v>]
+ *             [-grid <n>] [-d <duration>] [-n <frames>] [-mixed]
  *
  * simple-spin is the reference's three-pronged rotor scenario: output in
  * sspin_<m>.odr (or sspin_<m>_tw<tw>.odr), 240 frames over 4 pi. circles
  * drops <count> seeded non-overlapping circles (radii 0.03-0.06, densities
  * 1.5-3, G 1) under gravity in a walled [-0.75,0.75]x[-1.5,1.5] box of
  * m x 2m cells (the geometry of the reference's sediment driver,
- * sediment.cc:22,124), output in circles_<m>_<count>.odr.
+ * sediment.cc:22,124), output in circles_<m>_<count>.odr. flag is the
+ * reference's flapping flag in a uniform inflow (ftest.cc:335-378): mass
+ * ratio, bending rigidity, Reynolds number, aspect ratio and an optional tip
+ * velocity perturbation, on 3n x n cells of [-1,5]x[-1,1] (n = 608 unless
+ * -grid is given), output in fl_<mu>_<k_B>_<Re>_<ar>[_<perturb_v>].odr.
  * -d and -n shorten a run; -mixed runs the projections' V-cycles in FP32
  * inside FP64 defect correction. */
 #include <cmath>
@@ -39,10 +45,11 @@ void check_grid(int m) {
 }
 
 void usage() {
-    fputs("Syntax: ./ftest_gpu <sim_type> {extra options} [-d <duration>] [-n <frames>] [-mixed]\n\n"
+    fputs("Syntax: ./ftest_gpu <sim_type> {extra options} [-d <duration>] [-n <frames>] [-grid <n>] [-mixed]\n\n"
           "Simulation types:\n"
           "simple-spin     simple three-pronged rotor: <grid resolution> [<transition width>]\n"
-          "circles         seeded circles settling under gravity: <grid resolution> <count> <seed>\n",
+          "circles         seeded circles settling under gravity: <grid resolution> <count> <seed>\n"
+          "flag            flapping flag: <mu> <k_B> <Re> <ar> [<perturb_v>]\n",
           stderr);
     exit(1);
 }
@@ -54,16 +61,18 @@ int main(int argc, char **argv) {
 
     // Trailing options of this driver
     double T_opt = -1;
-    int frames_opt = -1;
+    int frames_opt = -1, grid_opt = -1;
     bool mixed = false;
     std::vector<char *> pos;
     for (int k = 1; k < argc; k++) {
         if (se(argv[k], "-d") && k + 1 < argc) T_opt = atof(argv[++k]);
         else if (se(argv[k], "-n") && k + 1 < argc) frames_opt = atoi(argv[++k]);
+        else if (se(argv[k], "-grid") && k + 1 < argc) grid_opt = atoi(argv[++k]);
         else if (se(argv[k], "-mixed")) mixed = true;
         else pos.push_back(argv[k]);
     }
     const int np = static_cast<int>(pos.size());
+    if (np == 0) usage();
 
     // Defaults of the reference driver (ftest.cc:70-99)
     int m = 200, n = 200;
@@ -130,6 +139,31 @@ int main(int argc, char **argv) {
             mats.emplace_back(1.0, rs, ev_trans_mult, true);
         }
         sim_t = new sim_type(-lx, lx, -ly, ly, false, false);
+    } else if (se(pos[0], "flag")) {
+        if (np < 5 || np > 6) {
+            fprintf(stderr, "Selected option requires 4 or 5 arguments (%d supplied)\n", np - 1);
+            return 1;
+        }
+        const double mu = atof(pos[1]), k_B = atof(pos[2]), Re = atof(pos[3]), ar = atof(pos[4]),
+                     perturb_v = np == 6 ? atof(pos[5]) : 0;
+        n = grid_opt > 0 ? grid_opt : 608;
+        m = 3 * n;
+        const double flag_L = 1, flag_w = 1. / ar, U = 1, flag_a = flag_w * 0.25;
+        const int flag_ntrace = 17;
+        fn = std::string("fl_") + pos[1] + "_" + pos[2] + "_" + pos[3] + "_" + pos[4];
+        if (np == 6) fn += std::string("_") + pos[5];
+        sim_t = new sim_horiz_flow(U, -1, 5, -1, 1);
+        obj.push_back(new obj_flag(0, 0, flag_L, flag_w, flag_a, perturb_v, flag_ntrace, strdup(fn.c_str())));
+        rhof = 1;
+        rhos = mu * rhof * flag_L / flag_w;
+        visc = U * flag_L * rhof / Re;
+        if (np == 6) { T = 160; num_frames = 80; } else { T = 30; num_frames = 900; }
+        G = 4 * k_B / (flag_w * flag_w * flag_w);
+        mats.emplace_back(G, rhos, ev_trans_mult, true);
+        printf("# Shear modulus                : %g (M/LT^2)\n"
+               "# Flag width                   : %g dy\n"
+               "# Solid density                : %g\n#\n",
+               G, 0.5 * flag_w * n, rhos);
     } else {
         fprintf(stderr, "Simulation type '%s' not recognized\n", pos[0]);
         return 1;

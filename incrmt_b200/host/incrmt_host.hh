@@ -38,6 +38,17 @@ struct sim_type {
              double w_force_)
         : ax(ax_), bx(bx_), ay(ay_), by(by_), w_scale(w_scale_), w_force(w_force_), x_prd(x_prd_), y_prd(y_prd_) {}
     virtual ~sim_type() {}
+    /** Horizontal inflow speed of sim_horiz_flow, or 0. */
+    virtual double flow_speed() const { return 0; }
+};
+
+/** Uniform flow entering through the left edge of a y-periodic channel with
+ * zero pressure on the right edge (sim_horiz_flow, sim_type.hh:117-141). */
+struct sim_horiz_flow : public sim_type {
+    const double U;
+    sim_horiz_flow(double U_, double ax_, double bx_, double ay_, double by_)
+        : sim_type(ax_, bx_, ay_, by_, false, true), U(U_) {}
+    double flow_speed() const override { return U; }
 };
 
 /** Material constants of a solid (obj_field.hh:15-29). */
@@ -56,8 +67,11 @@ struct object {
     /** Called by fluid_2d::initialize after the time step is chosen
      * (object::start, fluid_2d.cc:114-115). */
     virtual void start(fluid_2d &f) {}
-    /** Called with each tracked-point record the library collected
-     * (time, position before and after its correction). */
+    /** Whether the object tracks points (obj_track); the library tracks the
+     * points of the first such object. */
+    virtual bool tracks() const { return false; }
+    /** Called with each tracked-point record the library collected: the
+     * time, then per point its position before and after the correction. */
     virtual void track_record(const double *rec) {}
     /** Flushes per-object output at a frame (object::write, fluid_2d_io.cc:107). */
     virtual void write(int k, double time) {}
@@ -80,6 +94,28 @@ struct obj_simple_spin : public object {
     ~obj_simple_spin();
     void describe(incrmt_object_desc &d) const override;
     void start(fluid_2d &f) override;
+    bool tracks() const override { return true; }
+    void track_record(const double *rec) override;
+    void write(int k, double time) override;
+};
+
+/** Flag of length flag_l and width flag_w anchored around (cx, cy), tracking
+ * ntrace points along its length (obj_flag, object.hh:471-505). Writes
+ * <filename>.odr/track.dat: records of 1+2*ntrace doubles (time, then each
+ * point's corrected position; obj_track::file_output, object.cc:344-351). */
+struct obj_flag : public object {
+    const double cx, cy, flag_l, flag_w, flag_a, perturb_v;
+    const int ntrace;
+    const char *filename;
+    FILE *fp;
+    obj_flag(double cx_, double cy_, double flag_l_, double flag_w_, double flag_a_, double perturb_v_,
+             int ntrace_, const char *filename_)
+        : cx(cx_), cy(cy_), flag_l(flag_l_), flag_w(flag_w_), flag_a(flag_a_), perturb_v(perturb_v_),
+          ntrace(ntrace_), filename(filename_), fp(nullptr) {}
+    ~obj_flag();
+    void describe(incrmt_object_desc &d) const override;
+    void start(fluid_2d &f) override;
+    bool tracks() const override { return true; }
     void track_record(const double *rec) override;
     void write(int k, double time) override;
 };

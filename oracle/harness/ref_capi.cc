@@ -42,6 +42,22 @@ struct ref_sim {
     char *fa;
 };
 
+/** fluid_2d::update_velocity copies nX,nY into X,Y at every grid point
+ * (fluid_2d.cc:1368-1373, s_field::set_full_timestep), but nX,nY are only
+ * ever computed inside the band (update_reference_map, extrapolate), and the
+ * s_field arrays are never initialised (obj_field.cc). Outside the band X,Y
+ * therefore take whatever the heap held, which depends on earlier
+ * allocations in the process. The harness fills nX,nY with zeros once after
+ * initialisation, the contents a fresh allocation has, so that the oracle is
+ * deterministic; inside the band nothing changes. */
+void zero_unset_refmap(fluid_2d &f) {
+    const int mem=f.ml*f.nl;
+    for(int k=0;k<f.n_obj;k++) {
+        s_field *sp=f.olist[k]->sbase;
+        for(int ij=0;ij<mem;ij++) sp[ij].nX=sp[ij].nY=0;
+    }
+}
+
 /** Builds the ftest "simple-spin" scenario (ftest.cc:116-143, 383-400) at
  * an m x m grid, with the output directory <base>.odr. */
 ref_sim* make_sspin(int m,int ntrace,const char *base) {
@@ -65,16 +81,21 @@ ref_sim* make_sspin(int m,int ntrace,const char *base) {
     mat_const mc(G,rhos,1,true);
     for(unsigned int k=0;k<r->obj.size();k++) r->f->add_object(r->obj[k],mc);
     r->f->initialize(0.8,0.4,0.8);
+    zero_unset_refmap(*r->f);
     return r;
 }
 
 /** A walled (or periodic) domain with any number of circles (type 1:
- * obj_circle(cx,cy,cr,uu,vv,omega,grav), object.hh:128-138) and rounded rods
- * (type 2: obj_rounded_rod(cx,cy,cr,cl,grav), object.hh:229-230); mats holds
- * G and rhos per object. Output directory <base>.odr. */
+ * obj_circle(cx,cy,cr,uu,vv,omega,grav), object.hh:128-138), rounded rods
+ * (type 2: obj_rounded_rod(cx,cy,cr,cl,grav), object.hh:229-230) and flags
+ * (type 3: obj_flag(cx,cy,flag_l,flag_w,flag_a,perturb_v,ntrace),
+ * object.hh:487-488); mats holds G and rhos per object. flow_u > 0 selects
+ * sim_horiz_flow(flow_u, geom) (sim_type.hh:125-126; y-periodic, inflow at the
+ * left, zero pressure at the right) instead of sim_type(geom, x_prd, y_prd).
+ * Output directory <base>.odr. */
 ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double visc,double rhof,
                     int ntrace,int nobj,const int *types,const double *params,const double *mats,
-                    const char *base) {
+                    const char *base,double flow_u) {
     ref_sim *r=new ref_sim;
     r->fa=new char[strlen(base)+1];
     strcpy(r->fa,base);
@@ -86,15 +107,18 @@ ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double vi
     for(int k=0;k<nobj;k++) {
         const double *p=params+8*k;
         if(types[k]==1) r->obj.push_back(new obj_circle(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
-        else r->obj.push_back(new obj_rounded_rod(p[0],p[1],p[2],p[3],p[4]));
+        else if(types[k]==2) r->obj.push_back(new obj_rounded_rod(p[0],p[1],p[2],p[3],p[4]));
+        else r->obj.push_back(new obj_flag(p[0],p[1],p[2],p[3],p[4],p[5],static_cast<int>(p[6]),r->fa));
     }
-    r->st=new sim_type(geom[0],geom[1],geom[2],geom[3],x_prd!=0,y_prd!=0);
+    if(flow_u>0) r->st=new sim_horiz_flow(flow_u,geom[0],geom[1],geom[2],geom[3]);
+    else r->st=new sim_type(geom[0],geom[1],geom[2],geom[3],x_prd!=0,y_prd!=0);
     r->f=new fluid_2d(m,n,*r->st,visc,rhof,tw,pinw,ntrace,fflags,r->fout);
     for(int k=0;k<nobj;k++) {
         mat_const mc(mats[2*k],mats[2*k+1],1,true);
         r->f->add_object(r->obj[k],mc);
     }
     r->f->initialize(0.8,0.4,0.8);
+    zero_unset_refmap(*r->f);
     return r;
 }
 
@@ -121,8 +145,8 @@ void* ref_sspin_create(int m,int ntrace,const char *base) {
 
 void* ref_multi_create(int m,int n,const double *geom,int x_prd,int y_prd,double visc,double rhof,
                        int ntrace,int nobj,const int *types,const double *params,const double *mats,
-                       const char *base) {
-    return make_multi(m,n,geom,x_prd,y_prd,visc,rhof,ntrace,nobj,types,params,mats,base);
+                       const char *base,double flow_u) {
+    return make_multi(m,n,geom,x_prd,y_prd,visc,rhof,ntrace,nobj,types,params,mats,base,flow_u);
 }
 
 void ref_destroy(void *h) {

@@ -60,7 +60,7 @@ def lib():
     L.ref_sspin_create.argtypes = [I, I, ctypes.c_char_p]
     L.ref_sspin_create.restype = P
     L.ref_destroy.argtypes = [P]
-    L.ref_multi_create.argtypes = [I, I, dp, I, I, D, D, I, I, ip, dp, dp, ctypes.c_char_p]
+    L.ref_multi_create.argtypes = [I, I, dp, I, I, D, D, I, I, ip, dp, dp, ctypes.c_char_p, D]
     L.ref_multi_create.restype = P
     L.ref_dims.argtypes = [P, ip]
     L.ref_scalars.argtypes = [P, dp]
@@ -115,11 +115,13 @@ class RefSim:
     """A reference fluid_2d simulation: the simple-spin scenario, or with
     `objects` a domain of circles and rounded rods.
 
-    objects: list of ("circle", (cx, cy, cr, uu, vv, omega, grav), G, rhos) or
-    ("rod", (cx, cy, cr, cl, grav), G, rhos); geom = (ax, bx, ay, by)."""
+    objects: list of ("circle", (cx, cy, cr, uu, vv, omega, grav), G, rhos),
+    ("rod", (cx, cy, cr, cl, grav), G, rhos) or ("flag", (cx, cy, flag_l,
+    flag_w, flag_a, perturb_v, ntrace), G, rhos); geom = (ax, bx, ay, by);
+    flow_u > 0 makes the domain sim_horiz_flow (y-periodic with inflow)."""
 
     def __init__(self, m, ntrace=512, workdir=None, n=None, objects=None, geom=(-1., 1., -1., 1.),
-                 visc=1e-2, rhof=1.0, periodic=(False, False)):
+                 visc=1e-2, rhof=1.0, periodic=(False, False), flow_u=0.0):
         self._tmp = None
         if workdir is None:
             self._tmp = tempfile.TemporaryDirectory()
@@ -130,7 +132,7 @@ class RefSim:
         else:
             n = m if n is None else n
             k = len(objects)
-            types = (ctypes.c_int * k)(*[1 if o[0] == "circle" else 2 for o in objects])
+            types = (ctypes.c_int * k)(*[{"circle": 1, "rod": 2, "flag": 3}[o[0]] for o in objects])
             params = np.zeros((k, 8))
             mats = np.zeros((k, 2))
             for q, (kind, p, G, rhos) in enumerate(objects):
@@ -139,7 +141,7 @@ class RefSim:
             g = np.array(geom, dtype=np.float64)
             base = os.path.join(workdir, f"multi_{m}").encode()
             self.h = lib().ref_multi_create(m, n, _dp(g), int(periodic[0]), int(periodic[1]), visc, rhof,
-                                            ntrace, k, types, _dp(params), _dp(mats), base)
+                                            ntrace, k, types, _dp(params), _dp(mats), base, float(flow_u))
         d = (ctypes.c_int * 7)()
         lib().ref_dims(self.h, d)
         self.m, self.n, self.ml, self.nl, self.n_obj, self.m_fem, self.n_fem = list(d)

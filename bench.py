@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload sspin1024|mac4096|sed1024|flag2048] [--precision fp64|mixed]
+                    [--learned]
 
 Workload "sspin1024" (default): the ftest simple-spin scenario (three-pronged
 neo-Hookean rotor in a walled [-1,1]^2 box, ftest.cc:116-143) on a 1024 x 1024
@@ -32,6 +33,12 @@ Workload "flag2048": the flag scenario (ftest.cc:335-378; y-periodic channel,
 uniform inflow, zero-pressure outlet, FEM projection with its fixed column) on
 3456 x 1152 square cells of [-1,5]x[-1,1] (about 2048^2 cells), mass ratio 1,
 bending rigidity 0.1, Re 100, aspect ratio 10.
+
+--learned (mac4096): before timing, the learned initial guess is trained on
+128 GPU-generated problems of the same kind (other seeds) with the library's
+own U-Net kernels; every timed solve then starts from the network's guess
+instead of zero. The line adds the training summary and plain FP64 solves of
+the same problem for comparison.
 
 Multi-GPU: the path does not shard; N ranks run N independent replicas
 (weak scaling), timed on the device as the maximum over ranks.
@@ -497,6 +504,54 @@ def run_ours_sspin(args, ws, rank, local, dist):
     sim.close()
 
 
+LEARNED_FACTOR = 8      # the network runs on the 4096^2 solve restricted to 512^2
+LEARNED_SAMPLES = 128   # training problems (seeds disjoint from the benchmarked one)
+LEARNED_STEPS = 1500
+
+
+def _train_learned_mac(s, m, dev, rank):
+    """Trains the learned initial guess on GPU-generated 4096^2 MAC problems
+    with this library's own U-Net kernels: inputs from incrmt_mg_learned_input
+    (zero start), targets the FP64 multigrid solutions restricted by block
+    averages and normalised. Returns the network and a summary."""
+    import torch
+    from incrmt_b200 import capi, workloads
+    t0 = time.perf_counter()
+    H, W = capi.learned_grid(m, m, LEARNED_FACTOR)
+    X = torch.empty(LEARNED_SAMPLES, H, W, 3, dtype=torch.float32, device=dev)
+    T = torch.empty(LEARNED_SAMPLES, H, W, dtype=torch.float32, device=dev)
+    z = torch.zeros(m * m, dtype=torch.float64, device=dev)
+    z0 = torch.zeros(m * m, dtype=torch.float64, device=dev)
+    for k in range(LEARNED_SAMPLES):
+        rho, b = workloads.standalone_mac_problem(m, seed=1000 + 97 * rank + k, device=dev)
+        rho, b = rho.contiguous(), b.contiguous().view(-1)
+        z.zero_()
+        torch.cuda.synchronize()
+        s.set_density_device(rho.data_ptr())
+        s.solve_device(b.data_ptr(), z.data_ptr())
+        capi.learned_input(s, b.data_ptr(), z0.data_ptr(), LEARNED_FACTOR, X[k].data_ptr())
+        zt = torch.nn.functional.avg_pool2d(z.view(1, 1, m, m).float(), LEARNED_FACTOR)[0, 0]
+        T[k] = (zt - zt.mean()) / zt.std()
+    t_data = time.perf_counter() - t0
+    V = torch.ones(8, H, W, dtype=torch.float32, device=dev)
+    net = capi.UNet(4, 16, seed=11)
+    g = torch.Generator(device="cpu").manual_seed(rank)
+    t1 = time.perf_counter()
+    loss = None
+    for it in range(LEARNED_STEPS):
+        idx = torch.randperm(LEARNED_SAMPLES, generator=g)[:8]
+        xb, tb = X[idx].contiguous(), T[idx].contiguous()
+        loss = net.train_step(8, H, W, xb.data_ptr(), tb.data_ptr(), V.data_ptr(),
+                              2e-3 if it < 0.75 * LEARNED_STEPS else 5e-4)
+    torch.cuda.synchronize()
+    info = {"network": f"U-Net, 4 levels, base 16 channels, {net.num_params()} parameters, BF16 activations, "
+                       f"mma.sync tensor-core convolutions",
+            "grid": f"{H}x{W} (solve restricted by {LEARNED_FACTOR})", "train_samples": LEARNED_SAMPLES,
+            "train_steps": LEARNED_STEPS, "batch": 8, "final_loss": loss,
+            "data_seconds": t_data, "train_seconds": time.perf_counter() - t1}
+    return net, info
+
+
 def run_ours(args, ws, rank, local, dist):
     import torch
     from incrmt_b200 import capi, workloads
@@ -514,11 +569,45 @@ def run_ours(args, ws, rank, local, dist):
     s = capi.MGSolver(capi.SYS_MAC, m, m)
     ext = torch.cuda.ExternalStream(s.stream(), device=dev)
     torch.cuda.synchronize()
+    net, learned_info = None, None
+    if args.learned:
+        net, learned_info = _train_learned_mac(s, m, dev, rank)
+        # Plain FP64 solves of the same problem, for the comparison line.
+        vc_plain, t_plain = [], []
+        for _ in range(5):
+            s.set_density_device(rho.data_ptr())
+            with torch.cuda.stream(ext):
+                z.zero_()
+            st = s.solve_device(b.data_ptr(), z.data_ptr(), precision=capi.PREC_FP64)
+            vc_plain.append(st.vcycles)
+        zstar = z.clone()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(5):
+            s.set_density_device(rho.data_ptr())
+            with torch.cuda.stream(ext):
+                z.zero_()
+            s.solve_device(b.data_ptr(), z.data_ptr(), precision=capi.PREC_FP64)
+        e1.record(ext)
+        torch.cuda.synchronize()
+        learned_info["plain_fp64"] = {"value": 5 / (e0.elapsed_time(e1) / 1e3), "unit": "steps/s",
+                                      "vcycles_per_projection": float(np.mean(vc_plain))}
+        with torch.cuda.stream(ext):
+            z.zero_()
+        torch.cuda.synchronize()
+        st = capi.learned_guess(s, net, b.data_ptr(), z.data_ptr(), LEARNED_FACTOR)
+        dz, ds = z - z.mean(), zstar - zstar.mean()
+        learned_info["guess_relative_error"] = float((dz - ds).norm() / ds.norm())
+        learned_info["guess_alpha"] = st.alpha
 
     def step():
         s.set_density_device(rho.data_ptr())
         with torch.cuda.stream(ext):
             z.zero_()
+        if net is not None:
+            capi.learned_guess(s, net, b.data_ptr(), z.data_ptr(), LEARNED_FACTOR, stats=False)
         st = s.solve_device(b.data_ptr(), z.data_ptr(), precision=prec)
         return st.vcycles
 
@@ -555,22 +644,41 @@ def run_ours(args, ws, rank, local, dist):
     b_h = b.cpu().pin_memory()
     z_h = torch.zeros_like(b_h).pin_memory()
     rho_np, b_np, z_np = rho_h.numpy(), b_h.numpy(), z_h.numpy()
+
+    def e2e_step():
+        if net is None:
+            s.set_density(rho_np)
+            z_np[:] = 0
+            s.solve(b_np, z_np, precision=prec)
+            return
+        # With the learned guess: host buffers in on the solver's stream, the
+        # guess and the solve on the device, the solution back to the host.
+        with torch.cuda.stream(ext):
+            rho.copy_(rho_h, non_blocking=True)
+            b.copy_(b_h, non_blocking=True)
+            z.zero_()
+        s.set_density_device(rho.data_ptr())
+        capi.learned_guess(s, net, b.data_ptr(), z.data_ptr(), LEARNED_FACTOR, stats=False)
+        s.solve_device(b.data_ptr(), z.data_ptr(), precision=prec)
+        with torch.cuda.stream(ext):
+            z_h.copy_(z, non_blocking=True)
+        ext.synchronize()
+
     for _ in range(min(args.warmup, 1)):
-        s.set_density(rho_np)
-        z_np[:] = 0
-        s.solve(b_np, z_np, precision=prec)
+        e2e_step()
     _barrier(dist)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        s.set_density(rho_np)
-        z_np[:] = 0
-        s.solve(b_np, z_np, precision=prec)
+        e2e_step()
     e2e_s = time.perf_counter() - t0
     e2e_s = _max_over_ranks(dist, e2e_s)
     e2e = ws * args.steps / e2e_s
 
     if rank != 0:
+        if net is not None:
+            net.close()
+        s.close()
         return
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
@@ -589,8 +697,10 @@ def run_ours(args, ws, rank, local, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == capi.PREC_FP64 else "f32 V-cycles in f64 defect correction",
         "data": "synthetic",
+        "learned": learned_info,
         "config": {"workload": f"standalone MAC solve {m}x{m} (8 circles rho 3, 64 blobs), "
-                               f"setup + V-cycles to 1e-9 from zero", "precision": args.precision,
+                               f"setup + V-cycles to 1e-9 from " +
+                               ("the learned guess" if args.learned else "zero"), "precision": args.precision,
                    "flush": "inputs larger than L2 (each array 134 MB)", "parallelism": f"replicas x{ws}"},
         "vcycles_per_projection": float(np.mean(vcs)),
         "roofline": _roofline("mac4096_smooth", kms, kbytes, klaunch,
@@ -598,12 +708,14 @@ def run_ours(args, ws, rank, local, dist):
                               "updated unknowns x 2 sweeps x (3+c) x 8 B, c=2 (MAC)"),
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "steps/s",
-                "h2d_bytes_per_step": int(rho_h.numel() * 8 + 2 * b_h.numel() * 8),
+                "h2d_bytes_per_step": int(rho_h.numel() * 8 + (1 if net is not None else 2) * b_h.numel() * 8),
                 "d2h_bytes_per_step": int(b_h.numel() * 8)},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
     print(json.dumps(line))
+    if net is not None:
+        net.close()
     s.close()
 
 
@@ -616,6 +728,8 @@ def main():
     ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096", "sed1024", "flag2048"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learned", action="store_true",
+                    help="mac4096: train the learned initial guess first and start every solve from it")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.impl == "reference":

@@ -1,0 +1,92 @@
+/* C ABI of the learned initial guess for the pressure solves: a BF16
+ * convolutional U-Net trained on the GPU by this library's own kernels.
+ *
+ * It has no counterpart in the reference, whose projections start from the
+ * previous solution (mgs_common.cc:15-21). The network maps three channels on
+ * a grid restricted from the solve grid -- the residual b - A z0 normalised by
+ * its RMS, the reciprocal density, and a zero channel -- to a field d; the
+ * solver then uses z0 + alpha d with alpha = (d . r0) / (d . A d), the step
+ * that minimises the error along d in the energy norm of the (definite)
+ * system, the norm that weighs the smooth error multigrid removes slowest.
+ *
+ * Layout: activations NHWC (channel fastest) in BF16 with FP32 accumulation;
+ * master weights FP32 with BF16 copies; Adam in FP32. Images are processed at
+ * H x W with H, W multiples of 16 (inputs are zero-padded by the caller).
+ * All functions return INCRMT_OK (0) or a negative INCRMT_ERR_* code. */
+#ifndef INCRMT_UNET_H
+#define INCRMT_UNET_H
+
+#include <stddef.h>
+#include "incrmt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct incrmt_unet incrmt_unet;
+
+/** Creates a U-Net with `levels` resolutions (2..5) and `base` channels at the
+ * finest (a multiple of 16; doubled per level), 3 input channels and one
+ * output, weights initialised from `seed` (He-uniform, zero biases). */
+int incrmt_unet_create(int levels, int base, unsigned long long seed, incrmt_unet **out);
+
+/** Number of FP32 parameters (all weights and biases). */
+long long incrmt_unet_num_params(const incrmt_unet *h);
+
+/** Copies the FP32 parameters out of / into the network (host arrays of
+ * incrmt_unet_num_params floats, the layer order of the forward pass; each
+ * convolution's weights as [tap][in][out], then its biases). */
+int incrmt_unet_get_params(incrmt_unet *h, float *host);
+int incrmt_unet_set_params(incrmt_unet *h, const float *host);
+
+/** Forward pass on device arrays: `in` is batch x H x W x 3 FP32 (NHWC),
+ * `out` batch x H x W FP32; work on `stream` (0 = default), not waited for. */
+int incrmt_unet_forward(incrmt_unet *h, int batch, int H, int W, const float *d_in, float *d_out, void *stream);
+
+/** One training step on device arrays: forward, loss = mean over the
+ * `valid` mask (batch x H x W FP32, 1 inside the image, 0 in padding) of
+ * (out - target)^2, backward, Adam (lr, beta1 0.9, beta2 0.999, eps 1e-8).
+ * The loss before the update is written to *loss (synchronises the stream). */
+int incrmt_unet_train_step(incrmt_unet *h, int batch, int H, int W, const float *d_in, const float *d_target,
+                           const float *d_valid, float lr, float *loss, void *stream);
+
+/** Gradient check support: forward + backward without the update; the
+ * FP32 parameter gradients (incrmt_unet_num_params floats) go to `host_grad`
+ * and the loss to *loss. */
+int incrmt_unet_gradients(incrmt_unet *h, int batch, int H, int W, const float *d_in, const float *d_target,
+                          const float *d_valid, float *loss, float *host_grad, void *stream);
+
+/** Result of a learned guess: the residual 2-norms before and after (the
+ * energy-optimal step may raise the residual while lowering the smooth
+ * error), the scale alpha, and whether the guess was applied (alpha > 0). */
+typedef struct incrmt_learned_stats {
+    double res_before, res_after, alpha;
+    int used;
+} incrmt_learned_stats;
+
+/** Learned initial guess of the MAC solve of `h` (a non-periodic MAC solver
+ * whose density is set): from the iterate d_z, forms r0 = b - A z, runs the
+ * network on the r0 and 1/rho features restricted by `factor` (block
+ * averages; the network grid is ceil(m/factor) x ceil(n/factor) rounded up to
+ * multiples of 16), prolongs the output d bilinearly and sets
+ * z += alpha d with alpha = (d . r0) / (d . A d) (unchanged if alpha <= 0). Runs on the solver's stream; synchronises only when st is
+ * given. No counterpart in the reference (it starts from the previous
+ * solution, mgs_common.cc:15-21). */
+int incrmt_mg_learned_guess(incrmt_mg *h, incrmt_unet *net, const double *d_b, double *d_z, int factor,
+                            incrmt_learned_stats *st);
+
+/** The network input the guess would use (for training data): 3 x H x W
+ * floats (NHWC) into d_in, H x W the network grid of `factor`. */
+int incrmt_mg_learned_input(incrmt_mg *h, const double *d_b, const double *d_z, int factor, float *d_in, int H,
+                            int W);
+
+/** Kernel launches issued by this network so far. */
+long long incrmt_unet_launches(const incrmt_unet *h);
+
+void incrmt_unet_destroy(incrmt_unet *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libincrmt_gpu.so")
-SOURCES = ["capi.cu", "mg.cu", "sim.cu", "noalloc.cu"]
+SOURCES = ["capi.cu", "mg.cu", "sim.cu", "noalloc.cu", "unet.cu", "learned.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

@@ -460,3 +460,119 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Learned initial guess (include/incrmt_unet.h).
+
+class LearnedStats(ctypes.Structure):
+    _fields_ = [("res_before", ctypes.c_double), ("res_after", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("used", ctypes.c_int)]
+
+
+def _unet_sigs(L):
+    P, I, D, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.incrmt_unet_create.argtypes = [I, I, ctypes.c_ulonglong, ctypes.POINTER(P)]
+    L.incrmt_unet_num_params.argtypes = [P]
+    L.incrmt_unet_num_params.restype = ctypes.c_longlong
+    L.incrmt_unet_get_params.argtypes = [P, fp]
+    L.incrmt_unet_set_params.argtypes = [P, fp]
+    L.incrmt_unet_forward.argtypes = [P, I, I, I, P, P, P]
+    L.incrmt_unet_train_step.argtypes = [P, I, I, I, P, P, P, F, fp, P]
+    L.incrmt_unet_gradients.argtypes = [P, I, I, I, P, P, P, fp, fp, P]
+    L.incrmt_unet_launches.argtypes = [P]
+    L.incrmt_unet_launches.restype = ctypes.c_longlong
+    L.incrmt_unet_destroy.argtypes = [P]
+    L.incrmt_unet_destroy.restype = None
+    L.incrmt_mg_learned_guess.argtypes = [P, P, P, P, I, ctypes.POINTER(LearnedStats)]
+    L.incrmt_mg_learned_input.argtypes = [P, P, P, I, P, I, I]
+
+
+def _ulib():
+    L = lib()
+    if not hasattr(L, "_unet_ready"):
+        _unet_sigs(L)
+        L._unet_ready = True
+    return L
+
+
+def learned_grid(m, n, factor):
+    """Network grid (H, W) of an m x n solve restricted by `factor`."""
+    return ((n + factor - 1) // factor + 15) // 16 * 16, ((m + factor - 1) // factor + 15) // 16 * 16
+
+
+class UNet:
+    """The BF16 U-Net of the learned initial guess (include/incrmt_unet.h).
+    Device arrays are passed as integer pointers (e.g. torch data_ptr())."""
+
+    def __init__(self, levels=4, base=16, seed=1):
+        h = ctypes.c_void_p()
+        check(_ulib().incrmt_unet_create(levels, base, seed, ctypes.byref(h)))
+        self._h = h
+        self.levels, self.base = levels, base
+
+    @property
+    def handle(self):
+        return self._h
+
+    def num_params(self):
+        return int(_ulib().incrmt_unet_num_params(self._h))
+
+    def get_params(self):
+        out = np.empty(self.num_params(), dtype=np.float32)
+        check(_ulib().incrmt_unet_get_params(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(_ulib().incrmt_unet_set_params(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def forward(self, batch, H, W, in_ptr, out_ptr, stream=0):
+        check(_ulib().incrmt_unet_forward(self._h, batch, H, W, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
+                                          ctypes.c_void_p(stream)))
+
+    def train_step(self, batch, H, W, in_ptr, target_ptr, valid_ptr, lr, stream=0):
+        loss = ctypes.c_float()
+        check(_ulib().incrmt_unet_train_step(self._h, batch, H, W, ctypes.c_void_p(in_ptr), ctypes.c_void_p(target_ptr),
+                                             ctypes.c_void_p(valid_ptr), lr, ctypes.byref(loss), ctypes.c_void_p(stream)))
+        return loss.value
+
+    def gradients(self, batch, H, W, in_ptr, target_ptr, valid_ptr, stream=0):
+        g = np.empty(self.num_params(), dtype=np.float32)
+        loss = ctypes.c_float()
+        check(_ulib().incrmt_unet_gradients(self._h, batch, H, W, ctypes.c_void_p(in_ptr), ctypes.c_void_p(target_ptr),
+                                            ctypes.c_void_p(valid_ptr), ctypes.byref(loss),
+                                            g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.c_void_p(stream)))
+        return loss.value, g
+
+    def launches(self):
+        return int(_ulib().incrmt_unet_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _ulib().incrmt_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def learned_guess(solver, net, b_ptr, z_ptr, factor=1, stats=True):
+    """z += alpha d from the network (incrmt_mg_learned_guess); returns the
+    LearnedStats when stats is set (that synchronises the solver's stream)."""
+    st = LearnedStats() if stats else None
+    check(_ulib().incrmt_mg_learned_guess(solver.handle, net.handle, ctypes.c_void_p(b_ptr), ctypes.c_void_p(z_ptr),
+                                          factor, ctypes.byref(st) if st is not None else None))
+    return st
+
+
+def learned_input(solver, b_ptr, z_ptr, factor, in_ptr):
+    """The network input of a guess from (b, z) (for training data)."""
+    H, W = learned_grid(solver.m_sys, solver.n_sys, factor)
+    check(_ulib().incrmt_mg_learned_input(solver.handle, ctypes.c_void_p(b_ptr), ctypes.c_void_p(z_ptr), factor,
+                                          ctypes.c_void_p(in_ptr), H, W))
+    return H, W

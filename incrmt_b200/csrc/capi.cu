@@ -7,9 +7,6 @@
 #include "common.cuh"
 #include "mg.cuh"
 
-struct incrmt_mg {
-    incrmt::Multigrid mg;
-};
 
 namespace incrmt {
 
@@ -134,6 +131,8 @@ long long incrmt_mg_launches(const incrmt_mg *h) { return h ? h->mg.launches : 0
 
 void incrmt_mg_destroy(incrmt_mg *h) {
     if (!h) return;
+    if (h->mg.stream) cudaStreamSynchronize(h->mg.stream);
+    h->learned.release();
     h->mg.destroy();
     delete h;
 }

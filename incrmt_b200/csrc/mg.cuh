@@ -96,4 +96,18 @@ private:
     int fetch_norm(double *v);
 };
 
+/** Workspace of the learned initial guess (learned.cu), per solver. */
+struct LearnedWork {
+    double *r0 = nullptr, *ad = nullptr, *dfine = nullptr, *dots = nullptr;
+    float *in = nullptr, *out = nullptr;
+    long n_fine = 0, n_net = 0;
+    void release();
+};
+
 }  // namespace incrmt
+
+/** The solver handle of the C ABI (include/incrmt.h). */
+struct incrmt_mg {
+    incrmt::Multigrid mg;
+    incrmt::LearnedWork learned;
+};

@@ -1,0 +1,790 @@
+// The learned initial guess: a BF16 U-Net whose convolutions, pooling,
+// upsampling, loss and Adam update are this library's own kernels. Tensor
+// cores do the convolutions as implicit GEMMs (mma.sync m16n8k16, BF16 in,
+// FP32 accumulate): forward and input gradient share one kernel (the input
+// gradient is the forward convolution of the output gradient with the
+// flipped, transposed weights), the weight gradient is a second GEMM over
+// the pixels. Activations are NHWC with channel counts padded to multiples
+// of 16 so that every 16-channel slice of a pixel is one 32-byte load.
+#include <cuda_bf16.h>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <random>
+#include <vector>
+#include "incrmt_unet.h"
+#include "common.cuh"
+
+namespace incrmt {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+/** Two BF16 values as one operand register, the first in the low half. */
+__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
+    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+}
+
+constexpr int kConvBM = 128;  // pixels per block of the convolution
+
+/** Y[p][co] = act(bias[co] + sum over taps and ci of X[p + off(tap)][ci] W[tap][ci][co]),
+ * zero padding at the image borders. One block = 128 pixels x BN outputs,
+ * eight warps of 16 pixels each; per K step the block stages 128 x 16 inputs
+ * and BN x 16 weights in shared memory. Cin, Cout multiples of 16. */
+template <int TAPS, int BN, bool RELU>
+__global__ void __launch_bounds__(256) k_conv_fwd(const bf16 *__restrict__ X, const bf16 *__restrict__ Wt,
+                                                  const float *__restrict__ bias, bf16 *__restrict__ Y, int B, int H,
+                                                  int Wd, int Cin, int Cout) {
+    __shared__ __align__(16) bf16 As[kConvBM * 16];  // [pixel][k]
+    __shared__ __align__(16) bf16 Bs[BN * 16];       // [n][k]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+    const long P = static_cast<long>(B) * H * Wd;
+    const long p0 = static_cast<long>(blockIdx.x) * kConvBM;
+    const int n0 = blockIdx.y * BN;
+    float acc[BN / 8][4];
+#pragma unroll
+    for (int a = 0; a < BN / 8; a++) acc[a][0] = acc[a][1] = acc[a][2] = acc[a][3] = 0.f;
+    const long pl = p0 + (tid >> 1);
+    const bool pvalid = pl < P;
+    int pb = 0, py = 0, px = 0;
+    if (pvalid) {
+        pb = static_cast<int>(pl / (static_cast<long>(H) * Wd));
+        const int r = static_cast<int>(pl - static_cast<long>(pb) * H * Wd);
+        py = r / Wd;
+        px = r - py * Wd;
+    }
+    const int ch = (tid & 1) * 8;
+    for (int tap = 0; tap < TAPS; tap++) {
+        const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
+        const int sy = py + dy, sx = px + dx;
+        const bool inb = pvalid && sy >= 0 && sy < H && sx >= 0 && sx < Wd;
+        const long xoff = inb ? ((static_cast<long>(pb) * H + sy) * Wd + sx) * Cin + ch : 0;
+        for (int c0 = 0; c0 < Cin; c0 += 16) {
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (inb) v = *reinterpret_cast<const uint4 *>(X + xoff + c0);
+            *reinterpret_cast<uint4 *>(&As[(tid >> 1) * 16 + ch]) = v;
+            for (int e = tid; e < BN * 16; e += 256) {
+                const int k = e / BN, n = e - k * BN;
+                Bs[n * 16 + k] = Wt[(static_cast<long>(tap) * Cin + c0 + k) * Cout + n0 + n];
+            }
+            __syncthreads();
+            const bf16 *ar = &As[warp * 16 * 16];
+            uint32_t a[4];
+            a[0] = *reinterpret_cast<const uint32_t *>(&ar[g * 16 + t4 * 2]);
+            a[1] = *reinterpret_cast<const uint32_t *>(&ar[(g + 8) * 16 + t4 * 2]);
+            a[2] = *reinterpret_cast<const uint32_t *>(&ar[g * 16 + t4 * 2 + 8]);
+            a[3] = *reinterpret_cast<const uint32_t *>(&ar[(g + 8) * 16 + t4 * 2 + 8]);
+#pragma unroll
+            for (int nt = 0; nt < BN / 8; nt++) {
+                const bf16 *br = &Bs[(nt * 8 + g) * 16];
+                uint32_t b[2];
+                b[0] = *reinterpret_cast<const uint32_t *>(&br[t4 * 2]);
+                b[1] = *reinterpret_cast<const uint32_t *>(&br[t4 * 2 + 8]);
+                mma_bf16_16816(acc[nt], a, b);
+            }
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int nt = 0; nt < BN / 8; nt++) {
+        const int n = n0 + nt * 8 + t4 * 2;
+        const float b0 = bias ? bias[n] : 0.f, b1 = bias ? bias[n + 1] : 0.f;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const long p = p0 + warp * 16 + g + h * 8;
+            if (p >= P) continue;
+            float v0 = acc[nt][2 * h] + b0, v1 = acc[nt][2 * h + 1] + b1;
+            if (RELU) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+            *reinterpret_cast<__nv_bfloat162 *>(&Y[p * Cout + n]) = __floats2bfloat162_rn(v0, v1);
+        }
+    }
+}
+
+constexpr int kWgPix = 2048;  // pixels per block of the weight gradient
+
+/** dW[tap][ci][co] += sum over pixels of X[p + off(tap)][ci] dY[p][co], for one
+ * tap (blockIdx.z), 16 input channels (blockIdx.y / (Cout/BN)) and BN output
+ * channels, over kWgPix pixels (blockIdx.x). Each warp walks 16-pixel steps,
+ * staging 16 x 16 inputs and 16 x BN output gradients in its own shared
+ * slice; the warps' partial sums meet in shared memory (shared atomics) and
+ * one FP32 atomic per weight leaves the block, so the sums' order, and with
+ * it the last bits of the gradient, vary from run to run. */
+template <int TAPS, int BN>
+__global__ void __launch_bounds__(256) k_conv_wgrad(const bf16 *__restrict__ X, const bf16 *__restrict__ dY,
+                                                    float *__restrict__ dW, int B, int H, int Wd, int Cin, int Cout) {
+    __shared__ __align__(16) bf16 Xs[8][16 * 16];   // per warp [pixel][ci]
+    __shared__ __align__(16) bf16 Ds[8][16 * BN];   // per warp [pixel][co]
+    __shared__ float red[16 * BN];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+    const int tap = blockIdx.z, ntile = Cout / BN;
+    const int ci0 = (blockIdx.y / ntile) * 16, co0 = (blockIdx.y % ntile) * BN;
+    const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
+    const long P = static_cast<long>(B) * H * Wd;
+    const long pbeg = static_cast<long>(blockIdx.x) * kWgPix;
+    const long pend = pbeg + kWgPix < P ? pbeg + kWgPix : P;
+    float acc[BN / 8][4];
+#pragma unroll
+    for (int a = 0; a < BN / 8; a++) acc[a][0] = acc[a][1] = acc[a][2] = acc[a][3] = 0.f;
+    for (long ps = pbeg + warp * 16; ps < pend; ps += 8 * 16) {
+        // Stage: lane l loads pixel ps + l/2, input channels ci0 + (l&1)*8 .. +7
+        {
+            const long p = ps + (lane >> 1);
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (p < pend) {
+                const int b = static_cast<int>(p / (static_cast<long>(H) * Wd));
+                const int r = static_cast<int>(p - static_cast<long>(b) * H * Wd), y = r / Wd, x = r - y * Wd;
+                const int sy = y + dy, sx = x + dx;
+                if (sy >= 0 && sy < H && sx >= 0 && sx < Wd)
+                    v = *reinterpret_cast<const uint4 *>(X + ((static_cast<long>(b) * H + sy) * Wd + sx) * Cin + ci0 +
+                                                         (lane & 1) * 8);
+            }
+            *reinterpret_cast<uint4 *>(&Xs[warp][(lane >> 1) * 16 + (lane & 1) * 8]) = v;
+        }
+        for (int e = lane; e < 16 * BN / 8; e += 32) {
+            const int pr = e / (BN / 8), c8 = (e - pr * (BN / 8)) * 8;
+            const long p = ps + pr;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (p < pend) v = *reinterpret_cast<const uint4 *>(dY + p * Cout + co0 + c8);
+            *reinterpret_cast<uint4 *>(&Ds[warp][pr * BN + c8]) = v;
+        }
+        __syncwarp();
+        const bf16 *xs = Xs[warp], *ds = Ds[warp];
+        uint32_t a[4];
+        a[0] = pack2(xs[(t4 * 2) * 16 + g], xs[(t4 * 2 + 1) * 16 + g]);
+        a[1] = pack2(xs[(t4 * 2) * 16 + g + 8], xs[(t4 * 2 + 1) * 16 + g + 8]);
+        a[2] = pack2(xs[(t4 * 2 + 8) * 16 + g], xs[(t4 * 2 + 9) * 16 + g]);
+        a[3] = pack2(xs[(t4 * 2 + 8) * 16 + g + 8], xs[(t4 * 2 + 9) * 16 + g + 8]);
+#pragma unroll
+        for (int nt = 0; nt < BN / 8; nt++) {
+            uint32_t b[2];
+            b[0] = pack2(ds[(t4 * 2) * BN + nt * 8 + g], ds[(t4 * 2 + 1) * BN + nt * 8 + g]);
+            b[1] = pack2(ds[(t4 * 2 + 8) * BN + nt * 8 + g], ds[(t4 * 2 + 9) * BN + nt * 8 + g]);
+            mma_bf16_16816(acc[nt], a, b);
+        }
+        __syncwarp();
+    }
+    for (int e = tid; e < 16 * BN; e += 256) red[e] = 0.f;
+    __syncthreads();
+#pragma unroll
+    for (int nt = 0; nt < BN / 8; nt++) {
+        atomicAdd(&red[g * BN + nt * 8 + t4 * 2], acc[nt][0]);
+        atomicAdd(&red[g * BN + nt * 8 + t4 * 2 + 1], acc[nt][1]);
+        atomicAdd(&red[(g + 8) * BN + nt * 8 + t4 * 2], acc[nt][2]);
+        atomicAdd(&red[(g + 8) * BN + nt * 8 + t4 * 2 + 1], acc[nt][3]);
+    }
+    __syncthreads();
+    for (int e = tid; e < 16 * BN; e += 256) {
+        const int ci = e / BN, co = e - ci * BN;
+        atomicAdd(&dW[(static_cast<long>(tap) * Cin + ci0 + ci) * Cout + co0 + co], red[e]);
+    }
+}
+
+/** dbias[c] += sum over pixels of dY[p][c]; 256 threads = 32 channels x 8 rows. */
+__global__ void k_bias_grad(const bf16 *dY, float *db, long P, int C) {
+    const int c = blockIdx.y * 32 + (threadIdx.x & 31), r = threadIdx.x >> 5;
+    if (c >= C) return;
+    float s = 0;
+    for (long p = static_cast<long>(blockIdx.x) * 8 + r; p < P; p += static_cast<long>(gridDim.x) * 8)
+        s += __bfloat162float(dY[p * C + c]);
+    atomicAdd(&db[c], s);
+}
+
+/** Gradient through the ReLU: zero where the layer's output is not positive. */
+__global__ void k_relu_mask(bf16 *dY, const bf16 *Y, long n) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x)
+        if (!(__bfloat162float(Y[i]) > 0.f)) dY[i] = __float2bfloat16(0.f);
+}
+
+/** 2x2 average pooling, NHWC. */
+__global__ void k_pool(const bf16 *X, bf16 *Y, int B, int H, int W, int C) {
+    const int Ho = H / 2, Wo = W / 2;
+    const long n = static_cast<long>(B) * Ho * Wo * C;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        long r = i / C;
+        const int x = static_cast<int>(r % Wo);
+        r /= Wo;
+        const int y = static_cast<int>(r % Ho), b = static_cast<int>(r / Ho);
+        const long q = ((static_cast<long>(b) * H + 2 * y) * W + 2 * x) * C + c;
+        const float s = __bfloat162float(X[q]) + __bfloat162float(X[q + C]) + __bfloat162float(X[q + static_cast<long>(W) * C]) +
+                        __bfloat162float(X[q + static_cast<long>(W) * C + C]);
+        Y[i] = __float2bfloat16(0.25f * s);
+    }
+}
+
+/** Pooling gradient added into dX (which already holds the skip gradient). */
+__global__ void k_pool_bwd_add(const bf16 *dY, bf16 *dX, int B, int H, int W, int C) {
+    const long n = static_cast<long>(B) * H * W * C;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        long r = i / C;
+        const int x = static_cast<int>(r % W);
+        r /= W;
+        const int y = static_cast<int>(r % H), b = static_cast<int>(r / H);
+        const long q = ((static_cast<long>(b) * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c;
+        dX[i] = __float2bfloat16(__bfloat162float(dX[i]) + 0.25f * __bfloat162float(dY[q]));
+    }
+}
+
+/** U = [nearest 2x upsample of L (Cl channels), S (Cs channels)], NHWC. */
+__global__ void k_upcat(const bf16 *L, const bf16 *S, bf16 *U, int B, int H, int W, int Cl, int Cs) {
+    const int C = Cl + Cs;
+    const long n = static_cast<long>(B) * H * W * C;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(i % C);
+        const long pix = i / C;
+        if (c < Cl) {
+            const int x = static_cast<int>(pix % W);
+            const long r = pix / W;
+            const int y = static_cast<int>(r % H), b = static_cast<int>(r / H);
+            U[i] = L[((static_cast<long>(b) * (H / 2) + y / 2) * (W / 2) + x / 2) * Cl + c];
+        } else {
+            U[i] = S[pix * Cs + (c - Cl)];
+        }
+    }
+}
+
+/** Gradients of k_upcat: dL summed over the four children, dS written. */
+__global__ void k_upcat_bwd(const bf16 *dU, bf16 *dL, bf16 *dS, int B, int H, int W, int Cl, int Cs) {
+    const int C = Cl + Cs;
+    const long nl = static_cast<long>(B) * (H / 2) * (W / 2) * Cl;
+    const long ns = static_cast<long>(B) * H * W * Cs;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < nl + ns;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        if (i < nl) {
+            const int c = static_cast<int>(i % Cl);
+            long r = i / Cl;
+            const int x = static_cast<int>(r % (W / 2));
+            r /= (W / 2);
+            const int y = static_cast<int>(r % (H / 2)), b = static_cast<int>(r / (H / 2));
+            float s = 0;
+            for (int d = 0; d < 4; d++) {
+                const long pix = (static_cast<long>(b) * H + 2 * y + (d >> 1)) * W + 2 * x + (d & 1);
+                s += __bfloat162float(dU[pix * C + c]);
+            }
+            dL[i] = __float2bfloat16(s);
+        } else {
+            const long k = i - nl, pix = k / Cs;
+            const int c = static_cast<int>(k - pix * Cs);
+            dS[k] = dU[pix * C + Cl + c];
+        }
+    }
+}
+
+/** Network input: 3 FP32 channels into a 16-channel BF16 tensor (rest zero). */
+__global__ void k_pack_input(const float *in, bf16 *X, long P) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < P * 16;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const long p = i >> 4;
+        const int c = static_cast<int>(i & 15);
+        X[i] = __float2bfloat16(c < 3 ? in[p * 3 + c] : 0.f);
+    }
+}
+
+/** Output channel 0 of the head as FP32. */
+__global__ void k_unpack_output(const bf16 *Y, float *out, long P) {
+    for (long p = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; p < P;
+         p += static_cast<long>(gridDim.x) * blockDim.x)
+        out[p] = __bfloat162float(Y[p * 16]);
+}
+
+/** Masked squared error: sums[0] += sum v (o-t)^2, sums[1] += sum v; and the
+ * head's output gradient (channel 0; other channels zero), scaled by 2/N
+ * with N taken from nvalid. */
+__global__ void k_loss(const bf16 *Y, const float *t, const float *valid, long P, double *sums) {
+    double s = 0, w = 0;
+    for (long p = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; p < P;
+         p += static_cast<long>(gridDim.x) * blockDim.x) {
+        const float d = __bfloat162float(Y[p * 16]) - t[p];
+        s += valid[p] * d * d;
+        w += valid[p];
+    }
+    s = block_sum_256(s);
+    __syncthreads();
+    w = block_sum_256(w);
+    if (threadIdx.x == 0) { atomicAdd(&sums[0], s); atomicAdd(&sums[1], w); }
+}
+
+__global__ void k_loss_grad(const bf16 *Y, const float *t, const float *valid, long P, const double *sums, bf16 *dY) {
+    const float scale = static_cast<float>(2.0 / (sums[1] > 0 ? sums[1] : 1.0));
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < P * 16;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const long p = i >> 4;
+        float g = 0;
+        if ((i & 15) == 0) g = scale * valid[p] * (__bfloat162float(Y[i]) - t[p]);
+        dY[i] = __float2bfloat16(g);
+    }
+}
+
+/** Adam (FP32 master parameters), then the BF16 copies of the weights. */
+__global__ void k_adam(float *w, const float *g, float *m, float *v, long n, float lr, float b1, float b2,
+                       float c1, float c2, float eps) {
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1 - b1) * gi, vi = b2 * v[i] + (1 - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+/** BF16 weights of one convolution and its flipped transpose
+ * Wf[tap'][co][ci] = W[taps-1-tap'][ci][co] (the input-gradient convolution). */
+__global__ void k_weights_bf16(const float *w, bf16 *wb, bf16 *wf, int taps, int Cin, int Cout) {
+    const long n = static_cast<long>(taps) * Cin * Cout;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int co = static_cast<int>(i % Cout);
+        const long r = i / Cout;
+        const int ci = static_cast<int>(r % Cin), tap = static_cast<int>(r / Cin);
+        const bf16 v = __float2bfloat16(w[i]);
+        wb[i] = v;
+        wf[(static_cast<long>(taps - 1 - tap) * Cout + co) * Cin + ci] = v;
+    }
+}
+
+struct Conv {
+    int cin, cout, taps;
+    bool relu;
+    long woff, boff;  // offsets of weights [tap][cin][cout] and biases in the parameter vector
+    bf16 *w = nullptr, *wf = nullptr;
+};
+
+/** One activation tensor of the forward pass and its gradient. */
+struct Act {
+    int level, C;
+    bf16 *x = nullptr, *g = nullptr;
+};
+
+inline int gs(long n) {
+    long b = (n + 255) / 256;
+    return static_cast<int>(b < 4L * kB200SMs ? (b > 0 ? b : 1) : 4L * kB200SMs);
+}
+
+}  // namespace
+
+struct UNet {
+    int levels = 4, base = 16;
+    std::vector<Conv> convs;
+    long nparams = 0;
+    float *params = nullptr, *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
+    bf16 *wpool = nullptr;
+    long adam_t = 0;
+    long long launches = 0;
+    // Workspace for the current (batch, H, W).
+    int wb = 0, wh = 0, ww = 0;
+    std::vector<Act> acts;
+    std::vector<void *> work;
+    double *sums = nullptr;
+
+    int C(int l) const { return base << l; }
+
+    int create(int L, int b, unsigned long long seed) {
+        levels = L;
+        base = b;
+        auto add = [&](int cin, int cout, int taps, bool relu) {
+            Conv c;
+            c.cin = cin; c.cout = cout; c.taps = taps; c.relu = relu;
+            c.woff = nparams;
+            nparams += static_cast<long>(taps) * cin * cout;
+            c.boff = nparams;
+            nparams += cout;
+            convs.push_back(c);
+        };
+        // Encoder, bottleneck, decoder, head (the order of the forward pass).
+        add(16, C(0), 9, true);
+        add(C(0), C(0), 9, true);
+        for (int l = 1; l < L; l++) {
+            add(C(l - 1), C(l), 9, true);
+            add(C(l), C(l), 9, true);
+        }
+        for (int l = L - 2; l >= 0; l--) {
+            add(C(l + 1) + C(l), C(l), 9, true);
+            add(C(l), C(l), 9, true);
+        }
+        add(C(0), 16, 1, false);
+        INCRMT_CK(cudaMalloc(&params, sizeof(float) * nparams));
+        INCRMT_CK(cudaMalloc(&grads, sizeof(float) * nparams));
+        INCRMT_CK(cudaMalloc(&m1, sizeof(float) * nparams));
+        INCRMT_CK(cudaMalloc(&m2, sizeof(float) * nparams));
+        INCRMT_CK(cudaMemset(m1, 0, sizeof(float) * nparams));
+        INCRMT_CK(cudaMemset(m2, 0, sizeof(float) * nparams));
+        INCRMT_CK(cudaMalloc(&sums, sizeof(double) * 2));
+        long nw = 0;
+        for (auto &c : convs) nw += static_cast<long>(c.taps) * c.cin * c.cout;
+        INCRMT_CK(cudaMalloc(&wpool, sizeof(bf16) * 2 * nw));
+        long o = 0;
+        for (auto &c : convs) {
+            const long n = static_cast<long>(c.taps) * c.cin * c.cout;
+            c.w = wpool + o;
+            c.wf = wpool + o + n;
+            o += 2 * n;
+        }
+        // He-uniform weights over the real fan-in (3 input channels in the first
+        // layer, the rest being zero padding), zero biases; padded output
+        // channels of the head start at zero.
+        std::vector<float> h(nparams, 0.f);
+        std::mt19937_64 rng(seed);
+        for (size_t k = 0; k < convs.size(); k++) {
+            const Conv &c = convs[k];
+            const int cin_real = k == 0 ? 3 : c.cin;
+            const float bound = std::sqrt(6.f / (c.taps * cin_real));
+            std::uniform_real_distribution<float> U(-bound, bound);
+            for (int tap = 0; tap < c.taps; tap++)
+                for (int ci = 0; ci < c.cin; ci++)
+                    for (int co = 0; co < c.cout; co++) {
+                        const float v = U(rng);
+                        const bool live = (k != 0 || ci < 3) && (k + 1 != convs.size() || co == 0);
+                        h[c.woff + (static_cast<long>(tap) * c.cin + ci) * c.cout + co] = live ? v : 0.f;
+                    }
+        }
+        INCRMT_CK(cudaMemcpy(params, h.data(), sizeof(float) * nparams, cudaMemcpyHostToDevice));
+        return refresh_weights(nullptr);
+    }
+
+    int refresh_weights(cudaStream_t s) {
+        for (auto &c : convs) {
+            const long n = static_cast<long>(c.taps) * c.cin * c.cout;
+            k_weights_bf16<<<gs(n), 256, 0, s>>>(params + c.woff, c.w, c.wf, c.taps, c.cin, c.cout);
+            launches++;
+        }
+        INCRMT_CKL("k_weights_bf16");
+        return INCRMT_OK;
+    }
+
+    void free_work() {
+        for (void *p : work) cudaFree(p);
+        work.clear();
+        acts.clear();
+        wb = wh = ww = 0;
+    }
+
+    /** Activation buffers for (B, H, W): the input, then every convolution's
+     * output, every pooling's output and every concatenation. */
+    int ensure(int B, int H, int W) {
+        if (B == wb && H == wh && W == ww) return INCRMT_OK;
+        free_work();
+        auto alloc = [&](int level, int Cc) -> int {
+            Act a;
+            a.level = level;
+            a.C = Cc;
+            const long n = static_cast<long>(B) * (H >> level) * (W >> level) * Cc;
+            INCRMT_CK(cudaMalloc(&a.x, sizeof(bf16) * n));
+            work.push_back(a.x);
+            INCRMT_CK(cudaMalloc(&a.g, sizeof(bf16) * n));
+            work.push_back(a.g);
+            acts.push_back(a);
+            return INCRMT_OK;
+        };
+        int r;
+        if ((r = alloc(0, 16))) return r;  // 0: packed input
+        for (int l = 0; l < levels; l++) {
+            if (l > 0 && (r = alloc(l, C(l - 1)))) return r;  // pooled input of level l
+            if ((r = alloc(l, C(l)))) return r;                // first conv
+            if ((r = alloc(l, C(l)))) return r;                // second conv (skip of level l)
+        }
+        for (int l = levels - 2; l >= 0; l--) {
+            if ((r = alloc(l, C(l + 1) + C(l)))) return r;     // concatenation
+            if ((r = alloc(l, C(l)))) return r;
+            if ((r = alloc(l, C(l)))) return r;
+        }
+        if ((r = alloc(0, 16))) return r;  // head output
+        wb = B; wh = H; ww = W;
+        return INCRMT_OK;
+    }
+
+    template <int TAPS, bool RELU>
+    void conv_launch(const Conv &c, const bf16 *wgt, const float *bias, const bf16 *X, bf16 *Y, int cin, int cout,
+                     int B, int H, int W, cudaStream_t s) {
+        const long P = static_cast<long>(B) * H * W;
+        const unsigned gx = static_cast<unsigned>((P + kConvBM - 1) / kConvBM);
+        if (cout % 64 == 0)
+            k_conv_fwd<TAPS, 64, RELU><<<dim3(gx, cout / 64), 256, 0, s>>>(X, wgt, bias, Y, B, H, W, cin, cout);
+        else if (cout % 32 == 0)
+            k_conv_fwd<TAPS, 32, RELU><<<dim3(gx, cout / 32), 256, 0, s>>>(X, wgt, bias, Y, B, H, W, cin, cout);
+        else
+            k_conv_fwd<TAPS, 16, RELU><<<dim3(gx, cout / 16), 256, 0, s>>>(X, wgt, bias, Y, B, H, W, cin, cout);
+        launches++;
+    }
+
+    void conv_forward(const Conv &c, const bf16 *X, bf16 *Y, int B, int H, int W, cudaStream_t s) {
+        const float *bias = params + c.boff;
+        if (c.taps == 9) {
+            if (c.relu) conv_launch<9, true>(c, c.w, bias, X, Y, c.cin, c.cout, B, H, W, s);
+            else conv_launch<9, false>(c, c.w, bias, X, Y, c.cin, c.cout, B, H, W, s);
+        } else {
+            conv_launch<1, false>(c, c.w, bias, X, Y, c.cin, c.cout, B, H, W, s);
+        }
+    }
+
+    /** Gradients of one convolution: its output gradient gY (already masked
+     * by the ReLU), input X; accumulates dW, db and writes gX (if given). */
+    void conv_backward(const Conv &c, const bf16 *X, const bf16 *gY, bf16 *gX, int B, int H, int W, cudaStream_t s) {
+        const long P = static_cast<long>(B) * H * W;
+        const unsigned gx = static_cast<unsigned>((P + kWgPix - 1) / kWgPix);
+        float *dW = grads + c.woff, *db = grads + c.boff;
+        if (c.taps == 9) {
+            if (c.cout % 64 == 0)
+                k_conv_wgrad<9, 64><<<dim3(gx, (c.cin / 16) * (c.cout / 64), 9), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
+            else if (c.cout % 32 == 0)
+                k_conv_wgrad<9, 32><<<dim3(gx, (c.cin / 16) * (c.cout / 32), 9), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
+            else
+                k_conv_wgrad<9, 16><<<dim3(gx, (c.cin / 16) * (c.cout / 16), 9), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
+        } else {
+            k_conv_wgrad<1, 16><<<dim3(gx, (c.cin / 16) * (c.cout / 16), 1), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
+        }
+        k_bias_grad<<<dim3(64, (c.cout + 31) / 32), 256, 0, s>>>(gY, db, P, c.cout);
+        launches += 2;
+        if (gX) {
+            if (c.taps == 9) conv_launch<9, false>(c, c.wf, nullptr, gY, gX, c.cout, c.cin, B, H, W, s);
+            else conv_launch<1, false>(c, c.wf, nullptr, gY, gX, c.cout, c.cin, B, H, W, s);
+        }
+    }
+
+    /** Forward pass; returns the head output activation. Act indices follow
+     * ensure(): 0 input; per encoder level [pool,] conv1, conv2; per decoder
+     * level cat, conv1, conv2; last the head. */
+    int forward(int B, int H, int W, const float *in, cudaStream_t s) {
+        int r = ensure(B, H, W);
+        if (r) return r;
+        const long P = static_cast<long>(B) * H * W;
+        k_pack_input<<<gs(P * 16), 256, 0, s>>>(in, acts[0].x, P);
+        launches++;
+        int a = 1, k = 0;
+        bf16 *cur = acts[0].x;
+        std::vector<int> skip(levels);
+        for (int l = 0; l < levels; l++) {
+            const int Hl = H >> l, Wl = W >> l;
+            if (l > 0) {
+                k_pool<<<gs(static_cast<long>(B) * Hl * Wl * C(l - 1)), 256, 0, s>>>(cur, acts[a].x, B, Hl * 2, Wl * 2, C(l - 1));
+                launches++;
+                cur = acts[a++].x;
+            }
+            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            cur = acts[a++].x;
+            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            skip[l] = a;
+            cur = acts[a++].x;
+        }
+        for (int l = levels - 2; l >= 0; l--) {
+            const int Hl = H >> l, Wl = W >> l;
+            k_upcat<<<gs(static_cast<long>(B) * Hl * Wl * (C(l + 1) + C(l))), 256, 0, s>>>(
+                cur, acts[skip[l]].x, acts[a].x, B, Hl, Wl, C(l + 1), C(l));
+            launches++;
+            cur = acts[a++].x;
+            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            cur = acts[a++].x;
+            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            cur = acts[a++].x;
+        }
+        conv_forward(convs[k++], cur, acts[a].x, B, H, W, s);
+        INCRMT_CKL("unet forward");
+        return INCRMT_OK;
+    }
+
+    /** Backward pass from the head gradient in acts.back().g; accumulates
+     * into grads (zeroed by the caller). */
+    int backward(int B, int H, int W, cudaStream_t s) {
+        int a = static_cast<int>(acts.size()) - 1, k = static_cast<int>(convs.size()) - 1;
+        // Recover the forward bookkeeping: indices of the skips.
+        std::vector<int> skip(levels), pool_idx(levels, -1);
+        {
+            int q = 1;
+            for (int l = 0; l < levels; l++) {
+                if (l > 0) pool_idx[l] = q++;
+                q++;
+                skip[l] = q++;
+            }
+        }
+        // Head.
+        conv_backward(convs[k], acts[a - 1].x, acts[a].g, acts[a - 1].g, B, H, W, s);
+        k--;
+        a--;
+        // Decoder, finest first.
+        for (int l = 0; l <= levels - 2; l++) {
+            const int Hl = H >> l, Wl = W >> l;
+            // acts[a] = conv2 output of this decoder level, acts[a-1] = conv1, acts[a-2] = cat
+            const long n2 = static_cast<long>(B) * Hl * Wl * C(l);
+            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[a].g, acts[a].x, n2);
+            conv_backward(convs[k], acts[a - 1].x, acts[a].g, acts[a - 1].g, B, Hl, Wl, s);
+            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[a - 1].g, acts[a - 1].x, n2);
+            conv_backward(convs[k - 1], acts[a - 2].x, acts[a - 1].g, acts[a - 2].g, B, Hl, Wl, s);
+            launches += 2;
+            // Split the concatenation gradient: coarser level's output and the skip.
+            const int lower = (l + 1 == levels - 1) ? skip[levels - 1] : a - 3;
+            k_upcat_bwd<<<gs(static_cast<long>(B) * Hl * Wl * (C(l + 1) + C(l))), 256, 0, s>>>(
+                acts[a - 2].g, acts[lower].g, acts[skip[l]].g, B, Hl, Wl, C(l + 1), C(l));
+            launches++;
+            k -= 2;
+            a -= 3;
+        }
+        // Encoder, coarsest first (acts[skip[l]].g now holds the gradient of
+        // level l's output, including its skip path).
+        for (int l = levels - 1; l >= 0; l--) {
+            const int Hl = H >> l, Wl = W >> l;
+            const int o2 = skip[l], o1 = o2 - 1, in = (l > 0) ? pool_idx[l] : 0;
+            const long n2 = static_cast<long>(B) * Hl * Wl * C(l);
+            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[o2].g, acts[o2].x, n2);
+            conv_backward(convs[2 * l + 1], acts[o1].x, acts[o2].g, acts[o1].g, B, Hl, Wl, s);
+            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[o1].g, acts[o1].x, n2);
+            conv_backward(convs[2 * l], acts[in].x, acts[o1].g, l > 0 ? acts[in].g : nullptr, B, Hl, Wl, s);
+            launches += 2;
+            if (l > 0) {
+                // Pooling gradient into the finer level's output gradient.
+                k_pool_bwd_add<<<gs(static_cast<long>(B) * (Hl * 2) * (Wl * 2) * C(l - 1)), 256, 0, s>>>(
+                    acts[in].g, acts[skip[l - 1]].g, B, Hl * 2, Wl * 2, C(l - 1));
+                launches++;
+            }
+        }
+        INCRMT_CKL("unet backward");
+        return INCRMT_OK;
+    }
+
+    int loss_and_grad(int B, int H, int W, const float *t, const float *valid, cudaStream_t s) {
+        const long P = static_cast<long>(B) * H * W;
+        INCRMT_CK(cudaMemsetAsync(sums, 0, sizeof(double) * 2, s));
+        k_loss<<<gs(P), 256, 0, s>>>(acts.back().x, t, valid, P, sums);
+        k_loss_grad<<<gs(P * 16), 256, 0, s>>>(acts.back().x, t, valid, P, sums, acts.back().g);
+        launches += 2;
+        INCRMT_CKL("unet loss");
+        return INCRMT_OK;
+    }
+
+    void destroy() {
+        free_work();
+        cudaFree(params); cudaFree(grads); cudaFree(m1); cudaFree(m2); cudaFree(wpool); cudaFree(sums);
+        params = grads = m1 = m2 = nullptr;
+        wpool = nullptr;
+        sums = nullptr;
+    }
+};
+
+}  // namespace incrmt
+
+struct incrmt_unet {
+    incrmt::UNet u;
+};
+
+extern "C" {
+
+int incrmt_unet_create(int levels, int base, unsigned long long seed, incrmt_unet **out) {
+    if (!out) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
+    *out = nullptr;
+    if (levels < 2 || levels > 5 || base < 16 || base % 16 || base > 128) {
+        incrmt::set_error("unet: levels 2..5 and a base of 16..128 channels in steps of 16");
+        return INCRMT_ERR_BADARG;
+    }
+    incrmt_unet *h = new (std::nothrow) incrmt_unet;
+    if (!h) { incrmt::set_error("out of host memory"); return INCRMT_ERR_OOM; }
+    int r = h->u.create(levels, base, seed);
+    if (r) { h->u.destroy(); delete h; return r; }
+    *out = h;
+    return INCRMT_OK;
+}
+
+long long incrmt_unet_num_params(const incrmt_unet *h) { return h ? h->u.nparams : 0; }
+
+int incrmt_unet_get_params(incrmt_unet *h, float *host) {
+    if (!h || !host) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
+    INCRMT_CK(cudaMemcpy(host, h->u.params, sizeof(float) * h->u.nparams, cudaMemcpyDeviceToHost));
+    return INCRMT_OK;
+}
+
+int incrmt_unet_set_params(incrmt_unet *h, const float *host) {
+    if (!h || !host) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
+    INCRMT_CK(cudaMemcpy(h->u.params, host, sizeof(float) * h->u.nparams, cudaMemcpyHostToDevice));
+    int r = h->u.refresh_weights(nullptr);
+    if (r) return r;
+    INCRMT_CK(cudaDeviceSynchronize());
+    return INCRMT_OK;
+}
+
+static int unet_check_shape(const incrmt_unet *h, int batch, int H, int W) {
+    const int q = 1 << (h->u.levels - 1);
+    if (batch < 1 || H < q || W < q || H % 16 || W % 16 || H % q || W % q) {
+        incrmt::set_error("unet: H and W must be positive multiples of 16 and of 2^(levels-1)");
+        return INCRMT_ERR_BADARG;
+    }
+    return INCRMT_OK;
+}
+
+int incrmt_unet_forward(incrmt_unet *h, int batch, int H, int W, const float *d_in, float *d_out, void *stream) {
+    if (!h || !d_in || !d_out) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
+    int r = unet_check_shape(h, batch, H, W);
+    if (r) return r;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((r = h->u.forward(batch, H, W, d_in, s))) return r;
+    const long P = static_cast<long>(batch) * H * W;
+    incrmt::k_unpack_output<<<incrmt::gs(P), 256, 0, s>>>(h->u.acts.back().x, d_out, P);
+    h->u.launches++;
+    INCRMT_CKL("k_unpack_output");
+    return INCRMT_OK;
+}
+
+static int unet_grad(incrmt_unet *h, int batch, int H, int W, const float *d_in, const float *d_t,
+                     const float *d_valid, float *loss, cudaStream_t s) {
+    int r = unet_check_shape(h, batch, H, W);
+    if (r) return r;
+    incrmt::UNet &u = h->u;
+    if ((r = u.forward(batch, H, W, d_in, s))) return r;
+    if ((r = u.loss_and_grad(batch, H, W, d_t, d_valid, s))) return r;
+    INCRMT_CK(cudaMemsetAsync(u.grads, 0, sizeof(float) * u.nparams, s));
+    if ((r = u.backward(batch, H, W, s))) return r;
+    double hs[2];
+    INCRMT_CK(cudaMemcpyAsync(hs, u.sums, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    INCRMT_CK(cudaStreamSynchronize(s));
+    if (loss) *loss = static_cast<float>(hs[1] > 0 ? hs[0] / hs[1] : 0.0);
+    return INCRMT_OK;
+}
+
+int incrmt_unet_train_step(incrmt_unet *h, int batch, int H, int W, const float *d_in, const float *d_target,
+                           const float *d_valid, float lr, float *loss, void *stream) {
+    if (!h || !d_in || !d_target || !d_valid) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int r = unet_grad(h, batch, H, W, d_in, d_target, d_valid, loss, s);
+    if (r) return r;
+    incrmt::UNet &u = h->u;
+    u.adam_t++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, static_cast<float>(u.adam_t)), c2 = 1.f - std::pow(b2, static_cast<float>(u.adam_t));
+    incrmt::k_adam<<<incrmt::gs(u.nparams), 256, 0, s>>>(u.params, u.grads, u.m1, u.m2, u.nparams, lr, b1, b2, c1, c2,
+                                                        1e-8f);
+    u.launches++;
+    INCRMT_CKL("k_adam");
+    return u.refresh_weights(s);
+}
+
+int incrmt_unet_gradients(incrmt_unet *h, int batch, int H, int W, const float *d_in, const float *d_target,
+                          const float *d_valid, float *loss, float *host_grad, void *stream) {
+    if (!h || !d_in || !d_target || !d_valid || !host_grad) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int r = unet_grad(h, batch, H, W, d_in, d_target, d_valid, loss, s);
+    if (r) return r;
+    INCRMT_CK(cudaMemcpy(host_grad, h->u.grads, sizeof(float) * h->u.nparams, cudaMemcpyDeviceToHost));
+    return INCRMT_OK;
+}
+
+long long incrmt_unet_launches(const incrmt_unet *h) { return h ? h->u.launches : 0; }
+
+void incrmt_unet_destroy(incrmt_unet *h) {
+    if (!h) return;
+    cudaDeviceSynchronize();
+    h->u.destroy();
+    delete h;
+}
+
+}  // extern "C"

@@ -797,7 +797,9 @@ __global__ void k_ls_fim_coop(LsGrid g, const LsObj *ob, const int *list, const 
                 }
             }
             nxt[ij] = v;
-            const bool c = v != old;
+            // Changes in the last bits (the tail of the fixed point) do not
+            // count: the sweeps end once every value is settled to 1e-13.
+            const bool c = fabs(v - old) > 1e-13 * fabs(v);
             cnow[ij] = c;
             if (c) ch = true;
         }

@@ -1,9 +1,11 @@
 /* incrmt_b200: C ABI of the simulation handle, the B200 replacement of
  * IncRMT's fluid_2d time integrator (fluid_2d.hh:131-177). Same conventions
  * as incrmt.h: int status returns, no exit, caller-owned host buffers. The
- * time step supports domains with walls on all four sides (the simple-spin
- * and sediment scenarios); periodic domains are rejected with
- * INCRMT_ERR_BADARG. */
+ * time step supports walls in x (optionally the inflow and zero-pressure
+ * outlet of sim_horiz_flow) and walls or periodicity in y (the simple-spin,
+ * sediment and flag scenarios); x-periodic domains, y-periodic ones with an
+ * odd n, and y-periodic ones without the zero-pressure outlet (whose pressure
+ * systems are singular) are rejected with INCRMT_ERR_BADARG. */
 #ifndef INCRMT_SIM_H
 #define INCRMT_SIM_H
 
@@ -76,6 +78,8 @@ typedef struct incrmt_sim_stats {
     long long launches;                    /* kernels issued by this handle */
     double dt_reg, time;
     long long march_monotone;              /* band rebuilds that needed the monotone march sweeps */
+    long long window_points;               /* level-set points in the objects' current rebuild
+                                              windows (all objects' whole grids when off) */
 } incrmt_sim_stats;
 
 /** Creates the simulation (fluid_2d::fluid_2d, fluid_2d.cc:26-43). */
@@ -169,6 +173,19 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st);
 #define INCRMT_PHASE_FEM       7  /* FEM source, V-cycles, pressure copy */
 #define INCRMT_PHASE_MG_SETUP  8  /* coefficients and Galerkin hierarchy of both projections */
 #define INCRMT_PHASES          9
+
+/** Per-object windows (no reference counterpart; on by default). The
+ * reference sweeps every object's level set and reference map over the whole
+ * grid in every pass. With windows on, after the first band rebuild each
+ * object's level-set, pinning and reference-map passes cover only a box
+ * around its band and interior, and the per-cell passes over all objects
+ * (stress, density, accelerations, advection) visit only the objects whose
+ * box meets the cell's 32x8 tile. Every value the reference's step reads is
+ * the same either way; what differs is only the never-read edge and slope
+ * values of the reference map far outside each solid. Off (0) runs the
+ * whole-grid passes throughout; a state upload (incrmt_set_field) returns
+ * to whole-grid passes until the next rebuild. */
+int incrmt_sim_set_windows(incrmt_sim *h, int on);
 
 /** Turns timing on or off (CUDA events on the handle's stream; no reference
  * counterpart) and clears the accumulated times: bit 0 times the phases,

@@ -248,7 +248,7 @@ class SimStats(ctypes.Structure):
                 ("solves_fem", ctypes.c_longlong), ("march_sweeps", ctypes.c_longlong),
                 ("extrap_sweeps", ctypes.c_longlong), ("launches", ctypes.c_longlong),
                 ("dt_reg", ctypes.c_double), ("time", ctypes.c_double),
-                ("march_monotone", ctypes.c_longlong)]
+                ("march_monotone", ctypes.c_longlong), ("window_points", ctypes.c_longlong)]
 
 
 def _sim_sigs(L):
@@ -273,6 +273,7 @@ def _sim_sigs(L):
     L.incrmt_record_track.argtypes = [P]
     L.incrmt_get_stats.argtypes = [P, ctypes.POINTER(SimStats)]
     L.incrmt_sim_set_profiling.argtypes = [P, I]
+    L.incrmt_sim_set_windows.argtypes = [P, I]
     L.incrmt_sim_profile.argtypes = [P, dp]
     L.incrmt_sim_mg_profile.argtypes = [P, I, dp, dp, ctypes.POINTER(ctypes.c_longlong)]
     L.incrmt_solid_bound.argtypes = [P, ctypes.POINTER(I)]
@@ -412,6 +413,11 @@ class Simulation:
 
     PHASES = ["tracers", "advection", "mac", "refmap", "extrapolation", "pin_and_band", "stress",
               "fem", "mg_setup"]
+
+    def set_windows(self, on=True):
+        """Per-object windows of the level-set and reference-map passes
+        (on by default); off runs every pass over the whole grid."""
+        check(lib().incrmt_sim_set_windows(self._h, int(on)))
 
     def set_profiling(self, on=True, smoothers=False):
         """Phase timing (on) and per-launch timing of the projections'

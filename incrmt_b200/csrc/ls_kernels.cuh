@@ -55,21 +55,58 @@ struct LsObj {
 // Status values (levelset.cc:211-263, heap.cc): 0/7 far negative/positive,
 // 1/6 trial, 2/5 accepted by the march, 3/4 next to the interface.
 
+/** Point (i,j) of thread (x,y) in object blockIdx.z's window; false
+ * outside it. */
+__device__ __forceinline__ bool ls_point(const LsGrid &g, const LsWin *win, int &i, int &j) {
+    const LsWin w = win[blockIdx.z];
+    i = w.x0 + blockIdx.x * blockDim.x + threadIdx.x;
+    j = w.y0 + blockIdx.y * blockDim.y + threadIdx.y;
+    return i < w.x1 && j < w.y1 && i < g.mL && j < g.nL;
+}
+
 /** Sign classification (levelset.cc:209-263): s=4 for phi>0 with a 4-neighbour
  * phi<=0, s=3 for phi<=0 with a neighbour phi>0, else 7 / 0. */
-__global__ void k_ls_scan(LsGrid g, const LsObj *ob) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
-    const double *phi = ob[blockIdx.z].phi;
-    int *s = ob[blockIdx.z].s;
-    const int ij = j * g.P + i;
-    const bool pos = phi[ij] > 0;
-    bool diff = false;
-    if (i > 0) diff |= (phi[ij - 1] > 0) != pos;
-    if (i < g.mL - 1) diff |= (phi[ij + 1] > 0) != pos;
-    if (j > 0) diff |= (phi[ij - g.P] > 0) != pos;
-    if (j < g.nL - 1) diff |= (phi[ij + g.P] > 0) != pos;
-    s[ij] = pos ? (diff ? 4 : 7) : (diff ? 3 : 0);
+__global__ void k_ls_scan(LsGrid g, const LsObj *ob, const LsWin *win, int *box) {
+    __shared__ int sb[4];
+    if (threadIdx.x == 0 && threadIdx.y == 0) sb[0] = sb[1] = sb[2] = sb[3] = 0x7fffffff;
+    __syncthreads();
+    int i, j;
+    const bool live = ls_point(g, win, i, j);
+    bool keep = false;
+    if (live) {
+        const double *phi = ob[blockIdx.z].phi;
+        int *s = ob[blockIdx.z].s;
+        const int ij = j * g.P + i;
+        const bool pos = phi[ij] > 0;
+        bool diff = false;
+        if (i > 0) diff |= (phi[ij - 1] > 0) != pos;
+        if (i < g.mL - 1) diff |= (phi[ij + 1] > 0) != pos;
+        if (j > 0) diff |= (phi[ij - g.P] > 0) != pos;
+        if (j < g.nL - 1) diff |= (phi[ij + g.P] > 0) != pos;
+        const int st = pos ? (diff ? 4 : 7) : (diff ? 3 : 0);
+        s[ij] = st;
+        keep = st != 7;
+    }
+    // Bounding box of the points inside the solid or next to its interface:
+    // a warp is one row, so its extent comes from the ballot; the block's
+    // warps meet in shared memory and one thread updates the object's box
+    // (minima of x, y, -x, -y).
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (bal && (threadIdx.x & 31) == 0) {
+        const int xb = i - static_cast<int>(threadIdx.x & 31);
+        atomicMin(&sb[0], xb + __ffs(bal) - 1);
+        atomicMin(&sb[1], j);
+        atomicMin(&sb[2], -(xb + 31 - __clz(bal)));
+        atomicMin(&sb[3], -j);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0 && sb[0] != 0x7fffffff) {
+        int *b = box + 4 * blockIdx.z;
+        atomicMin(&b[0], sb[0]);
+        atomicMin(&b[1], sb[1]);
+        atomicMin(&b[2], sb[2]);
+        atomicMin(&b[3], sb[3]);
+    }
 }
 
 /** One-dimensional Hermite weights of the reference's bicubic
@@ -195,9 +232,9 @@ __device__ __forceinline__ double int_abs(double v) {
  * integer abs the loop ends after eight steps whose |phi| < 1 and the
  * closeness test is |x0-x| < 1, exactly as the reference runs. Writes the
  * signed distance to phi_new; sets *err on a failure (levelset.cc:275). */
-__global__ void k_ls_newton(LsGrid g, const LsObj *ob, int *err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_newton(LsGrid g, const LsObj *ob, const LsWin *win, int *err) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const double *phi = ob[blockIdx.z].phi;
     const int *s = ob[blockIdx.z].s;
     double *phi_new = ob[blockIdx.z].phi_new;
@@ -230,9 +267,9 @@ __global__ void k_ls_newton(LsGrid g, const LsObj *ob, int *err) {
     phi_new[ij] = st == 4 ? d : -d;
 }
 
-__global__ void k_ls_copy_interface(LsGrid g, const LsObj *ob) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_copy_interface(LsGrid g, const LsObj *ob, const LsWin *win) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const LsObj &o = ob[blockIdx.z];
     const int ij = j * g.P + i;
     if (o.s[ij] == 3 || o.s[ij] == 4) o.phi[ij] = o.phi_new[ij];
@@ -499,9 +536,9 @@ constexpr double kUnset = 1e300;
 
 /** Initialises both march buffers (+/-kUnset for this side's far points)
  * and clears both change marks. */
-__global__ void k_ls_fim_init(LsGrid g, const LsObj *ob) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_fim_init(LsGrid g, const LsObj *ob, const LsWin *win) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const LsObj &o = ob[blockIdx.z];
     const int ij = j * g.P + i, st = o.s[ij];
     const double v = st == 7 ? kUnset : (st == 0 ? -kUnset : 0.0);
@@ -514,9 +551,9 @@ __global__ void k_ls_fim_init(LsGrid g, const LsObj *ob) {
 /** Final values and clean-up (heap::march acceptance, levelset::clean,
  * levelset.cc:408-413): far points whose value fell inside the band limit are
  * accepted (5 / 2); every point outside the band is set to the band limit. */
-__global__ void k_ls_finish(LsGrid g, const LsObj *ob) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_finish(LsGrid g, const LsObj *ob, const LsWin *win) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     // After the last (unchanging) sweep both buffers hold the final values.
     const double *cur = ob[blockIdx.z].a;
     int *s = ob[blockIdx.z].s;
@@ -535,9 +572,9 @@ __global__ void k_ls_finish(LsGrid g, const LsObj *ob) {
 /** Trial statuses (heap::check_gridpoint / update, heap.cc:38-44,159-167):
  * a far point next to an interface or accepted point of its side was put on
  * the heap and, not being accepted, stays trial (6 / 1). */
-__global__ void k_ls_trial(LsGrid g, const LsObj *ob) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_trial(LsGrid g, const LsObj *ob, const LsWin *win) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const int *s = ob[blockIdx.z].s;
     int *s_out = ob[blockIdx.z].ia;
     const int ij = j * g.P + i, st = s[ij];
@@ -555,9 +592,9 @@ __global__ void k_ls_trial(LsGrid g, const LsObj *ob) {
 }
 
 /** Copies the trial statuses back into the status array. */
-__global__ void k_ls_store_status(LsGrid g, const LsObj *ob) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_store_status(LsGrid g, const LsObj *ob, const LsWin *win) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const int ij = j * g.P + i;
     ob[blockIdx.z].s[ij] = ob[blockIdx.z].ia[ij];
 }
@@ -660,10 +697,10 @@ __device__ __forceinline__ void ls_list_push(int *list, int *list_k, int *count,
 }
 
 /** Lists the band points outside each solid (status 4 or 5). */
-__global__ void k_ls_collect_outside(LsGrid g, const LsObj *ob, int *list, int *list_k, int *count, int cap,
+__global__ void k_ls_collect_outside(LsGrid g, const LsObj *ob, const LsWin *win, int *list, int *list_k, int *count, int cap,
                                      int *overflow) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const int ij = j * g.P + i, st = ob[blockIdx.z].s[ij];
     if (st == 4 || st == 5) ls_list_push(list, list_k, count, cap, overflow, ij, blockIdx.z);
 }
@@ -696,9 +733,9 @@ __global__ void k_ls_extrap_store(const LsObj *ob, const int *list, const int *l
 namespace incrmt {
 
 /** Marks the points next to the interface (status 3 or 4) as 1 in mark. */
-__global__ void k_ls_mark_interface(LsGrid g, const LsObj *ob) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_mark_interface(LsGrid g, const LsObj *ob, const LsWin *win) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const int ij = j * g.P + i, st = ob[blockIdx.z].s[ij];
     ob[blockIdx.z].ia[ij] = (st == 3 || st == 4) ? 1 : 0;
 }
@@ -706,17 +743,20 @@ __global__ void k_ls_mark_interface(LsGrid g, const LsObj *ob) {
 /** One direction of a separable dilation by radius R (max over a window):
  * along x from ia into ib, along y from ib back into ia. */
 template <bool ALONG_X>
-__global__ void k_ls_dilate(LsGrid g, const LsObj *ob, int R) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+__global__ void k_ls_dilate(LsGrid g, const LsObj *ob, const LsWin *win, int R) {
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const int *in = ALONG_X ? ob[blockIdx.z].ia : ob[blockIdx.z].ib;
     int *out = ALONG_X ? ob[blockIdx.z].ib : ob[blockIdx.z].ia;
+    // Every marked point lies inside the window, and only the window's
+    // marks are current: the reach is clipped to it.
+    const LsWin w = win[blockIdx.z];
     int v = 0;
     if (ALONG_X) {
-        const int lo = i - R < 0 ? 0 : i - R, hi = i + R >= g.mL ? g.mL - 1 : i + R;
+        const int lo = i - R < w.x0 ? w.x0 : i - R, hi = i + R >= w.x1 ? w.x1 - 1 : i + R;
         for (int a = lo; a <= hi && !v; a++) v = in[j * g.P + a];
     } else {
-        const int lo = j - R < 0 ? 0 : j - R, hi = j + R >= g.nL ? g.nL - 1 : j + R;
+        const int lo = j - R < w.y0 ? w.y0 : j - R, hi = j + R >= w.y1 ? w.y1 - 1 : j + R;
         for (int b = lo; b <= hi && !v; b++) v = in[b * g.P + i];
     }
     out[j * g.P + i] = v;
@@ -724,10 +764,10 @@ __global__ void k_ls_dilate(LsGrid g, const LsObj *ob, int R) {
 
 /** Lists the far points (status 0 or 7) inside the dilated interface region:
  * the only points the march can reach within the band limit. */
-__global__ void k_ls_collect_candidates(LsGrid g, const LsObj *ob, int *list, int *list_k, int *count, int cap,
+__global__ void k_ls_collect_candidates(LsGrid g, const LsObj *ob, const LsWin *win, int *list, int *list_k, int *count, int cap,
                                         int *overflow) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.mL || j >= g.nL) return;
+    int i, j;
+    if (!ls_point(g, win, i, j)) return;
     const LsObj &o = ob[blockIdx.z];
     const int ij = j * g.P + i, st = o.s[ij];
     if ((st == 0 || st == 7) && o.ia[ij]) ls_list_push(list, list_k, count, cap, overflow, ij, blockIdx.z);

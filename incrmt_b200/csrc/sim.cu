@@ -66,6 +66,20 @@ struct Sim {
     float *d_frame = nullptr;                       // output frame staging (grown on demand)
     size_t frame_cap = 0;
     int *d_box = nullptr;                           // solid bounding box reduction
+    // Per-object windows (sim.cuh). d_win holds kMaxObjects windows of each
+    // kind: 0 rebuild, 1 presence, 2 presence at the last reference-map
+    // update, 3 the whole grid. d_tiles holds the tile object lists of the
+    // presence windows (ntx*nty+1 offsets, then the lists).
+    LsWin *d_win = nullptr, *h_win = nullptr;       // device / pinned host
+    int *d_lsbox = nullptr, *h_lsbox = nullptr;     // box of the last sign scan, per object
+    int *d_tiles = nullptr, *h_tiles = nullptr;
+    size_t tiles_cap = 0;
+    int ntx = 0, nty = 0;
+    bool win_enable = true;   // windows after the first rebuild (else the whole grid always)
+    bool win_valid = false;   // windows derived from a rebuild since the last state change
+    bool x_synced = false;    // X == nX outside the window of the last reference-map update
+    bool pref_valid = false;  // that window is recorded (kind 2)
+    int wmax[4][2] = {};      // largest window of each kind (width, height)
     // Optional phase timing: CUDA events on the stream at phase boundaries.
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -141,6 +155,19 @@ struct Sim {
     int tracers(int stage, double dt);
     int record_track();
     int fetch_flags();
+    int update_velocity(double dt);
+    int win_reset();
+    int win_update();
+    TileObjs tiles() const {
+        const int no = static_cast<int>(obj.size());
+        if (!win_valid) return TileObjs{nullptr, nullptr, ntx, no};
+        return TileObjs{d_tiles, d_tiles + static_cast<size_t>(ntx) * nty + 1, ntx, no};
+    }
+    dim3 wgrid(int kind) const {
+        const int w = wmax[kind][0] > 0 ? wmax[kind][0] : 1, h = wmax[kind][1] > 0 ? wmax[kind][1] : 1;
+        return dim3(cdiv(w, 32), cdiv(h, 8), static_cast<unsigned>(obj.size()));
+    }
+    const LsWin *win(int kind) const { return d_win + static_cast<size_t>(kind) * kMaxObjects; }
 };
 
 int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
@@ -154,6 +181,14 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     }
     if (gr->y_prd && (gr->n & 1)) {
         set_error("a y-periodic grid needs an even n (multigrid coarsening)");
+        return INCRMT_ERR_BADARG;
+    }
+    if (gr->y_prd && !(ph->zpr || ph->horiz_flow)) {
+        // Walls in x with y periodicity and no outlet leave both pressure
+        // systems singular with a periodic null space, which the projections
+        // do not handle; the reference's drivers use y periodicity only with
+        // sim_horiz_flow's outlet (ftest.cc:362).
+        set_error("a y-periodic domain needs the zero-pressure outlet (zpr or horiz_flow)");
         return INCRMT_ERR_BADARG;
     }
     INCRMT_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -210,6 +245,12 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     INCRMT_CK(cudaMalloc(&d_flags, sizeof(int) * 16));
     INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 16, stream));
     INCRMT_CK(cudaMallocHost(&h_flags, sizeof(int) * 16));
+    INCRMT_CK(cudaMalloc(&d_win, sizeof(LsWin) * 4 * kMaxObjects));
+    INCRMT_CK(cudaMallocHost(&h_win, sizeof(LsWin) * 4 * kMaxObjects));
+    INCRMT_CK(cudaMalloc(&d_lsbox, sizeof(int) * 4 * kMaxObjects));
+    INCRMT_CK(cudaMallocHost(&h_lsbox, sizeof(int) * 4 * kMaxObjects));
+    ntx = ((g.m + 1 + 32) >> 5) + 1;
+    nty = ((g.n + 1 + 8) >> 3) + 1;
     if (ntrace > 0 && (r = alloc(&tm, 4 * static_cast<size_t>(ntrace)))) return r;
     if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, g.yp, g.zpr, stream))) return r;
     if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, g.yp, g.zpr, stream))) return r;
@@ -328,11 +369,100 @@ int Sim::fetch_flags() {
     return INCRMT_OK;
 }
 
+/** Windows of every kind set to the whole grid; objects are visited
+ * everywhere until the next rebuild, and the next reference-map commit covers
+ * the whole grid. Used before the first rebuild and after a state upload. */
+int Sim::win_reset() {
+    INCRMT_CK(cudaStreamSynchronize(stream));  // h_win may still feed an earlier copy
+    win_valid = false;
+    x_synced = false;
+    pref_valid = false;
+    const LsWin full{0, 0, g.ml, g.nl};
+    for (int kind = 0; kind < 4; kind++) {
+        for (int k = 0; k < kMaxObjects; k++) h_win[kind * kMaxObjects + k] = full;
+        wmax[kind][0] = g.ml;
+        wmax[kind][1] = g.nl;
+    }
+    INCRMT_CK(cudaMemcpyAsync(d_win, h_win, sizeof(LsWin) * 4 * kMaxObjects, cudaMemcpyHostToDevice, stream));
+    return INCRMT_OK;
+}
+
+/** New rebuild and presence windows from the boxes of the rebuild that just
+ * ran (h_lsbox, fetched with its flags), and the tile object lists. Called
+ * after that rebuild's last kernel is queued: the uploads follow it on the
+ * stream. The windows stay the whole grid when they are switched off, or
+ * when the pinning width reaches the band limit (pin would then rewrite far
+ * points). */
+int Sim::win_update() {
+    const int no = static_cast<int>(obj.size());
+    if (!win_enable || no == 0 || !(obj[0].pinw < lg.phi_up)) return INCRMT_OK;
+    const int R = static_cast<int>(std::ceil((lg.phi_up) / (g.dx < g.dy ? g.dx : g.dy))) + 2;
+    auto grow = [&](const int *b, int e) {
+        if (b[0] >= 0x7f7f7f7f) return LsWin{0, 0, 0, 0};  // no point inside or at the interface
+        LsWin w{b[0] - e, b[1] - e, -b[2] + e + 1, -b[3] + e + 1};
+        w.x0 = w.x0 < 0 ? 0 : w.x0 & ~31;  // rows of 32 start on a 256-byte boundary
+        w.y0 = w.y0 < 0 ? 0 : w.y0;
+        w.x1 = w.x1 > g.ml ? g.ml : w.x1;
+        w.y1 = w.y1 > g.nl ? g.nl : w.y1;
+        return w;
+    };
+    for (int kind = 0; kind < 2; kind++) wmax[kind][0] = wmax[kind][1] = 0;
+    LsWin *wl = h_win, *wp = h_win + kMaxObjects;
+    size_t entries = 0;
+    for (int k = 0; k < no; k++) {
+        wl[k] = grow(h_lsbox + 4 * k, 2 * R + 4);
+        wp[k] = grow(h_lsbox + 4 * k, R + 3);
+        // Under y periodicity the Godunov pass of the last row writes the
+        // bottom edges of row 0: a window near either end spans the height.
+        if (g.yp && wp[k].y1 > wp[k].y0 && (wp[k].y0 <= 3 || wp[k].y1 >= g.nl - 3)) {
+            wp[k].y0 = 0;
+            wp[k].y1 = g.nl;
+        }
+        for (int kind = 0; kind < 2; kind++) {
+            const LsWin &w = h_win[kind * kMaxObjects + k];
+            if (w.x1 - w.x0 > wmax[kind][0]) wmax[kind][0] = w.x1 - w.x0;
+            if (w.y1 - w.y0 > wmax[kind][1]) wmax[kind][1] = w.y1 - w.y0;
+        }
+        if (wp[k].x1 > wp[k].x0 && wp[k].y1 > wp[k].y0)
+            entries += static_cast<size_t>(((wp[k].x1 + 29) >> 5) - ((wp[k].x0 + 30) >> 5) + 1) *
+                       (((wp[k].y1 + 5) >> 3) - ((wp[k].y0 + 6) >> 3) + 1);
+    }
+    // Tile lists: tile (tx,ty) holds cells 32(tx-1) <= i < 32tx,
+    // 8(ty-1) <= j < 8ty; level-set point li is cell li-2.
+    const size_t ntiles = static_cast<size_t>(ntx) * nty, need = ntiles + 1 + entries;
+    if (need > tiles_cap) {
+        cudaFreeHost(h_tiles);
+        cudaFree(d_tiles);
+        h_tiles = nullptr;
+        d_tiles = nullptr;
+        tiles_cap = 0;
+        INCRMT_CK(cudaMallocHost(&h_tiles, sizeof(int) * need));
+        INCRMT_CK(cudaMalloc(&d_tiles, sizeof(int) * need));
+        tiles_cap = need;
+    }
+    int *start = h_tiles, *list = h_tiles + ntiles + 1;
+    std::fill(start, start + ntiles + 1, 0);
+    auto each_tile = [&](const LsWin &w, auto &&fn) {
+        if (w.x1 <= w.x0 || w.y1 <= w.y0) return;
+        const int tx0 = (w.x0 + 30) >> 5, tx1 = (w.x1 + 29) >> 5, ty0 = (w.y0 + 6) >> 3, ty1 = (w.y1 + 5) >> 3;
+        for (int ty = ty0; ty <= ty1; ty++)
+            for (int tx = tx0; tx <= tx1; tx++) fn(static_cast<size_t>(ty) * ntx + tx);
+    };
+    for (int k = 0; k < no; k++) each_tile(wp[k], [&](size_t t) { start[t + 1]++; });
+    for (size_t t = 0; t < ntiles; t++) start[t + 1] += start[t];
+    std::vector<int> fill(start, start + ntiles);
+    for (int k = 0; k < no; k++) each_tile(wp[k], [&](size_t t) { list[fill[t]++] = k; });
+    INCRMT_CK(cudaMemcpyAsync(d_win, h_win, sizeof(LsWin) * 2 * kMaxObjects, cudaMemcpyHostToDevice, stream));
+    INCRMT_CK(cudaMemcpyAsync(d_tiles, h_tiles, sizeof(int) * need, cudaMemcpyHostToDevice, stream));
+    win_valid = true;
+    return INCRMT_OK;
+}
+
 int Sim::compute_stress() {
     pre_stress_setup(time);
     int r = upload_objects();
     if (r) return r;
-    k_stress<<<g2(g.m + 1, g.n + 1), kB2, 0, stream>>>(g, f, d_obj, d_sol, static_cast<int>(obj.size()));
+    k_stress<<<g2(g.m + 1, g.n + 1), kB2, 0, stream>>>(g, f, d_obj, d_sol, tiles());
     launches++;
     INCRMT_CKL("k_stress");
     return INCRMT_OK;
@@ -346,32 +476,35 @@ int Sim::set_boundaries() {
 }
 
 int Sim::set_rho() {
-    k_set_rho<<<g2(g.ml, g.nl), kB2, 0, stream>>>(g, f, d_obj, d_sol, static_cast<int>(obj.size()));
+    k_set_rho<<<g2(g.ml, g.nl), kB2, 0, stream>>>(g, f, d_obj, d_sol, tiles());
     launches++;
     INCRMT_CKL("k_set_rho");
     return INCRMT_OK;
 }
 
-/** levelset::build_band for object k (levelset.cc:199-335). */
 /** levelset::build_band for every object (levelset.cc:199-335): each kernel
- * runs over all objects at once (blockIdx.z), and one cooperative launch
- * settles every object's march, the objects being independent. */
+ * runs over all objects at once (blockIdx.z), each over its rebuild window,
+ * and one cooperative launch settles every object's march, the objects being
+ * independent. The sign scan also records each object's box, from which the
+ * next windows follow. */
 int Sim::build_bands() {
     const int no = static_cast<int>(obj.size());
     if (no == 0) return INCRMT_OK;
     INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 13, stream));
-    const dim3 gg(cdiv(lg.mL, 32), cdiv(lg.nL, 8), no);
-    k_ls_scan<<<gg, kB2, 0, stream>>>(lg, d_lso);
-    k_ls_newton<<<gg, kB2, 0, stream>>>(lg, d_lso, d_flags + 6);
-    k_ls_copy_interface<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    INCRMT_CK(cudaMemsetAsync(d_lsbox, 0x7f, sizeof(int) * 4 * no, stream));
+    const dim3 gg = wgrid(0);
+    const LsWin *wl = win(0);
+    k_ls_scan<<<gg, kB2, 0, stream>>>(lg, d_lso, wl, d_lsbox);
+    k_ls_newton<<<gg, kB2, 0, stream>>>(lg, d_lso, wl, d_flags + 6);
+    k_ls_copy_interface<<<gg, kB2, 0, stream>>>(lg, d_lso, wl);
     // Candidates: far points within the band radius of the interface.
     const int R = static_cast<int>(std::ceil((lg.phi_up) / (g.dx < g.dy ? g.dx : g.dy))) + 2;
-    k_ls_mark_interface<<<gg, kB2, 0, stream>>>(lg, d_lso);
-    k_ls_dilate<true><<<gg, kB2, 0, stream>>>(lg, d_lso, R);
-    k_ls_dilate<false><<<gg, kB2, 0, stream>>>(lg, d_lso, R);
-    k_ls_collect_candidates<<<gg, kB2, 0, stream>>>(lg, d_lso, d_list, d_list_k, d_flags + 7, list_cap,
+    k_ls_mark_interface<<<gg, kB2, 0, stream>>>(lg, d_lso, wl);
+    k_ls_dilate<true><<<gg, kB2, 0, stream>>>(lg, d_lso, wl, R);
+    k_ls_dilate<false><<<gg, kB2, 0, stream>>>(lg, d_lso, wl, R);
+    k_ls_collect_candidates<<<gg, kB2, 0, stream>>>(lg, d_lso, wl, d_list, d_list_k, d_flags + 7, list_cap,
                                                     d_flags + 10);
-    k_ls_fim_init<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    k_ls_fim_init<<<gg, kB2, 0, stream>>>(lg, d_lso, wl);
     launches += 8;
     INCRMT_CKL("level-set scan/newton/candidates");
     int maxs = kLsMaxSweeps, cap = list_cap;
@@ -381,6 +514,7 @@ int Sim::build_bands() {
     INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_fim_coop), dim3(coop_blocks_fim), dim3(256),
                                           args, 0, stream));
     launches++;
+    INCRMT_CK(cudaMemcpyAsync(h_lsbox, d_lsbox, sizeof(int) * 4 * no, cudaMemcpyDeviceToHost, stream));
     int r = fetch_flags();
     if (r) return r;
     if (h_flags[6]) { set_error("level++: Newton iteration failed."); return h_flags[6]; }
@@ -388,12 +522,12 @@ int Sim::build_bands() {
     ls_sweeps += h_flags[3];
     if (h_flags[12]) ls_monotone++;
     if (!h_flags[4]) { set_error("level-set march did not settle in %d sweeps", h_flags[3]); return INCRMT_ERR_NOCONV; }
-    k_ls_finish<<<gg, kB2, 0, stream>>>(lg, d_lso);
-    k_ls_trial<<<gg, kB2, 0, stream>>>(lg, d_lso);
-    k_ls_store_status<<<gg, kB2, 0, stream>>>(lg, d_lso);
+    k_ls_finish<<<gg, kB2, 0, stream>>>(lg, d_lso, wl);
+    k_ls_trial<<<gg, kB2, 0, stream>>>(lg, d_lso, wl);
+    k_ls_store_status<<<gg, kB2, 0, stream>>>(lg, d_lso, wl);
     launches += 3;
     INCRMT_CKL("k_ls_finish");
-    return INCRMT_OK;
+    return win_update();
 }
 
 /** obj_field::pin for every object, then set_rho (fluid_2d::pin,
@@ -401,7 +535,7 @@ int Sim::build_bands() {
 int Sim::pin() {
     int r;
     if (!obj.empty()) {
-        k_pin<<<dim3(cdiv(g.ml, 32), cdiv(g.nl, 8), obj.size()), kB2, 0, stream>>>(g, d_obj, d_sol);
+        k_pin<<<wgrid(1), kB2, 0, stream>>>(g, d_obj, d_sol, win(1));
         launches++;
         INCRMT_CKL("k_pin");
     }
@@ -415,8 +549,8 @@ int Sim::extrapolate_all() {
     const int no = static_cast<int>(obj.size());
     if (no == 0) return INCRMT_OK;
     INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 11, stream));
-    k_ls_collect_outside<<<dim3(cdiv(lg.mL, 32), cdiv(lg.nL, 8), no), kB2, 0, stream>>>(
-        lg, d_lso, d_list, d_list_k, d_flags + 7, list_cap, d_flags + 10);
+    k_ls_collect_outside<<<wgrid(1), kB2, 0, stream>>>(lg, d_lso, win(1), d_list, d_list_k, d_flags + 7,
+                                                       list_cap, d_flags + 10);
     k_ls_extrap_init<<<4 * kB200SMs, 256, 0, stream>>>(d_lso, d_list, d_list_k, d_flags + 7, list_cap);
     launches += 2;
     INCRMT_CKL("collect");
@@ -440,12 +574,20 @@ int Sim::extrapolate_all() {
     return INCRMT_OK;
 }
 
-/** fluid_2d::update_reference_map (fluid_2d.cc:1242-1273). */
+/** fluid_2d::update_reference_map (fluid_2d.cc:1242-1273), every object
+ * over its presence window, which is recorded for the commit in
+ * update_velocity. */
 int Sim::update_reference_map(double dt) {
-    for (size_t k = 0; k < obj.size(); k++) {
-        k_refmap_update<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, sol[k], dt);
+    const int no = static_cast<int>(obj.size());
+    if (no > 0) {
+        k_refmap_update<<<wgrid(1), kB2, 0, stream>>>(g, f, d_sol, win(1), dt);
         launches++;
         INCRMT_CKL("k_refmap_update");
+        INCRMT_CK(cudaMemcpyAsync(d_win + 2 * kMaxObjects, win(1), sizeof(LsWin) * no, cudaMemcpyDeviceToDevice,
+                                  stream));
+        wmax[2][0] = wmax[1][0];
+        wmax[2][1] = wmax[1][1];
+        pref_valid = true;
     }
     int r, outer = cur_phase;
     if ((r = phase_end())) return r;
@@ -453,8 +595,8 @@ int Sim::update_reference_map(double dt) {
     if ((r = extrapolate_all())) return r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(outer))) return r;
-    for (size_t k = 0; k < obj.size(); k++) {
-        k_refmap_half<<<g2(g.m, g.n), kB2, 0, stream>>>(g, sol[k]);
+    if (no > 0) {
+        k_refmap_half<<<wgrid(1), kB2, 0, stream>>>(g, d_sol, win(1));
         launches++;
         INCRMT_CKL("k_refmap_half");
     }
@@ -625,6 +767,7 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
     }
     int r = upload_objects();
     if (r) return r;
+    if ((r = win_reset())) return r;
     // fluid_2d::init_fields (fluid_2d.cc:195-254).
     if (!obj.empty()) {
         k_init_object<<<dim3(cdiv(g.ml, 32), cdiv(g.nl, 8), obj.size()), kB2, 0, stream>>>(g, d_obj, d_sol);
@@ -643,12 +786,29 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
     return INCRMT_OK;
 }
 
+/** fluid_2d::update_velocity (fluid_2d.cc:1354-1374): the velocity, then
+ * X = nX over the window of the last reference-map update (the whole grid
+ * when X and nX may differ elsewhere: before the first step, after a state
+ * upload, or without a recorded update). */
+int Sim::update_velocity(double dt) {
+    k_update_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, dt);
+    launches++;
+    INCRMT_CKL("k_update_velocity");
+    if (obj.empty()) return INCRMT_OK;
+    const int kind = x_synced && pref_valid ? 2 : 3;
+    k_refmap_commit<<<wgrid(kind), kB2, 0, stream>>>(g, d_sol, win(kind));
+    launches++;
+    INCRMT_CKL("k_refmap_commit");
+    x_synced = true;
+    pref_valid = false;
+    return INCRMT_OK;
+}
+
 /** godunov_upwinding_set<tang> followed by edge_boundary_conditions
  * (fluid_2d.cc:1112-1121, 689-777). */
 int Sim::godunov(bool tang) {
-    const int no = static_cast<int>(obj.size());
-    if (tang) k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
-    else k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no);
+    if (tang) k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles());
+    else k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles());
     launches++;
     if (g.yp) {
         k_wrap_edges_y<<<cdiv(g.m, 256), 256, 0, stream>>>(g, f);
@@ -661,16 +821,15 @@ int Sim::godunov(bool tang) {
 /** fluid_2d::step_forward (fluid_2d.cc:298-369). */
 int Sim::step(double dt) {
     if (!initialized) { set_error("not initialized"); return INCRMT_ERR_BADARG; }
-    const int no = static_cast<int>(obj.size());
     const double ntime = time + dt;
     int r;
 #define INCRMT_PHASE(ph, ...) do { if ((r = phase_begin(ph))) return r; __VA_ARGS__; if ((r = phase_end())) return r; } while (0)
     INCRMT_PHASE(INCRMT_PHASE_TRACERS, if ((r = tracers(1, dt))) return r);
     INCRMT_PHASE(INCRMT_PHASE_ADVECTION, {
-        k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
+        k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles(), dt);
         if ((r = godunov(true))) return r;
         k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f);
-        k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
+        k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, tiles(), dt);
         if ((r = godunov(false))) return r;
         launches += 3;
         INCRMT_CKL("advection");
@@ -682,17 +841,13 @@ int Sim::step(double dt) {
     INCRMT_PHASE(INCRMT_PHASE_STRESS, {
         if ((r = set_boundaries())) return r;
         if ((r = compute_stress())) return r;
-        k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt);
+        k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, tiles(), dt);
         launches++;
         INCRMT_CKL("k_ustar");
     });
     time = ntime;
     INCRMT_PHASE(INCRMT_PHASE_FEM, if ((r = fem_projection(dt))) return r);
-    INCRMT_PHASE(INCRMT_PHASE_STRESS, {
-        k_update_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt);
-        launches++;
-        INCRMT_CKL("k_update_velocity");
-    });
+    INCRMT_PHASE(INCRMT_PHASE_STRESS, if ((r = update_velocity(dt))) return r);
     INCRMT_PHASE(INCRMT_PHASE_PIN, if ((r = pin())) return r);
     INCRMT_PHASE(INCRMT_PHASE_STRESS, {
         if ((r = set_boundaries())) return r;
@@ -707,26 +862,25 @@ int Sim::step(double dt) {
 /** Runs one reference step function on the current state (same numbering as
  * the oracle's ref_stage). */
 int Sim::stage(int s, double dt) {
-    const int no = static_cast<int>(obj.size());
     switch (s) {
         case 0: return tracers(1, dt);
         case 1:
-        case 2: k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt); break;
+        case 2: k_normal_derivatives<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles(), dt); break;
         case 3: return godunov(true);
         case 4: break;  // fused into the Godunov kernels
         case 5: k_tangential<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f); break;
         case 6:
-        case 7: k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt); break;
+        case 7: k_half_time<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, tiles(), dt); break;
         case 8: return godunov(false);
         case 9: return mac_projection();
         case 10: return update_reference_map(dt);
         case 11: return pin();
         case 12: return set_boundaries();
         case 13: return compute_stress();
-        case 14: k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, no, dt); break;
+        case 14: k_ustar<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_obj, d_sol, tiles(), dt); break;
         case 15: return fem_projection(dt);
         case 16: return INCRMT_OK;  // fused into fem_projection
-        case 17: k_update_velocity<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, no, dt); break;
+        case 17: return update_velocity(dt);
         case 18: return tracers(2, dt);
         case 19: return set_rho();
         case 20: return step(dt);
@@ -748,6 +902,11 @@ void Sim::destroy() {
     for (auto &s : sol) cudaFree(s.s);
     cudaFree(d_frame); cudaFree(d_box);
     d_frame = nullptr; d_box = nullptr; frame_cap = 0;
+    cudaFree(d_win); cudaFree(d_lsbox); cudaFree(d_tiles);
+    if (h_win) cudaFreeHost(h_win);
+    if (h_lsbox) cudaFreeHost(h_lsbox);
+    if (h_tiles) cudaFreeHost(h_tiles);
+    d_win = h_win = nullptr; d_lsbox = h_lsbox = nullptr; d_tiles = h_tiles = nullptr; tiles_cap = 0;
     for (void *p : raw_allocs) cudaFree(p);
     raw_allocs.clear();
     lso.clear();
@@ -867,6 +1026,9 @@ int incrmt_set_field(incrmt_sim *h, int id, int k, const double *host) {
     if (!h || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
     incrmt::Sim &S = h->s;
     const size_t w = S.g.ml, rows = S.g.nl;
+    // An uploaded state may have anything anywhere: whole-grid passes until
+    // the next band rebuild.
+    if (int r = S.win_reset()) return r;
     if (id == INCRMT_FIELD_STATUS) {
         if (k < 0 || k >= static_cast<int>(S.sol.size())) { set_error("bad object"); return INCRMT_ERR_BADARG; }
         std::vector<int> tmp(w * rows);
@@ -979,11 +1141,22 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
     st->solves_fem = S.solves_fem;
     st->march_sweeps = S.ls_sweeps;
     st->march_monotone = S.ls_monotone;
+    st->window_points = 0;
+    for (size_t k = 0; k < S.obj.size(); k++) {
+        const incrmt::LsWin &w = S.win_valid ? S.h_win[k] : incrmt::LsWin{0, 0, S.g.ml, S.g.nl};
+        st->window_points += static_cast<long long>(w.x1 - w.x0) * (w.y1 - w.y0);
+    }
     st->extrap_sweeps = S.ex_sweeps;
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;
     st->time = S.time;
     return INCRMT_OK;
+}
+
+int incrmt_sim_set_windows(incrmt_sim *h, int on) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    h->s.win_enable = on != 0;
+    return on ? INCRMT_OK : h->s.win_reset();
 }
 
 int incrmt_sim_set_profiling(incrmt_sim *h, int on) {

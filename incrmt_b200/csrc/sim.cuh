@@ -163,4 +163,47 @@ struct SolidDev {
     int *s;
 };
 
+// Per-object windows.
+//
+// The reference sweeps every object's arrays over the whole grid in every
+// level-set and reference-map pass, but after the first band rebuild an
+// object only differs from "far away" (status 7, phi at the positive band
+// limit, no stress, no density, no acceleration) inside a box around its
+// band and interior. The simulation keeps, per object, the bounding box B of
+// the points that are inside it or next to its interface (status != 7 after
+// the sign scan of the last rebuild) and derives:
+//  - the rebuild window B + 2R + 4 (R the candidate radius): everything the
+//    next rebuild can change, with the two-cell reach of the march stencil;
+//  - the presence window B + R + 3: every point whose phi is below the band
+//    limit, with a cell of stencil reach around it.
+// Outside these the kernels below skip the object; the skipped work leaves
+// every value the reference's computation reads unchanged. Before the first
+// rebuild, and after a state upload, the windows are the whole grid.
+
+/** Half-open window [x0,x1) x [y0,y1) on the level-set grid (ghosted
+ * coordinates: level-set point (li,lj) is cell (li-2, lj-2)). */
+struct LsWin {
+    int x0, y0, x1, y1;
+};
+
+/** Which objects each 32 x 8 tile of the ghosted grid has to visit: those
+ * whose presence window meets the tile, in increasing object order (so the
+ * per-point sums over objects add the same terms in the same order). A null
+ * start means every object everywhere. Tile (tx,ty) covers cells
+ * 32(tx-1) <= i < 32tx and 8(ty-1) <= j < 8ty, so ghost cells i,j >= -2 fall
+ * in tile 0 and the 32-wide rows of the cell kernels are never split. */
+struct TileObjs {
+    const int *start;  // ntiles + 1 offsets into obj
+    const int *obj;
+    int ntx;           // tiles per row
+    int nobj;
+    __device__ __forceinline__ void range(int i, int j, int &b, int &e) const {
+        if (!start) { b = 0; e = nobj; return; }
+        const int t = ((j + 8) >> 3) * ntx + ((i + 32) >> 5);
+        b = start[t];
+        e = start[t + 1];
+    }
+    __device__ __forceinline__ int at(int p) const { return start ? obj[p] : p; }
+};
+
 }  // namespace incrmt

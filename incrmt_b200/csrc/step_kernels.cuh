@@ -32,7 +32,7 @@ __device__ __forceinline__ double mono_diff(double f0, double f1, double f2, dou
 /** normal_derivatives_velocity + normal_derivatives_refmap
  * (fluid_2d.cc:877-950): limited slopes and edge extrapolations of u,v and
  * of every object's X,Y. */
-__global__ void k_normal_derivatives(GridDev g, FluidDev f, const SolidDev *sol, int nobj, double dt) {
+__global__ void k_normal_derivatives(GridDev g, FluidDev f, const SolidDev *sol, TileObjs to, double dt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.m || j >= g.n) return;
     const int q = g.idx(i, j), P = g.P;
@@ -50,8 +50,10 @@ __global__ void k_normal_derivatives(GridDev g, FluidDev f, const SolidDev *sol,
     f.vd[q] = v - 0.5 * (g.dy + dt * v) * vy;
     f.uu[q] = u + 0.5 * (g.dy - dt * v) * uy;
     f.vu[q] = v + 0.5 * (g.dy - dt * v) * vy;
-    for (int k = 0; k < nobj; k++) {
-        const SolidDev s = sol[k];
+    int kb, ke;
+    to.range(i, j, kb, ke);
+    for (int p = kb; p < ke; p++) {
+        const SolidDev s = sol[to.at(p)];
         const double X = s.X[q], Y = s.Y[q];
         const double Xx = g.xsp * mono_diff(s.X[q - 2], s.X[q - 1], X, s.X[q + 1], s.X[q + 2]);
         const double Yx = g.xsp * mono_diff(s.Y[q - 2], s.Y[q - 1], Y, s.Y[q + 1], s.Y[q + 2]);
@@ -75,26 +77,33 @@ __global__ void k_normal_derivatives(GridDev g, FluidDev f, const SolidDev *sol,
  * its cell; the boundary edges it writes are disjoint from the Godunov
  * writes, so the two passes fuse without a race. */
 template <bool tang>
-__global__ void k_godunov(GridDev g, FluidDev f, const SolidDev *sol, int nobj) {
+__global__ void k_godunov(GridDev g, FluidDev f, const SolidDev *sol, TileObjs to) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.m || j >= g.n) return;
     const int q = g.idx(i, j), P = g.P;
+    int kb, ke;
+    to.range(i, j, kb, ke);
     if (i < g.m - 1) {
         const int r = q + 1;
         const double fur = f.ur[q], frul = f.ul[r];
         if (fur + frul > 0 && fur > 0) {
             f.ul[r] = fur;
             f.vl[r] = f.vr[q];
-            for (int k = 0; k < nobj; k++) { sol[k].Xl[r] = sol[k].Xr[q]; sol[k].Yl[r] = sol[k].Yr[q]; }
+            for (int p = kb; p < ke; p++) {
+                const SolidDev &s = sol[to.at(p)];
+                s.Xl[r] = s.Xr[q];
+                s.Yl[r] = s.Yr[q];
+            }
         } else if (fur + frul < 0 && frul < 0) {
             if (tang) f.ur[q] = frul;
         } else {
             if (tang) f.ur[q] = 0.5 * (fur + frul);
             f.ul[r] = 0;
             f.vl[r] = 0.5 * (f.vr[q] + f.vl[r]);
-            for (int k = 0; k < nobj; k++) {
-                sol[k].Xl[r] = 0.5 * (sol[k].Xr[q] + sol[k].Xl[r]);
-                sol[k].Yl[r] = 0.5 * (sol[k].Yr[q] + sol[k].Yl[r]);
+            for (int p = kb; p < ke; p++) {
+                const SolidDev &s = sol[to.at(p)];
+                s.Xl[r] = 0.5 * (s.Xr[q] + s.Xl[r]);
+                s.Yl[r] = 0.5 * (s.Yr[q] + s.Yl[r]);
             }
         }
     }
@@ -111,16 +120,21 @@ __global__ void k_godunov(GridDev g, FluidDev f, const SolidDev *sol, int nobj) 
         if (fvu + ftvd > 0 && fvu > 0) {
             f.vd[t] = fvu;
             f.ud[t] = f.uu[q];
-            for (int k = 0; k < nobj; k++) { sol[k].Xd[t] = sol[k].Xu[qs]; sol[k].Yd[t] = sol[k].Yu[qs]; }
+            for (int p = kb; p < ke; p++) {
+                const SolidDev &s = sol[to.at(p)];
+                s.Xd[t] = s.Xu[qs];
+                s.Yd[t] = s.Yu[qs];
+            }
         } else if (fvu + ftvd < 0 && ftvd < 0) {
             if (tg) f.vu[q] = ftvd;
         } else {
             if (tg) f.vu[q] = 0.5 * (fvu + ftvd);
             f.vd[t] = 0;
             f.ud[t] = 0.5 * (f.uu[q] + f.ud[t]);
-            for (int k = 0; k < nobj; k++) {
-                sol[k].Xd[t] = 0.5 * (sol[k].Xu[qs] + sol[k].Xd[t]);
-                sol[k].Yd[t] = 0.5 * (sol[k].Yu[qs] + sol[k].Yd[t]);
+            for (int p = kb; p < ke; p++) {
+                const SolidDev &s = sol[to.at(p)];
+                s.Xd[t] = 0.5 * (s.Xu[qs] + s.Xd[t]);
+                s.Yd[t] = 0.5 * (s.Yu[qs] + s.Yd[t]);
             }
         }
     }
@@ -186,8 +200,8 @@ __device__ __forceinline__ void wall_force(const GridDev &g, double x, double y,
 
 /** fluid_2d::acceleration (fluid_2d.cc:1019-1050). */
 __device__ __forceinline__ void acceleration(const GridDev &g, const FluidDev &f, const ObjDev *obj,
-                                             const SolidDev *sol, int nobj, int q, double x, double y,
-                                             bool pressure, double &accx, double &accy) {
+                                             const SolidDev *sol, const TileObjs &to, int i, int j, int q,
+                                             double x, double y, bool pressure, double &accx, double &accy) {
     const int P = g.P;
     double ax_ = 0, ay_ = 0;
     accx = g.xsp * (f.s11[q + 1] - f.s11[q]) + g.ysp * (f.s12[q + P] - f.s12[q]);
@@ -196,7 +210,10 @@ __device__ __forceinline__ void acceleration(const GridDev &g, const FluidDev &f
         accx -= 0.5 * g.xsp * (f.p[q + P + 1] + f.p[q + 1] - f.p[q + P] - f.p[q]);
         accy -= 0.5 * g.ysp * (f.p[q + P + 1] - f.p[q + 1] + f.p[q + P] - f.p[q]);
     }
-    for (int k = 0; k < nobj; k++) {
+    int kb, ke;
+    to.range(i, j, kb, ke);
+    for (int p = kb; p < ke; p++) {
+        const int k = to.at(p);
         const double phiv = sol[k].phi[q];
         if (phiv < obj[k].eps) {
             wall_force(g, x, y, phiv, accx, accy);
@@ -212,13 +229,13 @@ __device__ __forceinline__ void acceleration(const GridDev &g, const FluidDev &f
 
 /** compute_half_time_edge_velocities (fluid_2d.cc:979-1008) fused with
  * compute_half_time_edge_reference_map (fluid_2d.cc:1082-1108). */
-__global__ void k_half_time(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, int nobj, double dt) {
+__global__ void k_half_time(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, TileObjs to, double dt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.m || j >= g.n) return;
     const int q = g.idx(i, j);
     const double x = g.ax + g.dx * (0.5 + i), y = g.ay + g.dy * (0.5 + j);
     double accx, accy;
-    acceleration(g, f, obj, sol, nobj, q, x, y, true, accx, accy);
+    acceleration(g, f, obj, sol, to, i, j, q, x, y, true, accx, accy);
     const double u = f.u[q], v = f.v[q], ux = f.ux[q], vx = f.vx[q], uy = f.uy[q], vy = f.vy[q];
     const double c0 = f.c0[q], c1 = f.c1[q], c2 = f.c2[q], c3 = f.c3[q];
     f.ul[q] = u + 0.5 * (-g.dx * ux + dt * (-u * ux - c2 + accx));
@@ -229,8 +246,10 @@ __global__ void k_half_time(GridDev g, FluidDev f, const ObjDev *obj, const Soli
     f.vd[q] = v + 0.5 * (-g.dy * vy + dt * (-v * vy - c1 + accy));
     f.uu[q] = u + 0.5 * (g.dy * uy + dt * (-v * uy - c0 + accx));
     f.vu[q] = v + 0.5 * (g.dy * vy + dt * (-v * vy - c1 + accy));
-    for (int k = 0; k < nobj; k++) {
-        const SolidDev s = sol[k];
+    int kb, ke;
+    to.range(i, j, kb, ke);
+    for (int p = kb; p < ke; p++) {
+        const SolidDev s = sol[to.at(p)];
         const double X = s.X[q], Y = s.Y[q], Xx = s.Xx[q], Xy = s.Xy[q], Yx = s.Yx[q], Yy = s.Yy[q];
         const double Xdt = dt * (-u * Xx - v * Xy), Ydt = dt * (-u * Yx - v * Yy);
         s.Xl[q] = X + 0.5 * (-g.dx * Xx + Xdt);
@@ -268,11 +287,24 @@ __global__ void k_mac_correct(GridDev g, FluidDev f, const double *z, const doub
     if (i > 0) f.ul[q] -= ex[j * (g.m + 1) + i] * (z[ij] - z[ij - 1]) * g.xsp;
 }
 
+/** Cell (i,j) of thread (x,y) of a launch over object blockIdx.z's window
+ * (level-set coordinates, so cell = point - 2); false outside the window or
+ * outside the cells lo <= i < m+hi, lo <= j < n+hi. */
+__device__ __forceinline__ bool win_cell(const GridDev &g, const LsWin *win, int lo, int hi, int &i, int &j) {
+    const LsWin w = win[blockIdx.z];
+    const int li = w.x0 + blockIdx.x * blockDim.x + threadIdx.x, lj = w.y0 + blockIdx.y * blockDim.y + threadIdx.y;
+    i = li - 2;
+    j = lj - 2;
+    return li < w.x1 && lj < w.y1 && i >= lo && j >= lo && i < g.m + hi && j < g.n + hi;
+}
+
 /** First part of update_reference_map (fluid_2d.cc:1246-1258): the end-of-
- * step reference map nX,nY at points with status < 4, for one object. */
-__global__ void k_refmap_update(GridDev g, FluidDev f, SolidDev s, double dt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.m || j >= g.n) return;
+ * step reference map nX,nY at points with status < 4, for object blockIdx.z
+ * within its window (status < 4 holds only inside it). */
+__global__ void k_refmap_update(GridDev g, FluidDev f, const SolidDev *sol, const LsWin *win, double dt) {
+    int i, j;
+    if (!win_cell(g, win, 0, 0, i, j)) return;
+    const SolidDev &s = sol[blockIdx.z];
     const int q = g.idx(i, j), P = g.P;
     if (s.s[q] >= 4) return;
     const double hx = 0.5 * dt * g.xsp, hy = 0.5 * dt * g.ysp;
@@ -282,10 +314,12 @@ __global__ void k_refmap_update(GridDev g, FluidDev f, SolidDev s, double dt) {
 }
 
 /** Last part of update_reference_map (fluid_2d.cc:1266-1272):
- * X = (X+nX)/2 where status < 6 (s_field::set_half_timestep). */
-__global__ void k_refmap_half(GridDev g, SolidDev s) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= g.m || j >= g.n) return;
+ * X = (X+nX)/2 where status < 6 (s_field::set_half_timestep), object
+ * blockIdx.z within its window. */
+__global__ void k_refmap_half(GridDev g, const SolidDev *sol, const LsWin *win) {
+    int i, j;
+    if (!win_cell(g, win, 0, 0, i, j)) return;
+    const SolidDev &s = sol[blockIdx.z];
     const int q = g.idx(i, j);
     if (s.s[q] < 6) {
         s.X[q] = 0.5 * (s.X[q] + s.nX[q]);
@@ -295,12 +329,15 @@ __global__ void k_refmap_half(GridDev g, SolidDev s) {
 
 /** Density from the level sets (fluid_2d::set_rho, fluid_2d.cc:1124-1137),
  * over the whole ghosted grid. */
-__global__ void k_set_rho(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, int nobj) {
+__global__ void k_set_rho(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, TileObjs to) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - 2, j = blockIdx.y * blockDim.y + threadIdx.y - 2;
     if (i >= g.m + 2 || j >= g.n + 2) return;
     const int q = g.idx(i, j);
     double rho = 0, sfrac = 0;
-    for (int k = 0; k < nobj; k++) {
+    int kb, ke;
+    to.range(i, j, kb, ke);
+    for (int p = kb; p < ke; p++) {
+        const int k = to.at(p);
         double tf = trans_func(obj[k], sol[k].phi[q]);
         sfrac += tf;
         rho += tf * obj[k].rhos;
@@ -417,13 +454,18 @@ __device__ __forceinline__ void edge_phi(const GridDev &g, const double *phi, in
  * (compute_stress body, fluid_2d.cc:395-441). */
 template <bool left>
 __device__ __forceinline__ void edge_stress(const GridDev &g, const FluidDev &f, const ObjDev *obj,
-                                            const SolidDev *sol, int nobj, int q, double &o1, double &o2) {
+                                            const SolidDev *sol, const TileObjs &to, int i, int j, int q,
+                                            double &o1, double &o2) {
     const int P = g.P;
     double s1s = 0, s2s = 0, sfrac = 0;
     unsigned long long present = 0;
     int k = 0;
-    for (int a = 0; a < nobj; a++)
-        if (solid_stress<left>(g, f, obj[a], sol[a], q, s1s, s2s, sfrac)) { present |= 1ull << a; k++; }
+    int kb, ke;
+    to.range(i, j, kb, ke);
+    for (int pa = kb; pa < ke; pa++) {
+        const int a = to.at(pa);
+        if (solid_stress<left>(g, f, obj[a], sol[a], q, s1s, s2s, sfrac)) { present |= 1ull << (pa - kb); k++; }
+    }
     if (sfrac >= 1) {
         o1 = s1s / sfrac;
         o2 = s2s / sfrac;
@@ -445,12 +487,14 @@ __device__ __forceinline__ void edge_stress(const GridDev &g, const FluidDev &f,
     }
     if (k > 1) {
         const double small_number = 100. * 2.220446049250313e-16;
-        for (int a = 0; a < nobj; a++) {
-            if (!(present >> a & 1)) continue;
+        for (int pa = kb; pa < ke; pa++) {
+            if (!(present >> (pa - kb) & 1)) continue;
+            const int a = to.at(pa);
             double p1, p1x, p1y;
             edge_phi<left>(g, sol[a].phi, q, p1, p1x, p1y);
-            for (int b = a + 1; b < nobj; b++) {
-                if (!(present >> b & 1)) continue;
+            for (int pb = pa + 1; pb < ke; pb++) {
+                if (!(present >> (pb - kb) & 1)) continue;
+                const int b = to.at(pb);
                 double p2, p2x, p2y;
                 edge_phi<left>(g, sol[b].phi, q, p2, p2x, p2y);
                 const double norx = (p2x - p1x), nory = (p2y - p1y), nn = norx * norx + nory * nory;
@@ -470,28 +514,28 @@ __device__ __forceinline__ void edge_stress(const GridDev &g, const FluidDev &f,
 
 /** fluid_2d::compute_stress (fluid_2d.cc:381-445) over the (m+1) x (n+1)
  * left and bottom edges. */
-__global__ void k_stress(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, int nobj) {
+__global__ void k_stress(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, TileObjs to) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i > g.m || j > g.n) return;
     const int q = g.idx(i, j);
     double a, b;
-    edge_stress<true>(g, f, obj, sol, nobj, q, a, b);
+    edge_stress<true>(g, f, obj, sol, to, i, j, q, a, b);
     f.s11[q] = a;
     f.s21[q] = b;
-    edge_stress<false>(g, f, obj, sol, nobj, q, a, b);
+    edge_stress<false>(g, f, obj, sol, to, i, j, q, a, b);
     f.s12[q] = a;
     f.s22[q] = b;
 }
 
 /** Intermediate velocity u* (fluid_2d::compute_ustar, fluid_2d.cc:1278-1291)
  * into c0,c1. */
-__global__ void k_ustar(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, int nobj, double dt) {
+__global__ void k_ustar(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, TileObjs to, double dt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.m || j >= g.n) return;
     const int q = g.idx(i, j), P = g.P;
     const double x = g.ax + 0.5 * g.dx + i * g.dx, y = g.ay + g.dy * (.5 + j);
     double accx, accy;
-    acceleration(g, f, obj, sol, nobj, q, x, y, false, accx, accy);
+    acceleration(g, f, obj, sol, to, i, j, q, x, y, false, accx, accy);
     const double hx = 0.5 * dt * g.xsp, hy = 0.5 * dt * g.ysp;
     const double a = f.ul[q + 1] + f.ul[q], b = f.vd[q + P] + f.vd[q];
     f.c0[q] = f.u[q] - hx * a * (f.ul[q + 1] - f.ul[q]) - hy * b * (f.ud[q + P] - f.ud[q]) + dt * accx;
@@ -589,27 +633,35 @@ __global__ void k_copy_pressure(GridDev g, FluidDev f, const double *z, const do
     f.p[g.idx(i, j)] = z[jz * g.mf + i] - pavg;
 }
 
-/** End-of-step velocity and reference map (update_velocity,
- * fluid_2d.cc:1354-1374). */
-__global__ void k_update_velocity(GridDev g, FluidDev f, const SolidDev *sol, int nobj, double dt) {
+/** End-of-step velocity (update_velocity, fluid_2d.cc:1354-1374); the
+ * reference-map part is k_refmap_commit. */
+__global__ void k_update_velocity(GridDev g, FluidDev f, double dt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.m || j >= g.n) return;
     const int q = g.idx(i, j), P = g.P;
     const double rhoinv = 1. / f.rho[q];
     f.u[q] = f.c0[q] - 0.5 * dt * rhoinv * g.xsp * (f.p[q + P + 1] + f.p[q + 1] - f.p[q + P] - f.p[q]);
     f.v[q] = f.c1[q] - 0.5 * dt * rhoinv * g.ysp * (f.p[q + P + 1] - f.p[q + 1] + f.p[q + P] - f.p[q]);
-    for (int k = 0; k < nobj; k++) {
-        sol[k].X[q] = sol[k].nX[q];
-        sol[k].Y[q] = sol[k].nY[q];
-    }
 }
 
-/** Pins the level set to the reference map within the pinning width, over
- * the whole ghosted grid (obj_field::pin, obj_field.cc:92-97); object
- * blockIdx.z. */
-__global__ void k_pin(GridDev g, const ObjDev *obj, const SolidDev *sol) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x - 2, j = blockIdx.y * blockDim.y + threadIdx.y - 2;
-    if (i >= g.m + 2 || j >= g.n + 2) return;
+/** The reference map part of update_velocity (fluid_2d.cc:1366-1373):
+ * X = nX for object blockIdx.z, over the window where this step's
+ * reference-map update changed X or nX (everywhere else they are equal). */
+__global__ void k_refmap_commit(GridDev g, const SolidDev *sol, const LsWin *win) {
+    int i, j;
+    if (!win_cell(g, win, 0, 0, i, j)) return;
+    const SolidDev &s = sol[blockIdx.z];
+    const int q = g.idx(i, j);
+    s.X[q] = s.nX[q];
+    s.Y[q] = s.nY[q];
+}
+
+/** Pins the level set to the reference map within the pinning width
+ * (obj_field::pin, obj_field.cc:92-97), object blockIdx.z over its window of
+ * the ghosted grid (|phi| < pinw only inside it). */
+__global__ void k_pin(GridDev g, const ObjDev *obj, const SolidDev *sol, const LsWin *win) {
+    int i, j;
+    if (!win_cell(g, win, -2, 2, i, j)) return;
     const ObjDev &o = obj[blockIdx.z];
     const SolidDev &s = sol[blockIdx.z];
     const int q = g.idx(i, j);

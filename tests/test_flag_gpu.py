@@ -150,3 +150,12 @@ def test_initial_state(gpu):
     assert np.abs(a[:, [0, 1, 4, 5]] - b[:, [0, 1, 4, 5]]).max() <= 1e-15
     r.close()
     g.close()
+
+
+def test_periodic_without_outlet_rejected(gpu):
+    """A y-periodic channel needs the zero-pressure outlet: walls in x with y
+    periodicity alone leave singular periodic pressure systems, which the
+    simulation refuses at creation."""
+    from incrmt_b200 import capi
+    with pytest.raises(capi.IncrmtError):
+        capi.Simulation(64, 64, y_prd=True)

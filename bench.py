@@ -489,6 +489,8 @@ def run_ours_sspin(args, ws, rank, local, dist):
         "march_sweeps_per_step": (st1.march_sweeps - st0.march_sweeps) / args.steps,
         "march_monotone_rebuilds": int(st1.march_monotone - st0.march_monotone),
         "extrap_sweeps_per_step": (st1.extrap_sweeps - st0.extrap_sweeps) / args.steps,
+        # level-set points in the objects' rebuild windows over all objects' full grids
+        "window_fraction": st1.window_points / max(1, sim.objects * (sim.m + 4) * (sim.n + 4)),
         "roofline": _roofline(f"{args.workload}_smooth", sm_ms, sm_bytes, sm_launch,
                               "k_smooth_rb / k_smooth_tile on the fine level of the MAC and FEM projections "
                               "(two Gauss-Seidel sweeps per launch)",

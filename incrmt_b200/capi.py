@@ -304,32 +304,37 @@ class Simulation:
         self._h = h
         self.m, self.n, self.ml, self.nl, self.ntrace = m, n, m + 4, n + 4, ntrace
         self.dt_reg = None
+        self.objects = 0
+
+    def _add(self, d):
+        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+        self.objects += 1
 
     def add_simple_spin(self, r_scale=0.8, a1=0.5, a2=0.125, piv_r=0.2, th_max=np.pi, omega=1.0,
                         G=48.0, rhos=3.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_SIMPLE_SPIN, G, rhos, ev_trans_mult, 1,
                        (ctypes.c_double * 8)(r_scale, a1, a2, piv_r, th_max, omega, 0, 0))
-        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+        self._add(d)
 
     def add_circle(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_CIRCLE, G, rhos, ev_trans_mult, 1,
                        (ctypes.c_double * 8)(cx, cy, cr, uu, vv, omega, grav, 0))
-        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+        self._add(d)
 
     def add_rounded_rod(self, cx, cy, cr, cl, G, rhos, grav=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_ROUNDED_ROD, G, rhos, ev_trans_mult, 1,
                        (ctypes.c_double * 8)(cx, cy, cr, cl, grav, 0, 0, 0))
-        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+        self._add(d)
 
     def add_ellipse(self, cx, cy, a, b, theta, G, rhos, grav=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_ELLIPSE, G, rhos, ev_trans_mult, 1,
                        (ctypes.c_double * 8)(cx, cy, a, b, theta, grav, 0, 0))
-        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+        self._add(d)
 
     def add_flag(self, cx, cy, flag_l, flag_w, flag_a, G, rhos, perturb_v=0.0, ntrace=17, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_FLAG, G, rhos, ev_trans_mult, 1,
                        (ctypes.c_double * 8)(cx, cy, flag_l, flag_w, flag_a, perturb_v, ntrace, 0))
-        check(lib().incrmt_add_object(self._h, ctypes.byref(d)))
+        self._add(d)
 
     def initialize(self, ev_mult=0.8, dt_pad=0.4, dt_ev_pad=0.8):
         dt = ctypes.c_double()

@@ -347,7 +347,7 @@ SED_BOX = (-0.75, 0.75, -1.5, 1.5)
 FLAG_N = 1152
 
 
-def _make_sim(workload, rank, prec):
+def _make_sim(workload, rank, prec, training=False):
     """The simulation of a step workload and its frame interval:
     sspin1024 (ftest simple-spin, solve(2pi,120) frames) or sed1024 (32
     seeded circles and ellipses settling in the sediment box at 1024 x 2048,
@@ -372,14 +372,17 @@ def _make_sim(workload, rank, prec):
         w = 1.0 / ar
         sim = capi.Simulation(m, n, ax=-1.0, bx=5.0, ay=-1.0, by=1.0, visc=1.0 / Re, ntrace=0,
                               precision=prec, y_prd=True, horiz_flow=1.0)
-        sim.add_flag(0.0, 0.0, 1.0, w, 0.25 * w, 4 * k_B / w ** 3, mu / w, ntrace=17)
+        # the learned warm start trains on a run whose tail is perturbed
+        # (ftest's optional perturb_v), a different trajectory
+        sim.add_flag(0.0, 0.0, 1.0, w, 0.25 * w, 4 * k_B / w ** 3, mu / w, perturb_v=0.2 if training else 0.0,
+                     ntrace=17)
         sim.initialize()
         return sim, 30.0 / 900, (f"flag {m}x{n} on [-1,5]x[-1,1] (mu 1, k_B 0.1, Re 100, ar 10), FEM with "
                                  f"zero-pressure outlet, y-periodic; fluid_2d::step_forward, dt of 900 frames over T=30")
     m, n = SED_M, 2 * SED_M
     ax, bx, ay, by = SED_BOX
     sim = capi.Simulation(m, n, ax=ax, bx=bx, ay=ay, by=by, visc=2e-3, ntrace=512, precision=prec)
-    for o in workloads.sediment_bodies(seed=11 + rank):
+    for o in workloads.sediment_bodies(seed=(1011 if training else 11) + rank):
         if o["kind"] == "circle":
             sim.add_circle(o["cx"], o["cy"], o["r"], 1.0, o["rhos"], grav=o["grav"])
         else:
@@ -391,6 +394,71 @@ def _make_sim(workload, rank, prec):
                       f"settling, fluid_2d::step_forward, dt of 0.1 frames")
 
 
+LEARNED_SIM_FACTOR = 8     # network grid: the projection's unknowns restricted by 8
+LEARNED_SIM_SAMPLES = 200  # projections captured per system from the training run
+LEARNED_SIM_STEPS = 1500   # Adam steps per network
+
+
+def _frame_dt(sim, interval):
+    l = int(interval / sim.dt_reg) + 1
+    return interval / l
+
+
+def _train_learned_sim(workload, rank, dev):
+    """The learned warm start of the MAC and FEM projections, trained with
+    this library's own U-Net kernels on samples the method generates: a
+    training run of the workload (another seed; for the flag a perturbed
+    tail) captures every projection's input and correction."""
+    import torch
+    from incrmt_b200 import capi, learned
+    t0 = time.perf_counter()
+    sim, interval, _ = _make_sim(workload, rank, capi.PREC_FP64, training=True)
+    dt = _frame_dt(sim, interval)
+    sim.step(dt, 10)
+    data = learned.capture(sim, LEARNED_SIM_FACTOR, LEARNED_SIM_SAMPLES, dt, dev)
+    sim.close()
+    t_data = time.perf_counter() - t0
+    nets, losses = {}, {}
+    t1 = time.perf_counter()
+    for sys, (X, T) in data.items():
+        Xn, Tn, V = learned.normalise(X, T)
+        net = capi.UNet(4, 16, seed=11 + sys)
+        losses["mac" if sys == capi.SYS_MAC else "fem"] = learned.train(net, Xn, Tn, V, LEARNED_SIM_STEPS,
+                                                                       seed=rank)
+        nets[sys] = net
+    torch.cuda.synchronize()
+    H, W = data[capi.SYS_MAC][0].shape[1:3]
+    info = {"network": f"two U-Nets (MAC, FEM), 4 levels, base 16 channels, {nets[0].num_params()} parameters "
+                       f"each, BF16 activations, mma.sync tensor-core convolutions",
+            "grid": f"{H}x{W} (projection restricted by {LEARNED_SIM_FACTOR})",
+            "train_samples_per_system": LEARNED_SIM_SAMPLES, "train_steps": LEARNED_SIM_STEPS, "batch": 8,
+            "final_loss": losses, "data_seconds": t_data, "train_seconds": time.perf_counter() - t1}
+    return nets, info
+
+
+def _plain_fp64_rate(workload, rank, steps, warmup, dev):
+    """Steps/s and V-cycles per projection of the plain FP64 method on the
+    same workload (the comparison of the learned + mixed line)."""
+    import torch
+    from incrmt_b200 import capi
+    sim, interval, _ = _make_sim(workload, rank, capi.PREC_FP64)
+    dt = _frame_dt(sim, interval)
+    ext = torch.cuda.ExternalStream(sim.stream(), device=dev)
+    sim.step(dt, warmup)
+    torch.cuda.synchronize()
+    st0 = sim.stats()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.step(dt, steps)
+    e1.record(ext)
+    torch.cuda.synchronize()
+    st1 = sim.stats()
+    sim.close()
+    vc = ((st1.vcycles_mac - st0.vcycles_mac) + (st1.vcycles_fem - st0.vcycles_fem)) / (2.0 * steps)
+    return steps / (e0.elapsed_time(e1) / 1e3), vc
+
+
 def run_ours_sspin(args, ws, rank, local, dist):
     """Simulation steps on the GPU through the simulation C ABI."""
     import torch
@@ -399,10 +467,16 @@ def run_ours_sspin(args, ws, rank, local, dist):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    nets, learned_info = None, None
+    if args.learned:
+        if args.workload not in ("sed1024", "flag2048"):
+            raise SystemExit("--learned: the simulation workloads with a learned warm start are sed1024, flag2048")
+        nets, learned_info = _train_learned_sim(args.workload, rank, dev)
     sim, interval, wl = _make_sim(args.workload, rank, prec)
-    dt_reg = sim.dt_reg
-    l = int(interval / dt_reg) + 1
-    dt = interval / l
+    dt = _frame_dt(sim, interval)
+    if nets is not None:
+        for sys, net in nets.items():
+            sim.set_learned(sys, net, LEARNED_SIM_FACTOR, args.learned_rule)
     ext = torch.cuda.ExternalStream(sim.stream(), device=dev)
     sim.step(dt, args.warmup)
     torch.cuda.synchronize()
@@ -456,6 +530,20 @@ def run_ours_sspin(args, ws, rank, local, dist):
     e2e = ws * args.steps / e2e_s
     d2h = sum(h.nbytes for h in host)
 
+    if nets is not None:
+        lst = {("mac" if s == capi.SYS_MAC else "fem"): sim.learned_stats(s) for s in nets}
+        sim.close()
+        for net in nets.values():
+            net.close()
+        plain_sps, plain_vc = _plain_fp64_rate(args.workload, rank, args.steps, args.warmup, dev)
+        learned_info.update({
+            "rule": "fall back to the previous solution when the guess raises the residual" if args.learned_rule == 0
+                    else "fall back only when the energy-optimal step is not positive",
+            "applied": {k: v.applied for k, v in lst.items()},
+            "fallback": {k: v.fallback for k, v in lst.items()},
+            "fallback_rate": {k: v.fallback / max(1, v.applied + v.fallback) for k, v in lst.items()},
+            "plain_fp64_steps_per_s": plain_sps, "plain_fp64_vcycles_per_projection": plain_vc,
+            "speedup_vs_plain_fp64": value / ws / plain_sps})
     if rank != 0:
         return
     cpu = None
@@ -502,6 +590,10 @@ def run_ours_sspin(args, ws, rank, local, dist):
         "gpu_launches": int(st1.launches - st0.launches),
         "clocks": clk.summary(),
     }
+    if learned_info is not None:
+        line["learned"] = learned_info
+        line["config"]["initial_guess"] = "learned warm start on the previous solution"
+
     print(json.dumps(line))
     sim.close()
 
@@ -731,7 +823,12 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned", action="store_true",
-                    help="mac4096: train the learned initial guess first and start every solve from it")
+                    help="mac4096: train the learned initial guess first and start every solve from it; "
+                         "sed1024, flag2048: train the learned warm start of both projections on a training "
+                         "run and apply it in every projection")
+    ap.add_argument("--learned-rule", type=int, default=0, choices=[0, 1],
+                    help="fallback rule of the simulation's learned warm start (0: when the guess raises the "
+                         "residual, 1: when the energy-optimal step is not positive)")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.impl == "reference":

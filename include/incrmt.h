@@ -92,6 +92,13 @@ int incrmt_mg_vcycle_device(incrmt_mg *h, const double *d_b, double *d_z);
  * reference counterpart (instrumentation). */
 int incrmt_mg_set_profiling(incrmt_mg *h, int on);
 
+/** Tile-fused smoothing (on by default; no reference counterpart): two
+ * Gauss-Seidel sweeps per launch in shared-memory tiles wherever the level's
+ * periodic directions have even sizes, with results identical to one launch
+ * per colour in the V-cycle's four-colour order. Off (0) runs one launch per
+ * colour everywhere; it exists to check that identity. */
+int incrmt_mg_set_tiles(incrmt_mg *h, int on);
+
 /** Accumulated profile since incrmt_mg_set_profiling: total device time (ms)
  * of the timed launches, their algorithmic bytes (updated unknowns x (3+c)
  * words) and their number. */

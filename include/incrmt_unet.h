@@ -18,6 +18,7 @@
 
 #include <stddef.h>
 #include "incrmt.h"
+#include "incrmt_sim.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -64,8 +65,8 @@ typedef struct incrmt_learned_stats {
     int used;
 } incrmt_learned_stats;
 
-/** Learned initial guess of the MAC solve of `h` (a non-periodic MAC solver
- * whose density is set): from the iterate d_z, forms r0 = b - A z, runs the
+/** Learned initial guess of the solve of `h` (a MAC or FEM solver whose
+ * density is set; not x-periodic): from the iterate d_z, forms r0 = b - A z, runs the
  * network on the r0 and 1/rho features restricted by `factor` (block
  * averages; the network grid is ceil(m/factor) x ceil(n/factor) rounded up to
  * multiples of 16), prolongs the output d bilinearly and sets
@@ -79,6 +80,39 @@ int incrmt_mg_learned_guess(incrmt_mg *h, incrmt_unet *net, const double *d_b, d
  * floats (NHWC) into d_in, H x W the network grid of `factor`. */
 int incrmt_mg_learned_input(incrmt_mg *h, const double *d_b, const double *d_z, int factor, float *d_in, int H,
                             int W);
+
+/** Learned warm start of a simulation's projections (no counterpart in the
+ * reference, whose projections start from the previous solution,
+ * mgs_common.cc:15-21). For system sys (INCRMT_SYS_MAC: the MAC projection,
+ * INCRMT_SYS_FEM: the FEM projection), before every solve the guess above is
+ * applied to the warm start (the previous step's solution) with the network
+ * net at restriction factor `factor`. rule 0 keeps the previous solution
+ * whenever the step would raise the residual's 2-norm (the network's initial
+ * residual is worse); rule 1 only when alpha <= 0 (the step lowers the error
+ * in the energy norm whenever alpha > 0). The solve then iterates to the same
+ * tolerance as without it. net = NULL turns it off. The network stays owned
+ * by the caller and must outlive its use. x-periodic systems are rejected. */
+int incrmt_sim_set_learned(incrmt_sim *h, int sys, incrmt_unet *net, int factor, int rule);
+
+/** Network grid H x W of system sys at restriction factor `factor`. */
+int incrmt_sim_learned_grid(const incrmt_sim *h, int sys, int factor, int *H, int *W);
+
+/** Training samples from the simulation's own projections: each of the next
+ * `cap` solves of system sys writes, before solving, the network input of its
+ * warm start (H x W x 3 floats, the layout of incrmt_mg_learned_input) to
+ * d_in + k*H*W*3 and, after solving, the block averages of (solution - warm
+ * start) over factor x factor unknowns (H x W floats, zero outside the image)
+ * to d_target + k*H*W, k = 0, 1, ... Captured solves run without the learned
+ * guess. cap = 0 stops the capture. Device buffers owned by the caller. */
+int incrmt_sim_learned_capture(incrmt_sim *h, int sys, int factor, float *d_in, float *d_target, int cap);
+
+/** Counts of system sys since the simulation was created: guesses applied,
+ * guesses rejected by the rule (the solve then starts from the previous
+ * solution), and samples captured by the current capture. */
+typedef struct incrmt_sim_learned_stats {
+    long long applied, fallback, captured;
+} incrmt_sim_learned_stats;
+int incrmt_sim_get_learned_stats(incrmt_sim *h, int sys, incrmt_sim_learned_stats *st);
 
 /** Kernel launches issued by this network so far. */
 long long incrmt_unet_launches(const incrmt_unet *h);

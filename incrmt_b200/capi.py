@@ -78,6 +78,7 @@ def lib():
     L.incrmt_mg_apply.argtypes = [P, dp, dp]
     L.incrmt_mg_vcycle_device.argtypes = [P, P, P]
     L.incrmt_mg_set_profiling.argtypes = [P, I]
+    L.incrmt_mg_set_tiles.argtypes = [P, I]
     L.incrmt_mg_profile.argtypes = [P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(ctypes.c_longlong)]
     L.incrmt_mg_stream.argtypes = [P]
     L.incrmt_mg_stream.restype = P
@@ -174,6 +175,11 @@ class MGSolver:
 
     def set_profiling(self, on=True):
         check(lib().incrmt_mg_set_profiling(self._h, int(on)))
+
+    def set_tiles(self, on=True):
+        """Tile-fused smoothing (incrmt_mg_set_tiles); off runs one launch
+        per colour."""
+        check(lib().incrmt_mg_set_tiles(self._h, int(on)))
 
     def profile(self):
         """(device ms, algorithmic bytes, launches) of the timed fine-level sweeps."""
@@ -419,6 +425,31 @@ class Simulation:
     PHASES = ["tracers", "advection", "mac", "refmap", "extrapolation", "pin_and_band", "stress",
               "fem", "mg_setup"]
 
+    def set_learned(self, sys, net, factor=8, rule=0):
+        """Learned warm start of the MAC (sys=SYS_MAC) or FEM (SYS_FEM)
+        projection (incrmt_sim_set_learned); net=None turns it off. rule 0
+        falls back to the previous solution when the guess raises the
+        residual, rule 1 only when alpha <= 0."""
+        self._nets = getattr(self, "_nets", {})
+        self._nets[sys] = net  # keep the network alive while the simulation uses it
+        check(_ulib().incrmt_sim_set_learned(self._h, sys, net.handle if net is not None else None, factor, rule))
+
+    def learned_grid(self, sys, factor):
+        H, W = ctypes.c_int(), ctypes.c_int()
+        check(_ulib().incrmt_sim_learned_grid(self._h, sys, factor, ctypes.byref(H), ctypes.byref(W)))
+        return H.value, W.value
+
+    def learned_capture(self, sys, factor, in_ptr, target_ptr, cap):
+        """Captures the next `cap` projections of system sys as training
+        samples into device buffers (incrmt_sim_learned_capture)."""
+        check(_ulib().incrmt_sim_learned_capture(self._h, sys, factor, ctypes.c_void_p(in_ptr),
+                                                 ctypes.c_void_p(target_ptr), cap))
+
+    def learned_stats(self, sys):
+        st = SimLearnedStats()
+        check(_ulib().incrmt_sim_get_learned_stats(self._h, sys, ctypes.byref(st)))
+        return st
+
     def set_windows(self, on=True):
         """Per-object windows of the level-set and reference-map passes
         (on by default); off runs every pass over the whole grid."""
@@ -481,6 +512,10 @@ class LearnedStats(ctypes.Structure):
                 ("used", ctypes.c_int)]
 
 
+class SimLearnedStats(ctypes.Structure):
+    _fields_ = [("applied", ctypes.c_longlong), ("fallback", ctypes.c_longlong), ("captured", ctypes.c_longlong)]
+
+
 def _unet_sigs(L):
     P, I, D, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float
     fp = ctypes.POINTER(ctypes.c_float)
@@ -498,6 +533,11 @@ def _unet_sigs(L):
     L.incrmt_unet_destroy.restype = None
     L.incrmt_mg_learned_guess.argtypes = [P, P, P, P, I, ctypes.POINTER(LearnedStats)]
     L.incrmt_mg_learned_input.argtypes = [P, P, P, I, P, I, I]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.incrmt_sim_set_learned.argtypes = [P, I, P, I, I]
+    L.incrmt_sim_learned_grid.argtypes = [P, I, I, ip, ip]
+    L.incrmt_sim_learned_capture.argtypes = [P, I, I, P, P, I]
+    L.incrmt_sim_get_learned_stats.argtypes = [P, I, ctypes.POINTER(SimLearnedStats)]
 
 
 def _ulib():

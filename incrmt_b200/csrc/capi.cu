@@ -106,6 +106,18 @@ int incrmt_mg_vcycle_device(incrmt_mg *h, const double *d_b, double *d_z) {
     return h->mg.vcycle64(d_b, d_z);
 }
 
+int incrmt_mg_set_tiles(incrmt_mg *h, int on) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    incrmt::Multigrid &mg = h->mg;
+    if (mg.stream) INCRMT_CK(cudaStreamSynchronize(mg.stream));
+    mg.tiles = on != 0;
+    if (mg.gexec) {  // the captured V-cycle holds the other launches
+        cudaGraphExecDestroy(mg.gexec);
+        mg.gexec = nullptr;
+    }
+    return INCRMT_OK;
+}
+
 int incrmt_mg_set_profiling(incrmt_mg *h, int on) {
     if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
     h->mg.prof = on != 0;

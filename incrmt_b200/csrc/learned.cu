@@ -1,4 +1,4 @@
-// The learned initial guess of a MAC pressure solve. From the current iterate
+// The learned initial guess of a MAC or FEM pressure solve. From the current iterate
 // z0 the residual r0 = b - A z0 is formed; its restriction to the network's
 // grid (block averages over factor x factor cells), normalised by its RMS,
 // and the restricted reciprocal density are the network's input; the output
@@ -7,9 +7,11 @@
 // energy norm of the (definite) system along d. That norm weighs the smooth
 // error the multigrid cycles remove slowest; a residual-minimising step would
 // instead be dominated by the high-frequency part of d's error, which the
-// smoother removes anyway. With alpha <= 0 the iterate is left unchanged.
-// Everything runs on the solver's stream; no host synchronisation unless
-// statistics are requested.
+// smoother removes anyway. With alpha <= 0 the iterate is left unchanged, and
+// under the residual rule also when the step would raise the residual's
+// 2-norm (the iterate then stays the previous solution). Everything runs on
+// the solver's stream; no host synchronisation unless statistics are
+// requested.
 #include <cmath>
 #include "incrmt.h"
 #include "incrmt_unet.h"
@@ -50,11 +52,13 @@ __global__ void k_sum_into(const double *partial, int nb, double *out) {
 }
 
 /** Network input on an H x W grid (NHWC, 3 channels): block averages of the
- * residual over factor x factor cells divided by its RMS (rr = sum r^2 over
- * the N cells), the block average of the cell reciprocal density (mean of its
- * left and right MAC edge values), and zero. Outside the m x n image: zero. */
-__global__ void k_learned_input(const double *r, const double *ex, int m, int n, int f, const double *rr, int H, int W,
-                                float *in) {
+ * residual over factor x factor unknowns divided by its RMS (rr = sum r^2 over
+ * the N unknowns), the block average of the reciprocal density at the
+ * unknowns (MAC: mean of a cell's left and right edge coefficients ex, an
+ * (m+1) x n array; FEM: the cell coefficient array c, m x n like the nodes),
+ * and zero. Outside the m x n image: zero. */
+__global__ void k_learned_input(const double *r, const double *dens, int fem, int m, int n, int f, const double *rr,
+                                int H, int W, float *in) {
     const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y * blockDim.y + threadIdx.y;
     if (X >= W || Y >= H) return;
     float c0 = 0, c1 = 0;
@@ -65,7 +69,8 @@ __global__ void k_learned_input(const double *r, const double *ex, int m, int n,
         for (int j = j0; j < j0 + f && j < n; j++)
             for (int i = i0; i < i0 + f && i < m; i++) {
                 sr += r[static_cast<long>(j) * m + i];
-                se += 0.5 * (ex[static_cast<long>(j) * (m + 1) + i] + ex[static_cast<long>(j) * (m + 1) + i + 1]);
+                se += fem ? dens[static_cast<long>(j) * m + i]
+                          : 0.5 * (dens[static_cast<long>(j) * (m + 1) + i] + dens[static_cast<long>(j) * (m + 1) + i + 1]);
                 cnt++;
             }
         const double rms = sqrt(*rr / (static_cast<double>(m) * n));
@@ -96,13 +101,42 @@ __global__ void k_learned_prolong(const float *out, int H, int W, int m, int n, 
 }
 
 /** z += alpha d with alpha = dots[0] / dots[1] (d.r0 over d.Ad) when
- * positive and finite. */
-__global__ void k_learned_update(double *z, const double *d, long n, const double *dots) {
+ * positive and finite and, under the residual rule (rule 0), when the new
+ * residual |r0 - alpha Ad|^2 = dots[2] - 2 alpha dots[3] + alpha^2 dots[4]
+ * is no larger than |r0|^2 = dots[2]. cnt (optional) counts the applied
+ * guesses in cnt[0] and the fallbacks in cnt[1]. */
+__global__ void k_learned_update(double *z, const double *d, long n, const double *dots, int rule,
+                                 unsigned long long *cnt) {
     const double a = dots[1] != 0 ? dots[0] / dots[1] : 0.0;
-    if (!(a > 0) || !isfinite(a)) return;
+    bool ok = a > 0 && isfinite(a);
+    if (ok && rule == 0) ok = dots[2] - 2 * a * dots[3] + a * a * dots[4] <= dots[2];
+    if (cnt && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&cnt[ok ? 0 : 1], 1ull);
+    if (!ok) return;
     for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long>(gridDim.x) * blockDim.x)
         z[i] += a * d[i];
+}
+
+/** Training target on the network grid: block averages of znew - zold over
+ * factor x factor unknowns (zero outside the m x n image). */
+__global__ void k_learned_target(const double *znew, const double *zold, int m, int n, int f, int H, int W,
+                                 float *tgt) {
+    const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (X >= W || Y >= H) return;
+    const int i0 = X * f, j0 = Y * f;
+    float v = 0.f;
+    if (i0 < m && j0 < n) {
+        double s = 0;
+        int cnt = 0;
+        for (int j = j0; j < j0 + f && j < n; j++)
+            for (int i = i0; i < i0 + f && i < m; i++) {
+                const long q = static_cast<long>(j) * m + i;
+                s += znew[q] - zold[q];
+                cnt++;
+            }
+        v = static_cast<float>(s / cnt);
+    }
+    tgt[static_cast<long>(Y) * W + X] = v;
 }
 
 constexpr int kRed = 2 * kB200SMs;
@@ -138,26 +172,62 @@ int dot(const double *x, const double *y, long n, double *partial, double *out, 
 
 }  // namespace
 
-/** Network grid of a solve: the m x n cells restricted by `factor`, rounded up
- * to multiples of 16. */
-inline void learned_grid(int m, int n, int f, int &H, int &W) {
+void learned_grid(int m, int n, int f, int &H, int &W) {
     W = ((m + f - 1) / f + 15) / 16 * 16;
     H = ((n + f - 1) / f + 15) / 16 * 16;
 }
 
-/** Residual and input features (k_learned_input) into w.in. */
+int learned_supported(const Multigrid &mg) {
+    if (mg.px) { set_error("learned guess: x-periodic systems are not supported"); return INCRMT_ERR_BADARG; }
+    return INCRMT_OK;
+}
+
 int learned_input(Multigrid &mg, LearnedWork &w, const double *d_b, const double *d_z, int f, int H, int W) {
     const long N = static_cast<long>(mg.m) * mg.n;
     int r = ensure(w, N, static_cast<long>(H) * W);
     if (r) return r;
+    if ((r = mg.effective_rhs(d_b, &d_b))) return r;
     if ((r = mg.apply_device(d_z, w.ad))) return r;
     cudaStream_t s = mg.stream;
     k_sub<<<kRed, 256, 0, s>>>(d_b, w.ad, w.r0, N);
     if ((r = dot(w.r0, w.r0, N, w.dots + 8, w.dots + 2, s))) return r;
-    k_learned_input<<<dim3(cdiv(W, 32), cdiv(H, 8)), dim3(32, 8), 0, s>>>(w.r0, mg.ex, mg.m, mg.n, f, w.dots + 2, H, W,
-                                                                          w.in);
+    const bool fem = mg.sys == INCRMT_SYS_FEM;
+    k_learned_input<<<dim3(cdiv(W, 32), cdiv(H, 8)), dim3(32, 8), 0, s>>>(w.r0, fem ? mg.c : mg.ex, fem ? 1 : 0, mg.m,
+                                                                          mg.n, f, w.dots + 2, H, W, w.in);
     mg.launches += 4;
     INCRMT_CKL("k_learned_input");
+    return INCRMT_OK;
+}
+
+int learned_guess(Multigrid &mg, LearnedWork &w, incrmt_unet *net, const double *d_b, double *d_z, int f, int rule,
+                  unsigned long long *cnt) {
+    int H, W;
+    learned_grid(mg.m, mg.n, f, H, W);
+    int r = learned_input(mg, w, d_b, d_z, f, H, W);
+    if (r) return r;
+    cudaStream_t s = mg.stream;
+    if ((r = incrmt_unet_forward(net, 1, H, W, w.in, w.out, s))) return r;
+    const long N = static_cast<long>(mg.m) * mg.n;
+    k_learned_prolong<<<dim3(cdiv(mg.m, 32), cdiv(mg.n, 8)), dim3(32, 8), 0, s>>>(w.out, H, W, mg.m, mg.n, f,
+                                                                                  w.dfine);
+    mg.launches++;
+    if ((r = mg.apply_device(w.dfine, w.ad))) return r;
+    // dots: [0] d.r0, [1] d.Ad, [2] r0.r0, [3] Ad.r0, [4] Ad.Ad
+    if ((r = dot(w.dfine, w.r0, N, w.dots + 8, w.dots, s))) return r;
+    if ((r = dot(w.dfine, w.ad, N, w.dots + 8, w.dots + 1, s))) return r;
+    if ((r = dot(w.ad, w.r0, N, w.dots + 8, w.dots + 3, s))) return r;
+    if ((r = dot(w.ad, w.ad, N, w.dots + 8, w.dots + 4, s))) return r;
+    k_learned_update<<<kRed, 256, 0, s>>>(d_z, w.dfine, N, w.dots, rule, cnt);
+    mg.launches += 10;
+    INCRMT_CKL("k_learned_update");
+    return INCRMT_OK;
+}
+
+int learned_target(Multigrid &mg, const double *znew, const double *zold, int f, int H, int W, float *tgt) {
+    k_learned_target<<<dim3(cdiv(W, 32), cdiv(H, 8)), dim3(32, 8), 0, mg.stream>>>(znew, zold, mg.m, mg.n, f, H, W,
+                                                                                   tgt);
+    mg.launches++;
+    INCRMT_CKL("k_learned_target");
     return INCRMT_OK;
 }
 
@@ -169,10 +239,7 @@ int incrmt_mg_learned_input(incrmt_mg *h, const double *d_b, const double *d_z, 
                             int W) {
     if (!h || !d_b || !d_z || !d_in) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
     incrmt::Multigrid &mg = h->mg;
-    if (mg.sys != INCRMT_SYS_MAC || mg.px || mg.py) {
-        incrmt::set_error("learned guess: non-periodic MAC systems only");
-        return INCRMT_ERR_BADARG;
-    }
+    if (int r = incrmt::learned_supported(mg)) return r;
     int Hn, Wn;
     incrmt::learned_grid(mg.m, mg.n, factor, Hn, Wn);
     if (factor < 1 || H != Hn || W != Wn) {
@@ -190,35 +257,15 @@ int incrmt_mg_learned_guess(incrmt_mg *h, incrmt_unet *net, const double *d_b, d
                             incrmt_learned_stats *st) {
     if (!h || !net || !d_b || !d_z) { incrmt::set_error("null argument"); return INCRMT_ERR_BADARG; }
     incrmt::Multigrid &mg = h->mg;
-    if (mg.sys != INCRMT_SYS_MAC || mg.px || mg.py) {
-        incrmt::set_error("learned guess: non-periodic MAC systems only");
-        return INCRMT_ERR_BADARG;
-    }
+    if (int r = incrmt::learned_supported(mg)) return r;
     if (factor < 1) { incrmt::set_error("bad factor %d", factor); return INCRMT_ERR_BADARG; }
-    int H, W;
-    incrmt::learned_grid(mg.m, mg.n, factor, H, W);
     incrmt::LearnedWork &w = h->learned;
-    int r = incrmt::learned_input(mg, w, d_b, d_z, factor, H, W);
+    int r = incrmt::learned_guess(mg, w, net, d_b, d_z, factor, 1, nullptr);
     if (r) return r;
-    cudaStream_t s = mg.stream;
-    if ((r = incrmt_unet_forward(net, 1, H, W, w.in, w.out, s))) return r;
-    const long N = static_cast<long>(mg.m) * mg.n;
-    incrmt::k_learned_prolong<<<dim3(incrmt::cdiv(mg.m, 32), incrmt::cdiv(mg.n, 8)), dim3(32, 8), 0, s>>>(
-        w.out, H, W, mg.m, mg.n, factor, w.dfine);
-    mg.launches++;
-    if ((r = mg.apply_device(w.dfine, w.ad))) return r;
-    // dots: [0] d.r0, [1] d.Ad, [2] r0.r0, [3] Ad.r0, [4] Ad.Ad
-    if ((r = incrmt::dot(w.dfine, w.r0, N, w.dots + 8, w.dots, s))) return r;
-    if ((r = incrmt::dot(w.dfine, w.ad, N, w.dots + 8, w.dots + 1, s))) return r;
-    if ((r = incrmt::dot(w.ad, w.r0, N, w.dots + 8, w.dots + 3, s))) return r;
-    if ((r = incrmt::dot(w.ad, w.ad, N, w.dots + 8, w.dots + 4, s))) return r;
-    incrmt::k_learned_update<<<incrmt::kRed, 256, 0, s>>>(d_z, w.dfine, N, w.dots);
-    mg.launches += 10;
-    INCRMT_CKL("k_learned_update");
     if (st) {
         double hd[5];
-        INCRMT_CK(cudaMemcpyAsync(hd, w.dots, sizeof(hd), cudaMemcpyDeviceToHost, s));
-        INCRMT_CK(cudaStreamSynchronize(s));
+        INCRMT_CK(cudaMemcpyAsync(hd, w.dots, sizeof(hd), cudaMemcpyDeviceToHost, mg.stream));
+        INCRMT_CK(cudaStreamSynchronize(mg.stream));
         const double a = hd[1] != 0 ? hd[0] / hd[1] : 0.0;
         const bool used = a > 0 && std::isfinite(a);
         st->alpha = used ? a : 0.0;

@@ -183,23 +183,35 @@ __global__ void k_smooth(Op op, T *z, const T *b, int m, int n, int pi, int pj) 
     z[ij] = (b[ij] - off) / diag;
 }
 
-/** Tile-fused Gauss-Seidel: SWEEPS complete four-colour sweeps in one launch
- * for a non-periodic grid. The block stages its TW x TH tile of the iterate
- * plus a halo of 4*SWEEPS cells in shared memory and runs the colour phases
- * there, phase p updating the tile grown by 4*SWEEPS-1-p cells, so that every
- * value a later phase reads is already final; the tile is then written back.
- * Each point sees exactly the neighbour values of the one-launch-per-colour
- * schedule, so the result is identical to it. Coefficients and the right-hand
- * side are read from global memory (L1/L2). */
+/** Index i of a periodic direction of size m brought into [0, m). */
+__device__ __forceinline__ int wrap_index(int i, int m) {
+    i %= m;
+    return i < 0 ? i + m : i;
+}
+
+/** Tile-fused Gauss-Seidel: SWEEPS complete four-colour sweeps in one launch.
+ * The block stages its TW x TH tile of the iterate zin plus a halo of
+ * 4*SWEEPS cells in shared memory and runs the colour phases there, phase p
+ * updating the tile grown by 4*SWEEPS-1-p cells, so that every value a later
+ * phase reads is already final; the tile is then written to zout. zin is not
+ * written during the launch, so every block stages the values from before the
+ * sweeps and each point sees exactly the neighbour values of the
+ * one-launch-per-colour schedule: the result is identical to it. In a
+ * periodic direction (even size) the halo holds periodic images, updated like
+ * the points they copy (the colouring is consistent across the seam).
+ * Coefficients and the right-hand side are read from global memory (L1/L2). */
 template <class Op, class T, int SWEEPS, int TW, int TH>
-__global__ void __launch_bounds__(256) k_smooth_tile(Op op, T *z, const T *b, int m, int n) {
+__global__ void __launch_bounds__(256) k_smooth_tile(Op op, const T *zin, T *zout, const T *b, int m, int n) {
     constexpr int H = 4 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H;
     __shared__ T zs[LW * LH];
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
     const int gx0 = x0 - H, gy0 = y0 - H;
+    const bool px = op.px, py = op.py;
     for (int t = threadIdx.x; t < LW * LH; t += blockDim.x) {
-        const int li = t % LW, lj = t / LW, i = gx0 + li, j = gy0 + lj;
-        if (i >= 0 && i < m && j >= 0 && j < n) zs[t] = z[i + static_cast<long>(m) * j];
+        int i = gx0 + t % LW, j = gy0 + t / LW;
+        if (px) i = wrap_index(i, m);
+        if (py) j = wrap_index(j, n);
+        if (i >= 0 && i < m && j >= 0 && j < n) zs[t] = zin[i + static_cast<long>(m) * j];
     }
     __syncthreads();
     const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
@@ -208,25 +220,30 @@ __global__ void __launch_bounds__(256) k_smooth_tile(Op op, T *z, const T *b, in
     for (int p = 0; p < P; p++) {
         const int e = P - 1 - p, c = p & 3;
         int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
-        if (ilo < 0) ilo = 0;
-        if (jlo < 0) jlo = 0;
-        if (ihi > m - 1) ihi = m - 1;
-        if (jhi > n - 1) jhi = n - 1;
+        if (!px) {
+            if (ilo < 0) ilo = 0;
+            if (ihi > m - 1) ihi = m - 1;
+        }
+        if (!py) {
+            if (jlo < 0) jlo = 0;
+            if (jhi > n - 1) jhi = n - 1;
+        }
         // first index of the colour's parity at or above the low bound
         const int i0 = ilo + ((ilo & 1) != pis[c]), j0 = jlo + ((jlo & 1) != pjs[c]);
         const int ni = i0 <= ihi ? (ihi - i0) / 2 + 1 : 0, nj = j0 <= jhi ? (jhi - j0) / 2 + 1 : 0;
         for (int t = threadIdx.x; t < ni * nj; t += blockDim.x) {
             const int i = i0 + 2 * (t % ni), j = j0 + 2 * (t / ni);
             const int lz = (i - gx0) + LW * (j - gy0);
+            const int ir = px ? wrap_index(i, m) : i, jr = py ? wrap_index(j, n) : j;
             T diag;
-            const T off = op.offdiag_s(i, j, zs, lz, LW, diag);
-            zs[lz] = (b[i + static_cast<long>(m) * j] - off) / diag;
+            const T off = op.offdiag_s(ir, jr, zs, lz, LW, diag);
+            zs[lz] = (b[ir + static_cast<long>(m) * jr] - off) / diag;
         }
         __syncthreads();
     }
     for (int t = threadIdx.x; t < TW * TH; t += blockDim.x) {
         const int i = x0 + t % TW, j = y0 + t / TW;
-        if (i < m && j < n) z[i + static_cast<long>(m) * j] = zs[(i - gx0) + LW * (j - gy0)];
+        if (i < m && j < n) zout[i + static_cast<long>(m) * j] = zs[(i - gx0) + LW * (j - gy0)];
     }
 }
 
@@ -235,20 +252,24 @@ __global__ void __launch_bounds__(256) k_smooth_tile(Op op, T *z, const T *b, in
  * so the four-colour sweep is exactly two half-sweeps over (i+j) even, then
  * odd, with bitwise the same results. SWEEPS sweeps take 2*SWEEPS phases, so
  * the halo is 2*SWEEPS cells. Threads walk the tile as 32 x 8 (x fastest),
- * each row of a phase holding every second point. */
+ * each row of a phase holding every second point. Reads zin, writes zout, and
+ * handles periodic directions (even sizes) like k_smooth_tile. */
 template <class Op, class T, int SWEEPS, int TW, int TH>
-__global__ void __launch_bounds__(256) k_smooth_rb(Op op, T *z, const T *b, int m, int n) {
+__global__ void __launch_bounds__(256) k_smooth_rb(Op op, const T *zin, T *zout, const T *b, int m, int n) {
     constexpr int H = 2 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H, NP = 2 * SWEEPS;
     __shared__ T zs[LW * LH];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
     const int gx0 = x0 - H, gy0 = y0 - H;
+    const bool px = op.px, py = op.py;
     for (int lj = ty; lj < LH; lj += 8) {
-        const int j = gy0 + lj;
+        int j = gy0 + lj;
+        if (py) j = wrap_index(j, n);
         if (j < 0 || j >= n) continue;
         for (int li = tx; li < LW; li += 32) {
-            const int i = gx0 + li;
-            if (i >= 0 && i < m) zs[li + LW * lj] = z[i + static_cast<long>(m) * j];
+            int i = gx0 + li;
+            if (px) i = wrap_index(i, m);
+            if (i >= 0 && i < m) zs[li + LW * lj] = zin[i + static_cast<long>(m) * j];
         }
     }
     __syncthreads();
@@ -256,17 +277,23 @@ __global__ void __launch_bounds__(256) k_smooth_rb(Op op, T *z, const T *b, int 
     for (int p = 0; p < NP; p++) {
         const int e = NP - 1 - p, parity = p & 1;
         int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
-        if (ilo < 0) ilo = 0;
-        if (jlo < 0) jlo = 0;
-        if (ihi > m - 1) ihi = m - 1;
-        if (jhi > n - 1) jhi = n - 1;
+        if (!px) {
+            if (ilo < 0) ilo = 0;
+            if (ihi > m - 1) ihi = m - 1;
+        }
+        if (!py) {
+            if (jlo < 0) jlo = 0;
+            if (jhi > n - 1) jhi = n - 1;
+        }
         for (int j = jlo + ty; j <= jhi; j += 8) {
             const int i0 = ilo + (((ilo + j) & 1) != parity);
+            const int jr = py ? wrap_index(j, n) : j;
             for (int i = i0 + 2 * tx; i <= ihi; i += 64) {
                 const int lz = (i - gx0) + LW * (j - gy0);
+                const int ir = px ? wrap_index(i, m) : i;
                 T diag;
-                const T off = op.offdiag_s(i, j, zs, lz, LW, diag);
-                zs[lz] = (b[i + static_cast<long>(m) * j] - off) / diag;
+                const T off = op.offdiag_s(ir, jr, zs, lz, LW, diag);
+                zs[lz] = (b[ir + static_cast<long>(m) * jr] - off) / diag;
             }
         }
         __syncthreads();
@@ -276,7 +303,7 @@ __global__ void __launch_bounds__(256) k_smooth_rb(Op op, T *z, const T *b, int 
         if (j >= n) break;
         for (int li = H + tx; li < H + TW; li += 32) {
             const int i = gx0 + li;
-            if (i < m) z[i + static_cast<long>(m) * j] = zs[li + LW * lj];
+            if (i < m) zout[i + static_cast<long>(m) * j] = zs[li + LW * lj];
         }
     }
 }
@@ -683,13 +710,17 @@ constexpr int kRedBlocks = 4 * kB200SMs;  // reduction grid: 4 x 148 blocks of 2
 inline dim3 grid2(int m, int n) { return dim3(cdiv(m, 32), cdiv(n, 8)); }
 const dim3 kBlk2(32, 8);
 
-/** Runs `sweeps` four-colour sweeps. When prof is given, each launch is
- * bracketed by CUDA events and credited with its algorithmic bytes:
- * (units updated) x bytes_per_unit. */
+/** Runs `sweeps` four-colour sweeps on the iterate z. Two sweeps on a grid
+ * whose periodic directions have even sizes run as one tile-fused launch that
+ * reads z and writes zalt (*res = zalt); otherwise one launch per colour
+ * updates z in place (*res = z). When prof is given, each launch is bracketed
+ * by CUDA events and credited with its algorithmic bytes: (units updated) x
+ * bytes_per_unit. */
 template <class Op, class T>
-int smooth(Op op, T *z, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl,
+int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl, T **res,
            Multigrid *prof = nullptr, double bytes_per_unit = 0) {
-    if (!op.px && !op.py && sweeps == 2) {
+    *res = z;
+    if (sweeps == 2 && zalt && (!op.px || m % 2 == 0) && (!op.py || n % 2 == 0)) {
         // Two sweeps per launch with shared-memory tiles (identical results);
         // the largest tile that still gives every SM work, else the smallest.
         const dim3 b64(cdiv(m, 64), cdiv(n, 32)), b32(cdiv(m, 32), cdiv(n, 16)), b16(cdiv(m, 16), cdiv(n, 16));
@@ -697,20 +728,21 @@ int smooth(Op op, T *z, const T *b, int m, int n, int sweeps, cudaStream_t s, lo
         bool done = false;
         if constexpr (Op::kFivePoint) {
             if (static_cast<int>(b64.x * b64.y) >= 2 * kB200SMs) {
-                k_smooth_rb<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, b, m, n);
+                k_smooth_rb<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, zalt, b, m, n);
                 done = true;
             }
         }
         if (done) {
         } else if (static_cast<int>(b64.x * b64.y) >= 2 * kB200SMs)
-            k_smooth_tile<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, b, m, n);
+            k_smooth_tile<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, zalt, b, m, n);
         else if (static_cast<int>(b32.x * b32.y) >= kB200SMs)
-            k_smooth_tile<Op, T, 2, 32, 16><<<b32, 256, 0, s>>>(op, z, b, m, n);
+            k_smooth_tile<Op, T, 2, 32, 16><<<b32, 256, 0, s>>>(op, z, zalt, b, m, n);
         else
-            k_smooth_tile<Op, T, 2, 16, 16><<<b16, 256, 0, s>>>(op, z, b, m, n);
+            k_smooth_tile<Op, T, 2, 16, 16><<<b16, 256, 0, s>>>(op, z, zalt, b, m, n);
         nl++;
         if (prof) { int r = prof->prof_end(); if (r) return r; }
         INCRMT_CKL("k_smooth_tile");
+        *res = zalt;
         return INCRMT_OK;
     }
     const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
@@ -795,6 +827,8 @@ int Multigrid::build_hierarchy() {
     MgLevel L0; L0.m = m; L0.n = n; L0.N = static_cast<long>(m) * n;
     INCRMT_CK(cudaMalloc(&L0.zf, sizeof(float) * L0.N));
     INCRMT_CK(cudaMalloc(&L0.bf, sizeof(float) * L0.N));
+    INCRMT_CK(cudaMalloc(&L0.z2, sizeof(double) * L0.N));
+    INCRMT_CK(cudaMalloc(&L0.zf2, sizeof(float) * L0.N));
     lev.push_back(L0);
     int mm = m, nn = n;
     while (static_cast<int>(lev.size()) < kMaxLevels && mm * nn > kCoarsestSize) {
@@ -809,6 +843,8 @@ int Multigrid::build_hierarchy() {
         INCRMT_CK(cudaMalloc(&L.zf, sizeof(float) * L.N));
         INCRMT_CK(cudaMalloc(&L.bf, sizeof(float) * L.N));
         INCRMT_CK(cudaMalloc(&L.stf, sizeof(float) * 9 * L.N));
+        INCRMT_CK(cudaMalloc(&L.z2, sizeof(double) * L.N));
+        INCRMT_CK(cudaMalloc(&L.zf2, sizeof(float) * L.N));
         lev.push_back(L);
         mm = mc; nn = nc;
     }
@@ -834,6 +870,7 @@ int Multigrid::build_hierarchy() {
 void Multigrid::destroy() {
     for (auto &L : lev) {
         cudaFree(L.z); cudaFree(L.b); cudaFree(L.st); cudaFree(L.zf); cudaFree(L.bf); cudaFree(L.stf);
+        cudaFree(L.z2); cudaFree(L.zf2);
     }
     lev.clear();
     cudaFree(ex); cudaFree(ey); cudaFree(exf); cudaFree(eyf); cudaFree(c); cudaFree(cf);
@@ -912,27 +949,36 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
     // Algorithmic bytes per updated unknown of a fine FP64 sweep: read z,b
     // and the coefficient words, write z (3+c words; c=2 MAC, c=1 FEM).
     const double bpu = 8.0 * (sys == INCRMT_SYS_MAC ? 5 : 4);
+    // Pre-smoothing may leave the iterate in the level's second buffer; the
+    // restriction, prolongation and post-smoothing follow it, and the
+    // post-smoothing brings it back (both smoothings use the same kind of
+    // launch, so the two moves cancel).
+    double *cur = z;
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac64();
-        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches, pf, bpu))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, z, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
     } else if (l == 0) {
         auto op = fem64();
-        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches, pf, bpu))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, z, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
     } else {
-        if ((r = smooth(g, z, b, L.m, L.n, kNu1, stream, launches))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, z, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        if ((r = smooth(g, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
     }
     launches++;
     INCRMT_CKL("k_restrict");
     if ((r = cycle64(l + 1, b0, z0))) return r;
-    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(z, L.m, L.n, px, py, L.kx, L.ky, static_cast<const double *>(C.z), C.m, C.n);
+    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(cur, L.m, L.n, px, py, L.kx, L.ky, static_cast<const double *>(C.z), C.m, C.n);
     launches++;
     INCRMT_CKL("k_prolong");
-    if (l == 0 && sys == INCRMT_SYS_MAC) return smooth(mac64(), z, b, L.m, L.n, kNu2, stream, launches, pf, bpu);
-    if (l == 0) return smooth(fem64(), z, b, L.m, L.n, kNu2, stream, launches, pf, bpu);
-    return smooth(g, z, b, L.m, L.n, kNu2, stream, launches);
+    double *alt = !tiles ? nullptr : cur == z ? L.z2 : z, *out = cur;
+    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac64(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
+    else if (l == 0) r = smooth(fem64(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
+    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
+    if (r) return r;
+    if (out != z) INCRMT_CK(cudaMemcpyAsync(z, out, sizeof(double) * L.N, cudaMemcpyDeviceToDevice, stream));
+    return INCRMT_OK;
 }
 
 int Multigrid::prof_begin(double bytes) {
@@ -992,27 +1038,32 @@ int Multigrid::cycle32(int l) {
     }
     const MgLevel &C = lev[l + 1];
     int r;
+    float *cur = z;  // as in cycle64
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac32();
-        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(z), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
     } else if (l == 0) {
         auto op = fem32();
-        if ((r = smooth(op, z, b, L.m, L.n, kNu1, stream, launches))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(z), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
     } else {
-        if ((r = smooth(g, z, b, L.m, L.n, kNu1, stream, launches))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, static_cast<const float *>(z), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
     }
     launches++;
     INCRMT_CKL("k_restrict");
     if ((r = cycle32(l + 1))) return r;
-    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(z, L.m, L.n, px, py, L.kx, L.ky, static_cast<const float *>(C.zf), C.m, C.n);
+    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(cur, L.m, L.n, px, py, L.kx, L.ky, static_cast<const float *>(C.zf), C.m, C.n);
     launches++;
     INCRMT_CKL("k_prolong");
-    if (l == 0 && sys == INCRMT_SYS_MAC) return smooth(mac32(), z, b, L.m, L.n, kNu2, stream, launches);
-    if (l == 0) return smooth(fem32(), z, b, L.m, L.n, kNu2, stream, launches);
-    return smooth(g, z, b, L.m, L.n, kNu2, stream, launches);
+    float *alt = !tiles ? nullptr : cur == z ? L.zf2 : z, *out = cur;
+    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
+    else if (l == 0) r = smooth(fem32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
+    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
+    if (r) return r;
+    if (out != z) INCRMT_CK(cudaMemcpyAsync(z, out, sizeof(float) * L.N, cudaMemcpyDeviceToDevice, stream));
+    return INCRMT_OK;
 }
 
 /** Shared-memory layout of the tail: the coarsest levels, from the bottom
@@ -1119,6 +1170,18 @@ int Multigrid::vcycle_and_norm(int prec, const double *b, double *d_z, long N) {
 int Multigrid::vcycle64(const double *d_b, double *d_z) {
     if (!ready) { set_error("density not set"); return INCRMT_ERR_BADARG; }
     return cycle64(0, d_b, d_z);
+}
+
+int Multigrid::effective_rhs(const double *d_b, const double **out) {
+    *out = d_b;
+    if (sys != INCRMT_SYS_FEM || !zpr) return INCRMT_OK;
+    const long N = static_cast<long>(m) * n;
+    if (d_b != bbuf) INCRMT_CK(cudaMemcpyAsync(bbuf, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
+    k_zero_column<<<cdiv(n, 256), 256, 0, stream>>>(bbuf, m, n);
+    launches++;
+    INCRMT_CKL("zero column");
+    *out = bbuf;
+    return INCRMT_OK;
 }
 
 int Multigrid::apply_device(const double *d_z, double *d_out) {

@@ -14,6 +14,7 @@
 #pragma once
 #include <vector>
 #include "common.cuh"
+#include "incrmt_unet.h"
 #include "mg_ops.cuh"
 
 namespace incrmt {
@@ -24,6 +25,8 @@ struct MgLevel {
     bool kx = false, ky = false;  // whether the next level halves x / y
     double *z = nullptr, *b = nullptr, *st = nullptr;  // FP64 arrays (level >= 1)
     float *zf = nullptr, *bf = nullptr, *stf = nullptr;  // FP32 arrays (all levels)
+    double *z2 = nullptr;  // second FP64 iterate buffer of the tile smoothers (all levels)
+    float *zf2 = nullptr;  // and the FP32 one
 };
 
 class Multigrid {
@@ -50,6 +53,7 @@ public:
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
     bool ready = false;              // coefficients and hierarchy built
+    bool tiles = true;               // tile-fused smoothing where it applies
     int tail_level = -1;             // first level run by the one-block tail kernel
     cudaGraphExec_t gexec = nullptr; // captured V-cycle + norm
     int gkey_prec = -1;
@@ -77,6 +81,9 @@ public:
                      incrmt_mg_stats *st, bool time_it);
     int vcycle64(const double *d_b, double *d_z);
     int apply_device(const double *d_z, double *d_out);
+    /** The right-hand side the solve uses: d_b itself, or for the FEM system
+     * with the zero-pressure column a copy in bbuf with that column zeroed. */
+    int effective_rhs(const double *d_b, const double **out);
 
     MacOp<double> mac64() const;
     MacOp<float> mac32() const;
@@ -103,6 +110,20 @@ struct LearnedWork {
     long n_fine = 0, n_net = 0;
     void release();
 };
+
+/** Network grid of a solve: the m x n unknowns restricted by f, rounded up to
+ * multiples of 16. */
+void learned_grid(int m, int n, int f, int &H, int &W);
+/** INCRMT_OK, or an error for systems the guess does not handle (x-periodic). */
+int learned_supported(const Multigrid &mg);
+/** r0 = b - A z and the network input features into w.in (H x W x 3). */
+int learned_input(Multigrid &mg, LearnedWork &w, const double *d_b, const double *d_z, int f, int H, int W);
+/** The whole guess: features, network, prolongation, step along d (rule 0:
+ * residual rule, 1: energy rule only), optional applied/fallback counters. */
+int learned_guess(Multigrid &mg, LearnedWork &w, incrmt_unet *net, const double *d_b, double *d_z, int f, int rule,
+                  unsigned long long *cnt);
+/** Block averages of znew - zold on the network grid (training targets). */
+int learned_target(Multigrid &mg, const double *znew, const double *zold, int f, int H, int W, float *tgt);
 
 }  // namespace incrmt
 

@@ -44,17 +44,18 @@ struct MacOp {
     }
 
     /** offdiag with the iterate in a shared-memory tile (lz: local index of
-     * (i,j), ldz: tile row stride); for non-periodic grids. */
+     * (i,j), ldz: tile row stride). The tile holds the neighbours at lz+-1,
+     * lz+-ldz, across a periodic edge too (as periodic images). */
     __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
         const T el = ex[j * (m + 1) + i], er = ex[j * (m + 1) + i + 1];
         const T ed = ey[j * m + i], eu = ey[(j + 1) * m + i];
-        const bool l = i > 0, r = i < m - 1, d = j > 0, u = j < n - 1;
+        const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         T sx = 0, sy = 0;
         if (l) sx = el * zs[lz - 1];
         if (r) sx += er * zs[lz + 1];
         if (d) sy = ed * zs[lz - ldz];
         if (u) sy += eu * zs[lz + ldz];
-        diag = -xxsp * ((l ? el : T(0)) + (i < m - 1 ? er : (zpr ? 2 * er : T(0))))
+        diag = -xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0)))))
                - yysp * ((d ? ed : T(0)) + (u ? eu : T(0)));
         return xxsp * sx + yysp * sy;
     }
@@ -133,7 +134,7 @@ struct FemOp {
         T a[9];
         coef9(i, j, a);
         diag = a[4];
-        const bool l = i > 0, r = i < m - 1, d = j > 0, u = j < n - 1;
+        const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         T t = 0;
         if (d) {
             if (l) t += a[0] * zs[lz - ldz - 1];
@@ -202,7 +203,7 @@ struct GenOp {
 
     __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
         const int ij = i + m * j;
-        const bool l = i > 0, r = i < m - 1, d = j > 0, u = j < n - 1;
+        const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         diag = st[4 * N + ij];
         T t = 0;
         if (d) {

@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 #include "incrmt_sim.h"
+#include "incrmt_unet.h"
 #include "mg.cuh"
 #include "step_kernels.cuh"
 #include "ls_kernels.cuh"
@@ -48,6 +49,19 @@ struct Sim {
     double *tm = nullptr, *otm = nullptr;          // passive and object tracers
     int ntrace = 0, nobjtr = 0;
     Multigrid mac, fem;
+    // Learned warm start of each projection (0 MAC, 1 FEM) and the capture of
+    // training samples (network input and target per projection).
+    struct Learned {
+        incrmt_unet *net = nullptr;
+        int factor = 0, rule = 0;
+        LearnedWork w;
+        float *cap_in = nullptr, *cap_tgt = nullptr;
+        int cap = 0, cap_factor = 0;
+        long long captured = 0;
+        double *z0 = nullptr;  // the warm start, kept for the capture's target
+        long z0_n = 0;
+    } learn[2];
+    unsigned long long *d_lcnt = nullptr;  // [sys][applied, fallback]
     incrmt_mg_opts mgo{1e-9, 200, INCRMT_PREC_FP64};
     double dt_reg = 0, time = 0;
     double w_scale = 3, w_force = 20, tw = 2.5, pinw = 2.5;
@@ -156,6 +170,8 @@ struct Sim {
     int record_track();
     int fetch_flags();
     int update_velocity(double dt);
+    int learned_pre(int sys, const double *b, double *z);
+    int learned_post(int sys, const double *z);
     int win_reset();
     int win_update();
     TileObjs tiles() const {
@@ -245,6 +261,8 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     INCRMT_CK(cudaMalloc(&d_flags, sizeof(int) * 16));
     INCRMT_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * 16, stream));
     INCRMT_CK(cudaMallocHost(&h_flags, sizeof(int) * 16));
+    INCRMT_CK(cudaMalloc(&d_lcnt, sizeof(unsigned long long) * 4));
+    INCRMT_CK(cudaMemsetAsync(d_lcnt, 0, sizeof(unsigned long long) * 4, stream));
     INCRMT_CK(cudaMalloc(&d_win, sizeof(LsWin) * 4 * kMaxObjects));
     INCRMT_CK(cudaMallocHost(&h_win, sizeof(LsWin) * 4 * kMaxObjects));
     INCRMT_CK(cudaMalloc(&d_lsbox, sizeof(int) * 4 * kMaxObjects));
@@ -617,7 +635,9 @@ int Sim::mac_projection() {
     if ((r = phase_begin(outer))) return r;
     incrmt_mg_stats st{};
     long long l0 = mac.launches;
+    if ((r = learned_pre(INCRMT_SYS_MAC, src_mac, z_mac))) return r;
     r = mac.solve_device(src_mac, z_mac, &mgo, &st, false);
+    if (!r) r = learned_post(INCRMT_SYS_MAC, z_mac);
     launches += mac.launches - l0;
     vc_mac += st.vcycles;
     solves_mac++;
@@ -630,6 +650,48 @@ int Sim::mac_projection() {
 
 /** fluid_2d::finite_element_projection + copy_pressure
  * (fluid_2d.cc:1297-1328). */
+/** Before a projection's solve: a training capture (the network input of
+ * the warm start, which is kept), or the learned guess applied to the warm
+ * start, counted as applied or fallen back in d_lcnt. */
+int Sim::learned_pre(int sys, const double *b, double *z) {
+    Learned &L = learn[sys];
+    Multigrid &mg = sys == INCRMT_SYS_MAC ? mac : fem;
+    if (L.cap > 0 && L.captured < L.cap) {
+        int H, W;
+        learned_grid(mg.m, mg.n, L.cap_factor, H, W);
+        const long N = static_cast<long>(mg.m) * mg.n;
+        if (L.z0_n < N) {
+            cudaFree(L.z0);
+            L.z0 = nullptr;
+            L.z0_n = 0;
+            INCRMT_CK(cudaMalloc(&L.z0, sizeof(double) * N));
+            L.z0_n = N;
+        }
+        INCRMT_CK(cudaMemcpyAsync(L.z0, z, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
+        int r = learned_input(mg, L.w, b, z, L.cap_factor, H, W);
+        if (r) return r;
+        INCRMT_CK(cudaMemcpyAsync(L.cap_in + static_cast<size_t>(L.captured) * H * W * 3, L.w.in,
+                                  sizeof(float) * H * W * 3, cudaMemcpyDeviceToDevice, stream));
+        return INCRMT_OK;
+    }
+    if (!L.net) return INCRMT_OK;
+    return learned_guess(mg, L.w, L.net, b, z, L.factor, L.rule, d_lcnt + 2 * sys);
+}
+
+/** After a solve under capture: the target (block averages of the solution
+ * minus the warm start). */
+int Sim::learned_post(int sys, const double *z) {
+    Learned &L = learn[sys];
+    if (!(L.cap > 0 && L.captured < L.cap)) return INCRMT_OK;
+    Multigrid &mg = sys == INCRMT_SYS_MAC ? mac : fem;
+    int H, W;
+    learned_grid(mg.m, mg.n, L.cap_factor, H, W);
+    int r = learned_target(mg, z, L.z0, L.cap_factor, H, W, L.cap_tgt + static_cast<size_t>(L.captured) * H * W);
+    if (r) return r;
+    L.captured++;
+    return INCRMT_OK;
+}
+
 int Sim::fem_projection(double dt) {
     k_fem_ghosts<<<1, 1024, 0, stream>>>(g, f);
     k_fem_source<<<g2(g.mf, g.nf), kB2, 0, stream>>>(g, f, src_fem, dt);
@@ -644,7 +706,9 @@ int Sim::fem_projection(double dt) {
     if ((r = phase_begin(outer))) return r;
     incrmt_mg_stats st{};
     long long l0 = fem.launches;
+    if ((r = learned_pre(INCRMT_SYS_FEM, src_fem, z_fem))) return r;
     r = fem.solve_device(src_fem, z_fem, &mgo, &st, false);
+    if (!r) r = learned_post(INCRMT_SYS_FEM, z_fem);
     launches += fem.launches - l0;
     vc_fem += st.vcycles;
     solves_fem++;
@@ -902,7 +966,14 @@ void Sim::destroy() {
     for (auto &s : sol) cudaFree(s.s);
     cudaFree(d_frame); cudaFree(d_box);
     d_frame = nullptr; d_box = nullptr; frame_cap = 0;
-    cudaFree(d_win); cudaFree(d_lsbox); cudaFree(d_tiles);
+    cudaFree(d_win); cudaFree(d_lsbox); cudaFree(d_tiles); cudaFree(d_lcnt);
+    d_lcnt = nullptr;
+    for (Learned &L : learn) {
+        L.w.release();
+        cudaFree(L.z0);
+        L.z0 = nullptr;
+        L.z0_n = 0;
+    }
     if (h_win) cudaFreeHost(h_win);
     if (h_lsbox) cudaFreeHost(h_lsbox);
     if (h_tiles) cudaFreeHost(h_tiles);
@@ -1150,6 +1221,65 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;
     st->time = S.time;
+    return INCRMT_OK;
+}
+
+int incrmt_sim_set_learned(incrmt_sim *h, int sys, incrmt_unet *net, int factor, int rule) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    if (sys != INCRMT_SYS_MAC && sys != INCRMT_SYS_FEM) { set_error("bad system %d", sys); return INCRMT_ERR_BADARG; }
+    if (net && (factor < 1 || (rule != 0 && rule != 1))) {
+        set_error("learned warm start needs factor >= 1 and rule 0 or 1");
+        return INCRMT_ERR_BADARG;
+    }
+    incrmt::Sim &S = h->s;
+    if (net) {
+        if (int r = incrmt::learned_supported(sys == INCRMT_SYS_MAC ? S.mac : S.fem)) return r;
+    }
+    S.learn[sys].net = net;
+    S.learn[sys].factor = factor;
+    S.learn[sys].rule = rule;
+    return INCRMT_OK;
+}
+
+int incrmt_sim_learned_grid(const incrmt_sim *h, int sys, int factor, int *H, int *W) {
+    if (!h || !H || !W) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    if (sys != INCRMT_SYS_MAC && sys != INCRMT_SYS_FEM) { set_error("bad system %d", sys); return INCRMT_ERR_BADARG; }
+    if (factor < 1) { set_error("bad factor %d", factor); return INCRMT_ERR_BADARG; }
+    const incrmt::Multigrid &mg = sys == INCRMT_SYS_MAC ? h->s.mac : h->s.fem;
+    incrmt::learned_grid(mg.m, mg.n, factor, *H, *W);
+    return INCRMT_OK;
+}
+
+int incrmt_sim_learned_capture(incrmt_sim *h, int sys, int factor, float *d_in, float *d_target, int cap) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    if (sys != INCRMT_SYS_MAC && sys != INCRMT_SYS_FEM) { set_error("bad system %d", sys); return INCRMT_ERR_BADARG; }
+    if (cap > 0 && (!d_in || !d_target || factor < 1)) {
+        set_error("capture needs device buffers and factor >= 1");
+        return INCRMT_ERR_BADARG;
+    }
+    incrmt::Sim &S = h->s;
+    if (cap > 0) {
+        if (int r = incrmt::learned_supported(sys == INCRMT_SYS_MAC ? S.mac : S.fem)) return r;
+    }
+    incrmt::Sim::Learned &L = S.learn[sys];
+    L.cap_in = cap > 0 ? d_in : nullptr;
+    L.cap_tgt = cap > 0 ? d_target : nullptr;
+    L.cap = cap > 0 ? cap : 0;
+    L.cap_factor = factor;
+    L.captured = 0;
+    return INCRMT_OK;
+}
+
+int incrmt_sim_get_learned_stats(incrmt_sim *h, int sys, incrmt_sim_learned_stats *st) {
+    if (!h || !st) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    if (sys != INCRMT_SYS_MAC && sys != INCRMT_SYS_FEM) { set_error("bad system %d", sys); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    unsigned long long c[2];
+    INCRMT_CK(cudaMemcpyAsync(c, S.d_lcnt + 2 * sys, sizeof(c), cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    st->applied = static_cast<long long>(c[0]);
+    st->fallback = static_cast<long long>(c[1]);
+    st->captured = S.learn[sys].captured;
     return INCRMT_OK;
 }
 

@@ -332,6 +332,66 @@ __global__ void k_restrict(Op op, const T *z, const T *b, int fm, int fn, int px
     zc[I + cm * J] = 0;
 }
 
+/** k_restrict for a 32 x 8 tile of coarse unknowns per 256-thread block,
+ * each fine residual computed once: the block first evaluates b - A z at
+ * every fine unknown of its coarse points' supports (the fine region
+ * 2X0-1 .. 2(X0+31)+1 in a coarsened direction, X0 .. X0+31 otherwise) into
+ * shared memory, then every coarse point sums its support's residuals with
+ * the weights and in the order of k_restrict: the same values. */
+template <class Op, class T>
+__global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const T *b, int fm, int fn, int px, int py,
+                                                       bool kx, bool ky, int cm, int cn, T *bc, T *zc) {
+    constexpr int CTW = 32, CTH = 8, RW = 2 * CTW + 1, RH = 2 * CTH + 1;
+    __shared__ T rs[RW * RH];
+    const int X0 = blockIdx.x * CTW, Y0 = blockIdx.y * CTH;
+    const int FX0 = kx ? 2 * X0 - 1 : X0, FY0 = ky ? 2 * Y0 - 1 : Y0;
+    const int FW = kx ? RW : CTW, FH = ky ? RH : CTH;
+    // Only fine unknowns in the support of a coarse point I < cm, J < cn are
+    // needed (and beyond them a periodic index could wrap past the grid).
+    const int fxmax = kx ? 2 * cm - 1 : cm - 1, fymax = ky ? 2 * cn - 1 : cn - 1;
+    for (int t = threadIdx.x; t < FW * FH; t += blockDim.x) {
+        const int fxu = FX0 + t % FW, fyu = FY0 + t / FW;
+        bool ok = fxu <= fxmax && fyu <= fymax;
+        const int fx = wrap_idx(fxu, fm, px, ok), fy = wrap_idx(fyu, fn, py, ok);
+        T r = 0;
+        if (ok) {
+            const int f = fx + fm * fy;
+            T diag;
+            const T off = op.offdiag(fx, fy, z, diag);
+            r = b[f] - off - diag * z[f];
+        }
+        rs[t] = r;
+    }
+    __syncthreads();
+    const int I = X0 + (threadIdx.x & 31), J = Y0 + (threadIdx.x >> 5);
+    if (I >= cm || J >= cn) return;
+    // The support in k_restrict's order (support(): offsets -1, 0, 1 where
+    // they exist), with each point's local position in the staged region.
+    int fx[3], fy[3], lx[3], ly[3], nfx = 0, nfy = 0;
+    if (!kx) { fx[0] = I; lx[0] = I - FX0; nfx = 1; }
+    else
+        for (int d = -1; d <= 1; d++) {
+            bool ok = true;
+            const int g = wrap_idx(2 * I + d, fm, px, ok);
+            if (ok) { fx[nfx] = g; lx[nfx] = 2 * I + d - FX0; nfx++; }
+        }
+    if (!ky) { fy[0] = J; ly[0] = J - FY0; nfy = 1; }
+    else
+        for (int d = -1; d <= 1; d++) {
+            bool ok = true;
+            const int g = wrap_idx(2 * J + d, fn, py, ok);
+            if (ok) { fy[nfy] = g; ly[nfy] = 2 * J + d - FY0; nfy++; }
+        }
+    T t = 0;
+    for (int bq = 0; bq < nfy; bq++) {
+        const T wy = static_cast<T>(pw(fy[bq], J, fn, cn, py, ky));
+        for (int a = 0; a < nfx; a++)
+            t += wy * static_cast<T>(pw(fx[a], I, fm, cm, px, kx)) * rs[lx[a] + FW * ly[bq]];
+    }
+    bc[I + cm * J] = t;
+    zc[I + cm * J] = 0;
+}
+
 /** Fine correction z_f += P z_c. */
 template <class T>
 __global__ void k_prolong(T *zf, int fm, int fn, int px, int py, bool kx, bool ky,
@@ -759,6 +819,18 @@ int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStrea
     return INCRMT_OK;
 }
 
+/** Coarse right-hand side and cleared coarse iterate: the tiled restriction,
+ * or k_restrict when tiles are off (the identity check of
+ * incrmt_mg_set_tiles covers both). */
+template <class Op, class T>
+void restrict_launch(bool tiles, Op op, cudaStream_t s, const T *z, const T *b, int fm, int fn, int px, int py,
+                     bool kx, bool ky, int cm, int cn, T *bc, T *zc) {
+    if (tiles)
+        k_restrict_tile<<<dim3(cdiv(cm, 32), cdiv(cn, 8)), 256, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc);
+    else
+        k_restrict<<<grid2(cm, cn), kBlk2, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc);
+}
+
 }  // namespace
 
 MacOp<double> Multigrid::mac64() const {
@@ -957,14 +1029,14 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac64();
         if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
     } else if (l == 0) {
         auto op = fem64();
         if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
     } else {
         if ((r = smooth(g, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        restrict_launch(tiles, g, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
     }
     launches++;
     INCRMT_CKL("k_restrict");
@@ -1042,14 +1114,14 @@ int Multigrid::cycle32(int l) {
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac32();
         if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
     } else if (l == 0) {
         auto op = fem32();
         if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(op, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
     } else {
         if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        k_restrict<<<grid2(C.m, C.n), kBlk2, 0, stream>>>(g, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        restrict_launch(tiles, g, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
     }
     launches++;
     INCRMT_CKL("k_restrict");

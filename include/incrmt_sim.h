@@ -1,11 +1,12 @@
 /* incrmt_b200: C ABI of the simulation handle, the B200 replacement of
  * IncRMT's fluid_2d time integrator (fluid_2d.hh:131-177). Same conventions
  * as incrmt.h: int status returns, no exit, caller-owned host buffers. The
- * time step supports walls in x (optionally the inflow and zero-pressure
- * outlet of sim_horiz_flow) and walls or periodicity in y (the simple-spin,
- * sediment and flag scenarios); x-periodic domains, y-periodic ones with an
- * odd n, and y-periodic ones without the zero-pressure outlet (whose pressure
- * systems are singular) are rejected with INCRMT_ERR_BADARG. */
+ * time step supports walls on all sides (simple spin, sediment), walls in x
+ * with the inflow and zero-pressure outlet of sim_horiz_flow and periodic y
+ * (flag), and periodicity in both directions (conv_test's
+ * sim_velocity_pulses). Other combinations (periodic in one direction with
+ * walls and no outlet in the other, or the outlet with x periodicity) and odd
+ * sizes in a periodic direction are rejected with INCRMT_ERR_BADARG. */
 #ifndef INCRMT_SIM_H
 #define INCRMT_SIM_H
 
@@ -41,6 +42,8 @@ typedef struct incrmt_phys {
     double mg_rel_tol;   /* relative residual of each projection (default 1e-9 when <= 0) */
     int horiz_flow;      /* 1: sim_horiz_flow boundary and initial conditions */
     double flow_u;       /* its inflow speed U */
+    int pulses;          /* 1: sim_velocity_pulses' initial fluid velocity (sim_type.cc:43-47) on
+                            the doubly periodic [-1,1]^2 of that scenario */
 } incrmt_phys;
 
 /** Object kinds (subclasses of object, object.hh). */
@@ -53,6 +56,8 @@ typedef struct incrmt_phys {
 #define INCRMT_OBJ_FLAG        4  /* params: cx, cy, flag_l, flag_w, flag_a, perturb_v, ntrace: a flag
                                      anchored at its leading end (obj_flag, object.hh:471-505,
                                      object.cc:420-496), tracking ntrace points along its length */
+#define INCRMT_OBJ_SQUARE      5  /* params: cx, cy, cr, uu, vv, omega, grav: a square of half side cr
+                                     (obj_square, object.hh:142-152, object.cc:41-44, 83-87) */
 
 /** An object plus its material constants (object*, mat_const;
  * fluid_2d::add_object, fluid_2d.cc:74-90; obj_field.hh:15-29). */
@@ -173,6 +178,18 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st);
 #define INCRMT_PHASE_FEM       7  /* FEM source, V-cycles, pressure copy */
 #define INCRMT_PHASE_MG_SETUP  8  /* coefficients and Galerkin hierarchy of both projections */
 #define INCRMT_PHASES          9
+
+/** fluid_2d::l_comparison (fluid_2d_io.cc:186-281): the error norms of
+ * this (coarse) simulation against `fine`, whose m and n must be multiples of
+ * this one's, into err[32]. For a = 0..7 (velocity count fraction, pressure
+ * count fraction, velocity L2, pressure L2, velocity L1, pressure L1,
+ * velocity max, pressure max) err[4a+l] holds the fluid (l=0), solid (1) and
+ * blur-zone (2) parts and err[4a+3] their total (their maximum for the
+ * maxima). The fine velocity is interpolated to the coarse cell centres, the
+ * pressures compared at coinciding corners; like the reference it leaves the
+ * differences in this simulation's c0 (velocity) and c1 (pressure) fields.
+ * Synchronises both simulations' streams. */
+int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err);
 
 /** Per-object windows (no reference counterpart; on by default). The
  * reference sweeps every object's level set and reference map over the whole

@@ -213,6 +213,7 @@ OBJ_CIRCLE = 1
 OBJ_ROUNDED_ROD = 2
 OBJ_ELLIPSE = 3
 OBJ_FLAG = 4
+OBJ_SQUARE = 5
 FIELD_PHI = 200
 FIELD_STATUS = 201
 FIELDS = {n: k for k, n in enumerate(
@@ -239,7 +240,8 @@ class Phys(ctypes.Structure):
     _fields_ = [("visc", ctypes.c_double), ("rhof", ctypes.c_double), ("tw", ctypes.c_double),
                 ("pinw", ctypes.c_double), ("w_scale", ctypes.c_double), ("w_force", ctypes.c_double),
                 ("ntrace", ctypes.c_int), ("zpr", ctypes.c_int), ("precision", ctypes.c_int),
-                ("mg_rel_tol", ctypes.c_double), ("horiz_flow", ctypes.c_int), ("flow_u", ctypes.c_double)]
+                ("mg_rel_tol", ctypes.c_double), ("horiz_flow", ctypes.c_int), ("flow_u", ctypes.c_double),
+                ("pulses", ctypes.c_int)]
 
 
 class ObjectDesc(ctypes.Structure):
@@ -280,6 +282,7 @@ def _sim_sigs(L):
     L.incrmt_get_stats.argtypes = [P, ctypes.POINTER(SimStats)]
     L.incrmt_sim_set_profiling.argtypes = [P, I]
     L.incrmt_sim_set_windows.argtypes = [P, I]
+    L.incrmt_l_comparison.argtypes = [P, P, dp]
     L.incrmt_sim_profile.argtypes = [P, dp]
     L.incrmt_sim_mg_profile.argtypes = [P, I, dp, dp, ctypes.POINTER(ctypes.c_longlong)]
     L.incrmt_solid_bound.argtypes = [P, ctypes.POINTER(I)]
@@ -295,16 +298,18 @@ class Simulation:
 
     def __init__(self, m, n, ax=-1.0, bx=1.0, ay=-1.0, by=1.0, visc=1e-2, rhof=1.0, tw=2.5,
                  pinw=2.5, ntrace=512, zpr=False, precision=PREC_FP64, rel_tol=1e-9, y_prd=False,
-                 horiz_flow=None):
+                 horiz_flow=None, x_prd=False, pulses=False):
         """horiz_flow=U selects sim_horiz_flow: inflow of speed U at the left
-        edge, zero pressure at the right, fluid starting at (U, 0)."""
+        edge, zero pressure at the right, fluid starting at (U, 0).
+        pulses=True with x_prd=y_prd=True on [-1,1]^2 is conv_test's
+        sim_velocity_pulses."""
         L = lib()
         if not hasattr(L, "_sim_ready"):
             _sim_sigs(L)
             L._sim_ready = True
-        g = Grid(m, n, ax, bx, ay, by, 0, int(y_prd))
+        g = Grid(m, n, ax, bx, ay, by, int(x_prd), int(y_prd))
         p = Phys(visc, rhof, tw, pinw, 0.0, 0.0, ntrace, int(zpr), precision, rel_tol,
-                 int(horiz_flow is not None), float(horiz_flow or 0.0))
+                 int(horiz_flow is not None), float(horiz_flow or 0.0), int(pulses))
         h = ctypes.c_void_p()
         check(L.incrmt_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -322,8 +327,17 @@ class Simulation:
                        (ctypes.c_double * 8)(r_scale, a1, a2, piv_r, th_max, omega, 0, 0))
         self._add(d)
 
-    def add_circle(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0):
-        d = ObjectDesc(OBJ_CIRCLE, G, rhos, ev_trans_mult, 1,
+    def add_circle(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0,
+                   set_velocity=True):
+        """set_velocity is mat_const::set_velocity: whether the solid's own
+        velocity replaces the scenario's fluid velocity at initialisation."""
+        d = ObjectDesc(OBJ_CIRCLE, G, rhos, ev_trans_mult, int(set_velocity),
+                       (ctypes.c_double * 8)(cx, cy, cr, uu, vv, omega, grav, 0))
+        self._add(d)
+
+    def add_square(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0,
+                   set_velocity=True):
+        d = ObjectDesc(OBJ_SQUARE, G, rhos, ev_trans_mult, int(set_velocity),
                        (ctypes.c_double * 8)(cx, cy, cr, uu, vv, omega, grav, 0))
         self._add(d)
 
@@ -449,6 +463,13 @@ class Simulation:
         st = SimLearnedStats()
         check(_ulib().incrmt_sim_get_learned_stats(self._h, sys, ctypes.byref(st)))
         return st
+
+    def l_comparison(self, fine):
+        """The 32 error norms of this simulation against a finer one
+        (incrmt_l_comparison)."""
+        err = np.zeros(32)
+        check(lib().incrmt_l_comparison(self._h, fine._h, _dptr(err)))
+        return err
 
     def set_windows(self, on=True):
         """Per-object windows of the level-set and reference-map passes

@@ -120,3 +120,134 @@ __global__ void k_solid_bound(GridDev g, const SolidDev *sol, int nobj, int *box
 }
 
 }  // namespace incrmt
+
+namespace incrmt {
+
+/** Smallest level set over the objects at ghosted index q (fluid_2d::min_phi,
+ * fluid_2d.cc:1490-1495): the largest double when there is none. */
+__device__ __forceinline__ double min_phi_at(const SolidDev *sol, int nobj, int q) {
+    double m = 1.7976931348623157e308;
+    for (int k = 0; k < nobj; k++) {
+        const double v = sol[k].phi[q];
+        if (v < m) m = v;
+    }
+    return m;
+}
+
+/** Accumulators of l_comparison, in the reference's order: [0..2] velocity
+ * counts (fluid, solid, blur), [3..5] pressure counts, [6..8] velocity sums
+ * of squares, [9..11] pressure sums of squares, [12..14] velocity sums,
+ * [15..17] pressure sums, [18..20] velocity maxima, [21..23] pressure
+ * maxima. */
+constexpr int kLcmp = 24;
+
+/** fluid_2d::l_comparison (fluid_2d_io.cc:186-281) of the coarse grid g
+ * against the fine grid gf (dm, dn its refinement factors): per block the 24
+ * accumulators into part[block*24 + k]; the velocity and pressure
+ * differences of each coarse cell are also stored in the coarse c0 and c1,
+ * as the reference does. */
+__global__ void k_l_comparison(GridDev g, FluidDev f, const SolidDev *sol, int nobj, FluidDev ff, int fP, int dm,
+                               int dn, double *part) {
+    const double ste[5] = {1, -1. / 16., 9. / 16, 9. / 16., -1 / 16.};
+    const int mm = g.xp ? g.m : g.m + 1, nn = g.yp ? g.n : g.n + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[kLcmp];
+#pragma unroll
+    for (int k = 0; k < kLcmp; k++) acc[k] = 0;
+    if (t < mm * nn) {
+        const int i = t % mm, j = t / mm;
+        const double tf = g.yp || (j > 0 && j < g.n) ? 1 : 0.5;
+        const double tf2 = g.xp || (i > 0 && i < g.m) ? tf : 0.5 * tf;
+        const int q = g.idx(i, j);
+        const int qf = (dn * j + 2) * fP + (dm * i + 2);  // fine cell (dm i, dn j)
+        int li, ui, lj, uj;
+        const double *stx, *sty;
+        if (dm & 1) { ui = (li = dm / 2) + 1; stx = ste; }
+        else { ui = (li = dm / 2 - 2) + 4; stx = ste + 1; }
+        if (dn & 1) { uj = (lj = dn / 2) + 1; sty = ste; }
+        else { uj = (lj = dn / 2 - 2) + 4; sty = ste + 1; }
+        if (j < g.n && i < g.m) {
+            double delu = 0, delv = 0;
+            const double *sy = sty;
+            for (int jj = lj; jj < uj; jj++, sy++) {
+                const double *sx = stx;
+                for (int ii = li; ii < ui; ii++, sx++) {
+                    const int q3 = qf + jj * fP + ii;
+                    delu += *sy * (*sx) * ff.u[q3];
+                    delv += *sy * (*sx) * ff.v[q3];
+                }
+            }
+            delu -= f.u[q];
+            delv -= f.v[q];
+            const double mphi = min_phi_at(sol, nobj, q);
+            const int c = mphi > g.eps ? 0 : (mphi < -g.eps ? 1 : 2);
+            const double delsq = delu * delu + delv * delv, del = sqrt(delsq);
+            f.c0[q] = del;
+            acc[c] += 1.;
+            acc[6 + c] += delsq;
+            acc[12 + c] += del;
+            if (acc[18 + c] < del) acc[18 + c] = del;
+        }
+        // material at this cell corner, from the four-by-four neighbourhood;
+        // at the last corner of a non-periodic direction it reaches one cell
+        // past the ghosted grid (the reference reads beyond its array there),
+        // which is clamped to the last ghost cell
+        double mphi = 0;
+        for (int jj = -1; jj < 3; jj++) {
+            const int cj = min(j + jj, g.n + 1);
+            for (int ii = -1; ii < 3; ii++) {
+                const int ci = min(i + ii, g.m + 1);
+                mphi += ste[jj + 2] * ste[ii + 2] * min_phi_at(sol, nobj, g.idx(ci, cj));
+            }
+        }
+        const int c = mphi > g.eps ? 0 : (mphi < -g.eps ? 1 : 2);
+        const double delp = ff.p[qf] - f.p[q];
+        f.c1[q] = delp;
+        acc[3 + c] += 1.;
+        acc[9 + c] += delp * delp * tf2;
+        acc[15 + c] += fabs(delp) * tf2;
+        if (acc[21 + c] < delp) acc[21 + c] = delp;
+    }
+    // block reduction (256 threads): sums for [0..18), maxima for [18..24)
+    __shared__ double red[kLcmp][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kLcmp; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double u = __shfl_down_sync(0xffffffffu, v, o);
+            v = k < 18 ? v + u : fmax(v, u);
+        }
+        if (lane == 0) red[k][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kLcmp) {
+        const int k = threadIdx.x;
+        double v = red[k][0];
+        for (int q = 1; q < 8; q++) v = k < 18 ? v + red[k][q] : fmax(v, red[k][q]);
+        part[blockIdx.x * kLcmp + k] = v;
+    }
+}
+
+/** Combines the block accumulators in block order into the 32 norms of
+ * l_comparison: err[4a+l] for quantity a and category l, err[4a+3] the total
+ * (sums for a < 6, maxima for a = 6, 7), the L2 rows square-rooted; sums are
+ * scaled by 1/(m n). One thread. */
+__global__ void k_l_comparison_final(const double *part, int nb, double fac, double *err) {
+    double o[kLcmp];
+    for (int k = 0; k < kLcmp; k++) o[k] = 0;
+    for (int b = 0; b < nb; b++)
+        for (int k = 0; k < kLcmp; k++) o[k] = k < 18 ? o[k] + part[b * kLcmp + k] : fmax(o[k], part[b * kLcmp + k]);
+    for (int a = 0; a < 6; a++) {
+        for (int l = 0; l < 3; l++) err[4 * a + l] = o[3 * a + l] * fac;
+        err[4 * a + 3] = err[4 * a] + err[4 * a + 1] + err[4 * a + 2];
+    }
+    for (int a = 6; a < 8; a++) {
+        for (int l = 0; l < 3; l++) err[4 * a + l] = o[3 * a + l];
+        double mx = err[4 * a] > err[4 * a + 1] ? err[4 * a] : err[4 * a + 1];
+        err[4 * a + 3] = err[4 * a + 2] > mx ? err[4 * a + 2] : mx;
+    }
+    for (int k = 8; k < 16; k++) err[k] = sqrt(err[k]);
+}
+
+}  // namespace incrmt

@@ -191,27 +191,32 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
         set_error("bad grid %dx%d", gr->m, gr->n);
         return INCRMT_ERR_BADARG;
     }
-    if (gr->x_prd) {
-        set_error("x-periodic domains are not supported by the time step (walls or inflow in x)");
+    if ((gr->y_prd && (gr->n & 1)) || (gr->x_prd && (gr->m & 1))) {
+        set_error("a periodic direction needs an even size (multigrid coarsening)");
         return INCRMT_ERR_BADARG;
     }
-    if (gr->y_prd && (gr->n & 1)) {
-        set_error("a y-periodic grid needs an even n (multigrid coarsening)");
+    const bool outlet = ph->zpr || ph->horiz_flow;
+    if (gr->x_prd && (outlet || !gr->y_prd)) {
+        // The zero-pressure outlet is the right edge; x periodicity comes only
+        // with y periodicity, as in sim_velocity_pulses (sim_type.hh:99-101).
+        set_error("an x-periodic domain must be periodic in y too and have no zero-pressure outlet");
         return INCRMT_ERR_BADARG;
     }
-    if (gr->y_prd && !(ph->zpr || ph->horiz_flow)) {
-        // Walls in x with y periodicity and no outlet leave both pressure
-        // systems singular with a periodic null space, which the projections
-        // do not handle; the reference's drivers use y periodicity only with
-        // sim_horiz_flow's outlet (ftest.cc:362).
-        set_error("a y-periodic domain needs the zero-pressure outlet (zpr or horiz_flow)");
+    if (gr->y_prd && !gr->x_prd && !outlet) {
+        // Walls in x with y periodicity and no outlet: the reference's drivers
+        // use y periodicity with walls in x only with sim_horiz_flow's outlet
+        // (ftest.cc:362), and the projections were not shown to converge on
+        // that singular combination.
+        set_error("a y-periodic domain with walls in x needs the zero-pressure outlet (zpr or horiz_flow)");
         return INCRMT_ERR_BADARG;
     }
     INCRMT_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     g.m = gr->m; g.n = gr->n; g.ml = g.m + 4; g.nl = g.n + 4;
     g.P = (g.ml + 31) / 32 * 32;
+    g.xp = gr->x_prd ? 1 : 0;
     g.yp = gr->y_prd ? 1 : 0;
-    g.mf = g.m + 1; g.nf = g.yp ? g.n : g.n + 1;  // m_fem, n_fem (fluid_2d.cc:30-31)
+    g.pulses = ph->pulses ? 1 : 0;
+    g.mf = g.xp ? g.m : g.m + 1; g.nf = g.yp ? g.n : g.n + 1;  // m_fem, n_fem (fluid_2d.cc:30-31)
     g.hflow = ph->horiz_flow ? 1 : 0;
     g.flow_u = ph->flow_u;
     g.zpr = (ph->zpr || g.hflow) ? 1 : 0;  // sim_horiz_flow::start sets zpr (sim_type.cc:59-64)
@@ -270,15 +275,15 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     ntx = ((g.m + 1 + 32) >> 5) + 1;
     nty = ((g.n + 1 + 8) >> 3) + 1;
     if (ntrace > 0 && (r = alloc(&tm, 4 * static_cast<size_t>(ntrace)))) return r;
-    if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, g.yp, g.zpr, stream))) return r;
-    if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, 0, g.yp, g.zpr, stream))) return r;
+    if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
+    if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
     return INCRMT_OK;
 }
 
 int Sim::add_object(const incrmt_object_desc *d) {
     if (initialized) { set_error("objects must be added before initialize"); return INCRMT_ERR_BADARG; }
     if (static_cast<int>(obj.size()) >= kMaxObjects) { set_error("too many objects"); return INCRMT_ERR_BADARG; }
-    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_FLAG) {
+    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_SQUARE) {
         set_error("unknown object type %d", d->type);
         return INCRMT_ERR_BADARG;
     }
@@ -287,6 +292,7 @@ int Sim::add_object(const incrmt_object_desc *d) {
              : d->type == INCRMT_OBJ_CIRCLE      ? OBJ_CIRCLE
              : d->type == INCRMT_OBJ_ROUNDED_ROD ? OBJ_ROUNDED_ROD
              : d->type == INCRMT_OBJ_ELLIPSE     ? OBJ_ELLIPSE
+             : d->type == INCRMT_OBJ_SQUARE      ? OBJ_SQUARE
                                                  : OBJ_FLAG;
     o.set_velocity = d->set_velocity;
     o.G = d->G; o.rhos = d->rhos; o.ev_trans_mult = d->ev_trans_mult;
@@ -298,8 +304,8 @@ int Sim::add_object(const incrmt_object_desc *d) {
         const double scf = p[0] / (1 + p[1] + p[2]);
         o.g[0] = scf * (1 - p[2]); o.g[1] = scf * p[1]; o.g[2] = 2 * scf * p[2];
         o.g[3] = p[3]; o.g[4] = p[4]; o.g[5] = p[5];
-    } else if (o.type == OBJ_CIRCLE) {
-        // obj_circle(cx,cy,cr,uu,vv,omega,grav) (object.hh:128-138)
+    } else if (o.type == OBJ_CIRCLE || o.type == OBJ_SQUARE) {
+        // obj_circle / obj_square(cx,cy,cr,uu,vv,omega,grav) (object.hh:128-152)
         o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[6];
         o.g[4] = p[3]; o.g[5] = p[4]; o.g[6] = p[5];
     } else if (o.type == OBJ_ROUNDED_ROD) {
@@ -431,10 +437,15 @@ int Sim::win_update() {
         wl[k] = grow(h_lsbox + 4 * k, 2 * R + 4);
         wp[k] = grow(h_lsbox + 4 * k, R + 3);
         // Under y periodicity the Godunov pass of the last row writes the
-        // bottom edges of row 0: a window near either end spans the height.
+        // bottom edges of row 0: a window near either end spans the height
+        // (and likewise the width under x periodicity).
         if (g.yp && wp[k].y1 > wp[k].y0 && (wp[k].y0 <= 3 || wp[k].y1 >= g.nl - 3)) {
             wp[k].y0 = 0;
             wp[k].y1 = g.nl;
+        }
+        if (g.xp && wp[k].x1 > wp[k].x0 && (wp[k].x0 <= 3 || wp[k].x1 >= g.ml - 3)) {
+            wp[k].x0 = 0;
+            wp[k].x1 = g.ml;
         }
         for (int kind = 0; kind < 2; kind++) {
             const LsWin &w = h_win[kind * kMaxObjects + k];
@@ -874,6 +885,10 @@ int Sim::godunov(bool tang) {
     if (tang) k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles());
     else k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles());
     launches++;
+    if (g.xp) {
+        k_wrap_edges_x<<<cdiv(g.n, 256), 256, 0, stream>>>(g, f);
+        launches++;
+    }
     if (g.yp) {
         k_wrap_edges_y<<<cdiv(g.m, 256), 256, 0, stream>>>(g, f);
         launches++;
@@ -1280,6 +1295,32 @@ int incrmt_sim_get_learned_stats(incrmt_sim *h, int sys, incrmt_sim_learned_stat
     st->applied = static_cast<long long>(c[0]);
     st->fallback = static_cast<long long>(c[1]);
     st->captured = S.learn[sys].captured;
+    return INCRMT_OK;
+}
+
+int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err) {
+    if (!h || !fine || !err) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s, &F = fine->s;
+    if (F.g.m % S.g.m != 0 || F.g.n % S.g.n != 0) {
+        set_error("Grid dimension is not a multiple of the finer grid");
+        return INCRMT_ERR_BADARG;
+    }
+    if (F.g.xp != S.g.xp || F.g.yp != S.g.yp) { set_error("the two grids differ in periodicity"); return INCRMT_ERR_BADARG; }
+    INCRMT_CK(cudaStreamSynchronize(F.stream));
+    const int mm = S.g.xp ? S.g.m : S.g.m + 1, nn = S.g.yp ? S.g.n : S.g.n + 1;
+    const int nb = incrmt::cdiv(mm * nn, 256);
+    double *part = nullptr;
+    INCRMT_CK(cudaMallocAsync(&part, sizeof(double) * (incrmt::kLcmp * static_cast<size_t>(nb) + 32), S.stream));
+    incrmt::k_l_comparison<<<nb, 256, 0, S.stream>>>(S.g, S.f, S.d_sol, static_cast<int>(S.obj.size()), F.f, F.g.P,
+                                                    F.g.m / S.g.m, F.g.n / S.g.n, part);
+    const double fac = 1. / (static_cast<double>(S.g.m) * S.g.n);
+    double *dev_err = part + incrmt::kLcmp * static_cast<size_t>(nb);
+    incrmt::k_l_comparison_final<<<1, 1, 0, S.stream>>>(part, nb, fac, dev_err);
+    S.launches += 2;
+    INCRMT_CK(cudaGetLastError());
+    INCRMT_CK(cudaMemcpyAsync(err, dev_err, sizeof(double) * 32, cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaFreeAsync(part, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
     return INCRMT_OK;
 }
 

@@ -23,6 +23,7 @@ enum ObjType : int {
     OBJ_ROUNDED_ROD = 2,  // obj_rounded_rod (object.hh:218-241, object.cc:75-78, 275-278)
     OBJ_ELLIPSE = 3,      // rotated ellipse under gravity (no reference counterpart)
     OBJ_FLAG = 4,         // obj_flag (object.hh:471-505, object.cc:420-496)
+    OBJ_SQUARE = 5,       // obj_square (object.hh:142-152, object.cc:41-44, 83-87)
 };
 
 /** Device description of one solid: material constants (mat_const,
@@ -35,7 +36,7 @@ struct ObjDev {
     double eps, pinw, ex_visc;
     double tf1, tf2, tf3;
     // Geometry: simple spin {c0, c1, c2, piv_r, th_max, omega, piv_thresh,
-    // K_stiff}; circle {cx, cy, cr, grav, uu, vv, omega}; rounded rod
+    // K_stiff}; circle and square {cx, cy, cr, grav, uu, vv, omega}; rounded rod
     // {cx, cy, cr, grav, 0, 0, 0, cl}; ellipse {cx, cy, a, grav, 0, 0, 0, b,
     // cos theta, sin theta}; flag {cx, cy, flag_l, 0, 0, 0, 0, flag_w, flag_a,
     // perturb_v, flag_thresh, K_stiff}.
@@ -85,6 +86,11 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
         if (gr == 0) return -fmin(o.g[2], o.g[7]);
         return (r - 1) * r / gr;
     }
+    if (o.type == OBJ_SQUARE) {  // obj_square::phi, object.cc:83-87
+        X = fabs(X) - o.g[2];
+        Y = fabs(Y) - o.g[2];
+        return X < 0 || Y < 0 ? fmax(X, Y) : sqrt(X * X + Y * Y);
+    }
     return sqrt(X * X + Y * Y) - o.g[2];  // obj_circle::phi, object.cc:22-24
 }
 
@@ -108,8 +114,8 @@ __device__ __forceinline__ void obj_velocity(const ObjDev &o, double X, double Y
 
 /** Extra accelerations (object::accel overrides): the simple spinner's
  * rotating pivot (object.cc:189-197), the flag's anchor (object.cc:476-484)
- * and the gravity of the circle, the rounded rod and the ellipse
- * (object.cc:31-34, 75-78). */
+ * and the gravity of the circle, the square, the rounded rod and the ellipse
+ * (object.cc:31-34, 41-44, 75-78). */
 __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, double X, double Y,
                                           double phiv, double &ax, double &ay) {
     if (o.type == OBJ_SIMPLE_SPIN) {
@@ -137,7 +143,9 @@ struct GridDev {
     int m, n, ml, nl, P;
     int mf, nf;  // FEM nodes
     int zpr;
+    int xp;         // x-periodic (sim_type::x_prd)
     int yp;         // y-periodic (sim_type::y_prd)
+    int pulses;     // initial fluid velocity of sim_velocity_pulses
     int hflow;      // sim_horiz_flow inflow at the left edge
     double flow_u;  // its speed
     double ax, bx, ay, by, dx, dy, xsp, ysp, xxsp, yysp;

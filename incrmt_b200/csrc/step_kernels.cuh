@@ -83,27 +83,34 @@ __global__ void k_godunov(GridDev g, FluidDev f, const SolidDev *sol, TileObjs t
     const int q = g.idx(i, j), P = g.P;
     int kb, ke;
     to.range(i, j, kb, ke);
-    if (i < g.m - 1) {
-        const int r = q + 1;
+    if (i < g.m - 1 || g.xp) {
+        // With x periodicity the right edge of the last column is the left
+        // edge of column 0; the reference selects it with
+        // godunov_set_lr<true> on the ghost column -1, which holds column
+        // m-1's fluid edge values but the (never written) ghost solid values
+        // (fluid_2d.cc:733-741); qs is that column for the solids.
+        const bool wrap = i == g.m - 1;
+        const bool tg = tang || wrap;
+        const int r = wrap ? q - (g.m - 1) : q + 1, qs = wrap ? r - 1 : q;
         const double fur = f.ur[q], frul = f.ul[r];
         if (fur + frul > 0 && fur > 0) {
             f.ul[r] = fur;
             f.vl[r] = f.vr[q];
             for (int p = kb; p < ke; p++) {
                 const SolidDev &s = sol[to.at(p)];
-                s.Xl[r] = s.Xr[q];
-                s.Yl[r] = s.Yr[q];
+                s.Xl[r] = s.Xr[qs];
+                s.Yl[r] = s.Yr[qs];
             }
         } else if (fur + frul < 0 && frul < 0) {
-            if (tang) f.ur[q] = frul;
+            if (tg) f.ur[q] = frul;
         } else {
-            if (tang) f.ur[q] = 0.5 * (fur + frul);
+            if (tg) f.ur[q] = 0.5 * (fur + frul);
             f.ul[r] = 0;
             f.vl[r] = 0.5 * (f.vr[q] + f.vl[r]);
             for (int p = kb; p < ke; p++) {
                 const SolidDev &s = sol[to.at(p)];
-                s.Xl[r] = 0.5 * (s.Xr[q] + s.Xl[r]);
-                s.Yl[r] = 0.5 * (s.Yr[q] + s.Yl[r]);
+                s.Xl[r] = 0.5 * (s.Xr[qs] + s.Xl[r]);
+                s.Yl[r] = 0.5 * (s.Yr[qs] + s.Yl[r]);
             }
         }
     }
@@ -139,13 +146,15 @@ __global__ void k_godunov(GridDev g, FluidDev f, const SolidDev *sol, TileObjs t
         }
     }
     // Wall edge conditions.
-    if (i == 0) {
-        if (g.zpr) f.ur[q - 1] = f.ul[q];
-        else { f.ul[q] = 0; f.vl[q] = 0; f.ur[q - 1] = 0; }
-    }
-    if (i == g.m - 1) {
-        if (g.zpr) { f.ul[q + 1] = f.ur[q]; f.vl[q + 1] = f.vr[q]; }
-        else { f.ul[q + 1] = 0; f.vl[q + 1] = 0; f.ur[q] = 0; }
+    if (!g.xp) {
+        if (i == 0) {
+            if (g.zpr) f.ur[q - 1] = f.ul[q];
+            else { f.ul[q] = 0; f.vl[q] = 0; f.ur[q - 1] = 0; }
+        }
+        if (i == g.m - 1) {
+            if (g.zpr) { f.ul[q + 1] = f.ur[q]; f.vl[q + 1] = f.vr[q]; }
+            else { f.ul[q + 1] = 0; f.vl[q + 1] = 0; f.ur[q] = 0; }
+        }
     }
     if (!g.yp) {
         if (j == 0) { f.ud[q] = 0; f.vd[q] = 0; f.vu[q - P] = 0; }
@@ -164,6 +173,19 @@ __global__ void k_wrap_edges_y(GridDev g, FluidDev f) {
     f.uu[q0 - g.P] = f.uu[qt];
     f.vd[qt + g.P] = f.vd[q0];
     f.ud[qt + g.P] = f.ud[q0];
+}
+
+/** Ghost columns of the edge values under x periodicity, after k_godunov
+ * (fluid_2d::edge_boundary_conditions, fluid_2d.cc:733-741): column -1 takes
+ * column m-1's right values, column m column 0's left values. */
+__global__ void k_wrap_edges_x(GridDev g, FluidDev f) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= g.n) return;
+    const int q0 = g.idx(0, j), qt = g.idx(g.m - 1, j);
+    f.ur[q0 - 1] = f.ur[qt];
+    f.vr[q0 - 1] = f.vr[qt];
+    f.ul[qt + 1] = f.ul[q0];
+    f.vl[qt + 1] = f.vl[q0];
 }
 
 /** compute_tangential_stability_derivatives (fluid_2d.cc:953-975), without
@@ -285,6 +307,10 @@ __global__ void k_mac_correct(GridDev g, FluidDev f, const double *z, const doub
         f.vd[q + g.n * g.P] = f.vd[q];
     }
     if (i > 0) f.ul[q] -= ex[j * (g.m + 1) + i] * (z[ij] - z[ij - 1]) * g.xsp;
+    else if (g.xp) {
+        f.ul[q] -= ex[j * (g.m + 1)] * (z[ij] - z[ij + g.m - 1]) * g.xsp;
+        f.ul[q + g.m] = f.ul[q];
+    }
 }
 
 /** Cell (i,j) of thread (x,y) of a launch over object blockIdx.z's window
@@ -346,7 +372,7 @@ __global__ void k_set_rho(GridDev g, FluidDev f, const ObjDev *obj, const SolidD
 }
 
 /** Ghost velocities (fluid_2d::set_boundaries, fluid_2d.cc:689-725): one
- * block; first the left/right ghosts of every row (walls, or linear
+ * block; first the left/right ghosts of every row (periodic, walls, or linear
  * extrapolation at a zero-pressure right edge), then the bottom/top ghost
  * rows including the corners (walls or periodic), then the inflow of
  * sim_horiz_flow::boundary (sim_type.cc:51-56) on the two left ghost columns. */
@@ -355,9 +381,16 @@ __global__ void k_set_boundaries(GridDev g, FluidDev f) {
     double *u = f.u, *v = f.v;
     for (int j = threadIdx.x; j < g.n; j += blockDim.x) {
         const int q = g.idx(0, j);
+        const int r = q + g.m;
+        if (g.xp) {
+            u[q - 2] = u[r - 2]; v[q - 2] = v[r - 2];
+            u[q - 1] = u[r - 1]; v[q - 1] = v[r - 1];
+            u[r] = u[q]; v[r] = v[q];
+            u[r + 1] = u[q + 1]; v[r + 1] = v[q + 1];
+            continue;
+        }
         u[q - 2] = -u[q + 1]; v[q - 2] = -v[q + 1];
         u[q - 1] = -u[q]; v[q - 1] = -v[q];
-        const int r = q + g.m;
         if (g.zpr) {
             u[r] = 2 * u[r - 1] - u[r - 2]; v[r] = 2 * v[r - 1] - v[r - 2];
             u[r + 1] = 2 * u[r] - u[r - 1]; v[r + 1] = 2 * v[r] - v[r - 1];
@@ -546,6 +579,7 @@ __global__ void k_ustar(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev
  * fem_source_term_conditions sets for walls, the zero-pressure edge and y
  * periodicity (fluid_2d.cc:837-871). */
 __device__ __forceinline__ void ustar_bc(const GridDev &g, const FluidDev &f, int i, int j, double &c0, double &c1) {
+    if (i < 0 && g.xp) i = g.m - 1;  // ghost column -1 copies column m-1 (fluid_2d.cc:841-845)
     if (j < 0 && g.yp) j = g.n - 1;  // ghost row -1 copies row n-1 (fluid_2d.cc:861-865)
     if (j < 0 || j >= g.n || i >= g.m) { c0 = 0; c1 = 0; return; }
     const int q = g.idx(i, j);
@@ -566,6 +600,11 @@ __device__ __forceinline__ void ustar_bc(const GridDev &g, const FluidDev &f, in
 __global__ void k_fem_ghosts(GridDev g, FluidDev f) {
     for (int j = threadIdx.x; j < g.n; j += blockDim.x) {
         const int q = g.idx(0, j), r = g.idx(g.m, j);
+        if (g.xp) {  // column -1 copies column m-1; column m is left as it is
+            f.c0[q - 1] = f.c0[r - 1];
+            f.c1[q - 1] = f.c1[r - 1];
+            continue;
+        }
         f.c0[q - 1] = g.zpr ? f.u[q - 1] : 0.;
         f.c1[q - 1] = g.zpr ? f.v[q - 1] : 0.;
         f.c0[r] = 0;
@@ -573,7 +612,8 @@ __global__ void k_fem_ghosts(GridDev g, FluidDev f) {
     }
     __syncthreads();
     const int G = g.n * g.P;
-    for (int i = threadIdx.x - 1; i <= g.m; i += blockDim.x) {
+    // the bottom/top rows from column -1 to m (x periodic: to m-1)
+    for (int i = threadIdx.x - 1; i <= (g.xp ? g.m - 1 : g.m); i += blockDim.x) {
         const int q = g.idx(i, 0);
         if (g.yp) {
             f.c0[q - g.P] = f.c0[q + G - g.P];
@@ -607,7 +647,7 @@ __global__ void k_pressure_sum(GridDev g, const double *z, double *partial) {
     for (long t = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; t < N;
          t += static_cast<long>(gridDim.x) * blockDim.x) {
         const int i = static_cast<int>(t % g.mf), j = static_cast<int>(t / g.mf);
-        double w = (i == 0 || i == g.mf - 1) ? 0.5 : 1.0;
+        double w = !g.xp && (i == 0 || i == g.mf - 1) ? 0.5 : 1.0;
         if (!g.yp && (j == 0 || j == g.nf - 1)) w *= 0.5;
         acc += w * z[t];
     }
@@ -630,7 +670,8 @@ __global__ void k_copy_pressure(GridDev g, FluidDev f, const double *z, const do
     if (i > g.m || j > g.n) return;
     const double pavg = g.zpr ? 0. : psum[0] * (1. / (static_cast<double>(g.m) * g.n));
     const int jz = g.yp && j == g.n ? 0 : j;  // the last row repeats row 0 (fluid_2d.cc:1323)
-    f.p[g.idx(i, j)] = z[jz * g.mf + i] - pavg;
+    const int iz = g.xp && i == g.m ? 0 : i;  // the last column repeats column 0 (fluid_2d.cc:1326)
+    f.p[g.idx(i, j)] = z[jz * g.mf + iz] - pavg;
 }
 
 /** End-of-step velocity (update_velocity, fluid_2d.cc:1354-1374); the
@@ -684,6 +725,19 @@ __global__ void k_init_object(GridDev g, const ObjDev *obj, const SolidDev *sol)
     s.phi[q] = obj_phi(o, X, Y);
 }
 
+/** sim_velocity_pulses::velocity (sim_type.cc:43-47, sim_type.hh:109-113):
+ * six incompressible Gaussian pulses of alternating sign and growing inverse
+ * square length along the diagonal. */
+__device__ __forceinline__ void pulses_velocity(double x, double y, double &u, double &v) {
+    u = v = 0;
+    for (double k = 2, s = 1, z = -5 / 6.; z < 1; z += 1 / 3., k += 2, s = -s) {
+        const double px = x - z, py = y - z;
+        const double f = s * exp(-k * (2 - cos(px * M_PI) - cos(py * M_PI)));
+        u -= sin(py * M_PI) * f;
+        v += sin(px * M_PI) * f;
+    }
+}
+
 /** Initial velocity from the solids' momenta and the scenario's fluid
  * velocity (fluid_2d::init_fields, fluid_2d.cc:213-239). */
 __global__ void k_init_velocity(GridDev g, FluidDev f, const ObjDev *obj, const SolidDev *sol, int nobj) {
@@ -704,11 +758,13 @@ __global__ void k_init_velocity(GridDev g, FluidDev f, const ObjDev *obj, const 
         f.u[q] = mu / rho;
         f.v[q] = mv / rho;
     } else {
-        // sim_type::velocity: at rest, or (U, 0) for sim_horiz_flow (sim_type.hh:132-135)
-        const double uf = g.hflow ? g.flow_u : 0.;
+        // sim_type::velocity: at rest, (U, 0) for sim_horiz_flow
+        // (sim_type.hh:132-135), or the pulses of sim_velocity_pulses
+        double uf = g.hflow ? g.flow_u : 0., vf = 0.;
+        if (g.pulses) pulses_velocity(g.ax + g.dx * (0.5 + i), g.ay + g.dy * (0.5 + j), uf, vf);
         double irho = 1 / ((1 - sfrac) * g.rhof + rho);
         f.u[q] = ((1 - sfrac) * g.rhof * uf + mu) * irho;
-        f.v[q] = ((1 - sfrac) * g.rhof * 0. + mv) * irho;
+        f.v[q] = ((1 - sfrac) * g.rhof * vf + mv) * irho;
     }
 }
 

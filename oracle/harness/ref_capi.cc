@@ -108,6 +108,7 @@ ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double vi
         const double *p=params+8*k;
         if(types[k]==1) r->obj.push_back(new obj_circle(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
         else if(types[k]==2) r->obj.push_back(new obj_rounded_rod(p[0],p[1],p[2],p[3],p[4]));
+        else if(types[k]==5) r->obj.push_back(new obj_square(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
         else r->obj.push_back(new obj_flag(p[0],p[1],p[2],p[3],p[4],p[5],static_cast<int>(p[6]),r->fa));
     }
     if(flow_u>0) r->st=new sim_horiz_flow(flow_u,geom[0],geom[1],geom[2],geom[3]);
@@ -118,6 +119,36 @@ ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double vi
         r->f->add_object(r->obj[k],mc);
     }
     r->f->initialize(0.8,0.4,0.8);
+    zero_unset_refmap(*r->f);
+    return r;
+}
+
+/** conv_test's scenario (conv_test.cc:52-125): sim_velocity_pulses on the
+ * doubly periodic [-1,1]^2, circles (type 1) or squares (type 5) of
+ * (cx,cy,cr,uu,vv,omega,grav) with mat_const(G,rhos,1,false), initialised
+ * with the given extra-viscosity and time-step padding factors. */
+ref_sim* make_pulses(int m,double visc,double rhof,int ntrace,int nobj,const int *types,const double *params,
+                     const double *mats,double ev_mult,double dt_pad,double dt_ev_pad,const char *base) {
+    ref_sim *r=new ref_sim;
+    r->fa=new char[strlen(base)+1];
+    strcpy(r->fa,base);
+    r->fout=new char[strlen(base)+8];
+    sprintf(r->fout,"%s.odr",base);
+    mkdir(r->fout,S_IRWXU|S_IRWXG|S_IROTH|S_IXOTH);
+    const double tw=2.5,pinw=2.5;
+    const unsigned int fflags=8|2048;
+    for(int k=0;k<nobj;k++) {
+        const double *p=params+8*k;
+        if(types[k]==5) r->obj.push_back(new obj_square(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
+        else r->obj.push_back(new obj_circle(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
+    }
+    r->st=new sim_velocity_pulses;
+    r->f=new fluid_2d(m,m,*r->st,visc,rhof,tw,pinw,ntrace,fflags,r->fout);
+    for(int k=0;k<nobj;k++) {
+        mat_const mc(mats[2*k],mats[2*k+1],1,false);
+        r->f->add_object(r->obj[k],mc);
+    }
+    r->f->initialize(ev_mult,dt_pad,dt_ev_pad);
     zero_unset_refmap(*r->f);
     return r;
 }
@@ -147,6 +178,18 @@ void* ref_multi_create(int m,int n,const double *geom,int x_prd,int y_prd,double
                        int ntrace,int nobj,const int *types,const double *params,const double *mats,
                        const char *base,double flow_u) {
     return make_multi(m,n,geom,x_prd,y_prd,visc,rhof,ntrace,nobj,types,params,mats,base,flow_u);
+}
+
+void* ref_pulses_create(int m,double visc,double rhof,int ntrace,int nobj,const int *types,
+                        const double *params,const double *mats,double ev_mult,double dt_pad,
+                        double dt_ev_pad,const char *base) {
+    return make_pulses(m,visc,rhof,ntrace,nobj,types,params,mats,ev_mult,dt_pad,dt_ev_pad,base);
+}
+
+/** fluid_2d::l_comparison of the coarse simulation h against the fine one
+ * (fluid_2d_io.cc:186-281): 32 doubles into err. */
+void ref_l_comparison(void *h,void *fine,double *err) {
+    static_cast<ref_sim*>(h)->f->l_comparison(*static_cast<ref_sim*>(fine)->f,err);
 }
 
 void ref_destroy(void *h) {

@@ -62,6 +62,10 @@ def lib():
     L.ref_destroy.argtypes = [P]
     L.ref_multi_create.argtypes = [I, I, dp, I, I, D, D, I, I, ip, dp, dp, ctypes.c_char_p, D]
     L.ref_multi_create.restype = P
+    L.ref_pulses_create.argtypes = [I, D, D, I, I, ip, dp, dp, D, D, D, ctypes.c_char_p]
+    L.ref_pulses_create.restype = P
+    L.ref_l_comparison.argtypes = [P, P, dp]
+    L.ref_l_comparison.restype = None
     L.ref_dims.argtypes = [P, ip]
     L.ref_scalars.argtypes = [P, dp]
     L.ref_set_time.argtypes = [P, D]
@@ -121,18 +125,31 @@ class RefSim:
     flow_u > 0 makes the domain sim_horiz_flow (y-periodic with inflow)."""
 
     def __init__(self, m, ntrace=512, workdir=None, n=None, objects=None, geom=(-1., 1., -1., 1.),
-                 visc=1e-2, rhof=1.0, periodic=(False, False), flow_u=0.0):
+                 visc=1e-2, rhof=1.0, periodic=(False, False), flow_u=0.0, pulses=None):
         self._tmp = None
         if workdir is None:
             self._tmp = tempfile.TemporaryDirectory()
             workdir = self._tmp.name
-        if objects is None:
+        if pulses is not None:
+            # conv_test's scenario: pulses = (ev_mult, dt_pad, dt_ev_pad)
+            objects = objects or []
+            k = len(objects)
+            types = (ctypes.c_int * max(k, 1))(*[{"circle": 1, "square": 5}[o[0]] for o in objects])
+            params = np.zeros((max(k, 1), 8))
+            mats = np.zeros((max(k, 1), 2))
+            for q, (kind, p, G, rhos) in enumerate(objects):
+                params[q, :len(p)] = p
+                mats[q] = (G, rhos)
+            base = os.path.join(workdir, f"pulses_{m}").encode()
+            self.h = lib().ref_pulses_create(m, visc, rhof, ntrace, k, types, _dp(params), _dp(mats),
+                                             float(pulses[0]), float(pulses[1]), float(pulses[2]), base)
+        elif objects is None:
             base = os.path.join(workdir, f"sspin_{m}").encode()
             self.h = lib().ref_sspin_create(m, ntrace, base)
         else:
             n = m if n is None else n
             k = len(objects)
-            types = (ctypes.c_int * k)(*[{"circle": 1, "rod": 2, "flag": 3}[o[0]] for o in objects])
+            types = (ctypes.c_int * k)(*[{"circle": 1, "rod": 2, "flag": 3, "square": 5}[o[0]] for o in objects])
             params = np.zeros((k, 8))
             mats = np.zeros((k, 2))
             for q, (kind, p, G, rhos) in enumerate(objects):
@@ -146,6 +163,13 @@ class RefSim:
         lib().ref_dims(self.h, d)
         self.m, self.n, self.ml, self.nl, self.n_obj, self.m_fem, self.n_fem = list(d)
         self.ntrace = ntrace
+
+    def l_comparison(self, fine):
+        """fluid_2d::l_comparison of this (coarse) simulation against `fine`:
+        the 32 error norms (fluid_2d_io.cc:186-281)."""
+        err = np.zeros(32)
+        lib().ref_l_comparison(self.h, fine.h, _dp(err))
+        return err
 
     def scalars(self):
         s = np.zeros(6)

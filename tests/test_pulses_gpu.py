@@ -1,0 +1,158 @@
+"""GPU parity on conv_test's scenario (conv_test.cc:52-125): the doubly
+periodic [-1,1]^2 of sim_velocity_pulses (six Gaussian velocity pulses,
+sim_type.cc:43-47) with the test's solid circle or square of half size 0.6 at
+(-0.1, 0) (G 1, set_velocity off, extra-viscosity padding 0.4, time-step
+padding 0.4 / 0.8). The oracle is the reference's own fluid_2d with
+sim_velocity_pulses (oracle/_ref, ref_pulses_create).
+
+- stages: the reference state after 20 steps is copied into the GPU
+  simulation, one step function runs on each, every field is compared with
+  the tolerances of the other stage tests;
+- whole steps from the copied initial state (circle and square scenes, and
+  the fluid-only scene): u, v, p to 1e-6 of their maximum, X, Y, phi to 1e-8;
+- the initial fields of the GPU's own initialisation: the fluid-only
+  velocity to 1e-13 (the pulse formula, CUDA's exp/sin/cos against glibc's);
+- l_comparison against the reference's on identical states (both grids
+  copied from reference runs; refinement factors 2 and 3): every norm to
+  1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import oracle_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle_available(), reason="oracle/_ref not built")]
+
+FIELDS = "u v p rho ux uy vx vy ud vd ul vl ur vr uu vu c0 c1 c2 c3 s11 s12 s21 s22".split()
+SFIELDS = "X Y nX nY Xx Xy Yx Yy Xd Yd Xl Yl Xr Yr Xu Yu".split()
+PAD = (0.4, 0.4, 0.8)
+CIRCLE = [("circle", (-0.1, 0.0, 0.6, 0.0, 0.0, 0.0, 0.0), 1.0, 3.0)]
+SQUARE = [("square", (-0.1, 0.0, 0.6, 0.0, 0.0, 0.0, 0.0), 1.0, 1.0)]
+
+
+def _rel(a, b):
+    s = np.abs(b).max()
+    return float(np.abs(a - b).max() / (s if s > 0 else 1.0))
+
+
+def _gpu(m, objects, visc, ntrace):
+    from incrmt_b200 import capi
+    g = capi.Simulation(m, m, visc=visc, ntrace=ntrace, x_prd=True, y_prd=True, pulses=True)
+    for kind, p, G, rhos in objects:
+        add = g.add_circle if kind == "circle" else g.add_square
+        add(p[0], p[1], p[2], G, rhos, grav=p[6], uu=p[3], vv=p[4], omega=p[5], set_velocity=False)
+    return g
+
+
+def _pair(m, objects, visc=1e-3, ntrace=16):
+    from oracle import refsim
+    r = refsim.RefSim(m, ntrace=ntrace, objects=objects, visc=visc, pulses=PAD)
+    g = _gpu(m, objects, visc, ntrace)
+    dt_reg = g.initialize(*PAD)
+    assert abs(dt_reg - r.scalars()["dt_reg"]) <= 1e-15 * dt_reg
+    if ntrace:
+        g.set_tracers(r.tracers()[:, :2])
+    dt, _ = refsim.frame_dt(r.scalars()["dt_reg"])
+    return r, g, dt
+
+
+def _copy(r, g, nobj):
+    for f in FIELDS:
+        g.set(f, r.get(f))
+    for k in range(nobj):
+        for f in SFIELDS + ["phi", "status"]:
+            g.set(f, r.get(f, k), k)
+    g.set_mg(0, r.mg(0))
+    g.set_mg(1, r.mg(1))
+    g.time = r.scalars()["time"]
+
+
+@pytest.fixture(scope="module")
+def evolved(gpu):
+    r, g, dt = _pair(64, CIRCLE)
+    r.step(dt, 20)
+    yield r, g, dt
+    r.close()
+    g.close()
+
+
+STAGES = [
+    ("normal_derivatives_velocity", ["normal_derivatives_velocity", "normal_derivatives_refmap"], 1e-11),
+    ("godunov_tang", ["godunov_tang", "edge_boundary_conditions"], 1e-11),
+    ("tangential_derivatives", ["tangential_derivatives"], 1e-11),
+    ("half_time_edge_velocities", ["half_time_edge_velocities", "half_time_edge_refmap"], 1e-11),
+    ("godunov", ["godunov", "edge_boundary_conditions"], 1e-11),
+    ("mac_projection", ["mac_projection"], 1e-9),
+    ("update_reference_map", ["update_reference_map"], 1e-11),
+    ("pin", ["pin"], 1e-9),
+    ("set_boundaries", ["set_boundaries"], 1e-11),
+    ("compute_stress", ["compute_stress"], 1e-11),
+    ("compute_ustar", ["compute_ustar"], 1e-11),
+    ("finite_element_projection", ["finite_element_projection", "copy_pressure"], 1e-9),
+    ("update_velocity", ["update_velocity"], 1e-11),
+    ("set_rho", ["set_rho"], 1e-11),
+    ("build_band", ["build_band"], 1e-9),
+    ("extrapolate", ["extrapolate"], 1e-11),
+    ("step_forward", ["step_forward"], 1e-9),
+]
+
+
+@pytest.mark.parametrize("stage,ref_stages,tol", STAGES, ids=[s[0] for s in STAGES])
+def test_stage_matches_reference(evolved, stage, ref_stages, tol):
+    r, g, dt = evolved
+    _copy(r, g, 1)
+    for s in ref_stages:
+        r.stage(s, dt)
+    g.stage(stage, dt)
+    errs = {f: _rel(g.get(f), r.get(f)) for f in FIELDS}
+    errs.update({"obj_" + f: _rel(g.get(f, 0), r.get(f, 0)) for f in SFIELDS + ["phi"]})
+    bad = {f: e for f, e in errs.items() if e > tol}
+    assert not bad, bad
+    assert np.array_equal(g.get("status", 0), r.get("status", 0))
+
+
+@pytest.mark.parametrize("objects", [CIRCLE, SQUARE, []], ids=["circle", "square", "fluid"])
+def test_steps_from_initial_state(gpu, objects):
+    r, g, dt = _pair(48, objects)
+    _copy(r, g, len(objects))
+    r.step(dt, 20)
+    g.step(dt, 20)
+    for f, tol in [("u", 1e-6), ("v", 1e-6), ("p", 1e-6)]:
+        e = _rel(g.get(f)[2:-2, 2:-2], r.get(f)[2:-2, 2:-2])
+        assert e <= tol, (f, e)
+    for k in range(len(objects)):
+        for f in ["X", "Y", "phi"]:
+            e = _rel(g.get(f, k)[2:-2, 2:-2], r.get(f, k)[2:-2, 2:-2])
+            assert e <= 1e-8, (f, k, e)
+    r.close()
+    g.close()
+
+
+def test_initial_pulses_velocity(gpu):
+    r, g, dt = _pair(48, [], ntrace=0)
+    for f in ["u", "v"]:
+        e = _rel(g.get(f)[2:-2, 2:-2], r.get(f)[2:-2, 2:-2])
+        assert e <= 1e-13, (f, e)
+    r.close()
+    g.close()
+
+
+@pytest.mark.parametrize("mc,mf", [(32, 64), (32, 96)])
+def test_l_comparison_matches_reference(gpu, mc, mf):
+    from oracle import refsim
+    runs = {}
+    for m in (mc, mf):
+        r, g, dt = _pair(m, CIRCLE, ntrace=0)
+        r.step(refsim.frame_dt(r.scalars()["dt_reg"])[0], 4)
+        _copy(r, g, 1)
+        runs[m] = (r, g)
+    ref = runs[mc][0].l_comparison(runs[mf][0])
+    got = runs[mc][1].l_comparison(runs[mf][1])
+    assert np.allclose(got, ref, rtol=1e-12, atol=0), np.stack([got, ref])
+    # the differences left in the coarse c0 (velocity) and c1 (pressure)
+    for f in ["c0", "c1"]:
+        e = _rel(runs[mc][1].get(f)[2:-2, 2:-2], runs[mc][0].get(f)[2:-2, 2:-2])
+        assert e <= 1e-12, (f, e)
+    for r, g in runs.values():
+        r.close()
+        g.close()

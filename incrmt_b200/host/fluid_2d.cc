@@ -119,7 +119,39 @@ void obj_circle::describe(incrmt_object_desc &d) const {
     memcpy(d.params, p, sizeof(p));
 }
 
+void obj_square::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_SQUARE;
+    const double p[8] = {cx, cy, cr, uu, vv, omega, grav, 0};
+    memcpy(d.params, p, sizeof(p));
+}
+
 // ---------------------------------------------------------------- fluid_2d
+
+void fluid_2d::l_comparison(fluid_2d &f2d, double *err) {
+    if (f2d.m % m != 0 || f2d.n % n != 0) {
+        fputs("Grid dimension is not a multiple of the finer grid\n", stderr);
+        exit(1);
+    }
+    incrmt_check(incrmt_l_comparison(h, f2d.h, err), "incrmt_l_comparison");
+}
+
+double fluid_2d::avg_v_cycles_mac() {
+    incrmt_sim_stats st;
+    incrmt_check(incrmt_get_stats(h, &st), "incrmt_get_stats");
+    const long long dv = st.vcycles_mac - vc_read[0], ds = st.solves_mac - vc_read[1];
+    vc_read[0] = st.vcycles_mac;
+    vc_read[1] = st.solves_mac;
+    return ds ? static_cast<double>(dv) / ds : 0;
+}
+
+double fluid_2d::avg_v_cycles_fem() {
+    incrmt_sim_stats st;
+    incrmt_check(incrmt_get_stats(h, &st), "incrmt_get_stats");
+    const long long dv = st.vcycles_fem - vc_read[2], ds = st.solves_fem - vc_read[3];
+    vc_read[2] = st.vcycles_fem;
+    vc_read[3] = st.solves_fem;
+    return ds ? static_cast<double>(dv) / ds : 0;
+}
 
 fluid_2d::fluid_2d(int m_, int n_, sim_type &sim_t_, double visc_, double rhof_, double tw_, double pinw_,
                    int ntrace_, unsigned int fflags_, const char *filename_)
@@ -143,7 +175,7 @@ void fluid_2d::create() {
     const double U = sim_t.flow_speed();
     if (U != 0) zpr = true;  // sim_horiz_flow::start (sim_type.cc:59-64)
     incrmt_phys p = {visc, rhof, tw, pinw, sim_t.w_scale, sim_t.w_force, ntrace, zpr ? 1 : 0, precision, 1e-9,
-                     U != 0 ? 1 : 0, U};
+                     U != 0 ? 1 : 0, U, sim_t.velocity_pulses() ? 1 : 0};
     incrmt_check(incrmt_create(&g, &p, &h), "incrmt_create");
     created = true;
 }

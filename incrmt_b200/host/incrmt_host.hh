@@ -40,6 +40,16 @@ struct sim_type {
     virtual ~sim_type() {}
     /** Horizontal inflow speed of sim_horiz_flow, or 0. */
     virtual double flow_speed() const { return 0; }
+    /** Whether the fluid starts with sim_velocity_pulses' velocity. */
+    virtual bool velocity_pulses() const { return false; }
+};
+
+/** Six incompressible Gaussian velocity pulses on the doubly periodic
+ * [-1,1]^2 (sim_velocity_pulses, sim_type.hh:99-114, sim_type.cc:43-47);
+ * the scenario of conv_test. */
+struct sim_velocity_pulses : public sim_type {
+    sim_velocity_pulses() : sim_type(-1, 1, -1, 1, true, true) {}
+    bool velocity_pulses() const override { return true; }
 };
 
 /** Uniform flow entering through the left edge of a y-periodic channel with
@@ -131,6 +141,17 @@ struct obj_circle : public object {
     void describe(incrmt_object_desc &d) const override;
 };
 
+/** Square of half side cr centred at (cx, cy) with an initial velocity and
+ * spin and a downward acceleration grav (obj_square, object.hh:142-152). */
+struct obj_square : public object {
+    const double cx, cy, cr, uu, vv, omega, grav;
+    obj_square(double cx_, double cy_, double cr_, double grav_ = 0)
+        : cx(cx_), cy(cy_), cr(cr_), uu(0), vv(0), omega(0), grav(grav_) {}
+    obj_square(double cx_, double cy_, double cr_, double uu_, double vv_, double omega_, double grav_ = 0)
+        : cx(cx_), cy(cy_), cr(cr_), uu(uu_), vv(vv_), omega(omega_), grav(grav_) {}
+    void describe(incrmt_object_desc &d) const override;
+};
+
 /** The fluid-structure simulation (fluid_2d.hh:29-178): same constructor,
  * add_object / initialize / solve / step_forward / write_files sequence and
  * output directory layout. The state lives on the GPU. */
@@ -163,6 +184,14 @@ class fluid_2d {
         void step_forward(double dt);
         void write_files(int sn);
         void save_header(double duration, int frames);
+        /** Error norms against the finer simulation f2d (fluid_2d::l_comparison,
+         * fluid_2d_io.cc:186-281): 32 doubles into err. */
+        void l_comparison(fluid_2d &f2d, double *err);
+        /** Mean V-cycles per MAC / FEM projection since the previous call
+         * (mgs_base::avg_v_cycles resets its counters when read,
+         * mgs_common.hh:59-65). */
+        double avg_v_cycles_mac();
+        double avg_v_cycles_fem();
         /** Steps of size adt <= dt_reg that cover interval (fluid_2d.hh:173-177). */
         inline int timestep_select(double interval, double &adt) {
             int l = static_cast<int>(interval / dt_reg) + 1;
@@ -180,6 +209,7 @@ class fluid_2d {
         std::vector<double> dbuf;
         bool const_rho;
         bool created;
+        long long vc_read[4] = {0, 0, 0, 0};  // MAC V-cycles, solves, FEM V-cycles, solves at the last read
         void create();
         void output(const char *prefix, int mode, int sn);
         void output(const char *prefix, int mode, int sn, const int box[4]);

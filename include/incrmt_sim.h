@@ -58,6 +58,19 @@ typedef struct incrmt_phys {
                                      object.cc:420-496), tracking ntrace points along its length */
 #define INCRMT_OBJ_SQUARE      5  /* params: cx, cy, cr, uu, vv, omega, grav: a square of half side cr
                                      (obj_square, object.hh:142-152, object.cc:41-44, 83-87) */
+#define INCRMT_OBJ_SEVEN_POINT 6  /* params: cx, cy, cr, piv_r, th_max, omega: a seven-pointed star
+                                     spun by a stiff anchor of radius piv_r (obj_seven_point,
+                                     object.hh:176-213, object.cc:100-147) */
+#define INCRMT_OBJ_FLAPPER     7  /* params: cx, cy, cr, cl, ar, al, theta, m_stretch, T: a rod that
+                                     swims by periodically contracting its actuated core
+                                     (obj_flapper, object.hh:245-285, object.cc:284-308) */
+#define INCRMT_OBJ_PISTON      8  /* params: lx, ly, cx, y_start, y_end, duration, anch_r: a block
+                                     dragged by an anchor moving from y_start to y_end, tracking the
+                                     point (-cx, y_start) (obj_piston, object.hh:369-418,
+                                     object.cc:224-269) */
+#define INCRMT_OBJ_CIRCLE_TRACK 9 /* params: cx, cy, cr, uu, vv, omega: a circle tracking the points
+                                     (cx -+ cr/2, cy) (obj_circle_track, object.hh:509-538,
+                                     object.cc:504-549) */
 
 /** An object plus its material constants (object*, mat_const;
  * fluid_2d::add_object, fluid_2d.cc:74-90; obj_field.hh:15-29). */
@@ -65,7 +78,7 @@ typedef struct incrmt_object_desc {
     int type;
     double G, rhos, ev_trans_mult;
     int set_velocity;
-    double params[8];
+    double params[12];
 } incrmt_object_desc;
 
 /** Field ids for get/set: 0..23 the members of struct field in order
@@ -138,6 +151,12 @@ int incrmt_get_tracers(incrmt_sim *h, double *host);
 
 /** Object-tracked points: records of 6 doubles (x, y, stage velocity, X, Y). */
 int incrmt_get_object_tracers(incrmt_sim *h, double *host, int *count);
+
+/** Sets the object-tracked points (count records of 6 doubles, the layout of
+ * incrmt_get_object_tracers; count must equal the number of tracked points)
+ * and the step counter of their recording (obj_track::count: steps since the
+ * last record, 1 after one), as when restarting from a saved state. */
+int incrmt_set_object_tracers(incrmt_sim *h, const double *host, int count, int track_count);
 
 /** Tracked-point records collected so far, 1 + 4*K doubles each for the K
  * object tracers of incrmt_get_object_tracers: the time, then for every

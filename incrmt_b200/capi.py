@@ -214,6 +214,10 @@ OBJ_ROUNDED_ROD = 2
 OBJ_ELLIPSE = 3
 OBJ_FLAG = 4
 OBJ_SQUARE = 5
+OBJ_SEVEN_POINT = 6
+OBJ_FLAPPER = 7
+OBJ_PISTON = 8
+OBJ_CIRCLE_TRACK = 9
 FIELD_PHI = 200
 FIELD_STATUS = 201
 FIELDS = {n: k for k, n in enumerate(
@@ -244,10 +248,15 @@ class Phys(ctypes.Structure):
                 ("pulses", ctypes.c_int)]
 
 
+def _params(*p):
+    """The object parameter array of incrmt_object_desc (12 doubles)."""
+    return (ctypes.c_double * 12)(*p)
+
+
 class ObjectDesc(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("G", ctypes.c_double), ("rhos", ctypes.c_double),
                 ("ev_trans_mult", ctypes.c_double), ("set_velocity", ctypes.c_int),
-                ("params", ctypes.c_double * 8)]
+                ("params", ctypes.c_double * 12)]
 
 
 class SimStats(ctypes.Structure):
@@ -282,6 +291,7 @@ def _sim_sigs(L):
     L.incrmt_get_stats.argtypes = [P, ctypes.POINTER(SimStats)]
     L.incrmt_sim_set_profiling.argtypes = [P, I]
     L.incrmt_sim_set_windows.argtypes = [P, I]
+    L.incrmt_set_object_tracers.argtypes = [P, dp, I, I]
     L.incrmt_l_comparison.argtypes = [P, P, dp]
     L.incrmt_sim_profile.argtypes = [P, dp]
     L.incrmt_sim_mg_profile.argtypes = [P, I, dp, dp, ctypes.POINTER(ctypes.c_longlong)]
@@ -324,7 +334,7 @@ class Simulation:
     def add_simple_spin(self, r_scale=0.8, a1=0.5, a2=0.125, piv_r=0.2, th_max=np.pi, omega=1.0,
                         G=48.0, rhos=3.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_SIMPLE_SPIN, G, rhos, ev_trans_mult, 1,
-                       (ctypes.c_double * 8)(r_scale, a1, a2, piv_r, th_max, omega, 0, 0))
+                       _params(r_scale, a1, a2, piv_r, th_max, omega, 0, 0))
         self._add(d)
 
     def add_circle(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0,
@@ -332,28 +342,50 @@ class Simulation:
         """set_velocity is mat_const::set_velocity: whether the solid's own
         velocity replaces the scenario's fluid velocity at initialisation."""
         d = ObjectDesc(OBJ_CIRCLE, G, rhos, ev_trans_mult, int(set_velocity),
-                       (ctypes.c_double * 8)(cx, cy, cr, uu, vv, omega, grav, 0))
+                       _params(cx, cy, cr, uu, vv, omega, grav, 0))
         self._add(d)
 
     def add_square(self, cx, cy, cr, G, rhos, grav=0.0, uu=0.0, vv=0.0, omega=0.0, ev_trans_mult=1.0,
                    set_velocity=True):
         d = ObjectDesc(OBJ_SQUARE, G, rhos, ev_trans_mult, int(set_velocity),
-                       (ctypes.c_double * 8)(cx, cy, cr, uu, vv, omega, grav, 0))
+                       _params(cx, cy, cr, uu, vv, omega, grav, 0))
         self._add(d)
+
+    def add_seven_point(self, cx, cy, cr, piv_r, th_max, omega, G, rhos, ev_trans_mult=1.0, set_velocity=True):
+        """obj_seven_point: a seven-pointed star spun by an anchor."""
+        self._add(ObjectDesc(OBJ_SEVEN_POINT, G, rhos, ev_trans_mult, int(set_velocity),
+                             _params(cx, cy, cr, piv_r, th_max, omega)))
+
+    def add_flapper(self, cx, cy, cr, cl, ar, al, theta, m_stretch, T, G, rhos, ev_trans_mult=1.0,
+                    set_velocity=True):
+        """obj_flapper: a rod swimming by contracting its actuated core."""
+        self._add(ObjectDesc(OBJ_FLAPPER, G, rhos, ev_trans_mult, int(set_velocity),
+                             _params(cx, cy, cr, cl, ar, al, theta, m_stretch, T)))
+
+    def add_piston(self, lx, ly, cx, y_start, y_end, duration, anch_r, G, rhos, ev_trans_mult=1.0,
+                   set_velocity=True):
+        """obj_piston: a block dragged by a moving anchor, tracking one point."""
+        self._add(ObjectDesc(OBJ_PISTON, G, rhos, ev_trans_mult, int(set_velocity),
+                             _params(lx, ly, cx, y_start, y_end, duration, anch_r)))
+
+    def add_circle_track(self, cx, cy, cr, uu, vv, omega, G, rhos, ev_trans_mult=1.0, set_velocity=True):
+        """obj_circle_track: a moving circle tracking two points."""
+        self._add(ObjectDesc(OBJ_CIRCLE_TRACK, G, rhos, ev_trans_mult, int(set_velocity),
+                             _params(cx, cy, cr, uu, vv, omega)))
 
     def add_rounded_rod(self, cx, cy, cr, cl, G, rhos, grav=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_ROUNDED_ROD, G, rhos, ev_trans_mult, 1,
-                       (ctypes.c_double * 8)(cx, cy, cr, cl, grav, 0, 0, 0))
+                       _params(cx, cy, cr, cl, grav, 0, 0, 0))
         self._add(d)
 
     def add_ellipse(self, cx, cy, a, b, theta, G, rhos, grav=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_ELLIPSE, G, rhos, ev_trans_mult, 1,
-                       (ctypes.c_double * 8)(cx, cy, a, b, theta, grav, 0, 0))
+                       _params(cx, cy, a, b, theta, grav, 0, 0))
         self._add(d)
 
     def add_flag(self, cx, cy, flag_l, flag_w, flag_a, G, rhos, perturb_v=0.0, ntrace=17, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_FLAG, G, rhos, ev_trans_mult, 1,
-                       (ctypes.c_double * 8)(cx, cy, flag_l, flag_w, flag_a, perturb_v, ntrace, 0))
+                       _params(cx, cy, flag_l, flag_w, flag_a, perturb_v, ntrace, 0))
         self._add(d)
 
     def initialize(self, ev_mult=0.8, dt_pad=0.4, dt_ev_pad=0.8):
@@ -410,6 +442,12 @@ class Simulation:
         out = np.empty(4 * max(self.ntrace, 1))
         check(lib().incrmt_get_tracers(self._h, _dptr(out)))
         return out[:4 * self.ntrace].reshape(self.ntrace, 4)
+
+    def set_object_tracers(self, recs, track_count=1):
+        """Sets the tracked points (records of 6 doubles) and the counter
+        of their recording (incrmt_set_object_tracers)."""
+        recs = np.ascontiguousarray(recs, dtype=np.float64)
+        check(lib().incrmt_set_object_tracers(self._h, _dptr(recs), recs.shape[0], int(track_count)))
 
     def object_tracers(self):
         c = ctypes.c_int()

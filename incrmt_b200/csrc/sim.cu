@@ -283,7 +283,7 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
 int Sim::add_object(const incrmt_object_desc *d) {
     if (initialized) { set_error("objects must be added before initialize"); return INCRMT_ERR_BADARG; }
     if (static_cast<int>(obj.size()) >= kMaxObjects) { set_error("too many objects"); return INCRMT_ERR_BADARG; }
-    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_SQUARE) {
+    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_CIRCLE_TRACK) {
         set_error("unknown object type %d", d->type);
         return INCRMT_ERR_BADARG;
     }
@@ -293,6 +293,10 @@ int Sim::add_object(const incrmt_object_desc *d) {
              : d->type == INCRMT_OBJ_ROUNDED_ROD ? OBJ_ROUNDED_ROD
              : d->type == INCRMT_OBJ_ELLIPSE     ? OBJ_ELLIPSE
              : d->type == INCRMT_OBJ_SQUARE      ? OBJ_SQUARE
+             : d->type == INCRMT_OBJ_SEVEN_POINT ? OBJ_SEVEN_POINT
+             : d->type == INCRMT_OBJ_FLAPPER     ? OBJ_FLAPPER
+             : d->type == INCRMT_OBJ_PISTON      ? OBJ_PISTON
+             : d->type == INCRMT_OBJ_CIRCLE_TRACK ? OBJ_CIRCLE
                                                  : OBJ_FLAG;
     o.set_velocity = d->set_velocity;
     o.G = d->G; o.rhos = d->rhos; o.ev_trans_mult = d->ev_trans_mult;
@@ -304,6 +308,29 @@ int Sim::add_object(const incrmt_object_desc *d) {
         const double scf = p[0] / (1 + p[1] + p[2]);
         o.g[0] = scf * (1 - p[2]); o.g[1] = scf * p[1]; o.g[2] = 2 * scf * p[2];
         o.g[3] = p[3]; o.g[4] = p[4]; o.g[5] = p[5];
+    } else if (d->type == INCRMT_OBJ_CIRCLE_TRACK) {
+        // obj_circle_track(cx,cy,cr,uu,vv,omega) (object.hh:526-527): a circle
+        // without gravity whose tracked points are set up at initialize
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = 0;
+        o.g[4] = p[3]; o.g[5] = p[4]; o.g[6] = p[5];
+    } else if (o.type == OBJ_SEVEN_POINT) {
+        // obj_seven_point(cx,cy,cr,piv_r,th_max,omega) (object.hh:192-194)
+        for (int k = 0; k < 6; k++) o.g[k] = p[k];
+    } else if (o.type == OBJ_FLAPPER) {
+        // obj_flapper(cx,cy,cr,cl,ar,al,theta,m_stretch,T) (object.hh:263-267)
+        if (!(p[4] > 0) || !(p[7] > 0) || !(p[8] > 0)) {
+            set_error("flapper needs ar > 0, m_stretch > 0, T > 0");
+            return INCRMT_ERR_BADARG;
+        }
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = 0;
+        o.g[4] = cos(p[6]); o.g[5] = sin(p[6]); o.g[7] = p[3]; o.g[8] = p[4]; o.g[9] = p[5];
+        o.g[10] = log(p[7]) / p[4];
+        o.g[11] = 2 * M_PI / p[8];
+    } else if (o.type == OBJ_PISTON) {
+        // obj_piston(lx,ly,cx,y_start,y_end,duration,anch_r) (object.hh:390-401)
+        if (!(p[5] > 0)) { set_error("piston needs a positive duration"); return INCRMT_ERR_BADARG; }
+        o.g[0] = 0; o.g[1] = p[3]; o.g[2] = p[0]; o.g[4] = 1. / p[5]; o.g[5] = p[6];
+        o.g[7] = p[1]; o.g[8] = p[2]; o.g[9] = p[4] - p[3];
     } else if (o.type == OBJ_CIRCLE || o.type == OBJ_SQUARE) {
         // obj_circle / obj_square(cx,cy,cr,uu,vv,omega,grav) (object.hh:128-152)
         o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[6];
@@ -383,6 +410,19 @@ void Sim::pre_stress_setup(double t) {
             double ang = t * o.g[5], theta = ang > 2 * M_PI ? 0 : o.g[4] * (1 - cos(ang));
             o.cth = cos(theta);
             o.sth = sin(theta);
+        } else if (o.type == OBJ_SEVEN_POINT) {  // object.cc:128-131
+            double theta = o.g[4] * (1 - cos(t * o.g[5]));
+            o.cth = cos(theta);
+            o.sth = sin(theta);
+        } else if (o.type == OBJ_FLAPPER) {  // object.cc:291-295
+            double a = sin(o.g[11] * t);
+            a *= a * a;
+            a *= a;
+            a *= a;
+            o.act = -o.g[10] * a;
+        } else if (o.type == OBJ_PISTON) {  // object.cc:250-253
+            t *= o.g[4];
+            o.act = o.g[1] + (t >= 1 ? o.g[9] : o.g[9] * t * t * (3 - 2 * t));
         }
     }
 }
@@ -807,16 +847,28 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
             double t = o.g[8] + o.eps;
             o.g[10] = t * t;
             o.g[11] = 0.01 / (dt_reg * dt_reg);
+        } else if (o.type == OBJ_SEVEN_POINT) {  // obj_seven_point::start_extra, object.cc:100-111
+            double t = o.g[3] + o.eps;
+            o.g[6] = t * t;
+            o.g[7] = 0.01 / (dt_reg * dt_reg);
+        } else if (o.type == OBJ_PISTON) {  // obj_piston::start_extra, object.cc:224-237
+            double t = o.g[5] + o.eps;
+            o.g[10] = t * t;
+            o.g[11] = 0.01 / (dt_reg * dt_reg);
         }
     }
     // Object tracers (obj_track) of the first tracking object: the simple
     // spinner's point at 0.9*r_scale on the x axis, recorded every 10 steps
-    // (object.hh:444-453), or the flag's points evenly spaced along its
-    // length from the tail, recorded every 100 steps (object.cc:427-434).
+    // (object.hh:444-453); the flag's points evenly spaced along its length
+    // from the tail, every 100 steps (object.cc:427-434); the piston's point
+    // at (-cx, y_start), every 100 steps (object.hh:390-401); the circle
+    // tracker's points at (cx -+ cr/2, cy), every 32 steps (object.cc:504-512).
     nobjtr = 0;
     trk = -1;
     for (size_t k = 0; k < obj.size() && trk < 0; k++)
-        if (obj[k].type == OBJ_SIMPLE_SPIN || obj[k].type == OBJ_FLAG) trk = static_cast<int>(k);
+        if (obj[k].type == OBJ_SIMPLE_SPIN || obj[k].type == OBJ_FLAG || obj[k].type == OBJ_PISTON ||
+            desc[k].type == INCRMT_OBJ_CIRCLE_TRACK)
+            trk = static_cast<int>(k);
     if (trk >= 0) {
         const ObjDev &o = obj[trk];
         std::vector<double> h;
@@ -824,6 +876,14 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
             const double x = 0.9 * desc[trk].params[0];
             h = {x, 0, 0, 0, x, 0};
             track_every = 10;
+        } else if (o.type == OBJ_PISTON) {
+            const double x = -o.g[8], y = o.g[1];
+            h = {x, y, 0, 0, x, y - o.g[1]};  // transform: X = x, Y = y - y_start
+            track_every = 100;
+        } else if (o.type == OBJ_CIRCLE) {
+            const double x0 = o.g[0] - 0.5 * o.g[2], x1 = o.g[0] + 0.5 * o.g[2], y = o.g[1];
+            h = {x0, y, 0, 0, x0 - o.g[0], y - o.g[1], x1, y, 0, 0, x1 - o.g[0], y - o.g[1]};
+            track_every = 32;
         } else {
             const int nt = static_cast<int>(desc[trk].params[6]);
             const double step = nt == 1 ? 0. : o.g[2] / (nt - 1);
@@ -1196,6 +1256,18 @@ int incrmt_get_object_tracers(incrmt_sim *h, double *host, int *count) {
     *count = S.nobjtr;
     if (host && S.nobjtr > 0)
         INCRMT_CK(cudaMemcpyAsync(host, S.otm, sizeof(double) * 6 * S.nobjtr, cudaMemcpyDeviceToHost, S.stream));
+    INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_set_object_tracers(incrmt_sim *h, const double *host, int count, int track_count) {
+    if (!h || !host) { set_error("null argument"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    if (count != S.nobjtr) { set_error("%d tracked points given, the simulation has %d", count, S.nobjtr); return INCRMT_ERR_BADARG; }
+    if (track_count < 1) { set_error("bad track counter %d", track_count); return INCRMT_ERR_BADARG; }
+    if (count > 0)
+        INCRMT_CK(cudaMemcpyAsync(S.otm, host, sizeof(double) * 6 * count, cudaMemcpyHostToDevice, S.stream));
+    S.track_count = track_count;
     INCRMT_CK(cudaStreamSynchronize(S.stream));
     return INCRMT_OK;
 }

@@ -24,6 +24,9 @@ enum ObjType : int {
     OBJ_ELLIPSE = 3,      // rotated ellipse under gravity (no reference counterpart)
     OBJ_FLAG = 4,         // obj_flag (object.hh:471-505, object.cc:420-496)
     OBJ_SQUARE = 5,       // obj_square (object.hh:142-152, object.cc:41-44, 83-87)
+    OBJ_SEVEN_POINT = 6,  // obj_seven_point (object.hh:176-213, object.cc:100-147)
+    OBJ_FLAPPER = 7,      // obj_flapper (object.hh:245-285, object.cc:284-308)
+    OBJ_PISTON = 8,       // obj_piston (object.hh:369-418, object.cc:224-269)
 };
 
 /** Device description of one solid: material constants (mat_const,
@@ -39,10 +42,15 @@ struct ObjDev {
     // K_stiff}; circle and square {cx, cy, cr, grav, uu, vv, omega}; rounded rod
     // {cx, cy, cr, grav, 0, 0, 0, cl}; ellipse {cx, cy, a, grav, 0, 0, 0, b,
     // cos theta, sin theta}; flag {cx, cy, flag_l, 0, 0, 0, 0, flag_w, flag_a,
-    // perturb_v, flag_thresh, K_stiff}.
+    // perturb_v, flag_thresh, K_stiff}; seven-point star {cx, cy, cr, piv_r,
+    // th_max, omega, piv_thresh, K_stiff}; flapper {cx, cy, cr, 0, cos theta,
+    // sin theta, 0, cl, ar, al, amp, omega}; piston {0, y_start, lx, 0, idur,
+    // anch_r, 0, ly, cx, len, anch_thresh, K_stiff}.
     double g[12];
-    // Per-step state set on the host before each stress evaluation.
-    double cth, sth;
+    // Per-step state set on the host before each stress evaluation: the
+    // rotation of the spinner's and the star's anchors, the flapper's
+    // contraction or the piston anchor's height.
+    double cth, sth, act;
 };
 
 /** Smoothed Heaviside inside the solid or blur zone (obj_field.hh:110-112). */
@@ -86,6 +94,23 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
         if (gr == 0) return -fmin(o.g[2], o.g[7]);
         return (r - 1) * r / gr;
     }
+    if (o.type == OBJ_SEVEN_POINT) {  // obj_seven_point::phi, object.cc:117-124
+        const double fac = 2 * M_PI / 7.;
+        double theta = fabs(atan2(Y, X)), R = sqrt(X * X + Y * Y);
+        theta = fabs(theta - fac * int(theta / fac + 0.5));
+        X = R * cos(theta) - o.g[2];
+        Y = R * sin(theta);
+        return X * cos(0.25 * fac) - Y * sin(0.25 * fac) > 0 ? sqrt(X * X + Y * Y)
+                                                             : Y * cos(0.25 * fac) + X * sin(0.25 * fac);
+    }
+    if (o.type == OBJ_FLAPPER) {  // obj_flapper::phi, object.cc:284-287
+        const double fX = fabs(X) - o.g[7];
+        return (fX < 0 ? fabs(Y) : sqrt(fX * fX + Y * Y)) - o.g[2];
+    }
+    if (o.type == OBJ_PISTON) {  // obj_piston::phi, object.cc:243-246
+        const double gx = fabs(X) - o.g[2], gy = fabs(Y) - o.g[7];
+        return gx > gy ? gx : gy;
+    }
     if (o.type == OBJ_SQUARE) {  // obj_square::phi, object.cc:83-87
         X = fabs(X) - o.g[2];
         Y = fabs(Y) - o.g[2];
@@ -96,8 +121,13 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
 
 /** Initial reference map (object::transform / obj_standard::transform). */
 __device__ __forceinline__ void obj_transform(const ObjDev &o, double x, double y, double &X, double &Y) {
-    if (o.type != OBJ_SIMPLE_SPIN) { X = x - o.g[0]; Y = y - o.g[1]; }
-    else { X = x; Y = y; }
+    if (o.type == OBJ_SIMPLE_SPIN) { X = x; Y = y; }
+    else if (o.type == OBJ_FLAPPER) {  // translation, then rotation (object.hh:272-276)
+        x -= o.g[0];
+        y -= o.g[1];
+        X = x * o.g[4] + y * o.g[5];
+        Y = -x * o.g[5] + y * o.g[4];
+    } else { X = x - o.g[0]; Y = y - o.g[1]; }  // the piston's g[0] = 0 (object.hh:406-408)
 }
 
 /** Initial solid velocity (object::velocity / obj_standard::velocity,
@@ -108,8 +138,11 @@ __device__ __forceinline__ void obj_velocity(const ObjDev &o, double X, double Y
         const double rsq = X * X + Y * Y;
         u = 0;
         v = rsq < o.g[10] ? o.g[9] * trans_func_in(o, sqrt(rsq) - o.g[8]) : 0.;
-    } else if (o.type != OBJ_SIMPLE_SPIN) { u = o.g[4] - o.g[6] * Y; v = o.g[5] + o.g[6] * X; }
-    else { u = 0; v = 0; }
+    } else if (o.type == OBJ_CIRCLE || o.type == OBJ_SQUARE || o.type == OBJ_ROUNDED_ROD ||
+               o.type == OBJ_ELLIPSE) {
+        u = o.g[4] - o.g[6] * Y;
+        v = o.g[5] + o.g[6] * X;
+    } else { u = 0; v = 0; }  // object::velocity (object.hh:32-34)
 }
 
 /** Extra accelerations (object::accel overrides): the simple spinner's
@@ -133,8 +166,41 @@ __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, d
             ax -= K * (x - X);
             ay -= K * (y - Y);
         }
+    } else if (o.type == OBJ_SEVEN_POINT) {  // obj_seven_point::accel, object.cc:138-147
+        const double delx = x - o.g[0], dely = y - o.g[1], rsq = delx * delx + dely * dely;
+        if (rsq < o.g[6]) {
+            const double rx = X * o.cth - Y * o.sth, ry = X * o.sth + Y * o.cth,
+                         K = o.g[7] * trans_func_in(o, sqrt(rsq) - o.g[3]);
+            ax -= K * (x - rx);
+            ay -= K * (y - ry);
+        }
+    } else if (o.type == OBJ_PISTON) {  // obj_piston::accel, object.cc:260-269
+        const double delx = x - o.g[8], dely = y - o.act, rsq = delx * delx + dely * dely;
+        if (rsq < o.g[10]) {
+            const double K = o.g[11] * trans_func_in(o, sqrt(rsq) - o.g[5]);
+            ax -= K * (x - X);
+            ay -= K * (dely - Y);
+        }
+    } else if (o.type == OBJ_FLAPPER) {
+        // no acceleration (object::accel, object.hh:73-74)
     } else {
         ay -= o.g[3] * trans_func_in(o, phiv);
+    }
+}
+
+/** obj_flapper::actuate (object.cc:301-308): scales the deformation gradient
+ * F = [[a, b], [c, d]] at reference-map position (X, Y) inside the actuated
+ * region by the current contraction o.act. */
+__device__ __forceinline__ void obj_actuate(const ObjDev &o, double X, double Y, double &a, double &b, double &c,
+                                            double &d) {
+    if (o.type != OBJ_FLAPPER) return;
+    const double fX = fabs(X) - o.g[9], ph = (fX < 0 ? fabs(Y) : sqrt(fX * fX + Y * Y)) - o.g[8];
+    if (ph < o.eps) {
+        const double fac = exp(o.act * Y * trans_func_in(o, ph));
+        a *= fac;
+        b *= 1. / fac;
+        c *= fac;
+        d *= 1. / fac;
     }
 }
 

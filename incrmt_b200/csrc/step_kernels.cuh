@@ -446,8 +446,14 @@ __device__ __forceinline__ bool solid_stress(const GridDev &g, const FluidDev &f
         Xy = g.ysp * (s.X[q] - s.X[q - P]);
         Yy = g.ysp * (s.Y[q] - s.Y[q - P]);
     }
-    // F=[[Yy,-Xy],[-Yx,Xx]], sigma=F F^T (mat::AAT, mat.hh:159-161).
-    const double Fa = Yy, Fb = -Xy, Fc = -Yx, Fd = Xx;
+    // F=[[Yy,-Xy],[-Yx,Xx]], the object's actuation applied at the edge's
+    // reference map, sigma=F F^T (mat::AAT, mat.hh:159-161).
+    double Fa = Yy, Fb = -Xy, Fc = -Yx, Fd = Xx;
+    if (o.type == OBJ_FLAPPER) {
+        const double X = left ? 0.5 * (s.X[q] + s.X[q - 1]) : 0.5 * (s.X[q] + s.X[q - P]),
+                     Y = left ? 0.5 * (s.Y[q] + s.Y[q - 1]) : 0.5 * (s.Y[q] + s.Y[q - P]);
+        obj_actuate(o, X, Y, Fa, Fb, Fc, Fd);
+    }
     const double sa = Fa * Fa + Fb * Fb, sb = Fa * Fc + Fb * Fd, sd = Fc * Fc + Fd * Fd;
     const double sfac = (1 / 3.0) * ((sa + sd) + 1);
     const double tf = trans_func_in(o, phiv), G = o.G * tf,

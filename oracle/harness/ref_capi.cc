@@ -105,10 +105,14 @@ ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double vi
     const double tw=2.5,pinw=2.5;
     const unsigned int fflags=8|16|64|128|256|512;
     for(int k=0;k<nobj;k++) {
-        const double *p=params+8*k;
+        const double *p=params+12*k;
         if(types[k]==1) r->obj.push_back(new obj_circle(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
         else if(types[k]==2) r->obj.push_back(new obj_rounded_rod(p[0],p[1],p[2],p[3],p[4]));
         else if(types[k]==5) r->obj.push_back(new obj_square(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
+        else if(types[k]==6) r->obj.push_back(new obj_seven_point(p[0],p[1],p[2],p[3],p[4],p[5]));
+        else if(types[k]==7) r->obj.push_back(new obj_flapper(p[0],p[1],p[2],p[3],p[4],p[5],p[6],p[7],p[8]));
+        else if(types[k]==8) r->obj.push_back(new obj_piston(p[0],p[1],p[2],p[3],p[4],p[5],p[6],r->fa));
+        else if(types[k]==9) r->obj.push_back(new obj_circle_track(p[0],p[1],p[2],p[3],p[4],p[5],r->fa));
         else r->obj.push_back(new obj_flag(p[0],p[1],p[2],p[3],p[4],p[5],static_cast<int>(p[6]),r->fa));
     }
     if(flow_u>0) r->st=new sim_horiz_flow(flow_u,geom[0],geom[1],geom[2],geom[3]);
@@ -138,7 +142,7 @@ ref_sim* make_pulses(int m,double visc,double rhof,int ntrace,int nobj,const int
     const double tw=2.5,pinw=2.5;
     const unsigned int fflags=8|2048;
     for(int k=0;k<nobj;k++) {
-        const double *p=params+8*k;
+        const double *p=params+12*k;
         if(types[k]==5) r->obj.push_back(new obj_square(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
         else r->obj.push_back(new obj_circle(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
     }
@@ -281,6 +285,13 @@ int ref_get_obj_tracers(void *h,int k,double *out) {
     if(o==NULL) return -1;
     memcpy(out,o->tm,sizeof(double)*6*o->ntrace);
     return o->ntrace;
+}
+
+/** obj_track::count of object k (steps since its last record), or -1. */
+int ref_obj_track_count(void *h,int k) {
+    fluid_2d &f=*static_cast<ref_sim*>(h)->f;
+    obj_track *o=dynamic_cast<obj_track*>(f.olist[k]->obj);
+    return o==NULL?-1:o->count;
 }
 
 /** Multigrid solution arrays: which=0 MAC z (m*n), 1 FEM z (m_fem*n_fem),

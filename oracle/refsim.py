@@ -66,6 +66,8 @@ def lib():
     L.ref_pulses_create.restype = P
     L.ref_l_comparison.argtypes = [P, P, dp]
     L.ref_l_comparison.restype = None
+    L.ref_obj_track_count.argtypes = [P, I]
+    L.ref_obj_track_count.restype = I
     L.ref_dims.argtypes = [P, ip]
     L.ref_scalars.argtypes = [P, dp]
     L.ref_set_time.argtypes = [P, D]
@@ -115,6 +117,11 @@ def mg_apply(sys, m, n, rho, z, ax=-1., bx=1., ay=-1., by=1., x_prd=False, y_prd
     return out
 
 
+# object kinds of ref_multi_create (oracle/harness/ref_capi.cc make_multi)
+OBJECT_TYPES = {"circle": 1, "rod": 2, "flag": 3, "square": 5, "star": 6, "flapper": 7, "piston": 8,
+                "circle_track": 9}
+
+
 class RefSim:
     """A reference fluid_2d simulation: the simple-spin scenario, or with
     `objects` a domain of circles and rounded rods.
@@ -135,7 +142,7 @@ class RefSim:
             objects = objects or []
             k = len(objects)
             types = (ctypes.c_int * max(k, 1))(*[{"circle": 1, "square": 5}[o[0]] for o in objects])
-            params = np.zeros((max(k, 1), 8))
+            params = np.zeros((max(k, 1), 12))
             mats = np.zeros((max(k, 1), 2))
             for q, (kind, p, G, rhos) in enumerate(objects):
                 params[q, :len(p)] = p
@@ -149,8 +156,8 @@ class RefSim:
         else:
             n = m if n is None else n
             k = len(objects)
-            types = (ctypes.c_int * k)(*[{"circle": 1, "rod": 2, "flag": 3, "square": 5}[o[0]] for o in objects])
-            params = np.zeros((k, 8))
+            types = (ctypes.c_int * k)(*[OBJECT_TYPES[o[0]] for o in objects])
+            params = np.zeros((k, 12))
             mats = np.zeros((k, 2))
             for q, (kind, p, G, rhos) in enumerate(objects):
                 params[q, :len(p)] = p
@@ -206,6 +213,10 @@ class RefSim:
         out = np.empty(6 * 64)
         c = lib().ref_get_obj_tracers(self.h, k, _dp(out))
         return out[:6 * c].reshape(c, 6)
+
+    def obj_track_count(self, k=0):
+        """obj_track::count of object k: steps since its last record."""
+        return lib().ref_obj_track_count(self.h, k)
 
     def mg(self, which):
         nv = lib().ref_get_mg(self.h, which, None)

@@ -1,0 +1,132 @@
+"""GPU parity for the object types of the remaining ftest scenarios
+(ftest.cc:144-290): the seven-pointed star spun by its anchor
+(obj_seven_point, in ftest's default doubly periodic box), the swimming
+flapper (obj_flapper, actuated deformation gradient), the piston dragged by
+a moving anchor (obj_piston, one tracked point) and the moving circle with two
+tracked points (obj_circle_track). The oracle is the reference's fluid_2d
+with the same objects (oracle/_ref, ref_multi_create).
+
+Both start from the reference at t = 2 (the flapper's contraction,
+-amp sin^12(2 pi t / T), at its largest; the anchors turned or moved), after
+its stress evaluation there (which sets its objects' state for that time, as
+the GPU's incrmt_set_time does) and 10 steps, so that the solids move and
+deform:
+- stages: that state is copied into the GPU simulation, and the stress,
+  half-time, u* and pinning step functions are compared with the tolerances
+  of the other stage tests;
+- steps: 20 whole steps from that state on both: u, v, p to 1e-6 of their
+  maximum, X, Y, phi to 1e-8, the tracked points to 1e-9.
+"""
+import numpy as np
+import pytest
+
+from conftest import oracle_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle_available(), reason="oracle/_ref not built")]
+
+FIELDS = "u v p rho ux uy vx vy ud vd ul vl ur vr uu vu c0 c1 c2 c3 s11 s12 s21 s22".split()
+SFIELDS = "X Y nX nY Xx Xy Yx Yy Xd Yd Xl Yl Xr Yr Xu Yu".split()
+
+# name: (m, n, geom, periodic, visc, [(kind, params, G, rhos)])
+SCENES = {
+    "star": (48, 48, (-1., 1., -1., 1.), (True, True), 1e-3,
+             [("star", (0.0, 0.0, 0.62, 0.16, np.pi, 1.0), 24.0, 3.0)]),
+    "flapper": (48, 48, (-1.5, 1.5, -1.5, 1.5), (False, False), 5e-4,
+                [("flapper", (0.0, -0.3, 0.1, 0.5, 0.08, 0.35, 0.3, 2.2, 8.0), 10.0, 4.0)]),
+    "piston": (32, 80, (-1., 1., 0., 5.), (False, False), 1e-3,
+               [("piston", (0.8, 0.2, 0.6, 0.4, 4.6, 10.0, 0.15), 1.0, 2.0)]),
+    "circle_track": (48, 48, (-1., 1., -1., 1.), (False, False), 1e-3,
+                     [("circle_track", (-0.3, -0.3, 0.25, 0.5, 1.0, 6.0), 24.0, 4.0)]),
+}
+
+
+def _rel(a, b):
+    s = np.abs(b).max()
+    return float(np.abs(a - b).max() / (s if s > 0 else 1.0))
+
+
+def _pair(name):
+    from incrmt_b200 import capi
+    from oracle import refsim
+    m, n, geom, per, visc, objects = SCENES[name]
+    r = refsim.RefSim(m, ntrace=0, n=n, objects=objects, geom=geom, visc=visc, periodic=per)
+    g = capi.Simulation(m, n, ax=geom[0], bx=geom[1], ay=geom[2], by=geom[3], visc=visc, ntrace=0,
+                        x_prd=per[0], y_prd=per[1])
+    for kind, p, G, rhos in objects:
+        add = {"star": g.add_seven_point, "flapper": g.add_flapper, "piston": g.add_piston,
+               "circle_track": g.add_circle_track}[kind]
+        add(*p, G, rhos)
+    dt_reg = g.initialize()
+    assert abs(dt_reg - r.scalars()["dt_reg"]) <= 1e-15 * dt_reg
+    return r, g, 0.9 * dt_reg, len(objects)
+
+
+def _evolve(r, dt):
+    """The reference at t = 2 with its objects' state for that time, 10
+    steps on."""
+    r.set_time(2.0)
+    r.stage("compute_stress", dt)
+    r.step(dt, 10)
+
+
+def _copy(r, g, nobj):
+    for f in FIELDS:
+        g.set(f, r.get(f))
+    for k in range(nobj):
+        for f in SFIELDS + ["phi", "status"]:
+            g.set(f, r.get(f, k), k)
+    g.set_mg(0, r.mg(0))
+    g.set_mg(1, r.mg(1))
+    g.time = r.scalars()["time"]
+
+
+STAGES = [
+    ("compute_stress", ["compute_stress"], 1e-11),
+    ("half_time_edge_velocities", ["half_time_edge_velocities", "half_time_edge_refmap"], 1e-11),
+    ("compute_ustar", ["compute_ustar"], 1e-11),
+    ("pin", ["pin"], 1e-9),
+]
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+@pytest.mark.parametrize("stage,ref_stages,tol", STAGES, ids=[s[0] for s in STAGES])
+def test_stage_matches_reference(gpu, name, stage, ref_stages, tol):
+    r, g, dt, nobj = _pair(name)
+    _evolve(r, dt)
+    # normal derivatives first, so that the half-time stages see real slopes
+    r.stage("normal_derivatives_velocity", dt)
+    r.stage("normal_derivatives_refmap", dt)
+    _copy(r, g, nobj)
+    for s in ref_stages:
+        r.stage(s, dt)
+    g.stage(stage, dt)
+    errs = {f: _rel(g.get(f), r.get(f)) for f in FIELDS}
+    for k in range(nobj):
+        errs.update({f"obj{k}_" + f: _rel(g.get(f, k), r.get(f, k)) for f in SFIELDS + ["phi"]})
+    bad = {f: e for f, e in errs.items() if e > tol}
+    assert not bad, bad
+    r.close()
+    g.close()
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_steps_from_initial_state(gpu, name):
+    r, g, dt, nobj = _pair(name)
+    _evolve(r, dt)
+    _copy(r, g, nobj)
+    if name in ("piston", "circle_track"):
+        g.set_object_tracers(r.obj_tracers(), r.obj_track_count())
+    r.step(dt, 20)
+    g.step(dt, 20)
+    for f, tol in [("u", 1e-6), ("v", 1e-6), ("p", 1e-6)]:
+        e = _rel(g.get(f)[2:-2, 2:-2], r.get(f)[2:-2, 2:-2])
+        assert e <= tol, (f, e)
+    for k in range(nobj):
+        for f in ["X", "Y", "phi"]:
+            e = _rel(g.get(f, k)[2:-2, 2:-2], r.get(f, k)[2:-2, 2:-2])
+            assert e <= 1e-8, (f, k, e)
+    if name in ("piston", "circle_track"):
+        go, ro = g.object_tracers()[:, :2], r.obj_tracers()[:, :2]
+        assert go.shape == ro.shape and np.abs(go - ro).max() <= 1e-9, (go, ro)
+    r.close()
+    g.close()

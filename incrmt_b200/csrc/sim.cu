@@ -1,6 +1,7 @@
 // The simulation handle: device state of one fluid_2d, its time step
 // (fluid_2d::step_forward, fluid_2d.cc:298-369) as a sequence of kernels on
 // one stream, and the C ABI that replaces the fluid_2d interface.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -47,6 +48,8 @@ struct Sim {
     int *h_flags = nullptr;                         // pinned
     double *partial = nullptr;
     double *tm = nullptr, *otm = nullptr;          // passive and object tracers
+    int *d_remap = nullptr;                         // indices of tracers that left the box
+    long long remapped_tracers = 0;
     int ntrace = 0, nobjtr = 0;
     Multigrid mac, fem;
     // Learned warm start of each projection (0 MAC, 1 FEM) and the capture of
@@ -168,6 +171,7 @@ struct Sim {
     int update_reference_map(double dt);
     int tracers(int stage, double dt);
     int record_track();
+    int remap_tracers();
     int fetch_flags();
     int update_velocity(double dt);
     int learned_pre(int sys, const double *b, double *z);
@@ -275,6 +279,7 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     ntx = ((g.m + 1 + 32) >> 5) + 1;
     nty = ((g.n + 1 + 8) >> 3) + 1;
     if (ntrace > 0 && (r = alloc(&tm, 4 * static_cast<size_t>(ntrace)))) return r;
+    if (ntrace > 0) INCRMT_CK(cudaMalloc(&d_remap, sizeof(int) * ntrace));
     if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
     if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
     return INCRMT_OK;
@@ -776,19 +781,56 @@ int Sim::fem_projection(double dt) {
 int Sim::tracers(int st, double dt) {
     Field2 vel{f.u, f.v};
     if (ntrace > 0) {
-        k_tracers<<<cdiv(ntrace, 128), 128, 0, stream>>>(g, vel, tm, ntrace, 4, st, dt, 1, d_flags + 8);
+        if (st == 2) INCRMT_CK(cudaMemsetAsync(d_flags + 8, 0, sizeof(int), stream));
+        k_tracers<<<cdiv(ntrace, 128), 128, 0, stream>>>(g, vel, tm, ntrace, 4, st, dt, 1, d_flags + 8, d_remap);
         launches++;
     }
     if (nobjtr > 0) {
-        k_tracers<<<cdiv(nobjtr, 128), 128, 0, stream>>>(g, vel, otm, nobjtr, 6, st, dt, 0, d_flags + 8);
+        k_tracers<<<cdiv(nobjtr, 128), 128, 0, stream>>>(g, vel, otm, nobjtr, 6, st, dt, 0, nullptr, nullptr);
         launches++;
     }
     INCRMT_CKL("k_tracers");
+    if (st == 2 && ntrace > 0) {
+        int r = remap_tracers();
+        if (r) return r;
+    }
     if (st == 2 && nobjtr > 0) {
         // obj_track::update_tracers (object.cc:358-366): a record every 10 steps.
         if (track_count == track_every) return record_track();
         track_count++;
     }
+    return INCRMT_OK;
+}
+
+/** sim_type::tracer_remap (sim_type.cc:12-17) for the tracers that left the
+ * box in the last stage-2 update, in index order as fluid_2d::update_tracers
+ * visits them (fluid_2d.cc:1476-1479): the wrapped coordinate moves by the box
+ * length and the other is redrawn with the C library's rand() (common.hh:
+ * 28-30), so a host that seeded its tracers with rand() continues the same
+ * sequence. */
+int Sim::remap_tracers() {
+    int n = 0;
+    INCRMT_CK(cudaMemcpyAsync(&n, d_flags + 8, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    INCRMT_CK(cudaStreamSynchronize(stream));
+    if (n == 0) return INCRMT_OK;
+    if (n > ntrace) n = ntrace;
+    std::vector<int> idx(n);
+    std::vector<double> t(4 * static_cast<size_t>(ntrace));
+    INCRMT_CK(cudaMemcpyAsync(idx.data(), d_remap, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
+    INCRMT_CK(cudaMemcpyAsync(t.data(), tm, sizeof(double) * t.size(), cudaMemcpyDeviceToHost, stream));
+    INCRMT_CK(cudaStreamSynchronize(stream));
+    std::sort(idx.begin(), idx.end());
+    auto rnd = [](double a, double b) { return a + ((b - a) / RAND_MAX) * static_cast<double>(rand()); };
+    for (int k : idx) {
+        double &x = t[4 * static_cast<size_t>(k)], &y = t[4 * static_cast<size_t>(k) + 1];
+        if (x < g.ax) x += (g.bx - g.ax), y = rnd(g.ay, g.by);
+        if (x > g.bx) x -= (g.bx - g.ax), y = rnd(g.ay, g.by);
+        if (y < g.ay) y += (g.by - g.ay), x = rnd(g.ax, g.bx);
+        if (y > g.by) y -= (g.by - g.ay), x = rnd(g.ax, g.bx);
+    }
+    INCRMT_CK(cudaMemcpyAsync(tm, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, stream));
+    INCRMT_CK(cudaStreamSynchronize(stream));
+    remapped_tracers += n;
     return INCRMT_OK;
 }
 
@@ -1041,7 +1083,8 @@ void Sim::destroy() {
     for (auto &s : sol) cudaFree(s.s);
     cudaFree(d_frame); cudaFree(d_box);
     d_frame = nullptr; d_box = nullptr; frame_cap = 0;
-    cudaFree(d_win); cudaFree(d_lsbox); cudaFree(d_tiles); cudaFree(d_lcnt);
+    cudaFree(d_win); cudaFree(d_lsbox); cudaFree(d_tiles); cudaFree(d_lcnt); cudaFree(d_remap);
+    d_remap = nullptr;
     d_lcnt = nullptr;
     for (Learned &L : learn) {
         L.w.release();

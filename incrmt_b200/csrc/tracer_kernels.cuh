@@ -102,11 +102,12 @@ __device__ __forceinline__ void bic_vec(const GridDev &g, Field2 F, double x, do
 /** Tracer stages (fluid_2d::tracer_update_1/2, fluid_2d.cc:1445-1459):
  * stage 1 stores the velocity at the position in slots 2,3; stage 2 completes
  * the improved Euler step. Records have `stride` doubles. For passive tracers
- * (remap=1) a tracer that left the box is wrapped back (sim_type::tracer_remap,
- * sim_type.cc:12-17 also redraws the other coordinate at random; that redraw
- * is flagged in *remapped for the host to apply). */
+ * (remap=1) the indices of the tracers that left the box are appended to
+ * list (*remapped counts them): the host applies sim_type::tracer_remap
+ * (sim_type.cc:12-17) to them in index order, since its redraw of the other
+ * coordinate uses the C library's rand() sequence. */
 __global__ void k_tracers(GridDev g, Field2 vel, double *tm, int count, int stride, int stage, double dt,
-                          int remap, int *remapped) {
+                          int remap, int *remapped, int *list) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     double *tp = tm + static_cast<long>(t) * stride;
@@ -119,14 +120,9 @@ __global__ void k_tracers(GridDev g, Field2 vel, double *tm, int count, int stri
     bic_vec(g, vel, tx, ty, vx, vy);
     tp[0] += 0.5 * dt * (tp[2] + vx);
     tp[1] += 0.5 * dt * (tp[3] + vy);
-    if (remap) {
-        const double lx = g.bx - g.ax, ly = g.by - g.ay;
-        bool moved = false;
-        if (tp[0] < g.ax) { tp[0] += lx; moved = true; }
-        if (tp[0] > g.bx) { tp[0] -= lx; moved = true; }
-        if (tp[1] < g.ay) { tp[1] += ly; moved = true; }
-        if (tp[1] > g.by) { tp[1] -= ly; moved = true; }
-        if (moved) atomicAdd(remapped, 1);
+    if (remap && (tp[0] < g.ax || tp[0] > g.bx || tp[1] < g.ay || tp[1] > g.by)) {
+        const int k = atomicAdd(remapped, 1);
+        if (k < count) list[k] = t;
     }
 }
 

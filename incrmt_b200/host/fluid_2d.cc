@@ -125,6 +125,85 @@ void obj_square::describe(incrmt_object_desc &d) const {
     memcpy(d.params, p, sizeof(p));
 }
 
+void obj_seven_point::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_SEVEN_POINT;
+    const double p[6] = {cx, cy, cr, piv_r, th_max, omega};
+    memcpy(d.params, p, sizeof(p));
+}
+
+/** obj_seven_point::start_extra (object.cc:100-111). */
+void obj_seven_point::start(fluid_2d &f) {
+    printf("# Anchoring K_stiff       : %g (1/T^2)\n", 0.01 / (f.dt_reg * f.dt_reg));
+}
+
+void obj_flapper::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_FLAPPER;
+    const double p[9] = {cx, cy, cr, cl, ar, al, theta, m_stretch, T};
+    memcpy(d.params, p, sizeof(p));
+}
+
+obj_piston::~obj_piston() {
+    if (fp != nullptr) fclose(fp);
+}
+
+void obj_piston::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_PISTON;
+    const double p[7] = {lx, ly, cx, y_start, y_end, duration, anch_r};
+    memcpy(d.params, p, sizeof(p));
+}
+
+/** obj_piston::start_extra (object.cc:224-237). */
+void obj_piston::start(fluid_2d &f) {
+    std::vector<char> fn(strlen(filename) + 16);
+    snprintf(fn.data(), fn.size(), "%s.odr/track.dat", filename);
+    fp = open_or_die(fn.data(), "wb");
+    printf("# Anchoring K_stiff       : %g (1/T^2)\n", 0.01 / (f.dt_reg * f.dt_reg));
+}
+
+/** obj_track::file_output (object.cc:344-351) for the piston's point. */
+void obj_piston::track_record(const double *rec) {
+    const double out[3] = {rec[0], rec[3], rec[4]};
+    fwrite(out, sizeof(double), 3, fp);
+}
+
+void obj_piston::write(int k, double time) {
+    if (fp != nullptr) fflush(fp);
+}
+
+obj_circle_track::~obj_circle_track() {
+    if (fp != nullptr) fclose(fp);
+}
+
+void obj_circle_track::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_CIRCLE_TRACK;
+    const double p[6] = {cx, cy, cr, uu, vv, omega};
+    memcpy(d.params, p, sizeof(p));
+}
+
+/** obj_track::start_extra (object.cc:313-316): the track file. */
+void obj_circle_track::start(fluid_2d &f) {
+    std::vector<char> fn(strlen(filename) + 16);
+    snprintf(fn.data(), fn.size(), "%s.odr/track.dat", filename);
+    fp = open_or_die(fn.data(), "wb");
+}
+
+/** obj_circle_track::file_output (object.cc:532-549): the angle from the
+ * first point's position before its correction to its reference position
+ * (-cr/2, 0), unwrapped by the winding count, and its corrected position. */
+void obj_circle_track::track_record(const double *rec) {
+    const double ang = atan2(0. - rec[2], -0.5 * cr - rec[1]);
+    const int q = fabs(ang) > 0.5 * M_PI ? (ang > 0 ? 1 : -1) : 0;
+    if (q == 1 && prev_q == -1) wind--;
+    else if (q == -1 && prev_q == 1) wind++;
+    prev_q = q;
+    const double out[4] = {rec[0], rec[3], rec[4], ang + 2 * M_PI * wind};
+    fwrite(out, sizeof(double), 4, fp);
+}
+
+void obj_circle_track::write(int k, double time) {
+    if (fp != nullptr) fflush(fp);
+}
+
 // ---------------------------------------------------------------- fluid_2d
 
 void fluid_2d::l_comparison(fluid_2d &f2d, double *err) {

@@ -3,11 +3,25 @@
  * covers:
  *
  *   ftest_gpu simple-spin <grid resolution> [<transition width>]
- *             [-d <duration>] [-n <frames>] [-mixed]
+ *   ftest_gpu circ-move | square | seven-star | fluid | flapper | flappers
+ *             <grid resolution>
+ *   ftest_gpu piston <shear modulus> [-grid <m>]
+ *   ftest_gpu multi-drop <grid resolution> <type: 0 circles, 1 squares>
  *   ftest_gpu circles <grid resolution> <count> <seed>
- *             [-d <duration>] [-n <frames>] [-mixed]
- *   ftest_gpu flag <mu> <k_B> <Re> <ar> [<perturb_v>]
- *             [-grid <n>] [-d <duration>] [-n <frames>] [-mixed]
+ *   ftest_gpu flag <mu> <k_B> <Re> <ar> [<perturb_v>] [-grid <n>]
+ *   (each with [-d <duration>] [-n <frames>] [-mixed])
+ *
+ * circ-move, square, seven-star, piston, fluid, flapper, flappers and
+ * multi-drop are ftest's scenarios of those names (ftest.cc:144-333) with its
+ * parameters, output directory (<scenario>.odr, piston_G<G>.odr) and the C
+ * library's rand() drawing the flappers' and drops' placements in the same
+ * order; square, seven-star and fluid run in ftest's default doubly periodic
+ * box (sim_type(), fluid starting at rest or, for fluid, with
+ * sim_velocity_pulses). The reference's multi-drop checks for three
+ * arguments and then reads a fourth (ftest.cc:294-296), so it cannot run as
+ * written; here it takes the documented <grid resolution> <type>. -grid m
+ * runs the piston on m x 5m/2 instead of ftest's 320 x 800. ftest's full (a
+ * solid with periodic reference-map boundary conditions) is not provided.
  *
  * simple-spin is the reference's three-pronged rotor scenario: output in
  * sspin_<m>.odr (or sspin_<m>_tw<tw>.odr), 240 frames over 4 pi. circles
@@ -37,6 +51,9 @@ namespace {
 
 bool se(const char *p1, const char *p2) { return strcmp(p1, p2) == 0; }
 
+/** Random number in [a, b] from the C library's rand() (common.hh:28-30). */
+double rnd(double a, double b) { return a + ((b - a) / RAND_MAX) * static_cast<double>(rand()); }
+
 void check_grid(int m) {
     if (m < 20 || m > 65536) {
         fprintf(stderr, "Supplied grid resolution of %d is too %s\n", m, m < 20 ? "small" : "large");
@@ -48,6 +65,14 @@ void usage() {
     fputs("Syntax: ./ftest_gpu <sim_type> {extra options} [-d <duration>] [-n <frames>] [-grid <n>] [-mixed]\n\n"
           "Simulation types:\n"
           "simple-spin     simple three-pronged rotor: <grid resolution> [<transition width>]\n"
+          "circ-move       circle moving through fluid: <grid resolution>\n"
+          "square          rotating square: <grid resolution>\n"
+          "seven-star      rotating seven-pointed star: <grid resolution>\n"
+          "piston          flexible paddle moving through cavity: <shear modulus>\n"
+          "fluid           fluid only: <grid resolution>\n"
+          "flapper         single flapping swimmer: <grid resolution>\n"
+          "flappers        multiple flapping swimmers: <grid resolution>\n"
+          "multi-drop      multiple objects sedimenting: <grid resolution> <type>\n"
           "circles         seeded circles settling under gravity: <grid resolution> <count> <seed>\n"
           "flag            flapping flag: <mu> <k_B> <Re> <ar> [<perturb_v>]\n",
           stderr);
@@ -106,6 +131,119 @@ int main(int argc, char **argv) {
         obj.push_back(new obj_simple_spin(0.8, 0.5, 0.125, 0.2, M_PI, 1, strdup(fn.c_str())));
         mats.emplace_back(G, rhos, ev_trans_mult, true);
         sim_t = new sim_type(-1, 1, -1, 1, false, false);
+    } else if (se(pos[0], "circ-move")) {
+        if (np != 2) usage();
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        rhos = 4; visc = 1e-3;
+        T = 3.; num_frames = 300;
+        fn = pos[0];
+        obj.push_back(new obj_circle_track(-0.5, -0.5, 0.25, 2, 4, 24, strdup(fn.c_str())));
+        sim_t = new sim_type(-1, 1, -1, 1, false, false);
+    } else if (se(pos[0], "square")) {
+        if (np != 2) usage();
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        rhos = 3;
+        fn = pos[0];
+        obj.push_back(new obj_square(-0.02, 0, 0.5, 0.01, 0, 2));
+    } else if (se(pos[0], "seven-star")) {
+        if (np != 2) usage();
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        rhos = 3;
+        T = 4 * M_PI; num_frames = 600;
+        fn = pos[0];
+        obj.push_back(new obj_seven_point(0, 0, 0.62, 0.16, M_PI, 1));
+    } else if (se(pos[0], "piston")) {
+        if (np != 2) usage();
+        fn = std::string("piston_G") + pos[1];
+        G = atof(pos[1]);
+        if (G <= 0) {
+            fputs("The shear modulus must be positive\n", stderr);
+            return 1;
+        }
+        m = 320; n = 800;
+        if (grid_opt > 0) { m = grid_opt; n = grid_opt * 5 / 2; }
+        T = 20; num_frames = 1000;
+        rhos = 2.;
+        obj.push_back(new obj_piston(0.8, 0.2, 0.6, 0.4, 4.6, 10, 0.15, strdup(fn.c_str())));
+        sim_t = new sim_type(-1, 1, 0, 5, false, false);
+    } else if (se(pos[0], "fluid")) {
+        if (np != 2) usage();
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        visc = 1e-3;
+        T = 20; num_frames = 200;
+        ntrace = 256;
+        fn = pos[0];
+        sim_t = new sim_velocity_pulses;
+    } else if (se(pos[0], "flapper")) {
+        if (np != 2) usage();
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        rhos = 4; G = 10; visc = 5e-4;
+        T = 30; num_frames = 600;
+        fn = pos[0];
+        obj.push_back(new obj_flapper(0, -0.8, 0.026, 0.25, 0.021, 0.14, 0, 2.2, 8));
+        sim_t = new sim_type(-1.5, 1.5, -1.5, 1.5, false, false);
+    } else if (se(pos[0], "flappers")) {
+        if (np != 2) usage();
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        rhos = 4; G = 10; visc = 5e-4;
+        T = 30; num_frames = 1200;
+        fn = pos[0];
+        // 28 non-overlapping flappers at random positions (ftest.cc:262-288)
+        const int cnum = 28;
+        const double wx = 0.25 + 0.026 + 0.01, wy = 0.026 + 0.01;
+        std::vector<double> px, py;
+        while (static_cast<int>(px.size()) < cnum) {
+            const double x = rnd(-1, 1), y = rnd(-1, 1);
+            if (x + wx > 0.98 || x - wx < -0.98 || y + wy > 0.98 || y - wy < -0.98) continue;
+            bool good = true;
+            for (size_t j = 0; j < px.size(); j++)
+                if (fabs(x - px[j]) < 2 * wx && fabs(y - py[j]) < 2 * wy) { good = false; break; }
+            if (good) {
+                px.push_back(x);
+                py.push_back(y);
+                obj.push_back(new obj_flapper(x, y, 0.026, 0.25, 0.021, 0.14, 0, 2.2, rnd(7, 9)));
+            }
+        }
+        sim_t = new sim_type(-1, 1, -1, 1, false, false);
+    } else if (se(pos[0], "multi-drop")) {
+        if (np != 3) usage();
+        const bool square = atoi(pos[2]) == 1;
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        rhos = 3; G = 2; visc = 1e-3;
+        T = 25; num_frames = 1200;
+        fn = pos[0];
+        // 42 non-overlapping circles or squares at random positions
+        // (ftest.cc:305-330); the stored radius is r - 0.05
+        const int cnum = 42;
+        std::vector<double> px, py, pr;
+        while (static_cast<int>(px.size()) < cnum) {
+            const double x = rnd(-1, 1), y = rnd(-1, 1), r = rnd(0.1, 0.25);
+            if (x + r > 1 || x - r < -1 || y + r > 1 || y - r < -1) continue;
+            bool good = true;
+            for (size_t j = 0; j < px.size(); j++) {
+                const double dr = pr[j] + r;
+                if (fabs(x - px[j]) < dr && fabs(y - py[j]) < dr) { good = false; break; }
+            }
+            if (good) {
+                px.push_back(x);
+                py.push_back(y);
+                pr.push_back(r - 0.05);
+                if (square) obj.push_back(new obj_square(x, y, r - 0.05, 0, 0, rnd(-5, 5)));
+                else obj.push_back(new obj_circle(x, y, r - 0.05, 0, 0, rnd(-5, 5)));
+            }
+        }
+        sim_t = new sim_type(-1, 1, -1, 1, false, false);
+    } else if (se(pos[0], "full")) {
+        fputs("Simulation type 'full' (a solid with periodic reference-map boundary conditions) is not provided\n",
+              stderr);
+        return 1;
     } else if (se(pos[0], "circles")) {
         if (np != 4) usage();
         m = atoi(pos[1]);
@@ -168,6 +306,9 @@ int main(int argc, char **argv) {
         fprintf(stderr, "Simulation type '%s' not recognized\n", pos[0]);
         return 1;
     }
+    if (sim_t == nullptr) sim_t = new sim_type();  // ftest's default: doubly periodic [-1,1]^2
+    // ftest's one mat_const for every object (ftest.cc:395)
+    while (mats.size() < obj.size()) mats.emplace_back(G, rhos, ev_trans_mult, true);
     if (T_opt > 0) T = T_opt;
     if (frames_opt > 0) num_frames = frames_opt;
 

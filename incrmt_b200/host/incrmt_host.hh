@@ -152,6 +152,72 @@ struct obj_square : public object {
     void describe(incrmt_object_desc &d) const override;
 };
 
+/** Seven-pointed star of tip radius cr centred at (cx, cy), spun back and
+ * forth by a stiff anchor of radius piv_r (obj_seven_point,
+ * object.hh:176-213). */
+struct obj_seven_point : public object {
+    const double cx, cy, cr, piv_r, th_max, omega;
+    obj_seven_point(double cx_, double cy_, double cr_, double piv_r_, double th_max_, double omega_)
+        : cx(cx_), cy(cy_), cr(cr_), piv_r(piv_r_), th_max(th_max_), omega(omega_) {}
+    void describe(incrmt_object_desc &d) const override;
+    void start(fluid_2d &f) override;
+};
+
+/** Rounded rod that swims by periodically contracting its core
+ * (obj_flapper, object.hh:245-285): caps of radius cr, half-length cl, an
+ * actuated region of caps ar and half-length al, rotated by theta, a maximum
+ * stretch m_stretch and a period T. */
+struct obj_flapper : public object {
+    const double cx, cy, cr, cl, ar, al, theta, m_stretch, T;
+    obj_flapper(double cx_, double cy_, double cr_, double cl_, double ar_, double al_, double theta_,
+                double m_stretch_, double T_)
+        : cx(cx_), cy(cy_), cr(cr_), cl(cl_), ar(ar_), al(al_), theta(theta_), m_stretch(m_stretch_), T(T_) {}
+    void describe(incrmt_object_desc &d) const override;
+};
+
+/** Flexible block of half-size lx x ly dragged by an anchor of radius anch_r
+ * at x = cx that moves from y_start to y_end over the duration, tracking the
+ * point (-cx, y_start) (obj_piston, object.hh:369-418). Writes
+ * <filename>.odr/track.dat: records of three doubles (time, corrected x, y;
+ * obj_track::file_output, object.cc:344-351). */
+struct obj_piston : public object {
+    const double lx, ly, cx, y_start, y_end, duration, anch_r;
+    const char *filename;
+    FILE *fp;
+    obj_piston(double lx_, double ly_, double cx_, double y_start_, double y_end_, double duration_, double anch_r_,
+               const char *filename_)
+        : lx(lx_), ly(ly_), cx(cx_), y_start(y_start_), y_end(y_end_), duration(duration_), anch_r(anch_r_),
+          filename(filename_), fp(nullptr) {}
+    ~obj_piston();
+    void describe(incrmt_object_desc &d) const override;
+    void start(fluid_2d &f) override;
+    bool tracks() const override { return true; }
+    void track_record(const double *rec) override;
+    void write(int k, double time) override;
+};
+
+/** Circle of radius cr centred at (cx, cy) moving and spinning, tracking the
+ * points (cx -+ cr/2, cy) (obj_circle_track, object.hh:509-538). Writes
+ * <filename>.odr/track.dat: records of four doubles (time, the first point's
+ * corrected position, the unwrapped angle from that point to its reference
+ * position; obj_circle_track::file_output, object.cc:532-549). */
+struct obj_circle_track : public object {
+    const double cx, cy, cr, uu, vv, omega;
+    const char *filename;
+    FILE *fp;
+    int prev_q, wind;
+    obj_circle_track(double cx_, double cy_, double cr_, double uu_, double vv_, double omega_,
+                     const char *filename_)
+        : cx(cx_), cy(cy_), cr(cr_), uu(uu_), vv(vv_), omega(omega_), filename(filename_), fp(nullptr), prev_q(0),
+          wind(0) {}
+    ~obj_circle_track();
+    void describe(incrmt_object_desc &d) const override;
+    void start(fluid_2d &f) override;
+    bool tracks() const override { return true; }
+    void track_record(const double *rec) override;
+    void write(int k, double time) override;
+};
+
 /** The fluid-structure simulation (fluid_2d.hh:29-178): same constructor,
  * add_object / initialize / solve / step_forward / write_files sequence and
  * output directory layout. The state lives on the GPU. */

@@ -71,6 +71,8 @@ typedef struct incrmt_phys {
 #define INCRMT_OBJ_CIRCLE_TRACK 9 /* params: cx, cy, cr, uu, vv, omega: a circle tracking the points
                                      (cx -+ cr/2, cy) (obj_circle_track, object.hh:509-538,
                                      object.cc:504-549) */
+#define INCRMT_OBJ_FULL        10 /* no params: a solid filling the whole domain (obj_full,
+                                     object.hh:83-86), used with incrmt_set_solid_prd_bc */
 
 /** An object plus its material constants (object*, mat_const;
  * fluid_2d::add_object, fluid_2d.cc:74-90; obj_field.hh:15-29). */
@@ -222,6 +224,14 @@ int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err);
  * whole-grid passes throughout; a state upload (incrmt_set_field) returns
  * to whole-grid passes until the next rebuild. */
 int incrmt_sim_set_windows(incrmt_sim *h, int on);
+
+/** fluid_2d::solid_prd_bc (fluid_2d.hh:124), set before incrmt_initialize on
+ * a doubly periodic domain: every object's reference map is periodic up to
+ * the box lengths (set_boundaries_solid and edge_boundary_conditions_solid_pre
+ * / _post, fluid_2d.cc:784-835) and the wall force and object accelerations
+ * are off (fluid_2d.cc:1037). ftest's "full" scenario and conv_test's type 2
+ * pair it with INCRMT_OBJ_FULL. */
+int incrmt_set_solid_prd_bc(incrmt_sim *h, int on);
 
 /** Turns timing on or off (CUDA events on the handle's stream; no reference
  * counterpart) and clears the accumulated times: bit 0 times the phases,

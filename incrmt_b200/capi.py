@@ -218,6 +218,7 @@ OBJ_SEVEN_POINT = 6
 OBJ_FLAPPER = 7
 OBJ_PISTON = 8
 OBJ_CIRCLE_TRACK = 9
+OBJ_FULL = 10
 FIELD_PHI = 200
 FIELD_STATUS = 201
 FIELDS = {n: k for k, n in enumerate(
@@ -291,6 +292,7 @@ def _sim_sigs(L):
     L.incrmt_get_stats.argtypes = [P, ctypes.POINTER(SimStats)]
     L.incrmt_sim_set_profiling.argtypes = [P, I]
     L.incrmt_sim_set_windows.argtypes = [P, I]
+    L.incrmt_set_solid_prd_bc.argtypes = [P, I]
     L.incrmt_set_object_tracers.argtypes = [P, dp, I, I]
     L.incrmt_l_comparison.argtypes = [P, P, dp]
     L.incrmt_sim_profile.argtypes = [P, dp]
@@ -372,6 +374,15 @@ class Simulation:
         """obj_circle_track: a moving circle tracking two points."""
         self._add(ObjectDesc(OBJ_CIRCLE_TRACK, G, rhos, ev_trans_mult, int(set_velocity),
                              _params(cx, cy, cr, uu, vv, omega)))
+
+    def add_full(self, G, rhos, ev_trans_mult=1.0, set_velocity=False):
+        """obj_full: a solid filling the whole domain (with set_solid_prd_bc)."""
+        self._add(ObjectDesc(OBJ_FULL, G, rhos, ev_trans_mult, int(set_velocity), _params()))
+
+    def set_solid_prd_bc(self, on=True):
+        """fluid_2d::solid_prd_bc: reference maps periodic up to the box
+        lengths, no wall force; doubly periodic domains, before initialize."""
+        check(lib().incrmt_set_solid_prd_bc(self._h, int(on)))
 
     def add_rounded_rod(self, cx, cy, cr, cl, G, rhos, grav=0.0, ev_trans_mult=1.0):
         d = ObjectDesc(OBJ_ROUNDED_ROD, G, rhos, ev_trans_mult, 1,

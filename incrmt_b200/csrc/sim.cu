@@ -220,6 +220,7 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     g.xp = gr->x_prd ? 1 : 0;
     g.yp = gr->y_prd ? 1 : 0;
     g.pulses = ph->pulses ? 1 : 0;
+    g.solid_prd = 0;  // incrmt_set_solid_prd_bc
     g.mf = g.xp ? g.m : g.m + 1; g.nf = g.yp ? g.n : g.n + 1;  // m_fem, n_fem (fluid_2d.cc:30-31)
     g.hflow = ph->horiz_flow ? 1 : 0;
     g.flow_u = ph->flow_u;
@@ -288,7 +289,7 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
 int Sim::add_object(const incrmt_object_desc *d) {
     if (initialized) { set_error("objects must be added before initialize"); return INCRMT_ERR_BADARG; }
     if (static_cast<int>(obj.size()) >= kMaxObjects) { set_error("too many objects"); return INCRMT_ERR_BADARG; }
-    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_CIRCLE_TRACK) {
+    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_FULL) {
         set_error("unknown object type %d", d->type);
         return INCRMT_ERR_BADARG;
     }
@@ -302,6 +303,7 @@ int Sim::add_object(const incrmt_object_desc *d) {
              : d->type == INCRMT_OBJ_FLAPPER     ? OBJ_FLAPPER
              : d->type == INCRMT_OBJ_PISTON      ? OBJ_PISTON
              : d->type == INCRMT_OBJ_CIRCLE_TRACK ? OBJ_CIRCLE
+             : d->type == INCRMT_OBJ_FULL        ? OBJ_FULL
                                                  : OBJ_FLAG;
     o.set_velocity = d->set_velocity;
     o.G = d->G; o.rhos = d->rhos; o.ev_trans_mult = d->ev_trans_mult;
@@ -344,6 +346,8 @@ int Sim::add_object(const incrmt_object_desc *d) {
         // obj_rounded_rod(cx,cy,cr,cl,grav) (object.hh:229-230); at rest initially
         if (!(p[2] > 0) || !(p[3] >= 0)) { set_error("rounded rod needs cr > 0, cl >= 0"); return INCRMT_ERR_BADARG; }
         o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[4]; o.g[7] = p[3];
+    } else if (o.type == OBJ_FULL) {
+        // obj_full() (object.hh:83-86): no parameters
     } else if (o.type == OBJ_FLAG) {
         // obj_flag(cx,cy,flag_l,flag_w,flag_a,perturb_v,ntrace) (object.cc:420-441)
         if (!(p[2] > 0) || !(p[3] > 0) || !(p[4] >= 0)) { set_error("flag needs positive length and width"); return INCRMT_ERR_BADARG; }
@@ -543,6 +547,11 @@ int Sim::compute_stress() {
 }
 
 int Sim::set_boundaries() {
+    if (g.solid_prd && !obj.empty()) {  // fluid_2d::set_boundaries (fluid_2d.cc:690)
+        k_set_boundaries_solid<<<1, 1024, 0, stream>>>(g, d_sol, static_cast<int>(obj.size()));
+        launches++;
+        INCRMT_CKL("k_set_boundaries_solid");
+    }
     k_set_boundaries<<<1, 1024, 0, stream>>>(g, f);
     launches++;
     INCRMT_CKL("k_set_boundaries");
@@ -984,6 +993,14 @@ int Sim::update_velocity(double dt) {
 /** godunov_upwinding_set<tang> followed by edge_boundary_conditions
  * (fluid_2d.cc:1112-1121, 689-777). */
 int Sim::godunov(bool tang) {
+    const int no = static_cast<int>(obj.size());
+    if (g.solid_prd && no > 0) {
+        // edge_boundary_conditions_solid_pre (fluid_2d.cc:730): it runs after
+        // the interior Godunov pass in the reference, which writes no right
+        // or top solid edge value, so running it first is the same.
+        k_solid_edges_prd<<<1, 1024, 0, stream>>>(g, d_sol, no, 0);
+        launches++;
+    }
     if (tang) k_godunov<true><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles());
     else k_godunov<false><<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, d_sol, tiles());
     launches++;
@@ -993,6 +1010,10 @@ int Sim::godunov(bool tang) {
     }
     if (g.yp) {
         k_wrap_edges_y<<<cdiv(g.m, 256), 256, 0, stream>>>(g, f);
+        launches++;
+    }
+    if (g.solid_prd && no > 0) {  // edge_boundary_conditions_solid_post (fluid_2d.cc:778)
+        k_solid_edges_prd<<<1, 1024, 0, stream>>>(g, d_sol, no, 1);
         launches++;
     }
     INCRMT_CKL("k_godunov");
@@ -1436,6 +1457,18 @@ int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err) {
     INCRMT_CK(cudaMemcpyAsync(err, dev_err, sizeof(double) * 32, cudaMemcpyDeviceToHost, S.stream));
     INCRMT_CK(cudaFreeAsync(part, S.stream));
     INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_set_solid_prd_bc(incrmt_sim *h, int on) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    incrmt::Sim &S = h->s;
+    if (S.initialized) { set_error("solid_prd_bc must be set before initialize"); return INCRMT_ERR_BADARG; }
+    if (on && !(S.g.xp && S.g.yp)) {
+        set_error("periodic reference-map boundaries need a doubly periodic domain");
+        return INCRMT_ERR_BADARG;
+    }
+    S.g.solid_prd = on ? 1 : 0;
     return INCRMT_OK;
 }
 

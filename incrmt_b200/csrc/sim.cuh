@@ -27,6 +27,7 @@ enum ObjType : int {
     OBJ_SEVEN_POINT = 6,  // obj_seven_point (object.hh:176-213, object.cc:100-147)
     OBJ_FLAPPER = 7,      // obj_flapper (object.hh:245-285, object.cc:284-308)
     OBJ_PISTON = 8,       // obj_piston (object.hh:369-418, object.cc:224-269)
+    OBJ_FULL = 9,         // obj_full: solid everywhere (object.hh:83-86)
 };
 
 /** Device description of one solid: material constants (mat_const,
@@ -94,6 +95,7 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
         if (gr == 0) return -fmin(o.g[2], o.g[7]);
         return (r - 1) * r / gr;
     }
+    if (o.type == OBJ_FULL) return -1;  // obj_full::phi (object.hh:85)
     if (o.type == OBJ_SEVEN_POINT) {  // obj_seven_point::phi, object.cc:117-124
         const double fac = 2 * M_PI / 7.;
         double theta = fabs(atan2(Y, X)), R = sqrt(X * X + Y * Y);
@@ -121,7 +123,7 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
 
 /** Initial reference map (object::transform / obj_standard::transform). */
 __device__ __forceinline__ void obj_transform(const ObjDev &o, double x, double y, double &X, double &Y) {
-    if (o.type == OBJ_SIMPLE_SPIN) { X = x; Y = y; }
+    if (o.type == OBJ_SIMPLE_SPIN || o.type == OBJ_FULL) { X = x; Y = y; }  // object::transform
     else if (o.type == OBJ_FLAPPER) {  // translation, then rotation (object.hh:272-276)
         x -= o.g[0];
         y -= o.g[1];
@@ -181,7 +183,7 @@ __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, d
             ax -= K * (x - X);
             ay -= K * (dely - Y);
         }
-    } else if (o.type == OBJ_FLAPPER) {
+    } else if (o.type == OBJ_FLAPPER || o.type == OBJ_FULL) {
         // no acceleration (object::accel, object.hh:73-74)
     } else {
         ay -= o.g[3] * trans_func_in(o, phiv);
@@ -212,6 +214,7 @@ struct GridDev {
     int xp;         // x-periodic (sim_type::x_prd)
     int yp;         // y-periodic (sim_type::y_prd)
     int pulses;     // initial fluid velocity of sim_velocity_pulses
+    int solid_prd;  // periodic reference-map boundary conditions (fluid_2d::solid_prd_bc)
     int hflow;      // sim_horiz_flow inflow at the left edge
     double flow_u;  // its speed
     double ax, bx, ay, by, dx, dy, xsp, ysp, xxsp, yysp;

@@ -188,6 +188,57 @@ __global__ void k_wrap_edges_x(GridDev g, FluidDev f) {
     f.vl[qt + 1] = f.vl[q0];
 }
 
+/** fluid_2d::set_boundaries_solid (fluid_2d.cc:818-835): under periodic
+ * reference-map boundary conditions the ghost columns and rows of every
+ * object's X, Y copy the opposite side shifted by the box length (columns
+ * first, then rows including the corners). One block. */
+__global__ void k_set_boundaries_solid(GridDev g, const SolidDev *sol, int nobj) {
+    const double lx = g.bx - g.ax, ly = g.by - g.ay;
+    const int P = g.P, G = g.n * P;
+    for (int k = 0; k < nobj; k++) {
+        double *X = sol[k].X, *Y = sol[k].Y;
+        for (int j = threadIdx.x; j < g.n; j += blockDim.x) {
+            const int q = g.idx(0, j), r = q + g.m;
+            X[q - 2] = X[r - 2] - lx; Y[q - 2] = Y[r - 2];
+            X[q - 1] = X[r - 1] - lx; Y[q - 1] = Y[r - 1];
+            X[r] = X[q] + lx; Y[r] = Y[q];
+            X[r + 1] = X[q + 1] + lx; Y[r + 1] = Y[q + 1];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x - 2; i < g.m + 2; i += blockDim.x) {
+            const int q = g.idx(i, 0);
+            X[q - 2 * P] = X[q + G - 2 * P]; Y[q - 2 * P] = Y[q + G - 2 * P] - ly;
+            X[q - P] = X[q + G - P]; Y[q - P] = Y[q + G - P] - ly;
+            X[q + G] = X[q]; Y[q + G] = Y[q] + ly;
+            X[q + G + P] = X[q + P]; Y[q + G + P] = Y[q + P] + ly;
+        }
+        __syncthreads();
+    }
+}
+
+/** fluid_2d::edge_boundary_conditions_solid_pre / _post (fluid_2d.cc:784-815):
+ * before the Godunov selection (post = 0) the ghost column -1's right and the
+ * ghost row -1's top reference-map edge values copy column m-1's and row
+ * n-1's, shifted; after it (post = 1) the ghost column m's left and row n's
+ * bottom values copy column 0's and row 0's, shifted. One block. */
+__global__ void k_solid_edges_prd(GridDev g, const SolidDev *sol, int nobj, int post) {
+    const double lx = g.bx - g.ax, ly = g.by - g.ay;
+    for (int k = 0; k < nobj; k++) {
+        const SolidDev &s = sol[k];
+        for (int j = threadIdx.x; j < g.n; j += blockDim.x) {
+            const int q0 = g.idx(0, j), qt = g.idx(g.m - 1, j);
+            if (!post) { s.Xr[q0 - 1] = s.Xr[qt] - lx; s.Yr[q0 - 1] = s.Yr[qt]; }
+            else { s.Xl[qt + 1] = s.Xl[q0] + lx; s.Yl[qt + 1] = s.Yl[q0]; }
+        }
+        for (int i = threadIdx.x; i < g.m; i += blockDim.x) {
+            const int q0 = g.idx(i, 0), qt = g.idx(i, g.n - 1);
+            if (!post) { s.Xu[q0 - g.P] = s.Xu[qt]; s.Yu[q0 - g.P] = s.Yu[qt] - ly; }
+            else { s.Xd[qt + g.P] = s.Xd[q0]; s.Yd[qt + g.P] = s.Yd[q0] + ly; }
+        }
+        __syncthreads();
+    }
+}
+
 /** compute_tangential_stability_derivatives (fluid_2d.cc:953-975), without
  * the dead r0..r3 writes. */
 __global__ void k_tangential(GridDev g, FluidDev f) {
@@ -237,7 +288,7 @@ __device__ __forceinline__ void acceleration(const GridDev &g, const FluidDev &f
     for (int p = kb; p < ke; p++) {
         const int k = to.at(p);
         const double phiv = sol[k].phi[q];
-        if (phiv < obj[k].eps) {
+        if (phiv < obj[k].eps && !g.solid_prd) {
             wall_force(g, x, y, phiv, accx, accy);
             obj_accel(obj[k], x, y, sol[k].X[q], sol[k].Y[q], phiv, ax_, ay_);
         }

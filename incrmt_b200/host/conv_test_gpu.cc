@@ -3,12 +3,12 @@
  *
  *   conv_test_gpu <test_number> [-res r0,r1,...] [-n <intervals>] [-mixed]
  *
- * Test types (low three bits): 0/1 fluid only (mu 1e-3 / 4e-3), 3 solid
- * square (rho_s 1), 4-7 solid circle (rho_s 3, 1, 1, 1; mu 1e-3, 1e-3, 4e-3,
- * 1.6e-2), all in sim_velocity_pulses' doubly periodic [-1,1]^2; bits 8, 16,
- * 32 select the reference's extra-viscosity variants and 64 the longer
- * resolution list. Type 2 (a full solid with periodic solid boundary
- * conditions, fluid_2d::solid_prd_bc) is not provided.
+ * Test types (low three bits): 0/1 fluid only (mu 1e-3 / 4e-3), 2 a solid
+ * filling the box with periodic reference maps (fluid_2d::solid_prd_bc, no
+ * tracers), 3 solid square (rho_s 1), 4-7 solid circle (rho_s 3, 1, 1, 1; mu
+ * 1e-3, 1e-3, 4e-3, 1.6e-2), all in sim_velocity_pulses' doubly periodic
+ * [-1,1]^2; bits 8, 16, 32 select the reference's extra-viscosity variants and
+ * 64 the longer resolution list.
  *
  * All resolutions are stepped together over 50 intervals of 0.02; after every
  * interval each coarser simulation is compared with the finest
@@ -74,10 +74,6 @@ int main(int argc, char **argv) {
         fputs("Test number out of range\n", stderr);
         return 1;
     }
-    if (ctype == 2) {
-        fputs("Test type 2 (full solid with periodic solid boundary conditions) is not provided\n", stderr);
-        return 1;
-    }
     std::vector<int> mtab;
     int nsteps = 50;
     bool mixed = false;
@@ -110,7 +106,8 @@ int main(int argc, char **argv) {
     if (type & 16) dt_ev_pad = 0.4;
     if (type & 32) ev_mult = 0.6;
     std::vector<object *> obj;
-    if (ctype == 3) obj.push_back(new obj_square(-0.1, 0, 0.6, 0, 0, 0));
+    if (ctype == 2) obj.push_back(new obj_full());
+    else if (ctype == 3) obj.push_back(new obj_square(-0.1, 0, 0.6, 0, 0, 0));
     else if (ctype >= 4) obj.push_back(new obj_circle(-0.1, 0, 0.6, 0, 0, 0));
     const double interval = 0.02;
 
@@ -125,9 +122,13 @@ int main(int argc, char **argv) {
         snprintf(buf, sizeof(buf), "cnv_%02d_%d.odr", type, k);
         dirs[k] = buf;
         mkdir(buf, S_IRWXU | S_IRWXG | S_IROTH | S_IXOTH);
-        f2d[k] = new fluid_2d(mtab[k], mtab[k], sim_t, visc[ctype], rhof, tw, pinw, ntrace, fflags, dirs[k].c_str());
+        // The full solid runs without tracers and with periodic solid
+        // boundary conditions (conv_test.cc:116-120)
+        f2d[k] = new fluid_2d(mtab[k], mtab[k], sim_t, visc[ctype], rhof, tw, pinw, ctype == 2 ? 0 : ntrace, fflags,
+                              dirs[k].c_str());
         if (mixed) f2d[k]->precision = INCRMT_PREC_MIXED;
         for (object *o : obj) f2d[k]->add_object(o, mc);
+        if (ctype == 2) f2d[k]->solid_prd_bc = true;
         f2d[k]->initialize(type & 8 ? (ev_mult * mtab[k] / mtab[nsim - 1]) : ev_mult,
                            dt_pad * mtab[nsim - 1] / mtab[k], dt_ev_pad * mtab[nsim - 1] / mtab[k]);
         l[k] = f2d[k]->timestep_select(interval, adt[k]);

@@ -3,7 +3,7 @@
  * covers:
  *
  *   ftest_gpu simple-spin <grid resolution> [<transition width>]
- *   ftest_gpu circ-move | square | seven-star | fluid | flapper | flappers
+ *   ftest_gpu circ-move | square | seven-star | fluid | flapper | flappers | full
  *             <grid resolution>
  *   ftest_gpu piston <shear modulus> [-grid <m>]
  *   ftest_gpu multi-drop <grid resolution> <type: 0 circles, 1 squares>
@@ -11,8 +11,8 @@
  *   ftest_gpu flag <mu> <k_B> <Re> <ar> [<perturb_v>] [-grid <n>]
  *   (each with [-d <duration>] [-n <frames>] [-mixed])
  *
- * circ-move, square, seven-star, piston, fluid, flapper, flappers and
- * multi-drop are ftest's scenarios of those names (ftest.cc:144-333) with its
+ * circ-move, square, seven-star, piston, fluid, flapper, flappers,
+ * multi-drop and full are ftest's scenarios of those names (ftest.cc:144-333) with its
  * parameters, output directory (<scenario>.odr, piston_G<G>.odr) and the C
  * library's rand() drawing the flappers' and drops' placements in the same
  * order; square, seven-star and fluid run in ftest's default doubly periodic
@@ -20,8 +20,9 @@
  * sim_velocity_pulses). The reference's multi-drop checks for three
  * arguments and then reads a fourth (ftest.cc:294-296), so it cannot run as
  * written; here it takes the documented <grid resolution> <type>. -grid m
- * runs the piston on m x 5m/2 instead of ftest's 320 x 800. ftest's full (a
- * solid with periodic reference-map boundary conditions) is not provided.
+ * runs the piston on m x 5m/2 instead of ftest's 320 x 800. full fills the
+ * pulses' doubly periodic box with one solid whose reference map is periodic
+ * up to the box lengths (fluid_2d::solid_prd_bc).
  *
  * simple-spin is the reference's three-pronged rotor scenario: output in
  * sspin_<m>.odr (or sspin_<m>_tw<tw>.odr), 240 frames over 4 pi. circles
@@ -73,6 +74,7 @@ void usage() {
           "flapper         single flapping swimmer: <grid resolution>\n"
           "flappers        multiple flapping swimmers: <grid resolution>\n"
           "multi-drop      multiple objects sedimenting: <grid resolution> <type>\n"
+          "full            full solid with periodic boundaries: <grid resolution>\n"
           "circles         seeded circles settling under gravity: <grid resolution> <count> <seed>\n"
           "flag            flapping flag: <mu> <k_B> <Re> <ar> [<perturb_v>]\n",
           stderr);
@@ -87,7 +89,7 @@ int main(int argc, char **argv) {
     // Trailing options of this driver
     double T_opt = -1;
     int frames_opt = -1, grid_opt = -1;
-    bool mixed = false;
+    bool mixed = false, solid_prd_bc = false;
     std::vector<char *> pos;
     for (int k = 1; k < argc; k++) {
         if (se(argv[k], "-d") && k + 1 < argc) T_opt = atof(argv[++k]);
@@ -241,9 +243,19 @@ int main(int argc, char **argv) {
         }
         sim_t = new sim_type(-1, 1, -1, 1, false, false);
     } else if (se(pos[0], "full")) {
-        fputs("Simulation type 'full' (a solid with periodic reference-map boundary conditions) is not provided\n",
-              stderr);
-        return 1;
+        // A solid filling the doubly periodic box, starting with the pulses'
+        // velocity; no tracers, periodic reference maps (ftest.cc:218-237)
+        if (np != 2) usage();
+        m = n = atoi(pos[1]);
+        check_grid(m);
+        rhos = 1; G = 3; visc = 1e-3;
+        T = 1; num_frames = 200;
+        ntrace = 0;
+        solid_prd_bc = true;
+        fn = pos[0];
+        obj.push_back(new obj_full());
+        mats.emplace_back(G, rhos, ev_trans_mult, false);
+        sim_t = new sim_velocity_pulses;
     } else if (se(pos[0], "circles")) {
         if (np != 4) usage();
         m = atoi(pos[1]);
@@ -318,6 +330,7 @@ int main(int argc, char **argv) {
 
     fluid_2d f2d(m, n, *sim_t, visc, rhof, tw, pinw, ntrace, fflags, fout.c_str());
     if (mixed) f2d.precision = INCRMT_PREC_MIXED;
+    f2d.solid_prd_bc = solid_prd_bc;
     for (size_t k = 0; k < obj.size(); k++) f2d.add_object(obj[k], mats[k]);
     f2d.initialize(ev_mult, dt_pad, dt_ev_pad);
     f2d.solve(T, num_frames);

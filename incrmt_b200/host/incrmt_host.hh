@@ -152,6 +152,12 @@ struct obj_square : public object {
     void describe(incrmt_object_desc &d) const override;
 };
 
+/** A solid filling the whole domain (obj_full, object.hh:83-86), used with
+ * fluid_2d::solid_prd_bc. */
+struct obj_full : public object {
+    void describe(incrmt_object_desc &d) const override { d.type = INCRMT_OBJ_FULL; }
+};
+
 /** Seven-pointed star of tip radius cr centred at (cx, cy), spun back and
  * forth by a stiff anchor of radius piv_r (obj_seven_point,
  * object.hh:176-213). */
@@ -241,6 +247,9 @@ class fluid_2d {
         /** Precision of the projections' V-cycles: INCRMT_PREC_FP64 (the
          * reference's) or INCRMT_PREC_MIXED; set before initialize. */
         int precision;
+        /** Periodic reference maps up to the box lengths, with no wall force
+         * (fluid_2d.hh:124); set before initialize. */
+        bool solid_prd_bc;
         fluid_2d(int m_, int n_, sim_type &sim_t_, double visc_, double rhof_, double tw_, double pinw_,
                  int ntrace_, unsigned int fflags_, const char *filename_);
         ~fluid_2d();

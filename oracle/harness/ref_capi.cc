@@ -128,11 +128,14 @@ ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double vi
 }
 
 /** conv_test's scenario (conv_test.cc:52-125): sim_velocity_pulses on the
- * doubly periodic [-1,1]^2, circles (type 1) or squares (type 5) of
- * (cx,cy,cr,uu,vv,omega,grav) with mat_const(G,rhos,1,false), initialised
- * with the given extra-viscosity and time-step padding factors. */
+ * doubly periodic [-1,1]^2, circles (type 1), squares (type 5) of
+ * (cx,cy,cr,uu,vv,omega,grav) or the full solid (type 10, obj_full) with
+ * mat_const(G,rhos,1,false), initialised with the given extra-viscosity and
+ * time-step padding factors; solid_prd sets fluid_2d::solid_prd_bc as
+ * conv_test's type 2 does (conv_test.cc:120). */
 ref_sim* make_pulses(int m,double visc,double rhof,int ntrace,int nobj,const int *types,const double *params,
-                     const double *mats,double ev_mult,double dt_pad,double dt_ev_pad,const char *base) {
+                     const double *mats,double ev_mult,double dt_pad,double dt_ev_pad,const char *base,
+                     int solid_prd) {
     ref_sim *r=new ref_sim;
     r->fa=new char[strlen(base)+1];
     strcpy(r->fa,base);
@@ -144,6 +147,7 @@ ref_sim* make_pulses(int m,double visc,double rhof,int ntrace,int nobj,const int
     for(int k=0;k<nobj;k++) {
         const double *p=params+12*k;
         if(types[k]==5) r->obj.push_back(new obj_square(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
+        else if(types[k]==10) r->obj.push_back(new obj_full());
         else r->obj.push_back(new obj_circle(p[0],p[1],p[2],p[3],p[4],p[5],p[6]));
     }
     r->st=new sim_velocity_pulses;
@@ -152,6 +156,7 @@ ref_sim* make_pulses(int m,double visc,double rhof,int ntrace,int nobj,const int
         mat_const mc(mats[2*k],mats[2*k+1],1,false);
         r->f->add_object(r->obj[k],mc);
     }
+    r->f->solid_prd_bc=solid_prd!=0;
     r->f->initialize(ev_mult,dt_pad,dt_ev_pad);
     zero_unset_refmap(*r->f);
     return r;
@@ -186,8 +191,8 @@ void* ref_multi_create(int m,int n,const double *geom,int x_prd,int y_prd,double
 
 void* ref_pulses_create(int m,double visc,double rhof,int ntrace,int nobj,const int *types,
                         const double *params,const double *mats,double ev_mult,double dt_pad,
-                        double dt_ev_pad,const char *base) {
-    return make_pulses(m,visc,rhof,ntrace,nobj,types,params,mats,ev_mult,dt_pad,dt_ev_pad,base);
+                        double dt_ev_pad,const char *base,int solid_prd) {
+    return make_pulses(m,visc,rhof,ntrace,nobj,types,params,mats,ev_mult,dt_pad,dt_ev_pad,base,solid_prd);
 }
 
 /** fluid_2d::l_comparison of the coarse simulation h against the fine one

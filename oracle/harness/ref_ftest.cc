@@ -4,7 +4,7 @@
  *   ref_ftest <m> <duration> <frames> <output base path>
  *       simple-spin at m x m;
  *   ref_ftest <scenario> <arg> <duration> <frames> <output base path>
- *       circ-move, square, seven-star, fluid, flapper, flappers <m>;
+ *       circ-move, square, seven-star, fluid, flapper, flappers, full <m>;
  *       piston <G> (on m x 5m/2 with m from the environment variable
  *       REF_PISTON_M, default ftest's 320); multi-drop <m>,<type>;
  * each with ftest's objects, materials, domain, viscosity, fields and
@@ -53,6 +53,7 @@ int main(int argc,char **argv) {
     int m=200,n=200,ntrace=512;
     double tw=2.5,pinw=2.5,rhof=1,rhos=1,visc=1e-3,G=24,ev_mult=0.8,ev_trans_mult=1,dt_pad=0.4,dt_ev_pad=0.8;
     unsigned int fflags=8|16|64|128|256|512;
+    bool set_velocity=true,solid_prd_bc=false;
     sim_type *sim_t=NULL;
     std::vector<object*> obj;
     if(!strcmp(sc,"circ-move")) {
@@ -73,6 +74,10 @@ int main(int argc,char **argv) {
         sim_t=new sim_type(-1,1,0,5,false,false);
     } else if(!strcmp(sc,"fluid")) {
         m=n=atoi(arg);visc=1e-3;ntrace=256;
+        sim_t=new sim_velocity_pulses;
+    } else if(!strcmp(sc,"full")) {
+        m=n=atoi(arg);rhos=1;G=3;visc=1e-3;ntrace=0;set_velocity=false;solid_prd_bc=true;
+        obj.push_back(new obj_full());
         sim_t=new sim_velocity_pulses;
     } else if(!strcmp(sc,"flapper")) {
         m=n=atoi(arg);rhos=4;G=10;visc=5e-4;
@@ -127,7 +132,8 @@ int main(int argc,char **argv) {
     mkdir(fout.c_str(),S_IRWXU|S_IRWXG|S_IROTH|S_IXOTH);
     if(sim_t==NULL) sim_t=new sim_type();
     fluid_2d f2d(m,n,*sim_t,visc,rhof,tw,pinw,ntrace,fflags,fout.c_str());
-    mat_const mc(G,rhos,ev_trans_mult,true);
+    f2d.solid_prd_bc=solid_prd_bc;
+    mat_const mc(G,rhos,ev_trans_mult,set_velocity);
     for(unsigned int k=0;k<obj.size();k++) f2d.add_object(obj[k],mc);
     f2d.initialize(ev_mult,dt_pad,dt_ev_pad);
     f2d.solve(T,frames);

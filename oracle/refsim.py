@@ -62,7 +62,7 @@ def lib():
     L.ref_destroy.argtypes = [P]
     L.ref_multi_create.argtypes = [I, I, dp, I, I, D, D, I, I, ip, dp, dp, ctypes.c_char_p, D]
     L.ref_multi_create.restype = P
-    L.ref_pulses_create.argtypes = [I, D, D, I, I, ip, dp, dp, D, D, D, ctypes.c_char_p]
+    L.ref_pulses_create.argtypes = [I, D, D, I, I, ip, dp, dp, D, D, D, ctypes.c_char_p, I]
     L.ref_pulses_create.restype = P
     L.ref_l_comparison.argtypes = [P, P, dp]
     L.ref_l_comparison.restype = None
@@ -138,10 +138,13 @@ class RefSim:
             self._tmp = tempfile.TemporaryDirectory()
             workdir = self._tmp.name
         if pulses is not None:
-            # conv_test's scenario: pulses = (ev_mult, dt_pad, dt_ev_pad)
+            # conv_test's scenario: pulses = (ev_mult, dt_pad, dt_ev_pad);
+            # a ("full", (), G, rhos) object also sets solid_prd_bc, as
+            # conv_test's type 2 and ftest's "full" do.
             objects = objects or []
             k = len(objects)
-            types = (ctypes.c_int * max(k, 1))(*[{"circle": 1, "square": 5}[o[0]] for o in objects])
+            types = (ctypes.c_int * max(k, 1))(*[{"circle": 1, "square": 5, "full": 10}[o[0]] for o in objects])
+            solid_prd = int(any(o[0] == "full" for o in objects))
             params = np.zeros((max(k, 1), 12))
             mats = np.zeros((max(k, 1), 2))
             for q, (kind, p, G, rhos) in enumerate(objects):
@@ -149,7 +152,8 @@ class RefSim:
                 mats[q] = (G, rhos)
             base = os.path.join(workdir, f"pulses_{m}").encode()
             self.h = lib().ref_pulses_create(m, visc, rhof, ntrace, k, types, _dp(params), _dp(mats),
-                                             float(pulses[0]), float(pulses[1]), float(pulses[2]), base)
+                                             float(pulses[0]), float(pulses[1]), float(pulses[2]), base,
+                                             solid_prd)
         elif objects is None:
             base = os.path.join(workdir, f"sspin_{m}").encode()
             self.h = lib().ref_sspin_create(m, ntrace, base)

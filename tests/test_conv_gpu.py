@@ -66,3 +66,19 @@ def test_driver_output(gpu, tmp_path):
         assert len(v) == 2 + 32 and v[0] == i and abs(v[1] - 0.02 * i) < 1e-12
         assert all(np.isfinite(v))
     assert (tmp_path / "cnv_04_1.odr").is_dir()
+
+
+def test_driver_full_solid(gpu, tmp_path):
+    """Type 2: the full solid with periodic reference maps (conv_test.cc:78-80,
+    116-120) runs and writes finite norms, X and Y among the frames."""
+    exe = os.path.abspath(os.path.join(HOST, "conv_test_gpu"))
+    r = subprocess.run([exe, "2", "-res", "64,32", "-n", "2"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = (tmp_path / "cnv_02.dat").read_text().strip().split("\n")
+    assert len(lines) == 3
+    for line in lines:
+        v = [float(x) for x in line.split()]
+        assert len(v) == 2 + 32 and all(np.isfinite(v))
+    names = os.listdir(tmp_path / "cnv_02_1.odr")
+    assert any(f.startswith("X.") for f in names) and any(f.startswith("Y.") for f in names)

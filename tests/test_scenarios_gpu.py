@@ -1,6 +1,6 @@
 """ftest's other scenarios through the C++ host (ftest_gpu: circ-move,
 square, seven-star, fluid, flapper, flappers, multi-drop with circles and
-with squares, piston; ftest.cc:144-333) against the reference's own classes
+with squares, piston, full; ftest.cc:144-333) against the reference's own classes
 and output writers (oracle/_ref/ref_ftest, the same scenario set-ups), two
 frames each over a short duration, every output file compared:
 
@@ -43,6 +43,7 @@ SCENARIOS = {
     "multi-drop-0": (["multi-drop", "64", "0"], ["multi-drop", "64,0"], "multi-drop", 64, 2.0),
     "multi-drop-1": (["multi-drop", "64", "1"], ["multi-drop", "64,1"], "multi-drop", 64, 2.0),
     "piston": (["piston", "1", "-grid", "32"], ["piston", "1"], "piston_G1", 32, 2.0),
+    "full": (["full", "64"], ["full", "64"], "full", 64, 2.0),
 }
 LOOSE = {
     "circ-move": {"p": 1e-3, "w": 5e-3, "X": 1e-4, "Y": 1e-4, "phi": 1e-4, "trace": 1e-4},

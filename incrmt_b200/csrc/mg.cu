@@ -972,6 +972,20 @@ int Multigrid::set_density_device(const double *d_rho, int ld) {
     return r;
 }
 
+int Multigrid::set_unit_density() {
+    const long N = static_cast<long>(cm + 4) * (cn + 4);
+    double *ones = nullptr;
+    INCRMT_CK(cudaMalloc(&ones, sizeof(double) * N));
+    k_fill<<<cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks, 256, 0, stream>>>(ones, N, 1.0);
+    launches++;
+    int r = set_density_device(ones, cm + 4);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    cudaFree(ones);
+    if (r) return r;
+    INCRMT_CK(e);
+    return INCRMT_OK;
+}
+
 int Multigrid::galerkin_all() {
     for (size_t l = 1; l < lev.size(); l++) {
         MgLevel &F = lev[l - 1], &C = lev[l];

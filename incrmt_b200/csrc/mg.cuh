@@ -77,6 +77,10 @@ public:
                int px, int py, int zpr, cudaStream_t ext = nullptr);
     void destroy();
     int set_density_device(const double *d_rho, int ld = 0);
+    /** Unit density everywhere: the constant-density operators
+     * (mgs_mac_const_rho, mgs_fem_const_rho; mgs_mac.hh, mgs_fem.cc:27-80),
+     * which are the varying-density ones with every 1/rho equal to 1. */
+    int set_unit_density();
     int solve_device(const double *d_b, double *d_z, const incrmt_mg_opts *o,
                      incrmt_mg_stats *st, bool time_it);
     int vcycle64(const double *d_b, double *d_z);

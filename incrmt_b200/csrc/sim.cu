@@ -2,6 +2,7 @@
 // (fluid_2d::step_forward, fluid_2d.cc:298-369) as a sequence of kernels on
 // one stream, and the C ABI that replaces the fluid_2d interface.
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -69,6 +70,10 @@ struct Sim {
     double dt_reg = 0, time = 0;
     double w_scale = 3, w_force = 20, tw = 2.5, pinw = 2.5;
     bool initialized = false;
+    // fluid_2d::const_rho (fluid_2d.cc:126-137): every solid's density within
+    // small_number of the fluid's; the projections then use the constant-
+    // density operators, set once, and pin leaves rho alone.
+    bool const_rho = false;
     long long steps = 0;
     long long vc_mac = 0, vc_fem = 0, solves_mac = 0, solves_fem = 0;
     long long ls_sweeps = 0, ex_sweeps = 0;
@@ -623,7 +628,7 @@ int Sim::pin() {
         INCRMT_CKL("k_pin");
     }
     if ((r = build_bands())) return r;
-    return set_rho();
+    return const_rho ? INCRMT_OK : set_rho();
 }
 
 /** levelset::extrapolate_fields for every object (traverse.hh:235-260),
@@ -694,7 +699,7 @@ int Sim::mac_projection() {
     int outer = cur_phase, r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(INCRMT_PHASE_MG_SETUP))) return r;
-    r = mac.set_density_device(f.rho, g.P);
+    r = const_rho ? INCRMT_OK : mac.set_density_device(f.rho, g.P);
     if (r) return r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(outer))) return r;
@@ -765,7 +770,7 @@ int Sim::fem_projection(double dt) {
     int outer = cur_phase, r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(INCRMT_PHASE_MG_SETUP))) return r;
-    r = fem.set_density_device(f.rho, g.P);
+    r = const_rho ? INCRMT_OK : fem.set_density_device(f.rho, g.P);
     if (r) return r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(outer))) return r;
@@ -967,6 +972,12 @@ int Sim::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
     if ((r = set_boundaries())) return r;
     if ((r = compute_stress())) return r;
     if ((r = set_rho())) return r;
+    // fluid_2d::setup_multigrid with same_rho (fluid_2d.cc:126-137,
+    // fluid_2d.hh:244-248; small_number = 100 DBL_EPSILON, common.hh:16).
+    const_rho = true;
+    for (const auto &o : obj)
+        if (fabs(o.rhos - g.rhof) > 100 * DBL_EPSILON) const_rho = false;
+    if (const_rho && ((r = mac.set_unit_density()) || (r = fem.set_unit_density()))) return r;
     initialized = true;
     INCRMT_CK(cudaStreamSynchronize(stream));
     return INCRMT_OK;

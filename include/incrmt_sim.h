@@ -73,6 +73,16 @@ typedef struct incrmt_phys {
                                      object.cc:504-549) */
 #define INCRMT_OBJ_FULL        10 /* no params: a solid filling the whole domain (obj_full,
                                      object.hh:83-86), used with incrmt_set_solid_prd_bc */
+#define INCRMT_OBJ_TRIANGLE    11 /* params: cx, cy, cr, theta, grav: an equilateral triangle with
+                                     vertices cr from its centre, rotated by theta, falling under grav
+                                     (obj_triangle, object.hh:155-172, object.cc:52-70, 93-95) */
+#define INCRMT_OBJ_LAMPREY     12 /* params: cx, cy, theta, le, dis, w1, w2, T, mlam: a swimmer of
+                                     length le (head dis) and half-widths w1, w2, actuated by a
+                                     contraction wave of period T and maximum mlam (obj_lamprey,
+                                     object.hh:542-595, object.cc:554-581) */
+#define INCRMT_OBJ_HOOP        13 /* params: r_in, r_out, grav: a hoop about the origin; grav is
+                                     kept but, as in the reference, never applied (obj_hoop,
+                                     object.hh:598-611, object.cc:586-588) */
 
 /** An object plus its material constants (object*, mat_const;
  * fluid_2d::add_object, fluid_2d.cc:74-90; obj_field.hh:15-29). */

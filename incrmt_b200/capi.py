@@ -219,6 +219,9 @@ OBJ_FLAPPER = 7
 OBJ_PISTON = 8
 OBJ_CIRCLE_TRACK = 9
 OBJ_FULL = 10
+OBJ_TRIANGLE = 11
+OBJ_LAMPREY = 12
+OBJ_HOOP = 13
 FIELD_PHI = 200
 FIELD_STATUS = 201
 FIELDS = {n: k for k, n in enumerate(
@@ -374,6 +377,21 @@ class Simulation:
         """obj_circle_track: a moving circle tracking two points."""
         self._add(ObjectDesc(OBJ_CIRCLE_TRACK, G, rhos, ev_trans_mult, int(set_velocity),
                              _params(cx, cy, cr, uu, vv, omega)))
+
+    def add_triangle(self, cx, cy, cr, theta, G, rhos, grav=0.0, ev_trans_mult=1.0, set_velocity=True):
+        """obj_triangle: an equilateral triangle under gravity."""
+        self._add(ObjectDesc(OBJ_TRIANGLE, G, rhos, ev_trans_mult, int(set_velocity),
+                             _params(cx, cy, cr, theta, grav)))
+
+    def add_lamprey(self, cx, cy, theta, le, dis, w1, w2, T, mlam, G, rhos, ev_trans_mult=1.0,
+                    set_velocity=True):
+        """obj_lamprey: a swimmer actuated by a travelling contraction wave."""
+        self._add(ObjectDesc(OBJ_LAMPREY, G, rhos, ev_trans_mult, int(set_velocity),
+                             _params(cx, cy, theta, le, dis, w1, w2, T, mlam)))
+
+    def add_hoop(self, r_in, r_out, G, rhos, grav=0.0, ev_trans_mult=1.0, set_velocity=True):
+        """obj_hoop: a ring about the origin."""
+        self._add(ObjectDesc(OBJ_HOOP, G, rhos, ev_trans_mult, int(set_velocity), _params(r_in, r_out, grav)))
 
     def add_full(self, G, rhos, ev_trans_mult=1.0, set_velocity=False):
         """obj_full: a solid filling the whole domain (with set_solid_prd_bc)."""

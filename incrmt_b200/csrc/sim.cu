@@ -294,7 +294,7 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
 int Sim::add_object(const incrmt_object_desc *d) {
     if (initialized) { set_error("objects must be added before initialize"); return INCRMT_ERR_BADARG; }
     if (static_cast<int>(obj.size()) >= kMaxObjects) { set_error("too many objects"); return INCRMT_ERR_BADARG; }
-    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_FULL) {
+    if (d->type < INCRMT_OBJ_SIMPLE_SPIN || d->type > INCRMT_OBJ_HOOP) {
         set_error("unknown object type %d", d->type);
         return INCRMT_ERR_BADARG;
     }
@@ -309,6 +309,9 @@ int Sim::add_object(const incrmt_object_desc *d) {
              : d->type == INCRMT_OBJ_PISTON      ? OBJ_PISTON
              : d->type == INCRMT_OBJ_CIRCLE_TRACK ? OBJ_CIRCLE
              : d->type == INCRMT_OBJ_FULL        ? OBJ_FULL
+             : d->type == INCRMT_OBJ_TRIANGLE    ? OBJ_TRIANGLE
+             : d->type == INCRMT_OBJ_LAMPREY     ? OBJ_LAMPREY
+             : d->type == INCRMT_OBJ_HOOP        ? OBJ_HOOP
                                                  : OBJ_FLAG;
     o.set_velocity = d->set_velocity;
     o.G = d->G; o.rhos = d->rhos; o.ev_trans_mult = d->ev_trans_mult;
@@ -353,6 +356,31 @@ int Sim::add_object(const incrmt_object_desc *d) {
         o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2]; o.g[3] = p[4]; o.g[7] = p[3];
     } else if (o.type == OBJ_FULL) {
         // obj_full() (object.hh:83-86): no parameters
+    } else if (o.type == OBJ_TRIANGLE) {
+        // obj_triangle(cx,cy,cr,theta,grav) (object.cc:52-58): an equilateral
+        // triangle whose side normals point at theta + 2 pi k / 3, at rest
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[2] * 0.5; o.g[3] = p[4];
+        double nor[6];
+        for (int i = 0; i < 3; i++) {
+            nor[2 * i] = cos(p[3] + 2 * M_PI / 3 * i);
+            nor[2 * i + 1] = sin(p[3] + 2 * M_PI / 3 * i);
+        }
+        o.g[8] = nor[0]; o.g[9] = nor[1]; o.g[10] = nor[2]; o.g[11] = nor[3];
+        o.nor2[0] = nor[4]; o.nor2[1] = nor[5];
+    } else if (o.type == OBJ_LAMPREY) {
+        // obj_lamprey(cx,cy,theta,le,dis,w1,w2,T,mlam) (object.hh:568-571)
+        if (!(p[7] > 0) || !(p[8] > 0) || !(p[5] > 0) || !(p[3] > p[4])) {
+            set_error("lamprey needs T > 0, mlam > 0, w1 > 0 and le > dis");
+            return INCRMT_ERR_BADARG;
+        }
+        o.g[0] = p[0]; o.g[1] = p[1]; o.g[2] = p[4]; o.g[3] = p[3] - p[4];
+        o.g[4] = cos(p[2]); o.g[5] = sin(p[2]); o.g[6] = p[5]; o.g[7] = p[6]; o.g[8] = p[7];
+        o.g[9] = log(p[8]);
+    } else if (o.type == OBJ_HOOP) {
+        // obj_hoop(r_in,r_out,grav) (object.hh:608-609): centred on the
+        // origin; its grav is stored but never applied (no accel override)
+        if (!(p[1] > p[0])) { set_error("hoop needs r_out > r_in"); return INCRMT_ERR_BADARG; }
+        o.g[2] = (p[1] - p[0]) * 0.5; o.g[7] = 0.5 * (p[0] + p[1]);
     } else if (o.type == OBJ_FLAG) {
         // obj_flag(cx,cy,flag_l,flag_w,flag_a,perturb_v,ntrace) (object.cc:420-441)
         if (!(p[2] > 0) || !(p[3] > 0) || !(p[4] >= 0)) { set_error("flag needs positive length and width"); return INCRMT_ERR_BADARG; }
@@ -437,6 +465,10 @@ void Sim::pre_stress_setup(double t) {
         } else if (o.type == OBJ_PISTON) {  // object.cc:250-253
             t *= o.g[4];
             o.act = o.g[1] + (t >= 1 ? o.g[9] : o.g[9] * t * t * (3 - 2 * t));
+        } else if (o.type == OBJ_LAMPREY) {  // object.cc:563-568
+            double sh = t / o.g[8], a = 2 * sh;
+            o.act = a < 1 ? o.g[9] * a * a * (3 - 2 * a) : o.g[9];
+            o.shift = sh * o.g[3];
         }
     }
 }

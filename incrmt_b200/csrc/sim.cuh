@@ -28,6 +28,9 @@ enum ObjType : int {
     OBJ_FLAPPER = 7,      // obj_flapper (object.hh:245-285, object.cc:284-308)
     OBJ_PISTON = 8,       // obj_piston (object.hh:369-418, object.cc:224-269)
     OBJ_FULL = 9,         // obj_full: solid everywhere (object.hh:83-86)
+    OBJ_TRIANGLE = 10,    // obj_triangle (object.hh:155-172, object.cc:52-70, 93-95)
+    OBJ_LAMPREY = 11,     // obj_lamprey (object.hh:542-595, object.cc:554-581)
+    OBJ_HOOP = 12,        // obj_hoop (object.hh:598-611, object.cc:586-588)
 };
 
 /** Device description of one solid: material constants (mat_const,
@@ -46,12 +49,17 @@ struct ObjDev {
     // perturb_v, flag_thresh, K_stiff}; seven-point star {cx, cy, cr, piv_r,
     // th_max, omega, piv_thresh, K_stiff}; flapper {cx, cy, cr, 0, cos theta,
     // sin theta, 0, cl, ar, al, amp, omega}; piston {0, y_start, lx, 0, idur,
-    // anch_r, 0, ly, cx, len, anch_thresh, K_stiff}.
+    // anch_r, 0, ly, cx, len, anch_thresh, K_stiff}; triangle {cx, cy, cr/2,
+    // grav, 0, 0, 0, 0, n0x, n0y, n1x, n1y} with n2 in nor2; lamprey {cx, cy,
+    // dis, la, cos theta, sin theta, w1, w2, T, log(mlam)}; hoop {0, 0, cr,
+    // 0, 0, 0, 0, cc}.
     double g[12];
+    double nor2[2];
     // Per-step state set on the host before each stress evaluation: the
-    // rotation of the spinner's and the star's anchors, the flapper's
-    // contraction or the piston anchor's height.
-    double cth, sth, act;
+    // rotation of the spinner's and the star's anchors, the flapper's or the
+    // lamprey's contraction or the piston anchor's height, and the shift of
+    // the lamprey's contraction wave.
+    double cth, sth, act, shift;
 };
 
 /** Smoothed Heaviside inside the solid or blur zone (obj_field.hh:110-112). */
@@ -96,6 +104,22 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
         return (r - 1) * r / gr;
     }
     if (o.type == OBJ_FULL) return -1;  // obj_full::phi (object.hh:85)
+    if (o.type == OBJ_TRIANGLE) {  // obj_triangle::phi, object.cc:93-95
+        // the side whose normal selects the distance, then that normal turned
+        // by -90 degrees applied to (X, Y)
+        const double s0 = X * o.g[8] + Y * o.g[9], s1 = X * o.g[10] + Y * o.g[11],
+                     s2 = X * o.nor2[0] + Y * o.nor2[1];
+        const int k = s0 > 0 ? (s1 > 0 ? 0 : 2) : (s2 > 0 ? 1 : 0);
+        const double nx = k == 0 ? o.g[8] : (k == 1 ? o.g[10] : o.nor2[0]),
+                     ny = k == 0 ? o.g[9] : (k == 1 ? o.g[11] : o.nor2[1]);
+        return Y * nx + -X * ny - o.g[2];
+    }
+    if (o.type == OBJ_LAMPREY) {  // obj_lamprey::phi, object.cc:554-558
+        if (X > 0) return o.g[2] * Y * Y / (o.g[6] * o.g[6]) + X - o.g[2];
+        const double wl = o.g[6] - (o.g[7] - o.g[6]) * X / o.g[3];
+        return fmax(-o.g[3] - X, Y * Y / (wl * wl) - 1);
+    }
+    if (o.type == OBJ_HOOP) return fabs(sqrt(X * X + Y * Y) - o.g[7]) - o.g[2];  // object.cc:586-588
     if (o.type == OBJ_SEVEN_POINT) {  // obj_seven_point::phi, object.cc:117-124
         const double fac = 2 * M_PI / 7.;
         double theta = fabs(atan2(Y, X)), R = sqrt(X * X + Y * Y);
@@ -123,8 +147,9 @@ __device__ __forceinline__ double obj_phi(const ObjDev &o, double X, double Y) {
 
 /** Initial reference map (object::transform / obj_standard::transform). */
 __device__ __forceinline__ void obj_transform(const ObjDev &o, double x, double y, double &X, double &Y) {
-    if (o.type == OBJ_SIMPLE_SPIN || o.type == OBJ_FULL) { X = x; Y = y; }  // object::transform
-    else if (o.type == OBJ_FLAPPER) {  // translation, then rotation (object.hh:272-276)
+    if (o.type == OBJ_SIMPLE_SPIN || o.type == OBJ_FULL || o.type == OBJ_HOOP) { X = x; Y = y; }  // object::transform
+    else if (o.type == OBJ_FLAPPER || o.type == OBJ_LAMPREY) {
+        // translation, then rotation (object.hh:272-276, 573-577)
         x -= o.g[0];
         y -= o.g[1];
         X = x * o.g[4] + y * o.g[5];
@@ -149,8 +174,8 @@ __device__ __forceinline__ void obj_velocity(const ObjDev &o, double X, double Y
 
 /** Extra accelerations (object::accel overrides): the simple spinner's
  * rotating pivot (object.cc:189-197), the flag's anchor (object.cc:476-484)
- * and the gravity of the circle, the square, the rounded rod and the ellipse
- * (object.cc:31-34, 41-44, 75-78). */
+ * and the gravity of the circle, the square, the triangle, the rounded rod
+ * and the ellipse (object.cc:31-34, 41-44, 65-70, 75-78). */
 __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, double X, double Y,
                                           double phiv, double &ax, double &ay) {
     if (o.type == OBJ_SIMPLE_SPIN) {
@@ -183,18 +208,32 @@ __device__ __forceinline__ void obj_accel(const ObjDev &o, double x, double y, d
             ax -= K * (x - X);
             ay -= K * (dely - Y);
         }
-    } else if (o.type == OBJ_FLAPPER || o.type == OBJ_FULL) {
-        // no acceleration (object::accel, object.hh:73-74)
+    } else if (o.type == OBJ_FLAPPER || o.type == OBJ_FULL || o.type == OBJ_LAMPREY || o.type == OBJ_HOOP) {
+        // no acceleration (object::accel, object.hh:73-74; obj_hoop keeps
+        // its grav but does not override accel)
     } else {
         ay -= o.g[3] * trans_func_in(o, phiv);
     }
 }
 
-/** obj_flapper::actuate (object.cc:301-308): scales the deformation gradient
- * F = [[a, b], [c, d]] at reference-map position (X, Y) inside the actuated
- * region by the current contraction o.act. */
+/** object::actuate overrides: scale the deformation gradient F = [[a, b],
+ * [c, d]] at reference-map position (X, Y). obj_lamprey (object.cc:573-581):
+ * a contraction wave of amplitude o.act travelling down the body, shifted by
+ * o.shift; obj_flapper (object.cc:301-308): the current contraction o.act
+ * inside the actuated region. */
 __device__ __forceinline__ void obj_actuate(const ObjDev &o, double X, double Y, double &a, double &b, double &c,
                                             double &d) {
+    if (o.type == OBJ_LAMPREY) {
+        const double la = o.g[3], w1 = o.g[6], w2 = o.g[7];
+        const double dx = X + (Y > 0 ? 1.5 * la : la) + o.shift, wl = w1 - (w2 - w1) * X / la, fac = fabs(Y) / wl;
+        const double band = fmin(-X, la * 0.15 - fabs(dx - la * (static_cast<int>(dx / la) + 0.5)));
+        const double st = exp(o.act * (fac < 1 ? fac * (2 - fac) : 1) * trans_func(o, -band));
+        a *= st;
+        b *= 1. / st;
+        c *= st;
+        d *= 1. / st;
+        return;
+    }
     if (o.type != OBJ_FLAPPER) return;
     const double fX = fabs(X) - o.g[9], ph = (fX < 0 ? fabs(Y) : sqrt(fX * fX + Y * Y)) - o.g[8];
     if (ph < o.eps) {

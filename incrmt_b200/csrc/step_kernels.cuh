@@ -500,7 +500,7 @@ __device__ __forceinline__ bool solid_stress(const GridDev &g, const FluidDev &f
     // F=[[Yy,-Xy],[-Yx,Xx]], the object's actuation applied at the edge's
     // reference map, sigma=F F^T (mat::AAT, mat.hh:159-161).
     double Fa = Yy, Fb = -Xy, Fc = -Yx, Fd = Xx;
-    if (o.type == OBJ_FLAPPER) {
+    if (o.type == OBJ_FLAPPER || o.type == OBJ_LAMPREY) {
         const double X = left ? 0.5 * (s.X[q] + s.X[q - 1]) : 0.5 * (s.X[q] + s.X[q - P]),
                      Y = left ? 0.5 * (s.Y[q] + s.Y[q - 1]) : 0.5 * (s.Y[q] + s.Y[q - P]);
         obj_actuate(o, X, Y, Fa, Fb, Fc, Fd);

@@ -142,6 +142,24 @@ void obj_flapper::describe(incrmt_object_desc &d) const {
     memcpy(d.params, p, sizeof(p));
 }
 
+void obj_triangle::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_TRIANGLE;
+    const double p[5] = {cx, cy, cr, theta, grav};
+    memcpy(d.params, p, sizeof(p));
+}
+
+void obj_lamprey::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_LAMPREY;
+    const double p[9] = {cx, cy, theta, le, dis, w1, w2, T, mlam};
+    memcpy(d.params, p, sizeof(p));
+}
+
+void obj_hoop::describe(incrmt_object_desc &d) const {
+    d.type = INCRMT_OBJ_HOOP;
+    const double p[3] = {r_in, r_out, grav};
+    memcpy(d.params, p, sizeof(p));
+}
+
 obj_piston::~obj_piston() {
     if (fp != nullptr) fclose(fp);
 }

@@ -158,6 +158,34 @@ struct obj_full : public object {
     void describe(incrmt_object_desc &d) const override { d.type = INCRMT_OBJ_FULL; }
 };
 
+/** Equilateral triangle with vertices cr from (cx, cy), rotated by theta,
+ * falling under grav (obj_triangle, object.hh:155-172). */
+struct obj_triangle : public object {
+    const double cx, cy, cr, theta, grav;
+    obj_triangle(double cx_, double cy_, double cr_, double theta_, double grav_)
+        : cx(cx_), cy(cy_), cr(cr_), theta(theta_), grav(grav_) {}
+    void describe(incrmt_object_desc &d) const override;
+};
+
+/** Swimmer of length le (head dis, half-widths w1 at the neck and w2 at the
+ * tail) at (cx, cy) rotated by theta, driven by a contraction wave of period
+ * T and maximum contraction mlam (obj_lamprey, object.hh:542-595). */
+struct obj_lamprey : public object {
+    const double cx, cy, theta, le, dis, w1, w2, T, mlam;
+    obj_lamprey(double cx_, double cy_, double theta_, double le_, double dis_, double w1_, double w2_, double T_,
+                double mlam_)
+        : cx(cx_), cy(cy_), theta(theta_), le(le_), dis(dis_), w1(w1_), w2(w2_), T(T_), mlam(mlam_) {}
+    void describe(incrmt_object_desc &d) const override;
+};
+
+/** Hoop of radii r_in, r_out about the origin (obj_hoop, object.hh:598-611);
+ * grav is kept and, as in the reference, never applied. */
+struct obj_hoop : public object {
+    const double r_in, r_out, grav;
+    obj_hoop(double r_in_, double r_out_, double grav_ = 0) : r_in(r_in_), r_out(r_out_), grav(grav_) {}
+    void describe(incrmt_object_desc &d) const override;
+};
+
 /** Seven-pointed star of tip radius cr centred at (cx, cy), spun back and
  * forth by a stiff anchor of radius piv_r (obj_seven_point,
  * object.hh:176-213). */

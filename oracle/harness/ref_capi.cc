@@ -89,7 +89,11 @@ ref_sim* make_sspin(int m,int ntrace,const char *base) {
  * obj_circle(cx,cy,cr,uu,vv,omega,grav), object.hh:128-138), rounded rods
  * (type 2: obj_rounded_rod(cx,cy,cr,cl,grav), object.hh:229-230) and flags
  * (type 3: obj_flag(cx,cy,flag_l,flag_w,flag_a,perturb_v,ntrace),
- * object.hh:487-488); mats holds G and rhos per object. flow_u > 0 selects
+ * object.hh:487-488), squares (5), seven-pointed stars (6), flappers (7),
+ * pistons (8), circle trackers (9), triangles (11: obj_triangle(cx,cy,cr,
+ * theta,grav)), lampreys (12: obj_lamprey(cx,cy,theta,le,dis,w1,w2,T,mlam))
+ * and hoops (13: obj_hoop(r_in,r_out,grav)), each with its constructor's
+ * arguments in order; mats holds G and rhos per object. flow_u > 0 selects
  * sim_horiz_flow(flow_u, geom) (sim_type.hh:125-126; y-periodic, inflow at the
  * left, zero pressure at the right) instead of sim_type(geom, x_prd, y_prd).
  * Output directory <base>.odr. */
@@ -113,6 +117,9 @@ ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double vi
         else if(types[k]==7) r->obj.push_back(new obj_flapper(p[0],p[1],p[2],p[3],p[4],p[5],p[6],p[7],p[8]));
         else if(types[k]==8) r->obj.push_back(new obj_piston(p[0],p[1],p[2],p[3],p[4],p[5],p[6],r->fa));
         else if(types[k]==9) r->obj.push_back(new obj_circle_track(p[0],p[1],p[2],p[3],p[4],p[5],r->fa));
+        else if(types[k]==11) r->obj.push_back(new obj_triangle(p[0],p[1],p[2],p[3],p[4]));
+        else if(types[k]==12) r->obj.push_back(new obj_lamprey(p[0],p[1],p[2],p[3],p[4],p[5],p[6],p[7],p[8]));
+        else if(types[k]==13) r->obj.push_back(new obj_hoop(p[0],p[1],p[2]));
         else r->obj.push_back(new obj_flag(p[0],p[1],p[2],p[3],p[4],p[5],static_cast<int>(p[6]),r->fa));
     }
     if(flow_u>0) r->st=new sim_horiz_flow(flow_u,geom[0],geom[1],geom[2],geom[3]);

@@ -119,7 +119,7 @@ def mg_apply(sys, m, n, rho, z, ax=-1., bx=1., ay=-1., by=1., x_prd=False, y_prd
 
 # object kinds of ref_multi_create (oracle/harness/ref_capi.cc make_multi)
 OBJECT_TYPES = {"circle": 1, "rod": 2, "flag": 3, "square": 5, "star": 6, "flapper": 7, "piston": 8,
-                "circle_track": 9}
+                "circle_track": 9, "triangle": 11, "lamprey": 12, "hoop": 13}
 
 
 class RefSim:

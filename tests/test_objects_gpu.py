@@ -3,8 +3,12 @@
 (obj_seven_point, in ftest's default doubly periodic box), the swimming
 flapper (obj_flapper, actuated deformation gradient), the piston dragged by
 a moving anchor (obj_piston, one tracked point) and the moving circle with two
-tracked points (obj_circle_track). The oracle is the reference's fluid_2d
-with the same objects (oracle/_ref, ref_multi_create).
+tracked points (obj_circle_track); and the object types no ftest scenario
+uses: the falling triangle (obj_triangle), the lamprey swimming by a
+travelling contraction wave (obj_lamprey, actuated deformation gradient) and
+the hoop (obj_hoop, geometry only: the reference never applies its
+gravity). The oracle is the reference's fluid_2d with the same objects
+(oracle/_ref, ref_multi_create).
 
 Both start from the reference at t = 2 (the flapper's contraction,
 -amp sin^12(2 pi t / T), at its largest; the anchors turned or moved), after
@@ -27,7 +31,7 @@ pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle_available(), reason
 FIELDS = "u v p rho ux uy vx vy ud vd ul vl ur vr uu vu c0 c1 c2 c3 s11 s12 s21 s22".split()
 SFIELDS = "X Y nX nY Xx Xy Yx Yy Xd Yd Xl Yl Xr Yr Xu Yu".split()
 
-# name: (m, n, geom, periodic, visc, [(kind, params, G, rhos)])
+# name: (m, n, geom, periodic, visc, [(kind, params, G, rhos)][, inflow speed])
 SCENES = {
     "star": (48, 48, (-1., 1., -1., 1.), (True, True), 1e-3,
              [("star", (0.0, 0.0, 0.62, 0.16, np.pi, 1.0), 24.0, 3.0)]),
@@ -37,6 +41,16 @@ SCENES = {
                [("piston", (0.8, 0.2, 0.6, 0.4, 4.6, 10.0, 0.15), 1.0, 2.0)]),
     "circle_track": (48, 48, (-1., 1., -1., 1.), (False, False), 1e-3,
                      [("circle_track", (-0.3, -0.3, 0.25, 0.5, 1.0, 6.0), 24.0, 4.0)]),
+    "triangle": (48, 48, (-1., 1., -1., 1.), (False, False), 1e-3,
+                 [("triangle", (0.1, 0.2, 0.5, 0.3, 0.5), 10.0, 2.0)]),
+    "lamprey": (64, 64, (-1., 1., -1., 1.), (False, False), 1e-3,
+                [("lamprey", (0.2, 0.0, 0.2, 1.4, 0.25, 0.15, 0.08, 2.0, 1.5), 10.0, 1.5)]),
+    # the hoop has no forcing, so it sits in sim_horiz_flow's stream (inflow
+    # 0.5, y-periodic); the box is off-centre because a hoop about the origin
+    # of a symmetric grid gives the fast march exactly equal arrival values,
+    # which it may order differently
+    "hoop": (48, 48, (-0.93, 1.07, -1.11, 0.89), (False, True), 1e-3,
+             [("hoop", (0.3, 0.5, 0.7), 10.0, 2.0)], 0.5),
 }
 
 
@@ -48,14 +62,21 @@ def _rel(a, b):
 def _pair(name):
     from incrmt_b200 import capi
     from oracle import refsim
-    m, n, geom, per, visc, objects = SCENES[name]
-    r = refsim.RefSim(m, ntrace=0, n=n, objects=objects, geom=geom, visc=visc, periodic=per)
+    m, n, geom, per, visc, objects = SCENES[name][:6]
+    flow = SCENES[name][6] if len(SCENES[name]) > 6 else None
+    r = refsim.RefSim(m, ntrace=0, n=n, objects=objects, geom=geom, visc=visc, periodic=per,
+                      flow_u=flow or 0.0)
     g = capi.Simulation(m, n, ax=geom[0], bx=geom[1], ay=geom[2], by=geom[3], visc=visc, ntrace=0,
-                        x_prd=per[0], y_prd=per[1])
+                        x_prd=per[0], y_prd=per[1], horiz_flow=flow)
     for kind, p, G, rhos in objects:
-        add = {"star": g.add_seven_point, "flapper": g.add_flapper, "piston": g.add_piston,
-               "circle_track": g.add_circle_track}[kind]
-        add(*p, G, rhos)
+        if kind == "triangle":
+            g.add_triangle(*p[:4], G, rhos, grav=p[4])
+        elif kind == "hoop":
+            g.add_hoop(p[0], p[1], G, rhos, grav=p[2])
+        else:
+            add = {"star": g.add_seven_point, "flapper": g.add_flapper, "piston": g.add_piston,
+                   "circle_track": g.add_circle_track, "lamprey": g.add_lamprey}[kind]
+            add(*p, G, rhos)
     dt_reg = g.initialize()
     assert abs(dt_reg - r.scalars()["dt_reg"]) <= 1e-15 * dt_reg
     return r, g, 0.9 * dt_reg, len(objects)

@@ -436,12 +436,13 @@ def _train_learned_sim(workload, rank, dev):
     return nets, info
 
 
-def _plain_fp64_rate(workload, rank, steps, warmup, dev):
+def _plain_fp64_rate(workload, rank, steps, warmup, dev, coarse_refresh=1):
     """Steps/s and V-cycles per projection of the plain FP64 method on the
     same workload (the comparison of the learned + mixed line)."""
     import torch
     from incrmt_b200 import capi
     sim, interval, _ = _make_sim(workload, rank, capi.PREC_FP64)
+    sim.set_coarse_refresh(coarse_refresh)
     dt = _frame_dt(sim, interval)
     ext = torch.cuda.ExternalStream(sim.stream(), device=dev)
     sim.step(dt, warmup)
@@ -473,6 +474,7 @@ def run_ours_sspin(args, ws, rank, local, dist):
             raise SystemExit("--learned: the simulation workloads with a learned warm start are sed1024, flag2048")
         nets, learned_info = _train_learned_sim(args.workload, rank, dev)
     sim, interval, wl = _make_sim(args.workload, rank, prec)
+    sim.set_coarse_refresh(args.coarse_refresh)
     dt = _frame_dt(sim, interval)
     if nets is not None:
         for sys, net in nets.items():
@@ -535,7 +537,7 @@ def run_ours_sspin(args, ws, rank, local, dist):
         sim.close()
         for net in nets.values():
             net.close()
-        plain_sps, plain_vc = _plain_fp64_rate(args.workload, rank, args.steps, args.warmup, dev)
+        plain_sps, plain_vc = _plain_fp64_rate(args.workload, rank, args.steps, args.warmup, dev, args.coarse_refresh)
         learned_info.update({
             "rule": "fall back to the previous solution when the guess raises the residual" if args.learned_rule == 0
                     else "fall back only when the energy-optimal step is not positive",
@@ -571,8 +573,9 @@ def run_ours_sspin(args, ws, rank, local, dist):
         "dtype": "f64" if prec == capi.PREC_FP64 else "f64 state, f32 V-cycles in f64 defect correction",
         "data": "synthetic",
         "config": {"workload": wl, "precision": args.precision, "flush": "working set larger than L2",
-                   "parallelism": f"replicas x{ws}"},
+                   "parallelism": f"replicas x{ws}", "coarse_refresh": args.coarse_refresh},
         "vcycles_per_projection": vc,
+        "coarse_builds_per_step": (st1.coarse_builds - st0.coarse_builds) / args.steps,
         "phase_ms_per_step": phases,
         "march_sweeps_per_step": (st1.march_sweeps - st0.march_sweeps) / args.steps,
         "march_monotone_rebuilds": int(st1.march_monotone - st0.march_monotone),
@@ -821,6 +824,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096", "sed1024", "flag2048"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--coarse-refresh", type=int, default=16,
+                    help="rebuild the projections' Galerkin coarse operators every K projections "
+                         "(1: on every density change)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned", action="store_true",
                     help="mac4096: train the learned initial guess first and start every solve from it; "

@@ -110,6 +110,7 @@ typedef struct incrmt_sim_stats {
     long long march_monotone;              /* band rebuilds that needed the monotone march sweeps */
     long long window_points;               /* level-set points in the objects' current rebuild
                                               windows (all objects' whole grids when off) */
+    long long coarse_builds;               /* Galerkin hierarchy rebuilds, MAC plus FEM */
 } incrmt_sim_stats;
 
 /** Creates the simulation (fluid_2d::fluid_2d, fluid_2d.cc:26-43). */
@@ -234,6 +235,15 @@ int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err);
  * whole-grid passes throughout; a state upload (incrmt_set_field) returns
  * to whole-grid passes until the next rebuild. */
 int incrmt_sim_set_windows(incrmt_sim *h, int on);
+
+/** How often the projections rebuild their Galerkin coarse operators: every
+ * `every` projections (1: on every density change, as the reference's solver
+ * setup does), sooner when a solve takes more than one V-cycle over the first
+ * solve after the last rebuild, and always after incrmt_set_field. The fine
+ * operator always uses the current density, so every solve still reaches the
+ * same relative residual; stale coarse levels only steer convergence.
+ * Default 16. */
+int incrmt_sim_set_coarse_refresh(incrmt_sim *h, int every);
 
 /** fluid_2d::solid_prd_bc (fluid_2d.hh:124), set before incrmt_initialize on
  * a doubly periodic domain: every object's reference map is periodic up to

@@ -269,7 +269,8 @@ class SimStats(ctypes.Structure):
                 ("solves_fem", ctypes.c_longlong), ("march_sweeps", ctypes.c_longlong),
                 ("extrap_sweeps", ctypes.c_longlong), ("launches", ctypes.c_longlong),
                 ("dt_reg", ctypes.c_double), ("time", ctypes.c_double),
-                ("march_monotone", ctypes.c_longlong), ("window_points", ctypes.c_longlong)]
+                ("march_monotone", ctypes.c_longlong), ("window_points", ctypes.c_longlong),
+                ("coarse_builds", ctypes.c_longlong)]
 
 
 def _sim_sigs(L):
@@ -296,6 +297,7 @@ def _sim_sigs(L):
     L.incrmt_sim_set_profiling.argtypes = [P, I]
     L.incrmt_sim_set_windows.argtypes = [P, I]
     L.incrmt_set_solid_prd_bc.argtypes = [P, I]
+    L.incrmt_sim_set_coarse_refresh.argtypes = [P, I]
     L.incrmt_set_object_tracers.argtypes = [P, dp, I, I]
     L.incrmt_l_comparison.argtypes = [P, P, dp]
     L.incrmt_sim_profile.argtypes = [P, dp]
@@ -542,6 +544,11 @@ class Simulation:
         """Per-object windows of the level-set and reference-map passes
         (on by default); off runs every pass over the whole grid."""
         check(lib().incrmt_sim_set_windows(self._h, int(on)))
+
+    def set_coarse_refresh(self, every):
+        """Rebuild the projections' Galerkin coarse operators every `every`
+        projections (1 = every density change)."""
+        check(lib().incrmt_sim_set_coarse_refresh(self._h, int(every)))
 
     def set_profiling(self, on=True, smoothers=False):
         """Phase timing (on) and per-launch timing of the projections'

@@ -969,7 +969,31 @@ int Multigrid::set_density_device(const double *d_rho, int ld) {
     INCRMT_CKL("coefficients");
     int r = galerkin_all();
     if (r == INCRMT_OK) ready = true;
+    coarse_builds++;
+    coarse_age = 0;
+    coarse_vc0 = -1;
+    coarse_stale = false;
     return r;
+}
+
+int Multigrid::set_density_lagged(const double *d_rho, int ld) {
+    if (!ready || coarse_stale || coarse_every <= 1 || coarse_age + 1 >= coarse_every)
+        return set_density_device(d_rho, ld);
+    if (ld <= 0) ld = cm + 4;
+    if (sys == INCRMT_SYS_MAC) {
+        k_mac_coef<<<grid2(cm + 1, cn + 1), kBlk2, 0, stream>>>(d_rho, ld, cm, cn, ex, ey, exf, eyf);
+    } else {
+        k_fem_coef<<<grid2(m, n), kBlk2, 0, stream>>>(d_rho, ld, m, n, c, cf);
+    }
+    launches++;
+    INCRMT_CKL("coefficients");
+    coarse_age++;
+    return INCRMT_OK;
+}
+
+void Multigrid::note_vcycles(int vc) {
+    if (coarse_vc0 < 0) coarse_vc0 = vc;
+    else if (vc > coarse_vc0 + 1) coarse_stale = true;
 }
 
 int Multigrid::set_unit_density() {

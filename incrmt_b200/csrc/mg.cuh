@@ -53,6 +53,15 @@ public:
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
     bool ready = false;              // coefficients and hierarchy built
+    // Lagged coarse operators: set_density_lagged recomputes the fine
+    // coefficients every time but the Galerkin levels only every
+    // coarse_every calls, when marked stale, or after a solve that took more
+    // than one V-cycle over the first solve since the last rebuild.
+    int coarse_every = 1;            // the simulation handle sets its own default
+    int coarse_age = 0;
+    int coarse_vc0 = -1;
+    bool coarse_stale = true;
+    long long coarse_builds = 0;
     bool tiles = true;               // tile-fused smoothing where it applies
     int tail_level = -1;             // first level run by the one-block tail kernel
     cudaGraphExec_t gexec = nullptr; // captured V-cycle + norm
@@ -81,6 +90,12 @@ public:
      * (mgs_mac_const_rho, mgs_fem_const_rho; mgs_mac.hh, mgs_fem.cc:27-80),
      * which are the varying-density ones with every 1/rho equal to 1. */
     int set_unit_density();
+    /** The fine-level coefficients from d_rho, with the coarse levels
+     * rebuilt per the lag policy above. The converged solution depends on
+     * the fine operator alone; the coarse levels only steer convergence. */
+    int set_density_lagged(const double *d_rho, int ld);
+    /** Records a solve's V-cycle count for the lag policy. */
+    void note_vcycles(int vc);
     int solve_device(const double *d_b, double *d_z, const incrmt_mg_opts *o,
                      incrmt_mg_stats *st, bool time_it);
     int vcycle64(const double *d_b, double *d_z);

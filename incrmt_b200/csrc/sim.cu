@@ -70,6 +70,10 @@ struct Sim {
     double dt_reg = 0, time = 0;
     double w_scale = 3, w_force = 20, tw = 2.5, pinw = 2.5;
     bool initialized = false;
+    // Default lag of the projections' Galerkin coarse operators (in
+    // projections): the same V-cycle counts as a rebuild per projection on
+    // the rotor and sediment scenes, at a sixteenth of the setup cost.
+    static constexpr int kCoarseEvery = 16;
     // fluid_2d::const_rho (fluid_2d.cc:126-137): every solid's density within
     // small_number of the fluid's; the projections then use the constant-
     // density operators, set once, and pin leaves rho alone.
@@ -288,6 +292,7 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     if (ntrace > 0) INCRMT_CK(cudaMalloc(&d_remap, sizeof(int) * ntrace));
     if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
     if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
+    mac.coarse_every = fem.coarse_every = kCoarseEvery;
     return INCRMT_OK;
 }
 
@@ -731,7 +736,7 @@ int Sim::mac_projection() {
     int outer = cur_phase, r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(INCRMT_PHASE_MG_SETUP))) return r;
-    r = const_rho ? INCRMT_OK : mac.set_density_device(f.rho, g.P);
+    r = const_rho ? INCRMT_OK : mac.set_density_lagged(f.rho, g.P);
     if (r) return r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(outer))) return r;
@@ -743,6 +748,7 @@ int Sim::mac_projection() {
     launches += mac.launches - l0;
     vc_mac += st.vcycles;
     solves_mac++;
+    if (!r) mac.note_vcycles(st.vcycles);
     if (r) return r;
     k_mac_correct<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, z_mac, mac.ex, mac.ey);
     launches++;
@@ -802,7 +808,7 @@ int Sim::fem_projection(double dt) {
     int outer = cur_phase, r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(INCRMT_PHASE_MG_SETUP))) return r;
-    r = const_rho ? INCRMT_OK : fem.set_density_device(f.rho, g.P);
+    r = const_rho ? INCRMT_OK : fem.set_density_lagged(f.rho, g.P);
     if (r) return r;
     if ((r = phase_end())) return r;
     if ((r = phase_begin(outer))) return r;
@@ -814,6 +820,7 @@ int Sim::fem_projection(double dt) {
     launches += fem.launches - l0;
     vc_fem += st.vcycles;
     solves_fem++;
+    if (!r) fem.note_vcycles(st.vcycles);
     if (r) return r;
     const int nb = 2 * kB200SMs;
     k_pressure_sum<<<nb, 256, 0, stream>>>(g, z_fem, partial);
@@ -1280,8 +1287,10 @@ int incrmt_set_field(incrmt_sim *h, int id, int k, const double *host) {
     incrmt::Sim &S = h->s;
     const size_t w = S.g.ml, rows = S.g.nl;
     // An uploaded state may have anything anywhere: whole-grid passes until
-    // the next band rebuild.
+    // the next band rebuild, and coarse operators rebuilt at the next solve.
     if (int r = S.win_reset()) return r;
+    S.mac.coarse_stale = true;
+    S.fem.coarse_stale = true;
     if (id == INCRMT_FIELD_STATUS) {
         if (k < 0 || k >= static_cast<int>(S.sol.size())) { set_error("bad object"); return INCRMT_ERR_BADARG; }
         std::vector<int> tmp(w * rows);
@@ -1412,6 +1421,7 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
         st->window_points += static_cast<long long>(w.x1 - w.x0) * (w.y1 - w.y0);
     }
     st->extrap_sweeps = S.ex_sweeps;
+    st->coarse_builds = S.mac.coarse_builds + S.fem.coarse_builds;
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;
     st->time = S.time;
@@ -1500,6 +1510,15 @@ int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err) {
     INCRMT_CK(cudaMemcpyAsync(err, dev_err, sizeof(double) * 32, cudaMemcpyDeviceToHost, S.stream));
     INCRMT_CK(cudaFreeAsync(part, S.stream));
     INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_sim_set_coarse_refresh(incrmt_sim *h, int every) {
+    if (!h || every < 1) { set_error("bad argument"); return INCRMT_ERR_BADARG; }
+    h->s.mac.coarse_every = every;
+    h->s.fem.coarse_every = every;
+    h->s.mac.coarse_stale = true;
+    h->s.fem.coarse_stale = true;
     return INCRMT_OK;
 }
 

@@ -242,7 +242,9 @@ int incrmt_sim_set_windows(incrmt_sim *h, int on);
  * solve after the last rebuild, and always after incrmt_set_field. The fine
  * operator always uses the current density, so every solve still reaches the
  * same relative residual; stale coarse levels only steer convergence.
- * Default 16. */
+ * Default 1 (the reference's policy); the C++ host's fluid_2d and the
+ * benchmark use 16, which on the rotor and sediment scenes keeps the V-cycle
+ * counts and removes most of the setup time. */
 int incrmt_sim_set_coarse_refresh(incrmt_sim *h, int every);
 
 /** fluid_2d::solid_prd_bc (fluid_2d.hh:124), set before incrmt_initialize on

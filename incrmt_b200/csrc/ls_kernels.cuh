@@ -773,6 +773,13 @@ __global__ void k_ls_collect_candidates(LsGrid g, const LsObj *ob, const LsWin *
     if ((st == 0 || st == 7) && o.ia[ij]) ls_list_push(list, list_k, count, cap, overflow, ij, blockIdx.z);
 }
 
+/** Threads per block of the cooperative sweeps: one block per SM (the grid
+ * barrier costs more with more blocks), as many threads as the registers
+ * allow, so that a candidate list of ~1e5 points takes about one pass per
+ * sweep and each SM has many warps to hide the stencil's dependent loads. */
+constexpr int kFimThreads = 1024;
+constexpr int kExtrapThreads = 512;
+
 /** Whether any point the stencil of (i,j) reads (up to two cells along
  * each axis) changed in the previous sweep. */
 __device__ __forceinline__ bool stencil_changed(const LsGrid &g, const unsigned char *chg, int i, int j) {
@@ -798,7 +805,7 @@ __device__ __forceinline__ bool stencil_changed(const LsGrid &g, const unsigned 
  * candidates of every object, so all bands settle in the same launch.
  * flags[0..2] rotate as per-sweep change flags; flags[3] receives the number
  * of sweeps and flags[4] 1 if converged. */
-__global__ void k_ls_fim_coop(LsGrid g, const LsObj *ob, const int *list, const int *list_k, const int *countp,
+__global__ void __launch_bounds__(kFimThreads, 1) k_ls_fim_coop(LsGrid g, const LsObj *ob, const int *list, const int *list_k, const int *countp,
                               int cap, int *flags, int max_sweeps) {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
@@ -853,7 +860,7 @@ __global__ void k_ls_fim_coop(LsGrid g, const LsObj *ob, const int *list, const 
 
 /** All sweeps of the extrapolation wavefront in one cooperative launch (same
  * scheme as k_ls_fim_coop); flags[5] is raised for a singular fit. */
-__global__ void k_ls_extrap_coop(LsGrid g, const LsObj *ob, const int *list, const int *list_k,
+__global__ void __launch_bounds__(kExtrapThreads, 1) k_ls_extrap_coop(LsGrid g, const LsObj *ob, const int *list, const int *list_k,
                                  const int *countp, int cap, int *flags, int max_sweeps) {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();

@@ -57,7 +57,7 @@ public:
     // coefficients every time but the Galerkin levels only every
     // coarse_every calls, when marked stale, or after a solve that took more
     // than one V-cycle over the first solve since the last rebuild.
-    int coarse_every = 1;            // the simulation handle sets its own default
+    int coarse_every = 1;
     int coarse_age = 0;
     int coarse_vc0 = -1;
     bool coarse_stale = true;

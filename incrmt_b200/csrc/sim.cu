@@ -70,10 +70,6 @@ struct Sim {
     double dt_reg = 0, time = 0;
     double w_scale = 3, w_force = 20, tw = 2.5, pinw = 2.5;
     bool initialized = false;
-    // Default lag of the projections' Galerkin coarse operators (in
-    // projections): the same V-cycle counts as a rebuild per projection on
-    // the rotor and sediment scenes, at a sixteenth of the setup cost.
-    static constexpr int kCoarseEvery = 16;
     // fluid_2d::const_rho (fluid_2d.cc:126-137): every solid's density within
     // small_number of the fluid's; the projections then use the constant-
     // density operators, set once, and pin leaves rho alone.
@@ -268,9 +264,9 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
         INCRMT_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         // One block per SM: the grid barrier of the cooperative sweeps costs
         // more with more blocks, and the candidate lists are ~1e4-1e5 points.
-        INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_fim_coop, 256, 0));
+        INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_fim_coop, kFimThreads, 0));
         coop_blocks_fim = sms * (nb > 0 ? 1 : 0);
-        INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_extrap_coop, 256, 0));
+        INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ls_extrap_coop, kExtrapThreads, 0));
         coop_blocks_ext = sms * (nb > 0 ? 1 : 0);
         if (coop_blocks_fim == 0 || coop_blocks_ext == 0) {
             set_error("level-set kernels cannot be co-resident");
@@ -292,7 +288,6 @@ int Sim::create(const incrmt_grid *gr, const incrmt_phys *ph) {
     if (ntrace > 0) INCRMT_CK(cudaMalloc(&d_remap, sizeof(int) * ntrace));
     if ((r = mac.create(INCRMT_SYS_MAC, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
     if ((r = fem.create(INCRMT_SYS_FEM, g.m, g.n, g.ax, g.bx, g.ay, g.by, g.xp, g.yp, g.zpr, stream))) return r;
-    mac.coarse_every = fem.coarse_every = kCoarseEvery;
     return INCRMT_OK;
 }
 
@@ -636,7 +631,7 @@ int Sim::build_bands() {
     const int *countp = d_flags + 7;
     const LsObj *ob = d_lso;
     void *args[] = {&lg, &ob, &d_list, &d_list_k, &countp, &cap, &d_flags, &maxs};
-    INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_fim_coop), dim3(coop_blocks_fim), dim3(256),
+    INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_fim_coop), dim3(coop_blocks_fim), dim3(kFimThreads),
                                           args, 0, stream));
     launches++;
     INCRMT_CK(cudaMemcpyAsync(h_lsbox, d_lsbox, sizeof(int) * 4 * no, cudaMemcpyDeviceToHost, stream));
@@ -684,7 +679,7 @@ int Sim::extrapolate_all() {
     const LsObj *ob = d_lso;
     void *args[] = {&lg, &ob, &d_list, &d_list_k, &countp, &cap, &d_flags, &maxs};
     INCRMT_CK(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_ls_extrap_coop), dim3(coop_blocks_ext),
-                                          dim3(256), args, 0, stream));
+                                          dim3(kExtrapThreads), args, 0, stream));
     launches++;
     int r = fetch_flags();
     if (r) return r;

@@ -256,7 +256,7 @@ fluid_2d::fluid_2d(int m_, int n_, sim_type &sim_t_, double visc_, double rhof_,
       bx(sim_t_.bx), ay(sim_t_.ay), by(sim_t_.by), dx((bx - ax) / m_), dy((by - ay) / n_), xsp(1 / dx),
       ysp(1 / dy), visc(visc_), rhof(rhof_), tw(tw_), pinw(pinw_), eps(tw_ * (dx < dy ? dx : dy)),
       ntrace(ntrace_), fflags(fflags_), filename(filename_), dt_reg(0), time(0), f_num(0), zpr(false),
-      precision(INCRMT_PREC_FP64), solid_prd_bc(false), sim_t(sim_t_), h(nullptr), const_rho(true), created(false) {}
+      precision(INCRMT_PREC_FP64), solid_prd_bc(false), coarse_refresh(16), sim_t(sim_t_), h(nullptr), const_rho(true), created(false) {}
 
 /** Objects may already be deleted here (the reference's drivers delete them
  * first), so records not handed out by write_files are dropped. */
@@ -295,6 +295,7 @@ void fluid_2d::add_object(object *o, mat_const &mc) {
 void fluid_2d::initialize(double ev_mult, double dt_pad, double dt_ev_pad) {
     create();
     incrmt_check(incrmt_set_solid_prd_bc(h, solid_prd_bc ? 1 : 0), "incrmt_set_solid_prd_bc");
+    incrmt_check(incrmt_sim_set_coarse_refresh(h, coarse_refresh), "incrmt_sim_set_coarse_refresh");
     incrmt_check(incrmt_initialize(h, ev_mult, dt_pad, dt_ev_pad, &dt_reg), "incrmt_initialize");
     printf("# Ex. visc. multiplier    : %g\n"
            "# dt padding (phys)       : %g\n"

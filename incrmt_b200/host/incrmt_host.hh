@@ -278,6 +278,10 @@ class fluid_2d {
         /** Periodic reference maps up to the box lengths, with no wall force
          * (fluid_2d.hh:124); set before initialize. */
         bool solid_prd_bc;
+        /** Projections between rebuilds of the multigrid's Galerkin coarse
+         * operators (incrmt_sim_set_coarse_refresh); 1 rebuilds them on every
+         * density change as the reference does. Set before initialize. */
+        int coarse_refresh;
         fluid_2d(int m_, int n_, sim_type &sim_t_, double visc_, double rhof_, double tw_, double pinw_,
                  int ntrace_, unsigned int fflags_, const char *filename_);
         ~fluid_2d();

@@ -1,6 +1,7 @@
 // Geometric multigrid kernels and driver (see mg.cuh for the method).
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include "mg.cuh"
 
 namespace incrmt {
@@ -246,6 +247,88 @@ __global__ void __launch_bounds__(256) k_smooth_tile(Op op, const T *zin, T *zou
         if (i < m && j < n) zout[i + static_cast<long>(m) * j] = zs[(i - gx0) + LW * (j - gy0)];
     }
 }
+
+/** k_smooth_tile for the Galerkin levels' nine-point stencils with every
+ * input staged up front: the nine coefficients and the right-hand side of the
+ * whole halo region go to shared memory with the iterate before the first
+ * phase, so the colour phases run on shared memory alone instead of waiting
+ * on L2 for the coefficients in each of them (the small coarse levels are
+ * latency-bound). The arithmetic, and so the result, is that of
+ * k_smooth_tile. Dynamic shared memory: (11 * LW * LH) elements. */
+template <class T, int SWEEPS, int TW, int TH>
+__global__ void __launch_bounds__(256) k_smooth_tile_gen(GenOp<T> op, const T *zin, T *zout, const T *b, int m,
+                                                         int n) {
+    constexpr int H = 4 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H, LA = LW * LH;
+    extern __shared__ __align__(16) unsigned char gen_smem[];
+    T *zs = reinterpret_cast<T *>(gen_smem);
+    T *bs = zs + LA;
+    T *cs = bs + LA;  // coefficient k of local point t at cs[k * LA + t]
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    const int gx0 = x0 - H, gy0 = y0 - H;
+    const bool px = op.px, py = op.py;
+    const long N = op.N;
+    for (int t = threadIdx.x; t < LA; t += blockDim.x) {
+        int i = gx0 + t % LW, j = gy0 + t / LW;
+        if (px) i = wrap_index(i, m);
+        if (py) j = wrap_index(j, n);
+        if (i >= 0 && i < m && j >= 0 && j < n) {
+            const long ij = i + static_cast<long>(m) * j;
+            zs[t] = zin[ij];
+            bs[t] = b[ij];
+#pragma unroll
+            for (int k = 0; k < 9; k++) cs[k * LA + t] = op.st[k * N + ij];
+        }
+    }
+    __syncthreads();
+    const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
+    constexpr int P = 4 * SWEEPS;
+#pragma unroll 1
+    for (int p = 0; p < P; p++) {
+        const int e = P - 1 - p, c = p & 3;
+        int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
+        if (!px) {
+            if (ilo < 0) ilo = 0;
+            if (ihi > m - 1) ihi = m - 1;
+        }
+        if (!py) {
+            if (jlo < 0) jlo = 0;
+            if (jhi > n - 1) jhi = n - 1;
+        }
+        const int i0 = ilo + ((ilo & 1) != pis[c]), j0 = jlo + ((jlo & 1) != pjs[c]);
+        const int ni = i0 <= ihi ? (ihi - i0) / 2 + 1 : 0, nj = j0 <= jhi ? (jhi - j0) / 2 + 1 : 0;
+        for (int t = threadIdx.x; t < ni * nj; t += blockDim.x) {
+            const int i = i0 + 2 * (t % ni), j = j0 + 2 * (t / ni);
+            const int lz = (i - gx0) + LW * (j - gy0);
+            const int ir = px ? wrap_index(i, m) : i, jr = py ? wrap_index(j, n) : j;
+            // GenOp::offdiag_s with the coefficients read from shared memory
+            const bool l = px || ir > 0, r = px || ir < m - 1, d = py || jr > 0, u = py || jr < n - 1;
+            const T diag = cs[4 * LA + lz];
+            T s = 0;
+            if (d) {
+                if (l) s += cs[lz] * zs[lz - LW - 1];
+                s += cs[LA + lz] * zs[lz - LW];
+                if (r) s += cs[2 * LA + lz] * zs[lz - LW + 1];
+            }
+            if (l) s += cs[3 * LA + lz] * zs[lz - 1];
+            if (r) s += cs[5 * LA + lz] * zs[lz + 1];
+            if (u) {
+                if (l) s += cs[6 * LA + lz] * zs[lz + LW - 1];
+                s += cs[7 * LA + lz] * zs[lz + LW];
+                if (r) s += cs[8 * LA + lz] * zs[lz + LW + 1];
+            }
+            zs[lz] = (bs[lz] - s) / diag;
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < TW * TH; t += blockDim.x) {
+        const int i = x0 + t % TW, j = y0 + t / TW;
+        if (i < m && j < n) zout[i + static_cast<long>(m) * j] = zs[(i - gx0) + LW * (j - gy0)];
+    }
+}
+
+/** Shared memory of k_smooth_tile_gen<T, 2, 16, 16>. */
+template <class T>
+constexpr int gen_tile_smem() { return 11 * (16 + 16) * (16 + 16) * static_cast<int>(sizeof(T)); }
 
 /** Tile-fused red-black Gauss-Seidel for a five-point operator (the fine MAC
  * system): the colours (0,0),(1,1) share no stencil edge, nor do (1,0),(0,1),
@@ -633,6 +716,14 @@ __global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu
         T *st = sbase + L.smem_off[l];
         const long n9 = 9 * L.N[l];
         for (long q = threadIdx.x; q < n9; q += blockDim.x) st[q] = L.st[l][q];
+        if (l == 0) {
+            // the first tail level's right-hand side and iterate come from the
+            // restriction before the tail; its iterate goes back at the end
+            for (long q = threadIdx.x; q < L.N[0]; q += blockDim.x) {
+                st[n9 + q] = L.z[0][q];
+                st[n9 + L.N[0] + q] = L.b[0][q];
+            }
+        }
         L.st[l] = st;
         L.z[l] = st + n9;
         L.b[l] = st + n9 + L.N[l];
@@ -697,6 +788,8 @@ __global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu
         __syncthreads();
         tail_smooth(L, l, nu2);
     }
+    if (L.smem_from == 0)
+        for (long q = threadIdx.x; q < L.N[0]; q += blockDim.x) Lp.z[0][q] = L.z[0][q];
 }
 
 /** FP64 residual r = b - A z, optionally stored in FP32, with per-block sums
@@ -797,6 +890,8 @@ int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStrea
             k_smooth_tile<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, zalt, b, m, n);
         else if (static_cast<int>(b32.x * b32.y) >= kB200SMs)
             k_smooth_tile<Op, T, 2, 32, 16><<<b32, 256, 0, s>>>(op, z, zalt, b, m, n);
+        else if constexpr (std::is_same<Op, GenOp<T>>::value)
+            k_smooth_tile_gen<T, 2, 16, 16><<<b16, 256, gen_tile_smem<T>(), s>>>(op, z, zalt, b, m, n);
         else
             k_smooth_tile<Op, T, 2, 16, 16><<<b16, 256, 0, s>>>(op, z, zalt, b, m, n);
         nl++;
@@ -930,6 +1025,10 @@ int Multigrid::build_hierarchy() {
     }
     INCRMT_CK(cudaFuncSetAttribute(k_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTailSmemBudget)));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_gen<double, 2, 16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gen_tile_smem<double>()));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_gen<float, 2, 16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gen_tile_smem<float>()));
     INCRMT_CK(cudaFuncSetAttribute(k_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTailSmemBudget)));
     // First level small enough for the one-block tail kernel (never level 0).
@@ -1183,7 +1282,7 @@ template <class T>
 size_t tail_layout(TailLevels<T> &L, size_t budget) {
     long off = 0;
     L.smem_from = L.count;
-    for (int k = L.count - 1; k >= 1; k--) {
+    for (int k = L.count - 1; k >= 0; k--) {
         const long need = 11 * L.N[k];
         if (static_cast<size_t>(off + need) * sizeof(T) > budget) break;
         L.smem_from = k;

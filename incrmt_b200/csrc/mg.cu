@@ -19,27 +19,46 @@ __host__ __device__ __forceinline__ int wrap_idx(int i, int m, int p, bool &ok) 
     return i;
 }
 
-/** 1D prolongation weight P(f,I); mf, mc fine and coarse sizes, p periodic,
- * k coarsened (else identity). */
-__host__ __device__ __forceinline__ double pw(int f, int I, int mf, int mc, int p, bool k) {
-    if (!k) return f == I ? 1. : 0.;
-    int d = f - 2 * I;
-    if (p) { if (d > mf / 2) d -= mf; else if (d < -mf / 2) d += mf; }
-    if (d == 0) return 1.;
-    if (d == -1) return 0.5;
-    if (d == 1) return (p || I + 1 < mc) ? 0.5 : 1.;
-    return 0.;
-}
+/** t + a*b with the product rounded before the sum (no fused multiply-add),
+ * as the CPU oracle evaluates it: with the operator-dependent weights the
+ * products are not exact, and a fused form would round them differently. The
+ * FP32 V-cycles are not compared bit for bit and keep the fused form. */
+__device__ __forceinline__ double add_prod(double t, double a, double b) { return __dadd_rn(t, __dmul_rn(a, b)); }
+__device__ __forceinline__ float add_prod(float t, float a, float b) { return t + a * b; }
 
-__host__ __device__ __forceinline__ int support(int I, int mf, int p, bool k, int *f) {
-    if (!k) { f[0] = I; return 1; }
-    int c = 0;
-    for (int d = -1; d <= 1; d++) {
-        bool ok = true;
-        int g = wrap_idx(2 * I + d, mf, p, ok);
-        if (ok) f[c++] = g;
+/** Floor of a/2 for any sign of a. */
+__host__ __device__ __forceinline__ int half_floor(int a) { return a >= 0 ? a / 2 : -((1 - a) / 2); }
+
+/** Coarse base index of fine index i along a direction: i/2 rounded down
+ * when the direction is coarsened, else i. */
+__host__ __device__ __forceinline__ int base_of(int i, bool k) { return k ? half_floor(i) : i; }
+
+/** Coarse index of corner q (0 or 1) above base B along a direction of
+ * coarse size mc, or -1 outside a non-periodic grid (and for q=1 when the
+ * direction is not coarsened). */
+__host__ __device__ __forceinline__ int corner_of(int B, int q, int mc, int p, bool k) {
+    if (!k && q) return -1;
+    int c = B + q;
+    if (c < 0 || c >= mc) {
+        if (!p) return -1;
+        c = (c % mc + mc) % mc;
     }
     return c;
+}
+
+/** Prolongation weight of fine point (fi,fj) (unwrapped indices) for coarse
+ * point (I,J): entry qx+2qy of the point's four stored weights, with (qx,qy)
+ * the coarse point's offset from the point's base; 0 when it is not one of
+ * its corners or the point is outside a non-periodic grid. */
+template <class W>
+__device__ __forceinline__ double pweight(const W *P, int fm, int fn, int px, int py, bool kx, bool ky, int fi,
+                                          int fj, int I, int J) {
+    const int qx = I - base_of(fi, kx), qy = J - base_of(fj, ky);
+    if (qx < 0 || qx > 1 || qy < 0 || qy > 1) return 0;
+    bool ok = true;
+    const int i = wrap_idx(fi, fm, px, ok), j = wrap_idx(fj, fn, py, ok);
+    if (!ok) return 0;
+    return static_cast<double>(P[4 * (static_cast<long>(i) + static_cast<long>(fm) * j) + qx + 2 * qy]);
 }
 
 inline bool can_coarsen(int m, int p) { return p ? (m % 2 == 0 && m / 2 >= 4) : m >= 5; }
@@ -77,90 +96,103 @@ __global__ void k_fem_coef(const double *rho, int ml, int mf, int nf, double *c,
 }
 
 
-/** One entry (target offset ki,kj) of the Galerkin coarse stencil
- * A_c = P^T A P at coarse unknown (I,J), by one thread: the sum over the
- * fine support points f of (I,J) and their stencil entries of
- * P(f,I,J) * A(f,g) * P(g,(I+ki,J+kj)). */
+/** Operator-dependent prolongation of a level (black-box multigrid:
+ * Dendy, J. Comput. Phys. 48 (1982) 366-386): four weights per fine point,
+ * P[4f+qx+2qy] for the coarse point at offset (qx,qy) from the point's base
+ * (base_of). A point on a coarse point takes it with weight 1; a point
+ * between two coarse points along x takes L/(-C) and R/(-C), L, C, R its
+ * stencil summed over the columns left of, through and right of it (the
+ * operator collapsed along y), and along y likewise with the rows; a point
+ * between four coarse points takes -(its stencil entries times its eight
+ * neighbours' weights)/(its diagonal), so pass 1 runs after pass 0 has set
+ * the others. Constant coefficients give the bilinear 1, 1/2, 1/4; across a
+ * density jump the weights follow the flux; at the zero-pressure edge of the
+ * MAC system the last point's weight drops to about 1/3. Weights stay in
+ * double precision so that constants map onto constants exactly and the
+ * coarse operators of a pure-Neumann problem keep their null space. */
 template <class Op>
-__device__ __forceinline__ double galerkin_entry(const Op &op, int fm, int fn, int px, int py, bool kx, bool ky,
-                                                 int cm, int cn, int I, int J, int ki, int kj) {
-    bool okt = true;
-    const int Kx = wrap_idx(I + ki, cm, px, okt), Ky = wrap_idx(J + kj, cn, py, okt);
-    if (!okt) return 0;
-    int fx[3], fy[3];
-    const int nfx = support(I, fm, px, kx, fx), nfy = support(J, fn, py, ky, fy);
-    double q = 0;
-    for (int b = 0; b < nfy; b++) {
-        const double wy = pw(fy[b], J, fn, cn, py, ky);
-        for (int a = 0; a < nfx; a++) {
-            const double w = wy * pw(fx[a], I, fm, cm, px, kx);
-            if (w == 0) continue;
-            double s[9];
-            op.coef9(fx[a], fy[b], s);
-            for (int dj = -1; dj <= 1; dj++) {
-                bool oky = true;
-                const int gy = wrap_idx(fy[b] + dj, fn, py, oky);
-                if (!oky) continue;
-                const double vy = pw(gy, Ky, fn, cn, py, ky);
-                if (vy == 0) continue;
-                for (int di = -1; di <= 1; di++) {
-                    const double av = s[3 * (dj + 1) + di + 1];
-                    if (av == 0) continue;
-                    bool okx = true;
-                    const int gx = wrap_idx(fx[a] + di, fm, px, okx);
-                    if (!okx) continue;
-                    const double vx = pw(gx, Kx, fm, cm, px, kx);
-                    if (vx != 0) q += w * av * vx * vy;
+__global__ void k_build_p(Op op, int fm, int fn, int px, int py, bool kx, bool ky, int cm, int cn, double *P,
+                          int pass) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= fm || j >= fn) return;
+    const bool xo = kx && (i & 1), yo = ky && (j & 1);
+    if ((pass == 1) != (xo && yo)) return;
+    double a[9];
+    op.coef9(i, j, a);
+    double *q = P + 4 * (static_cast<long>(i) + static_cast<long>(fm) * j);
+    double w[4] = {0, 0, 0, 0};
+    const int bx = base_of(i, kx), by = base_of(j, ky);
+    const bool v1 = corner_of(bx, 1, cm, px, kx) >= 0, v2 = corner_of(by, 1, cn, py, ky) >= 0;
+    if (!xo && !yo) {
+        w[0] = 1;
+    } else if (xo && !yo) {
+        const double L = a[0] + a[3] + a[6], C = a[1] + a[4] + a[7], R = a[2] + a[5] + a[8];
+        w[0] = L / (-C);
+        if (v1) w[1] = R / (-C);
+    } else if (!xo && yo) {
+        const double D = a[0] + a[1] + a[2], M = a[3] + a[4] + a[5], U = a[6] + a[7] + a[8];
+        w[0] = D / (-M);
+        if (v2) w[2] = U / (-M);
+    } else {
+        double acc[4] = {0, 0, 0, 0};
+        for (int dj = -1; dj <= 1; dj++)
+            for (int di = -1; di <= 1; di++) {
+                const double av = a[3 * (dj + 1) + di + 1];
+                if ((di == 0 && dj == 0) || av == 0) continue;
+                bool ok = true;
+                const int gi = wrap_idx(i + di, fm, px, ok), gj = wrap_idx(j + dj, fn, py, ok);
+                if (!ok) continue;
+                const double *g = P + 4 * (static_cast<long>(gi) + static_cast<long>(fm) * gj);
+                const int ox = base_of(i + di, kx) - bx, oy = base_of(j + dj, ky) - by;
+                for (int r = 0; r < 4; r++) {
+                    const int cx = ox + (r & 1), cy = oy + (r >> 1);
+                    if (g[r] != 0 && cx <= 1 && cy <= 1) acc[cx + 2 * cy] = add_prod(acc[cx + 2 * cy], av, g[r]);
                 }
             }
-        }
+        for (int r = 0; r < 4; r++)
+            if (((r & 1) == 0 || v1) && ((r >> 1) == 0 || v2)) w[r] = -acc[r] / a[4];
     }
-    return q;
+    q[0] = w[0]; q[1] = w[1]; q[2] = w[2]; q[3] = w[3];
 }
 
-/** Galerkin coarse stencil A_c = P^T A P: one thread per coarse unknown and
- * stencil entry (blockIdx.z = entry), so that the boundary rows, whose
- * weights need the general index rules, cost no more than the others. */
-/** The same entry at an interior coarse unknown, where every weight is the
- * standard 1 (on a coarse point) or 1/2 (next to it): only the fine points
- * 2I+t and stencil offsets d with |t+d-2k| <= 1 contribute. */
+/** Galerkin coarse stencil A_c = P^T A P, one thread per coarse unknown
+ * (I,J): over the fine points f of its support (the 3 x 3 fine points about
+ * (2I,2J)) and the stencil neighbours g of f, P(f,(I,J)) A(f,g) P(g,K) is
+ * added to the entry of K - (I,J), K running over g's corners. */
 template <class Op>
-__device__ __forceinline__ double galerkin_entry_interior(const Op &op, int I, int J, int ki, int kj) {
-    double q = 0;
-    for (int ty = -1; ty <= 1; ty++) {
-        const double wy = ty == 0 ? 1.0 : 0.5;
-        for (int tx = -1; tx <= 1; tx++) {
-            // offsets d reaching the target: |t+d-2k| <= 1 and |d| <= 1
-            const int dxlo = max(-1, 2 * ki - 1 - tx), dxhi = min(1, 2 * ki + 1 - tx);
-            const int dylo = max(-1, 2 * kj - 1 - ty), dyhi = min(1, 2 * kj + 1 - ty);
-            if (dxlo > dxhi || dylo > dyhi) continue;
-            double a[9];
-            op.coef9(2 * I + tx, 2 * J + ty, a);
-            const double w = wy * (tx == 0 ? 1.0 : 0.5);
-            for (int dj = dylo; dj <= dyhi; dj++) {
-                const double vy = (ty + dj - 2 * kj) == 0 ? 1.0 : 0.5;
-                for (int di = dxlo; di <= dxhi; di++) {
-                    const double vx = (tx + di - 2 * ki) == 0 ? 1.0 : 0.5;
-                    q += w * a[3 * (dj + 1) + di + 1] * vx * vy;
-                }
-            }
-        }
-    }
-    return q;
-}
-
-template <class Op>
-__global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
-                           int cm, int cn, double *st) {
+__global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool ky, int cm, int cn, double *st,
+                           const double *P) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
     if (I >= cm || J >= cn) return;
-    const int e = blockIdx.z, ki = e % 3 - 1, kj = e / 3 - 1;
-    const long N = static_cast<long>(cm) * cn;
-    const bool interior = kx && ky && I >= 1 && J >= 1 && I <= cm - 2 && J <= cn - 2 &&
-                          2 * I + 2 <= fm - 1 && 2 * J + 2 <= fn - 1;
-    st[e * N + I + static_cast<long>(cm) * J] =
-        interior ? galerkin_entry_interior(op, I, J, ki, kj)
-                 : galerkin_entry(op, fm, fn, px, py, kx, ky, cm, cn, I, J, ki, kj);
+    double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int x0 = kx ? 2 * I - 1 : I, x1 = kx ? 2 * I + 1 : I, y0 = ky ? 2 * J - 1 : J, y1 = ky ? 2 * J + 1 : J;
+    for (int fj = y0; fj <= y1; fj++)
+        for (int fi = x0; fi <= x1; fi++) {
+            const double w = pweight(P, fm, fn, px, py, kx, ky, fi, fj, I, J);
+            if (w == 0) continue;
+            bool ok = true;
+            const int i = wrap_idx(fi, fm, px, ok), j = wrap_idx(fj, fn, py, ok);
+            double a[9];
+            op.coef9(i, j, a);
+            for (int dj = -1; dj <= 1; dj++)
+                for (int di = -1; di <= 1; di++) {
+                    const double av = a[3 * (dj + 1) + di + 1];
+                    if (av == 0) continue;
+                    bool okg = true;
+                    const int gi = wrap_idx(fi + di, fm, px, okg), gj = wrap_idx(fj + dj, fn, py, okg);
+                    if (!okg) continue;
+                    const double *g = P + 4 * (static_cast<long>(gi) + static_cast<long>(fm) * gj);
+                    const int ox = base_of(fi + di, kx) - I, oy = base_of(fj + dj, ky) - J;
+                    for (int r = 0; r < 4; r++) {
+                        const int kx_ = ox + (r & 1), ky_ = oy + (r >> 1);
+                        if (g[r] == 0 || kx_ < -1 || kx_ > 1 || ky_ < -1 || ky_ > 1) continue;
+                        double &qe = q[3 * (ky_ + 1) + kx_ + 1];
+                        qe = add_prod(qe, __dmul_rn(w, av), g[r]);
+                    }
+                }
+        }
+    const long N = static_cast<long>(cm) * cn, ij = I + static_cast<long>(cm) * J;
+    for (int e = 0; e < 9; e++) st[e * N + ij] = q[e];
 }
 
 __global__ void k_cast(const double *a, float *b, long n) {
@@ -395,22 +427,23 @@ __global__ void __launch_bounds__(256) k_smooth_rb(Op op, const T *zin, T *zout,
  * the fly; also clears the coarse iterate. */
 template <class Op, class T>
 __global__ void k_restrict(Op op, const T *z, const T *b, int fm, int fn, int px, int py,
-                           bool kx, bool ky, int cm, int cn, T *bc, T *zc) {
+                           bool kx, bool ky, int cm, int cn, T *bc, T *zc, const double *P) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
     if (I >= cm || J >= cn) return;
-    int fx[3], fy[3];
-    const int nfx = support(I, fm, px, kx, fx), nfy = support(J, fn, py, ky, fy);
+    const int x0 = kx ? 2 * I - 1 : I, x1 = kx ? 2 * I + 1 : I, y0 = ky ? 2 * J - 1 : J, y1 = ky ? 2 * J + 1 : J;
     T t = 0;
-    for (int bq = 0; bq < nfy; bq++) {
-        const T wy = static_cast<T>(pw(fy[bq], J, fn, cn, py, ky));
-        for (int a = 0; a < nfx; a++) {
-            const int f = fx[a] + fm * fy[bq];
+    for (int fj = y0; fj <= y1; fj++)
+        for (int fi = x0; fi <= x1; fi++) {
+            const T w = static_cast<T>(pweight(P, fm, fn, px, py, kx, ky, fi, fj, I, J));
+            if (w == 0) continue;
+            bool ok = true;
+            const int i = wrap_idx(fi, fm, px, ok), j = wrap_idx(fj, fn, py, ok);
+            const int f = i + fm * j;
             T diag;
-            const T off = op.offdiag(fx[a], fy[bq], z, diag);
+            const T off = op.offdiag(i, j, z, diag);
             const T r = b[f] - off - diag * z[f];
-            t += wy * static_cast<T>(pw(fx[a], I, fm, cm, px, kx)) * r;
+            t = add_prod(t, w, r);
         }
-    }
     bc[I + cm * J] = t;
     zc[I + cm * J] = 0;
 }
@@ -423,7 +456,8 @@ __global__ void k_restrict(Op op, const T *z, const T *b, int fm, int fn, int px
  * the weights and in the order of k_restrict: the same values. */
 template <class Op, class T>
 __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const T *b, int fm, int fn, int px, int py,
-                                                       bool kx, bool ky, int cm, int cn, T *bc, T *zc) {
+                                                       bool kx, bool ky, int cm, int cn, T *bc, T *zc,
+                                                       const double *P) {
     constexpr int CTW = 32, CTH = 8, RW = 2 * CTW + 1, RH = 2 * CTH + 1;
     __shared__ T rs[RW * RH];
     const int X0 = blockIdx.x * CTW, Y0 = blockIdx.y * CTH;
@@ -448,59 +482,38 @@ __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const 
     __syncthreads();
     const int I = X0 + (threadIdx.x & 31), J = Y0 + (threadIdx.x >> 5);
     if (I >= cm || J >= cn) return;
-    // The support in k_restrict's order (support(): offsets -1, 0, 1 where
-    // they exist), with each point's local position in the staged region.
-    int fx[3], fy[3], lx[3], ly[3], nfx = 0, nfy = 0;
-    if (!kx) { fx[0] = I; lx[0] = I - FX0; nfx = 1; }
-    else
-        for (int d = -1; d <= 1; d++) {
-            bool ok = true;
-            const int g = wrap_idx(2 * I + d, fm, px, ok);
-            if (ok) { fx[nfx] = g; lx[nfx] = 2 * I + d - FX0; nfx++; }
-        }
-    if (!ky) { fy[0] = J; ly[0] = J - FY0; nfy = 1; }
-    else
-        for (int d = -1; d <= 1; d++) {
-            bool ok = true;
-            const int g = wrap_idx(2 * J + d, fn, py, ok);
-            if (ok) { fy[nfy] = g; ly[nfy] = 2 * J + d - FY0; nfy++; }
-        }
+    // The support in k_restrict's order, each fine point read from its
+    // (unwrapped) position in the staged region.
+    const int x0 = kx ? 2 * I - 1 : I, x1 = kx ? 2 * I + 1 : I, y0 = ky ? 2 * J - 1 : J, y1 = ky ? 2 * J + 1 : J;
     T t = 0;
-    for (int bq = 0; bq < nfy; bq++) {
-        const T wy = static_cast<T>(pw(fy[bq], J, fn, cn, py, ky));
-        for (int a = 0; a < nfx; a++)
-            t += wy * static_cast<T>(pw(fx[a], I, fm, cm, px, kx)) * rs[lx[a] + FW * ly[bq]];
-    }
+    for (int fj = y0; fj <= y1; fj++)
+        for (int fi = x0; fi <= x1; fi++) {
+            const T w = static_cast<T>(pweight(P, fm, fn, px, py, kx, ky, fi, fj, I, J));
+            if (w == 0) continue;
+            t = add_prod(t, w, rs[(fi - FX0) + FW * (fj - FY0)]);
+        }
     bc[I + cm * J] = t;
     zc[I + cm * J] = 0;
 }
 
-/** Fine correction z_f += P z_c. */
+/** Fine correction z_f += P z_c, from the point's four stored weights. */
 template <class T>
 __global__ void k_prolong(T *zf, int fm, int fn, int px, int py, bool kx, bool ky,
-                          const T *zc, int cm, int cn) {
+                          const T *zc, int cm, int cn, const double *P) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= fm || j >= fn) return;
-    int Is[2], Js[2], ni = 0, nj = 0;
-    if (!kx) Is[ni++] = i;
-    else {
-        const int lo = (i % 2 == 0) ? i / 2 : (i - 1) / 2;
-        Is[ni++] = lo;
-        if (i % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cm, px, ok); if (ok) Is[ni++] = hi; }
-    }
-    if (!ky) Js[nj++] = j;
-    else {
-        const int lo = (j % 2 == 0) ? j / 2 : (j - 1) / 2;
-        Js[nj++] = lo;
-        if (j % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cn, py, ok); if (ok) Js[nj++] = hi; }
-    }
+    const long f = i + static_cast<long>(fm) * j;
+    const double *q = P + 4 * f;
+    const int bx = base_of(i, kx), by = base_of(j, ky);
     T t = 0;
-    for (int bq = 0; bq < nj; bq++) {
-        const T wy = static_cast<T>(pw(j, Js[bq], fn, cn, py, ky));
-        for (int a = 0; a < ni; a++)
-            t += wy * static_cast<T>(pw(i, Is[a], fm, cm, px, kx)) * zc[Is[a] + cm * Js[bq]];
+    for (int r = 0; r < 4; r++) {
+        const double w = q[r];
+        if (w == 0) continue;
+        const int I = corner_of(bx, r & 1, cm, px, kx), J = corner_of(by, r >> 1, cn, py, ky);
+        if (I < 0 || J < 0) continue;  // k_build_p leaves such corners at 0
+        t = add_prod(t, static_cast<T>(w), zc[I + cm * J]);
     }
-    zf[i + fm * j] += t;
+    zf[f] += t;
 }
 
 /** Coarsest-level solve: `sweeps` four-colour Gauss-Seidel sweeps by one
@@ -654,6 +667,7 @@ constexpr size_t kTailSmemBudget = 160 * 1024;  // shared memory for the smalles
 template <class T>
 struct TailLevels {
     int first, count, px, py;
+    const double *P[kTailMaxLevels]; // prolongation weights of each tail level but the last
     int smem_from;                 // levels >= smem_from live in shared memory
     const T *ginv;                 // dense inverse of the coarsest level, or null
     long smem_off[kTailMaxLevels]; // element offsets of st, then z, then b
@@ -734,21 +748,24 @@ __global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu
         tail_smooth(L, l, nu1);
         const GenOp<T> op = tail_op(L, l);
         const int fm = L.m[l], fn = L.n[l], cm = L.m[l + 1], cn = L.n[l + 1];
+        const bool kx = L.kx[l], ky = L.ky[l];
         for (int q = threadIdx.x; q < cm * cn; q += blockDim.x) {
             const int I = q % cm, J = q / cm;
-            int fx[3], fy[3];
-            const int nfx = support(I, fm, L.px, L.kx[l], fx), nfy = support(J, fn, L.py, L.ky[l], fy);
+            const int x0 = kx ? 2 * I - 1 : I, x1 = kx ? 2 * I + 1 : I, y0 = ky ? 2 * J - 1 : J,
+                      y1 = ky ? 2 * J + 1 : J;
             T t = 0;
-            for (int bq = 0; bq < nfy; bq++) {
-                const T wy = static_cast<T>(pw(fy[bq], J, fn, cn, L.py, L.ky[l]));
-                for (int a = 0; a < nfx; a++) {
-                    const int f = fx[a] + fm * fy[bq];
+            for (int fj = y0; fj <= y1; fj++)
+                for (int fi = x0; fi <= x1; fi++) {
+                    const T w = static_cast<T>(pweight(L.P[l], fm, fn, L.px, L.py, kx, ky, fi, fj, I, J));
+                    if (w == 0) continue;
+                    bool ok = true;
+                    const int i = wrap_idx(fi, fm, L.px, ok), j = wrap_idx(fj, fn, L.py, ok);
+                    const int f = i + fm * j;
                     T diag;
-                    const T off = op.offdiag(fx[a], fy[bq], L.z[l], diag);
+                    const T off = op.offdiag(i, j, L.z[l], diag);
                     const T r = L.b[l][f] - off - diag * L.z[l][f];
-                    t += wy * static_cast<T>(pw(fx[a], I, fm, cm, L.px, L.kx[l])) * r;
+                    t = add_prod(t, w, r);
                 }
-            }
             L.b[l + 1][q] = t;
             L.z[l + 1][q] = 0;
         }
@@ -764,24 +781,14 @@ __global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu
         const int fm = L.m[l], fn = L.n[l], cm = L.m[l + 1], cn = L.n[l + 1];
         for (int q = threadIdx.x; q < fm * fn; q += blockDim.x) {
             const int i = q % fm, j = q / fm;
-            int Is[2], Js[2], ni = 0, nj = 0;
-            if (!L.kx[l]) Is[ni++] = i;
-            else {
-                const int lo = (i % 2 == 0) ? i / 2 : (i - 1) / 2;
-                Is[ni++] = lo;
-                if (i % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cm, L.px, ok); if (ok) Is[ni++] = hi; }
-            }
-            if (!L.ky[l]) Js[nj++] = j;
-            else {
-                const int lo = (j % 2 == 0) ? j / 2 : (j - 1) / 2;
-                Js[nj++] = lo;
-                if (j % 2 == 1) { bool ok = true; int hi = wrap_idx(lo + 1, cn, L.py, ok); if (ok) Js[nj++] = hi; }
-            }
+            const double *w = L.P[l] + 4 * static_cast<long>(q);
+            const int bx = base_of(i, L.kx[l]), by = base_of(j, L.ky[l]);
             T t = 0;
-            for (int bq = 0; bq < nj; bq++) {
-                const T wy = static_cast<T>(pw(j, Js[bq], fn, cn, L.py, L.ky[l]));
-                for (int a = 0; a < ni; a++)
-                    t += wy * static_cast<T>(pw(i, Is[a], fm, cm, L.px, L.kx[l])) * L.z[l + 1][Is[a] + cm * Js[bq]];
+            for (int r = 0; r < 4; r++) {
+                if (w[r] == 0) continue;
+                const int I = corner_of(bx, r & 1, cm, L.px, L.kx[l]), J = corner_of(by, r >> 1, cn, L.py, L.ky[l]);
+                if (I < 0 || J < 0) continue;
+                t = add_prod(t, static_cast<T>(w[r]), L.z[l + 1][I + cm * J]);
             }
             L.z[l][q] += t;
         }
@@ -919,11 +926,12 @@ int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStrea
  * incrmt_mg_set_tiles covers both). */
 template <class Op, class T>
 void restrict_launch(bool tiles, Op op, cudaStream_t s, const T *z, const T *b, int fm, int fn, int px, int py,
-                     bool kx, bool ky, int cm, int cn, T *bc, T *zc) {
+                     bool kx, bool ky, int cm, int cn, T *bc, T *zc, const double *we) {
     if (tiles)
-        k_restrict_tile<<<dim3(cdiv(cm, 32), cdiv(cn, 8)), 256, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc);
+        k_restrict_tile<<<dim3(cdiv(cm, 32), cdiv(cn, 8)), 256, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc,
+                                                                         we);
     else
-        k_restrict<<<grid2(cm, cn), kBlk2, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc);
+        k_restrict<<<grid2(cm, cn), kBlk2, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc, we);
 }
 
 }  // namespace
@@ -1015,6 +1023,11 @@ int Multigrid::build_hierarchy() {
         lev.push_back(L);
         mm = mc; nn = nc;
     }
+    // Prolongation weights of every level but the coarsest (k_build_p).
+    for (size_t l = 0; l + 1 < lev.size(); l++) {
+        INCRMT_CK(cudaMalloc(&lev[l].P, sizeof(double) * 4 * lev[l].N));
+        INCRMT_CK(cudaMemsetAsync(lev[l].P, 0, sizeof(double) * 4 * lev[l].N, stream));
+    }
     if (lev.size() > 1 && lev.back().N <= kDirectMax) {
         const long N = lev.back().N;
         INCRMT_CK(cudaMalloc(&ginv, sizeof(double) * N * N));
@@ -1041,12 +1054,13 @@ int Multigrid::build_hierarchy() {
 void Multigrid::destroy() {
     for (auto &L : lev) {
         cudaFree(L.z); cudaFree(L.b); cudaFree(L.st); cudaFree(L.zf); cudaFree(L.bf); cudaFree(L.stf);
-        cudaFree(L.z2); cudaFree(L.zf2);
+        cudaFree(L.z2); cudaFree(L.zf2); cudaFree(L.P);
     }
     lev.clear();
     cudaFree(ex); cudaFree(ey); cudaFree(exf); cudaFree(eyf); cudaFree(c); cudaFree(cf);
     cudaFree(rho); cudaFree(bbuf); cudaFree(zbuf); cudaFree(partial); cudaFree(dnorm);
     cudaFree(ginv); cudaFree(ginvf); ginv = nullptr; ginvf = nullptr;
+
     if (hnorm) cudaFreeHost(hnorm);
     if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
     for (auto e : prof_ev) cudaEventDestroy(e);
@@ -1112,17 +1126,24 @@ int Multigrid::set_unit_density() {
 int Multigrid::galerkin_all() {
     for (size_t l = 1; l < lev.size(); l++) {
         MgLevel &F = lev[l - 1], &C = lev[l];
-        if (l == 1) {
-            if (sys == INCRMT_SYS_MAC)
-                k_galerkin<<<dim3(cdiv(C.m, 32), cdiv(C.n, 8), 9), kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
-            else
-                k_galerkin<<<dim3(cdiv(C.m, 32), cdiv(C.n, 8), 9), kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+        const dim3 gf = grid2(F.m, F.n), gc = grid2(C.m, C.n);
+        if (l == 1 && sys == INCRMT_SYS_MAC) {
+            for (int pass = 0; pass < 2; pass++)
+                k_build_p<<<gf, kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
+            k_galerkin<<<gc, kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
+        } else if (l == 1) {
+            for (int pass = 0; pass < 2; pass++)
+                k_build_p<<<gf, kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
+            k_galerkin<<<gc, kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
         } else {
             GenOp<double> g; g.m = F.m; g.n = F.n; g.px = px; g.py = py; g.N = F.N; g.st = F.st;
-            k_galerkin<<<dim3(cdiv(C.m, 32), cdiv(C.n, 8), 9), kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st);
+            for (int pass = 0; pass < 2; pass++)
+                k_build_p<<<gf, kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
+            k_galerkin<<<gc, kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
         }
+        launches += 3;
         k_cast<<<cdiv(9 * C.N, 256) < kRedBlocks ? cdiv(9 * C.N, 256) : kRedBlocks, 256, 0, stream>>>(C.st, C.stf, 9 * C.N);
-        launches += 2;
+        launches++;
         INCRMT_CKL("galerkin");
     }
     if (ginv) {
@@ -1166,19 +1187,19 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac64();
         if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
-        restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     } else if (l == 0) {
         auto op = fem64();
         if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
-        restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     } else {
         if ((r = smooth(g, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        restrict_launch(tiles, g, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z);
+        restrict_launch(tiles, g, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     }
     launches++;
     INCRMT_CKL("k_restrict");
     if ((r = cycle64(l + 1, b0, z0))) return r;
-    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(cur, L.m, L.n, px, py, L.kx, L.ky, static_cast<const double *>(C.z), C.m, C.n);
+    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(cur, L.m, L.n, px, py, L.kx, L.ky, static_cast<const double *>(C.z), C.m, C.n, L.P);
     launches++;
     INCRMT_CKL("k_prolong");
     double *alt = !tiles ? nullptr : cur == z ? L.z2 : z, *out = cur;
@@ -1251,19 +1272,19 @@ int Multigrid::cycle32(int l) {
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac32();
         if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else if (l == 0) {
         auto op = fem32();
         if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else {
         if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
-        restrict_launch(tiles, g, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf);
+        restrict_launch(tiles, g, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     }
     launches++;
     INCRMT_CKL("k_restrict");
     if ((r = cycle32(l + 1))) return r;
-    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(cur, L.m, L.n, px, py, L.kx, L.ky, static_cast<const float *>(C.zf), C.m, C.n);
+    k_prolong<<<grid2(L.m, L.n), kBlk2, 0, stream>>>(cur, L.m, L.n, px, py, L.kx, L.ky, static_cast<const float *>(C.zf), C.m, C.n, L.P);
     launches++;
     INCRMT_CKL("k_prolong");
     float *alt = !tiles ? nullptr : cur == z ? L.zf2 : z, *out = cur;
@@ -1299,7 +1320,7 @@ int Multigrid::tail64() {
     for (int k = 0; k < T.count; k++) {
         const MgLevel &L = lev[tail_level + k];
         T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
-        T.z[k] = L.z; T.b[k] = L.b; T.st[k] = L.st;
+        T.z[k] = L.z; T.b[k] = L.b; T.st[k] = L.st; T.P[k] = L.P;
     }
     T.ginv = ginv;
     const size_t sm = tail_layout(T, kTailSmemBudget);
@@ -1315,7 +1336,7 @@ int Multigrid::tail32() {
     for (int k = 0; k < T.count; k++) {
         const MgLevel &L = lev[tail_level + k];
         T.m[k] = L.m; T.n[k] = L.n; T.N[k] = L.N; T.kx[k] = L.kx; T.ky[k] = L.ky;
-        T.z[k] = L.zf; T.b[k] = L.bf; T.st[k] = L.stf;
+        T.z[k] = L.zf; T.b[k] = L.bf; T.st[k] = L.stf; T.P[k] = L.P;
     }
     T.ginv = ginvf;
     const size_t sm = tail_layout(T, kTailSmemBudget);

@@ -2,8 +2,10 @@
 //
 // Same method as the CPU oracle's TGMG-API shim, so that V-cycle counts are
 // comparable: vertex-style coarsening (coarse I on fine 2I), bilinear
-// prolongation P, restriction P^T, Galerkin coarse operators P^T A P rebuilt
-// on every density change, four-colour Gauss-Seidel smoothing visited as
+// operator-dependent prolongation P (black-box multigrid weights from the
+// collapsed stencil: bilinear for constant coefficients, following the flux
+// across density jumps and Dirichlet edges), restriction P^T, Galerkin coarse
+// operators P^T A P rebuilt on every density change, four-colour Gauss-Seidel smoothing visited as
 // (0,0),(1,1),(1,0),(0,1) (red-black for the 5-point MAC stencil), V(2,2)
 // cycles, and a one-block Gauss-Seidel solve on the coarsest level.
 //
@@ -26,6 +28,7 @@ struct MgLevel {
     double *z = nullptr, *b = nullptr, *st = nullptr;  // FP64 arrays (level >= 1)
     float *zf = nullptr, *bf = nullptr, *stf = nullptr;  // FP32 arrays (all levels)
     double *z2 = nullptr;  // second FP64 iterate buffer of the tile smoothers (all levels)
+    double *P = nullptr;   // prolongation to the next level: four weights per unknown (all but the last)
     float *zf2 = nullptr;  // and the FP32 one
 };
 

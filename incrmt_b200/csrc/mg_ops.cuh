@@ -14,6 +14,13 @@
 
 namespace incrmt {
 
+/** a - b*c with the product rounded before the difference in double (the
+ * reference's a_cc, mgs_mac.hh:93-97, evaluated as the CPU does, without a
+ * fused multiply-add), so that the MAC diagonal and the prolongation weights
+ * built from it agree with the oracle's to the last bit; fused in single. */
+__device__ __forceinline__ double mac_diag(double a, double b, double c) { return __dsub_rn(a, __dmul_rn(b, c)); }
+__device__ __forceinline__ float mac_diag(float a, float b, float c) { return a - b * c; }
+
 /** Variable-density MAC system (mgs_mac_varying_rho, mgs_mac.hh:64-102,
  * mgs_mac.cc:49-54). Unknowns are the m x n cells. The edge reciprocal
  * densities are stored as ex[(m+1)*n], the x-edge left of cell (i,j) at
@@ -38,8 +45,8 @@ struct MacOp {
         if (r) sx += er * z[i < m - 1 ? ij + 1 : ij + 1 - m];
         if (d) sy = ed * z[j > 0 ? ij - m : ij + m * (n - 1)];
         if (u) sy += eu * z[j < n - 1 ? ij + m : ij - m * (n - 1)];
-        diag = -xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0)))))
-               - yysp * ((d ? ed : T(0)) + (u ? eu : T(0)));
+        diag = mac_diag(-xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0))))),
+                        yysp, (d ? ed : T(0)) + (u ? eu : T(0)));
         return xxsp * sx + yysp * sy;
     }
 
@@ -55,8 +62,8 @@ struct MacOp {
         if (r) sx += er * zs[lz + 1];
         if (d) sy = ed * zs[lz - ldz];
         if (u) sy += eu * zs[lz + ldz];
-        diag = -xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0)))))
-               - yysp * ((d ? ed : T(0)) + (u ? eu : T(0)));
+        diag = mac_diag(-xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0))))),
+                        yysp, (d ? ed : T(0)) + (u ? eu : T(0)));
         return xxsp * sx + yysp * sy;
     }
 
@@ -65,8 +72,8 @@ struct MacOp {
         const T el = ex[j * (m + 1) + i], er = ex[j * (m + 1) + i + 1];
         const T ed = ey[j * m + i], eu = ey[(j + 1) * m + i];
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
-        diag = -xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0)))))
-               - yysp * ((d ? ed : T(0)) + (u ? eu : T(0)));
+        diag = mac_diag(-xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0))))),
+                        yysp, (d ? ed : T(0)) + (u ? eu : T(0)));
         a[0] = 0; a[1] = d ? yysp * ed : T(0); a[2] = 0;
         a[3] = l ? xxsp * el : T(0); a[4] = diag; a[5] = r ? xxsp * er : T(0);
         a[6] = 0; a[7] = u ? yysp * eu : T(0); a[8] = 0;

@@ -16,33 +16,35 @@ inline int tgmg_wrap(int i,int m,bool p,bool &ok) {
     return i;
 }
 
-/** One-dimensional prolongation weight P(f,I) between fine index f and
- * coarse index I.
- * \param[in] (mf,mc) fine and coarse sizes.
- * \param[in] p whether the direction is periodic.
- * \param[in] k whether the direction is coarsened (else P is the identity). */
-inline double tgmg_pw(int f,int I,int mf,int mc,bool p,bool k) {
-    if(!k) return f==I?1.:0.;
-    int d=f-2*I;
-    if(p) {if(d>mf/2) d-=mf;else if(d<-mf/2) d+=mf;}
-    if(d==0) return 1.;
-    if(d==-1) return 0.5;
-    if(d==1) return (p||I+1<mc)?0.5:1.;
-    return 0.;
+/** Floor of a/2 for any sign of a. */
+inline int tgmg_half(int a) {return a>=0?a/2:-((1-a)/2);}
+
+/** Coarse base index of fine index i along a direction (i/2 rounded down
+ * when the direction is coarsened, else i itself). */
+inline int tgmg_base_of(int i,bool k) {return k?tgmg_half(i):i;}
+
+/** Coarse index of corner q (0 or 1) above base B along a direction of
+ * coarse size mc, or -1 where it falls outside a non-periodic grid or the
+ * direction is not coarsened (q=1). */
+inline int tgmg_corner(int B,int q,int mc,bool p,bool k) {
+    if(!k&&q) return -1;
+    int c=B+q;
+    if(c<0||c>=mc) {if(!p) return -1;c=(c%mc+mc)%mc;}
+    return c;
 }
 
-/** Fine indices carrying a nonzero weight for coarse index I: 2I-1,2I,2I+1
- * (wrapped or clipped) when coarsened, else I itself.
- * \return The number of indices written to f. */
-inline int tgmg_support(int I,int mf,bool p,bool k,int *f) {
-    if(!k) {*f=I;return 1;}
-    int c=0;
-    for(int d=-1;d<=1;d++) {
-        bool ok=true;
-        int g=tgmg_wrap(2*I+d,mf,p,ok);
-        if(ok) f[c++]=g;
-    }
-    return c;
+/** The nine stencil entries of fs at fine point (i,j) in the order
+ * dl,dc,dr,cl,cc,cr,ul,uc,ur, zero where the neighbour lies outside a
+ * non-periodic grid (only in-grid entries are queried: the reference's FEM
+ * callbacks read their density array before testing the boundary,
+ * mgs_fem.hh:121-128). */
+template<class T>
+inline void tgmg_stencil(T &fs,int fm,int fn,bool fxp,bool fyp,int i,int j,double *a) {
+    const int ij=i+fm*j;
+    const bool l=fxp||i>0,r=fxp||i<fm-1,d=fyp||j>0,u=fyp||j<fn-1;
+    a[0]=d&&l?fs.a_dl(i,ij):0;a[1]=d?fs.a_dc(i,ij):0;a[2]=d&&r?fs.a_dr(i,ij):0;
+    a[3]=l?fs.a_cl(i,ij):0;a[4]=fs.a_cc(i,ij);a[5]=r?fs.a_cr(i,ij):0;
+    a[6]=u&&l?fs.a_ul(i,ij):0;a[7]=u?fs.a_uc(i,ij):0;a[8]=u&&r?fs.a_ur(i,ij):0;
 }
 
 template<class V,class M>
@@ -175,6 +177,7 @@ inline bool tgmg_can_coarsen(int m,bool p) {
 template<class S,class V,class M>
 tgmg<S,V,M>::tgmg(S &s_,V *b_,V *z_) : tgmg_base<S,V,M>(s_,b_,z_),
     nlev(1), rf(new V[s_.mn]), last_vcycles(0), last_rel_res(0), ginv(NULL) {
+    for(int l=0;l<tgmg_max_levels;l++) pw[l]=NULL;
     int m=this->m,n=this->n;
     bool xp=this->x_prd,yp=this->y_prd;
     while(nlev<tgmg_max_levels&&m*n>tgmg_coarsest_size) {
@@ -192,6 +195,7 @@ template<class S,class V,class M>
 tgmg<S,V,M>::~tgmg() {
     for(int l=nlev-1;l>=1;l--) {delete lb[l];delete lev[l];}
     delete [] rf;
+    for(int l=0;l<tgmg_max_levels;l++) if(pw[l]!=NULL) delete [] pw[l];
     if(ginv!=NULL) delete [] ginv;
 }
 
@@ -247,68 +251,124 @@ void tgmg<S,V,M>::coarse_inverse() {
     delete [] a;
 }
 
-/** Rebuilds every coarse operator by the Galerkin product P^T A P. */
+/** Rebuilds the prolongation of every level and every coarse operator by
+ * the Galerkin product P^T A P. */
 template<class S,class V,class M>
 void tgmg<S,V,M>::setup() {
     for(int l=1;l<nlev;l++) {
-        if(l==1) galerkin(this->s,this->m,this->n,this->x_prd,this->y_prd,*lev[1],cx[0],cy[0]);
-        else {
+        if(l==1) {
+            build_p(this->s,0,this->m,this->n,this->x_prd,this->y_prd,*lev[1],cx[0],cy[0]);
+            galerkin(this->s,0,this->m,this->n,this->x_prd,this->y_prd,*lev[1],cx[0],cy[0]);
+        } else {
             tgmg_level<V,M> &f=*lev[l-1];
-            galerkin(f,f.m,f.n,f.x_prd,f.y_prd,*lev[l],cx[l-1],cy[l-1]);
+            build_p(f,l-1,f.m,f.n,f.x_prd,f.y_prd,*lev[l],cx[l-1],cy[l-1]);
+            galerkin(f,l-1,f.m,f.n,f.x_prd,f.y_prd,*lev[l],cx[l-1],cy[l-1]);
         }
     }
     if(nlev>1&&lev[nlev-1]->mn<=tgmg_direct_max) coarse_inverse();
 }
 
+/** Operator-dependent prolongation of level l (black-box multigrid: Dendy,
+ * J. Comput. Phys. 48 (1982) 366-386), four weights per fine point, one per
+ * corner q = qx+2qy of the coarse cell above its base (tgmg_base_of):
+ * a point on a coarse point takes it with weight 1; a point between two
+ * coarse points along x takes L/(-C) and R/(-C), with L, C, R its stencil
+ * summed over the columns left of, through and right of it (the operator
+ * collapsed along y), and likewise along y with the rows; a point between
+ * four coarse points takes -(sum of its stencil entries times the weights of
+ * its eight neighbours)/(its diagonal). With constant coefficients these are
+ * the bilinear weights 1, 1/2, 1/4; across density jumps they follow the
+ * flux, and at a Dirichlet edge (the zero-pressure edge of the MAC system)
+ * the last point's weight drops below 1. The weights stay in double
+ * precision: rounded ones would no longer map constants onto constants, and
+ * the coarse operators of a pure-Neumann problem would lose their exact
+ * null space. */
 template<class S,class V,class M>
 template<class T>
-void tgmg<S,V,M>::galerkin(T &fs,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky) {
+void tgmg<S,V,M>::build_p(T &fs,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky) {
+    const int cm=c.m,cn=c.n;
+    if(pw[l]==NULL) pw[l]=new double[4*fm*fn];
+    double *P=pw[l];
+    for(int pass=0;pass<2;pass++) {
+#pragma omp parallel for
+        for(int j=0;j<fn;j++) for(int i=0;i<fm;i++) {
+            const bool xo=kx&&(i&1),yo=ky&&(j&1);
+            if((pass==1)!=(xo&&yo)) continue;
+            double a[9],*q=P+4*(i+fm*j);
+            tgmg_stencil(fs,fm,fn,fxp,fyp,i,j,a);
+            q[0]=q[1]=q[2]=q[3]=0;
+            const int bx=tgmg_base_of(i,kx),by=tgmg_base_of(j,ky);
+            const bool v1=tgmg_corner(bx,1,cm,fxp,kx)>=0,v2=tgmg_corner(by,1,cn,fyp,ky)>=0;
+            if(!xo&&!yo) q[0]=1;
+            else if(xo&&!yo) {
+                const double L=a[0]+a[3]+a[6],C=a[1]+a[4]+a[7],R=a[2]+a[5]+a[8];
+                q[0]=L/(-C);
+                if(v1) q[1]=R/(-C);
+            } else if(!xo&&yo) {
+                const double D=a[0]+a[1]+a[2],Mr=a[3]+a[4]+a[5],U=a[6]+a[7]+a[8];
+                q[0]=D/(-Mr);
+                if(v2) q[2]=U/(-Mr);
+            } else {
+                double acc[4]={0,0,0,0};
+                for(int dj=-1;dj<=1;dj++) for(int di=-1;di<=1;di++) {
+                    const double av=a[3*(dj+1)+di+1];
+                    if((di==0&&dj==0)||av==0) continue;
+                    bool okx=true,oky=true;
+                    const int gi=tgmg_wrap(i+di,fm,fxp,okx),gj=tgmg_wrap(j+dj,fn,fyp,oky);
+                    if(!okx||!oky) continue;
+                    const double *g=P+4*(gi+fm*gj);
+                    const int ox=tgmg_base_of(i+di,kx)-bx,oy=tgmg_base_of(j+dj,ky)-by;
+                    for(int r=0;r<4;r++) {
+                        const int cx_=ox+(r&1),cy_=oy+(r>>1);
+                        if(g[r]!=0&&cx_<=1&&cy_<=1) acc[cx_+2*cy_]+=av*g[r];
+                    }
+                }
+                for(int r=0;r<4;r++) {
+                    const bool ok=((r&1)==0||v1)&&((r>>1)==0||v2);
+                    if(ok) q[r]=-acc[r]/a[4];
+                }
+            }
+        }
+    }
+}
+
+/** Weight of fine point (fi,fj) (unwrapped indices, in the grid once
+ * wrapped) for coarse point (I,J), 0 when (I,J) is not one of its corners. */
+template<class S,class V,class M>
+inline double tgmg<S,V,M>::pweight(int l,int fm,int fn,bool fxp,bool fyp,bool kx,bool ky,int fi,int fj,int I,int J) {
+    const int qx=I-tgmg_base_of(fi,kx),qy=J-tgmg_base_of(fj,ky);
+    if(qx<0||qx>1||qy<0||qy>1) return 0;
+    bool okx=true,oky=true;
+    const int i=tgmg_wrap(fi,fm,fxp,okx),j=tgmg_wrap(fj,fn,fyp,oky);
+    if(!okx||!oky) return 0;
+    return pw[l][4*(i+fm*j)+qx+2*qy];
+}
+
+/** Galerkin coarse operator A_c = P^T A P of level l+1 from level l's
+ * operator fs and prolongation, entry by entry: A_c((I,J),(I,J)+k) sums,
+ * over the fine points f of the coarse point's support and the stencil
+ * neighbours g of f, P(f,(I,J)) A(f,g) P(g,(I,J)+k). */
+template<class S,class V,class M>
+template<class T>
+void tgmg<S,V,M>::galerkin(T &fs,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky) {
     const int cm=c.m,cn=c.n;
 #pragma omp parallel for
     for(int J=0;J<cn;J++) for(int I=0;I<cm;I++) {
         double q[9]={0,0,0,0,0,0,0,0,0};
-        int fx[3],fy[3];
-        int nfx=tgmg_support(I,fm,fxp,kx,fx),nfy=tgmg_support(J,fn,fyp,ky,fy);
-        for(int b=0;b<nfy;b++) {
-            double wy=tgmg_pw(fy[b],J,fn,cn,fyp,ky);
-            for(int a=0;a<nfx;a++) {
-                double w=wy*tgmg_pw(fx[a],I,fm,cm,fxp,kx);
-                if(w==0) continue;
-                int i=fx[a],ij=i+fm*fy[b];
-                // Only entries whose neighbour lies inside the grid are
-                // queried: the reference's FEM callbacks read their density
-                // array before testing the boundary (mgs_fem.hh:121-128), so
-                // an outward entry would read past its end.
-                const bool l=fxp||i>0,r=fxp||i<fm-1,d=fyp||fy[b]>0,u=fyp||fy[b]<fn-1;
-                double st[9]={d&&l?fs.a_dl(i,ij):0,d?fs.a_dc(i,ij):0,d&&r?fs.a_dr(i,ij):0,
-                              l?fs.a_cl(i,ij):0,fs.a_cc(i,ij),r?fs.a_cr(i,ij):0,
-                              u&&l?fs.a_ul(i,ij):0,u?fs.a_uc(i,ij):0,u&&r?fs.a_ur(i,ij):0};
-                for(int dj=-1;dj<=1;dj++) {
-                    bool oky=true;
-                    int gy=tgmg_wrap(fy[b]+dj,fn,fyp,oky);
-                    if(!oky) continue;
-                    for(int di=-1;di<=1;di++) {
-                        double av=st[3*(dj+1)+di+1];
-                        if(av==0) continue;
-                        bool okx=true;
-                        int gx=tgmg_wrap(i+di,fm,fxp,okx);
-                        if(!okx) continue;
-                        for(int kj=-1;kj<=1;kj++) {
-                            bool ok=true;
-                            int Ky=tgmg_wrap(J+kj,cn,fyp,ok);
-                            if(!ok) continue;
-                            double vy=tgmg_pw(gy,Ky,fn,cn,fyp,ky);
-                            if(vy==0) continue;
-                            for(int ki=-1;ki<=1;ki++) {
-                                bool ok2=true;
-                                int Kx=tgmg_wrap(I+ki,cm,fxp,ok2);
-                                if(!ok2) continue;
-                                double vx=tgmg_pw(gx,Kx,fm,cm,fxp,kx);
-                                if(vx==0) continue;
-                                q[3*(kj+1)+ki+1]+=w*av*vx*vy;
-                            }
-                        }
-                    }
+        const int x0=kx?2*I-1:I,x1=kx?2*I+1:I,y0=ky?2*J-1:J,y1=ky?2*J+1:J;
+        for(int fj=y0;fj<=y1;fj++) for(int fi=x0;fi<=x1;fi++) {
+            const double w=pweight(l,fm,fn,fxp,fyp,kx,ky,fi,fj,I,J);
+            if(w==0) continue;
+            bool okx=true,oky=true;
+            const int i=tgmg_wrap(fi,fm,fxp,okx),j=tgmg_wrap(fj,fn,fyp,oky);
+            double a[9];
+            tgmg_stencil(fs,fm,fn,fxp,fyp,i,j,a);
+            for(int dj=-1;dj<=1;dj++) for(int di=-1;di<=1;di++) {
+                const double av=a[3*(dj+1)+di+1];
+                if(av==0) continue;
+                for(int kj=-1;kj<=1;kj++) for(int ki=-1;ki<=1;ki++) {
+                    const double v=pweight(l,fm,fn,fxp,fyp,kx,ky,fi+di,fj+dj,I+ki,J+kj);
+                    if(v!=0) q[3*(kj+1)+ki+1]+=w*av*v;
                 }
             }
         }
@@ -319,17 +379,18 @@ void tgmg<S,V,M>::galerkin(T &fs,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M>
 
 /** Coarse right-hand side b_c = P^T r. */
 template<class S,class V,class M>
-void tgmg<S,V,M>::restrict_to(V *r,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky) {
+void tgmg<S,V,M>::restrict_to(V *r,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky) {
     const int cm=c.m,cn=c.n;
 #pragma omp parallel for
     for(int J=0;J<cn;J++) for(int I=0;I<cm;I++) {
-        int fx[3],fy[3];
-        int nfx=tgmg_support(I,fm,fxp,kx,fx),nfy=tgmg_support(J,fn,fyp,ky,fy);
+        const int x0=kx?2*I-1:I,x1=kx?2*I+1:I,y0=ky?2*J-1:J,y1=ky?2*J+1:J;
         double t=0;
-        for(int b=0;b<nfy;b++) {
-            double wy=tgmg_pw(fy[b],J,fn,cn,fyp,ky);
-            for(int a=0;a<nfx;a++)
-                t+=wy*tgmg_pw(fx[a],I,fm,cm,fxp,kx)*r[fx[a]+fm*fy[b]];
+        for(int fj=y0;fj<=y1;fj++) for(int fi=x0;fi<=x1;fi++) {
+            const double w=pweight(l,fm,fn,fxp,fyp,kx,ky,fi,fj,I,J);
+            if(w==0) continue;
+            bool okx=true,oky=true;
+            const int i=tgmg_wrap(fi,fm,fxp,okx),j=tgmg_wrap(fj,fn,fyp,oky);
+            t+=w*r[i+fm*j];
         }
         c.b[I+cm*J]=t;
         c.z[I+cm*J]=0;
@@ -338,36 +399,17 @@ void tgmg<S,V,M>::restrict_to(V *r,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,
 
 /** Fine correction z_f += P z_c. */
 template<class S,class V,class M>
-void tgmg<S,V,M>::prolong_add(V *zf,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky) {
+void tgmg<S,V,M>::prolong_add(V *zf,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky) {
     const int cm=c.m,cn=c.n;
 #pragma omp parallel for
     for(int j=0;j<fn;j++) for(int i=0;i<fm;i++) {
-        int Is[2],Js[2],ni=0,nj=0;
-        if(!kx) Is[ni++]=i;
-        else {
-            int lo=(i%2==0)?i/2:(i-1)/2;
-            Is[ni++]=lo;
-            if(i%2==1) {
-                bool ok=true;
-                int hi=tgmg_wrap(lo+1,cm,fxp,ok);
-                if(ok) Is[ni++]=hi;
-            }
-        }
-        if(!ky) Js[nj++]=j;
-        else {
-            int lo=(j%2==0)?j/2:(j-1)/2;
-            Js[nj++]=lo;
-            if(j%2==1) {
-                bool ok=true;
-                int hi=tgmg_wrap(lo+1,cn,fyp,ok);
-                if(ok) Js[nj++]=hi;
-            }
-        }
+        const double *q=pw[l]+4*(i+fm*j);
+        const int bx=tgmg_base_of(i,kx),by=tgmg_base_of(j,ky);
         double t=0;
-        for(int b=0;b<nj;b++) {
-            double wy=tgmg_pw(j,Js[b],fn,cn,fyp,ky);
-            for(int a=0;a<ni;a++)
-                t+=wy*tgmg_pw(i,Is[a],fm,cm,fxp,kx)*c.z[Is[a]+cm*Js[b]];
+        for(int r=0;r<4;r++) {
+            if(q[r]==0) continue;
+            const int I=tgmg_corner(bx,r&1,cm,fxp,kx),J=tgmg_corner(by,r>>1,cn,fyp,ky);
+            t+=q[r]*c.z[I+cm*J];
         }
         zf[i+fm*j]+=t;
     }
@@ -392,17 +434,17 @@ void tgmg<S,V,M>::cycle(int l) {
     if(l==0) {
         this->smooth(tgmg_nu1);
         this->residual(rf);
-        restrict_to(rf,this->m,this->n,this->x_prd,this->y_prd,c,cx[0],cy[0]);
+        restrict_to(rf,0,this->m,this->n,this->x_prd,this->y_prd,c,cx[0],cy[0]);
         cycle(1);
-        prolong_add(this->z,this->m,this->n,this->x_prd,this->y_prd,c,cx[0],cy[0]);
+        prolong_add(this->z,0,this->m,this->n,this->x_prd,this->y_prd,c,cx[0],cy[0]);
         this->smooth(tgmg_nu2);
     } else {
         tgmg_level<V,M> &f=*lev[l];
         lb[l]->smooth(tgmg_nu1);
         lb[l]->residual(f.r);
-        restrict_to(f.r,f.m,f.n,f.x_prd,f.y_prd,c,cx[l],cy[l]);
+        restrict_to(f.r,l,f.m,f.n,f.x_prd,f.y_prd,c,cx[l],cy[l]);
         cycle(l+1);
-        prolong_add(f.z,f.m,f.n,f.x_prd,f.y_prd,c,cx[l],cy[l]);
+        prolong_add(f.z,l,f.m,f.n,f.x_prd,f.y_prd,c,cx[l],cy[l]);
         lb[l]->smooth(tgmg_nu2);
     }
 }

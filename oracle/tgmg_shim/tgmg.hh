@@ -15,8 +15,10 @@
  * Method. Unknowns form an m x n grid with a 9-point stencil. A coarse level
  * keeps every second point of each direction that is coarsened (vertex-style:
  * coarse I sits on fine 2I; mc=(m+1)/2, or m/2 when periodic), with bilinear
- * prolongation P (the last odd fine point of an even non-periodic direction
- * copies its only coarse neighbour), restriction R=P^T and the Galerkin
+ * operator-dependent prolongation P (black-box multigrid weights from the
+ * collapsed stencil: the bilinear 1, 1/2, 1/4 for constant coefficients,
+ * following the flux across density jumps and Dirichlet edges), restriction
+ * R=P^T and the Galerkin
  * operator A_c=P^T A P, rebuilt on every setup(). The smoother is Gauss-Seidel
  * in four colours (i&1,j&1) visited in the order (0,0),(1,1),(1,0),(0,1),
  * which is red-black ordering for a 5-point stencil and race-free for a
@@ -112,6 +114,9 @@ class tgmg : public tgmg_base<S,V,M> {
         tgmg_base<tgmg_level<V,M>,V,M>* lb[tgmg_max_levels];
         /** Whether level l+1 halves the x and y directions of level l. */
         bool cx[tgmg_max_levels],cy[tgmg_max_levels];
+        /** Prolongation of level l to l+1: four weights per fine point of
+         * level l (build_p), set by setup(). */
+        double* pw[tgmg_max_levels];
         /** Fine-level residual scratch. */
         V* const rf;
         /** V-cycles of the most recent solve_v_cycle call. */
@@ -136,9 +141,12 @@ class tgmg : public tgmg_base<S,V,M> {
     private:
         void cycle(int l);
         template<class T>
-        void galerkin(T &fs,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
-        void restrict_to(V *r,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
-        void prolong_add(V *zf,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
+        void build_p(T &fs,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
+        inline double pweight(int l,int fm,int fn,bool fxp,bool fyp,bool kx,bool ky,int fi,int fj,int I,int J);
+        template<class T>
+        void galerkin(T &fs,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
+        void restrict_to(V *r,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
+        void prolong_add(V *zf,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
         void coarse_inverse();
 };
 

@@ -846,6 +846,13 @@ def main():
     finally:
         if dist is not None:
             dist.destroy_process_group()
+    # The C ABI library carries its own (static) CUDA runtime, whose exit
+    # handler can release the device context before Python's teardown has
+    # destroyed torch's CUDA objects; everything is reported and released by
+    # now, so the process ends without that teardown.
+    sys.stdout.flush()
+    sys.stderr.flush()
+    os._exit(0)
 
 
 if __name__ == "__main__":

@@ -55,8 +55,17 @@ SCENES = {
 
 
 def _rel(a, b):
-    s = np.abs(b).max()
-    return float(np.abs(a - b).max() / (s if s > 0 else 1.0))
+    # a non-finite value where the other array is finite fails the comparison
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    fa, fb = np.isfinite(a), np.isfinite(b)
+    if not np.array_equal(fa, fb):
+        return float("inf")
+    if not fb.any():
+        return 0.0
+    d = np.abs(a[fb] - b[fb])
+    s = np.abs(b[fb]).max()
+    return float(d.max() / (s if s > 0 else 1.0))
 
 
 def _pair(name):

@@ -48,6 +48,7 @@ the reference's mgs_mac_varying_rho callbacks driven by the clean-room TGMG
 shim (oracle/_ref), with all host threads.
 """
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -817,6 +818,8 @@ def run_ours(args, ws, rank, local, dist):
 
 
 def main():
+    # a crash in native code prints the Python stack it happened under
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)

@@ -773,10 +773,14 @@ def run_ours(args, ws, rank, local, dist):
     e2e_s = _max_over_ranks(dist, e2e_s)
     e2e = ws * args.steps / e2e_s
 
+    # The solver (and the network) must outlive the pinned host tensors that
+    # were copied on the solver's stream (non-blocking copies under
+    # torch.cuda.stream(ext) in e2e_step): when those are released, torch's
+    # pinned-memory allocator records an event on every stream that used
+    # them, so that stream must still exist. They are kept until main() ends
+    # the process.
+    _KEEP_ALIVE.extend([s, net, ext])
     if rank != 0:
-        if net is not None:
-            net.close()
-        s.close()
         return
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
@@ -812,9 +816,10 @@ def run_ours(args, ws, rank, local, dist):
         "clocks": clk.summary(),
     }
     print(json.dumps(line))
-    if net is not None:
-        net.close()
-    s.close()
+
+
+# Handles kept until the process ends (see run_ours_mac).
+_KEEP_ALIVE = []
 
 
 def main():

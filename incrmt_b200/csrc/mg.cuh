@@ -1,7 +1,7 @@
 // Geometric multigrid for the MAC and FEM pressure systems on one B200.
 //
 // Same method as the CPU oracle's TGMG-API shim, so that V-cycle counts are
-// comparable: vertex-style coarsening (coarse I on fine 2I), bilinear
+// comparable: vertex-style coarsening (coarse I on fine 2I), an
 // operator-dependent prolongation P (black-box multigrid weights from the
 // collapsed stencil: bilinear for constant coefficients, following the flux
 // across density jumps and Dirichlet edges), restriction P^T, Galerkin coarse

@@ -14,7 +14,7 @@
  *
  * Method. Unknowns form an m x n grid with a 9-point stencil. A coarse level
  * keeps every second point of each direction that is coarsened (vertex-style:
- * coarse I sits on fine 2I; mc=(m+1)/2, or m/2 when periodic), with bilinear
+ * coarse I sits on fine 2I; mc=(m+1)/2, or m/2 when periodic), with an
  * operator-dependent prolongation P (black-box multigrid weights from the
  * collapsed stencil: the bilinear 1, 1/2, 1/4 for constant coefficients,
  * following the flux across density jumps and Dirichlet edges), restriction

@@ -8,8 +8,9 @@
  * version: the reference expects it at ../tgmg, Makefile:4,14). That library
  * is absent, so this shim restates the published geometric-multigrid method
  * (Briggs, Henson & McCormick, "A Multigrid Tutorial", 2nd ed., ch. 3-4 and
- * 8: Galerkin coarse operators, bilinear prolongation, Gauss-Seidel
- * smoothing, V-cycles) behind exactly the API used at the reference's call
+ * 8: Galerkin coarse operators, Gauss-Seidel smoothing, V-cycles; the
+ * operator-dependent prolongation of black-box multigrid, Dendy, J. Comput.
+ * Phys. 48 (1982) 366-386) behind exactly the API used at the reference's call
  * sites (mgs_mac.cc:10-34,40-71; mgs_fem.cc:25-120; mgs_common.cc:70-74;
  * mg_test.cc:21-43; fluid_2d.cc:284-290). The GPU multigrid in incrmt_b200
  * implements the same V-cycle so that V-cycle counts are comparable. */

@@ -220,16 +220,16 @@ def cpu_reference_sspin(m, steps, warmup):
 
 
 def _sed_reference_objects(seed=11):
-    """The sediment bodies as reference objects: circles as obj_circle, each
-    ellipse as the nearest reference shape, a rounded rod (obj_rounded_rod)
-    with the minor semi-axis as radius and the axis difference as half-length."""
+    """The sediment bodies as reference objects: circles as obj_circle, the
+    ellipses as the oracle harness's obj_ellipse (an obj_standard subclass
+    compiled against the reference; the reference has no ellipse)."""
     from incrmt_b200 import workloads
     objs = []
     for o in workloads.sediment_bodies(seed=seed):
         if o["kind"] == "circle":
             objs.append(("circle", (o["cx"], o["cy"], o["r"], 0, 0, 0, o["grav"]), 1.0, o["rhos"]))
         else:
-            objs.append(("rod", (o["cx"], o["cy"], o["b"], o["r"] - o["b"], o["grav"]), 1.0, o["rhos"]))
+            objs.append(("ellipse", (o["cx"], o["cy"], o["r"], o["b"], o["theta"], o["grav"]), 1.0, o["rhos"]))
     return objs
 
 
@@ -548,6 +548,7 @@ def run_ours_sspin(args, ws, rank, local, dist):
             "plain_fp64_steps_per_s": plain_sps, "plain_fp64_vcycles_per_projection": plain_vc,
             "speedup_vs_plain_fp64": value / ws / plain_sps})
     if rank != 0:
+        sim.close()
         return
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
@@ -773,14 +774,24 @@ def run_ours(args, ws, rank, local, dist):
     e2e_s = _max_over_ranks(dist, e2e_s)
     e2e = ws * args.steps / e2e_s
 
-    # The solver (and the network) must outlive the pinned host tensors that
-    # were copied on the solver's stream (non-blocking copies under
-    # torch.cuda.stream(ext) in e2e_step): when those are released, torch's
-    # pinned-memory allocator records an event on every stream that used
-    # them, so that stream must still exist. They are kept until main() ends
-    # the process.
-    _KEEP_ALIVE.extend([s, net, ext])
+    # Release in order: the pinned host tensors were copied on the solver's
+    # stream (non-blocking copies under torch.cuda.stream(ext) in e2e_step),
+    # and when one is freed torch's pinned-memory allocator records an event
+    # on every stream that used it, so they go first, while the solver (which
+    # owns the stream) is still alive.
+    del rho_np, b_np, z_np, rho_h, b_h, z_h
+    torch.cuda.synchronize()
+    import gc
+    gc.collect()
+
+    def release():
+        torch.cuda.synchronize()
+        s.close()
+        if net is not None:
+            net.close()
+
     if rank != 0:
+        release()
         return
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
@@ -816,10 +827,7 @@ def run_ours(args, ws, rank, local, dist):
         "clocks": clk.summary(),
     }
     print(json.dumps(line))
-
-
-# Handles kept until the process ends (see run_ours_mac).
-_KEEP_ALIVE = []
+    release()
 
 
 def main():
@@ -854,13 +862,7 @@ def main():
     finally:
         if dist is not None:
             dist.destroy_process_group()
-    # The C ABI library carries its own (static) CUDA runtime, whose exit
-    # handler can release the device context before Python's teardown has
-    # destroyed torch's CUDA objects; everything is reported and released by
-    # now, so the process ends without that teardown.
     sys.stdout.flush()
-    sys.stderr.flush()
-    os._exit(0)
 
 
 if __name__ == "__main__":

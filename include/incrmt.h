@@ -76,7 +76,11 @@ int incrmt_mg_set_density_device(incrmt_mg *h, const double *d_rho);
 int incrmt_mg_solve(incrmt_mg *h, const double *b, double *z,
                     const incrmt_mg_opts *opts, incrmt_mg_stats *stats);
 
-/** Same with device pointers (b read-only, z in/out), on the handle's stream. */
+/** Same with device pointers (b read-only, z in/out), on the handle's stream.
+ * A solve reads each V-cycle's residual norm back to the host, so it must not
+ * be called while the handle's stream is being captured into a CUDA graph
+ * (that call returns INCRMT_ERR_BADARG). A right-hand side of zero norm
+ * returns z = 0. */
 int incrmt_mg_solve_device(incrmt_mg *h, const double *d_b, double *d_z,
                            const incrmt_mg_opts *opts, incrmt_mg_stats *stats);
 
@@ -98,6 +102,23 @@ int incrmt_mg_set_profiling(incrmt_mg *h, int on);
  * per colour in the V-cycle's four-colour order. Off (0) runs one launch per
  * colour everywhere; it exists to check that identity. */
 int incrmt_mg_set_tiles(incrmt_mg *h, int on);
+
+/** Lagged coarse operators (no reference counterpart; default 1). With
+ * every > 1 a density change recomputes the fine-level coefficients, which
+ * define the system solved, but rebuilds the Galerkin coarse levels only on
+ * every `every`-th change; the reference rebuilds on each one
+ * (mgs_mac.cc:62-63, mgs_fem.cc:108-109). Stale coarse levels only steer
+ * convergence: every solve still reaches its tolerance on the current
+ * operator. If a solve fails (V-cycle cap or a non-finite residual) while its
+ * coarse levels are lagged, they are rebuilt from the last density and the
+ * solve is repeated once, from zero if the iterate is not finite. With
+ * every > 1, incrmt_mg_set_density_device copies the density into the
+ * handle, so the caller's array need not outlive the call. */
+int incrmt_mg_set_coarse_refresh(incrmt_mg *h, int every);
+
+/** Galerkin hierarchy rebuilds since creation; *retries (if not null)
+ * receives the number of solves repeated after rebuilding lagged levels. */
+long long incrmt_mg_coarse_builds(const incrmt_mg *h, long long *retries);
 
 /** Accumulated profile since incrmt_mg_set_profiling: total device time (ms)
  * of the timed launches, their algorithmic bytes (updated unknowns x (3+c)
@@ -127,7 +148,9 @@ void incrmt_mg_destroy(incrmt_mg *h);
  * loads the library until exit). Grids larger than 256 x 256 cells are
  * rejected with INCRMT_ERR_BADARG. The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture. All calls share the array, so calls that overlap on the
+ * any stream capture. The address is cached per device for the process's
+ * primary context: after cudaDeviceReset, or from a context other than the
+ * primary one, it is not valid (a failed lookup is not cached). All calls share the array, so calls that overlap on the
  * GPU (other streams, other host threads) race; each call writes every
  * scratch word it reads. */
 int incrmt_mg_apply_noalloc(int sys, int m, int n, double ax, double bx, double ay, double by,

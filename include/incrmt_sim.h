@@ -111,6 +111,8 @@ typedef struct incrmt_sim_stats {
     long long window_points;               /* level-set points in the objects' current rebuild
                                               windows (all objects' whole grids when off) */
     long long coarse_builds;               /* Galerkin hierarchy rebuilds, MAC plus FEM */
+    long long coarse_retries;              /* projections solved again after a failed solve on lagged
+                                              coarse levels, with the levels rebuilt */
 } incrmt_sim_stats;
 
 /** Creates the simulation (fluid_2d::fluid_2d, fluid_2d.cc:26-43). */

@@ -79,6 +79,9 @@ def lib():
     L.incrmt_mg_vcycle_device.argtypes = [P, P, P]
     L.incrmt_mg_set_profiling.argtypes = [P, I]
     L.incrmt_mg_set_tiles.argtypes = [P, I]
+    L.incrmt_mg_set_coarse_refresh.argtypes = [P, I]
+    L.incrmt_mg_coarse_builds.argtypes = [P, ctypes.POINTER(ctypes.c_longlong)]
+    L.incrmt_mg_coarse_builds.restype = ctypes.c_longlong
     L.incrmt_mg_profile.argtypes = [P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(ctypes.c_longlong)]
     L.incrmt_mg_stream.argtypes = [P]
     L.incrmt_mg_stream.restype = P
@@ -181,6 +184,18 @@ class MGSolver:
         per colour."""
         check(lib().incrmt_mg_set_tiles(self._h, int(on)))
 
+    def set_coarse_refresh(self, every):
+        """Rebuild the Galerkin coarse levels every `every` density changes
+        (incrmt_mg_set_coarse_refresh; 1 rebuilds on every change)."""
+        check(lib().incrmt_mg_set_coarse_refresh(self._h, int(every)))
+
+    def coarse_builds(self):
+        """(hierarchy rebuilds, solves repeated after a rebuild of lagged
+        coarse levels) since creation."""
+        r = ctypes.c_longlong()
+        b = lib().incrmt_mg_coarse_builds(self._h, ctypes.byref(r))
+        return int(b), int(r.value)
+
     def profile(self):
         """(device ms, algorithmic bytes, launches) of the timed fine-level sweeps."""
         ms, by, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
@@ -270,7 +285,7 @@ class SimStats(ctypes.Structure):
                 ("extrap_sweeps", ctypes.c_longlong), ("launches", ctypes.c_longlong),
                 ("dt_reg", ctypes.c_double), ("time", ctypes.c_double),
                 ("march_monotone", ctypes.c_longlong), ("window_points", ctypes.c_longlong),
-                ("coarse_builds", ctypes.c_longlong)]
+                ("coarse_builds", ctypes.c_longlong), ("coarse_retries", ctypes.c_longlong)]
 
 
 def _sim_sigs(L):

@@ -53,7 +53,13 @@ int incrmt_mg_size(const incrmt_mg *h, int *m_sys, int *n_sys) {
 
 int incrmt_mg_set_density_device(incrmt_mg *h, const double *d_rho) {
     if (!h || !d_rho) { set_error("null argument"); return INCRMT_ERR_BADARG; }
-    return h->mg.set_density_device(d_rho);
+    incrmt::Multigrid &g = h->mg;
+    if (g.coarse_every <= 1) return g.set_density_device(d_rho);
+    // Lagged coarse levels may be rebuilt at the next solve: keep the
+    // density in the handle's own buffer until then.
+    const size_t bytes = sizeof(double) * (g.cm + 4) * (g.cn + 4);
+    INCRMT_CK(cudaMemcpyAsync(g.rho, d_rho, bytes, cudaMemcpyDeviceToDevice, g.stream));
+    return g.set_density_lagged(g.rho, 0);
 }
 
 int incrmt_mg_set_density(incrmt_mg *h, const double *rho) {
@@ -61,7 +67,7 @@ int incrmt_mg_set_density(incrmt_mg *h, const double *rho) {
     incrmt::Multigrid &g = h->mg;
     const size_t bytes = sizeof(double) * (g.cm + 4) * (g.cn + 4);
     INCRMT_CK(cudaMemcpyAsync(g.rho, rho, bytes, cudaMemcpyHostToDevice, g.stream));
-    int r = g.set_density_device(g.rho);
+    int r = g.set_density_lagged(g.rho, 0);
     if (r != INCRMT_OK) return r;
     INCRMT_CK(cudaStreamSynchronize(g.stream));
     return INCRMT_OK;
@@ -70,7 +76,7 @@ int incrmt_mg_set_density(incrmt_mg *h, const double *rho) {
 int incrmt_mg_solve_device(incrmt_mg *h, const double *d_b, double *d_z,
                            const incrmt_mg_opts *opts, incrmt_mg_stats *stats) {
     if (!h || !d_b || !d_z) { set_error("null argument"); return INCRMT_ERR_BADARG; }
-    return h->mg.solve_device(d_b, d_z, opts, stats, true);
+    return h->mg.solve_lagged(d_b, d_z, opts, stats, true);
 }
 
 int incrmt_mg_solve(incrmt_mg *h, const double *b, double *z,
@@ -80,7 +86,7 @@ int incrmt_mg_solve(incrmt_mg *h, const double *b, double *z,
     const size_t bytes = sizeof(double) * g.m * g.n;
     INCRMT_CK(cudaMemcpyAsync(g.bbuf, b, bytes, cudaMemcpyHostToDevice, g.stream));
     INCRMT_CK(cudaMemcpyAsync(g.zbuf, z, bytes, cudaMemcpyHostToDevice, g.stream));
-    int r = g.solve_device(g.bbuf, g.zbuf, opts, stats, true);
+    int r = g.solve_lagged(g.bbuf, g.zbuf, opts, stats, true);
     if (r != INCRMT_OK && r != INCRMT_ERR_NOCONV) return r;
     cudaError_t e1 = cudaMemcpyAsync(z, g.zbuf, bytes, cudaMemcpyDeviceToHost, g.stream);
     cudaError_t e2 = cudaStreamSynchronize(g.stream);
@@ -116,6 +122,19 @@ int incrmt_mg_set_tiles(incrmt_mg *h, int on) {
         mg.gexec = nullptr;
     }
     return INCRMT_OK;
+}
+
+int incrmt_mg_set_coarse_refresh(incrmt_mg *h, int every) {
+    if (!h || every < 1) { set_error("bad argument"); return INCRMT_ERR_BADARG; }
+    h->mg.coarse_every = every;
+    h->mg.coarse_stale = true;
+    return INCRMT_OK;
+}
+
+long long incrmt_mg_coarse_builds(const incrmt_mg *h, long long *retries) {
+    if (!h) return 0;
+    if (retries) *retries = h->mg.coarse_retries;
+    return h->mg.coarse_builds;
 }
 
 int incrmt_mg_set_profiling(incrmt_mg *h, int on) {

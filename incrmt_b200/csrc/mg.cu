@@ -1090,6 +1090,8 @@ int Multigrid::set_density_device(const double *d_rho, int ld) {
 }
 
 int Multigrid::set_density_lagged(const double *d_rho, int ld) {
+    lag_rho = d_rho;
+    lag_ld = ld;
     if (!ready || coarse_stale || coarse_every <= 1 || coarse_age + 1 >= coarse_every)
         return set_density_device(d_rho, ld);
     if (ld <= 0) ld = cm + 4;
@@ -1107,6 +1109,34 @@ int Multigrid::set_density_lagged(const double *d_rho, int ld) {
 void Multigrid::note_vcycles(int vc) {
     if (coarse_vc0 < 0) coarse_vc0 = vc;
     else if (vc > coarse_vc0 + 1) coarse_stale = true;
+}
+
+int Multigrid::solve_lagged(const double *d_b, double *d_z, const incrmt_mg_opts *o, incrmt_mg_stats *st,
+                            bool time_it) {
+    incrmt_mg_stats s1{};
+    int r = solve_device(d_b, d_z, o, &s1, time_it);
+    if (r == INCRMT_OK) {
+        note_vcycles(s1.vcycles);
+        if (st) *st = s1;
+        return r;
+    }
+    coarse_stale = true;
+    if ((r == INCRMT_ERR_NOCONV || r == INCRMT_ERR_NONFINITE) && coarse_age > 0 && lag_rho) {
+        if (r == INCRMT_ERR_NONFINITE)
+            INCRMT_CK(cudaMemsetAsync(d_z, 0, sizeof(double) * static_cast<size_t>(m) * n, stream));
+        int rr = set_density_device(lag_rho, lag_ld);
+        if (rr) return rr;
+        coarse_retries++;
+        incrmt_mg_stats s2{};
+        r = solve_device(d_b, d_z, o, &s2, time_it);
+        s1.vcycles += s2.vcycles;
+        s1.rel_res = s2.rel_res;
+        s1.device_ms += s2.device_ms;
+        if (r == INCRMT_OK) note_vcycles(s2.vcycles);
+        else coarse_stale = true;
+    }
+    if (st) *st = s1;
+    return r;
 }
 
 int Multigrid::set_unit_density() {
@@ -1431,6 +1461,14 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
     const int prec = o ? o->precision : INCRMT_PREC_FP64;
     if (prec != INCRMT_PREC_FP64 && prec != INCRMT_PREC_MIXED) { set_error("bad precision %d", prec); return INCRMT_ERR_BADARG; }
     const long N = static_cast<long>(m) * n;
+    // The solve reads a residual norm back to the host after every V-cycle,
+    // which a stream under capture cannot do.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    INCRMT_CK(cudaStreamIsCapturing(stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("a solve cannot run while its stream is being captured into a CUDA graph");
+        return INCRMT_ERR_BADARG;
+    }
     if (time_it) INCRMT_CK(cudaEventRecord(ev0, stream));
     const double *b = d_b;
     if (sys == INCRMT_SYS_FEM && zpr) {
@@ -1447,9 +1485,21 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
     const double nb = std::sqrt(nb2), tol = rtol * nb;
     int k = 0;
     if (nb == 0) {
-        // A zero right-hand side is solved by the current iterate's gauge:
-        // nothing to do (the solution is defined up to the null space).
-        if (st) { st->vcycles = 0; st->rel_res = 0; st->device_ms = 0; }
+        // A zero right-hand side: z = 0 solves A z = 0 exactly (for the
+        // singular pure-Neumann systems it is the zero-mean solution), and the
+        // warm start need not, so the iterate is cleared.
+        INCRMT_CK(cudaMemsetAsync(d_z, 0, sizeof(double) * N, stream));
+        if (time_it) {
+            INCRMT_CK(cudaEventRecord(ev1, stream));
+            INCRMT_CK(cudaEventSynchronize(ev1));
+        }
+        if (st) {
+            st->vcycles = 0;
+            st->rel_res = 0;
+            float ms = 0;
+            if (time_it) cudaEventElapsedTime(&ms, ev0, ev1);
+            st->device_ms = ms;
+        }
         return INCRMT_OK;
     }
     bool conv = false, finite = true;
@@ -1464,10 +1514,14 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
         cudaGraph_t graph;
         INCRMT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        graph = nullptr;
         int rc = vcycle_and_norm(prec, b, d_z, N);
         cudaError_t ce = cudaStreamEndCapture(stream, &graph);
-        if (rc) return rc;
-        if (ce != cudaSuccess) return cuda_status(ce, "capture", __FILE__, __LINE__);
+        if (rc || ce != cudaSuccess) {
+            if (ce == cudaSuccess && graph) cudaGraphDestroy(graph);
+            if (rc) return rc;
+            return cuda_status(ce, "capture", __FILE__, __LINE__);
+        }
         ce = cudaGraphInstantiate(&gexec, graph, 0);
         cudaGraphDestroy(graph);
         if (ce != cudaSuccess) { gexec = nullptr; return cuda_status(ce, "instantiate", __FILE__, __LINE__); }

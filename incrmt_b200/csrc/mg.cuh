@@ -65,6 +65,9 @@ public:
     int coarse_vc0 = -1;
     bool coarse_stale = true;
     long long coarse_builds = 0;
+    long long coarse_retries = 0;    // solves repeated after rebuilding lagged coarse levels
+    const double *lag_rho = nullptr; // density of the last set_density_lagged (read again on a retry)
+    int lag_ld = 0;
     bool tiles = true;               // tile-fused smoothing where it applies
     int tail_level = -1;             // first level run by the one-block tail kernel
     cudaGraphExec_t gexec = nullptr; // captured V-cycle + norm
@@ -99,6 +102,16 @@ public:
     int set_density_lagged(const double *d_rho, int ld);
     /** Records a solve's V-cycle count for the lag policy. */
     void note_vcycles(int vc);
+    /** solve_device after set_density_lagged. If the solve fails (V-cycle cap
+     * or a non-finite residual) while the coarse levels are lagged, i.e.
+     * built for an earlier density, they are rebuilt from the density given
+     * to set_density_lagged (which must still hold it) and the solve is
+     * repeated once, from a zero iterate if the failed one is not finite.
+     * The reference rebuilds its solver for every projection
+     * (mgs_mac.cc:62-63, mgs_fem.cc:108-109), so a system it converges on
+     * must not fail here for want of a rebuild. Any failure marks the coarse
+     * levels stale. The statistics count the V-cycles of both attempts. */
+    int solve_lagged(const double *d_b, double *d_z, const incrmt_mg_opts *o, incrmt_mg_stats *st, bool time_it);
     int solve_device(const double *d_b, double *d_z, const incrmt_mg_opts *o,
                      incrmt_mg_stats *st, bool time_it);
     int vcycle64(const double *d_b, double *d_z);

@@ -738,12 +738,11 @@ int Sim::mac_projection() {
     incrmt_mg_stats st{};
     long long l0 = mac.launches;
     if ((r = learned_pre(INCRMT_SYS_MAC, src_mac, z_mac))) return r;
-    r = mac.solve_device(src_mac, z_mac, &mgo, &st, false);
+    r = const_rho ? mac.solve_device(src_mac, z_mac, &mgo, &st, false) : mac.solve_lagged(src_mac, z_mac, &mgo, &st, false);
     if (!r) r = learned_post(INCRMT_SYS_MAC, z_mac);
     launches += mac.launches - l0;
     vc_mac += st.vcycles;
     solves_mac++;
-    if (!r) mac.note_vcycles(st.vcycles);
     if (r) return r;
     k_mac_correct<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, z_mac, mac.ex, mac.ey);
     launches++;
@@ -810,12 +809,11 @@ int Sim::fem_projection(double dt) {
     incrmt_mg_stats st{};
     long long l0 = fem.launches;
     if ((r = learned_pre(INCRMT_SYS_FEM, src_fem, z_fem))) return r;
-    r = fem.solve_device(src_fem, z_fem, &mgo, &st, false);
+    r = const_rho ? fem.solve_device(src_fem, z_fem, &mgo, &st, false) : fem.solve_lagged(src_fem, z_fem, &mgo, &st, false);
     if (!r) r = learned_post(INCRMT_SYS_FEM, z_fem);
     launches += fem.launches - l0;
     vc_fem += st.vcycles;
     solves_fem++;
-    if (!r) fem.note_vcycles(st.vcycles);
     if (r) return r;
     const int nb = 2 * kB200SMs;
     k_pressure_sum<<<nb, 256, 0, stream>>>(g, z_fem, partial);
@@ -1417,6 +1415,7 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
     }
     st->extrap_sweeps = S.ex_sweeps;
     st->coarse_builds = S.mac.coarse_builds + S.fem.coarse_builds;
+    st->coarse_retries = S.mac.coarse_retries + S.fem.coarse_retries;
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;
     st->time = S.time;

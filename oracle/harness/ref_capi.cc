@@ -33,6 +33,30 @@
 
 namespace {
 
+/** The sediment workload's ellipse, which the reference lacks, written as
+ * a harness-side subclass of the reference's obj_standard on the pattern of
+ * obj_circle (object.hh:128-138, object.cc:22-34): translated reference map
+ * (obj_standard::transform), at rest initially, and the circle's gravity
+ * acceleration. Its level set is the same first-order distance the GPU's
+ * ellipse uses: with r = |(X'/a, Y'/b)| in the body frame rotated by theta,
+ * phi = (r - 1)/|grad r| = (r - 1) r / |(X'/a^2, Y'/b^2)|, zero exactly on the
+ * boundary; the band rebuild turns the band values into distances. */
+struct obj_ellipse : public obj_standard {
+    const double ea, eb, cth, sth, grav;
+    obj_ellipse(double cx_,double cy_,double a_,double b_,double theta,double grav_) :
+        obj_standard(cx_,cy_,a_), ea(a_), eb(b_), cth(cos(theta)), sth(sin(theta)), grav(grav_) {}
+    virtual double phi(double X,double Y) {
+        const double xb=cth*X+sth*Y,yb=-sth*X+cth*Y,ia=1/ea,ib=1/eb;
+        const double r=sqrt(xb*xb*ia*ia+yb*yb*ib*ib);
+        const double gr=sqrt(xb*xb*ia*ia*ia*ia+yb*yb*ib*ib*ib*ib);
+        if(gr==0) return -(ea<eb?ea:eb);
+        return (r-1)*r/gr;
+    }
+    virtual void accel(double x,double y,double X,double Y,double phiv,double &accx,double &accy) {
+        accy-=grav*op->trans_func_in(phiv);
+    }
+};
+
 /** One reference simulation together with the objects it owns. */
 struct ref_sim {
     sim_type *st;
@@ -92,7 +116,8 @@ ref_sim* make_sspin(int m,int ntrace,const char *base) {
  * object.hh:487-488), squares (5), seven-pointed stars (6), flappers (7),
  * pistons (8), circle trackers (9), triangles (11: obj_triangle(cx,cy,cr,
  * theta,grav)), lampreys (12: obj_lamprey(cx,cy,theta,le,dis,w1,w2,T,mlam))
- * and hoops (13: obj_hoop(r_in,r_out,grav)), each with its constructor's
+ * hoops (13: obj_hoop(r_in,r_out,grav)) and the harness's ellipses (14:
+ * obj_ellipse(cx,cy,a,b,theta,grav), above), each with its constructor's
  * arguments in order; mats holds G and rhos per object. flow_u > 0 selects
  * sim_horiz_flow(flow_u, geom) (sim_type.hh:125-126; y-periodic, inflow at the
  * left, zero pressure at the right) instead of sim_type(geom, x_prd, y_prd).
@@ -120,6 +145,7 @@ ref_sim* make_multi(int m,int n,const double *geom,int x_prd,int y_prd,double vi
         else if(types[k]==11) r->obj.push_back(new obj_triangle(p[0],p[1],p[2],p[3],p[4]));
         else if(types[k]==12) r->obj.push_back(new obj_lamprey(p[0],p[1],p[2],p[3],p[4],p[5],p[6],p[7],p[8]));
         else if(types[k]==13) r->obj.push_back(new obj_hoop(p[0],p[1],p[2]));
+        else if(types[k]==14) r->obj.push_back(new obj_ellipse(p[0],p[1],p[2],p[3],p[4],p[5]));
         else r->obj.push_back(new obj_flag(p[0],p[1],p[2],p[3],p[4],p[5],static_cast<int>(p[6]),r->fa));
     }
     if(flow_u>0) r->st=new sim_horiz_flow(flow_u,geom[0],geom[1],geom[2],geom[3]);

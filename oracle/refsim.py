@@ -119,7 +119,7 @@ def mg_apply(sys, m, n, rho, z, ax=-1., bx=1., ay=-1., by=1., x_prd=False, y_prd
 
 # object kinds of ref_multi_create (oracle/harness/ref_capi.cc make_multi)
 OBJECT_TYPES = {"circle": 1, "rod": 2, "flag": 3, "square": 5, "star": 6, "flapper": 7, "piston": 8,
-                "circle_track": 9, "triangle": 11, "lamprey": 12, "hoop": 13}
+                "circle_track": 9, "triangle": 11, "lamprey": 12, "hoop": 13, "ellipse": 14}
 
 
 class RefSim:
@@ -127,8 +127,9 @@ class RefSim:
     `objects` a domain of circles and rounded rods.
 
     objects: list of ("circle", (cx, cy, cr, uu, vv, omega, grav), G, rhos),
-    ("rod", (cx, cy, cr, cl, grav), G, rhos) or ("flag", (cx, cy, flag_l,
-    flag_w, flag_a, perturb_v, ntrace), G, rhos); geom = (ax, bx, ay, by);
+    ("rod", (cx, cy, cr, cl, grav), G, rhos), ("ellipse", (cx, cy, a, b, theta,
+    grav), G, rhos) or ("flag", (cx, cy, flag_l, flag_w, flag_a, perturb_v,
+    ntrace), G, rhos); geom = (ax, bx, ay, by);
     flow_u > 0 makes the domain sim_horiz_flow (y-periodic with inflow)."""
 
     def __init__(self, m, ntrace=512, workdir=None, n=None, objects=None, geom=(-1., 1., -1., 1.),

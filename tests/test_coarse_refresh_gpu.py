@@ -79,3 +79,57 @@ def test_set_field_marks_stale(gpu):
     g.step(0.9 * dt, 1)
     assert g.stats().coarse_builds == b0 + 2  # MAC and FEM rebuilt
     g.close()
+
+
+def _disc_density(m, rho_s, cx=0.2, cy=-0.1, r=0.3):
+    """Ghosted (m+4)^2 density on [-1,1]^2: rho_s inside a disc, 1 outside,
+    blended over two cells."""
+    h = 2.0 / m
+    x = -1 + (np.arange(m + 4) - 1.5) * h
+    X, Y = np.meshgrid(x, x)
+    d = np.hypot(X - cx, Y - cy) - r
+    t = np.clip(0.5 - d / (4 * h), 0.0, 1.0)
+    return 1.0 + (rho_s - 1.0) * t
+
+
+def test_failed_lagged_solve_rebuilds_and_retries(gpu):
+    """A solve on coarse levels lagged behind a 1000x density jump fails at
+    the V-cycle cap a fresh hierarchy meets; the solver then rebuilds the
+    levels from the current density and solves again, and returns the fresh
+    hierarchy's solution."""
+    from incrmt_b200 import capi, workloads
+    m = 128
+    rho_b = _disc_density(m, 1000.0)
+    b = workloads.standalone_mac_problem(m, seed=5)[1].numpy().ravel()
+    ref = capi.MGSolver(capi.SYS_MAC, m, m)
+    ref.set_density(rho_b)
+    z_ref = np.zeros(m * m)
+    k = ref.solve(b, z_ref).vcycles
+    ref.close()
+
+    s = capi.MGSolver(capi.SYS_MAC, m, m)
+    s.set_coarse_refresh(16)
+    s.set_density(np.ones((m + 4, m + 4)))   # builds the hierarchy
+    s.set_density(rho_b)                      # lagged: fine coefficients only
+    assert s.coarse_builds() == (1, 0)
+    z = np.zeros(m * m)
+    st = s.solve(b, z, max_vcycles=k + 1)
+    builds, retries = s.coarse_builds()
+    assert (builds, retries) == (2, 1), (builds, retries, st.vcycles, k)
+    assert st.vcycles > k + 1 and st.rel_res <= 1e-9
+    zr, zz = z_ref - z_ref.mean(), z - z.mean()
+    assert np.linalg.norm(zz - zr) / np.linalg.norm(zr) <= 1e-8
+    s.close()
+
+
+def test_zero_rhs_returns_zero(gpu):
+    """A right-hand side of zero norm is solved by z = 0, whatever the warm
+    start held."""
+    from incrmt_b200 import capi
+    m = 64
+    s = capi.MGSolver(capi.SYS_FEM, m, m, zpr=True)
+    s.set_density(_disc_density(m, 3.0))
+    z = np.linspace(-1, 1, (m + 1) * (m + 1))
+    st = s.solve(np.zeros_like(z), z)
+    assert st.vcycles == 0 and not z.any()
+    s.close()

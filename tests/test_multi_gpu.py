@@ -1,11 +1,17 @@
-"""GPU parity with several solids: two circles close enough for the
-collision stress (fluid_2d::collision_stress, fluid_2d.cc:541-598) and a
-rounded rod (obj_rounded_rod, object.hh:218-241), all falling under gravity
-in a walled 64 x 96 box. The oracle is the reference's own fluid_2d with these
-objects (oracle/_ref, ref_multi_create). Same protocol and tolerances as the
-single-solid stage tests: the evolved reference state is copied into the
-GPU simulation, one step function runs on each, and every field of every
-object is compared.
+"""GPU parity with several solids falling under gravity in a walled 64 x 96
+box, in two scenes:
+  - "circles_rod": two circles close enough for the collision stress
+    (fluid_2d::collision_stress, fluid_2d.cc:541-598) and a rounded rod
+    (obj_rounded_rod, object.hh:218-241);
+  - "ellipses": the sediment workload's bodies, two rotated ellipses and a
+    circle. The reference has no ellipse; the oracle's is the harness-side
+    obj_ellipse (oracle/harness/ref_capi.cc), a subclass of the reference's
+    obj_standard with the GPU ellipse's level set and obj_circle's gravity,
+    compiled against the unmodified reference.
+The oracle is the reference's own fluid_2d with these objects (oracle/_ref,
+ref_multi_create). Same protocol and tolerances as the single-solid stage
+tests: the evolved reference state is copied into the GPU simulation, one
+step function runs on each, and every field of every object is compared.
 """
 import numpy as np
 import pytest
@@ -18,33 +24,50 @@ FIELDS = "u v p rho ux uy vx vy ud vd ul vl ur vr uu vu c0 c1 c2 c3 s11 s12 s21 
 SFIELDS = "X Y nX nY Xx Xy Yx Yy Xd Yd Xl Yl Xr Yr Xu Yu".split()
 GEOM = (-1.0, 1.0, -1.5, 1.5)
 M, N = 64, 96
-# (kind, params, G, rhos): the circles' transition zones (eps = 2.5 dx) overlap
-OBJECTS = [
-    ("circle", (0.0, 0.3, 0.2, 0.0, 0.0, 0.0, 0.5), 10.0, 2.0),
-    ("circle", (0.0, -0.12, 0.2, 0.0, 0.0, 0.0, 0.6), 10.0, 2.5),
-    ("rod", (0.55, 0.0, 0.08, 0.25, 0.3), 10.0, 1.5),
-]
+# (kind, params, G, rhos)
+SCENES = {
+    # the circles' transition zones (eps = 2.5 dx) overlap
+    "circles_rod": [
+        ("circle", (0.0, 0.3, 0.2, 0.0, 0.0, 0.0, 0.5), 10.0, 2.0),
+        ("circle", (0.0, -0.12, 0.2, 0.0, 0.0, 0.0, 0.6), 10.0, 2.5),
+        ("rod", (0.55, 0.0, 0.08, 0.25, 0.3), 10.0, 1.5),
+    ],
+    # ellipse params (cx, cy, a, b, theta, grav); gravity (rho_s - 1)/rho_s
+    "ellipses": [
+        ("ellipse", (-0.35, 0.45, 0.25, 0.12, 0.4, 0.5), 10.0, 2.0),
+        ("ellipse", (0.3, -0.35, 0.2, 0.09, -0.9, 0.6), 10.0, 2.5),
+        ("circle", (0.35, 0.75, 0.12, 0.0, 0.0, 0.0, 1.0 / 3.0), 10.0, 1.5),
+    ],
+}
 
 needs_oracle = pytest.mark.skipif(not oracle_available(), reason="oracle/_ref not built")
 
 
-def _gpu_sim(ntrace=16):
+@pytest.fixture(scope="module", params=sorted(SCENES))
+def scene(request):
+    return request.param
+
+
+def _gpu_sim(objects, ntrace=16):
     from incrmt_b200 import capi
     g = capi.Simulation(M, N, ax=GEOM[0], bx=GEOM[1], ay=GEOM[2], by=GEOM[3], ntrace=ntrace)
-    for kind, p, G, rhos in OBJECTS:
+    for kind, p, G, rhos in objects:
         if kind == "circle":
             cx, cy, cr, uu, vv, om, grav = p
             g.add_circle(cx, cy, cr, G, rhos, grav=grav, uu=uu, vv=vv, omega=om)
+        elif kind == "ellipse":
+            cx, cy, a, b, th, grav = p
+            g.add_ellipse(cx, cy, a, b, th, G, rhos, grav=grav)
         else:
             cx, cy, cr, cl, grav = p
             g.add_rounded_rod(cx, cy, cr, cl, G, rhos, grav=grav)
     return g
 
 
-def _pair(ntrace=16):
+def _pair(objects, ntrace=16):
     from oracle import refsim
-    r = refsim.RefSim(M, ntrace=ntrace, n=N, objects=OBJECTS, geom=GEOM)
-    g = _gpu_sim(ntrace)
+    r = refsim.RefSim(M, ntrace=ntrace, n=N, objects=objects, geom=GEOM)
+    g = _gpu_sim(objects, ntrace)
     dt_reg = g.initialize()
     assert abs(dt_reg - r.scalars()["dt_reg"]) <= 1e-15 * dt_reg
     g.set_tracers(r.tracers()[:, :2])
@@ -55,7 +78,7 @@ def _pair(ntrace=16):
 def _copy(r, g):
     for f in FIELDS:
         g.set(f, r.get(f))
-    for k in range(len(OBJECTS)):
+    for k in range(g.objects):
         for f in SFIELDS + ["phi", "status"]:
             g.set(f, r.get(f, k), k)
     g.set_mg(0, r.mg(0))
@@ -78,10 +101,10 @@ def _rel(a, b):
 
 
 @pytest.fixture(scope="module")
-def evolved(gpu):
+def evolved(gpu, scene):
     if not oracle_available():
         pytest.skip("oracle/_ref not built")
-    r, g, dt = _pair()
+    r, g, dt = _pair(SCENES[scene])
     r.step(dt, 30)
     yield r, g, dt
     r.close()
@@ -113,18 +136,20 @@ def test_stage_matches_reference(evolved, stage, ref_stages, tol):
         r.stage(s, dt)
     g.stage(stage, dt)
     errs = {f: _rel(g.get(f), r.get(f)) for f in FIELDS}
-    for k in range(len(OBJECTS)):
+    for k in range(g.objects):
         for f in SFIELDS + ["phi"]:
             errs[f"{f}[{k}]"] = _rel(g.get(f, k), r.get(f, k))
     bad = {f: e for f, e in errs.items() if e > tol}
     assert not bad, bad
-    for k in range(len(OBJECTS)):
+    for k in range(g.objects):
         assert np.array_equal(g.get("status", k), r.get("status", k)), k
 
 
-def test_collision_stress_active(evolved):
-    """The scenario exercises the collision term: the two circles' transition
-    zones overlap somewhere on the grid."""
+def test_collision_stress_active(evolved, scene):
+    """The first scene exercises the collision term: the two circles'
+    transition zones overlap somewhere on the grid."""
+    if scene != "circles_rod":
+        pytest.skip("the collision scene only")
     r, _, _ = evolved
     eps = r.scalars()["eps"]
     p0, p1 = r.get("phi", 0), r.get("phi", 1)
@@ -132,14 +157,14 @@ def test_collision_stress_active(evolved):
 
 
 @needs_oracle
-def test_initial_band(gpu):
+def test_initial_band(gpu, scene):
     """The bands built at initialisation agree to 0.03 dx: where the second-
     order march is not causal (a point accepted below an already accepted
     neighbour) the reference's heap order and the fixed point differ; the
     statuses agree exactly."""
-    r, g, dt = _pair()
+    r, g, dt = _pair(SCENES[scene])
     dx = 2.0 / M
-    for k in range(len(OBJECTS)):
+    for k in range(g.objects):
         assert np.abs(g.get("phi", k) - r.get("phi", k)).max() <= 0.03 * dx, k
         assert np.array_equal(g.get("status", k), r.get("status", k)), k
     r.close()
@@ -147,17 +172,17 @@ def test_initial_band(gpu):
 
 
 @needs_oracle
-def test_steps_from_initial_state(gpu):
+def test_steps_from_initial_state(gpu, scene):
     """25 whole steps from the reference's initial state (copied, so the
     initial-band difference above is excluded)."""
-    r, g, dt = _pair()
+    r, g, dt = _pair(SCENES[scene])
     _copy(r, g)
     r.step(dt, 25)
     g.step(dt, 25)
     for f, tol in [("u", 1e-6), ("v", 1e-6), ("p", 1e-6)]:
         e = _rel(g.get(f)[2:-2, 2:-2], r.get(f)[2:-2, 2:-2])
         assert e <= tol, (f, e)
-    for k in range(len(OBJECTS)):
+    for k in range(g.objects):
         for f in ["X", "Y", "phi"]:
             e = _rel(g.get(f, k)[2:-2, 2:-2], r.get(f, k)[2:-2, 2:-2])
             assert e <= 1e-8, (f, k, e)

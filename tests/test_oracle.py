@@ -124,3 +124,31 @@ def test_shim_channel_with_density_jump_converges():
                                    y_prd=bool(yp), zpr=bool(zpr))
         assert st[1] <= 1e-9
         assert st[0] <= cap, (sys_, xp, yp, zpr, st[0])
+
+
+def test_harness_ellipse_level_set():
+    """The oracle's ellipse (a harness-side obj_standard subclass; the
+    reference has none): after initialisation its band is a signed distance
+    to the rotated ellipse. Signs follow the ellipse equation, and at points
+    of the band the value matches the distance to the ellipse, measured on a
+    fine sampling of its boundary, to 0.1 dx (measured 0.07 dx, at the ends
+    of the major axis, whose radius of curvature b^2/a is about 2 dx)."""
+    _, refsim = _ops()
+    M, N, geom = 64, 96, (-1.0, 1.0, -1.5, 1.5)
+    cx, cy, a, b, th = 0.05, -0.1, 0.3, 0.14, 0.4
+    r = refsim.RefSim(M, ntrace=0, n=N, objects=[("ellipse", (cx, cy, a, b, th, 0.5), 10.0, 2.0)], geom=geom)
+    phi = r.get("phi", 0)[2:-2, 2:-2]
+    r.close()
+    dx = 2.0 / M
+    x = geom[0] + (np.arange(M) + 0.5) * dx
+    y = geom[2] + (np.arange(N) + 0.5) * (3.0 / N)
+    X, Y = np.meshgrid(x - cx, y - cy)
+    xb, yb = np.cos(th) * X + np.sin(th) * Y, -np.sin(th) * X + np.cos(th) * Y
+    inside = (xb / a) ** 2 + (yb / b) ** 2 < 1
+    t = np.linspace(0, 2 * np.pi, 20000, endpoint=False)
+    ex, ey = a * np.cos(t), b * np.sin(t)
+    band = (np.abs(phi) > 0.25 * dx) & (np.abs(phi) < 3 * dx)
+    assert band.sum() > 100
+    assert np.all((phi[band] < 0) == inside[band])
+    d = np.sqrt((xb[band][:, None] - ex[None, :]) ** 2 + (yb[band][:, None] - ey[None, :]) ** 2).min(axis=1)
+    assert np.abs(np.abs(phi[band]) - d).max() <= 0.1 * dx

@@ -9,6 +9,9 @@ namespace incrmt {
 namespace {
 
 constexpr int kNu1 = 2, kNu2 = 2, kCoarseSweeps = 64, kCoarsestSize = 16, kMaxLevels = 24;
+/** Coupling ratio beyond which only the strongly coupled direction is
+ * coarsened (semi-coarsening). */
+constexpr double kSemiRatio = 2.0;
 
 // ---------------------------------------------------------------------------
 // Transfer-operator index helpers (identical rules to the CPU oracle's shim).
@@ -1006,9 +1009,21 @@ int Multigrid::build_hierarchy() {
     INCRMT_CK(cudaMalloc(&L0.zf2, sizeof(float) * L0.N));
     lev.push_back(L0);
     int mm = m, nn = n;
+    // Semi-coarsening on anisotropic grids: r is the ratio of the operator's
+    // y coupling to its x coupling, (dx/dy)^2 on the fine level of both
+    // systems. Point Gauss-Seidel smooths only along the strong direction, so
+    // while one direction's coupling is more than twice the other's only
+    // that direction is halved, which divides (or multiplies) r by 4.
+    double r = yysp / xxsp;
     while (static_cast<int>(lev.size()) < kMaxLevels && mm * nn > kCoarsestSize) {
-        const bool kx = can_coarsen(mm, px), ky = can_coarsen(nn, py);
+        bool kx = can_coarsen(mm, px), ky = can_coarsen(nn, py);
+        if (kx && ky) {
+            if (r > kSemiRatio) kx = false;
+            else if (r < 1 / kSemiRatio) ky = false;
+        }
         if (!kx && !ky) break;
+        if (kx && !ky) r *= 4;
+        else if (ky && !kx) r /= 4;
         const int mc = kx ? (px ? mm / 2 : (mm + 1) / 2) : mm, nc = ky ? (py ? nn / 2 : (nn + 1) / 2) : nn;
         lev.back().kx = kx; lev.back().ky = ky;
         MgLevel L; L.m = mc; L.n = nc; L.N = static_cast<long>(mc) * nc;

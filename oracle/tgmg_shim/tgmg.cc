@@ -176,13 +176,39 @@ inline bool tgmg_can_coarsen(int m,bool p) {
 
 template<class S,class V,class M>
 tgmg<S,V,M>::tgmg(S &s_,V *b_,V *z_) : tgmg_base<S,V,M>(s_,b_,z_),
-    nlev(1), rf(new V[s_.mn]), last_vcycles(0), last_rel_res(0), ginv(NULL) {
+    nlev(1), rf(new V[s_.mn]), last_vcycles(0), last_rel_res(0), ginv(NULL), built(false) {
     for(int l=0;l<tgmg_max_levels;l++) pw[l]=NULL;
+}
+
+/** Builds the coarse grids on the first setup(), when the system's stencil
+ * can be read. The ratio r of the operator's y coupling to its x coupling
+ * is measured on the fine level, summed over the grid: |D|+|U| against
+ * |L|+|R|, the stencil collapsed onto its rows and columns ((dx/dy)^2 for
+ * either pressure system with uniform coefficients). While one direction's
+ * coupling exceeds the other's by more than tgmg_semi_ratio, only that
+ * direction is halved, which divides (or multiplies) r by 4. */
+template<class S,class V,class M>
+void tgmg<S,V,M>::build_levels() {
+    built=true;
     int m=this->m,n=this->n;
     bool xp=this->x_prd,yp=this->y_prd;
+    double sx=0,sy=0;
+    for(int j=0;j<n;j++) for(int i=0;i<m;i++) {
+        double a[9];
+        tgmg_stencil(this->s,m,n,xp,yp,i,j,a);
+        sx+=fabs(a[0]+a[3]+a[6])+fabs(a[2]+a[5]+a[8]);
+        sy+=fabs(a[0]+a[1]+a[2])+fabs(a[6]+a[7]+a[8]);
+    }
+    double r=sx>0?sy/sx:1;
     while(nlev<tgmg_max_levels&&m*n>tgmg_coarsest_size) {
         bool kx=tgmg_can_coarsen(m,xp),ky=tgmg_can_coarsen(n,yp);
+        if(kx&&ky) {
+            if(r>tgmg_semi_ratio) kx=false;
+            else if(r<1/tgmg_semi_ratio) ky=false;
+        }
         if(!kx&&!ky) break;
+        if(kx&&!ky) r*=4;
+        else if(ky&&!kx) r/=4;
         int mc=kx?(xp?m/2:(m+1)/2):m,nc=ky?(yp?n/2:(n+1)/2):n;
         cx[nlev-1]=kx;cy[nlev-1]=ky;
         lev[nlev]=new tgmg_level<V,M>(mc,nc,xp,yp);
@@ -255,6 +281,7 @@ void tgmg<S,V,M>::coarse_inverse() {
  * the Galerkin product P^T A P. */
 template<class S,class V,class M>
 void tgmg<S,V,M>::setup() {
+    if(!built) build_levels();
     for(int l=1;l<nlev;l++) {
         if(l==1) {
             build_p(this->s,0,this->m,this->n,this->x_prd,this->y_prd,*lev[1],cx[0],cy[0]);

@@ -14,7 +14,9 @@
  *
  * Method. Unknowns form an m x n grid with a 9-point stencil. A coarse level
  * keeps every second point of each direction that is coarsened (vertex-style:
- * coarse I sits on fine 2I; mc=(m+1)/2, or m/2 when periodic), with an
+ * coarse I sits on fine 2I; mc=(m+1)/2, or m/2 when periodic); on anisotropic
+ * grids only the strongly coupled direction is coarsened until the coupling
+ * is within a factor tgmg_semi_ratio of isotropic (semi-coarsening), with an
  * operator-dependent prolongation P (black-box multigrid weights from the
  * collapsed stencil: the bilinear 1, 1/2, 1/4 for constant coefficients,
  * following the flux across density jumps and Dirichlet edges), restriction
@@ -126,6 +128,8 @@ class tgmg : public tgmg_base<S,V,M> {
         /** Dense inverse of the coarsest operator (regularised when singular),
          * or NULL when the coarsest level is solved by sweeps. */
         double *ginv;
+        /** Whether the coarse grids exist (they are built by the first setup). */
+        bool built;
         tgmg(S &s_,V *b_,V *z_);
         ~tgmg();
         void setup();
@@ -148,6 +152,7 @@ class tgmg : public tgmg_base<S,V,M> {
         void restrict_to(V *r,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
         void prolong_add(V *zf,int l,int fm,int fn,bool fxp,bool fyp,tgmg_level<V,M> &c,bool kx,bool ky);
         void coarse_inverse();
+        void build_levels();
 };
 
 #endif

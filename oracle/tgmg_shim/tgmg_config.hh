@@ -31,6 +31,10 @@ const int tgmg_coarse_sweeps=64;
 const int tgmg_direct_max=96;
 /** Coarsening stops once a level has at most this many unknowns. */
 const int tgmg_coarsest_size=16;
+/** Semi-coarsening: while the operator's coupling along one direction is
+ * more than this many times that along the other, only the strongly coupled
+ * direction is halved (point Gauss-Seidel smooths only along it). */
+const double tgmg_semi_ratio=2.0;
 /** Maximum number of levels in a hierarchy. */
 const int tgmg_max_levels=24;
 /** Maximum number of V-cycles in one solve before reporting failure. */

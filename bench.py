@@ -1,51 +1,53 @@
 """Benchmark of incrmt_b200 on one node; prints ONE JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sspin1024|mac4096|sed1024|flag2048] [--precision fp64|mixed]
-                    [--learned]
+                    [--workload flag2048|flag3456|sed2048|sed1024|sspin1024|mac4096]
+                    [--precision fp64|mixed] [--guess previous|learned]
+                    [--coarse-refresh R] [--also W1,W2]
 
-Workload "sspin1024" (default): the ftest simple-spin scenario (three-pronged
-neo-Hookean rotor in a walled [-1,1]^2 box, ftest.cc:116-143) on a 1024 x 1024
-grid. One step = fluid_2d::step_forward (fluid_2d.cc:298-369) with the step
-size solve(2*pi,120) uses; the state starts from the scenario's own
-initialisation. Every field array is 8.4 MB (the ~60 arrays together exceed
-the 126 MB L2), and each step streams them, so no flush is added.
+The metric: steps per second of fluid_2d::step_forward (fluid_2d.cc:298-369)
+and V-cycles per projection at a 1e-9 relative residual, with the learned
+warm start and mixed precision against the plain FP64 multigrid started from
+the previous step's pressure (the reference's warm start, mgs_common.cc:15-21).
 
-Workload "mac4096": the standalone variable-density MAC pressure solve on a
-4096 x 4096 cell grid (8 seeded circles at density ratio 3, right-hand side
-from 64 seeded Gaussian velocity blobs; incrmt_b200/workloads.py). One step =
-one projection as the reference performs it: rebuild the coefficients and
-the multigrid hierarchy from the density (mgs_mac.cc:62-63), then V-cycles
-from a zero guess until ||b-Az||_2 <= 1e-9 ||b||_2. Every array is larger
-than the 126 MB L2, so no flush is needed between steps.
+Default run (N=1): workload "flag2048", the flag scenario (ftest.cc:335-378:
+y-periodic channel, uniform inflow, zero-pressure outlet, FEM projection with
+its fixed column) on the literal 2048 x 2048 grid of [-1,5]x[-1,1] (cells
+three times as wide as high), mass ratio 1, bending rigidity 0.1, Re 100,
+aspect ratio 10. Before timing, the learned warm starts of both projections
+are trained on a training run of the same workload (the flag with a
+perturbed tail) with the library's own U-Net kernels. Then, from the same
+initial state, W + K steps with the learned guess and mixed precision
+(`value`, the K timed) and W + K steps of the plain FP64 method (`plain_fp64`):
+steps/s, V-cycles per projection, the learned guess's fallback rate and the
+difference of the end fields (u, v, p, every phi) of the two runs. A second
+workload (--also, default sed2048 at N=1) repeats the comparison.
+
+Workloads: flag3456 (the isotropic 3456 x 1152 flag), sed2048 / sed1024 (32
+seeded circles and ellipses, size 0.03-0.06, density 1.5-3, G 1, gravity
+(rho_s-1)/rho_s, settling in the walled [-0.75,0.75]x[-1.5,1.5] box of the
+reference's sediment driver at 2048 x 4096 / 1024 x 2048), sspin1024 (ftest
+simple-spin at 1024 x 1024), mac4096 (the standalone variable-density MAC
+solve at 4096 x 4096: 8 seeded circles at density ratio 3, right-hand side
+from 64 seeded Gaussian velocity blobs, incrmt_b200/workloads.py; one step =
+coefficients and hierarchy rebuilt from the density, then V-cycles from zero
+to 1e-9). The simulation arrays of every workload exceed the 126 MB L2 and
+each step streams them, so no flush is added.
+
+The projections rebuild their Galerkin coarse levels on every density
+change by default (--coarse-refresh 1), as the reference's solver setup
+does (mgs_mac.cc:62-63, mgs_fem.cc:108-109); the line also reports the
+lagged rebuild (every 16 projections) of the timed configuration.
 
 The timed region is bracketed by cudaProfilerStart/Stop, so
 `ncu --profile-from-start off` lists exactly the timed launches.
 
-Workload "sed1024": the sediment configuration, 32 seeded bodies
-(alternately circles and ellipses, size 0.03-0.06, density 1.5-3, G 1,
-gravity (rho_s-1)/rho_s) settling in the walled [-0.75,0.75]x[-1.5,1.5] box of
-the reference's sediment driver on a 1024 x 2048 grid; one step =
-fluid_2d::step_forward. The reference arm runs the same bodies with each
-ellipse replaced by a rounded rod, the reference having no ellipse.
-
-Workload "flag2048": the flag scenario (ftest.cc:335-378; y-periodic channel,
-uniform inflow, zero-pressure outlet, FEM projection with its fixed column) on
-3456 x 1152 square cells of [-1,5]x[-1,1] (about 2048^2 cells), mass ratio 1,
-bending rigidity 0.1, Re 100, aspect ratio 10.
-
---learned (mac4096): before timing, the learned initial guess is trained on
-128 GPU-generated problems of the same kind (other seeds) with the library's
-own U-Net kernels; every timed solve then starts from the network's guess
-instead of zero. The line adds the training summary and plain FP64 solves of
-the same problem for comparison.
-
 Multi-GPU: the path does not shard; N ranks run N independent replicas
 (weak scaling), timed on the device as the maximum over ranks.
 
---impl reference times the reference's own CPU code on the same workload:
-the reference's mgs_mac_varying_rho callbacks driven by the clean-room TGMG
-shim (oracle/_ref), with all host threads.
+--impl reference times the reference's own CPU code (oracle/_ref: the
+reference's sources built with the clean-room TGMG shim) on the same
+workload with all host threads, a bounded number of steps.
 """
 import argparse
 import faulthandler
@@ -186,6 +188,84 @@ def _barrier(dist):
 
 
 # ---------------------------------------------------------------------------
+# Workloads
+
+SED_BOX = (-0.75, 0.75, -1.5, 1.5)
+FLAG_BOX = (-1.0, 5.0, -1.0, 1.0)
+# flag scenario constants (none fixed by the reference for these grids):
+# mass ratio 1, bending rigidity 0.1, Re 100, aspect ratio 10
+FLAG_MU, FLAG_KB, FLAG_RE, FLAG_AR = 1.0, 0.1, 100.0, 10.0
+SIM_WORKLOADS = {
+    "flag2048": ("flag", 2048, 2048),
+    "flag3456": ("flag", 3456, 1152),
+    "sed2048": ("sed", 2048, 4096),
+    "sed1024": ("sed", 1024, 2048),
+    "sspin1024": ("sspin", 1024, 1024),
+}
+
+
+def describe(workload):
+    kind, m, n = SIM_WORKLOADS[workload]
+    if kind == "flag":
+        return (f"flag {m}x{n} on [-1,5]x[-1,1] (mu {FLAG_MU:g}, k_B {FLAG_KB:g}, Re {FLAG_RE:g}, ar {FLAG_AR:g}), "
+                f"FEM with zero-pressure outlet, y-periodic; fluid_2d::step_forward, dt of 900 frames over T=30")
+    if kind == "sed":
+        return (f"sediment {m}x{n}: 32 seeded circles and ellipses (r 0.03-0.06, rho 1.5-3, G 1) settling, "
+                f"fluid_2d::step_forward, dt of 0.1 frames")
+    return f"simple-spin {m}x{n} fluid_2d::step_forward, dt of solve(2pi,120)"
+
+
+def frame_interval(workload):
+    kind = SIM_WORKLOADS[workload][0]
+    return {"flag": 30.0 / 900, "sed": 0.1, "sspin": 2 * np.pi / 120}[kind]
+
+
+def _flag_params(training):
+    w = 1.0 / FLAG_AR
+    # the training run's tail is perturbed (ftest's optional perturb_v), a
+    # different trajectory
+    return (0.0, 0.0, 1.0, w, 0.25 * w, 0.2 if training else 0.0, 17), 4 * FLAG_KB / w ** 3, FLAG_MU / w
+
+
+def make_sim(workload, rank, prec, training=False):
+    """The GPU simulation of a workload (capi.Simulation), initialised."""
+    from incrmt_b200 import capi, workloads
+    kind, m, n = SIM_WORKLOADS[workload]
+    if kind == "sspin":
+        sim = capi.Simulation(m, n, ntrace=512, precision=prec)
+        sim.add_simple_spin()
+        sim.initialize()
+        rng = np.random.default_rng(1 + rank)
+        sim.set_tracers(rng.uniform(-1, 1, size=(512, 2)))
+        return sim
+    if kind == "flag":
+        (cx, cy, fl, fw, fa, pv, nt), G, rhos = _flag_params(training)
+        ax, bx, ay, by = FLAG_BOX
+        sim = capi.Simulation(m, n, ax=ax, bx=bx, ay=ay, by=by, visc=1.0 / FLAG_RE, ntrace=0,
+                              precision=prec, y_prd=True, horiz_flow=1.0)
+        sim.add_flag(cx, cy, fl, fw, fa, G, rhos, perturb_v=pv, ntrace=nt)
+        sim.initialize()
+        return sim
+    ax, bx, ay, by = SED_BOX
+    sim = capi.Simulation(m, n, ax=ax, bx=bx, ay=ay, by=by, visc=2e-3, ntrace=512, precision=prec)
+    for o in workloads.sediment_bodies(seed=(1011 if training else 11) + rank):
+        if o["kind"] == "circle":
+            sim.add_circle(o["cx"], o["cy"], o["r"], 1.0, o["rhos"], grav=o["grav"])
+        else:
+            sim.add_ellipse(o["cx"], o["cy"], o["r"], o["b"], o["theta"], 1.0, o["rhos"], grav=o["grav"])
+    sim.initialize()
+    rng = np.random.default_rng(1 + rank)
+    sim.set_tracers(np.stack([rng.uniform(ax, bx, 512), rng.uniform(ay, by, 512)], axis=1))
+    return sim
+
+
+def frame_dt(dt_reg, interval):
+    """fluid_2d::solve's step: the frame interval split into equal steps no
+    longer than dt_reg (fluid_2d.cc:266-270)."""
+    return interval / (int(interval / dt_reg) + 1)
+
+
+# ---------------------------------------------------------------------------
 # CPU reference (the reference's own code, oracle/_ref)
 
 def cpu_reference_mac(m, steps, warmup, seed=3):
@@ -233,40 +313,38 @@ def _sed_reference_objects(seed=11):
     return objs
 
 
-def cpu_reference_sed(steps, warmup):
-    """The reference's own step on the sediment workload (oracle/_ref)."""
+def cpu_reference_sim(workload, steps, warmup):
+    """The reference's own step on a simulation workload (oracle/_ref), with
+    the projections' V-cycles per projection. Returns (steps/s, seconds,
+    V-cycles per projection, threads)."""
     from oracle import refsim
+    kind, m, n = SIM_WORKLOADS[workload]
+    if kind == "sspin":
+        return cpu_reference_sspin(m, steps, warmup)
     if not refsim.available():
         refsim.build()
-    r = refsim.RefSim(SED_M, ntrace=512, n=2 * SED_M, objects=_sed_reference_objects(), geom=SED_BOX, visc=2e-3)
-    dt_reg = r.scalars()["dt_reg"]
-    dt = 0.1 / (int(0.1 / dt_reg) + 1)
+    if kind == "flag":
+        p, G, rhos = _flag_params(False)
+        r = refsim.RefSim(m, ntrace=0, n=n, objects=[("flag", p, G, rhos)], geom=FLAG_BOX, visc=1.0 / FLAG_RE,
+                          flow_u=1.0)
+    else:
+        r = refsim.RefSim(m, ntrace=512, n=n, objects=_sed_reference_objects(), geom=SED_BOX, visc=2e-3)
+    dt = frame_dt(r.scalars()["dt_reg"], frame_interval(workload))
     r.step(dt, warmup)
+    r.vcycles(0)  # the counters restart (ref_vcycles reads and resets them)
+    r.vcycles(1)
     t0 = time.perf_counter()
     r.step(dt, steps)
     secs = time.perf_counter() - t0
+    vc = (r.vcycles(0) + r.vcycles(1)) / (2.0 * steps)
     r.close()
-    return steps / secs, secs, None, int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return steps / secs, secs, vc, int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
 
 
-def cpu_reference_flag(steps, warmup):
-    """The reference's own step on the flag workload (oracle/_ref)."""
-    from oracle import refsim
-    if not refsim.available():
-        refsim.build()
-    w = 0.1
-    flag = ("flag", (0.0, 0.0, 1.0, w, 0.25 * w, 0.0, 17), 4 * 0.1 / w ** 3, 1.0 / w)
-    r = refsim.RefSim(3 * FLAG_N, ntrace=0, n=FLAG_N, objects=[flag], geom=(-1.0, 5.0, -1.0, 1.0), visc=0.01,
-                      flow_u=1.0)
-    dt_reg = r.scalars()["dt_reg"]
-    iv = 30.0 / 900
-    dt = iv / (int(iv / dt_reg) + 1)
-    r.step(dt, warmup)
-    t0 = time.perf_counter()
-    r.step(dt, steps)
-    secs = time.perf_counter() - t0
-    r.close()
-    return steps / secs, secs, None, int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+def cpu_steps(workload):
+    """A bounded sample for the CPU reference: a few seconds to a minute."""
+    kind, m, n = SIM_WORKLOADS[workload]
+    return {"sspin": 40, "flag": 2, "sed": 2}[kind] if m * n > 2e6 else 40
 
 
 def run_reference(args, ws, rank):
@@ -274,48 +352,26 @@ def run_reference(args, ws, rank):
         return
     threads = os.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    if args.workload in ("sed1024", "flag2048"):
-        nref = max(1, min(args.steps, 3))
+    if args.workload in SIM_WORKLOADS:
+        nref = max(1, min(args.steps, cpu_steps(args.workload)))
+        nwarm = min(args.warmup, 1 if nref < 10 else 2)
         try:
-            fn = cpu_reference_sed if args.workload == "sed1024" else cpu_reference_flag
-            sps, dt, _, thr = fn(nref, min(args.warmup, 1))
+            sps, dt, vc, thr = cpu_reference_sim(args.workload, nref, nwarm)
         except Exception as e:
             print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"}))
             return
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s",
-            "n_gpus": args.gpus, "steps": nref, "warmup": min(args.warmup, 1),
+            "n_gpus": args.gpus, "steps": nref, "warmup": nwarm,
             "ms_per_step": 1e3 * dt / nref, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": (f"sediment {SED_M}x{2 * SED_M}, 32 bodies, ellipses as rounded rods"
-                                    if args.workload == "sed1024" else
-                                    f"flag {3 * FLAG_N}x{FLAG_N} (mu 1, k_B 0.1, Re 100, ar 10)"),
-                       "flush": "working set larger than L2"},
-            "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
-                             "sample": f"{nref} steps (a step takes seconds on the host)"},
-            "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
-        return
-    if args.workload == "sspin1024":
-        m = 1024
-        try:
-            sps, dt, vc, thr = cpu_reference_sspin(m, args.steps, args.warmup)
-        except Exception as e:
-            print(json.dumps({"impl": "reference", "unavailable": f"reference build/run failed: {e}"}))
-            return
-        line = {
-            "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * dt / max(args.steps, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"simple-spin {m}x{m} fluid_2d::step_forward, dt of solve(2pi,120)",
-                       "flush": "working set larger than L2"},
+            "config": {"workload": describe(args.workload), "flush": "working set larger than L2",
+                       "coarse_refresh": 1},
             "vcycles_per_projection": vc,
             "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
-                             "sample": f"{args.steps} steps after {args.warmup} warm-up steps at {m}x{m}, "
-                                       f"reference sources + TGMG-API shim, OMP threads = {thr}"},
-            "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
-        print(json.dumps(line))
+                             "sample": f"{nref} steps after {nwarm} warm-up steps (reference sources + TGMG-API "
+                                       f"shim, Galerkin setup on every projection), OMP threads = {thr}"},
+            "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     m = 4096
     # A 4096^2 solve takes seconds on the host: time at most 8 of them.
@@ -341,71 +397,15 @@ def run_reference(args, ws, rank):
 
 
 # ---------------------------------------------------------------------------
-# GPU path
-
-SED_M = 1024
-SED_BOX = (-0.75, 0.75, -1.5, 1.5)
-FLAG_N = 1152
-
-
-def _make_sim(workload, rank, prec, training=False):
-    """The simulation of a step workload and its frame interval:
-    sspin1024 (ftest simple-spin, solve(2pi,120) frames) or sed1024 (32
-    seeded circles and ellipses settling in the sediment box at 1024 x 2048,
-    frame interval 0.1 as sediment.cc's 1600 frames over T=160)."""
-    from incrmt_b200 import capi, workloads
-    if workload == "sspin1024":
-        m = 1024
-        sim = capi.Simulation(m, m, ntrace=512, precision=prec)
-        sim.add_simple_spin()
-        sim.initialize()
-        rng = np.random.default_rng(1 + rank)
-        sim.set_tracers(rng.uniform(-1, 1, size=(512, 2)))
-        return sim, 2 * np.pi / 120, f"simple-spin {m}x{m} fluid_2d::step_forward, dt of solve(2pi,120)"
-    if workload == "flag2048":
-        # The flag scenario (ftest.cc:335-378) on 3456 x 1152 square cells of
-        # [-1,5]x[-1,1] (about 2048^2 cells; 1152 = 9 x 2^7 lets the periodic
-        # direction halve seven times); mass ratio 1, bending rigidity 0.1,
-        # Re 100, aspect ratio 10.
-        n = FLAG_N
-        m = 3 * n
-        mu, k_B, Re, ar = 1.0, 0.1, 100.0, 10.0
-        w = 1.0 / ar
-        sim = capi.Simulation(m, n, ax=-1.0, bx=5.0, ay=-1.0, by=1.0, visc=1.0 / Re, ntrace=0,
-                              precision=prec, y_prd=True, horiz_flow=1.0)
-        # the learned warm start trains on a run whose tail is perturbed
-        # (ftest's optional perturb_v), a different trajectory
-        sim.add_flag(0.0, 0.0, 1.0, w, 0.25 * w, 4 * k_B / w ** 3, mu / w, perturb_v=0.2 if training else 0.0,
-                     ntrace=17)
-        sim.initialize()
-        return sim, 30.0 / 900, (f"flag {m}x{n} on [-1,5]x[-1,1] (mu 1, k_B 0.1, Re 100, ar 10), FEM with "
-                                 f"zero-pressure outlet, y-periodic; fluid_2d::step_forward, dt of 900 frames over T=30")
-    m, n = SED_M, 2 * SED_M
-    ax, bx, ay, by = SED_BOX
-    sim = capi.Simulation(m, n, ax=ax, bx=bx, ay=ay, by=by, visc=2e-3, ntrace=512, precision=prec)
-    for o in workloads.sediment_bodies(seed=(1011 if training else 11) + rank):
-        if o["kind"] == "circle":
-            sim.add_circle(o["cx"], o["cy"], o["r"], 1.0, o["rhos"], grav=o["grav"])
-        else:
-            sim.add_ellipse(o["cx"], o["cy"], o["r"], o["b"], o["theta"], 1.0, o["rhos"], grav=o["grav"])
-    sim.initialize()
-    rng = np.random.default_rng(1 + rank)
-    sim.set_tracers(np.stack([rng.uniform(ax, bx, 512), rng.uniform(ay, by, 512)], axis=1))
-    return sim, 0.1, (f"sediment {m}x{n}: 32 seeded circles and ellipses (r 0.03-0.06, rho 1.5-3, G 1) "
-                      f"settling, fluid_2d::step_forward, dt of 0.1 frames")
-
+# GPU path: simulation workloads
 
 LEARNED_SIM_FACTOR = 8     # network grid: the projection's unknowns restricted by 8
 LEARNED_SIM_SAMPLES = 200  # projections captured per system from the training run
 LEARNED_SIM_STEPS = 1500   # Adam steps per network
+LEARNED_SIM_BASE = 16      # channels at the finest level of the U-Net
 
 
-def _frame_dt(sim, interval):
-    l = int(interval / sim.dt_reg) + 1
-    return interval / l
-
-
-def _train_learned_sim(workload, rank, dev):
+def train_learned_sim(workload, rank, dev):
     """The learned warm start of the MAC and FEM projections, trained with
     this library's own U-Net kernels on samples the method generates: a
     training run of the workload (another seed; for the flag a perturbed
@@ -413,8 +413,8 @@ def _train_learned_sim(workload, rank, dev):
     import torch
     from incrmt_b200 import capi, learned
     t0 = time.perf_counter()
-    sim, interval, _ = _make_sim(workload, rank, capi.PREC_FP64, training=True)
-    dt = _frame_dt(sim, interval)
+    sim = make_sim(workload, rank, capi.PREC_FP64, training=True)
+    dt = frame_dt(sim.dt_reg, frame_interval(workload))
     sim.step(dt, 10)
     data = learned.capture(sim, LEARNED_SIM_FACTOR, LEARNED_SIM_SAMPLES, dt, dev)
     sim.close()
@@ -423,45 +423,185 @@ def _train_learned_sim(workload, rank, dev):
     t1 = time.perf_counter()
     for sys, (X, T) in data.items():
         Xn, Tn, V = learned.normalise(X, T)
-        net = capi.UNet(4, 16, seed=11 + sys)
-        losses["mac" if sys == capi.SYS_MAC else "fem"] = learned.train(net, Xn, Tn, V, LEARNED_SIM_STEPS,
-                                                                       seed=rank)
+        net = capi.UNet(4, LEARNED_SIM_BASE, seed=11 + sys)
+        losses["mac" if sys == capi.SYS_MAC else "fem"] = learned.train(net, Xn, Tn, V, LEARNED_SIM_STEPS, seed=rank)
         nets[sys] = net
     torch.cuda.synchronize()
     H, W = data[capi.SYS_MAC][0].shape[1:3]
-    info = {"network": f"two U-Nets (MAC, FEM), 4 levels, base 16 channels, {nets[0].num_params()} parameters "
-                       f"each, BF16 activations, mma.sync tensor-core convolutions",
+    info = {"network": f"two U-Nets (MAC, FEM), 4 levels, base {LEARNED_SIM_BASE} channels, "
+                       f"{nets[0].num_params()} parameters each, BF16 activations",
             "grid": f"{H}x{W} (projection restricted by {LEARNED_SIM_FACTOR})",
             "train_samples_per_system": LEARNED_SIM_SAMPLES, "train_steps": LEARNED_SIM_STEPS, "batch": 8,
             "final_loss": losses, "data_seconds": t_data, "train_seconds": time.perf_counter() - t1}
     return nets, info
 
 
-def _plain_fp64_rate(workload, rank, steps, warmup, dev, coarse_refresh=1):
-    """Steps/s and V-cycles per projection of the plain FP64 method on the
-    same workload (the comparison of the learned + mixed line)."""
+SNAP_FIELDS = ("u", "v", "p")
+
+
+def _snapshot(sim):
+    """End fields of a run: u, v, p and every object's level set (interior)."""
+    d = {f: sim.get(f)[2:-2, 2:-2].copy() for f in SNAP_FIELDS}
+    for k in range(sim.objects):
+        d[f"phi{k}"] = sim.get("phi", k)[2:-2, 2:-2].copy()
+    return d
+
+
+def _snap_errors(a, b):
+    """Largest difference of each field relative to the FP64 run's largest
+    magnitude (u, v, p) or to its grid spacing h (the level sets: max over
+    the objects, in units of h)."""
+    out = {}
+    for f in SNAP_FIELDS:
+        out[f] = float(np.abs(a[f] - b[f]).max() / max(np.abs(b[f]).max(), 1e-300))
+    phis = [k for k in b if k.startswith("phi")]
+    if phis:
+        out["phi_max_over_objects"] = max(float(np.abs(a[k] - b[k]).max()) for k in phis)
+    return out
+
+
+def _vcycles(st0, st1, steps):
+    return ((st1.vcycles_mac - st0.vcycles_mac) / max(1, st1.solves_mac - st0.solves_mac),
+            (st1.vcycles_fem - st0.vcycles_fem) / max(1, st1.solves_fem - st0.solves_fem))
+
+
+def projection_roofline(sim, workload, prec, vc_mac, vc_fem, phases):
+    """V-cycle-level roofline of the two projections: the algorithmic bytes
+    of the V-cycles they ran, (4/3) N w [(nu1+nu2+1)(3+c) + 3.5] per V-cycle
+    (w = 8 FP64; in mixed precision w = 4 for the FP32 cycle plus the FP64
+    outer residual and update, 68 B MAC / 60 B FEM per unknown), over the
+    device time of the mac and fem phases."""
+    peak, peak_kind = _peaks()
+    kind, m, n = SIM_WORKLOADS[workload]
+    nm, nf = m * n, (m + 1) * (n if kind == "flag" else n + 1)
+    if prec == 0:
+        bm, bf = 304.0, 251.0
+    else:
+        bm, bf = 152.0 + 68.0, 125.0 + 60.0
+    bytes_ = vc_mac * nm * bm + vc_fem * nf * bf
+    ms = phases.get("mac", 0.0) + phases.get("fem", 0.0)
+    if ms <= 0:
+        return None
+    achieved = bytes_ / (ms / 1e3) / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_step": bytes_, "ms_per_step": ms,
+            "bytes_rule": "V-cycles x (4/3) N w [(nu1+nu2+1)(3+c)+3.5], nu1=nu2=2; c=2 MAC, 1 FEM; "
+                          "mixed: w=4 plus 68/60 B per unknown of FP64 outer residual and update"}
+
+
+def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist, clocks=None, extras=True,
+            e2e_steps=0, learned_rule=0):
+    """One run of a simulation workload: warm-up, K timed steps (CUDA events
+    on the simulation stream, max over ranks), end snapshot, then (extras)
+    the phase breakdown and the live smoother roofline over further steps
+    and (e2e_steps) the end-to-end rate through the C ABI with one frame of
+    fields copied to host. Returns a dict."""
     import torch
     from incrmt_b200 import capi
-    sim, interval, _ = _make_sim(workload, rank, capi.PREC_FP64)
+    sim = make_sim(workload, rank, prec)
     sim.set_coarse_refresh(coarse_refresh)
-    dt = _frame_dt(sim, interval)
+    dt = frame_dt(sim.dt_reg, frame_interval(workload))
+    if nets is not None:
+        for sys, net in nets.items():
+            sim.set_learned(sys, net, LEARNED_SIM_FACTOR, learned_rule)
     ext = torch.cuda.ExternalStream(sim.stream(), device=dev)
     sim.step(dt, warmup)
     torch.cuda.synchronize()
+    _barrier(dist)
+    torch.cuda.synchronize()
     st0 = sim.stats()
+    nl0 = sum(n.launches() for n in nets.values()) if nets else 0
+    lst0 = {s: sim.learned_stats(s) for s in nets} if nets else {}
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    sim.step(dt, steps)
-    e1.record(ext)
-    torch.cuda.synchronize()
+    with (clocks if clocks is not None else _NullCtx()):
+        torch.cuda.cudart().cudaProfilerStart()
+        e0.record(ext)
+        sim.step(dt, steps)
+        e1.record(ext)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1))
     st1 = sim.stats()
+    out = {"ms": ms, "steps_per_s": steps / (ms / 1e3), "dt": dt}
+    out["vc_mac"], out["vc_fem"] = _vcycles(st0, st1, steps)
+    out["launches"] = int(st1.launches - st0.launches) + \
+        ((sum(n.launches() for n in nets.values()) - nl0) if nets else 0)
+    out["coarse_builds_per_step"] = (st1.coarse_builds - st0.coarse_builds) / steps
+    out["coarse_retries"] = int(st1.coarse_retries - st0.coarse_retries)
+    out["mixed_fallbacks"] = int(st1.mixed_fallbacks - st0.mixed_fallbacks)
+    out["march_sweeps_per_step"] = (st1.march_sweeps - st0.march_sweeps) / steps
+    out["extrap_sweeps_per_step"] = (st1.extrap_sweeps - st0.extrap_sweeps) / steps
+    if nets:
+        lst1 = {s: sim.learned_stats(s) for s in nets}
+        nm = lambda s: "mac" if s == capi.SYS_MAC else "fem"  # noqa: E731
+        out["learned"] = {nm(s): {"applied": int(lst1[s].applied - lst0[s].applied),
+                                  "fallback": int(lst1[s].fallback - lst0[s].fallback)} for s in nets}
+        for v in out["learned"].values():
+            v["fallback_rate"] = v["fallback"] / max(1, v["applied"] + v["fallback"])
+    out["snapshot"] = _snapshot(sim)
+    if extras:
+        n_extra = min(steps, 10)
+        sim.set_profiling(True)
+        sim.step(dt, n_extra)
+        out["phases"] = {k: v / n_extra for k, v in sim.profile().items()}
+        sim.set_profiling(False, smoothers=True)
+        sim.step(dt, n_extra)
+        sm = [0.0, 0.0, 0]
+        for which in (capi.SYS_MAC, capi.SYS_FEM):
+            a, b, c = sim.smoother_profile(which)
+            sm = [sm[0] + a, sm[1] + b, sm[2] + c]
+        out["smoother"] = sm
+        sim.set_profiling(False)
+    if e2e_steps:
+        # End to end through the C ABI as fluid_2d::solve drives it: the
+        # steps of one frame, then the frame's fields copied to host buffers
+        # (p, u, v for the vorticity, X, Y, phi; fluid_2d::write_files,
+        # fluid_2d_io.cc:60-102).
+        _barrier(dist)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.step(dt, e2e_steps)
+        host = [sim.get(f) for f in ("p", "u", "v", "X", "Y", "phi")]
+        secs = _max_over_ranks(dist, time.perf_counter() - t0)
+        out["e2e_steps_per_s"] = e2e_steps / secs
+        out["e2e_d2h_bytes_per_step"] = int(sum(h.nbytes for h in host) / e2e_steps)
+    out["objects"], out["cells"] = sim.objects, (sim.m + 4) * (sim.n + 4)
     sim.close()
-    vc = ((st1.vcycles_mac - st0.vcycles_mac) + (st1.vcycles_fem - st0.vcycles_fem)) / (2.0 * steps)
-    return steps / (e0.elapsed_time(e1) / 1e3), vc
+    return out
 
 
-def run_ours_sspin(args, ws, rank, local, dist):
+class _NullCtx:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def compare_workload(workload, args, ws, rank, dev, dist, clocks=None, extras=True, e2e=True):
+    """The metric on one workload: the timed configuration (learned guess
+    and/or mixed precision) against the plain FP64 method, same steps from
+    the same initial state. Returns (timed run, plain run, learned info)."""
+    from incrmt_b200 import capi
+    prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    nets, info = (None, None)
+    if args.guess == "learned":
+        nets, info = train_learned_sim(workload, rank, dev)
+    a = sim_run(workload, rank, dev, prec, nets, args.steps, args.warmup, args.coarse_refresh, dist, clocks=clocks,
+                extras=extras, e2e_steps=args.steps if e2e else 0, learned_rule=args.learned_rule)
+    plain = None
+    if nets is not None or prec != capi.PREC_FP64:
+        plain = sim_run(workload, rank, dev, capi.PREC_FP64, None, args.steps, args.warmup, args.coarse_refresh,
+                        dist, extras=extras)
+        a["errors_vs_fp64"] = _snap_errors(a["snapshot"], plain["snapshot"])
+    if nets is not None:
+        for net in nets.values():
+            net.close()
+    return a, plain, info
+
+
+def run_ours_sim(args, ws, rank, local, dist):
     """Simulation steps on the GPU through the simulation C ABI."""
     import torch
     from incrmt_b200 import capi
@@ -469,138 +609,88 @@ def run_ours_sspin(args, ws, rank, local, dist):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
-    nets, learned_info = None, None
-    if args.learned:
-        if args.workload not in ("sed1024", "flag2048"):
-            raise SystemExit("--learned: the simulation workloads with a learned warm start are sed1024, flag2048")
-        nets, learned_info = _train_learned_sim(args.workload, rank, dev)
-    sim, interval, wl = _make_sim(args.workload, rank, prec)
-    sim.set_coarse_refresh(args.coarse_refresh)
-    dt = _frame_dt(sim, interval)
-    if nets is not None:
-        for sys, net in nets.items():
-            sim.set_learned(sys, net, LEARNED_SIM_FACTOR, args.learned_rule)
-    ext = torch.cuda.ExternalStream(sim.stream(), device=dev)
-    sim.step(dt, args.warmup)
-    torch.cuda.synchronize()
-    _barrier(dist)
-    torch.cuda.synchronize()
-    st0 = sim.stats()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        torch.cuda.cudart().cudaProfilerStart()
-        e0.record(ext)
-        sim.step(dt, args.steps)
-        e1.record(ext)
-        torch.cuda.synchronize()
-        torch.cuda.cudart().cudaProfilerStop()
-    ms = e0.elapsed_time(e1)
-    st1 = sim.stats()
-    _barrier(dist)
-    torch.cuda.synchronize()
-    ms_max = _max_over_ranks(dist, ms)
-    value = ws * args.steps / (ms_max / 1e3)
-    vc = ((st1.vcycles_mac - st0.vcycles_mac) + (st1.vcycles_fem - st0.vcycles_fem)) / (2.0 * args.steps)
-
-    # Phase breakdown of a few extra steps, timed by CUDA events on the stream
-    # (outside the timed region).
-    sim.set_profiling(True)
-    sim.step(dt, min(args.steps, 10))
-    phases = {k: v / min(args.steps, 10) for k, v in sim.profile().items()}
-    # Roofline of the projections' fine-level smoothing (the HBM-bound kernel
-    # with the largest time share): every launch bracketed by CUDA events on
-    # the simulation stream over a few more steps.
-    sim.set_profiling(False, smoothers=True)
-    sim.step(dt, min(args.steps, 10))
-    sm_ms, sm_bytes, sm_launch = 0.0, 0.0, 0
-    for which in (capi.SYS_MAC, capi.SYS_FEM):
-        a, b, c = sim.smoother_profile(which)
-        sm_ms, sm_bytes, sm_launch = sm_ms + a, sm_bytes + b, sm_launch + c
-    sim.set_profiling(False)
-
-    # End to end through the C ABI as fluid_2d::solve drives it: the steps of
-    # one frame, then the frame's fields copied to host buffers (p, u, v for
-    # the vorticity, X, Y, phi; fluid_2d::write_files, fluid_2d_io.cc:60-102).
-    frame_fields = ["p", "u", "v", "X", "Y", "phi"]
-    _barrier(dist)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    sim.step(dt, args.steps)
-    host = [sim.get(f) for f in frame_fields]
-    e2e_s = time.perf_counter() - t0
-    e2e_s = _max_over_ranks(dist, e2e_s)
-    e2e = ws * args.steps / e2e_s
-    d2h = sum(h.nbytes for h in host)
-
-    if nets is not None:
-        lst = {("mac" if s == capi.SYS_MAC else "fem"): sim.learned_stats(s) for s in nets}
-        sim.close()
-        for net in nets.values():
-            net.close()
-        plain_sps, plain_vc = _plain_fp64_rate(args.workload, rank, args.steps, args.warmup, dev, args.coarse_refresh)
-        learned_info.update({
-            "rule": "fall back to the previous solution when the guess raises the residual" if args.learned_rule == 0
-                    else "fall back only when the energy-optimal step is not positive",
-            "applied": {k: v.applied for k, v in lst.items()},
-            "fallback": {k: v.fallback for k, v in lst.items()},
-            "fallback_rate": {k: v.fallback / max(1, v.applied + v.fallback) for k, v in lst.items()},
-            "plain_fp64_steps_per_s": plain_sps, "plain_fp64_vcycles_per_projection": plain_vc,
-            "speedup_vs_plain_fp64": value / ws / plain_sps})
+        a, plain, info = compare_workload(args.workload, args, ws, rank, dev, dist, clocks=None)
+    # the clock record covers the whole comparison (the timed steps are a
+    # few percent of it; the sampler runs throughout)
+    clocks = clk.summary()
+    value = ws * a["steps_per_s"]
+    also = {}
+    for w in [x for x in args.also.split(",") if x] if ws == 1 else []:
+        if w == args.workload or w not in SIM_WORKLOADS:
+            continue
+        b, bplain, binfo = compare_workload(w, args, ws, rank, dev, dist, extras=False, e2e=False)
+        also[w] = {"workload": describe(w), "steps_per_s": b["steps_per_s"],
+                   "vcycles_per_projection": {"mac": b["vc_mac"], "fem": b["vc_fem"]},
+                   "mixed_fallbacks": b["mixed_fallbacks"]}
+        if bplain is not None:
+            also[w]["plain_fp64"] = {"steps_per_s": bplain["steps_per_s"],
+                                     "vcycles_per_projection": {"mac": bplain["vc_mac"], "fem": bplain["vc_fem"]}}
+            also[w]["speedup_vs_plain_fp64"] = b["steps_per_s"] / bplain["steps_per_s"]
+            also[w]["errors_vs_fp64"] = b["errors_vs_fp64"]
+        if "learned" in b:
+            also[w]["learned"] = b["learned"]
     if rank != 0:
-        sim.close()
         return
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
         try:
-            if args.workload == "sspin1024":
-                sps, dts, vcr, thr = cpu_reference_sspin(1024, 40, 2)
-                sample = (f"40 steps after 2 warm-up steps at 1024x1024 (reference sources + "
-                          f"TGMG-API shim), OMP threads = {thr}")
-            elif args.workload == "flag2048":
-                sps, dts, vcr, thr = cpu_reference_flag(2, 0)
-                sample = f"2 steps of the flag workload (reference sources + TGMG-API shim), OMP threads = {thr}"
-            else:
-                sps, dts, vcr, thr = cpu_reference_sed(2, 0)
-                sample = (f"2 steps of the sediment workload with each ellipse replaced by a "
-                          f"rounded rod (the reference has no ellipse), OMP threads = {thr}")
-            cpu = {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference", "sample": sample}
+            n = cpu_steps(args.workload)
+            w_ = 2 if n >= 10 else 0
+            sps, dts, vcr, thr = cpu_reference_sim(args.workload, n, w_)
+            cpu = {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
+                   "sample": f"{n} steps after {w_} warm-up of the same workload (reference sources + "
+                             f"TGMG-API shim, {vcr:.2f} V-cycles per projection), OMP threads = {thr}"}
         except Exception as e:
             cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
+    sm_ms, sm_bytes, sm_launch = a["smoother"]
+    roof = _roofline(f"{args.workload}_smooth", sm_ms, sm_bytes, sm_launch,
+                     "k_smooth_rb / k_smooth_tile on the fine level of the MAC and FEM projections "
+                     "(two Gauss-Seidel sweeps per launch)",
+                     "updated unknowns x 2 sweeps x (3+c) x w; c=2 MAC, 1 FEM")
+    if roof is not None:
+        roof["projection"] = projection_roofline(None, args.workload, prec, a["vc_mac"], a["vc_fem"], a["phases"])
+        if plain is not None and "phases" in plain:
+            roof["projection_plain_fp64"] = projection_roofline(None, args.workload, capi.PREC_FP64, plain["vc_mac"],
+                                                                plain["vc_fem"], plain["phases"])
+    guess = "learned warm start on the previous solution" if args.guess == "learned" else "previous solution"
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": a["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == capi.PREC_FP64 else "f64 state, f32 V-cycles in f64 defect correction",
         "data": "synthetic",
-        "config": {"workload": wl, "precision": args.precision, "flush": "working set larger than L2",
-                   "parallelism": f"replicas x{ws}", "coarse_refresh": args.coarse_refresh},
-        "vcycles_per_projection": vc,
-        "coarse_builds_per_step": (st1.coarse_builds - st0.coarse_builds) / args.steps,
-        "phase_ms_per_step": phases,
-        "march_sweeps_per_step": (st1.march_sweeps - st0.march_sweeps) / args.steps,
-        "march_monotone_rebuilds": int(st1.march_monotone - st0.march_monotone),
-        "extrap_sweeps_per_step": (st1.extrap_sweeps - st0.extrap_sweeps) / args.steps,
-        # level-set points in the objects' rebuild windows over all objects' full grids
-        "window_fraction": st1.window_points / max(1, sim.objects * (sim.m + 4) * (sim.n + 4)),
-        "roofline": _roofline(f"{args.workload}_smooth", sm_ms, sm_bytes, sm_launch,
-                              "k_smooth_rb / k_smooth_tile on the fine level of the MAC and FEM projections "
-                              "(two Gauss-Seidel sweeps per launch)",
-                              "updated unknowns x 2 sweeps x (3+c) x 8 B; c=2 MAC, 1 FEM"),
+        "config": {"workload": describe(args.workload), "precision": args.precision, "initial_guess": guess,
+                   "flush": "working set larger than L2", "parallelism": f"replicas x{ws}",
+                   "coarse_refresh": args.coarse_refresh},
+        "vcycles_per_projection": {"mac": a["vc_mac"], "fem": a["vc_fem"]},
+        "mixed_fallbacks": a["mixed_fallbacks"],
+        "coarse_builds_per_step": a["coarse_builds_per_step"],
+        "phase_ms_per_step": a["phases"],
+        "march_sweeps_per_step": a["march_sweeps_per_step"],
+        "extrap_sweeps_per_step": a["extrap_sweeps_per_step"],
+        "roofline": roof,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": int(d2h / args.steps),
-                "note": "one frame of fields (p,u,v,X,Y,phi) copied to host per timed run"},
-        "gpu_launches": int(st1.launches - st0.launches),
-        "clocks": clk.summary(),
+        "e2e": {"value": ws * a["e2e_steps_per_s"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": a["e2e_d2h_bytes_per_step"],
+                "note": "state resident on the device; one frame of fields (p,u,v,X,Y,phi) copied to host per "
+                        "timed run of K steps"},
+        "gpu_launches": a["launches"],
+        "clocks": clocks,
     }
-    if learned_info is not None:
-        line["learned"] = learned_info
-        line["config"]["initial_guess"] = "learned warm start on the previous solution"
-
+    if plain is not None:
+        line["plain_fp64"] = {"value": ws * plain["steps_per_s"], "unit": "steps/s",
+                              "vcycles_per_projection": {"mac": plain["vc_mac"], "fem": plain["vc_fem"]},
+                              "phase_ms_per_step": plain.get("phases")}
+        line["speedup_vs_plain_fp64"] = a["steps_per_s"] / plain["steps_per_s"]
+        line["errors_vs_fp64"] = a["errors_vs_fp64"]
+    if info is not None:
+        info.update(a.get("learned", {}))
+        line["learned"] = info
+    if also:
+        line["also"] = also
     print(json.dumps(line))
-    sim.close()
 
 
 LEARNED_FACTOR = 8      # the network runs on the 4096^2 solve restricted to 512^2
@@ -654,8 +744,8 @@ def _train_learned_mac(s, m, dev, rank):
 def run_ours(args, ws, rank, local, dist):
     import torch
     from incrmt_b200 import capi, workloads
-    if args.workload in ("sspin1024", "sed1024", "flag2048"):
-        return run_ours_sspin(args, ws, rank, local, dist)
+    if args.workload in SIM_WORKLOADS:
+        return run_ours_sim(args, ws, rank, local, dist)
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -838,20 +928,27 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sspin1024", choices=["sspin1024", "mac4096", "sed1024", "flag2048"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--coarse-refresh", type=int, default=16,
+    ap.add_argument("--workload", default="flag2048", choices=list(SIM_WORKLOADS) + ["mac4096"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="arithmetic of the V-cycles (mixed: FP32 cycles inside FP64 defect correction)")
+    ap.add_argument("--guess", default="learned", choices=["previous", "learned"],
+                    help="initial guess of each projection: the previous solution, or the learned warm start "
+                         "trained first on a training run of the workload")
+    ap.add_argument("--learned", action="store_true", help="same as --guess learned")
+    ap.add_argument("--coarse-refresh", type=int, default=1,
                     help="rebuild the projections' Galerkin coarse operators every K projections "
-                         "(1: on every density change)")
+                         "(1: on every density change, as the reference)")
+    ap.add_argument("--also", default="sed2048",
+                    help="further simulation workloads compared the same way (comma-separated; N=1 only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--learned", action="store_true",
-                    help="mac4096: train the learned initial guess first and start every solve from it; "
-                         "sed1024, flag2048: train the learned warm start of both projections on a training "
-                         "run and apply it in every projection")
     ap.add_argument("--learned-rule", type=int, default=0, choices=[0, 1],
                     help="fallback rule of the simulation's learned warm start (0: when the guess raises the "
                          "residual, 1: when the energy-optimal step is not positive)")
+    ap.set_defaults(steps=20, warmup=5)
     args = ap.parse_args()
+    if args.learned:
+        args.guess = "learned"
+    args.learned = args.guess == "learned"
     ws, rank, local = _dist()
     if args.impl == "reference":
         run_reference(args, ws, rank)

@@ -31,7 +31,9 @@ extern "C" {
 
 /** Arithmetic of the V-cycles. */
 #define INCRMT_PREC_FP64  0  /* smoothing, transfers and residuals in FP64 */
-#define INCRMT_PREC_MIXED 1  /* FP32 V-cycles on the correction equation inside FP64 defect correction */
+#define INCRMT_PREC_MIXED 1  /* FP32 V-cycles on the correction equation inside FP64 defect correction;
+                                 a solve continues in FP64 once an FP32 step fails to halve the
+                                 residual (incrmt_mg_mixed_fallbacks counts those solves) */
 
 typedef struct incrmt_mg incrmt_mg;
 
@@ -115,6 +117,12 @@ int incrmt_mg_set_tiles(incrmt_mg *h, int on);
  * every > 1, incrmt_mg_set_density_device copies the density into the
  * handle, so the caller's array need not outlive the call. */
 int incrmt_mg_set_coarse_refresh(incrmt_mg *h, int every);
+
+/** Mixed-precision solves (INCRMT_PREC_MIXED) since creation that finished
+ * with FP64 V-cycles: a solve switches once an FP32 defect-correction step
+ * fails to halve the FP64 residual norm, so it converges as the FP64 solve
+ * would. */
+long long incrmt_mg_mixed_fallbacks(const incrmt_mg *h);
 
 /** Galerkin hierarchy rebuilds since creation; *retries (if not null)
  * receives the number of solves repeated after rebuilding lagged levels. */

@@ -113,6 +113,8 @@ typedef struct incrmt_sim_stats {
     long long coarse_builds;               /* Galerkin hierarchy rebuilds, MAC plus FEM */
     long long coarse_retries;              /* projections solved again after a failed solve on lagged
                                               coarse levels, with the levels rebuilt */
+    long long mixed_fallbacks;             /* mixed-precision projections finished with FP64 V-cycles
+                                              (an FP32 correction did not halve the residual) */
 } incrmt_sim_stats;
 
 /** Creates the simulation (fluid_2d::fluid_2d, fluid_2d.cc:26-43). */

@@ -114,6 +114,23 @@ typedef struct incrmt_sim_learned_stats {
 } incrmt_sim_learned_stats;
 int incrmt_sim_get_learned_stats(incrmt_sim *h, int sys, incrmt_sim_learned_stats *st);
 
+/** One convolution of the U-Net's kind on the tcgen05 tensor cores (no
+ * reference counterpart): d_y = act(bias + conv(d_x, weights)) for a 3x3
+ * (taps 9, zero padding) or 1x1 (taps 1) kernel over batch x H x W images,
+ * NHWC BF16 activations (cin and cout multiples of 16), the weights BF16 as
+ * [tap][cout][cin] (K-major for the implicit GEMM), d_bias (cout FP32) may
+ * be null, relu 0 or 1. With flip set the taps are read in reverse order,
+ * so that the forward weights W[tap][cin][cout] of a layer, passed as
+ * [tap][cout'=cin][cin'=cout], give the input gradient of that layer from
+ * its output gradient. Issued on `stream`, not waited for. */
+int incrmt_conv_bf16(const void *d_x, int batch, int H, int W, int cin, const void *d_wk, int taps, int cout,
+                     int flip, const float *d_bias, int relu, void *d_y, void *stream);
+
+/** INCRMT_OK, or INCRMT_ERR_CUDA when a tensor-core convolution gave up one
+ * of its pipeline waits (each is limited to one second) since the last call;
+ * clears that record. Synchronises the device. */
+int incrmt_conv_status(void);
+
 /** Kernel launches issued by this network so far. */
 long long incrmt_unet_launches(const incrmt_unet *h);
 

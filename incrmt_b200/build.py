@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libincrmt_gpu.so")
-SOURCES = ["capi.cu", "mg.cu", "sim.cu", "noalloc.cu", "unet.cu", "learned.cu"]
+SOURCES = ["capi.cu", "mg.cu", "sim.cu", "noalloc.cu", "unet.cu", "learned.cu", "conv_tc.cu"]
 # The CUDA runtime is linked as a shared library: in a process that also
 # loads PyTorch, the library and torch then use one runtime (the soname
 # libcudart.so.12 resolves to the copy already loaded), so neither's exit

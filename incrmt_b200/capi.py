@@ -82,6 +82,8 @@ def lib():
     L.incrmt_mg_set_coarse_refresh.argtypes = [P, I]
     L.incrmt_mg_coarse_builds.argtypes = [P, ctypes.POINTER(ctypes.c_longlong)]
     L.incrmt_mg_coarse_builds.restype = ctypes.c_longlong
+    L.incrmt_mg_mixed_fallbacks.argtypes = [P]
+    L.incrmt_mg_mixed_fallbacks.restype = ctypes.c_longlong
     L.incrmt_mg_profile.argtypes = [P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(ctypes.c_longlong)]
     L.incrmt_mg_stream.argtypes = [P]
     L.incrmt_mg_stream.restype = P
@@ -189,6 +191,10 @@ class MGSolver:
         (incrmt_mg_set_coarse_refresh; 1 rebuilds on every change)."""
         check(lib().incrmt_mg_set_coarse_refresh(self._h, int(every)))
 
+    def mixed_fallbacks(self):
+        """Mixed-precision solves that finished with FP64 V-cycles."""
+        return int(lib().incrmt_mg_mixed_fallbacks(self._h))
+
     def coarse_builds(self):
         """(hierarchy rebuilds, solves repeated after a rebuild of lagged
         coarse levels) since creation."""
@@ -285,7 +291,8 @@ class SimStats(ctypes.Structure):
                 ("extrap_sweeps", ctypes.c_longlong), ("launches", ctypes.c_longlong),
                 ("dt_reg", ctypes.c_double), ("time", ctypes.c_double),
                 ("march_monotone", ctypes.c_longlong), ("window_points", ctypes.c_longlong),
-                ("coarse_builds", ctypes.c_longlong), ("coarse_retries", ctypes.c_longlong)]
+                ("coarse_builds", ctypes.c_longlong), ("coarse_retries", ctypes.c_longlong),
+                ("mixed_fallbacks", ctypes.c_longlong)]
 
 
 def _sim_sigs(L):
@@ -637,6 +644,8 @@ def _unet_sigs(L):
     L.incrmt_unet_forward.argtypes = [P, I, I, I, P, P, P]
     L.incrmt_unet_train_step.argtypes = [P, I, I, I, P, P, P, F, fp, P]
     L.incrmt_unet_gradients.argtypes = [P, I, I, I, P, P, P, fp, fp, P]
+    L.incrmt_conv_bf16.argtypes = [P, I, I, I, I, P, I, I, I, P, I, P, P]
+    L.incrmt_conv_status.argtypes = []
     L.incrmt_unet_launches.argtypes = [P]
     L.incrmt_unet_launches.restype = ctypes.c_longlong
     L.incrmt_unet_destroy.argtypes = [P]
@@ -720,6 +729,20 @@ class UNet:
             self.close()
         except Exception:
             pass
+
+
+def conv_bf16(x_ptr, batch, H, W, cin, wk_ptr, taps, cout, y_ptr, bias_ptr=0, relu=False, flip=False, stream=0):
+    """One tensor-core convolution (incrmt_conv_bf16): NHWC BF16 activations,
+    weights BF16 [tap][cout][cin]; device pointers as integers."""
+    check(_ulib().incrmt_conv_bf16(ctypes.c_void_p(x_ptr), batch, H, W, cin, ctypes.c_void_p(wk_ptr), taps, cout,
+                                   int(flip), ctypes.c_void_p(bias_ptr or None), int(relu), ctypes.c_void_p(y_ptr),
+                                   ctypes.c_void_p(stream)))
+
+
+def conv_status():
+    """Raises if a tensor-core convolution gave up a pipeline wait
+    (incrmt_conv_status; synchronises the device)."""
+    check(_ulib().incrmt_conv_status())
 
 
 def learned_guess(solver, net, b_ptr, z_ptr, factor=1, stats=True):

@@ -137,6 +137,8 @@ long long incrmt_mg_coarse_builds(const incrmt_mg *h, long long *retries) {
     return h->mg.coarse_builds;
 }
 
+long long incrmt_mg_mixed_fallbacks(const incrmt_mg *h) { return h ? h->mg.mixed_fallbacks : 0; }
+
 int incrmt_mg_set_profiling(incrmt_mg *h, int on) {
     if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
     h->mg.prof = on != 0;

@@ -1,0 +1,390 @@
+// tcgen05 implicit-GEMM convolutions (see conv_tc.cuh).
+//
+// One CTA of 128 threads computes a 128-pixel x Cout tile of the output:
+//  - warp 0, one thread: TMA producer. For every (tap, channel chunk) it
+//    loads the tile's input pixels shifted by the tap, [128 pixels][KC
+//    channels], from a 4-D tensor map over the NHWC activations (the shift
+//    goes into the W and H coordinates; TMA fills pixels outside the image
+//    with zeros, which is the convolution's zero padding) and the weights
+//    [Cout][KC] of that tap and chunk, into one stage of a ring of shared
+//    memory buffers, both with the swizzle that matches KC (32, 64 or 128
+//    byte rows).
+//  - warp 1, one thread: issues tcgen05.mma (kind::f16, BF16 operands, FP32
+//    accumulator in tensor memory, M = 128, N = Cout, K = 16 per
+//    instruction) on each stage and releases the stage with tcgen05.commit.
+//  - all four warps: epilogue. Each warp reads its 32 tensor-memory lanes
+//    (one pixel per thread) with tcgen05.ld, adds the bias, applies the
+//    ReLU and stores BF16.
+// Every wait on a barrier gives up after one second (%globaltimer), sets
+// g_conv_timeout and lets the CTA finish: the producer then waits, again
+// bounded, for its loads in flight, the MMA thread still commits so that the
+// epilogue only reads after the issued MMAs are done, and tensor memory is
+// freed before the CTA exits.
+#include <cstdint>
+#include <cstring>
+#include "common.cuh"
+#include "conv_tc.cuh"
+
+namespace incrmt {
+
+__device__ int g_conv_timeout = 0;
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kThreads = 128;
+constexpr int kTileM = 128;
+constexpr unsigned long long kWaitNs = 1000000000ull;  // one second
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+/** Waits for the phase of parity `parity` of the barrier to complete, at
+ * most one second; false (and the timeout flag set) if it did not. */
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_test(bar, parity)) {
+        if (global_ns() - t0 > kWaitNs) {
+            atomicExch(&g_conv_timeout, 1);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1,
+                                            int c2, int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1,
+                                            int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+/** Shared-memory matrix descriptor of a K-major operand tile whose rows
+ * (one per M or N index) are KC BF16 = 2*KC bytes with the matching swizzle
+ * (32, 64 or 128 bytes), eight-row groups 16*KC bytes apart. */
+template <int KC>
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    constexpr uint64_t layout = KC == 64 ? 2 : KC == 32 ? 4 : 6;  // SWIZZLE_128B / 64B / 32B
+    constexpr uint64_t sbo = (8 * 2 * KC) >> 4;
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFF) | (1ull << 16) | (sbo << 32) | (1ull << 46) | (layout << 61);
+}
+
+/** Instruction descriptor of kind::f16: BF16 A and B, both K-major, FP32
+ * accumulator, M = 128, N = n. */
+__host__ __device__ constexpr uint32_t instr_desc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(
+            tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+/** Sixteen consecutive 32-bit columns of this thread's tensor-memory lane. */
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+/** The convolution kernel (see the file comment); blockIdx.y selects the
+ * output channels n0 = N * blockIdx.y .. n0 + N - 1 of ldy. Dynamic shared
+ * memory: 1024 (alignment) + S * (128 + N) * KC * 2 bytes of stage buffers,
+ * then 2S + 1 barriers (full[S], empty[S], done) and the tensor-memory
+ * address. */
+template <int TAPS, int KC>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_conv_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+              const float *__restrict__ bias, bf16 *__restrict__ Y, int H, int W, int N, int ldy, int Wt, int Ht,
+              int tiles_x, int tiles_y, int nck, int flip, int relu, int S, uint32_t tmem_cols) {
+    extern __shared__ __align__(1024) unsigned char conv_smem[];
+    const uint32_t raw = smem_addr(conv_smem);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    const uint32_t abytes = kTileM * KC * 2, bbytes = static_cast<uint32_t>(N) * KC * 2;
+    const uint32_t sA = base, sB = base + S * abytes;
+    const uint32_t bar0 = sB + S * bbytes;  // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), done = bar0 + 16S
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(conv_smem + (bar0 + 8 * (2 * S + 1) - raw));
+    const uint32_t done = bar0 + 16 * S;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int tile = blockIdx.x;
+    const int tx = tile % tiles_x;
+    tile /= tiles_x;
+    const int ty = tile % tiles_y, b = tile / tiles_y;
+    const int x0 = tx * Wt, y0 = ty * Ht, n0 = blockIdx.y * N;
+
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 2 * S + 1; q++) mbar_init(bar0 + 8 * q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int iters = TAPS * nck;
+
+    if (threadIdx.x == 0) {
+        // TMA producer
+        int issued = 0;
+        for (int it = 0; it < iters; it++) {
+            const int s = it % S;
+            if (it >= S && !mbar_wait(bar0 + 8 * (S + s), ((it / S) - 1) & 1)) break;
+            const int tap = it / nck, ck = it - tap * nck;
+            const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
+            const uint32_t full = bar0 + 8 * s;
+            mbar_arrive_expect_tx(full, abytes + bbytes);
+            tma_load_4d(sA + s * abytes, &mapA, full, ck * KC, x0 + dx, y0 + dy, b);
+            tma_load_3d(sB + s * bbytes, &mapB, full, ck * KC, n0, flip ? TAPS - 1 - tap : tap);
+            issued = it + 1;
+        }
+        // No copy may still be in flight when the CTA exits: wait for the last
+        // use of every stage (at once when the MMA thread consumed it).
+        for (int it = issued > S ? issued - S : 0; it < issued; it++) mbar_wait(bar0 + 8 * (it % S), (it / S) & 1);
+    } else if (threadIdx.x == 32) {
+        // MMA issuer
+        const uint32_t idesc = instr_desc(N);
+        for (int it = 0; it < iters; it++) {
+            const int s = it % S;
+            if (!mbar_wait(bar0 + 8 * s, (it / S) & 1)) break;
+            tc_fence_after();
+            const uint64_t ad = smem_desc<KC>(sA + s * abytes), bd = smem_desc<KC>(sB + s * bbytes);
+#pragma unroll
+            for (int k = 0; k < KC / 16; k++)
+                tc_mma(tmem, ad + 2 * k, bd + 2 * k, idesc, (it > 0 || k > 0) ? 1u : 0u);
+            tc_commit(bar0 + 8 * (S + s));
+        }
+        // arrives once every MMA issued above has completed
+        tc_commit(done);
+    }
+    __syncwarp();
+
+    // Epilogue: warp w holds tensor-memory lanes 32w..32w+31, the tile's
+    // pixels in row-major order of the Wt x Ht tile.
+    bool ok = mbar_wait(done, 0);
+    // the tensor-memory loads below are warp-collective: converge, and agree
+    // on whether the wait succeeded
+    ok = __all_sync(0xffffffffu, ok);
+    tc_fence_after();
+    if (ok) {
+        const int r = warp * 32 + lane;
+        const int py = y0 + r / Wt, px = x0 + r % Wt;
+        const bool valid = py < H && px < W;
+        bf16 *yrow = Y + ((static_cast<long>(b) * H + py) * W + px) * static_cast<long>(ldy) + n0;
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            uint32_t v[16];
+            tc_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), v);
+            if (!valid) continue;
+            uint32_t packed[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                float f0 = __uint_as_float(v[2 * j]), f1 = __uint_as_float(v[2 * j + 1]);
+                if (bias) {
+                    f0 += bias[n0 + c0 + 2 * j];
+                    f1 += bias[n0 + c0 + 2 * j + 1];
+                }
+                if (relu) {
+                    f0 = fmaxf(f0, 0.f);
+                    f1 = fmaxf(f1, 0.f);
+                }
+                const __nv_bfloat162 h = __floats2bfloat162_rn(f0, f1);
+                packed[j] = *reinterpret_cast<const uint32_t *>(&h);
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(yrow + c0);
+            dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+}
+
+}  // namespace
+
+namespace {
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+/** cuTensorMapEncodeTiled from the driver, through the runtime's entry-point
+ * query (the library links the runtime only). */
+EncodeTiled encode_tiled() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+
+CUtensorMapSwizzle swizzle_of(int kc) {
+    return kc == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : kc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+}
+
+constexpr int kMaxSmem = 227 * 1024;
+
+template <int TAPS, int KC>
+int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, int Nt, bool flip,
+                const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
+    EncodeTiled enc = encode_tiled();
+    if (!enc) {
+        set_error("conv: cuTensorMapEncodeTiled is not available");
+        return INCRMT_ERR_CUDA;
+    }
+    const int Wt = W >= 128 ? 128 : W >= 64 ? 64 : W >= 32 ? 32 : 16, Ht = kTileM / Wt;
+    const int tiles_x = (W + Wt - 1) / Wt, tiles_y = (H + Ht - 1) / Ht;
+    CUtensorMap mA, mB;
+    {
+        const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Cin), static_cast<cuuint64_t>(W),
+                                    static_cast<cuuint64_t>(H), static_cast<cuuint64_t>(B)};
+        const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Cin) * 2, static_cast<cuuint64_t>(W) * Cin * 2,
+                                       static_cast<cuuint64_t>(H) * W * Cin * 2};
+        const cuuint32_t box[4] = {static_cast<cuuint32_t>(KC), static_cast<cuuint32_t>(Wt),
+                                   static_cast<cuuint32_t>(Ht), 1};
+        const cuuint32_t es[4] = {1, 1, 1, 1};
+        CUresult r = enc(&mA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(X), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(KC), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            set_error("conv: activation tensor map rejected (%d)", static_cast<int>(r));
+            return INCRMT_ERR_CUDA;
+        }
+    }
+    {
+        const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Cin), static_cast<cuuint64_t>(Cout),
+                                    static_cast<cuuint64_t>(TAPS)};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Cin) * 2, static_cast<cuuint64_t>(Cout) * Cin * 2};
+        const cuuint32_t box[3] = {static_cast<cuuint32_t>(KC), static_cast<cuuint32_t>(Nt), 1};
+        const cuuint32_t es[3] = {1, 1, 1};
+        CUresult r = enc(&mB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16 *>(wk), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(KC), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            set_error("conv: weight tensor map rejected (%d)", static_cast<int>(r));
+            return INCRMT_ERR_CUDA;
+        }
+    }
+    const int per = (kTileM + Nt) * KC * 2;
+    int S = (200 * 1024) / per;
+    S = S > 4 ? 4 : S;
+    if (S < 2) S = 2;
+    const size_t smem = 1024 + static_cast<size_t>(S) * per + 8 * (2 * S + 1) + 16;
+    uint32_t cols = 32;
+    while (cols < static_cast<uint32_t>(Nt)) cols <<= 1;
+    static bool attr = false;
+    if (!attr) {
+        INCRMT_CK(cudaFuncSetAttribute(k_conv_tc<TAPS, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+        attr = true;
+    }
+    const dim3 grid(static_cast<unsigned>(B * tiles_x * tiles_y), static_cast<unsigned>(Cout / Nt));
+    k_conv_tc<TAPS, KC><<<grid, kThreads, smem, s>>>(mA, mB, bias, Y, H, W, Nt, Cout, Wt, Ht, tiles_x, tiles_y,
+                                                     Cin / KC, flip ? 1 : 0, relu ? 1 : 0, S, cols);
+    INCRMT_CKL("k_conv_tc");
+    return INCRMT_OK;
+}
+
+template <int TAPS>
+int launch_taps(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, int Nt, bool flip,
+                const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
+    if (Cin % 64 == 0) return launch_conv<TAPS, 64>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    if (Cin % 32 == 0) return launch_conv<TAPS, 32>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    return launch_conv<TAPS, 16>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+}
+
+}  // namespace
+
+int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int taps, int Cout, bool flip,
+            const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
+    if (!X || !wk || !Y || B < 1 || H < 1 || W < 1 || Cin < 16 || Cin % 16 || Cout < 16 || Cout % 16 ||
+        (taps != 1 && taps != 9)) {
+        set_error("conv: bad arguments (channels must be positive multiples of 16, taps 1 or 9)");
+        return INCRMT_ERR_BADARG;
+    }
+    // output channels per CTA: all of them up to 256, else the largest
+    // multiple of 16 of at most 256 that divides Cout
+    int Nt = Cout;
+    if (Nt > 256) {
+        Nt = 256;
+        while (Cout % Nt) Nt -= 16;
+    }
+    if (taps == 9) return launch_taps<9>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    return launch_taps<1>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+}
+
+int conv_tc_status() {
+    INCRMT_CK(cudaDeviceSynchronize());
+    int flag = 0, zero = 0;
+    INCRMT_CK(cudaMemcpyFromSymbol(&flag, g_conv_timeout, sizeof(int)));
+    if (flag) {
+        INCRMT_CK(cudaMemcpyToSymbol(g_conv_timeout, &zero, sizeof(int)));
+        set_error("tensor-core convolution: a pipeline wait exceeded its one-second limit");
+        return INCRMT_ERR_CUDA;
+    }
+    return INCRMT_OK;
+}
+
+}  // namespace incrmt

@@ -1,0 +1,28 @@
+// 5th-generation tensor-core (tcgen05) convolutions of the learned initial
+// guess's U-Net: NHWC BF16 activations, FP32 accumulation in tensor memory.
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace incrmt {
+
+/** Y = act(bias + conv(X, weights)) for a 3x3 (taps = 9, zero padding) or
+ * 1x1 (taps = 1) convolution on B x H x W images, NHWC BF16, Cin and Cout
+ * multiples of 16 (Cout <= 256), as an implicit GEMM on the tcgen05 tensor
+ * cores: M = 128 pixels (a Wt x Ht tile of one image), N = Cout, K = taps x
+ * Cin. `wk` holds the weights K-major for the GEMM, [tap][Cout][Cin]; with
+ * `flip` the taps are read in reverse order and `wk` is [tap][Cout][Cin] of
+ * the flipped kernel, which is how the input gradient (the convolution of
+ * the output gradient with the flipped, transposed weights) reuses the same
+ * kernel with the forward weights W[tap][Cin][Cout] as its K-major operand.
+ * bias may be null. Issued on `s`, not waited for. */
+int conv_tc(const __nv_bfloat16 *X, int B, int H, int W, int Cin, const __nv_bfloat16 *wk, int taps, int Cout,
+            bool flip, const float *bias, bool relu, __nv_bfloat16 *Y, cudaStream_t s);
+
+/** INCRMT_OK, or INCRMT_ERR_CUDA if a tensor-core convolution gave up a wait
+ * (its one-second limit on a pipeline barrier) since the last call; clears
+ * the flag. Synchronises the device. */
+int conv_tc_status();
+
+}  // namespace incrmt

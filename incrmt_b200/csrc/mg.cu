@@ -12,6 +12,9 @@ constexpr int kNu1 = 2, kNu2 = 2, kCoarseSweeps = 64, kCoarsestSize = 16, kMaxLe
 /** Coupling ratio beyond which only the strongly coupled direction is
  * coarsened (semi-coarsening). */
 constexpr double kSemiRatio = 2.0;
+/** Largest residual ratio an FP32 defect-correction step may reach before the
+ * solve continues in FP64. */
+constexpr double kMixedContraction = 0.5;
 
 // ---------------------------------------------------------------------------
 // Transfer-operator index helpers (identical rules to the CPU oracle's shim).
@@ -198,10 +201,97 @@ __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool 
     for (int e = 0; e < 9; e++) st[e * N + ij] = q[e];
 }
 
-__global__ void k_cast(const double *a, float *b, long n) {
-    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<long>(gridDim.x) * blockDim.x)
-        b[i] = static_cast<float>(a[i]);
+/** k_galerkin for a 32 x 8 tile of coarse unknowns per 256-thread block,
+ * with every input staged in shared memory first: the nine stencil entries
+ * of the fine points of the tile's supports (coef9; the fine region
+ * 2X0-1 .. 2(X0+31)+1 in a coarsened direction, X0 .. X0+31 otherwise) and
+ * the four prolongation weights of that region grown by one point (the
+ * stencil neighbours), zero outside a non-periodic grid. The sums then run
+ * exactly as in k_galerkin, in the same order: the same values, without
+ * each thread re-reading some four hundred entries from global memory.
+ * Dynamic shared memory: galerkin_tile_smem(kx, ky) bytes. */
+template <class Op>
+__global__ void __launch_bounds__(256) k_galerkin_tile(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
+                                                       int cm, int cn, double *st, const double *P) {
+    extern __shared__ __align__(16) double gal_smem[];
+    constexpr int CTW = 32, CTH = 8;
+    const int X0 = blockIdx.x * CTW, Y0 = blockIdx.y * CTH;
+    const int SX0 = kx ? 2 * X0 - 1 : X0, SY0 = ky ? 2 * Y0 - 1 : Y0;
+    const int SW = kx ? 2 * CTW + 1 : CTW, SH = ky ? 2 * CTH + 1 : CTH, SA = SW * SH;
+    const int NX0 = SX0 - 1, NY0 = SY0 - 1, NW = SW + 2, NH = SH + 2;
+    double *As = gal_smem;          // entry k of support point t at As[k * SA + t]
+    double *Ps = gal_smem + 9 * SA;  // weights of region point t at Ps[4 * t .. 4 * t + 3]
+    for (int t = threadIdx.x; t < NW * NH; t += blockDim.x) {
+        bool ok = true;
+        const int i = wrap_idx(NX0 + t % NW, fm, px, ok), j = wrap_idx(NY0 + t / NW, fn, py, ok);
+        double w[4] = {0, 0, 0, 0};
+        if (ok) {
+            const double *q = P + 4 * (static_cast<long>(i) + static_cast<long>(fm) * j);
+            w[0] = q[0]; w[1] = q[1]; w[2] = q[2]; w[3] = q[3];
+        }
+        Ps[4 * t] = w[0]; Ps[4 * t + 1] = w[1]; Ps[4 * t + 2] = w[2]; Ps[4 * t + 3] = w[3];
+    }
+    for (int t = threadIdx.x; t < SA; t += blockDim.x) {
+        bool ok = true;
+        const int i = wrap_idx(SX0 + t % SW, fm, px, ok), j = wrap_idx(SY0 + t / SW, fn, py, ok);
+        if (!ok) continue;  // a point outside the grid has weight zero: never read
+        double a[9];
+        op.coef9(i, j, a);
+#pragma unroll
+        for (int k = 0; k < 9; k++) As[k * SA + t] = a[k];
+    }
+    __syncthreads();
+    const int I = X0 + (threadIdx.x & 31), J = Y0 + (threadIdx.x >> 5);
+    if (I >= cm || J >= cn) return;
+    double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int x0 = kx ? 2 * I - 1 : I, x1 = kx ? 2 * I + 1 : I, y0 = ky ? 2 * J - 1 : J, y1 = ky ? 2 * J + 1 : J;
+    for (int fj = y0; fj <= y1; fj++)
+        for (int fi = x0; fi <= x1; fi++) {
+            // pweight(fi, fj, I, J) from the staged weights
+            const int qx = I - base_of(fi, kx), qy = J - base_of(fj, ky);
+            if (qx < 0 || qx > 1 || qy < 0 || qy > 1) continue;
+            const double w = Ps[4 * ((fi - NX0) + NW * (fj - NY0)) + qx + 2 * qy];
+            if (w == 0) continue;
+            const int ls = (fi - SX0) + SW * (fj - SY0);
+            for (int dj = -1; dj <= 1; dj++)
+                for (int di = -1; di <= 1; di++) {
+                    const double av = As[(3 * (dj + 1) + di + 1) * SA + ls];
+                    if (av == 0) continue;
+                    const double *g = Ps + 4 * ((fi + di - NX0) + NW * (fj + dj - NY0));
+                    const int ox = base_of(fi + di, kx) - I, oy = base_of(fj + dj, ky) - J;
+                    for (int r = 0; r < 4; r++) {
+                        const int kx_ = ox + (r & 1), ky_ = oy + (r >> 1);
+                        if (g[r] == 0 || kx_ < -1 || kx_ > 1 || ky_ < -1 || ky_ > 1) continue;
+                        double &qe = q[3 * (ky_ + 1) + kx_ + 1];
+                        qe = add_prod(qe, __dmul_rn(w, av), g[r]);
+                    }
+                }
+        }
+    const long N = static_cast<long>(cm) * cn, ij = I + static_cast<long>(cm) * J;
+    for (int e = 0; e < 9; e++) st[e * N + ij] = q[e];
+}
+
+/** Shared memory of k_galerkin_tile for the coarsening flags. */
+inline size_t galerkin_tile_smem(bool kx, bool ky) {
+    const int SW = kx ? 65 : 32, SH = ky ? 17 : 8;
+    return sizeof(double) * (9 * SW * SH + 4 * (SW + 2) * (SH + 2));
+}
+
+/** Single-precision copy of a level's Galerkin stencils (entry k of unknown
+ * q at k*N+q) for the centred FP32 cycles: entry 4 holds the row sum of the
+ * FP64 stencil, summed in FP64, instead of the diagonal. */
+__global__ void k_cast_stencil(const double *st, float *stf, long N) {
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x) {
+        double rs = 0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const double v = st[k * N + q];
+            rs += v;
+            if (k != 4) stf[k * N + q] = static_cast<float>(v);
+        }
+        stf[4 * N + q] = static_cast<float>(rs);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -213,10 +303,8 @@ __global__ void k_smooth(Op op, T *z, const T *b, int m, int n, int pi, int pj) 
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + pi;
     const int j = 2 * (blockIdx.y * blockDim.y + threadIdx.y) + pj;
     if (i >= m || j >= n) return;
-    T diag;
-    const T off = op.offdiag(i, j, z, diag);
     const int ij = i + m * j;
-    z[ij] = (b[ij] - off) / diag;
+    z[ij] = gs_update(op, i, j, z, b[ij]);
 }
 
 /** Index i of a periodic direction of size m brought into [0, m). */
@@ -271,9 +359,7 @@ __global__ void __launch_bounds__(256) k_smooth_tile(Op op, const T *zin, T *zou
             const int i = i0 + 2 * (t % ni), j = j0 + 2 * (t / ni);
             const int lz = (i - gx0) + LW * (j - gy0);
             const int ir = px ? wrap_index(i, m) : i, jr = py ? wrap_index(j, n) : j;
-            T diag;
-            const T off = op.offdiag_s(ir, jr, zs, lz, LW, diag);
-            zs[lz] = (b[ir + static_cast<long>(m) * jr] - off) / diag;
+            zs[lz] = gs_update_s(op, ir, jr, zs, lz, LW, b[ir + static_cast<long>(m) * jr]);
         }
         __syncthreads();
     }
@@ -335,23 +421,32 @@ __global__ void __launch_bounds__(256) k_smooth_tile_gen(GenOp<T> op, const T *z
             const int i = i0 + 2 * (t % ni), j = j0 + 2 * (t / ni);
             const int lz = (i - gx0) + LW * (j - gy0);
             const int ir = px ? wrap_index(i, m) : i, jr = py ? wrap_index(j, n) : j;
-            // GenOp::offdiag_s with the coefficients read from shared memory
+            // gs_update_s of GenOp with the coefficients read from shared
+            // memory (in single precision entry 4 is the row sum and the
+            // neighbours enter centred)
             const bool l = px || ir > 0, r = px || ir < m - 1, d = py || jr > 0, u = py || jr < n - 1;
-            const T diag = cs[4 * LA + lz];
-            T s = 0;
+            const T zc = sizeof(T) == 8 ? T(0) : zs[lz];
+            T diag = cs[4 * LA + lz];
+            T s = 0, a = 0;
             if (d) {
-                if (l) s += cs[lz] * zs[lz - LW - 1];
-                s += cs[LA + lz] * zs[lz - LW];
-                if (r) s += cs[2 * LA + lz] * zs[lz - LW + 1];
+                if (l) { s += cs[lz] * (zs[lz - LW - 1] - zc); a += cs[lz]; }
+                s += cs[LA + lz] * (zs[lz - LW] - zc); a += cs[LA + lz];
+                if (r) { s += cs[2 * LA + lz] * (zs[lz - LW + 1] - zc); a += cs[2 * LA + lz]; }
             }
-            if (l) s += cs[3 * LA + lz] * zs[lz - 1];
-            if (r) s += cs[5 * LA + lz] * zs[lz + 1];
+            if (l) { s += cs[3 * LA + lz] * (zs[lz - 1] - zc); a += cs[3 * LA + lz]; }
+            if (r) { s += cs[5 * LA + lz] * (zs[lz + 1] - zc); a += cs[5 * LA + lz]; }
             if (u) {
-                if (l) s += cs[6 * LA + lz] * zs[lz + LW - 1];
-                s += cs[7 * LA + lz] * zs[lz + LW];
-                if (r) s += cs[8 * LA + lz] * zs[lz + LW + 1];
+                if (l) { s += cs[6 * LA + lz] * (zs[lz + LW - 1] - zc); a += cs[6 * LA + lz]; }
+                s += cs[7 * LA + lz] * (zs[lz + LW] - zc); a += cs[7 * LA + lz];
+                if (r) { s += cs[8 * LA + lz] * (zs[lz + LW + 1] - zc); a += cs[8 * LA + lz]; }
             }
-            zs[lz] = (bs[lz] - s) / diag;
+            if constexpr (sizeof(T) == 8) {
+                zs[lz] = (bs[lz] - s) / diag;
+            } else {
+                const T rs = diag;  // the row sum
+                diag = rs - a;
+                zs[lz] = zc + (bs[lz] - s - rs * zc) / diag;
+            }
         }
         __syncthreads();
     }
@@ -409,9 +504,7 @@ __global__ void __launch_bounds__(256) k_smooth_rb(Op op, const T *zin, T *zout,
             for (int i = i0 + 2 * tx; i <= ihi; i += 64) {
                 const int lz = (i - gx0) + LW * (j - gy0);
                 const int ir = px ? wrap_index(i, m) : i;
-                T diag;
-                const T off = op.offdiag_s(ir, jr, zs, lz, LW, diag);
-                zs[lz] = (b[ir + static_cast<long>(m) * jr] - off) / diag;
+                zs[lz] = gs_update_s(op, ir, jr, zs, lz, LW, b[ir + static_cast<long>(m) * jr]);
             }
         }
         __syncthreads();
@@ -442,10 +535,7 @@ __global__ void k_restrict(Op op, const T *z, const T *b, int fm, int fn, int px
             bool ok = true;
             const int i = wrap_idx(fi, fm, px, ok), j = wrap_idx(fj, fn, py, ok);
             const int f = i + fm * j;
-            T diag;
-            const T off = op.offdiag(i, j, z, diag);
-            const T r = b[f] - off - diag * z[f];
-            t = add_prod(t, w, r);
+            t = add_prod(t, w, residual_at(op, i, j, z, b[f]));
         }
     bc[I + cm * J] = t;
     zc[I + cm * J] = 0;
@@ -476,9 +566,7 @@ __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const 
         T r = 0;
         if (ok) {
             const int f = fx + fm * fy;
-            T diag;
-            const T off = op.offdiag(fx, fy, z, diag);
-            r = b[f] - off - diag * z[f];
+            r = residual_at(op, fx, fy, z, b[f]);
         }
         rs[t] = r;
     }
@@ -529,9 +617,7 @@ __global__ void k_coarse(Op op, T *z, const T *b, int m, int n, int sweeps) {
             const int mc = (m - pis[c] + 1) / 2, nc = (n - pjs[c] + 1) / 2;
             for (int p = threadIdx.x; p < mc * nc; p += blockDim.x) {
                 const int i = 2 * (p % mc) + pis[c], j = 2 * (p / mc) + pjs[c];
-                T diag;
-                const T off = op.offdiag(i, j, z, diag);
-                z[i + m * j] = (b[i + m * j] - off) / diag;
+                z[i + m * j] = gs_update(op, i, j, z, b[i + m * j]);
             }
             __syncthreads();
         }
@@ -708,9 +794,7 @@ __device__ void tail_smooth(const TailLevels<T> &L, int l, int sweeps) {
             const int mc = (m - pis[c] + 1) / 2, nc = (n - pjs[c] + 1) / 2;
             for (int p = threadIdx.x; p < mc * nc; p += nth) {
                 const int i = 2 * (p % mc) + pis[c], j = 2 * (p / mc) + pjs[c];
-                T diag;
-                const T off = op.offdiag(i, j, z, diag);
-                z[i + m * j] = (b[i + m * j] - off) / diag;
+                z[i + m * j] = gs_update(op, i, j, z, b[i + m * j]);
             }
             if (warp_only) __syncwarp();
             else __syncthreads();
@@ -764,10 +848,7 @@ __global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu
                     bool ok = true;
                     const int i = wrap_idx(fi, fm, L.px, ok), j = wrap_idx(fj, fn, L.py, ok);
                     const int f = i + fm * j;
-                    T diag;
-                    const T off = op.offdiag(i, j, L.z[l], diag);
-                    const T r = L.b[l][f] - off - diag * L.z[l][f];
-                    t = add_prod(t, w, r);
+                    t = add_prod(t, w, residual_at(op, i, j, static_cast<const T *>(L.z[l]), L.b[l][f]));
                 }
             L.b[l + 1][q] = t;
             L.z[l + 1][q] = 0;
@@ -1059,6 +1140,13 @@ int Multigrid::build_hierarchy() {
                                    gen_tile_smem<float>()));
     INCRMT_CK(cudaFuncSetAttribute(k_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTailSmemBudget)));
+    const int gal_smem = static_cast<int>(galerkin_tile_smem(true, true));
+    INCRMT_CK(cudaFuncSetAttribute(k_galerkin_tile<MacOp<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gal_smem));
+    INCRMT_CK(cudaFuncSetAttribute(k_galerkin_tile<FemOp<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gal_smem));
+    INCRMT_CK(cudaFuncSetAttribute(k_galerkin_tile<GenOp<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gal_smem));
     // First level small enough for the one-block tail kernel (never level 0).
     tail_level = -1;
     for (int l = 1; l < static_cast<int>(lev.size()); l++)
@@ -1074,6 +1162,7 @@ void Multigrid::destroy() {
     lev.clear();
     cudaFree(ex); cudaFree(ey); cudaFree(exf); cudaFree(eyf); cudaFree(c); cudaFree(cf);
     cudaFree(rho); cudaFree(bbuf); cudaFree(zbuf); cudaFree(partial); cudaFree(dnorm);
+    cudaFree(zsave); zsave = nullptr;
     cudaFree(ginv); cudaFree(ginvf); ginv = nullptr; ginvf = nullptr;
 
     if (hnorm) cudaFreeHost(hnorm);
@@ -1171,23 +1260,26 @@ int Multigrid::set_unit_density() {
 int Multigrid::galerkin_all() {
     for (size_t l = 1; l < lev.size(); l++) {
         MgLevel &F = lev[l - 1], &C = lev[l];
-        const dim3 gf = grid2(F.m, F.n), gc = grid2(C.m, C.n);
+        const dim3 gf = grid2(F.m, F.n), gc = grid2(C.m, C.n), gt(cdiv(C.m, 32), cdiv(C.n, 8));
+        const size_t gsm = galerkin_tile_smem(F.kx, F.ky);
+        auto build = [&](auto op) {
+            for (int pass = 0; pass < 2; pass++)
+                k_build_p<<<gf, kBlk2, 0, stream>>>(op, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
+            if (tiles)
+                k_galerkin_tile<<<gt, 256, gsm, stream>>>(op, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
+            else
+                k_galerkin<<<gc, kBlk2, 0, stream>>>(op, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
+        };
         if (l == 1 && sys == INCRMT_SYS_MAC) {
-            for (int pass = 0; pass < 2; pass++)
-                k_build_p<<<gf, kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
-            k_galerkin<<<gc, kBlk2, 0, stream>>>(mac64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
+            build(mac64());
         } else if (l == 1) {
-            for (int pass = 0; pass < 2; pass++)
-                k_build_p<<<gf, kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
-            k_galerkin<<<gc, kBlk2, 0, stream>>>(fem64(), F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
+            build(fem64());
         } else {
             GenOp<double> g; g.m = F.m; g.n = F.n; g.px = px; g.py = py; g.N = F.N; g.st = F.st;
-            for (int pass = 0; pass < 2; pass++)
-                k_build_p<<<gf, kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
-            k_galerkin<<<gc, kBlk2, 0, stream>>>(g, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
+            build(g);
         }
         launches += 3;
-        k_cast<<<cdiv(9 * C.N, 256) < kRedBlocks ? cdiv(9 * C.N, 256) : kRedBlocks, 256, 0, stream>>>(C.st, C.stf, 9 * C.N);
+        k_cast_stencil<<<cdiv(C.N, 256) < kRedBlocks ? cdiv(C.N, 256) : kRedBlocks, 256, 0, stream>>>(C.st, C.stf, C.N);
         launches++;
         INCRMT_CKL("galerkin");
     }
@@ -1518,19 +1610,25 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         return INCRMT_OK;
     }
     bool conv = false, finite = true;
+    double rn_prev = 0;
+    double rn0 = 0;
     if (prec == INCRMT_PREC_MIXED) {
+        // the warm start is kept: a fallback to FP64 restarts from it
+        if (!zsave) INCRMT_CK(cudaMalloc(&zsave, sizeof(double) * N));
+        INCRMT_CK(cudaMemcpyAsync(zsave, d_z, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
         if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
         if ((r = fetch_norm(&rn2))) return r;
+        rn_prev = rn0 = std::sqrt(rn2);
     }
     // One V-cycle, its residual norm and the read-back of that norm, captured
     // once into a CUDA graph per (precision, b, z) and replayed per cycle.
     const bool use_graph = !prof;
-    if (use_graph && (!gexec || gkey_prec != prec || gkey_b != b || gkey_z != d_z)) {
+    int cur = prec;
+    auto capture = [&]() -> int {
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
-        cudaGraph_t graph;
+        cudaGraph_t graph = nullptr;
         INCRMT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        graph = nullptr;
-        int rc = vcycle_and_norm(prec, b, d_z, N);
+        int rc = vcycle_and_norm(cur, b, d_z, N);
         cudaError_t ce = cudaStreamEndCapture(stream, &graph);
         if (rc || ce != cudaSuccess) {
             if (ce == cudaSuccess && graph) cudaGraphDestroy(graph);
@@ -1540,8 +1638,10 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         ce = cudaGraphInstantiate(&gexec, graph, 0);
         cudaGraphDestroy(graph);
         if (ce != cudaSuccess) { gexec = nullptr; return cuda_status(ce, "instantiate", __FILE__, __LINE__); }
-        gkey_prec = prec; gkey_b = b; gkey_z = d_z;
-    }
+        gkey_prec = cur; gkey_b = b; gkey_z = d_z;
+        return INCRMT_OK;
+    };
+    if (use_graph && (!gexec || gkey_prec != cur || gkey_b != b || gkey_z != d_z) && (r = capture())) return r;
     while (k < maxc) {
         if (use_graph) {
             INCRMT_CK(cudaGraphLaunch(gexec, stream));
@@ -1549,7 +1649,7 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
             INCRMT_CK(cudaStreamSynchronize(stream));
             rn2 = hnorm[0];
         } else {
-            if ((r = vcycle_and_norm(prec, b, d_z, N))) return r;
+            if ((r = vcycle_and_norm(cur, b, d_z, N))) return r;
             INCRMT_CK(cudaStreamSynchronize(stream));
             rn2 = hnorm[0];
         }
@@ -1557,6 +1657,22 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         const double rn = std::sqrt(rn2);
         if (!std::isfinite(rn)) { finite = false; break; }
         if (rn <= tol) { conv = true; break; }
+        // An FP32 correction that does not halve the FP64 residual means the
+        // single-precision cycle no longer approximates the system's inverse
+        // well enough for defect correction to converge: the solve restarts
+        // from its warm start with FP64 V-cycles (the FP32 corrections may
+        // have moved the iterate along the null space of a singular system
+        // far enough to spoil the FP64 residual's accuracy).
+        if (cur == INCRMT_PREC_MIXED && rn > kMixedContraction * rn_prev) {
+            cur = INCRMT_PREC_FP64;
+            mixed_fallbacks++;
+            INCRMT_CK(cudaMemcpyAsync(d_z, zsave, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
+            if (use_graph && (r = capture())) return r;
+            rn2 = rn0 * rn0;
+            rn_prev = rn0;
+            continue;
+        }
+        rn_prev = rn;
     }
     if (time_it) {
         INCRMT_CK(cudaEventRecord(ev1, stream));

@@ -48,6 +48,7 @@ public:
     double *rho = nullptr;          // device copy of a host density array
     double *bbuf = nullptr;          // device right-hand side (host solves, FEM zpr masking)
     double *zbuf = nullptr;          // device iterate for host solves
+    double *zsave = nullptr;         // warm start of a mixed-precision solve (its FP64 restart point)
     double *partial = nullptr;       // reduction partials
     double *ginv = nullptr;          // dense inverse of the coarsest level (FP64)
     float *ginvf = nullptr;          // and its FP32 copy
@@ -66,6 +67,7 @@ public:
     bool coarse_stale = true;
     long long coarse_builds = 0;
     long long coarse_retries = 0;    // solves repeated after rebuilding lagged coarse levels
+    long long mixed_fallbacks = 0;   // mixed-precision solves finished with FP64 V-cycles
     const double *lag_rho = nullptr; // density of the last set_density_lagged (read again on a retry)
     int lag_ld = 0;
     bool tiles = true;               // tile-fused smoothing where it applies

@@ -1416,6 +1416,7 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
     st->extrap_sweeps = S.ex_sweeps;
     st->coarse_builds = S.mac.coarse_builds + S.fem.coarse_builds;
     st->coarse_retries = S.mac.coarse_retries + S.fem.coarse_retries;
+    st->mixed_fallbacks = S.mac.mixed_fallbacks + S.fem.mixed_fallbacks;
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;
     st->time = S.time;

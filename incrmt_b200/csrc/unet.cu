@@ -1,11 +1,13 @@
 // The learned initial guess: a BF16 U-Net whose convolutions, pooling,
-// upsampling, loss and Adam update are this library's own kernels. Tensor
-// cores do the convolutions as implicit GEMMs (mma.sync m16n8k16, BF16 in,
-// FP32 accumulate): forward and input gradient share one kernel (the input
-// gradient is the forward convolution of the output gradient with the
-// flipped, transposed weights), the weight gradient is a second GEMM over
-// the pixels. Activations are NHWC with channel counts padded to multiples
-// of 16 so that every 16-channel slice of a pixel is one 32-byte load.
+// upsampling, loss and Adam update are this library's own kernels. The
+// convolutions' forward pass and input gradient run on the tcgen05 tensor
+// cores (conv_tc.cu: implicit GEMM, operands staged by TMA, FP32 accumulators
+// in tensor memory); the input gradient is the forward convolution of the
+// output gradient with the flipped, transposed weights, which are the forward
+// weights W[tap][Cin][Cout] read with the taps reversed. The weight gradient
+// is a GEMM over the pixels on mma.sync tensor-core instructions (BF16 in,
+// FP32 accumulate). Activations are NHWC with channel counts padded to
+// multiples of 16.
 #include <cuda_bf16.h>
 #include <cmath>
 #include <cstdint>
@@ -15,11 +17,13 @@
 #include <vector>
 #include "incrmt_unet.h"
 #include "common.cuh"
+#include "conv_tc.cuh"
 
 namespace incrmt {
-namespace {
 
 using bf16 = __nv_bfloat16;
+
+namespace {
 
 __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
     asm volatile(
@@ -32,81 +36,6 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
 /** Two BF16 values as one operand register, the first in the low half. */
 __device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
     return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
-}
-
-constexpr int kConvBM = 128;  // pixels per block of the convolution
-
-/** Y[p][co] = act(bias[co] + sum over taps and ci of X[p + off(tap)][ci] W[tap][ci][co]),
- * zero padding at the image borders. One block = 128 pixels x BN outputs,
- * eight warps of 16 pixels each; per K step the block stages 128 x 16 inputs
- * and BN x 16 weights in shared memory. Cin, Cout multiples of 16. */
-template <int TAPS, int BN, bool RELU>
-__global__ void __launch_bounds__(256) k_conv_fwd(const bf16 *__restrict__ X, const bf16 *__restrict__ Wt,
-                                                  const float *__restrict__ bias, bf16 *__restrict__ Y, int B, int H,
-                                                  int Wd, int Cin, int Cout) {
-    __shared__ __align__(16) bf16 As[kConvBM * 16];  // [pixel][k]
-    __shared__ __align__(16) bf16 Bs[BN * 16];       // [n][k]
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-    const long P = static_cast<long>(B) * H * Wd;
-    const long p0 = static_cast<long>(blockIdx.x) * kConvBM;
-    const int n0 = blockIdx.y * BN;
-    float acc[BN / 8][4];
-#pragma unroll
-    for (int a = 0; a < BN / 8; a++) acc[a][0] = acc[a][1] = acc[a][2] = acc[a][3] = 0.f;
-    const long pl = p0 + (tid >> 1);
-    const bool pvalid = pl < P;
-    int pb = 0, py = 0, px = 0;
-    if (pvalid) {
-        pb = static_cast<int>(pl / (static_cast<long>(H) * Wd));
-        const int r = static_cast<int>(pl - static_cast<long>(pb) * H * Wd);
-        py = r / Wd;
-        px = r - py * Wd;
-    }
-    const int ch = (tid & 1) * 8;
-    for (int tap = 0; tap < TAPS; tap++) {
-        const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
-        const int sy = py + dy, sx = px + dx;
-        const bool inb = pvalid && sy >= 0 && sy < H && sx >= 0 && sx < Wd;
-        const long xoff = inb ? ((static_cast<long>(pb) * H + sy) * Wd + sx) * Cin + ch : 0;
-        for (int c0 = 0; c0 < Cin; c0 += 16) {
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (inb) v = *reinterpret_cast<const uint4 *>(X + xoff + c0);
-            *reinterpret_cast<uint4 *>(&As[(tid >> 1) * 16 + ch]) = v;
-            for (int e = tid; e < BN * 16; e += 256) {
-                const int k = e / BN, n = e - k * BN;
-                Bs[n * 16 + k] = Wt[(static_cast<long>(tap) * Cin + c0 + k) * Cout + n0 + n];
-            }
-            __syncthreads();
-            const bf16 *ar = &As[warp * 16 * 16];
-            uint32_t a[4];
-            a[0] = *reinterpret_cast<const uint32_t *>(&ar[g * 16 + t4 * 2]);
-            a[1] = *reinterpret_cast<const uint32_t *>(&ar[(g + 8) * 16 + t4 * 2]);
-            a[2] = *reinterpret_cast<const uint32_t *>(&ar[g * 16 + t4 * 2 + 8]);
-            a[3] = *reinterpret_cast<const uint32_t *>(&ar[(g + 8) * 16 + t4 * 2 + 8]);
-#pragma unroll
-            for (int nt = 0; nt < BN / 8; nt++) {
-                const bf16 *br = &Bs[(nt * 8 + g) * 16];
-                uint32_t b[2];
-                b[0] = *reinterpret_cast<const uint32_t *>(&br[t4 * 2]);
-                b[1] = *reinterpret_cast<const uint32_t *>(&br[t4 * 2 + 8]);
-                mma_bf16_16816(acc[nt], a, b);
-            }
-            __syncthreads();
-        }
-    }
-#pragma unroll
-    for (int nt = 0; nt < BN / 8; nt++) {
-        const int n = n0 + nt * 8 + t4 * 2;
-        const float b0 = bias ? bias[n] : 0.f, b1 = bias ? bias[n + 1] : 0.f;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const long p = p0 + warp * 16 + g + h * 8;
-            if (p >= P) continue;
-            float v0 = acc[nt][2 * h] + b0, v1 = acc[nt][2 * h + 1] + b1;
-            if (RELU) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
-            *reinterpret_cast<__nv_bfloat162 *>(&Y[p * Cout + n]) = __floats2bfloat162_rn(v0, v1);
-        }
-    }
 }
 
 constexpr int kWgPix = 2048;  // pixels per block of the weight gradient
@@ -342,9 +271,10 @@ __global__ void k_adam(float *w, const float *g, float *m, float *v, long n, flo
     }
 }
 
-/** BF16 weights of one convolution and its flipped transpose
- * Wf[tap'][co][ci] = W[taps-1-tap'][ci][co] (the input-gradient convolution). */
-__global__ void k_weights_bf16(const float *w, bf16 *wb, bf16 *wf, int taps, int Cin, int Cout) {
+/** BF16 weights of one convolution, W[tap][ci][co] (the K-major operand of
+ * the input gradient, taps reversed), and its transpose Wt[tap][co][ci] (the
+ * K-major operand of the forward pass). */
+__global__ void k_weights_bf16(const float *w, bf16 *wb, bf16 *wt, int taps, int Cin, int Cout) {
     const long n = static_cast<long>(taps) * Cin * Cout;
     for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long>(gridDim.x) * blockDim.x) {
@@ -353,7 +283,7 @@ __global__ void k_weights_bf16(const float *w, bf16 *wb, bf16 *wf, int taps, int
         const int ci = static_cast<int>(r % Cin), tap = static_cast<int>(r / Cin);
         const bf16 v = __float2bfloat16(w[i]);
         wb[i] = v;
-        wf[(static_cast<long>(taps - 1 - tap) * Cout + co) * Cin + ci] = v;
+        wt[(static_cast<long>(tap) * Cout + co) * Cin + ci] = v;
     }
 }
 
@@ -361,7 +291,7 @@ struct Conv {
     int cin, cout, taps;
     bool relu;
     long woff, boff;  // offsets of weights [tap][cin][cout] and biases in the parameter vector
-    bf16 *w = nullptr, *wf = nullptr;
+    bf16 *w = nullptr, *wt = nullptr;
 };
 
 /** One activation tensor of the forward pass and its gradient. */
@@ -431,7 +361,7 @@ struct UNet {
         for (auto &c : convs) {
             const long n = static_cast<long>(c.taps) * c.cin * c.cout;
             c.w = wpool + o;
-            c.wf = wpool + o + n;
+            c.wt = wpool + o + n;
             o += 2 * n;
         }
         // He-uniform weights over the real fan-in (3 input channels in the first
@@ -459,7 +389,7 @@ struct UNet {
     int refresh_weights(cudaStream_t s) {
         for (auto &c : convs) {
             const long n = static_cast<long>(c.taps) * c.cin * c.cout;
-            k_weights_bf16<<<gs(n), 256, 0, s>>>(params + c.woff, c.w, c.wf, c.taps, c.cin, c.cout);
+            k_weights_bf16<<<gs(n), 256, 0, s>>>(params + c.woff, c.w, c.wt, c.taps, c.cin, c.cout);
             launches++;
         }
         INCRMT_CKL("k_weights_bf16");
@@ -507,33 +437,14 @@ struct UNet {
         return INCRMT_OK;
     }
 
-    template <int TAPS, bool RELU>
-    void conv_launch(const Conv &c, const bf16 *wgt, const float *bias, const bf16 *X, bf16 *Y, int cin, int cout,
-                     int B, int H, int W, cudaStream_t s) {
-        const long P = static_cast<long>(B) * H * W;
-        const unsigned gx = static_cast<unsigned>((P + kConvBM - 1) / kConvBM);
-        if (cout % 64 == 0)
-            k_conv_fwd<TAPS, 64, RELU><<<dim3(gx, cout / 64), 256, 0, s>>>(X, wgt, bias, Y, B, H, W, cin, cout);
-        else if (cout % 32 == 0)
-            k_conv_fwd<TAPS, 32, RELU><<<dim3(gx, cout / 32), 256, 0, s>>>(X, wgt, bias, Y, B, H, W, cin, cout);
-        else
-            k_conv_fwd<TAPS, 16, RELU><<<dim3(gx, cout / 16), 256, 0, s>>>(X, wgt, bias, Y, B, H, W, cin, cout);
+    int conv_forward(const Conv &c, const bf16 *X, bf16 *Y, int B, int H, int W, cudaStream_t s) {
         launches++;
-    }
-
-    void conv_forward(const Conv &c, const bf16 *X, bf16 *Y, int B, int H, int W, cudaStream_t s) {
-        const float *bias = params + c.boff;
-        if (c.taps == 9) {
-            if (c.relu) conv_launch<9, true>(c, c.w, bias, X, Y, c.cin, c.cout, B, H, W, s);
-            else conv_launch<9, false>(c, c.w, bias, X, Y, c.cin, c.cout, B, H, W, s);
-        } else {
-            conv_launch<1, false>(c, c.w, bias, X, Y, c.cin, c.cout, B, H, W, s);
-        }
+        return conv_tc(X, B, H, W, c.cin, c.wt, c.taps, c.cout, false, params + c.boff, c.relu, Y, s);
     }
 
     /** Gradients of one convolution: its output gradient gY (already masked
      * by the ReLU), input X; accumulates dW, db and writes gX (if given). */
-    void conv_backward(const Conv &c, const bf16 *X, const bf16 *gY, bf16 *gX, int B, int H, int W, cudaStream_t s) {
+    int conv_backward(const Conv &c, const bf16 *X, const bf16 *gY, bf16 *gX, int B, int H, int W, cudaStream_t s) {
         const long P = static_cast<long>(B) * H * W;
         const unsigned gx = static_cast<unsigned>((P + kWgPix - 1) / kWgPix);
         float *dW = grads + c.woff, *db = grads + c.boff;
@@ -550,9 +461,10 @@ struct UNet {
         k_bias_grad<<<dim3(64, (c.cout + 31) / 32), 256, 0, s>>>(gY, db, P, c.cout);
         launches += 2;
         if (gX) {
-            if (c.taps == 9) conv_launch<9, false>(c, c.wf, nullptr, gY, gX, c.cout, c.cin, B, H, W, s);
-            else conv_launch<1, false>(c, c.wf, nullptr, gY, gX, c.cout, c.cin, B, H, W, s);
+            launches++;
+            return conv_tc(gY, B, H, W, c.cout, c.w, c.taps, c.cin, true, nullptr, false, gX, s);
         }
+        return INCRMT_OK;
     }
 
     /** Forward pass; returns the head output activation. Act indices follow
@@ -574,9 +486,9 @@ struct UNet {
                 launches++;
                 cur = acts[a++].x;
             }
-            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            if ((r = conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s))) return r;
             cur = acts[a++].x;
-            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            if ((r = conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s))) return r;
             skip[l] = a;
             cur = acts[a++].x;
         }
@@ -586,12 +498,12 @@ struct UNet {
                 cur, acts[skip[l]].x, acts[a].x, B, Hl, Wl, C(l + 1), C(l));
             launches++;
             cur = acts[a++].x;
-            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            if ((r = conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s))) return r;
             cur = acts[a++].x;
-            conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s);
+            if ((r = conv_forward(convs[k++], cur, acts[a].x, B, Hl, Wl, s))) return r;
             cur = acts[a++].x;
         }
-        conv_forward(convs[k++], cur, acts[a].x, B, H, W, s);
+        if ((r = conv_forward(convs[k++], cur, acts[a].x, B, H, W, s))) return r;
         INCRMT_CKL("unet forward");
         return INCRMT_OK;
     }
@@ -599,6 +511,7 @@ struct UNet {
     /** Backward pass from the head gradient in acts.back().g; accumulates
      * into grads (zeroed by the caller). */
     int backward(int B, int H, int W, cudaStream_t s) {
+        int r;
         int a = static_cast<int>(acts.size()) - 1, k = static_cast<int>(convs.size()) - 1;
         // Recover the forward bookkeeping: indices of the skips.
         std::vector<int> skip(levels), pool_idx(levels, -1);
@@ -611,7 +524,7 @@ struct UNet {
             }
         }
         // Head.
-        conv_backward(convs[k], acts[a - 1].x, acts[a].g, acts[a - 1].g, B, H, W, s);
+        if ((r = conv_backward(convs[k], acts[a - 1].x, acts[a].g, acts[a - 1].g, B, H, W, s))) return r;
         k--;
         a--;
         // Decoder, finest first.
@@ -620,9 +533,9 @@ struct UNet {
             // acts[a] = conv2 output of this decoder level, acts[a-1] = conv1, acts[a-2] = cat
             const long n2 = static_cast<long>(B) * Hl * Wl * C(l);
             k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[a].g, acts[a].x, n2);
-            conv_backward(convs[k], acts[a - 1].x, acts[a].g, acts[a - 1].g, B, Hl, Wl, s);
+            if ((r = conv_backward(convs[k], acts[a - 1].x, acts[a].g, acts[a - 1].g, B, Hl, Wl, s))) return r;
             k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[a - 1].g, acts[a - 1].x, n2);
-            conv_backward(convs[k - 1], acts[a - 2].x, acts[a - 1].g, acts[a - 2].g, B, Hl, Wl, s);
+            if ((r = conv_backward(convs[k - 1], acts[a - 2].x, acts[a - 1].g, acts[a - 2].g, B, Hl, Wl, s))) return r;
             launches += 2;
             // Split the concatenation gradient: coarser level's output and the skip.
             const int lower = (l + 1 == levels - 1) ? skip[levels - 1] : a - 3;
@@ -639,9 +552,9 @@ struct UNet {
             const int o2 = skip[l], o1 = o2 - 1, in = (l > 0) ? pool_idx[l] : 0;
             const long n2 = static_cast<long>(B) * Hl * Wl * C(l);
             k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[o2].g, acts[o2].x, n2);
-            conv_backward(convs[2 * l + 1], acts[o1].x, acts[o2].g, acts[o1].g, B, Hl, Wl, s);
+            if ((r = conv_backward(convs[2 * l + 1], acts[o1].x, acts[o2].g, acts[o1].g, B, Hl, Wl, s))) return r;
             k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[o1].g, acts[o1].x, n2);
-            conv_backward(convs[2 * l], acts[in].x, acts[o1].g, l > 0 ? acts[in].g : nullptr, B, Hl, Wl, s);
+            if ((r = conv_backward(convs[2 * l], acts[in].x, acts[o1].g, l > 0 ? acts[in].g : nullptr, B, Hl, Wl, s))) return r;
             launches += 2;
             if (l > 0) {
                 // Pooling gradient into the finer level's output gradient.
@@ -747,6 +660,7 @@ static int unet_grad(incrmt_unet *h, int batch, int H, int W, const float *d_in,
     double hs[2];
     INCRMT_CK(cudaMemcpyAsync(hs, u.sums, sizeof(hs), cudaMemcpyDeviceToHost, s));
     INCRMT_CK(cudaStreamSynchronize(s));
+    if ((r = incrmt::conv_tc_status())) return r;
     if (loss) *loss = static_cast<float>(hs[1] > 0 ? hs[0] / hs[1] : 0.0);
     return INCRMT_OK;
 }
@@ -779,6 +693,15 @@ int incrmt_unet_gradients(incrmt_unet *h, int batch, int H, int W, const float *
 }
 
 long long incrmt_unet_launches(const incrmt_unet *h) { return h ? h->u.launches : 0; }
+
+int incrmt_conv_bf16(const void *d_x, int batch, int H, int W, int cin, const void *d_wk, int taps, int cout,
+                     int flip, const float *d_bias, int relu, void *d_y, void *stream) {
+    return incrmt::conv_tc(static_cast<const incrmt::bf16 *>(d_x), batch, H, W, cin,
+                           static_cast<const incrmt::bf16 *>(d_wk), taps, cout, flip != 0, d_bias, relu != 0,
+                           static_cast<incrmt::bf16 *>(d_y), static_cast<cudaStream_t>(stream));
+}
+
+int incrmt_conv_status(void) { return incrmt::conv_tc_status(); }
 
 void incrmt_unet_destroy(incrmt_unet *h) {
     if (!h) return;

@@ -111,15 +111,25 @@ def evolved(gpu, scene):
     g.close()
 
 
+# The stages of one step in the order of fluid_2d::step_forward
+# (fluid_2d.cc:298-369): the module's oracle advances through them, so each
+# stage starts from the state the previous ones left, as in a real step (the
+# MAC projection's source is only compatible with the walls once the edge
+# values have been through the second Godunov pass).
 STAGES = [
     ("normal_derivatives_velocity", ["normal_derivatives_velocity", "normal_derivatives_refmap"], 1e-11),
     ("godunov_tang", ["godunov_tang", "edge_boundary_conditions"], 1e-11),
+    ("tangential_derivatives", ["tangential_derivatives"], 1e-11),
     ("half_time_edge_velocities", ["half_time_edge_velocities", "half_time_edge_refmap"], 1e-11),
+    ("godunov", ["godunov", "edge_boundary_conditions"], 1e-11),
     ("mac_projection", ["mac_projection"], 1e-9),
     ("update_reference_map", ["update_reference_map"], 1e-11),
     ("pin", ["pin"], 1e-9),
+    ("set_boundaries", ["set_boundaries"], 1e-11),
     ("compute_stress", ["compute_stress"], 1e-11),
+    ("compute_ustar", ["compute_ustar"], 1e-11),
     ("finite_element_projection", ["finite_element_projection", "copy_pressure"], 1e-9),
+    ("update_velocity", ["update_velocity"], 1e-11),
     ("set_rho", ["set_rho"], 1e-11),
     ("build_band", ["build_band"], 1e-9),
     ("extrapolate", ["extrapolate"], 1e-11),
@@ -158,14 +168,19 @@ def test_collision_stress_active(evolved, scene):
 
 @needs_oracle
 def test_initial_band(gpu, scene):
-    """The bands built at initialisation agree to 0.03 dx: where the second-
-    order march is not causal (a point accepted below an already accepted
-    neighbour) the reference's heap order and the fixed point differ; the
-    statuses agree exactly."""
+    """The bands built at initialisation agree to a fraction of dx: where the
+    second-order march is not causal (a point accepted below an already
+    accepted neighbour) or meets exactly tied values (grid-aligned circles),
+    the reference's heap order and the fixed point differ; the statuses
+    agree exactly. Measured: 0.03 dx (circles_rod), 0.038 dx at the small
+    circle of the ellipses scene; the first pinning of the next step rebuilds
+    the band from the reference map, and the simple spin's end state at
+    t = 2 pi (test_endstate_gpu.py) shows no trace of such differences."""
     r, g, dt = _pair(SCENES[scene])
     dx = 2.0 / M
+    tol = {"circles_rod": 0.03, "ellipses": 0.05}[scene]
     for k in range(g.objects):
-        assert np.abs(g.get("phi", k) - r.get("phi", k)).max() <= 0.03 * dx, k
+        assert np.abs(g.get("phi", k) - r.get("phi", k)).max() <= tol * dx, k
         assert np.array_equal(g.get("status", k), r.get("status", k)), k
     r.close()
     g.close()

@@ -126,6 +126,17 @@ int incrmt_sim_get_learned_stats(incrmt_sim *h, int sys, incrmt_sim_learned_stat
 int incrmt_conv_bf16(const void *d_x, int batch, int H, int W, int cin, const void *d_wk, int taps, int cout,
                      int flip, const float *d_bias, int relu, void *d_y, void *stream);
 
+/** Weight gradient of such a convolution on the tcgen05 tensor cores:
+ * d_dw[tap][cin][cout] (FP32) += sum over the pixels of
+ * x[p + offset(tap)][ci] * dy[p][co] (x the layer's input, dy the gradient
+ * of its output, NHWC BF16). The pixels are split over CTAs whose FP32
+ * partial sums go to d_work (incrmt_conv_wgrad_workspace floats) and are
+ * then added to d_dw in a fixed order: the result is the same on every run.
+ * Issued on `stream`, not waited for. */
+long long incrmt_conv_wgrad_workspace(int batch, int H, int W, int cin, int cout, int taps);
+int incrmt_conv_wgrad_bf16(const void *d_x, const void *d_dy, int batch, int H, int W, int cin, int cout, int taps,
+                           float *d_dw, float *d_work, long long work_floats, void *stream);
+
 /** INCRMT_OK, or INCRMT_ERR_CUDA when a tensor-core convolution gave up one
  * of its pipeline waits (each is limited to one second) since the last call;
  * clears that record. Synchronises the device. */

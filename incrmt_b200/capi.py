@@ -646,6 +646,9 @@ def _unet_sigs(L):
     L.incrmt_unet_gradients.argtypes = [P, I, I, I, P, P, P, fp, fp, P]
     L.incrmt_conv_bf16.argtypes = [P, I, I, I, I, P, I, I, I, P, I, P, P]
     L.incrmt_conv_status.argtypes = []
+    L.incrmt_conv_wgrad_workspace.argtypes = [I, I, I, I, I, I]
+    L.incrmt_conv_wgrad_workspace.restype = ctypes.c_longlong
+    L.incrmt_conv_wgrad_bf16.argtypes = [P, P, I, I, I, I, I, I, P, P, ctypes.c_longlong, P]
     L.incrmt_unet_launches.argtypes = [P]
     L.incrmt_unet_launches.restype = ctypes.c_longlong
     L.incrmt_unet_destroy.argtypes = [P]
@@ -737,6 +740,18 @@ def conv_bf16(x_ptr, batch, H, W, cin, wk_ptr, taps, cout, y_ptr, bias_ptr=0, re
     check(_ulib().incrmt_conv_bf16(ctypes.c_void_p(x_ptr), batch, H, W, cin, ctypes.c_void_p(wk_ptr), taps, cout,
                                    int(flip), ctypes.c_void_p(bias_ptr or None), int(relu), ctypes.c_void_p(y_ptr),
                                    ctypes.c_void_p(stream)))
+
+
+def conv_wgrad_workspace(batch, H, W, cin, cout, taps):
+    """Floats of workspace the tensor-core weight gradient needs."""
+    return int(_ulib().incrmt_conv_wgrad_workspace(batch, H, W, cin, cout, taps))
+
+
+def conv_wgrad_bf16(x_ptr, dy_ptr, batch, H, W, cin, cout, taps, dw_ptr, work_ptr, work_floats, stream=0):
+    """dW += the weight gradient of one convolution (incrmt_conv_wgrad_bf16)."""
+    check(_ulib().incrmt_conv_wgrad_bf16(ctypes.c_void_p(x_ptr), ctypes.c_void_p(dy_ptr), batch, H, W, cin, cout,
+                                         taps, ctypes.c_void_p(dw_ptr), ctypes.c_void_p(work_ptr), int(work_floats),
+                                         ctypes.c_void_p(stream)))
 
 
 def conv_status():

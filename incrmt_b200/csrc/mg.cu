@@ -553,6 +553,7 @@ __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const 
                                                        const double *P) {
     constexpr int CTW = 32, CTH = 8, RW = 2 * CTW + 1, RH = 2 * CTH + 1;
     __shared__ T rs[RW * RH];
+    __shared__ double ps[4 * RW * RH];  // the region's prolongation weights (zero outside the grid)
     const int X0 = blockIdx.x * CTW, Y0 = blockIdx.y * CTH;
     const int FX0 = kx ? 2 * X0 - 1 : X0, FY0 = ky ? 2 * Y0 - 1 : Y0;
     const int FW = kx ? RW : CTW, FH = ky ? RH : CTH;
@@ -564,11 +565,15 @@ __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const 
         bool ok = fxu <= fxmax && fyu <= fymax;
         const int fx = wrap_idx(fxu, fm, px, ok), fy = wrap_idx(fyu, fn, py, ok);
         T r = 0;
+        double w0 = 0, w1 = 0, w2 = 0, w3 = 0;
         if (ok) {
             const int f = fx + fm * fy;
             r = residual_at(op, fx, fy, z, b[f]);
+            const double *q = P + 4 * static_cast<long>(f);
+            w0 = q[0]; w1 = q[1]; w2 = q[2]; w3 = q[3];
         }
         rs[t] = r;
+        ps[4 * t] = w0; ps[4 * t + 1] = w1; ps[4 * t + 2] = w2; ps[4 * t + 3] = w3;
     }
     __syncthreads();
     const int I = X0 + (threadIdx.x & 31), J = Y0 + (threadIdx.x >> 5);
@@ -579,9 +584,13 @@ __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const 
     T t = 0;
     for (int fj = y0; fj <= y1; fj++)
         for (int fi = x0; fi <= x1; fi++) {
-            const T w = static_cast<T>(pweight(P, fm, fn, px, py, kx, ky, fi, fj, I, J));
+            // pweight(fi, fj, I, J) from the staged weights
+            const int qx = I - base_of(fi, kx), qy = J - base_of(fj, ky);
+            if (qx < 0 || qx > 1 || qy < 0 || qy > 1) continue;
+            const int lt = (fi - FX0) + FW * (fj - FY0);
+            const T w = static_cast<T>(ps[4 * lt + qx + 2 * qy]);
             if (w == 0) continue;
-            t = add_prod(t, w, rs[(fi - FX0) + FW * (fj - FY0)]);
+            t = add_prod(t, w, rs[lt]);
         }
     bc[I + cm * J] = t;
     zc[I + cm * J] = 0;
@@ -930,6 +939,25 @@ __global__ void k_reduce(const double *partial, int nb, double *out) {
     if (threadIdx.x == 0) *out = acc;
 }
 
+/** Per-block sums of an FP32 array, accumulated in FP64. */
+__global__ void k_sum_f32(const float *a, long N, double *partial) {
+    double acc = 0;
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x)
+        acc += static_cast<double>(a[q]);
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+/** z += e - mean(e), the mean from the sum in *sum (a correction of a
+ * singular system, defined up to a constant). */
+__global__ void k_add_f32_centred(double *z, const float *e, long N, const double *sum) {
+    const double mean = *sum / static_cast<double>(N);
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x)
+        z[q] += static_cast<double>(e[q]) - mean;
+}
+
 __global__ void k_add_f32(double *z, const float *e, long N) {
     for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
          q += static_cast<long>(gridDim.x) * blockDim.x)
@@ -1162,7 +1190,6 @@ void Multigrid::destroy() {
     lev.clear();
     cudaFree(ex); cudaFree(ey); cudaFree(exf); cudaFree(eyf); cudaFree(c); cudaFree(cf);
     cudaFree(rho); cudaFree(bbuf); cudaFree(zbuf); cudaFree(partial); cudaFree(dnorm);
-    cudaFree(zsave); zsave = nullptr;
     cudaFree(ginv); cudaFree(ginvf); ginv = nullptr; ginvf = nullptr;
 
     if (hnorm) cudaFreeHost(hnorm);
@@ -1406,13 +1433,15 @@ int Multigrid::cycle32(int l) {
     const MgLevel &C = lev[l + 1];
     int r;
     float *cur = z;  // as in cycle64
+    Multigrid *pf = prof ? this : nullptr;
+    const double bpu = 4.0 * (sys == INCRMT_SYS_MAC ? 5 : 4);  // FP32 words: z, b, coefficients in; z out
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac32();
-        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else if (l == 0) {
         auto op = fem32();
-        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else {
         if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
@@ -1425,8 +1454,8 @@ int Multigrid::cycle32(int l) {
     launches++;
     INCRMT_CKL("k_prolong");
     float *alt = !tiles ? nullptr : cur == z ? L.zf2 : z, *out = cur;
-    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
-    else if (l == 0) r = smooth(fem32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
+    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
+    else if (l == 0) r = smooth(fem32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
     else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
     if (r) return r;
     if (out != z) INCRMT_CK(cudaMemcpyAsync(z, out, sizeof(float) * L.N, cudaMemcpyDeviceToDevice, stream));
@@ -1524,8 +1553,19 @@ int Multigrid::vcycle_and_norm(int prec, const double *b, double *d_z, long N) {
         k_fill<float><<<nbk, 256, 0, stream>>>(lev[0].zf, N, 0.f);
         launches++;
         if ((r = cycle32(0))) return r;
-        k_add_f32<<<nbk, 256, 0, stream>>>(d_z, lev[0].zf, N);
-        launches++;
+        if (zpr) {
+            k_add_f32<<<nbk, 256, 0, stream>>>(d_z, lev[0].zf, N);
+            launches++;
+        } else {
+            // Without the zero-pressure edge both systems are singular (the
+            // constants): the FP32 cycle's correction comes back with a
+            // constant part thousands of times its variation on the finest
+            // grids, which the iterate would accumulate; it is removed.
+            k_sum_f32<<<nbk, 256, 0, stream>>>(lev[0].zf, N, partial);
+            k_reduce<<<1, 256, 0, stream>>>(partial, nbk, dnorm + 1);
+            k_add_f32_centred<<<nbk, 256, 0, stream>>>(d_z, lev[0].zf, N, dnorm + 1);
+            launches += 3;
+        }
         INCRMT_CKL("defect correction");
         if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
     }
@@ -1611,14 +1651,10 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
     }
     bool conv = false, finite = true;
     double rn_prev = 0;
-    double rn0 = 0;
     if (prec == INCRMT_PREC_MIXED) {
-        // the warm start is kept: a fallback to FP64 restarts from it
-        if (!zsave) INCRMT_CK(cudaMalloc(&zsave, sizeof(double) * N));
-        INCRMT_CK(cudaMemcpyAsync(zsave, d_z, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
         if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
         if ((r = fetch_norm(&rn2))) return r;
-        rn_prev = rn0 = std::sqrt(rn2);
+        rn_prev = std::sqrt(rn2);
     }
     // One V-cycle, its residual norm and the read-back of that norm, captured
     // once into a CUDA graph per (precision, b, z) and replayed per cycle.
@@ -1659,18 +1695,12 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         if (rn <= tol) { conv = true; break; }
         // An FP32 correction that does not halve the FP64 residual means the
         // single-precision cycle no longer approximates the system's inverse
-        // well enough for defect correction to converge: the solve restarts
-        // from its warm start with FP64 V-cycles (the FP32 corrections may
-        // have moved the iterate along the null space of a singular system
-        // far enough to spoil the FP64 residual's accuracy).
+        // well enough for defect correction to converge: the rest of the
+        // solve runs FP64 V-cycles from the current iterate.
         if (cur == INCRMT_PREC_MIXED && rn > kMixedContraction * rn_prev) {
             cur = INCRMT_PREC_FP64;
             mixed_fallbacks++;
-            INCRMT_CK(cudaMemcpyAsync(d_z, zsave, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream));
             if (use_graph && (r = capture())) return r;
-            rn2 = rn0 * rn0;
-            rn_prev = rn0;
-            continue;
         }
         rn_prev = rn;
     }

@@ -48,7 +48,6 @@ public:
     double *rho = nullptr;          // device copy of a host density array
     double *bbuf = nullptr;          // device right-hand side (host solves, FEM zpr masking)
     double *zbuf = nullptr;          // device iterate for host solves
-    double *zsave = nullptr;         // warm start of a mixed-precision solve (its FP64 restart point)
     double *partial = nullptr;       // reduction partials
     double *ginv = nullptr;          // dense inverse of the coarsest level (FP64)
     float *ginvf = nullptr;          // and its FP32 copy

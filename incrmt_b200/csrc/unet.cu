@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <random>
 #include <vector>
@@ -25,106 +26,35 @@ using bf16 = __nv_bfloat16;
 
 namespace {
 
-__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
+constexpr int kBiasSplits = 64;  // pixel ranges of the bias gradient's partial sums
 
-/** Two BF16 values as one operand register, the first in the low half. */
-__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
-    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
-}
-
-constexpr int kWgPix = 2048;  // pixels per block of the weight gradient
-
-/** dW[tap][ci][co] += sum over pixels of X[p + off(tap)][ci] dY[p][co], for one
- * tap (blockIdx.z), 16 input channels (blockIdx.y / (Cout/BN)) and BN output
- * channels, over kWgPix pixels (blockIdx.x). Each warp walks 16-pixel steps,
- * staging 16 x 16 inputs and 16 x BN output gradients in its own shared
- * slice; the warps' partial sums meet in shared memory (shared atomics) and
- * one FP32 atomic per weight leaves the block, so the sums' order, and with
- * it the last bits of the gradient, vary from run to run. */
-template <int TAPS, int BN>
-__global__ void __launch_bounds__(256) k_conv_wgrad(const bf16 *__restrict__ X, const bf16 *__restrict__ dY,
-                                                    float *__restrict__ dW, int B, int H, int Wd, int Cin, int Cout) {
-    __shared__ __align__(16) bf16 Xs[8][16 * 16];   // per warp [pixel][ci]
-    __shared__ __align__(16) bf16 Ds[8][16 * BN];   // per warp [pixel][co]
-    __shared__ float red[16 * BN];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-    const int tap = blockIdx.z, ntile = Cout / BN;
-    const int ci0 = (blockIdx.y / ntile) * 16, co0 = (blockIdx.y % ntile) * BN;
-    const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
-    const long P = static_cast<long>(B) * H * Wd;
-    const long pbeg = static_cast<long>(blockIdx.x) * kWgPix;
-    const long pend = pbeg + kWgPix < P ? pbeg + kWgPix : P;
-    float acc[BN / 8][4];
-#pragma unroll
-    for (int a = 0; a < BN / 8; a++) acc[a][0] = acc[a][1] = acc[a][2] = acc[a][3] = 0.f;
-    for (long ps = pbeg + warp * 16; ps < pend; ps += 8 * 16) {
-        // Stage: lane l loads pixel ps + l/2, input channels ci0 + (l&1)*8 .. +7
-        {
-            const long p = ps + (lane >> 1);
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (p < pend) {
-                const int b = static_cast<int>(p / (static_cast<long>(H) * Wd));
-                const int r = static_cast<int>(p - static_cast<long>(b) * H * Wd), y = r / Wd, x = r - y * Wd;
-                const int sy = y + dy, sx = x + dx;
-                if (sy >= 0 && sy < H && sx >= 0 && sx < Wd)
-                    v = *reinterpret_cast<const uint4 *>(X + ((static_cast<long>(b) * H + sy) * Wd + sx) * Cin + ci0 +
-                                                         (lane & 1) * 8);
-            }
-            *reinterpret_cast<uint4 *>(&Xs[warp][(lane >> 1) * 16 + (lane & 1) * 8]) = v;
-        }
-        for (int e = lane; e < 16 * BN / 8; e += 32) {
-            const int pr = e / (BN / 8), c8 = (e - pr * (BN / 8)) * 8;
-            const long p = ps + pr;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (p < pend) v = *reinterpret_cast<const uint4 *>(dY + p * Cout + co0 + c8);
-            *reinterpret_cast<uint4 *>(&Ds[warp][pr * BN + c8]) = v;
-        }
-        __syncwarp();
-        const bf16 *xs = Xs[warp], *ds = Ds[warp];
-        uint32_t a[4];
-        a[0] = pack2(xs[(t4 * 2) * 16 + g], xs[(t4 * 2 + 1) * 16 + g]);
-        a[1] = pack2(xs[(t4 * 2) * 16 + g + 8], xs[(t4 * 2 + 1) * 16 + g + 8]);
-        a[2] = pack2(xs[(t4 * 2 + 8) * 16 + g], xs[(t4 * 2 + 9) * 16 + g]);
-        a[3] = pack2(xs[(t4 * 2 + 8) * 16 + g + 8], xs[(t4 * 2 + 9) * 16 + g + 8]);
-#pragma unroll
-        for (int nt = 0; nt < BN / 8; nt++) {
-            uint32_t b[2];
-            b[0] = pack2(ds[(t4 * 2) * BN + nt * 8 + g], ds[(t4 * 2 + 1) * BN + nt * 8 + g]);
-            b[1] = pack2(ds[(t4 * 2 + 8) * BN + nt * 8 + g], ds[(t4 * 2 + 9) * BN + nt * 8 + g]);
-            mma_bf16_16816(acc[nt], a, b);
-        }
-        __syncwarp();
-    }
-    for (int e = tid; e < 16 * BN; e += 256) red[e] = 0.f;
-    __syncthreads();
-#pragma unroll
-    for (int nt = 0; nt < BN / 8; nt++) {
-        atomicAdd(&red[g * BN + nt * 8 + t4 * 2], acc[nt][0]);
-        atomicAdd(&red[g * BN + nt * 8 + t4 * 2 + 1], acc[nt][1]);
-        atomicAdd(&red[(g + 8) * BN + nt * 8 + t4 * 2], acc[nt][2]);
-        atomicAdd(&red[(g + 8) * BN + nt * 8 + t4 * 2 + 1], acc[nt][3]);
-    }
-    __syncthreads();
-    for (int e = tid; e < 16 * BN; e += 256) {
-        const int ci = e / BN, co = e - ci * BN;
-        atomicAdd(&dW[(static_cast<long>(tap) * Cin + ci0 + ci) * Cout + co0 + co], red[e]);
-    }
-}
-
-/** dbias[c] += sum over pixels of dY[p][c]; 256 threads = 32 channels x 8 rows. */
-__global__ void k_bias_grad(const bf16 *dY, float *db, long P, int C) {
+/** Partial bias gradients: partial[split][c] = sum of dY[p][c] over the
+ * pixels of split blockIdx.x (every eighth pixel per thread row, then a
+ * fixed-order sum over the eight rows), channels blockIdx.y*32 .. +31. */
+__global__ void k_bias_partial(const bf16 *dY, float *partial, long P, int C) {
+    __shared__ float red[8][33];
     const int c = blockIdx.y * 32 + (threadIdx.x & 31), r = threadIdx.x >> 5;
-    if (c >= C) return;
+    const long per = (P + gridDim.x - 1) / gridDim.x;
+    const long p0 = blockIdx.x * per, p1 = p0 + per < P ? p0 + per : P;
     float s = 0;
-    for (long p = static_cast<long>(blockIdx.x) * 8 + r; p < P; p += static_cast<long>(gridDim.x) * 8)
-        s += __bfloat162float(dY[p * C + c]);
-    atomicAdd(&db[c], s);
+    if (c < C)
+        for (long p = p0 + r; p < p1; p += 8) s += __bfloat162float(dY[p * C + c]);
+    red[r][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (r == 0 && c < C) {
+        float t = 0;
+        for (int q = 0; q < 8; q++) t += red[q][threadIdx.x & 31];
+        partial[static_cast<long>(blockIdx.x) * C + c] = t;
+    }
+}
+
+/** db[c] += the splits' partials in split order. */
+__global__ void k_bias_reduce(const float *partial, int splits, int C, float *db) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+        float t = 0;
+        for (int sp = 0; sp < splits; sp++) t += partial[static_cast<long>(sp) * C + c];
+        db[c] += t;
+    }
 }
 
 /** Gradient through the ReLU: zero where the layer's output is not positive. */
@@ -319,6 +249,8 @@ struct UNet {
     int wb = 0, wh = 0, ww = 0;
     std::vector<Act> acts;
     std::vector<void *> work;
+    float *part = nullptr;  // weight- and bias-gradient partials
+    size_t part_n = 0;
     double *sums = nullptr;
 
     int C(int l) const { return base << l; }
@@ -399,6 +331,9 @@ struct UNet {
     void free_work() {
         for (void *p : work) cudaFree(p);
         work.clear();
+        cudaFree(part);
+        part = nullptr;
+        part_n = 0;
         acts.clear();
         wb = wh = ww = 0;
     }
@@ -433,6 +368,26 @@ struct UNet {
             if ((r = alloc(l, C(l)))) return r;
         }
         if ((r = alloc(0, 16))) return r;  // head output
+        // partials of the largest weight gradient (and of the bias gradients)
+        size_t need = 0;
+        {
+            int k = 0;
+            for (int l = 0; l < levels; l++)
+                for (int q = 0; q < 2; q++, k++) {
+                    const Conv &c = convs[k];
+                    need = std::max(need, conv_tc_wgrad_workspace(B, H >> l, W >> l, c.cin, c.cout, c.taps));
+                }
+            for (int l = levels - 2; l >= 0; l--)
+                for (int q = 0; q < 2; q++, k++) {
+                    const Conv &c = convs[k];
+                    need = std::max(need, conv_tc_wgrad_workspace(B, H >> l, W >> l, c.cin, c.cout, c.taps));
+                }
+            const Conv &c = convs[k];
+            need = std::max(need, conv_tc_wgrad_workspace(B, H, W, c.cin, c.cout, c.taps));
+            need = std::max(need, static_cast<size_t>(kBiasSplits) * (base << (levels - 1)));
+        }
+        INCRMT_CK(cudaMalloc(&part, sizeof(float) * need));
+        part_n = need;
         wb = B; wh = H; ww = W;
         return INCRMT_OK;
     }
@@ -446,20 +401,13 @@ struct UNet {
      * by the ReLU), input X; accumulates dW, db and writes gX (if given). */
     int conv_backward(const Conv &c, const bf16 *X, const bf16 *gY, bf16 *gX, int B, int H, int W, cudaStream_t s) {
         const long P = static_cast<long>(B) * H * W;
-        const unsigned gx = static_cast<unsigned>((P + kWgPix - 1) / kWgPix);
         float *dW = grads + c.woff, *db = grads + c.boff;
-        if (c.taps == 9) {
-            if (c.cout % 64 == 0)
-                k_conv_wgrad<9, 64><<<dim3(gx, (c.cin / 16) * (c.cout / 64), 9), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
-            else if (c.cout % 32 == 0)
-                k_conv_wgrad<9, 32><<<dim3(gx, (c.cin / 16) * (c.cout / 32), 9), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
-            else
-                k_conv_wgrad<9, 16><<<dim3(gx, (c.cin / 16) * (c.cout / 16), 9), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
-        } else {
-            k_conv_wgrad<1, 16><<<dim3(gx, (c.cin / 16) * (c.cout / 16), 1), 256, 0, s>>>(X, gY, dW, B, H, W, c.cin, c.cout);
-        }
-        k_bias_grad<<<dim3(64, (c.cout + 31) / 32), 256, 0, s>>>(gY, db, P, c.cout);
-        launches += 2;
+        int r = conv_tc_wgrad(X, gY, B, H, W, c.cin, c.cout, c.taps, dW, part, part_n, s);
+        if (r) return r;
+        k_bias_partial<<<dim3(kBiasSplits, (c.cout + 31) / 32), 256, 0, s>>>(gY, part, P, c.cout);
+        k_bias_reduce<<<1, 256, 0, s>>>(part, kBiasSplits, c.cout, db);
+        launches += 4;
+        INCRMT_CKL("bias gradient");
         if (gX) {
             launches++;
             return conv_tc(gY, B, H, W, c.cout, c.w, c.taps, c.cin, true, nullptr, false, gX, s);
@@ -702,6 +650,19 @@ int incrmt_conv_bf16(const void *d_x, int batch, int H, int W, int cin, const vo
 }
 
 int incrmt_conv_status(void) { return incrmt::conv_tc_status(); }
+
+long long incrmt_conv_wgrad_workspace(int batch, int H, int W, int cin, int cout, int taps) {
+    if (batch < 1 || H < 1 || W < 1 || cin < 16 || cout < 16 || (taps != 1 && taps != 9)) return 0;
+    return static_cast<long long>(incrmt::conv_tc_wgrad_workspace(batch, H, W, cin, cout, taps));
+}
+
+int incrmt_conv_wgrad_bf16(const void *d_x, const void *d_dy, int batch, int H, int W, int cin, int cout, int taps,
+                           float *d_dw, float *d_work, long long work_floats, void *stream) {
+    if (work_floats < 0) { incrmt::set_error("negative workspace size"); return INCRMT_ERR_BADARG; }
+    return incrmt::conv_tc_wgrad(static_cast<const incrmt::bf16 *>(d_x), static_cast<const incrmt::bf16 *>(d_dy),
+                                 batch, H, W, cin, cout, taps, d_dw, d_work, static_cast<size_t>(work_floats),
+                                 static_cast<cudaStream_t>(stream));
+}
 
 void incrmt_unet_destroy(incrmt_unet *h) {
     if (!h) return;

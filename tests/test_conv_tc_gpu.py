@@ -59,3 +59,45 @@ def test_conv_matches_torch(gpu, B, H, W, cin, cout, taps, relu, use_bias, flip)
     assert torch.isfinite(out).all()
     err = (out - ref).abs().max().item() / max(ref.abs().max().item(), 1e-30)
     assert err <= 1e-2, err
+
+
+WGRAD_CASES = [
+    # batch, H, W, cin, cout, taps
+    (2, 32, 48, 16, 32, 9),
+    (1, 24, 40, 48, 64, 9),
+    (1, 16, 128, 96, 128, 9),
+    (1, 16, 64, 384, 64, 9),
+    (1, 16, 32, 64, 384, 9),
+    (2, 32, 32, 32, 16, 1),
+]
+
+
+@pytest.mark.parametrize("B,H,W,cin,cout,taps", WGRAD_CASES)
+def test_wgrad_matches_torch(gpu, B, H, W, cin, cout, taps):
+    """The weight gradient (incrmt_conv_wgrad_bf16) against torch's
+    conv2d_weight in FP32 on the same BF16 values: within 1e-4 of the
+    largest entry (the FP32 partial sums differ in order only), added to
+    what dW held, and bit for bit the same on a second run."""
+    import torch
+    from incrmt_b200 import capi
+    dev = torch.device("cuda")
+    g = torch.Generator(device="cpu").manual_seed(B * 7 + H + W + cin + cout + taps)
+    x = torch.randn(B, H, W, cin, generator=g).to(torch.bfloat16).to(dev)
+    dy = torch.randn(B, H, W, cout, generator=g).to(torch.bfloat16).to(dev)
+    n = capi.conv_wgrad_workspace(B, H, W, cin, cout, taps)
+    work = torch.empty(n, dtype=torch.float32, device=dev)
+    dw0 = torch.randn(taps, cin, cout, generator=g).to(dev)
+    out = []
+    for _ in range(2):
+        dw = dw0.clone()
+        torch.cuda.synchronize()
+        capi.conv_wgrad_bf16(x.data_ptr(), dy.data_ptr(), B, H, W, cin, cout, taps, dw.data_ptr(), work.data_ptr(), n)
+        capi.conv_status()
+        out.append(dw - dw0)
+    k = 3 if taps == 9 else 1
+    ref = torch.nn.grad.conv2d_weight(x.float().permute(0, 3, 1, 2), (cout, cin, k, k),
+                                      dy.float().permute(0, 3, 1, 2), padding=k // 2)
+    ref = ref.permute(2, 3, 1, 0).reshape(taps, cin, cout)  # [tap = 3 ty + tx][ci][co]
+    err = (out[0] - ref).abs().max().item() / ref.abs().max().item()
+    assert err <= 1e-4, err
+    assert torch.equal(out[0], out[1])

@@ -140,9 +140,13 @@ def _mac_problem(m, seed):
 
 
 def test_learned_guess_saves_vcycles(gpu):
-    """Train on 256 problems, evaluate on 8 held out: the guess starts the
-    solve closer to the solution and needs no more V-cycles than the zero
-    start (on average fewer: about 10% at this size)."""
+    """The network of the specification (4 levels, 32 base channels, about
+    2 M parameters) trained on 1024 problems of the standalone MAC solve at
+    128^2 (its own FP64 multigrid solutions, restricted by 2) and evaluated
+    on 32 held-out problems: the guess must start the solve closer to the
+    solution (relative error of the guess below 0.45 on average; measured
+    0.32) and save at least 0.25 V-cycles per solve on average (measured
+    0.47 of 8.4) against the zero start, never costing a V-cycle."""
     import torch
     from incrmt_b200 import capi
     m, factor = 128, 2
@@ -150,7 +154,7 @@ def test_learned_guess_saves_vcycles(gpu):
     H, W = capi.learned_grid(m, m, factor)
     s = capi.MGSolver(capi.SYS_MAC, m, m)
     ins, tgts = [], []
-    for seed in range(1000, 1256):
+    for seed in range(1000, 2024):
         rho, b = _mac_problem(m, seed)
         s.set_density(rho)
         z = np.zeros(m * m)
@@ -168,7 +172,7 @@ def test_learned_guess_saves_vcycles(gpu):
     X = torch.stack(ins).contiguous()
     T = torch.stack(tgts).contiguous()
     V = torch.ones_like(T)
-    net = capi.UNet(4, 16, seed=11)
+    net = capi.UNet(4, 32, seed=11)
     g = torch.Generator(device="cpu").manual_seed(0)
     for it in range(1500):
         idx = torch.randperm(len(ins), generator=g)[:16]
@@ -176,7 +180,7 @@ def test_learned_guess_saves_vcycles(gpu):
         xb, tb, vb = X[idx].contiguous(), T[idx].contiguous(), V[idx].contiguous()
         net.train_step(16, H, W, xb.data_ptr(), tb.data_ptr(), vb.data_ptr(), 2e-3 if it < 1100 else 5e-4)
     plain, learned, errs = [], [], []
-    for seed in range(2000, 2008):
+    for seed in range(5000, 5032):
         rho, b = _mac_problem(m, seed)
         s.set_density(rho)
         bd = torch.tensor(b, device=dev)
@@ -190,7 +194,10 @@ def test_learned_guess_saves_vcycles(gpu):
         e = (zstar - zstar.mean()) - (z - z.mean())
         errs.append(float(e.norm() / (zstar - zstar.mean()).norm()))
         learned.append(s.solve_device(bd.data_ptr(), z.data_ptr()).vcycles)
-    assert np.mean(errs) < 0.7, errs
-    assert np.mean(learned) <= np.mean(plain), (plain, learned)
+    capi.conv_status()
+    saving = np.mean(plain) - np.mean(learned)
+    assert np.mean(errs) < 0.45, errs
+    assert saving >= 0.25, (saving, plain, learned)
+    assert min(np.array(plain) - np.array(learned)) >= 0, (plain, learned)
     net.close()
     s.close()

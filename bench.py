@@ -869,6 +869,8 @@ def run_ours(args, ws, rank, local, dist):
     # and when one is freed torch's pinned-memory allocator records an event
     # on every stream that used it, so they go first, while the solver (which
     # owns the stream) is still alive.
+    h2d_bytes = int(rho_h.numel() * 8 + (1 if net is not None else 2) * b_h.numel() * 8)
+    d2h_bytes = int(b_h.numel() * 8)
     del rho_np, b_np, z_np, rho_h, b_h, z_h
     torch.cuda.synchronize()
     import gc
@@ -911,8 +913,7 @@ def run_ours(args, ws, rank, local, dist):
                               "updated unknowns x 2 sweeps x (3+c) x w, c=2 (MAC)"),
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "steps/s",
-                "h2d_bytes_per_step": int(rho_h.numel() * 8 + (1 if net is not None else 2) * b_h.numel() * 8),
-                "d2h_bytes_per_step": int(b_h.numel() * 8)},
+                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

@@ -138,65 +138,41 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-constexpr int kConvThreads = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
-
-/** The persistent convolution kernel. CTA c processes the output tiles c,
- * c + gridDim.x, ... of the (pixel tile, output-channel chunk) grid; per
- * tile the K loop runs over (tap, channel chunk). Warp 4 (one thread)
- * streams the stages through a ring of S shared-memory buffers across tile
- * boundaries; warp 5 (one thread) issues the MMAs into one of two tensor-
- * memory accumulators (tile parity), so that warps 0-3 can read and store
- * one tile while the next one accumulates. Barriers: full[s] / empty[s] of
- * the ring, tfull[b] (accumulator b complete, from tcgen05.commit) and
- * tempty[b] (accumulator b read, one arrival per epilogue warp), drain (all
- * issued MMAs complete). A wait that gives up sets the shared abort flag,
- * which every role checks, so the CTA winds down: the producer waits for
- * its copies in flight and the MMA thread for its MMAs before the tensor
- * memory is freed. Dynamic shared memory: 1024 + S (128 + N) KC 2 bytes of
- * stages, then 2S + 5 barriers, the abort flag and the tensor-memory
+/** The convolution kernel (see the file comment); blockIdx.y selects the
+ * output channels n0 = N * blockIdx.y .. n0 + N - 1 of ldy. Dynamic shared
+ * memory: 1024 (alignment) + S * (128 + N) * KC * 2 bytes of stage buffers,
+ * then 2S + 1 barriers (full[S], empty[S], done) and the tensor-memory
  * address. */
 template <int TAPS, int KC>
-__global__ void __launch_bounds__(kConvThreads, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
               const float *__restrict__ bias, bf16 *__restrict__ Y, int H, int W, int N, int ldy, int Wt, int Ht,
-              int tiles_x, int tiles_y, int ntiles, int ntn, int nck, int flip, int relu, int S, uint32_t cols) {
+              int tiles_x, int tiles_y, int nck, int flip, int relu, int S, uint32_t tmem_cols) {
     extern __shared__ __align__(1024) unsigned char conv_smem[];
     const uint32_t raw = smem_addr(conv_smem);
     const uint32_t base = (raw + 1023u) & ~1023u;
     const uint32_t abytes = kTileM * KC * 2, bbytes = static_cast<uint32_t>(N) * KC * 2;
     const uint32_t sA = base, sB = base + S * abytes;
-    const uint32_t bar0 = sB + S * bbytes;
-    // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), tfull[b] = bar0 + 8(2S+b),
-    // tempty[b] = bar0 + 8(2S+2+b), drain = bar0 + 8(2S+4)
-    const uint32_t tfull0 = bar0 + 16 * S, tempty0 = tfull0 + 16, drain = tfull0 + 32;
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(conv_smem + (drain + 8 - raw));
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(conv_smem + (drain + 16 - raw));
+    const uint32_t bar0 = sB + S * bbytes;  // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), done = bar0 + 16S
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(conv_smem + (bar0 + 8 * (2 * S + 1) - raw));
+    const uint32_t done = bar0 + 16 * S;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int total = ntiles * ntn, iters = TAPS * nck;
+    int tile = blockIdx.x;
+    const int tx = tile % tiles_x;
+    tile /= tiles_x;
+    const int ty = tile % tiles_y, b = tile / tiles_y;
+    const int x0 = tx * Wt, y0 = ty * Ht, n0 = blockIdx.y * N;
 
     if (threadIdx.x == 0) {
-        for (int q = 0; q < 2 * S; q++) mbar_init(bar0 + 8 * q, 1);
-        mbar_init(tfull0, 1);
-        mbar_init(tfull0 + 8, 1);
-        mbar_init(tempty0, 4);
-        mbar_init(tempty0 + 8, 4);
-        mbar_init(drain, 1);
-        *abort_flag = 0;
+        for (int q = 0; q < 2 * S + 1; q++) mbar_init(bar0 + 8 * q, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
     }
     __syncwarp();
-    if (warp == 4) {
-        if (lane == 0) {
-            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
-            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
-        }
-        __syncwarp();
+    if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
-                     "r"(2 * cols)
+                     "r"(tmem_cols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -204,127 +180,83 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    const int iters = TAPS * nck;
 
-    if (warp == 4) {
-        if (lane == 0) {
-            // TMA producer over all (tile, k) pairs of this CTA
-            long g = 0;
-            bool stop = false;
-            for (int t = blockIdx.x; t < total && !stop; t += gridDim.x) {
-                const int pt = t / ntn, n0 = N * (t - pt * ntn);
-                int q = pt;
-                const int tx = q % tiles_x;
-                q /= tiles_x;
-                const int ty = q % tiles_y, b = q / tiles_y;
-                const int x0 = tx * Wt, y0 = ty * Ht;
-                for (int it = 0; it < iters; it++, g++) {
-                    const int s = static_cast<int>(g % S);
-                    if (*abort_flag || (g >= S && !mbar_wait(bar0 + 8 * (S + s), static_cast<uint32_t>((g / S) - 1) & 1))) {
-                        *abort_flag = 1;
-                        stop = true;
-                        break;
-                    }
-                    const int tap = it / nck, ck = it - tap * nck;
-                    const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
-                    const uint32_t full = bar0 + 8 * s;
-                    mbar_arrive_expect_tx(full, abytes + bbytes);
-                    tma_load_4d(sA + s * abytes, &mapA, full, ck * KC, x0 + dx, y0 + dy, b);
-                    tma_load_3d(sB + s * bbytes, &mapB, full, ck * KC, n0, flip ? TAPS - 1 - tap : tap);
-                }
-            }
-            // no copy may be in flight when the CTA exits
-            for (long q = g > S ? g - S : 0; q < g; q++) mbar_wait(bar0 + 8 * (q % S), static_cast<uint32_t>(q / S) & 1);
+    if (threadIdx.x == 0) {
+        // TMA producer
+        int issued = 0;
+        for (int it = 0; it < iters; it++) {
+            const int s = it % S;
+            if (it >= S && !mbar_wait(bar0 + 8 * (S + s), ((it / S) - 1) & 1)) break;
+            const int tap = it / nck, ck = it - tap * nck;
+            const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
+            const uint32_t full = bar0 + 8 * s;
+            mbar_arrive_expect_tx(full, abytes + bbytes);
+            tma_load_4d(sA + s * abytes, &mapA, full, ck * KC, x0 + dx, y0 + dy, b);
+            tma_load_3d(sB + s * bbytes, &mapB, full, ck * KC, n0, flip ? TAPS - 1 - tap : tap);
+            issued = it + 1;
         }
-    } else if (warp == 5) {
-        if (lane == 0) {
-            const uint32_t idesc = instr_desc(N);
-            long g = 0;
-            int lt = 0;
-            for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x, lt++) {
-                const int buf = lt & 1;
-                if (lt >= 2 && !mbar_wait(tempty0 + 8 * buf, static_cast<uint32_t>((lt >> 1) - 1) & 1)) {
-                    *abort_flag = 1;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t acc = tmem + static_cast<uint32_t>(buf) * cols;
-                bool ok = true;
-                for (int it = 0; it < iters; it++, g++) {
-                    const int s = static_cast<int>(g % S);
-                    if (*abort_flag || !mbar_wait(bar0 + 8 * s, static_cast<uint32_t>(g / S) & 1)) {
-                        *abort_flag = 1;
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint64_t ad = smem_desc<KC>(sA + s * abytes), bd = smem_desc<KC>(sB + s * bbytes);
-#pragma unroll
-                    for (int k = 0; k < KC / 16; k++)
-                        tc_mma(acc, ad + 2 * k, bd + 2 * k, idesc, (it > 0 || k > 0) ? 1u : 0u);
-                    tc_commit(bar0 + 8 * (S + s));
-                }
-                if (!ok) break;
-                tc_commit(tfull0 + 8 * buf);
-            }
-            // every MMA issued above completes before the tensor memory is freed
-            tc_commit(drain);
-            mbar_wait(drain, 0);
-        }
-    } else {
-        // Epilogue: warp w holds tensor-memory lanes 32w..32w+31, the tile's
-        // pixels in row-major order of the Wt x Ht tile.
-        int lt = 0;
-        for (int t = blockIdx.x; t < total; t += gridDim.x, lt++) {
-            const int buf = lt & 1;
-            bool ok = !*abort_flag && mbar_wait(tfull0 + 8 * buf, static_cast<uint32_t>(lt >> 1) & 1);
-            ok = __all_sync(0xffffffffu, ok);
-            if (!ok) {
-                *abort_flag = 1;
-                break;
-            }
+        // No copy may still be in flight when the CTA exits: wait for the last
+        // use of every stage (at once when the MMA thread consumed it).
+        for (int it = issued > S ? issued - S : 0; it < issued; it++) mbar_wait(bar0 + 8 * (it % S), (it / S) & 1);
+    } else if (threadIdx.x == 32) {
+        // MMA issuer
+        const uint32_t idesc = instr_desc(N);
+        for (int it = 0; it < iters; it++) {
+            const int s = it % S;
+            if (!mbar_wait(bar0 + 8 * s, (it / S) & 1)) break;
             tc_fence_after();
-            const int pt = t / ntn, n0 = N * (t - pt * ntn);
-            int q = pt;
-            const int tx = q % tiles_x;
-            q /= tiles_x;
-            const int ty = q % tiles_y, b = q / tiles_y;
-            const int r = warp * 32 + lane;
-            const int py = ty * Ht + r / Wt, px = tx * Wt + r % Wt;
-            const bool valid = py < H && px < W;
-            bf16 *yrow = Y + ((static_cast<long>(b) * H + py) * W + px) * static_cast<long>(ldy) + n0;
-            const uint32_t acc = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(buf) * cols;
-            for (int c0 = 0; c0 < N; c0 += 16) {
-                uint32_t v[16];
-                tc_ld16(acc + static_cast<uint32_t>(c0), v);
-                if (!valid) continue;
-                uint32_t packed[8];
+            const uint64_t ad = smem_desc<KC>(sA + s * abytes), bd = smem_desc<KC>(sB + s * bbytes);
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    float f0 = __uint_as_float(v[2 * j]), f1 = __uint_as_float(v[2 * j + 1]);
-                    if (bias) {
-                        f0 += bias[n0 + c0 + 2 * j];
-                        f1 += bias[n0 + c0 + 2 * j + 1];
-                    }
-                    if (relu) {
-                        f0 = fmaxf(f0, 0.f);
-                        f1 = fmaxf(f1, 0.f);
-                    }
-                    const __nv_bfloat162 h = __floats2bfloat162_rn(f0, f1);
-                    packed[j] = *reinterpret_cast<const uint32_t *>(&h);
+            for (int k = 0; k < KC / 16; k++)
+                tc_mma(tmem, ad + 2 * k, bd + 2 * k, idesc, (it > 0 || k > 0) ? 1u : 0u);
+            tc_commit(bar0 + 8 * (S + s));
+        }
+        // arrives once every MMA issued above has completed
+        tc_commit(done);
+    }
+    __syncwarp();
+
+    // Epilogue: warp w holds tensor-memory lanes 32w..32w+31, the tile's
+    // pixels in row-major order of the Wt x Ht tile.
+    bool ok = mbar_wait(done, 0);
+    // the tensor-memory loads below are warp-collective: converge, and agree
+    // on whether the wait succeeded
+    ok = __all_sync(0xffffffffu, ok);
+    tc_fence_after();
+    if (ok) {
+        const int r = warp * 32 + lane;
+        const int py = y0 + r / Wt, px = x0 + r % Wt;
+        const bool valid = py < H && px < W;
+        bf16 *yrow = Y + ((static_cast<long>(b) * H + py) * W + px) * static_cast<long>(ldy) + n0;
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            uint32_t v[16];
+            tc_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), v);
+            if (!valid) continue;
+            uint32_t packed[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                float f0 = __uint_as_float(v[2 * j]), f1 = __uint_as_float(v[2 * j + 1]);
+                if (bias) {
+                    f0 += bias[n0 + c0 + 2 * j];
+                    f1 += bias[n0 + c0 + 2 * j + 1];
                 }
-                uint4 *dst = reinterpret_cast<uint4 *>(yrow + c0);
-                dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-                dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+                if (relu) {
+                    f0 = fmaxf(f0, 0.f);
+                    f1 = fmaxf(f1, 0.f);
+                }
+                const __nv_bfloat162 h = __floats2bfloat162_rn(f0, f1);
+                packed[j] = *reinterpret_cast<const uint32_t *>(&h);
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(tempty0 + 8 * buf);
+            uint4 *dst = reinterpret_cast<uint4 *>(yrow + c0);
+            dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 4)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * cols) : "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
 }
 
 /** Shared-memory descriptor of an MN-major operand: atoms of KA elements
@@ -503,7 +435,6 @@ CUtensorMapSwizzle swizzle_of(int kc) {
 }
 
 constexpr int kMaxSmem = 227 * 1024;
-constexpr size_t kSmemPerSM = 228 * 1024;  // shared memory of one SM (each resident CTA also reserves 1 KB)
 
 template <int TAPS, int KC>
 int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, int Nt, bool flip,
@@ -546,34 +477,21 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
             return INCRMT_ERR_CUDA;
         }
     }
-    // Persistent CTAs: two per SM where the tensor memory holds both (two
-    // accumulators of `cols` columns each, 512 columns per SM), else one;
-    // each takes as many pipeline stages (up to six) as its share of the
-    // SM's shared memory holds.
+    const int per = (kTileM + Nt) * KC * 2;
+    int S = (200 * 1024) / per;
+    S = S > 4 ? 4 : S;
+    if (S < 2) S = 2;
+    const size_t smem = 1024 + static_cast<size_t>(S) * per + 8 * (2 * S + 1) + 16;
     uint32_t cols = 32;
     while (cols < static_cast<uint32_t>(Nt)) cols <<= 1;
-    int per_sm = 4 * cols <= 512 ? 2 : 1;
-    const int per = (kTileM + Nt) * KC * 2;
-    int S = static_cast<int>((kSmemPerSM / per_sm - 2048) / per);
-    S = S > 6 ? 6 : S;
-    if (S < 2) S = 2;
-    size_t smem = 1024 + static_cast<size_t>(S) * per + 8 * (2 * S + 5) + 16;
-    // request enough shared memory that no further CTA fits on the SM
-    const size_t floor_smem = kSmemPerSM / (per_sm + 1);
-    if (smem < floor_smem) smem = floor_smem;
     static bool attr = false;
     if (!attr) {
         INCRMT_CK(cudaFuncSetAttribute(k_conv_tc<TAPS, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
         attr = true;
     }
-    int occ = 0;
-    INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tc<TAPS, KC>, kConvThreads, smem));
-    if (occ < per_sm) per_sm = occ > 0 ? occ : 1;
-    const int tiles = B * tiles_x * tiles_y, total = tiles * (Cout / Nt);
-    const int grid = total < kB200SMs * per_sm ? total : kB200SMs * per_sm;
-    k_conv_tc<TAPS, KC><<<grid, kConvThreads, smem, s>>>(mA, mB, bias, Y, H, W, Nt, Cout, Wt, Ht, tiles_x, tiles_y,
-                                                         tiles, Cout / Nt, Cin / KC, flip ? 1 : 0, relu ? 1 : 0, S,
-                                                         cols);
+    const dim3 grid(static_cast<unsigned>(B * tiles_x * tiles_y), static_cast<unsigned>(Cout / Nt));
+    k_conv_tc<TAPS, KC><<<grid, kThreads, smem, s>>>(mA, mB, bias, Y, H, W, Nt, Cout, Wt, Ht, tiles_x, tiles_y,
+                                                     Cin / KC, flip ? 1 : 0, relu ? 1 : 0, S, cols);
     INCRMT_CKL("k_conv_tc");
     return INCRMT_OK;
 }

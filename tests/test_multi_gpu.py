@@ -171,10 +171,10 @@ def test_initial_band(gpu, scene):
     """The bands built at initialisation agree to a fraction of dx: where the
     second-order march is not causal (a point accepted below an already
     accepted neighbour) or meets exactly tied values (grid-aligned circles),
-    the reference's heap order and the fixed point differ; the statuses
-    agree wherever the two values do. Measured: 0.03 dx (circles_rod), 0.038
-    dx at the small circle of the ellipses scene, where a few points whose
-    values differ also change status; the first pinning of the next step
+    the reference's heap order and the fixed point differ. Measured: 0.03 dx
+    with identical statuses (circles_rod); 0.038 dx at the small circle of
+    the ellipses scene, where the far/trial status of a few neighbours of
+    the differing points changes with them; the first pinning of the next step
     rebuilds the band from the reference map, and the simple spin's end state
     at t = 2 pi (test_endstate_gpu.py) shows no trace of such differences."""
     r, g, dt = _pair(SCENES[scene])
@@ -183,10 +183,24 @@ def test_initial_band(gpu, scene):
     for k in range(g.objects):
         pg, pr = g.get("phi", k), r.get("phi", k)
         assert np.abs(pg - pr).max() <= tol * dx, k
-        same = np.abs(pg - pr) <= 1e-12 * dx
         sg, sr = g.get("status", k), r.get("status", k)
-        assert np.array_equal(sg[same], sr[same]), k
-        assert (sg != sr).sum() <= max(4, (~same).sum()), k
+        if scene == "circles_rod":
+            assert np.array_equal(sg, sr), k
+            continue
+        # A band-edge point whose value falls below the cap in one solution
+        # only is accepted there (status 5 / 2) and its far neighbours become
+        # trial (6 / 1): the only status change allowed where the values agree
+        # is far <-> trial, next to a point whose value differs.
+        differ = np.abs(pg - pr) > 1e-12 * dx
+        near = differ.copy()
+        near[1:, :] |= differ[:-1, :]
+        near[:-1, :] |= differ[1:, :]
+        near[:, 1:] |= differ[:, :-1]
+        near[:, :-1] |= differ[:, 1:]
+        moved = (sg != sr) & ~differ
+        pair = np.minimum(sg, sr) * 8 + np.maximum(sg, sr)
+        assert np.all(near[moved]), (k, int(moved.sum()), int((moved & ~near).sum()))
+        assert np.all(np.isin(pair[moved], [0 * 8 + 1, 6 * 8 + 7])), (k, np.unique(pair[moved]))
     r.close()
     g.close()
 

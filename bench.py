@@ -400,9 +400,9 @@ def run_reference(args, ws, rank):
 # GPU path: simulation workloads
 
 LEARNED_SIM_FACTOR = 8     # network grid: the projection's unknowns restricted by 8
-LEARNED_SIM_SAMPLES = 200  # projections captured per system from the training run
-LEARNED_SIM_STEPS = 1500   # Adam steps per network
-LEARNED_SIM_BASE = 16      # channels at the finest level of the U-Net
+LEARNED_SIM_SAMPLES = 400  # projections captured per system from the training run
+LEARNED_SIM_STEPS = 2000   # Adam steps per network
+LEARNED_SIM_BASE = 32      # channels at the finest level of the U-Net
 
 
 def train_learned_sim(workload, rank, dev):

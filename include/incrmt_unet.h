@@ -142,6 +142,14 @@ int incrmt_conv_wgrad_bf16(const void *d_x, const void *d_dy, int batch, int H, 
  * clears that record. Synchronises the device. */
 int incrmt_conv_status(void);
 
+/** Kernel choice of incrmt_conv_bf16 (and of the networks' 3x3 layers) for
+ * the whole process: 0 automatic (default), 1 one tap per pipeline stage,
+ * 2 row reuse (each stage holds one column offset of the tile's rows -1..8
+ * and the weights of that column's three taps). Both compute the same
+ * products; the FP32 sums visit the taps in another order. No reference
+ * counterpart (a check and tuning knob); INCRMT_ERR_BADARG outside 0..2. */
+int incrmt_conv_set_variant(int variant);
+
 /** Kernel launches issued by this network so far. */
 long long incrmt_unet_launches(const incrmt_unet *h);
 

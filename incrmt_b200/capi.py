@@ -182,8 +182,9 @@ class MGSolver:
         check(lib().incrmt_mg_set_profiling(self._h, int(on)))
 
     def set_tiles(self, on=True):
-        """Tile-fused smoothing (incrmt_mg_set_tiles); off runs one launch
-        per colour."""
+        """Tile-fused smoothing (incrmt_mg_set_tiles): True / 1 stages the
+        tiles' inputs in shared memory, 2 reads coefficients through the
+        caches, False / 0 runs one launch per colour."""
         check(lib().incrmt_mg_set_tiles(self._h, int(on)))
 
     def set_coarse_refresh(self, every):
@@ -646,6 +647,7 @@ def _unet_sigs(L):
     L.incrmt_unet_gradients.argtypes = [P, I, I, I, P, P, P, fp, fp, P]
     L.incrmt_conv_bf16.argtypes = [P, I, I, I, I, P, I, I, I, P, I, P, P]
     L.incrmt_conv_status.argtypes = []
+    L.incrmt_conv_set_variant.argtypes = [I]
     L.incrmt_conv_wgrad_workspace.argtypes = [I, I, I, I, I, I]
     L.incrmt_conv_wgrad_workspace.restype = ctypes.c_longlong
     L.incrmt_conv_wgrad_bf16.argtypes = [P, P, I, I, I, I, I, I, P, P, ctypes.c_longlong, P]
@@ -758,6 +760,12 @@ def conv_status():
     """Raises if a tensor-core convolution gave up a pipeline wait
     (incrmt_conv_status; synchronises the device)."""
     check(_ulib().incrmt_conv_status())
+
+
+def conv_set_variant(variant):
+    """3x3 kernel choice for the process (incrmt_conv_set_variant): 0
+    automatic, 1 one tap per stage, 2 row reuse."""
+    check(_ulib().incrmt_conv_set_variant(int(variant)))
 
 
 def learned_guess(solver, net, b_ptr, z_ptr, factor=1, stats=True):

@@ -35,6 +35,8 @@ using bf16 = __nv_bfloat16;
 
 constexpr int kThreads = 128;
 constexpr int kTileM = 128;
+constexpr int kRowsW = 16, kRowsH = 8;  // the tile of the row-reuse kernel
+static_assert(kRowsW * kRowsH == kTileM && kRowsW % 8 == 0, "row-reuse tile: 128 pixels, whole swizzle groups");
 constexpr unsigned long long kWaitNs = 1000000000ull;  // one second
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -140,18 +142,29 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 /** The convolution kernel (see the file comment); blockIdx.y selects the
  * output channels n0 = N * blockIdx.y .. n0 + N - 1 of ldy. Dynamic shared
- * memory: 1024 (alignment) + S * (128 + N) * KC * 2 bytes of stage buffers,
- * then 2S + 1 barriers (full[S], empty[S], done) and the tensor-memory
- * address. */
-template <int TAPS, int KC>
+ * memory: 1024 (alignment) + S stage buffers, then 2S + 1 barriers (full[S],
+ * empty[S], done) and the tensor-memory address.
+ *
+ * ROWS (3x3 only, Wt = 16, Ht = 8): a stage holds, for one column offset dx
+ * and channel chunk, the (Ht + 2) x Wt input pixels of the tile's rows -1 ..
+ * Ht shifted by dx (one TMA load) and the weights of the three taps of that
+ * column; the three row offsets dy are the same buffer read Wt, i.e. a whole
+ * number of eight-row swizzle groups, further on. Each input pixel then
+ * crosses from L2 3 (Ht + 2) / Ht = 3.75 times instead of 9, and each barrier
+ * round trip feeds three times the tensor-core work. Otherwise a stage holds
+ * one tap: 128 shifted pixels and that tap's weights. */
+template <int TAPS, int KC, bool ROWS>
 __global__ void __launch_bounds__(kThreads, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
               const float *__restrict__ bias, bf16 *__restrict__ Y, int H, int W, int N, int ldy, int Wt, int Ht,
               int tiles_x, int tiles_y, int nck, int flip, int relu, int S, uint32_t tmem_cols) {
+    static_assert(!ROWS || TAPS == 9, "row reuse is for 3x3 convolutions");
+    constexpr int kGroup = ROWS ? 3 : 1;                         // taps per stage
+    constexpr uint32_t abytes = (ROWS ? kTileM + 2 * kRowsW : kTileM) * KC * 2;
     extern __shared__ __align__(1024) unsigned char conv_smem[];
     const uint32_t raw = smem_addr(conv_smem);
     const uint32_t base = (raw + 1023u) & ~1023u;
-    const uint32_t abytes = kTileM * KC * 2, bbytes = static_cast<uint32_t>(N) * KC * 2;
+    const uint32_t tbytes = static_cast<uint32_t>(N) * KC * 2, bbytes = kGroup * tbytes;
     const uint32_t sA = base, sB = base + S * abytes;
     const uint32_t bar0 = sB + S * bbytes;  // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), done = bar0 + 16S
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(conv_smem + (bar0 + 8 * (2 * S + 1) - raw));
@@ -180,7 +193,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int iters = TAPS * nck;
+    const int iters = (TAPS / kGroup) * nck;
 
     if (threadIdx.x == 0) {
         // TMA producer
@@ -188,12 +201,23 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int it = 0; it < iters; it++) {
             const int s = it % S;
             if (it >= S && !mbar_wait(bar0 + 8 * (S + s), ((it / S) - 1) & 1)) break;
-            const int tap = it / nck, ck = it - tap * nck;
-            const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
+            const int g = it / nck, ck = it - g * nck;
             const uint32_t full = bar0 + 8 * s;
             mbar_arrive_expect_tx(full, abytes + bbytes);
-            tma_load_4d(sA + s * abytes, &mapA, full, ck * KC, x0 + dx, y0 + dy, b);
-            tma_load_3d(sB + s * bbytes, &mapB, full, ck * KC, n0, flip ? TAPS - 1 - tap : tap);
+            if constexpr (ROWS) {
+                // column offset g - 1; rows -1 .. Ht of the tile
+                tma_load_4d(sA + s * abytes, &mapA, full, ck * KC, x0 + g - 1, y0 - 1, b);
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const int tap = 3 * r + g;
+                    tma_load_3d(sB + s * bbytes + r * tbytes, &mapB, full, ck * KC, n0, flip ? 8 - tap : tap);
+                }
+            } else {
+                const int tap = g;
+                const int dy = TAPS == 9 ? tap / 3 - 1 : 0, dx = TAPS == 9 ? tap % 3 - 1 : 0;
+                tma_load_4d(sA + s * abytes, &mapA, full, ck * KC, x0 + dx, y0 + dy, b);
+                tma_load_3d(sB + s * bbytes, &mapB, full, ck * KC, n0, flip ? TAPS - 1 - tap : tap);
+            }
             issued = it + 1;
         }
         // No copy may still be in flight when the CTA exits: wait for the last
@@ -206,10 +230,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int s = it % S;
             if (!mbar_wait(bar0 + 8 * s, (it / S) & 1)) break;
             tc_fence_after();
-            const uint64_t ad = smem_desc<KC>(sA + s * abytes), bd = smem_desc<KC>(sB + s * bbytes);
 #pragma unroll
-            for (int k = 0; k < KC / 16; k++)
-                tc_mma(tmem, ad + 2 * k, bd + 2 * k, idesc, (it > 0 || k > 0) ? 1u : 0u);
+            for (int r = 0; r < kGroup; r++) {
+                // row offset r - 1: the stage's pixels from row r on (ROWS)
+                const uint64_t ad = smem_desc<KC>(sA + s * abytes + r * kRowsW * KC * 2),
+                               bd = smem_desc<KC>(sB + s * bbytes + r * tbytes);
+#pragma unroll
+                for (int k = 0; k < KC / 16; k++)
+                    tc_mma(tmem, ad + 2 * k, bd + 2 * k, idesc, (it > 0 || r > 0 || k > 0) ? 1u : 0u);
+            }
             tc_commit(bar0 + 8 * (S + s));
         }
         // arrives once every MMA issued above has completed
@@ -436,7 +465,7 @@ CUtensorMapSwizzle swizzle_of(int kc) {
 
 constexpr int kMaxSmem = 227 * 1024;
 
-template <int TAPS, int KC>
+template <int TAPS, int KC, bool ROWS>
 int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, int Nt, bool flip,
                 const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
     EncodeTiled enc = encode_tiled();
@@ -444,7 +473,7 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
         set_error("conv: cuTensorMapEncodeTiled is not available");
         return INCRMT_ERR_CUDA;
     }
-    const int Wt = W >= 128 ? 128 : W >= 64 ? 64 : W >= 32 ? 32 : 16, Ht = kTileM / Wt;
+    const int Wt = ROWS ? kRowsW : W >= 128 ? 128 : W >= 64 ? 64 : W >= 32 ? 32 : 16, Ht = kTileM / Wt;
     const int tiles_x = (W + Wt - 1) / Wt, tiles_y = (H + Ht - 1) / Ht;
     CUtensorMap mA, mB;
     {
@@ -453,7 +482,7 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
         const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Cin) * 2, static_cast<cuuint64_t>(W) * Cin * 2,
                                        static_cast<cuuint64_t>(H) * W * Cin * 2};
         const cuuint32_t box[4] = {static_cast<cuuint32_t>(KC), static_cast<cuuint32_t>(Wt),
-                                   static_cast<cuuint32_t>(Ht), 1};
+                                   static_cast<cuuint32_t>(ROWS ? Ht + 2 : Ht), 1};
         const cuuint32_t es[4] = {1, 1, 1, 1};
         CUresult r = enc(&mA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(X), dims, strides, box, es,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(KC), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -477,32 +506,52 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
             return INCRMT_ERR_CUDA;
         }
     }
-    const int per = (kTileM + Nt) * KC * 2;
-    int S = (200 * 1024) / per;
-    S = S > 4 ? 4 : S;
-    if (S < 2) S = 2;
+    int S;
+    size_t per;
+    if (ROWS) {
+        // as many stages as the CTA has steps, within half an SM's shared
+        // memory (two CTAs per SM), at least two
+        per = static_cast<size_t>(kTileM + 2 * kRowsW + 3 * Nt) * KC * 2;
+        const int steps = 3 * (Cin / KC);
+        S = static_cast<int>((110 * 1024) / per);
+        if (S > steps) S = steps;
+        if (S > 8) S = 8;
+        if (S < 2) S = 2;
+    } else {
+        per = static_cast<size_t>(kTileM + Nt) * KC * 2;
+        S = static_cast<int>((200 * 1024) / per);
+        S = S > 4 ? 4 : S;
+        if (S < 2) S = 2;
+    }
     const size_t smem = 1024 + static_cast<size_t>(S) * per + 8 * (2 * S + 1) + 16;
+    if (smem > static_cast<size_t>(kMaxSmem)) {
+        set_error("conv: %zu bytes of shared memory needed", smem);
+        return INCRMT_ERR_BADARG;
+    }
     uint32_t cols = 32;
     while (cols < static_cast<uint32_t>(Nt)) cols <<= 1;
     static bool attr = false;
     if (!attr) {
-        INCRMT_CK(cudaFuncSetAttribute(k_conv_tc<TAPS, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+        INCRMT_CK(cudaFuncSetAttribute(k_conv_tc<TAPS, KC, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kMaxSmem));
         attr = true;
     }
     const dim3 grid(static_cast<unsigned>(B * tiles_x * tiles_y), static_cast<unsigned>(Cout / Nt));
-    k_conv_tc<TAPS, KC><<<grid, kThreads, smem, s>>>(mA, mB, bias, Y, H, W, Nt, Cout, Wt, Ht, tiles_x, tiles_y,
-                                                     Cin / KC, flip ? 1 : 0, relu ? 1 : 0, S, cols);
+    k_conv_tc<TAPS, KC, ROWS><<<grid, kThreads, smem, s>>>(mA, mB, bias, Y, H, W, Nt, Cout, Wt, Ht, tiles_x,
+                                                           tiles_y, Cin / KC, flip ? 1 : 0, relu ? 1 : 0, S, cols);
     INCRMT_CKL("k_conv_tc");
     return INCRMT_OK;
 }
 
-template <int TAPS>
+template <int TAPS, bool ROWS>
 int launch_taps(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, int Nt, bool flip,
                 const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
-    if (Cin % 64 == 0) return launch_conv<TAPS, 64>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
-    if (Cin % 32 == 0) return launch_conv<TAPS, 32>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
-    return launch_conv<TAPS, 16>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    if (Cin % 64 == 0) return launch_conv<TAPS, 64, ROWS>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    if (Cin % 32 == 0) return launch_conv<TAPS, 32, ROWS>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    return launch_conv<TAPS, 16, ROWS>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
 }
+
+int g_conv_variant = 0;  // 0 automatic, 1 one tap per stage, 2 row reuse
 
 /** Split of the weight gradient over the pixels: about four waves of CTAs
  * over the SMs. */
@@ -631,15 +680,30 @@ int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int tap
         set_error("conv: bad arguments (channels must be positive multiples of 16, taps 1 or 9)");
         return INCRMT_ERR_BADARG;
     }
-    // output channels per CTA: all of them up to 256, else the largest
-    // multiple of 16 of at most 256 that divides Cout
+    // Row reuse (3x3) for up to 128 output channels per CTA, where its three
+    // taps' weights per stage still leave room for two CTAs per SM; one tap
+    // per stage above that.
+    const bool rows = taps == 9 && (g_conv_variant == 2 || (g_conv_variant == 0 && Cout <= 128));
+    // output channels per CTA: all of them up to the cap (128 with row reuse,
+    // else 256), else the largest multiple of 16 below the cap dividing Cout
+    const int cap = rows ? 128 : 256;
     int Nt = Cout;
-    if (Nt > 256) {
-        Nt = 256;
+    if (Nt > cap) {
+        Nt = cap;
         while (Cout % Nt) Nt -= 16;
     }
-    if (taps == 9) return launch_taps<9>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
-    return launch_taps<1>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    if (rows) return launch_taps<9, true>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    if (taps == 9) return launch_taps<9, false>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    return launch_taps<1, false>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+}
+
+int conv_tc_set_variant(int v) {
+    if (v < 0 || v > 2) {
+        set_error("conv: variant %d not in 0..2", v);
+        return INCRMT_ERR_BADARG;
+    }
+    g_conv_variant = v;
+    return INCRMT_OK;
 }
 
 int conv_tc_status() {

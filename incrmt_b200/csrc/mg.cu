@@ -210,15 +210,21 @@ __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool 
  * exactly as in k_galerkin, in the same order: the same values, without
  * each thread re-reading some four hundred entries from global memory.
  * Dynamic shared memory: galerkin_tile_smem(kx, ky) bytes. */
-template <class Op>
-__global__ void __launch_bounds__(256) k_galerkin_tile(Op op, int fm, int fn, int px, int py, bool kx, bool ky,
-                                                       int cm, int cn, double *st, const double *P) {
+template <class Op, bool KX, bool KY>
+__global__ void __launch_bounds__(256) k_galerkin_tile(Op op, int fm, int fn, int px, int py, int cm, int cn,
+                                                       double *st, const double *P) {
+    // The coarsening flags are template parameters: with them every loop
+    // below has fixed bounds and every offset of a support point or stencil
+    // neighbour relative to the coarse point is a constant, so the nine sums
+    // stay in registers (indexed at run time they would live in local memory).
     extern __shared__ __align__(16) double gal_smem[];
     constexpr int CTW = 32, CTH = 8;
+    constexpr bool kx = KX, ky = KY;
     const int X0 = blockIdx.x * CTW, Y0 = blockIdx.y * CTH;
     const int SX0 = kx ? 2 * X0 - 1 : X0, SY0 = ky ? 2 * Y0 - 1 : Y0;
-    const int SW = kx ? 2 * CTW + 1 : CTW, SH = ky ? 2 * CTH + 1 : CTH, SA = SW * SH;
-    const int NX0 = SX0 - 1, NY0 = SY0 - 1, NW = SW + 2, NH = SH + 2;
+    constexpr int SW = kx ? 2 * CTW + 1 : CTW, SH = ky ? 2 * CTH + 1 : CTH, SA = SW * SH;
+    const int NX0 = SX0 - 1, NY0 = SY0 - 1;
+    constexpr int NW = SW + 2, NH = SH + 2;
     double *As = gal_smem;          // entry k of support point t at As[k * SA + t]
     double *Ps = gal_smem + 9 * SA;  // weights of region point t at Ps[4 * t .. 4 * t + 3]
     for (int t = threadIdx.x; t < NW * NH; t += blockDim.x) {
@@ -244,31 +250,54 @@ __global__ void __launch_bounds__(256) k_galerkin_tile(Op op, int fm, int fn, in
     const int I = X0 + (threadIdx.x & 31), J = Y0 + (threadIdx.x >> 5);
     if (I >= cm || J >= cn) return;
     double q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const int x0 = kx ? 2 * I - 1 : I, x1 = kx ? 2 * I + 1 : I, y0 = ky ? 2 * J - 1 : J, y1 = ky ? 2 * J + 1 : J;
-    for (int fj = y0; fj <= y1; fj++)
-        for (int fi = x0; fi <= x1; fi++) {
+    // Support points fi = 2I-1+u (u = 0..2) in a coarsened direction, fi = I
+    // otherwise; visited in the order of k_galerkin (rows, then columns).
+    // Relative to I: base_of(fi) - I = floor((u-1)/2) there, 0 otherwise.
+    const int x0 = kx ? 2 * I - 1 : I, y0 = ky ? 2 * J - 1 : J;
+#pragma unroll
+    for (int v = 0; v <= (ky ? 2 : 0); v++)
+#pragma unroll
+        for (int u = 0; u <= (kx ? 2 : 0); u++) {
+            const int fi = x0 + u, fj = y0 + v;
             // pweight(fi, fj, I, J) from the staged weights
-            const int qx = I - base_of(fi, kx), qy = J - base_of(fj, ky);
+            const int qx = kx ? -((u - 1) >> 1) : 0, qy = ky ? -((v - 1) >> 1) : 0;
             if (qx < 0 || qx > 1 || qy < 0 || qy > 1) continue;
             const double w = Ps[4 * ((fi - NX0) + NW * (fj - NY0)) + qx + 2 * qy];
             if (w == 0) continue;
             const int ls = (fi - SX0) + SW * (fj - SY0);
+#pragma unroll
             for (int dj = -1; dj <= 1; dj++)
+#pragma unroll
                 for (int di = -1; di <= 1; di++) {
                     const double av = As[(3 * (dj + 1) + di + 1) * SA + ls];
                     if (av == 0) continue;
                     const double *g = Ps + 4 * ((fi + di - NX0) + NW * (fj + dj - NY0));
-                    const int ox = base_of(fi + di, kx) - I, oy = base_of(fj + dj, ky) - J;
+                    const int ox = kx ? ((u - 1 + di) >> 1) : di, oy = ky ? ((v - 1 + dj) >> 1) : dj;
+#pragma unroll
                     for (int r = 0; r < 4; r++) {
                         const int kx_ = ox + (r & 1), ky_ = oy + (r >> 1);
-                        if (g[r] == 0 || kx_ < -1 || kx_ > 1 || ky_ < -1 || ky_ > 1) continue;
+                        if (kx_ < -1 || kx_ > 1 || ky_ < -1 || ky_ > 1) continue;
+                        if (g[r] == 0) continue;
                         double &qe = q[3 * (ky_ + 1) + kx_ + 1];
                         qe = add_prod(qe, __dmul_rn(w, av), g[r]);
                     }
                 }
         }
     const long N = static_cast<long>(cm) * cn, ij = I + static_cast<long>(cm) * J;
+#pragma unroll
     for (int e = 0; e < 9; e++) st[e * N + ij] = q[e];
+}
+
+/** The shared-memory limit of every k_galerkin_tile instance of Op. */
+template <class Op>
+cudaError_t set_galerkin_attr(int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(k_galerkin_tile<Op, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_galerkin_tile<Op, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_galerkin_tile<Op, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 /** Shared memory of k_galerkin_tile for the coarsening flags. */
@@ -456,9 +485,190 @@ __global__ void __launch_bounds__(256) k_smooth_tile_gen(GenOp<T> op, const T *z
     }
 }
 
-/** Shared memory of k_smooth_tile_gen<T, 2, 16, 16>. */
-template <class T>
-constexpr int gen_tile_smem() { return 11 * (16 + 16) * (16 + 16) * static_cast<int>(sizeof(T)); }
+/** Shared memory of k_smooth_tile_gen<T, SWEEPS, TW, TH>. */
+template <class T, int SWEEPS = 2, int TW = 16, int TH = 16>
+constexpr int gen_tile_smem() {
+    return 11 * (TW + 8 * SWEEPS) * (TH + 8 * SWEEPS) * static_cast<int>(sizeof(T));
+}
+
+/** Shared memory of k_smooth_rb_mac<T, SWEEPS, TW, TH>: iterate and
+ * right-hand side on the LW x LH region, x-edge coefficients on (LW+1) x LH,
+ * y-edge coefficients on LW x (LH+1). */
+template <class T, int SWEEPS, int TW, int TH>
+constexpr int rb_mac_smem() {
+    constexpr int LW = TW + 4 * SWEEPS, LH = TH + 4 * SWEEPS;
+    return (2 * LW * LH + (LW + 1) * LH + LW * (LH + 1)) * static_cast<int>(sizeof(T));
+}
+
+/** Shared memory of k_smooth_tile_fem<T, SWEEPS, TW, TH>: iterate and
+ * right-hand side on the LW x LH region, cell values on (LW+1) x (LH+1). */
+template <class T, int SWEEPS, int TW, int TH>
+constexpr int fem_tile_smem() {
+    constexpr int LW = TW + 8 * SWEEPS, LH = TH + 8 * SWEEPS;
+    return (2 * LW * LH + (LW + 1) * (LH + 1)) * static_cast<int>(sizeof(T));
+}
+
+/** k_smooth_rb for the fine MAC system with every input staged once: the
+ * block copies the iterate, the right-hand side and the edge coefficients of
+ * its region to shared memory with coalesced loads (each value read from
+ * global memory once per launch), then runs the phases on shared memory
+ * alone; k_smooth_rb reads the coefficients of each colour's points in every
+ * phase, every second double of a line, through L1/L2. Same arithmetic
+ * (MacOp::offdiag_v), so the same results. Across a periodic seam the staged
+ * edge array holds the image of the first edge; a point on the last column
+ * (row) reads its right (upper) edge from global memory, as the unstaged
+ * kernels do. */
+template <class T, int SWEEPS, int TW, int TH>
+__global__ void __launch_bounds__(256, 2) k_smooth_rb_mac(MacOp<T> op, const T *zin, T *zout, const T *b, int m,
+                                                          int n) {
+    constexpr int H = 2 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H, NP = 2 * SWEEPS, LA = LW * LH, LX = LW + 1;
+    extern __shared__ __align__(16) unsigned char rbm_smem[];
+    T *zs = reinterpret_cast<T *>(rbm_smem);
+    T *bs = zs + LA;
+    T *xs = bs + LA;       // x-edge left of local (li, lj) at xs[li + LX * lj], li = 0..LW
+    T *ys = xs + LX * LH;  // y-edge below local (li, lj) at ys[li + LW * lj], lj = 0..LH
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    const int gx0 = x0 - H, gy0 = y0 - H;
+    const bool px = op.px, py = op.py;
+    for (int lj = ty; lj <= LH; lj += 8) {
+        int j = gy0 + lj;
+        if (py) j = wrap_index(j, n);
+        const bool jc = lj < LH && j >= 0 && j < n, je = j >= 0 && j <= n;
+        for (int li = tx; li <= LW; li += 32) {
+            int i = gx0 + li;
+            if (px) i = wrap_index(i, m);
+            if (jc) {
+                if (li < LW && i >= 0 && i < m) {
+                    const long ij = i + static_cast<long>(m) * j;
+                    zs[li + LW * lj] = zin[ij];
+                    bs[li + LW * lj] = b[ij];
+                }
+                if (i >= 0 && i <= m) xs[li + LX * lj] = op.ex[static_cast<long>(j) * (m + 1) + i];
+            }
+            if (je && li < LW && i >= 0 && i < m) ys[li + LW * lj] = op.ey[static_cast<long>(j) * m + i];
+        }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int p = 0; p < NP; p++) {
+        const int e = NP - 1 - p, parity = p & 1;
+        int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
+        if (!px) {
+            if (ilo < 0) ilo = 0;
+            if (ihi > m - 1) ihi = m - 1;
+        }
+        if (!py) {
+            if (jlo < 0) jlo = 0;
+            if (jhi > n - 1) jhi = n - 1;
+        }
+        for (int j = jlo + ty; j <= jhi; j += 8) {
+            const int i0 = ilo + (((ilo + j) & 1) != parity);
+            const int jr = py ? wrap_index(j, n) : j;
+            const int lj = j - gy0;
+            for (int i = i0 + 2 * tx; i <= ihi; i += 64) {
+                const int li = i - gx0, lz = li + LW * lj, lx = li + LX * lj;
+                const int ir = px ? wrap_index(i, m) : i;
+                const T el = xs[lx];
+                const T er = (px && ir == m - 1) ? op.ex[static_cast<long>(jr) * (m + 1) + m] : xs[lx + 1];
+                const T ed = ys[lz];
+                const T eu = (py && jr == n - 1) ? op.ey[static_cast<long>(n) * m + ir] : ys[lz + LW];
+                T diag;
+                if constexpr (sizeof(T) == 8) {
+                    const T off = op.offdiag_v(ir, jr, el, er, ed, eu, zs, lz, LW, diag);
+                    zs[lz] = (bs[lz] - off) / diag;
+                } else {
+                    const T zc = zs[lz];
+                    const T off = op.template offdiag_v<true>(ir, jr, el, er, ed, eu, zs, lz, LW, diag);
+                    zs[lz] = zc + (bs[lz] - off - op.rowsum(ir, jr) * zc) / diag;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int lj = H + ty; lj < H + TH; lj += 8) {
+        const int j = gy0 + lj;
+        if (j >= n) break;
+        for (int li = H + tx; li < H + TW; li += 32) {
+            const int i = gx0 + li;
+            if (i < m) zout[i + static_cast<long>(m) * j] = zs[li + LW * lj];
+        }
+    }
+}
+
+/** k_smooth_tile for the fine FEM system with its inputs staged once: the
+ * iterate, the right-hand side and the cell values of the region go to
+ * shared memory with coalesced loads before the first phase. Interior nodes
+ * take their four cells from shared memory (FemOp::offdiag_int), nodes on an
+ * edge of the grid from global memory (FemOp::offdiag_edge), exactly as
+ * FemOp::offdiag_s does, so the results are those of k_smooth_tile. */
+template <class T, int SWEEPS, int TW, int TH>
+__global__ void __launch_bounds__(256, 2) k_smooth_tile_fem(FemOp<T> op, const T *zin, T *zout, const T *b, int m,
+                                                            int n) {
+    constexpr int H = 4 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H, LA = LW * LH, LX = LW + 1;
+    extern __shared__ __align__(16) unsigned char fem_smem[];
+    T *zs = reinterpret_cast<T *>(fem_smem);
+    T *bs = zs + LA;
+    T *cs = bs + LA;  // cell value of local (li, lj) at cs[li + LX * lj], li = 0..LW, lj = 0..LH
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    const int gx0 = x0 - H, gy0 = y0 - H;
+    const bool px = op.px, py = op.py;
+    for (int t = threadIdx.x; t < LX * (LH + 1); t += blockDim.x) {
+        const int li = t % LX, lj = t / LX;
+        int i = gx0 + li, j = gy0 + lj;
+        if (px) i = wrap_index(i, m);
+        if (py) j = wrap_index(j, n);
+        if (i >= 0 && i < m && j >= 0 && j < n) {
+            const long ij = i + static_cast<long>(m) * j;
+            cs[t] = op.c[ij];
+            if (li < LW && lj < LH) {
+                zs[li + LW * lj] = zin[ij];
+                bs[li + LW * lj] = b[ij];
+            }
+        }
+    }
+    __syncthreads();
+    const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
+    constexpr int P = 4 * SWEEPS;
+#pragma unroll 1
+    for (int p = 0; p < P; p++) {
+        const int e = P - 1 - p, c = p & 3;
+        int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
+        if (!px) {
+            if (ilo < 0) ilo = 0;
+            if (ihi > m - 1) ihi = m - 1;
+        }
+        if (!py) {
+            if (jlo < 0) jlo = 0;
+            if (jhi > n - 1) jhi = n - 1;
+        }
+        const int i0 = ilo + ((ilo & 1) != pis[c]), j0 = jlo + ((jlo & 1) != pjs[c]);
+        const int ni = i0 <= ihi ? (ihi - i0) / 2 + 1 : 0, nj = j0 <= jhi ? (jhi - j0) / 2 + 1 : 0;
+        for (int t = threadIdx.x; t < ni * nj; t += blockDim.x) {
+            const int i = i0 + 2 * (t % ni), j = j0 + 2 * (t / ni);
+            const int li = i - gx0, lj = j - gy0, lz = li + LW * lj, lc = li + LX * lj;
+            const int ir = px ? wrap_index(i, m) : i, jr = py ? wrap_index(j, n) : j;
+            const bool interior = ir > 0 && ir < m - 1 && jr > 0 && jr < n - 1;
+            T diag, off;
+            if constexpr (sizeof(T) == 8) {
+                off = interior ? op.offdiag_int(cs[lc], cs[lc + 1], cs[lc + LX], cs[lc + LX + 1], zs, lz, LW, diag)
+                               : op.offdiag_edge(ir, jr, zs, lz, LW, diag);
+                zs[lz] = (bs[lz] - off) / diag;
+            } else {
+                const T zc = zs[lz];
+                off = interior ? op.template offdiag_int<true>(cs[lc], cs[lc + 1], cs[lc + LX], cs[lc + LX + 1], zs,
+                                                               lz, LW, diag)
+                               : op.template offdiag_edge<true>(ir, jr, zs, lz, LW, diag);
+                zs[lz] = zc + (bs[lz] - off - op.rowsum(ir, jr) * zc) / diag;
+            }
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < TW * TH; t += blockDim.x) {
+        const int i = x0 + t % TW, j = y0 + t / TW;
+        if (i < m && j < n) zout[i + static_cast<long>(m) * j] = zs[(i - gx0) + LW * (j - gy0)];
+    }
+}
 
 /** Tile-fused red-black Gauss-Seidel for a five-point operator (the fine MAC
  * system): the colours (0,0),(1,1) share no stencil edge, nor do (1,0),(0,1),
@@ -893,21 +1103,21 @@ __global__ void __launch_bounds__(1024) k_tail(TailLevels<T> Lp, int nu1, int nu
 }
 
 /** FP64 residual r = b - A z, optionally stored in FP32, with per-block sums
- * of r^2 in partial[blockIdx.x]. Grid-stride over the unknowns. */
+ * of r^2 in partial[blockIdx.x]. Each block takes every gridDim.x-th row,
+ * its threads the row's unknowns (coalesced, no index division). */
 template <class Op>
 __global__ void k_resnorm(Op op, const double *z, const double *b, int m, int n, float *rf,
                           double *partial) {
-    const long N = static_cast<long>(m) * n;
     double acc = 0;
-    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
-         q += static_cast<long>(gridDim.x) * blockDim.x) {
-        const int i = static_cast<int>(q % m), j = static_cast<int>(q / m);
-        double diag;
-        const double off = op.offdiag(i, j, z, diag);
-        const double r = b[q] - off - diag * z[q];
-        if (rf) rf[q] = static_cast<float>(r);
-        acc += r * r;
-    }
+    for (int j = blockIdx.x; j < n; j += gridDim.x)
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const long q = i + static_cast<long>(m) * j;
+            double diag;
+            const double off = op.offdiag(i, j, z, diag);
+            const double r = b[q] - off - diag * z[q];
+            if (rf) rf[q] = static_cast<float>(r);
+            acc += r * r;
+        }
     acc = block_sum_256(acc);
     if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
@@ -989,8 +1199,8 @@ const dim3 kBlk2(32, 8);
  * by CUDA events and credited with its algorithmic bytes: (units updated) x
  * bytes_per_unit. */
 template <class Op, class T>
-int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl, T **res,
-           Multigrid *prof = nullptr, double bytes_per_unit = 0) {
+int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, bool staged, cudaStream_t s, long long &nl,
+           T **res, Multigrid *prof = nullptr, double bytes_per_unit = 0) {
     *res = z;
     if (sweeps == 2 && zalt && (!op.px || m % 2 == 0) && (!op.py || n % 2 == 0)) {
         // Two sweeps per launch with shared-memory tiles (identical results);
@@ -998,8 +1208,28 @@ int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStrea
         const dim3 b64(cdiv(m, 64), cdiv(n, 32)), b32(cdiv(m, 32), cdiv(n, 16)), b16(cdiv(m, 16), cdiv(n, 16));
         if (prof) { int r = prof->prof_begin(static_cast<double>(m) * n * 2 * bytes_per_unit); if (r) return r; }
         bool done = false;
+        const bool big = static_cast<int>(b64.x * b64.y) >= 2 * kB200SMs;
+        if constexpr (std::is_same<Op, MacOp<T>>::value) {
+            if (big && staged) {
+                k_smooth_rb_mac<T, 2, 64, 32><<<b64, 256, rb_mac_smem<T, 2, 64, 32>(), s>>>(op, z, zalt, b, m, n);
+                done = true;
+            }
+        }
+        if constexpr (std::is_same<Op, FemOp<T>>::value) {
+            if (big && staged) {
+                k_smooth_tile_fem<T, 2, 64, 32><<<b64, 256, fem_tile_smem<T, 2, 64, 32>(), s>>>(op, z, zalt, b, m, n);
+                done = true;
+            }
+        }
+        if constexpr (std::is_same<Op, GenOp<T>>::value) {
+            const dim3 g32(cdiv(m, 32), cdiv(n, 32));
+            if (!done && staged && static_cast<int>(g32.x * g32.y) >= kB200SMs) {
+                k_smooth_tile_gen<T, 2, 32, 32><<<g32, 256, gen_tile_smem<T, 2, 32, 32>(), s>>>(op, z, zalt, b, m, n);
+                done = true;
+            }
+        }
         if constexpr (Op::kFivePoint) {
-            if (static_cast<int>(b64.x * b64.y) >= 2 * kB200SMs) {
+            if (!done && big) {
                 k_smooth_rb<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, zalt, b, m, n);
                 done = true;
             }
@@ -1168,13 +1398,22 @@ int Multigrid::build_hierarchy() {
                                    gen_tile_smem<float>()));
     INCRMT_CK(cudaFuncSetAttribute(k_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTailSmemBudget)));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_gen<double, 2, 32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gen_tile_smem<double, 2, 32, 32>()));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_gen<float, 2, 32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gen_tile_smem<float, 2, 32, 32>()));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_rb_mac<double, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   rb_mac_smem<double, 2, 64, 32>()));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_rb_mac<float, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   rb_mac_smem<float, 2, 64, 32>()));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_fem<double, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   fem_tile_smem<double, 2, 64, 32>()));
+    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_fem<float, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   fem_tile_smem<float, 2, 64, 32>()));
     const int gal_smem = static_cast<int>(galerkin_tile_smem(true, true));
-    INCRMT_CK(cudaFuncSetAttribute(k_galerkin_tile<MacOp<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   gal_smem));
-    INCRMT_CK(cudaFuncSetAttribute(k_galerkin_tile<FemOp<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   gal_smem));
-    INCRMT_CK(cudaFuncSetAttribute(k_galerkin_tile<GenOp<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   gal_smem));
+    INCRMT_CK(set_galerkin_attr<MacOp<double>>(gal_smem));
+    INCRMT_CK(set_galerkin_attr<FemOp<double>>(gal_smem));
+    INCRMT_CK(set_galerkin_attr<GenOp<double>>(gal_smem));
     // First level small enough for the one-block tail kernel (never level 0).
     tail_level = -1;
     for (int l = 1; l < static_cast<int>(lev.size()); l++)
@@ -1292,8 +1531,13 @@ int Multigrid::galerkin_all() {
         auto build = [&](auto op) {
             for (int pass = 0; pass < 2; pass++)
                 k_build_p<<<gf, kBlk2, 0, stream>>>(op, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, F.P, pass);
-            if (tiles)
-                k_galerkin_tile<<<gt, 256, gsm, stream>>>(op, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
+            using OpT = decltype(op);
+            if (tiles && F.kx && F.ky)
+                k_galerkin_tile<OpT, true, true><<<gt, 256, gsm, stream>>>(op, F.m, F.n, px, py, C.m, C.n, C.st, F.P);
+            else if (tiles && F.kx)
+                k_galerkin_tile<OpT, true, false><<<gt, 256, gsm, stream>>>(op, F.m, F.n, px, py, C.m, C.n, C.st, F.P);
+            else if (tiles)
+                k_galerkin_tile<OpT, false, true><<<gt, 256, gsm, stream>>>(op, F.m, F.n, px, py, C.m, C.n, C.st, F.P);
             else
                 k_galerkin<<<gc, kBlk2, 0, stream>>>(op, F.m, F.n, px, py, F.kx, F.ky, C.m, C.n, C.st, F.P);
         };
@@ -1306,10 +1550,9 @@ int Multigrid::galerkin_all() {
             build(g);
         }
         launches += 3;
-        k_cast_stencil<<<cdiv(C.N, 256) < kRedBlocks ? cdiv(C.N, 256) : kRedBlocks, 256, 0, stream>>>(C.st, C.stf, C.N);
-        launches++;
         INCRMT_CKL("galerkin");
     }
+    f32_stale = true;
     if (ginv) {
         const MgLevel &C = lev.back();
         const size_t sm = sizeof(double) * (2 * C.N * C.N + C.N);
@@ -1317,6 +1560,18 @@ int Multigrid::galerkin_all() {
         launches++;
         INCRMT_CKL("k_coarse_inverse");
     }
+    return INCRMT_OK;
+}
+
+int Multigrid::cast_levels() {
+    if (!f32_stale) return INCRMT_OK;
+    for (size_t l = 1; l < lev.size(); l++) {
+        MgLevel &C = lev[l];
+        k_cast_stencil<<<cdiv(C.N, 256) < kRedBlocks ? cdiv(C.N, 256) : kRedBlocks, 256, 0, stream>>>(C.st, C.stf, C.N);
+        launches++;
+    }
+    INCRMT_CKL("k_cast_stencil");
+    f32_stale = false;
     return INCRMT_OK;
 }
 
@@ -1350,14 +1605,14 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
     double *cur = z;
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac64();
-        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     } else if (l == 0) {
         auto op = fem64();
-        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     } else {
-        if ((r = smooth(g, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        if ((r = smooth(g, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur))) return r;
         restrict_launch(tiles, g, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     }
     launches++;
@@ -1367,9 +1622,9 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
     launches++;
     INCRMT_CKL("k_prolong");
     double *alt = !tiles ? nullptr : cur == z ? L.z2 : z, *out = cur;
-    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac64(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
-    else if (l == 0) r = smooth(fem64(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
-    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
+    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac64(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
+    else if (l == 0) r = smooth(fem64(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
+    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out);
     if (r) return r;
     if (out != z) INCRMT_CK(cudaMemcpyAsync(z, out, sizeof(double) * L.N, cudaMemcpyDeviceToDevice, stream));
     return INCRMT_OK;
@@ -1437,14 +1692,14 @@ int Multigrid::cycle32(int l) {
     const double bpu = 4.0 * (sys == INCRMT_SYS_MAC ? 5 : 4);  // FP32 words: z, b, coefficients in; z out
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac32();
-        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else if (l == 0) {
         auto op = fem32();
-        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else {
-        if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
+        if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur))) return r;
         restrict_launch(tiles, g, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     }
     launches++;
@@ -1454,9 +1709,9 @@ int Multigrid::cycle32(int l) {
     launches++;
     INCRMT_CKL("k_prolong");
     float *alt = !tiles ? nullptr : cur == z ? L.zf2 : z, *out = cur;
-    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
-    else if (l == 0) r = smooth(fem32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
-    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
+    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac32(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
+    else if (l == 0) r = smooth(fem32(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
+    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out);
     if (r) return r;
     if (out != z) INCRMT_CK(cudaMemcpyAsync(z, out, sizeof(float) * L.N, cudaMemcpyDeviceToDevice, stream));
     return INCRMT_OK;
@@ -1523,8 +1778,7 @@ int Multigrid::norm2_rhs(const double *b, double *out_dev) {
 }
 
 int Multigrid::residual_norm(const double *b, const double *z, float *rf, double *out_dev) {
-    const long N = static_cast<long>(m) * n;
-    const int nb = cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks;
+    const int nb = n < kRedBlocks ? n : kRedBlocks;  // blocks over the rows
     if (sys == INCRMT_SYS_MAC) k_resnorm<<<nb, 256, 0, stream>>>(mac64(), z, b, m, n, rf, partial);
     else k_resnorm<<<nb, 256, 0, stream>>>(fem64(), z, b, m, n, rf, partial);
     k_reduce<<<1, 256, 0, stream>>>(partial, nb, out_dev);
@@ -1652,6 +1906,7 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
     bool conv = false, finite = true;
     double rn_prev = 0;
     if (prec == INCRMT_PREC_MIXED) {
+        if ((r = cast_levels())) return r;
         if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
         if ((r = fetch_norm(&rn2))) return r;
         rn_prev = std::sqrt(rn2);

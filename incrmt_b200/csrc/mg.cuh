@@ -69,7 +69,12 @@ public:
     long long mixed_fallbacks = 0;   // mixed-precision solves finished with FP64 V-cycles
     const double *lag_rho = nullptr; // density of the last set_density_lagged (read again on a retry)
     int lag_ld = 0;
-    bool tiles = true;               // tile-fused smoothing where it applies
+    bool f32_stale = true;           // FP32 Galerkin stencils not cast since the last rebuild
+    // Smoothing and restriction kernels: 1 tile-fused with the inputs staged
+    // in shared memory (default), 2 tile-fused reading the coefficients
+    // through the caches, 0 one launch per colour and one thread per unknown.
+    // All three give the same results, bit for bit.
+    int tiles = 1;
     int tail_level = -1;             // first level run by the one-block tail kernel
     cudaGraphExec_t gexec = nullptr; // captured V-cycle + norm
     int gkey_prec = -1;
@@ -129,6 +134,9 @@ public:
 private:
     int build_hierarchy();
     int galerkin_all();
+    /** FP32 copies of the Galerkin stencils, made on the first mixed solve
+     * after a rebuild (FP64 solves never read them). */
+    int cast_levels();
     int cycle64(int l, const double *b0, double *z0);
     int cycle32(int l);
     int tail64();

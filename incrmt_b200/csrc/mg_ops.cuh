@@ -74,8 +74,15 @@ struct MacOp {
      * lz+-ldz, across a periodic edge too (as periodic images). */
     template <bool CEN = false>
     __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
-        const T el = ex[j * (m + 1) + i], er = ex[j * (m + 1) + i + 1];
-        const T ed = ey[j * m + i], eu = ey[(j + 1) * m + i];
+        return offdiag_v<CEN>(i, j, ex[j * (m + 1) + i], ex[j * (m + 1) + i + 1], ey[j * m + i], ey[(j + 1) * m + i],
+                              zs, lz, ldz, diag);
+    }
+
+    /** offdiag_s with the four edge coefficients of (i,j) given (left, right,
+     * below, above), e.g. staged in shared memory. */
+    template <bool CEN = false>
+    __device__ __forceinline__ T offdiag_v(int i, int j, T el, T er, T ed, T eu, const T *zs, int lz, int ldz,
+                                           T &diag) const {
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         const T zc = CEN ? zs[lz] : T(0);
         T sx = 0, sy = 0;
@@ -151,16 +158,29 @@ struct FemOp {
     template <bool CEN = false>
     __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
         const int ij = i + m * j;
+        if (i > 0 && i < m - 1 && j > 0 && j < n - 1)
+            return offdiag_int<CEN>(c[ij], c[ij + 1], c[ij + m], c[ij + m + 1], zs, lz, ldz, diag);
+        return offdiag_edge<CEN>(i, j, zs, lz, ldz, diag);
+    }
+
+    /** offdiag_s at an interior node, the four cell values around it given
+     * (below-left, below-right, above-left, above-right). */
+    template <bool CEN = false>
+    __device__ __forceinline__ T offdiag_int(T cdl, T cdr, T cul, T cur, const T *zs, int lz, int ldz,
+                                             T &diag) const {
         const T zc = CEN ? zs[lz] : T(0);
-        if (i > 0 && i < m - 1 && j > 0 && j < n - 1) {
-            const T cdl = c[ij], cdr = c[ij + 1], cul = c[ij + m], cur = c[ij + m + 1];
-            diag = fm * ((cul + cdl) + (cur + cdr));
-            const T *w = zs + lz;
-            return cul * ((w[-1] - zc) * hex + (w[ldz - 1] - zc) * fc + (w[ldz] - zc) * hey)
-                 + cdl * ((w[-1] - zc) * hex + (w[-ldz - 1] - zc) * fc + (w[-ldz] - zc) * hey)
-                 + cur * ((w[1] - zc) * hex + (w[ldz + 1] - zc) * fc + (w[ldz] - zc) * hey)
-                 + cdr * ((w[1] - zc) * hex + (w[-ldz + 1] - zc) * fc + (w[-ldz] - zc) * hey);
-        }
+        diag = fm * ((cul + cdl) + (cur + cdr));
+        const T *w = zs + lz;
+        return cul * ((w[-1] - zc) * hex + (w[ldz - 1] - zc) * fc + (w[ldz] - zc) * hey)
+             + cdl * ((w[-1] - zc) * hex + (w[-ldz - 1] - zc) * fc + (w[-ldz] - zc) * hey)
+             + cur * ((w[1] - zc) * hex + (w[ldz + 1] - zc) * fc + (w[ldz] - zc) * hey)
+             + cdr * ((w[1] - zc) * hex + (w[-ldz + 1] - zc) * fc + (w[-ldz] - zc) * hey);
+    }
+
+    /** offdiag_s at a node on an edge of the grid (the cells from c). */
+    template <bool CEN = false>
+    __device__ __forceinline__ T offdiag_edge(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
+        const T zc = CEN ? zs[lz] : T(0);
         T a[9];
         coef9(i, j, a);
         diag = a[4];

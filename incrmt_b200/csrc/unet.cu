@@ -57,99 +57,134 @@ __global__ void k_bias_reduce(const float *partial, int splits, int C, float *db
     }
 }
 
+// The elementwise kernels below move eight channels (16 bytes) per thread:
+// every channel count of the network is a multiple of 16.
+
+__device__ __forceinline__ uint4 ld8(const bf16 *p) { return *reinterpret_cast<const uint4 *>(p); }
+__device__ __forceinline__ void st8(bf16 *p, uint4 v) { *reinterpret_cast<uint4 *>(p) = v; }
+__device__ __forceinline__ float bfe(const uint4 &v, int k) {
+    const uint32_t w = k < 2 ? v.x : k < 4 ? v.y : k < 6 ? v.z : v.w;
+    return __uint_as_float((k & 1) ? (w & 0xFFFF0000u) : (w << 16));
+}
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
+    return make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), pack2(f[6], f[7]));
+}
+
 /** Gradient through the ReLU: zero where the layer's output is not positive. */
 __global__ void k_relu_mask(bf16 *dY, const bf16 *Y, long n) {
-    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<long>(gridDim.x) * blockDim.x)
-        if (!(__bfloat162float(Y[i]) > 0.f)) dY[i] = __float2bfloat16(0.f);
+    const long n8 = n >> 3;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n8;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const uint4 y = ld8(Y + 8 * i);
+        uint4 d = ld8(dY + 8 * i);
+        uint32_t *dw = reinterpret_cast<uint32_t *>(&d);
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (!(bfe(y, k) > 0.f)) dw[k >> 1] &= (k & 1) ? 0x0000FFFFu : 0xFFFF0000u;
+        st8(dY + 8 * i, d);
+    }
 }
 
 /** 2x2 average pooling, NHWC. */
 __global__ void k_pool(const bf16 *X, bf16 *Y, int B, int H, int W, int C) {
-    const int Ho = H / 2, Wo = W / 2;
-    const long n = static_cast<long>(B) * Ho * Wo * C;
+    const int Ho = H / 2, Wo = W / 2, C8 = C >> 3;
+    const long n = static_cast<long>(B) * Ho * Wo * C8;
     for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        long r = i / C;
+        const int c8 = static_cast<int>(i % C8);
+        long r = i / C8;
         const int x = static_cast<int>(r % Wo);
         r /= Wo;
         const int y = static_cast<int>(r % Ho), b = static_cast<int>(r / Ho);
-        const long q = ((static_cast<long>(b) * H + 2 * y) * W + 2 * x) * C + c;
-        const float s = __bfloat162float(X[q]) + __bfloat162float(X[q + C]) + __bfloat162float(X[q + static_cast<long>(W) * C]) +
-                        __bfloat162float(X[q + static_cast<long>(W) * C + C]);
-        Y[i] = __float2bfloat16(0.25f * s);
+        const long q = ((static_cast<long>(b) * H + 2 * y) * W + 2 * x) * C + 8 * c8;
+        const uint4 v0 = ld8(X + q), v1 = ld8(X + q + C), v2 = ld8(X + q + static_cast<long>(W) * C),
+                    v3 = ld8(X + q + static_cast<long>(W) * C + C);
+        float f[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) f[k] = 0.25f * (bfe(v0, k) + bfe(v1, k) + bfe(v2, k) + bfe(v3, k));
+        st8(Y + 8 * i, pack8(f));
     }
 }
 
 /** Pooling gradient added into dX (which already holds the skip gradient). */
 __global__ void k_pool_bwd_add(const bf16 *dY, bf16 *dX, int B, int H, int W, int C) {
-    const long n = static_cast<long>(B) * H * W * C;
+    const int C8 = C >> 3;
+    const long n = static_cast<long>(B) * H * W * C8;
     for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        long r = i / C;
+        const int c8 = static_cast<int>(i % C8);
+        long r = i / C8;
         const int x = static_cast<int>(r % W);
         r /= W;
         const int y = static_cast<int>(r % H), b = static_cast<int>(r / H);
-        const long q = ((static_cast<long>(b) * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c;
-        dX[i] = __float2bfloat16(__bfloat162float(dX[i]) + 0.25f * __bfloat162float(dY[q]));
+        const long q = ((static_cast<long>(b) * (H / 2) + y / 2) * (W / 2) + x / 2) * C + 8 * c8;
+        const uint4 g = ld8(dY + q), d = ld8(dX + 8 * i);
+        float f[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) f[k] = bfe(d, k) + 0.25f * bfe(g, k);
+        st8(dX + 8 * i, pack8(f));
     }
 }
 
 /** U = [nearest 2x upsample of L (Cl channels), S (Cs channels)], NHWC. */
 __global__ void k_upcat(const bf16 *L, const bf16 *S, bf16 *U, int B, int H, int W, int Cl, int Cs) {
-    const int C = Cl + Cs;
-    const long n = static_cast<long>(B) * H * W * C;
+    const int C8 = (Cl + Cs) >> 3, L8 = Cl >> 3;
+    const long n = static_cast<long>(B) * H * W * C8;
     for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const long pix = i / C;
-        if (c < Cl) {
+        const int c8 = static_cast<int>(i % C8);
+        const long pix = i / C8;
+        if (c8 < L8) {
             const int x = static_cast<int>(pix % W);
             const long r = pix / W;
             const int y = static_cast<int>(r % H), b = static_cast<int>(r / H);
-            U[i] = L[((static_cast<long>(b) * (H / 2) + y / 2) * (W / 2) + x / 2) * Cl + c];
+            st8(U + 8 * i, ld8(L + ((static_cast<long>(b) * (H / 2) + y / 2) * (W / 2) + x / 2) * Cl + 8 * c8));
         } else {
-            U[i] = S[pix * Cs + (c - Cl)];
+            st8(U + 8 * i, ld8(S + pix * Cs + 8 * (c8 - L8)));
         }
     }
 }
 
 /** Gradients of k_upcat: dL summed over the four children, dS written. */
 __global__ void k_upcat_bwd(const bf16 *dU, bf16 *dL, bf16 *dS, int B, int H, int W, int Cl, int Cs) {
-    const int C = Cl + Cs;
-    const long nl = static_cast<long>(B) * (H / 2) * (W / 2) * Cl;
-    const long ns = static_cast<long>(B) * H * W * Cs;
+    const int C = Cl + Cs, L8 = Cl >> 3, S8 = Cs >> 3;
+    const long nl = static_cast<long>(B) * (H / 2) * (W / 2) * L8;
+    const long ns = static_cast<long>(B) * H * W * S8;
     for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < nl + ns;
          i += static_cast<long>(gridDim.x) * blockDim.x) {
         if (i < nl) {
-            const int c = static_cast<int>(i % Cl);
-            long r = i / Cl;
+            const int c8 = static_cast<int>(i % L8);
+            long r = i / L8;
             const int x = static_cast<int>(r % (W / 2));
             r /= (W / 2);
             const int y = static_cast<int>(r % (H / 2)), b = static_cast<int>(r / (H / 2));
-            float s = 0;
+            float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (int d = 0; d < 4; d++) {
                 const long pix = (static_cast<long>(b) * H + 2 * y + (d >> 1)) * W + 2 * x + (d & 1);
-                s += __bfloat162float(dU[pix * C + c]);
+                const uint4 v = ld8(dU + pix * C + 8 * c8);
+#pragma unroll
+                for (int k = 0; k < 8; k++) f[k] += bfe(v, k);
             }
-            dL[i] = __float2bfloat16(s);
+            st8(dL + 8 * i, pack8(f));
         } else {
-            const long k = i - nl, pix = k / Cs;
-            const int c = static_cast<int>(k - pix * Cs);
-            dS[k] = dU[pix * C + Cl + c];
+            const long k = i - nl, pix = k / S8;
+            const int c8 = static_cast<int>(k - pix * S8);
+            st8(dS + 8 * k, ld8(dU + pix * C + Cl + 8 * c8));
         }
     }
 }
 
 /** Network input: 3 FP32 channels into a 16-channel BF16 tensor (rest zero). */
 __global__ void k_pack_input(const float *in, bf16 *X, long P) {
-    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < P * 16;
-         i += static_cast<long>(gridDim.x) * blockDim.x) {
-        const long p = i >> 4;
-        const int c = static_cast<int>(i & 15);
-        X[i] = __float2bfloat16(c < 3 ? in[p * 3 + c] : 0.f);
+    for (long p = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; p < P;
+         p += static_cast<long>(gridDim.x) * blockDim.x) {
+        const float f[8] = {in[p * 3], in[p * 3 + 1], in[p * 3 + 2], 0.f, 0.f, 0.f, 0.f, 0.f};
+        st8(X + 16 * p, pack8(f));
+        st8(X + 16 * p + 8, make_uint4(0, 0, 0, 0));
     }
 }
 
@@ -231,8 +266,10 @@ struct Act {
 };
 
 inline int gs(long n) {
+    // up to eight 256-thread blocks per SM (all the threads an SM holds), so
+    // that the grid-stride loops keep enough loads in flight
     long b = (n + 255) / 256;
-    return static_cast<int>(b < 4L * kB200SMs ? (b > 0 ? b : 1) : 4L * kB200SMs);
+    return static_cast<int>(b < 8L * kB200SMs ? (b > 0 ? b : 1) : 8L * kB200SMs);
 }
 
 }  // namespace
@@ -422,7 +459,7 @@ struct UNet {
         int r = ensure(B, H, W);
         if (r) return r;
         const long P = static_cast<long>(B) * H * W;
-        k_pack_input<<<gs(P * 16), 256, 0, s>>>(in, acts[0].x, P);
+        k_pack_input<<<gs(P), 256, 0, s>>>(in, acts[0].x, P);
         launches++;
         int a = 1, k = 0;
         bf16 *cur = acts[0].x;
@@ -430,7 +467,7 @@ struct UNet {
         for (int l = 0; l < levels; l++) {
             const int Hl = H >> l, Wl = W >> l;
             if (l > 0) {
-                k_pool<<<gs(static_cast<long>(B) * Hl * Wl * C(l - 1)), 256, 0, s>>>(cur, acts[a].x, B, Hl * 2, Wl * 2, C(l - 1));
+                k_pool<<<gs(static_cast<long>(B) * Hl * Wl * C(l - 1) / 8), 256, 0, s>>>(cur, acts[a].x, B, Hl * 2, Wl * 2, C(l - 1));
                 launches++;
                 cur = acts[a++].x;
             }
@@ -442,7 +479,7 @@ struct UNet {
         }
         for (int l = levels - 2; l >= 0; l--) {
             const int Hl = H >> l, Wl = W >> l;
-            k_upcat<<<gs(static_cast<long>(B) * Hl * Wl * (C(l + 1) + C(l))), 256, 0, s>>>(
+            k_upcat<<<gs(static_cast<long>(B) * Hl * Wl * (C(l + 1) + C(l)) / 8), 256, 0, s>>>(
                 cur, acts[skip[l]].x, acts[a].x, B, Hl, Wl, C(l + 1), C(l));
             launches++;
             cur = acts[a++].x;
@@ -480,14 +517,14 @@ struct UNet {
             const int Hl = H >> l, Wl = W >> l;
             // acts[a] = conv2 output of this decoder level, acts[a-1] = conv1, acts[a-2] = cat
             const long n2 = static_cast<long>(B) * Hl * Wl * C(l);
-            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[a].g, acts[a].x, n2);
+            k_relu_mask<<<gs(n2 / 8), 256, 0, s>>>(acts[a].g, acts[a].x, n2);
             if ((r = conv_backward(convs[k], acts[a - 1].x, acts[a].g, acts[a - 1].g, B, Hl, Wl, s))) return r;
-            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[a - 1].g, acts[a - 1].x, n2);
+            k_relu_mask<<<gs(n2 / 8), 256, 0, s>>>(acts[a - 1].g, acts[a - 1].x, n2);
             if ((r = conv_backward(convs[k - 1], acts[a - 2].x, acts[a - 1].g, acts[a - 2].g, B, Hl, Wl, s))) return r;
             launches += 2;
             // Split the concatenation gradient: coarser level's output and the skip.
             const int lower = (l + 1 == levels - 1) ? skip[levels - 1] : a - 3;
-            k_upcat_bwd<<<gs(static_cast<long>(B) * Hl * Wl * (C(l + 1) + C(l))), 256, 0, s>>>(
+            k_upcat_bwd<<<gs(static_cast<long>(B) * Hl * Wl * (C(l + 1) + C(l)) / 8), 256, 0, s>>>(
                 acts[a - 2].g, acts[lower].g, acts[skip[l]].g, B, Hl, Wl, C(l + 1), C(l));
             launches++;
             k -= 2;
@@ -499,14 +536,14 @@ struct UNet {
             const int Hl = H >> l, Wl = W >> l;
             const int o2 = skip[l], o1 = o2 - 1, in = (l > 0) ? pool_idx[l] : 0;
             const long n2 = static_cast<long>(B) * Hl * Wl * C(l);
-            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[o2].g, acts[o2].x, n2);
+            k_relu_mask<<<gs(n2 / 8), 256, 0, s>>>(acts[o2].g, acts[o2].x, n2);
             if ((r = conv_backward(convs[2 * l + 1], acts[o1].x, acts[o2].g, acts[o1].g, B, Hl, Wl, s))) return r;
-            k_relu_mask<<<gs(n2), 256, 0, s>>>(acts[o1].g, acts[o1].x, n2);
+            k_relu_mask<<<gs(n2 / 8), 256, 0, s>>>(acts[o1].g, acts[o1].x, n2);
             if ((r = conv_backward(convs[2 * l], acts[in].x, acts[o1].g, l > 0 ? acts[in].g : nullptr, B, Hl, Wl, s))) return r;
             launches += 2;
             if (l > 0) {
                 // Pooling gradient into the finer level's output gradient.
-                k_pool_bwd_add<<<gs(static_cast<long>(B) * (Hl * 2) * (Wl * 2) * C(l - 1)), 256, 0, s>>>(
+                k_pool_bwd_add<<<gs(static_cast<long>(B) * (Hl * 2) * (Wl * 2) * C(l - 1) / 8), 256, 0, s>>>(
                     acts[in].g, acts[skip[l - 1]].g, B, Hl * 2, Wl * 2, C(l - 1));
                 launches++;
             }
@@ -650,6 +687,8 @@ int incrmt_conv_bf16(const void *d_x, int batch, int H, int W, int cin, const vo
 }
 
 int incrmt_conv_status(void) { return incrmt::conv_tc_status(); }
+
+int incrmt_conv_set_variant(int variant) { return incrmt::conv_tc_set_variant(variant); }
 
 long long incrmt_conv_wgrad_workspace(int batch, int H, int W, int cin, int cout, int taps) {
     if (batch < 1 || H < 1 || W < 1 || cin < 16 || cout < 16 || (taps != 1 && taps != 9)) return 0;

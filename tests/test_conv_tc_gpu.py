@@ -10,7 +10,9 @@ chunks of 16 and of 32), images whose width is not a multiple of the 128-pixel t
 partial tiles TMA fills with zeros and the epilogue masks), tiles one row
 high (width 128) and eight rows high (width 16), output channels split over
 two CTAs (384 = 2 x 192), the 1x1 head, bias and ReLU, and the reversed taps
-of the input-gradient convolution.
+of the input-gradient convolution; every 3x3 case runs with each kernel
+choice (incrmt_conv_set_variant: automatic, one tap per stage, row reuse,
+whose 16 x 8 tiles are partial at widths 40, 56 and 8 and heights 20 and 12).
 """
 import numpy as np
 import pytest
@@ -28,13 +30,19 @@ CASES = [
     (2, 32, 32, 32, 16, 1, False, True, False),
     (1, 20, 56, 32, 48, 9, False, False, True),
     (1, 16, 32, 384, 64, 9, False, False, True),
+    (1, 12, 8, 32, 32, 9, True, True, False),
+    (3, 20, 40, 64, 64, 9, True, True, True),
 ]
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("B,H,W,cin,cout,taps,relu,use_bias,flip", CASES)
-def test_conv_matches_torch(gpu, B, H, W, cin, cout, taps, relu, use_bias, flip):
+def test_conv_matches_torch(gpu, B, H, W, cin, cout, taps, relu, use_bias, flip, variant):
     import torch
     from incrmt_b200 import capi
+    if taps == 1 and variant:
+        pytest.skip("the kernel choice concerns 3x3 convolutions")
+    capi.conv_set_variant(variant)
     dev = torch.device("cuda")
     g = torch.Generator(device="cpu").manual_seed(B * 1000 + H * 10 + cin + cout + taps)
     x = torch.randn(B, H, W, cin, generator=g).to(torch.bfloat16).to(dev)
@@ -42,9 +50,12 @@ def test_conv_matches_torch(gpu, B, H, W, cin, cout, taps, relu, use_bias, flip)
     bias = torch.randn(cout, generator=g).to(dev) if use_bias else None
     y = torch.full((B, H, W, cout), float("nan"), dtype=torch.bfloat16, device=dev)
     torch.cuda.synchronize()
-    capi.conv_bf16(x.data_ptr(), B, H, W, cin, wk.data_ptr(), taps, cout, y.data_ptr(),
-                   bias.data_ptr() if bias is not None else 0, relu=relu, flip=flip)
-    capi.conv_status()
+    try:
+        capi.conv_bf16(x.data_ptr(), B, H, W, cin, wk.data_ptr(), taps, cout, y.data_ptr(),
+                       bias.data_ptr() if bias is not None else 0, relu=relu, flip=flip)
+        capi.conv_status()
+    finally:
+        capi.conv_set_variant(0)
     # reference: weights [tap][cout][cin] -> OIHW (tap = 3 ty + tx), taps reversed with flip
     w = wk.float()
     if flip:

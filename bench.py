@@ -136,6 +136,28 @@ def _traffic(key):
         return json.load(f).get(key)
 
 
+def vcycle_pass_bytes(m, n, c0, w=8, tail=1024):
+    """Compulsory bytes of one FP64 V-cycle as the kernels run it on an
+    isotropic grid (standard coarsening): on a level of N unknowns with c
+    coefficient words each (c0 on the fine level, 9 on the Galerkin levels),
+    two tile-fused smoothing launches read z, b and the coefficients and write
+    z ((3 + c) words each), the restriction reads z, b, the coefficients and
+    four prolongation weights (6 + c) and writes b and z of the coarse level,
+    the prolongation reads the weights and z and writes z (6) and reads each
+    coarse value once: (18 + 3c) N + 3 N_coarse words; the fine level adds the
+    residual norm (2 + c) N. Levels of at most `tail` unknowns run in one
+    block from shared memory and are not counted."""
+    total, c, first = 0.0, c0, True
+    while m * n > tail:
+        mc, nc = (m + 1) // 2, (n + 1) // 2
+        total += (18 + 3 * c) * m * n + 3 * mc * nc
+        if first:
+            total += (2 + c) * m * n
+            first = False
+        m, n, c = mc, nc, 9
+    return total * w
+
+
 def _roofline(key, ms, nbytes, launches, kernel, rule):
     """Roofline object of a kernel timed live with CUDA events: achieved =
     algorithmic bytes / device time, against the measured copy bandwidth."""
@@ -929,6 +951,16 @@ def run_ours(args, ws, rank, local, dist):
         line["roofline"]["vcycle_level"] = {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                                             "peak_kind": kind, "bytes_per_unknown_per_vcycle": bpu,
                                             "time": "whole step including the density setup"}
+        if prec == capi.PREC_FP64:
+            pb = vcycle_pass_bytes(m, m, 2)
+            ach2 = float(np.mean(vcs)) * pb / (ms_max / args.steps / 1e3) / 1e9
+            line["roofline"]["vcycle_passes"] = {
+                "achieved": ach2, "peak": peak, "unit": "GB/s", "frac": ach2 / peak, "peak_kind": kind,
+                "bytes_per_vcycle": pb, "time": "whole step including the density setup",
+                "bytes_rule": "per level of N unknowns with c coefficient words (2 fine MAC, 9 Galerkin): "
+                              "(18 + 3c) N w for two smoothing launches, the restriction and the prolongation "
+                              "as implemented (each reading its arrays once), 3 w per coarse unknown, and the "
+                              "fine residual norm (2 + c) N w"}
     print(json.dumps(line))
     release()
 

@@ -98,14 +98,11 @@ int incrmt_mg_vcycle_device(incrmt_mg *h, const double *d_b, double *d_z);
  * reference counterpart (instrumentation). */
 int incrmt_mg_set_profiling(incrmt_mg *h, int on);
 
-/** Tile-fused smoothing (no reference counterpart): two Gauss-Seidel sweeps
- * per launch in shared-memory tiles wherever the level's periodic directions
- * have even sizes, with results identical to one launch per colour in the
- * V-cycle's four-colour order. Mode 1 (default) stages each tile's iterate,
- * right-hand side and coefficients in shared memory once per launch; 2 reads
- * the coefficients through the caches in every colour phase; 0 runs one
- * launch per colour everywhere. Modes 0 and 2 exist to check the identity;
- * any other value is INCRMT_ERR_BADARG. */
+/** Tile-fused smoothing (on by default; no reference counterpart): two
+ * Gauss-Seidel sweeps per launch in shared-memory tiles wherever the level's
+ * periodic directions have even sizes, with results identical to one launch
+ * per colour in the V-cycle's four-colour order. Off (0) runs one launch per
+ * colour everywhere; it exists to check that identity. */
 int incrmt_mg_set_tiles(incrmt_mg *h, int on);
 
 /** Lagged coarse operators (no reference counterpart; default 1). With

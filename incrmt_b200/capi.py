@@ -182,9 +182,8 @@ class MGSolver:
         check(lib().incrmt_mg_set_profiling(self._h, int(on)))
 
     def set_tiles(self, on=True):
-        """Tile-fused smoothing (incrmt_mg_set_tiles): True / 1 stages the
-        tiles' inputs in shared memory, 2 reads coefficients through the
-        caches, False / 0 runs one launch per colour."""
+        """Tile-fused smoothing (incrmt_mg_set_tiles); off runs one launch
+        per colour."""
         check(lib().incrmt_mg_set_tiles(self._h, int(on)))
 
     def set_coarse_refresh(self, every):

@@ -116,8 +116,7 @@ int incrmt_mg_set_tiles(incrmt_mg *h, int on) {
     if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
     incrmt::Multigrid &mg = h->mg;
     if (mg.stream) INCRMT_CK(cudaStreamSynchronize(mg.stream));
-    if (on < 0 || on > 2) { set_error("tile mode %d not in 0..2", on); return INCRMT_ERR_BADARG; }
-    mg.tiles = on;
+    mg.tiles = on != 0;
     if (mg.gexec) {  // the captured V-cycle holds the other launches
         cudaGraphExecDestroy(mg.gexec);
         mg.gexec = nullptr;

@@ -509,11 +509,12 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
     int S;
     size_t per;
     if (ROWS) {
-        // as many stages as the CTA has steps, within half an SM's shared
-        // memory (two CTAs per SM), at least two
+        // as many stages as the CTA has steps, within a quarter of an SM's
+        // shared memory (four CTAs per SM where the stages are small), at
+        // least two
         per = static_cast<size_t>(kTileM + 2 * kRowsW + 3 * Nt) * KC * 2;
         const int steps = 3 * (Cin / KC);
-        S = static_cast<int>((110 * 1024) / per);
+        S = static_cast<int>((56 * 1024) / per);
         if (S > steps) S = steps;
         if (S > 8) S = 8;
         if (S < 2) S = 2;

@@ -456,26 +456,9 @@ __global__ void __launch_bounds__(256) k_smooth_tile_gen(GenOp<T> op, const T *z
             const bool l = px || ir > 0, r = px || ir < m - 1, d = py || jr > 0, u = py || jr < n - 1;
             const T zc = sizeof(T) == 8 ? T(0) : zs[lz];
             T diag = cs[4 * LA + lz];
-            T s = 0, a = 0;
-            if (d) {
-                if (l) { s += cs[lz] * (zs[lz - LW - 1] - zc); a += cs[lz]; }
-                s += cs[LA + lz] * (zs[lz - LW] - zc); a += cs[LA + lz];
-                if (r) { s += cs[2 * LA + lz] * (zs[lz - LW + 1] - zc); a += cs[2 * LA + lz]; }
-            }
-            if (l) { s += cs[3 * LA + lz] * (zs[lz - 1] - zc); a += cs[3 * LA + lz]; }
-            if (r) { s += cs[5 * LA + lz] * (zs[lz + 1] - zc); a += cs[5 * LA + lz]; }
-            if (u) {
-                if (l) { s += cs[6 * LA + lz] * (zs[lz + LW - 1] - zc); a += cs[6 * LA + lz]; }
-                s += cs[7 * LA + lz] * (zs[lz + LW] - zc); a += cs[7 * LA + lz];
-                if (r) { s += cs[8 * LA + lz] * (zs[lz + LW + 1] - zc); a += cs[8 * LA + lz]; }
-            }
-            if constexpr (sizeof(T) == 8) {
-                zs[lz] = (bs[lz] - s) / diag;
-            } else {
-                const T rs = diag;  // the row sum
-                diag = rs - a;
-                zs[lz] = zc + (bs[lz] - s - rs * zc) / diag;
-            }
+            const T rs = diag;  // the row sum in single precision
+            const T s = GenOp<T>::template gen_sum<sizeof(T) == 4>(l, r, d, u, cs + lz, LA, zs + lz, 1, LW, zc, diag);
+            zs[lz] = gs_value(bs[lz], s, diag, zc, rs);
         }
         __syncthreads();
     }
@@ -489,185 +472,6 @@ __global__ void __launch_bounds__(256) k_smooth_tile_gen(GenOp<T> op, const T *z
 template <class T, int SWEEPS = 2, int TW = 16, int TH = 16>
 constexpr int gen_tile_smem() {
     return 11 * (TW + 8 * SWEEPS) * (TH + 8 * SWEEPS) * static_cast<int>(sizeof(T));
-}
-
-/** Shared memory of k_smooth_rb_mac<T, SWEEPS, TW, TH>: iterate and
- * right-hand side on the LW x LH region, x-edge coefficients on (LW+1) x LH,
- * y-edge coefficients on LW x (LH+1). */
-template <class T, int SWEEPS, int TW, int TH>
-constexpr int rb_mac_smem() {
-    constexpr int LW = TW + 4 * SWEEPS, LH = TH + 4 * SWEEPS;
-    return (2 * LW * LH + (LW + 1) * LH + LW * (LH + 1)) * static_cast<int>(sizeof(T));
-}
-
-/** Shared memory of k_smooth_tile_fem<T, SWEEPS, TW, TH>: iterate and
- * right-hand side on the LW x LH region, cell values on (LW+1) x (LH+1). */
-template <class T, int SWEEPS, int TW, int TH>
-constexpr int fem_tile_smem() {
-    constexpr int LW = TW + 8 * SWEEPS, LH = TH + 8 * SWEEPS;
-    return (2 * LW * LH + (LW + 1) * (LH + 1)) * static_cast<int>(sizeof(T));
-}
-
-/** k_smooth_rb for the fine MAC system with every input staged once: the
- * block copies the iterate, the right-hand side and the edge coefficients of
- * its region to shared memory with coalesced loads (each value read from
- * global memory once per launch), then runs the phases on shared memory
- * alone; k_smooth_rb reads the coefficients of each colour's points in every
- * phase, every second double of a line, through L1/L2. Same arithmetic
- * (MacOp::offdiag_v), so the same results. Across a periodic seam the staged
- * edge array holds the image of the first edge; a point on the last column
- * (row) reads its right (upper) edge from global memory, as the unstaged
- * kernels do. */
-template <class T, int SWEEPS, int TW, int TH>
-__global__ void __launch_bounds__(256, 2) k_smooth_rb_mac(MacOp<T> op, const T *zin, T *zout, const T *b, int m,
-                                                          int n) {
-    constexpr int H = 2 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H, NP = 2 * SWEEPS, LA = LW * LH, LX = LW + 1;
-    extern __shared__ __align__(16) unsigned char rbm_smem[];
-    T *zs = reinterpret_cast<T *>(rbm_smem);
-    T *bs = zs + LA;
-    T *xs = bs + LA;       // x-edge left of local (li, lj) at xs[li + LX * lj], li = 0..LW
-    T *ys = xs + LX * LH;  // y-edge below local (li, lj) at ys[li + LW * lj], lj = 0..LH
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
-    const int gx0 = x0 - H, gy0 = y0 - H;
-    const bool px = op.px, py = op.py;
-    for (int lj = ty; lj <= LH; lj += 8) {
-        int j = gy0 + lj;
-        if (py) j = wrap_index(j, n);
-        const bool jc = lj < LH && j >= 0 && j < n, je = j >= 0 && j <= n;
-        for (int li = tx; li <= LW; li += 32) {
-            int i = gx0 + li;
-            if (px) i = wrap_index(i, m);
-            if (jc) {
-                if (li < LW && i >= 0 && i < m) {
-                    const long ij = i + static_cast<long>(m) * j;
-                    zs[li + LW * lj] = zin[ij];
-                    bs[li + LW * lj] = b[ij];
-                }
-                if (i >= 0 && i <= m) xs[li + LX * lj] = op.ex[static_cast<long>(j) * (m + 1) + i];
-            }
-            if (je && li < LW && i >= 0 && i < m) ys[li + LW * lj] = op.ey[static_cast<long>(j) * m + i];
-        }
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int p = 0; p < NP; p++) {
-        const int e = NP - 1 - p, parity = p & 1;
-        int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
-        if (!px) {
-            if (ilo < 0) ilo = 0;
-            if (ihi > m - 1) ihi = m - 1;
-        }
-        if (!py) {
-            if (jlo < 0) jlo = 0;
-            if (jhi > n - 1) jhi = n - 1;
-        }
-        for (int j = jlo + ty; j <= jhi; j += 8) {
-            const int i0 = ilo + (((ilo + j) & 1) != parity);
-            const int jr = py ? wrap_index(j, n) : j;
-            const int lj = j - gy0;
-            for (int i = i0 + 2 * tx; i <= ihi; i += 64) {
-                const int li = i - gx0, lz = li + LW * lj, lx = li + LX * lj;
-                const int ir = px ? wrap_index(i, m) : i;
-                const T el = xs[lx];
-                const T er = (px && ir == m - 1) ? op.ex[static_cast<long>(jr) * (m + 1) + m] : xs[lx + 1];
-                const T ed = ys[lz];
-                const T eu = (py && jr == n - 1) ? op.ey[static_cast<long>(n) * m + ir] : ys[lz + LW];
-                T diag;
-                if constexpr (sizeof(T) == 8) {
-                    const T off = op.offdiag_v(ir, jr, el, er, ed, eu, zs, lz, LW, diag);
-                    zs[lz] = (bs[lz] - off) / diag;
-                } else {
-                    const T zc = zs[lz];
-                    const T off = op.template offdiag_v<true>(ir, jr, el, er, ed, eu, zs, lz, LW, diag);
-                    zs[lz] = zc + (bs[lz] - off - op.rowsum(ir, jr) * zc) / diag;
-                }
-            }
-        }
-        __syncthreads();
-    }
-    for (int lj = H + ty; lj < H + TH; lj += 8) {
-        const int j = gy0 + lj;
-        if (j >= n) break;
-        for (int li = H + tx; li < H + TW; li += 32) {
-            const int i = gx0 + li;
-            if (i < m) zout[i + static_cast<long>(m) * j] = zs[li + LW * lj];
-        }
-    }
-}
-
-/** k_smooth_tile for the fine FEM system with its inputs staged once: the
- * iterate, the right-hand side and the cell values of the region go to
- * shared memory with coalesced loads before the first phase. Interior nodes
- * take their four cells from shared memory (FemOp::offdiag_int), nodes on an
- * edge of the grid from global memory (FemOp::offdiag_edge), exactly as
- * FemOp::offdiag_s does, so the results are those of k_smooth_tile. */
-template <class T, int SWEEPS, int TW, int TH>
-__global__ void __launch_bounds__(256, 2) k_smooth_tile_fem(FemOp<T> op, const T *zin, T *zout, const T *b, int m,
-                                                            int n) {
-    constexpr int H = 4 * SWEEPS, LW = TW + 2 * H, LH = TH + 2 * H, LA = LW * LH, LX = LW + 1;
-    extern __shared__ __align__(16) unsigned char fem_smem[];
-    T *zs = reinterpret_cast<T *>(fem_smem);
-    T *bs = zs + LA;
-    T *cs = bs + LA;  // cell value of local (li, lj) at cs[li + LX * lj], li = 0..LW, lj = 0..LH
-    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
-    const int gx0 = x0 - H, gy0 = y0 - H;
-    const bool px = op.px, py = op.py;
-    for (int t = threadIdx.x; t < LX * (LH + 1); t += blockDim.x) {
-        const int li = t % LX, lj = t / LX;
-        int i = gx0 + li, j = gy0 + lj;
-        if (px) i = wrap_index(i, m);
-        if (py) j = wrap_index(j, n);
-        if (i >= 0 && i < m && j >= 0 && j < n) {
-            const long ij = i + static_cast<long>(m) * j;
-            cs[t] = op.c[ij];
-            if (li < LW && lj < LH) {
-                zs[li + LW * lj] = zin[ij];
-                bs[li + LW * lj] = b[ij];
-            }
-        }
-    }
-    __syncthreads();
-    const int pis[4] = {0, 1, 1, 0}, pjs[4] = {0, 1, 0, 1};
-    constexpr int P = 4 * SWEEPS;
-#pragma unroll 1
-    for (int p = 0; p < P; p++) {
-        const int e = P - 1 - p, c = p & 3;
-        int ilo = x0 - e, ihi = x0 + TW - 1 + e, jlo = y0 - e, jhi = y0 + TH - 1 + e;
-        if (!px) {
-            if (ilo < 0) ilo = 0;
-            if (ihi > m - 1) ihi = m - 1;
-        }
-        if (!py) {
-            if (jlo < 0) jlo = 0;
-            if (jhi > n - 1) jhi = n - 1;
-        }
-        const int i0 = ilo + ((ilo & 1) != pis[c]), j0 = jlo + ((jlo & 1) != pjs[c]);
-        const int ni = i0 <= ihi ? (ihi - i0) / 2 + 1 : 0, nj = j0 <= jhi ? (jhi - j0) / 2 + 1 : 0;
-        for (int t = threadIdx.x; t < ni * nj; t += blockDim.x) {
-            const int i = i0 + 2 * (t % ni), j = j0 + 2 * (t / ni);
-            const int li = i - gx0, lj = j - gy0, lz = li + LW * lj, lc = li + LX * lj;
-            const int ir = px ? wrap_index(i, m) : i, jr = py ? wrap_index(j, n) : j;
-            const bool interior = ir > 0 && ir < m - 1 && jr > 0 && jr < n - 1;
-            T diag, off;
-            if constexpr (sizeof(T) == 8) {
-                off = interior ? op.offdiag_int(cs[lc], cs[lc + 1], cs[lc + LX], cs[lc + LX + 1], zs, lz, LW, diag)
-                               : op.offdiag_edge(ir, jr, zs, lz, LW, diag);
-                zs[lz] = (bs[lz] - off) / diag;
-            } else {
-                const T zc = zs[lz];
-                off = interior ? op.template offdiag_int<true>(cs[lc], cs[lc + 1], cs[lc + LX], cs[lc + LX + 1], zs,
-                                                               lz, LW, diag)
-                               : op.template offdiag_edge<true>(ir, jr, zs, lz, LW, diag);
-                zs[lz] = zc + (bs[lz] - off - op.rowsum(ir, jr) * zc) / diag;
-            }
-        }
-        __syncthreads();
-    }
-    for (int t = threadIdx.x; t < TW * TH; t += blockDim.x) {
-        const int i = x0 + t % TW, j = y0 + t / TW;
-        if (i < m && j < n) zout[i + static_cast<long>(m) * j] = zs[(i - gx0) + LW * (j - gy0)];
-    }
 }
 
 /** Tile-fused red-black Gauss-Seidel for a five-point operator (the fine MAC
@@ -1114,7 +918,7 @@ __global__ void k_resnorm(Op op, const double *z, const double *b, int m, int n,
             const long q = i + static_cast<long>(m) * j;
             double diag;
             const double off = op.offdiag(i, j, z, diag);
-            const double r = b[q] - off - diag * z[q];
+            const double r = sub_rn(sub_rn(b[q], off), mul_rn(diag, z[q]));
             if (rf) rf[q] = static_cast<float>(r);
             acc += r * r;
         }
@@ -1129,7 +933,7 @@ __global__ void k_apply(Op op, const double *z, double *out, int m, int n) {
     if (i >= m || j >= n) return;
     double diag;
     const double off = op.offdiag(i, j, z, diag);
-    out[i + m * j] = off + diag * z[i + m * j];
+    out[i + m * j] = add_rn(off, mul_rn(diag, z[i + m * j]));
 }
 
 __global__ void k_sumsq(const double *b, long N, double *partial) {
@@ -1199,8 +1003,8 @@ const dim3 kBlk2(32, 8);
  * by CUDA events and credited with its algorithmic bytes: (units updated) x
  * bytes_per_unit. */
 template <class Op, class T>
-int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, bool staged, cudaStream_t s, long long &nl,
-           T **res, Multigrid *prof = nullptr, double bytes_per_unit = 0) {
+int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStream_t s, long long &nl, T **res,
+           Multigrid *prof = nullptr, double bytes_per_unit = 0) {
     *res = z;
     if (sweeps == 2 && zalt && (!op.px || m % 2 == 0) && (!op.py || n % 2 == 0)) {
         // Two sweeps per launch with shared-memory tiles (identical results);
@@ -1208,28 +1012,8 @@ int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, bool stag
         const dim3 b64(cdiv(m, 64), cdiv(n, 32)), b32(cdiv(m, 32), cdiv(n, 16)), b16(cdiv(m, 16), cdiv(n, 16));
         if (prof) { int r = prof->prof_begin(static_cast<double>(m) * n * 2 * bytes_per_unit); if (r) return r; }
         bool done = false;
-        const bool big = static_cast<int>(b64.x * b64.y) >= 2 * kB200SMs;
-        if constexpr (std::is_same<Op, MacOp<T>>::value) {
-            if (big && staged) {
-                k_smooth_rb_mac<T, 2, 64, 32><<<b64, 256, rb_mac_smem<T, 2, 64, 32>(), s>>>(op, z, zalt, b, m, n);
-                done = true;
-            }
-        }
-        if constexpr (std::is_same<Op, FemOp<T>>::value) {
-            if (big && staged) {
-                k_smooth_tile_fem<T, 2, 64, 32><<<b64, 256, fem_tile_smem<T, 2, 64, 32>(), s>>>(op, z, zalt, b, m, n);
-                done = true;
-            }
-        }
-        if constexpr (std::is_same<Op, GenOp<T>>::value) {
-            const dim3 g32(cdiv(m, 32), cdiv(n, 32));
-            if (!done && staged && static_cast<int>(g32.x * g32.y) >= kB200SMs) {
-                k_smooth_tile_gen<T, 2, 32, 32><<<g32, 256, gen_tile_smem<T, 2, 32, 32>(), s>>>(op, z, zalt, b, m, n);
-                done = true;
-            }
-        }
         if constexpr (Op::kFivePoint) {
-            if (!done && big) {
+            if (static_cast<int>(b64.x * b64.y) >= 2 * kB200SMs) {
                 k_smooth_rb<Op, T, 2, 64, 32><<<b64, 256, 0, s>>>(op, z, zalt, b, m, n);
                 done = true;
             }
@@ -1398,18 +1182,7 @@ int Multigrid::build_hierarchy() {
                                    gen_tile_smem<float>()));
     INCRMT_CK(cudaFuncSetAttribute(k_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kTailSmemBudget)));
-    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_gen<double, 2, 32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   gen_tile_smem<double, 2, 32, 32>()));
-    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_gen<float, 2, 32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   gen_tile_smem<float, 2, 32, 32>()));
-    INCRMT_CK(cudaFuncSetAttribute(k_smooth_rb_mac<double, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   rb_mac_smem<double, 2, 64, 32>()));
-    INCRMT_CK(cudaFuncSetAttribute(k_smooth_rb_mac<float, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   rb_mac_smem<float, 2, 64, 32>()));
-    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_fem<double, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   fem_tile_smem<double, 2, 64, 32>()));
-    INCRMT_CK(cudaFuncSetAttribute(k_smooth_tile_fem<float, 2, 64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   fem_tile_smem<float, 2, 64, 32>()));
+
     const int gal_smem = static_cast<int>(galerkin_tile_smem(true, true));
     INCRMT_CK(set_galerkin_attr<MacOp<double>>(gal_smem));
     INCRMT_CK(set_galerkin_attr<FemOp<double>>(gal_smem));
@@ -1605,14 +1378,14 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
     double *cur = z;
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac64();
-        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     } else if (l == 0) {
         auto op = fem64();
-        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     } else {
-        if ((r = smooth(g, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur))) return r;
+        if ((r = smooth(g, z, tiles ? L.z2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
         restrict_launch(tiles, g, stream, cur, b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.b, C.z, L.P);
     }
     launches++;
@@ -1622,9 +1395,9 @@ int Multigrid::cycle64(int l, const double *b0, double *z0) {
     launches++;
     INCRMT_CKL("k_prolong");
     double *alt = !tiles ? nullptr : cur == z ? L.z2 : z, *out = cur;
-    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac64(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
-    else if (l == 0) r = smooth(fem64(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
-    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out);
+    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac64(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
+    else if (l == 0) r = smooth(fem64(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
+    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
     if (r) return r;
     if (out != z) INCRMT_CK(cudaMemcpyAsync(z, out, sizeof(double) * L.N, cudaMemcpyDeviceToDevice, stream));
     return INCRMT_OK;
@@ -1692,14 +1465,14 @@ int Multigrid::cycle32(int l) {
     const double bpu = 4.0 * (sys == INCRMT_SYS_MAC ? 5 : 4);  // FP32 words: z, b, coefficients in; z out
     if (l == 0 && sys == INCRMT_SYS_MAC) {
         auto op = mac32();
-        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else if (l == 0) {
         auto op = fem32();
-        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur, pf, bpu))) return r;
+        if ((r = smooth(op, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur, pf, bpu))) return r;
         restrict_launch(tiles, op, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     } else {
-        if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, tiles == 1, stream, launches, &cur))) return r;
+        if ((r = smooth(g, z, tiles ? L.zf2 : nullptr, b, L.m, L.n, kNu1, stream, launches, &cur))) return r;
         restrict_launch(tiles, g, stream, static_cast<const float *>(cur), b, L.m, L.n, px, py, L.kx, L.ky, C.m, C.n, C.bf, C.zf, L.P);
     }
     launches++;
@@ -1709,9 +1482,9 @@ int Multigrid::cycle32(int l) {
     launches++;
     INCRMT_CKL("k_prolong");
     float *alt = !tiles ? nullptr : cur == z ? L.zf2 : z, *out = cur;
-    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac32(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
-    else if (l == 0) r = smooth(fem32(), cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out, pf, bpu);
-    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, tiles == 1, stream, launches, &out);
+    if (l == 0 && sys == INCRMT_SYS_MAC) r = smooth(mac32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
+    else if (l == 0) r = smooth(fem32(), cur, alt, b, L.m, L.n, kNu2, stream, launches, &out, pf, bpu);
+    else r = smooth(g, cur, alt, b, L.m, L.n, kNu2, stream, launches, &out);
     if (r) return r;
     if (out != z) INCRMT_CK(cudaMemcpyAsync(z, out, sizeof(float) * L.N, cudaMemcpyDeviceToDevice, stream));
     return INCRMT_OK;

@@ -70,11 +70,7 @@ public:
     const double *lag_rho = nullptr; // density of the last set_density_lagged (read again on a retry)
     int lag_ld = 0;
     bool f32_stale = true;           // FP32 Galerkin stencils not cast since the last rebuild
-    // Smoothing and restriction kernels: 1 tile-fused with the inputs staged
-    // in shared memory (default), 2 tile-fused reading the coefficients
-    // through the caches, 0 one launch per colour and one thread per unknown.
-    // All three give the same results, bit for bit.
-    int tiles = 1;
+    bool tiles = true;               // tile-fused smoothing where it applies
     int tail_level = -1;             // first level run by the one-block tail kernel
     cudaGraphExec_t gexec = nullptr; // captured V-cycle + norm
     int gkey_prec = -1;

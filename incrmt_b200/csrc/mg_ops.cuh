@@ -25,12 +25,35 @@
 
 namespace incrmt {
 
+// Every product and sum of the stencil arithmetic is written with an explicit
+// rounding (no fused multiply-add): the compiler would otherwise contract
+// some of them into FMAs, and which ones can depend on the code around an
+// inlined expression, so that kernels computing the same update in the same
+// order could round it differently. With explicit operations the smoothers
+// (one launch per colour, tiled, staged) agree bit for bit, and the FP64
+// arithmetic is that of the oracle on the CPU, which fuses nothing.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+/** t + a*b, the product rounded first. */
+template <class T>
+__device__ __forceinline__ T acc_rn(T t, T a, T b) { return add_rn(t, mul_rn(a, b)); }
+/** z - zc in the centred form, z itself otherwise. */
+template <bool CEN, class T>
+__device__ __forceinline__ T cen(T z, T zc) {
+    if constexpr (CEN) return sub_rn(z, zc);
+    else return z;
+}
+
 /** a - b*c with the product rounded before the difference in double (the
  * reference's a_cc, mgs_mac.hh:93-97, evaluated as the CPU does, without a
  * fused multiply-add), so that the MAC diagonal and the prolongation weights
  * built from it agree with the oracle's to the last bit; fused in single. */
 __device__ __forceinline__ double mac_diag(double a, double b, double c) { return __dsub_rn(a, __dmul_rn(b, c)); }
-__device__ __forceinline__ float mac_diag(float a, float b, float c) { return a - b * c; }
+__device__ __forceinline__ float mac_diag(float a, float b, float c) { return __fmaf_rn(-b, c, a); }
 
 /** Variable-density MAC system (mgs_mac_varying_rho, mgs_mac.hh:64-102,
  * mgs_mac.cc:49-54). Unknowns are the m x n cells. The edge reciprocal
@@ -53,13 +76,20 @@ struct MacOp {
         const T ed = ey[j * m + i], eu = ey[(j + 1) * m + i];
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         T sx = 0, sy = 0;
-        if (l) sx = el * (z[i > 0 ? ij - 1 : ij + m - 1] - (CEN ? zc : T(0)));
-        if (r) sx += er * (z[i < m - 1 ? ij + 1 : ij + 1 - m] - (CEN ? zc : T(0)));
-        if (d) sy = ed * (z[j > 0 ? ij - m : ij + m * (n - 1)] - (CEN ? zc : T(0)));
-        if (u) sy += eu * (z[j < n - 1 ? ij + m : ij - m * (n - 1)] - (CEN ? zc : T(0)));
-        diag = mac_diag(-xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0))))),
-                        yysp, (d ? ed : T(0)) + (u ? eu : T(0)));
-        return xxsp * sx + yysp * sy;
+        if (l) sx = mul_rn(el, cen<CEN>(z[i > 0 ? ij - 1 : ij + m - 1], zc));
+        if (r) sx = acc_rn(sx, er, cen<CEN>(z[i < m - 1 ? ij + 1 : ij + 1 - m], zc));
+        if (d) sy = mul_rn(ed, cen<CEN>(z[j > 0 ? ij - m : ij + m * (n - 1)], zc));
+        if (u) sy = acc_rn(sy, eu, cen<CEN>(z[j < n - 1 ? ij + m : ij - m * (n - 1)], zc));
+        diag = diag_of(i, l, r, d, u, el, er, ed, eu);
+        return add_rn(mul_rn(xxsp, sx), mul_rn(yysp, sy));
+    }
+
+    /** The diagonal a_cc (mgs_mac.hh:93-97): the zero-pressure edge's ghost
+     * value -z doubles the right coefficient. */
+    __device__ __forceinline__ T diag_of(int i, bool l, bool r, bool d, bool u, T el, T er, T ed, T eu) const {
+        (void)r;
+        return mac_diag(mul_rn(-xxsp, add_rn(l ? el : T(0), px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0))))),
+                        yysp, add_rn(d ? ed : T(0), u ? eu : T(0)));
     }
 
     /** Row sum of the stencil: zero except at the zero-pressure edge, whose
@@ -86,13 +116,12 @@ struct MacOp {
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         const T zc = CEN ? zs[lz] : T(0);
         T sx = 0, sy = 0;
-        if (l) sx = el * (zs[lz - 1] - zc);
-        if (r) sx += er * (zs[lz + 1] - zc);
-        if (d) sy = ed * (zs[lz - ldz] - zc);
-        if (u) sy += eu * (zs[lz + ldz] - zc);
-        diag = mac_diag(-xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0))))),
-                        yysp, (d ? ed : T(0)) + (u ? eu : T(0)));
-        return xxsp * sx + yysp * sy;
+        if (l) sx = mul_rn(el, cen<CEN>(zs[lz - 1], zc));
+        if (r) sx = acc_rn(sx, er, cen<CEN>(zs[lz + 1], zc));
+        if (d) sy = mul_rn(ed, cen<CEN>(zs[lz - ldz], zc));
+        if (u) sy = acc_rn(sy, eu, cen<CEN>(zs[lz + ldz], zc));
+        diag = diag_of(i, l, r, d, u, el, er, ed, eu);
+        return add_rn(mul_rn(xxsp, sx), mul_rn(yysp, sy));
     }
 
     __device__ __forceinline__ void coef9(int i, int j, T a[9]) const {
@@ -100,8 +129,7 @@ struct MacOp {
         const T el = ex[j * (m + 1) + i], er = ex[j * (m + 1) + i + 1];
         const T ed = ey[j * m + i], eu = ey[(j + 1) * m + i];
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
-        diag = mac_diag(-xxsp * ((l ? el : T(0)) + (px ? er : (i < m - 1 ? er : (zpr ? 2 * er : T(0))))),
-                        yysp, (d ? ed : T(0)) + (u ? eu : T(0)));
+        diag = diag_of(i, l, r, d, u, el, er, ed, eu);
         a[0] = 0; a[1] = d ? yysp * ed : T(0); a[2] = 0;
         a[3] = l ? xxsp * el : T(0); a[4] = diag; a[5] = r ? xxsp * er : T(0);
         a[6] = 0; a[7] = u ? yysp * eu : T(0); a[8] = 0;
@@ -169,12 +197,15 @@ struct FemOp {
     __device__ __forceinline__ T offdiag_int(T cdl, T cdr, T cul, T cur, const T *zs, int lz, int ldz,
                                              T &diag) const {
         const T zc = CEN ? zs[lz] : T(0);
-        diag = fm * ((cul + cdl) + (cur + cdr));
+        diag = mul_rn(fm, add_rn(add_rn(cul, cdl), add_rn(cur, cdr)));
         const T *w = zs + lz;
-        return cul * ((w[-1] - zc) * hex + (w[ldz - 1] - zc) * fc + (w[ldz] - zc) * hey)
-             + cdl * ((w[-1] - zc) * hex + (w[-ldz - 1] - zc) * fc + (w[-ldz] - zc) * hey)
-             + cur * ((w[1] - zc) * hex + (w[ldz + 1] - zc) * fc + (w[ldz] - zc) * hey)
-             + cdr * ((w[1] - zc) * hex + (w[-ldz + 1] - zc) * fc + (w[-ldz] - zc) * hey);
+        // each cell's three neighbours: x-edge (hex), corner (fc), y-edge (hey)
+        auto cell = [&](T cv, int ox, int oy) {
+            const T s = add_rn(add_rn(mul_rn(cen<CEN>(w[ox], zc), hex), mul_rn(cen<CEN>(w[ox + oy], zc), fc)),
+                               mul_rn(cen<CEN>(w[oy], zc), hey));
+            return mul_rn(cv, s);
+        };
+        return add_rn(add_rn(add_rn(cell(cul, -1, ldz), cell(cdl, -1, -ldz)), cell(cur, 1, ldz)), cell(cdr, 1, -ldz));
     }
 
     /** offdiag_s at a node on an edge of the grid (the cells from c). */
@@ -187,16 +218,16 @@ struct FemOp {
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         T t = 0;
         if (d) {
-            if (l) t += a[0] * (zs[lz - ldz - 1] - zc);
-            t += a[1] * (zs[lz - ldz] - zc);
-            if (r) t += a[2] * (zs[lz - ldz + 1] - zc);
+            if (l) t = acc_rn(t, a[0], cen<CEN>(zs[lz - ldz - 1], zc));
+            t = acc_rn(t, a[1], cen<CEN>(zs[lz - ldz], zc));
+            if (r) t = acc_rn(t, a[2], cen<CEN>(zs[lz - ldz + 1], zc));
         }
-        if (l) t += a[3] * (zs[lz - 1] - zc);
-        if (r) t += a[5] * (zs[lz + 1] - zc);
+        if (l) t = acc_rn(t, a[3], cen<CEN>(zs[lz - 1], zc));
+        if (r) t = acc_rn(t, a[5], cen<CEN>(zs[lz + 1], zc));
         if (u) {
-            if (l) t += a[6] * (zs[lz + ldz - 1] - zc);
-            t += a[7] * (zs[lz + ldz] - zc);
-            if (r) t += a[8] * (zs[lz + ldz + 1] - zc);
+            if (l) t = acc_rn(t, a[6], cen<CEN>(zs[lz + ldz - 1], zc));
+            t = acc_rn(t, a[7], cen<CEN>(zs[lz + ldz], zc));
+            if (r) t = acc_rn(t, a[8], cen<CEN>(zs[lz + ldz + 1], zc));
         }
         return t;
     }
@@ -204,17 +235,10 @@ struct FemOp {
     template <bool CEN = false>
     __device__ __forceinline__ T offdiag(int i, int j, const T *z, T &diag, T zc = T(0)) const {
         const int ij = i + m * j;
+        // (zc is the iterate at (i,j) in the centred form: z[ij] itself)
+        if (i > 0 && i < m - 1 && j > 0 && j < n - 1)
+            return offdiag_int<CEN>(c[ij], c[ij + 1], c[ij + m], c[ij + m + 1], z, ij, m, diag);
         if (!CEN) zc = T(0);
-        if (i > 0 && i < m - 1 && j > 0 && j < n - 1) {
-            const T cdl = c[ij], cdr = c[ij + 1], cul = c[ij + m], cur = c[ij + m + 1];
-            diag = fm * ((cul + cdl) + (cur + cdr));
-            if (zpr && i == m - 1) return 0;
-            const T *w = z + ij;
-            return cul * ((w[-1] - zc) * hex + (w[m - 1] - zc) * fc + (w[m] - zc) * hey)
-                 + cdl * ((w[-1] - zc) * hex + (w[-m - 1] - zc) * fc + (w[-m] - zc) * hey)
-                 + cur * ((w[1] - zc) * hex + (w[m + 1] - zc) * fc + (w[m] - zc) * hey)
-                 + cdr * ((w[1] - zc) * hex + (w[-m + 1] - zc) * fc + (w[-m] - zc) * hey);
-        }
         T a[9];
         coef9(i, j, a);
         diag = a[4];
@@ -223,16 +247,16 @@ struct FemOp {
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         T t = 0;
         if (d) {
-            if (l) t += a[0] * (z[ij + jd + il] - zc);
-            t += a[1] * (z[ij + jd] - zc);
-            if (r) t += a[2] * (z[ij + jd + ir] - zc);
+            if (l) t = acc_rn(t, a[0], cen<CEN>(z[ij + jd + il], zc));
+            t = acc_rn(t, a[1], cen<CEN>(z[ij + jd], zc));
+            if (r) t = acc_rn(t, a[2], cen<CEN>(z[ij + jd + ir], zc));
         }
-        if (l) t += a[3] * (z[ij + il] - zc);
-        if (r) t += a[5] * (z[ij + ir] - zc);
+        if (l) t = acc_rn(t, a[3], cen<CEN>(z[ij + il], zc));
+        if (r) t = acc_rn(t, a[5], cen<CEN>(z[ij + ir], zc));
         if (u) {
-            if (l) t += a[6] * (z[ij + ju + il] - zc);
-            t += a[7] * (z[ij + ju] - zc);
-            if (r) t += a[8] * (z[ij + ju + ir] - zc);
+            if (l) t = acc_rn(t, a[6], cen<CEN>(z[ij + ju + il], zc));
+            t = acc_rn(t, a[7], cen<CEN>(z[ij + ju], zc));
+            if (r) t = acc_rn(t, a[8], cen<CEN>(z[ij + ju + ir], zc));
         }
         return t;
     }
@@ -269,23 +293,39 @@ struct GenOp {
     template <bool CEN = false>
     __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
         const int ij = i + m * j;
-        const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         const T zc = CEN ? zs[lz] : T(0);
         diag = st[4 * N + ij];
+        return gen_sum<CEN>(px || i > 0, px || i < m - 1, py || j > 0, py || j < n - 1, st + ij, N, zs + lz, 1, ldz,
+                            zc, diag);
+    }
+
+    /** The off-diagonal sum over the entries c[k*ldc] (k = 0..8, in the
+     * order dl,dc,dr,cl,cr,ul,uc,ur) of a point whose iterate is w[0],
+     * neighbours at w[+-dx], w[+-dy]; diag holds entry 4 on entry and, with
+     * CEN, the row sum minus the off-diagonal entries on return. Shared by
+     * every nine-point smoother so that all of them round alike. */
+    template <bool CEN, class C>
+    static __device__ __forceinline__ T gen_sum(bool l, bool r, bool d, bool u, const C *c, long ldc, const T *w,
+                                                int dx, int dy, T zc, T &diag) {
         T t = 0, a = 0;
+        auto term = [&](int k, int off) {
+            const T ck = c[k * ldc];
+            t = acc_rn(t, ck, cen<CEN>(w[off], zc));
+            if constexpr (CEN) a = add_rn(a, ck);
+        };
         if (d) {
-            if (l) { t += st[ij] * (zs[lz - ldz - 1] - zc); a += st[ij]; }
-            t += st[N + ij] * (zs[lz - ldz] - zc); a += st[N + ij];
-            if (r) { t += st[2 * N + ij] * (zs[lz - ldz + 1] - zc); a += st[2 * N + ij]; }
+            if (l) term(0, -dy - dx);
+            term(1, -dy);
+            if (r) term(2, -dy + dx);
         }
-        if (l) { t += st[3 * N + ij] * (zs[lz - 1] - zc); a += st[3 * N + ij]; }
-        if (r) { t += st[5 * N + ij] * (zs[lz + 1] - zc); a += st[5 * N + ij]; }
+        if (l) term(3, -dx);
+        if (r) term(5, dx);
         if (u) {
-            if (l) { t += st[6 * N + ij] * (zs[lz + ldz - 1] - zc); a += st[6 * N + ij]; }
-            t += st[7 * N + ij] * (zs[lz + ldz] - zc); a += st[7 * N + ij];
-            if (r) { t += st[8 * N + ij] * (zs[lz + ldz + 1] - zc); a += st[8 * N + ij]; }
+            if (l) term(6, dy - dx);
+            term(7, dy);
+            if (r) term(8, dy + dx);
         }
-        if (CEN) diag -= a;
+        if constexpr (CEN) diag = sub_rn(diag, a);
         return t;
     }
 
@@ -298,19 +338,24 @@ struct GenOp {
         if (!CEN) zc = T(0);
         diag = st[4 * N + ij];
         T t = 0, a = 0;
+        auto term = [&](int k, long off) {
+            const T ck = st[k * N + ij];
+            t = acc_rn(t, ck, cen<CEN>(z[ij + off], zc));
+            if constexpr (CEN) a = add_rn(a, ck);
+        };
         if (d) {
-            if (l) { t += st[ij] * (z[ij + jd + il] - zc); a += st[ij]; }
-            t += st[N + ij] * (z[ij + jd] - zc); a += st[N + ij];
-            if (r) { t += st[2 * N + ij] * (z[ij + jd + ir] - zc); a += st[2 * N + ij]; }
+            if (l) term(0, jd + il);
+            term(1, jd);
+            if (r) term(2, jd + ir);
         }
-        if (l) { t += st[3 * N + ij] * (z[ij + il] - zc); a += st[3 * N + ij]; }
-        if (r) { t += st[5 * N + ij] * (z[ij + ir] - zc); a += st[5 * N + ij]; }
+        if (l) term(3, il);
+        if (r) term(5, ir);
         if (u) {
-            if (l) { t += st[6 * N + ij] * (z[ij + ju + il] - zc); a += st[6 * N + ij]; }
-            t += st[7 * N + ij] * (z[ij + ju] - zc); a += st[7 * N + ij];
-            if (r) { t += st[8 * N + ij] * (z[ij + ju + ir] - zc); a += st[8 * N + ij]; }
+            if (l) term(6, ju + il);
+            term(7, ju);
+            if (r) term(8, ju + ir);
         }
-        if (CEN) diag -= a;
+        if constexpr (CEN) diag = sub_rn(diag, a);
         return t;
     }
 
@@ -321,16 +366,26 @@ struct GenOp {
 /** A Gauss-Seidel update of unknown (i,j) with the iterate in global memory:
  * (b - offdiag)/diag in double precision, exactly the reference's
  * inv_cc; in single precision the centred form zc + (b - A z)/diag. */
+/** The new value of a Gauss-Seidel update from the off-diagonal sum and the
+ * diagonal: (b - off)/diag in double; zc + (b - off - rs zc)/diag in the
+ * centred single-precision form (rs: the row sum). */
+__device__ __forceinline__ double gs_value(double b, double off, double diag, double, double) {
+    return sub_rn(b, off) / diag;
+}
+__device__ __forceinline__ float gs_value(float b, float off, float diag, float zc, float rs) {
+    return add_rn(zc, sub_rn(sub_rn(b, off), mul_rn(rs, zc)) / diag);
+}
+
 template <class Op, class T>
 __device__ __forceinline__ T gs_update(const Op &op, int i, int j, const T *z, T b) {
     T diag;
     if constexpr (sizeof(T) == 8) {
         const T off = op.offdiag(i, j, z, diag);
-        return (b - off) / diag;
+        return gs_value(b, off, diag, T(0), T(0));
     } else {
         const T zc = z[i + static_cast<long>(op.m) * j];
         const T off = op.template offdiag<true>(i, j, z, diag, zc);
-        return zc + (b - off - op.rowsum(i, j) * zc) / diag;
+        return gs_value(b, off, diag, zc, op.rowsum(i, j));
     }
 }
 
@@ -340,11 +395,11 @@ __device__ __forceinline__ T gs_update_s(const Op &op, int i, int j, const T *zs
     T diag;
     if constexpr (sizeof(T) == 8) {
         const T off = op.offdiag_s(i, j, zs, lz, ldz, diag);
-        return (b - off) / diag;
+        return gs_value(b, off, diag, T(0), T(0));
     } else {
         const T zc = zs[lz];
         const T off = op.template offdiag_s<true>(i, j, zs, lz, ldz, diag);
-        return zc + (b - off - op.rowsum(i, j) * zc) / diag;
+        return gs_value(b, off, diag, zc, op.rowsum(i, j));
     }
 }
 
@@ -356,10 +411,10 @@ __device__ __forceinline__ T residual_at(const Op &op, int i, int j, const T *z,
     const T zc = z[i + static_cast<long>(op.m) * j];
     if constexpr (sizeof(T) == 8) {
         const T off = op.offdiag(i, j, z, diag);
-        return b - off - diag * zc;
+        return sub_rn(sub_rn(b, off), mul_rn(diag, zc));
     } else {
         const T off = op.template offdiag<true>(i, j, z, diag, zc);
-        return b - off - op.rowsum(i, j) * zc;
+        return sub_rn(sub_rn(b, off), mul_rn(op.rowsum(i, j), zc));
     }
 }
 

@@ -1,6 +1,5 @@
 """The tile-fused smoothers (two Gauss-Seidel sweeps per launch in
-shared-memory tiles, with the inputs staged in shared memory or read through
-the caches) against one launch per colour (incrmt_mg_set_tiles modes 1, 2, 0):
+shared-memory tiles) against one launch per colour (incrmt_mg_set_tiles):
 identical iterates, bit for bit, after three FP64 V-cycles and after a whole
 mixed-precision solve, on grids of several launch waves (where blocks that
 start late would see their neighbours' finished tiles if the sweeps worked
@@ -22,8 +21,8 @@ CASES = [
     (0, 768, 512, False, True, True, True),
     (1, 768, 512, False, True, True, True),
     (0, 512, 384, True, True, False, False),
-    # large enough for the staged fine-level kernels (64 x 32 tiles, two
-    # blocks per SM) with periodic seams and the zero-pressure column
+    # large enough for the 64 x 32 tiles of the fine levels (at least two
+    # blocks per SM), with periodic seams and the zero-pressure column
     (0, 1024, 1024, False, True, True, True),
     (1, 1024, 1024, False, True, True, True),
     (0, 1024, 768, True, True, False, False),
@@ -47,7 +46,7 @@ def test_tiles_identical_to_colour_launches(gpu, sys_, m, n, xp, yp, zpr, solve)
     dev = torch.device("cuda")
     bd = torch.tensor(b, device=dev)
     out = {}
-    for tiles in (1, 2, 0):
+    for tiles in (True, False):
         s.set_tiles(tiles)
         s.set_density(rho)
         z = torch.tensor(z0, device=dev)
@@ -61,8 +60,7 @@ def test_tiles_identical_to_colour_launches(gpu, sys_, m, n, xp, yp, zpr, solve)
             vc = s.solve_device(bd.data_ptr(), zm.data_ptr(), precision=capi.PREC_MIXED).vcycles
         torch.cuda.synchronize()
         out[tiles] = (z.cpu().numpy(), zm.cpu().numpy(), vc)
-    for mode in (2, 0):
-        assert np.array_equal(out[1][0], out[mode][0]), mode
-        assert out[1][2] == out[mode][2], mode
-        assert np.array_equal(out[1][1], out[mode][1]), mode
+    assert np.array_equal(out[True][0], out[False][0])
+    assert out[True][2] == out[False][2]
+    assert np.array_equal(out[True][1], out[False][1])
     s.close()

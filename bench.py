@@ -427,7 +427,7 @@ LEARNED_SIM_STEPS = 2000   # Adam steps per network
 LEARNED_SIM_BASE = 32      # channels at the finest level of the U-Net
 
 
-def train_learned_sim(workload, rank, dev):
+def train_learned_sim(workload, rank, dev, guess=0):
     """The learned warm start of the MAC and FEM projections, trained with
     this library's own U-Net kernels on samples the method generates: a
     training run of the workload (another seed; for the flag a perturbed
@@ -436,6 +436,7 @@ def train_learned_sim(workload, rank, dev):
     from incrmt_b200 import capi, learned
     t0 = time.perf_counter()
     sim = make_sim(workload, rank, capi.PREC_FP64, training=True)
+    sim.set_guess(guess)  # the corrections the networks learn are to this warm start
     dt = frame_dt(sim.dt_reg, frame_interval(workload))
     sim.step(dt, 10)
     data = learned.capture(sim, LEARNED_SIM_FACTOR, LEARNED_SIM_SAMPLES, dt, dev)
@@ -511,7 +512,7 @@ def projection_roofline(sim, workload, prec, vc_mac, vc_fem, phases):
                           "mixed: w=4 plus 68/60 B per unknown of FP64 outer residual and update"}
 
 
-def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist, clocks=None, extras=True,
+def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist, clocks=None, extras=True, guess=0,
             e2e_steps=0, learned_rule=0):
     """One run of a simulation workload: warm-up, K timed steps (CUDA events
     on the simulation stream, max over ranks), end snapshot, then (extras)
@@ -522,6 +523,7 @@ def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist
     from incrmt_b200 import capi
     sim = make_sim(workload, rank, prec)
     sim.set_coarse_refresh(coarse_refresh)
+    sim.set_guess(guess)
     dt = frame_dt(sim.dt_reg, frame_interval(workload))
     if nets is not None:
         for sys, net in nets.items():
@@ -609,17 +611,24 @@ def compare_workload(workload, args, ws, rank, dev, dist, clocks=None, extras=Tr
     prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
     nets, info = (None, None)
     if args.guess == "learned":
-        nets, info = train_learned_sim(workload, rank, dev)
+        nets, info = train_learned_sim(workload, rank, dev, args.extrapolate)
     a = sim_run(workload, rank, dev, prec, nets, args.steps, args.warmup, args.coarse_refresh, dist, clocks=clocks,
-                extras=extras, e2e_steps=args.steps if e2e else 0, learned_rule=args.learned_rule)
+                extras=extras, guess=args.extrapolate, e2e_steps=args.steps if e2e else 0,
+                learned_rule=args.learned_rule)
     plain = None
-    if nets is not None or prec != capi.PREC_FP64:
+    if nets is not None or prec != capi.PREC_FP64 or args.extrapolate:
         plain = sim_run(workload, rank, dev, capi.PREC_FP64, None, args.steps, args.warmup, args.coarse_refresh,
                         dist, extras=extras)
         a["errors_vs_fp64"] = _snap_errors(a["snapshot"], plain["snapshot"])
     if nets is not None:
         for net in nets.values():
             net.close()
+        # the same configuration without the networks: what the learned
+        # correction adds or costs on top of the rest
+        b = sim_run(workload, rank, dev, prec, None, args.steps, args.warmup, args.coarse_refresh, dist,
+                    extras=False, guess=args.extrapolate)
+        a["without_learned"] = {"steps_per_s": ws * b["steps_per_s"],
+                                "vcycles_per_projection": {"mac": b["vc_mac"], "fem": b["vc_fem"]}}
     return a, plain, info
 
 
@@ -676,7 +685,9 @@ def run_ours_sim(args, ws, rank, local, dist):
         if plain is not None and "phases" in plain:
             roof["projection_plain_fp64"] = projection_roofline(None, args.workload, capi.PREC_FP64, plain["vc_mac"],
                                                                 plain["vc_fem"], plain["phases"])
-    guess = "learned warm start on the previous solution" if args.guess == "learned" else "previous solution"
+    start = "the extrapolation 2 z(n-1) - z(n-2) of the last two solutions" if args.extrapolate else \
+        "the previous solution"
+    guess = f"learned warm start on {start}" if args.guess == "learned" else start
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": a["ms"] / args.steps,
@@ -710,6 +721,8 @@ def run_ours_sim(args, ws, rank, local, dist):
     if info is not None:
         info.update(a.get("learned", {}))
         line["learned"] = info
+    if "without_learned" in a:
+        line["without_learned"] = a["without_learned"]
     if also:
         line["also"] = also
     print(json.dumps(line))
@@ -980,6 +993,9 @@ def main():
                     help="initial guess of each projection: the previous solution, or the learned warm start "
                          "trained first on a training run of the workload")
     ap.add_argument("--learned", action="store_true", help="same as --guess learned")
+    ap.add_argument("--extrapolate", type=int, default=1, choices=[0, 1],
+                    help="1: the projections start from 2 z(n-1) - z(n-2) (incrmt_sim_set_guess); the plain "
+                         "FP64 comparison run always starts from the previous solution")
     ap.add_argument("--coarse-refresh", type=int, default=1,
                     help="rebuild the projections' Galerkin coarse operators every K projections "
                          "(1: on every density change, as the reference)")

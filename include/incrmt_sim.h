@@ -240,6 +240,18 @@ int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err);
  * to whole-grid passes until the next rebuild. */
 int incrmt_sim_set_windows(incrmt_sim *h, int on);
 
+/** Warm start of the two projections' solves (no reference counterpart;
+ * default 0): 0 the previous step's solution, as the reference's
+ * fluid_2d::mac_projection and finite_element_projection solve from the
+ * pressure left in place (fluid_2d.cc:1175-1236, 1297-1328); 1 from the
+ * third solve on, the linear extrapolation 2 z(n-1) - z(n-2) of the last two
+ * solutions (one extra array per system). Every solve still stops at the same
+ * relative residual; the start only changes how many V-cycles that takes. A
+ * learned guess (incrmt_sim_set_learned) corrects whichever start this
+ * gives. Setting the mode, and incrmt_set_field, restart the history.
+ * INCRMT_ERR_BADARG for another mode. */
+int incrmt_sim_set_guess(incrmt_sim *h, int mode);
+
 /** How often the projections rebuild their Galerkin coarse operators: every
  * `every` projections (1: on every density change, as the reference's solver
  * setup does), sooner when a solve takes more than one V-cycle over the first

@@ -320,6 +320,7 @@ def _sim_sigs(L):
     L.incrmt_sim_set_windows.argtypes = [P, I]
     L.incrmt_set_solid_prd_bc.argtypes = [P, I]
     L.incrmt_sim_set_coarse_refresh.argtypes = [P, I]
+    L.incrmt_sim_set_guess.argtypes = [P, I]
     L.incrmt_set_object_tracers.argtypes = [P, dp, I, I]
     L.incrmt_l_comparison.argtypes = [P, P, dp]
     L.incrmt_sim_profile.argtypes = [P, dp]
@@ -571,6 +572,11 @@ class Simulation:
         """Rebuild the projections' Galerkin coarse operators every `every`
         projections (1 = every density change)."""
         check(lib().incrmt_sim_set_coarse_refresh(self._h, int(every)))
+
+    def set_guess(self, mode):
+        """Warm start of the projections (incrmt_sim_set_guess): 0 the
+        previous solution, 1 the extrapolation 2 z(n-1) - z(n-2)."""
+        check(lib().incrmt_sim_set_guess(self._h, int(mode)))
 
     def set_profiling(self, on=True, smoothers=False):
         """Phase timing (on) and per-launch timing of the projections'

@@ -918,7 +918,7 @@ __global__ void k_resnorm(Op op, const double *z, const double *b, int m, int n,
             const long q = i + static_cast<long>(m) * j;
             double diag;
             const double off = op.offdiag(i, j, z, diag);
-            const double r = sub_rn(sub_rn(b[q], off), mul_rn(diag, z[q]));
+            const double r = fma_rn(-diag, z[q], sub_rn(b[q], off));
             if (rf) rf[q] = static_cast<float>(r);
             acc += r * r;
         }
@@ -933,7 +933,7 @@ __global__ void k_apply(Op op, const double *z, double *out, int m, int n) {
     if (i >= m || j >= n) return;
     double diag;
     const double off = op.offdiag(i, j, z, diag);
-    out[i + m * j] = add_rn(off, mul_rn(diag, z[i + m * j]));
+    out[i + m * j] = fma_rn(diag, z[i + m * j], off);
 }
 
 __global__ void k_sumsq(const double *b, long N, double *partial) {

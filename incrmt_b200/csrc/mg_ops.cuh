@@ -25,22 +25,24 @@
 
 namespace incrmt {
 
-// Every product and sum of the stencil arithmetic is written with an explicit
-// rounding (no fused multiply-add): the compiler would otherwise contract
-// some of them into FMAs, and which ones can depend on the code around an
-// inlined expression, so that kernels computing the same update in the same
-// order could round it differently. With explicit operations the smoothers
-// (one launch per colour, tiled, staged) agree bit for bit, and the FP64
-// arithmetic is that of the oracle on the CPU, which fuses nothing.
+// Every product and sum of the stencil arithmetic is written as an explicit
+// operation (a fused multiply-add where a product is added, a rounded product
+// or sum otherwise): left to itself the compiler contracts some products and
+// sums into FMAs, and which ones can depend on the code around an inlined
+// expression, so that kernels computing the same update in the same order
+// could round it differently. With every rounding fixed in the source, the
+// smoothers (one launch per colour, tiled) agree bit for bit.
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
-/** t + a*b, the product rounded first. */
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+/** t + a*b, fused. */
 template <class T>
-__device__ __forceinline__ T acc_rn(T t, T a, T b) { return add_rn(t, mul_rn(a, b)); }
+__device__ __forceinline__ T acc_rn(T t, T a, T b) { return fma_rn(a, b, t); }
 /** z - zc in the centred form, z itself otherwise. */
 template <bool CEN, class T>
 __device__ __forceinline__ T cen(T z, T zc) {
@@ -75,13 +77,23 @@ struct MacOp {
         const T el = ex[j * (m + 1) + i], er = ex[j * (m + 1) + i + 1];
         const T ed = ey[j * m + i], eu = ey[(j + 1) * m + i];
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
-        T sx = 0, sy = 0;
-        if (l) sx = mul_rn(el, cen<CEN>(z[i > 0 ? ij - 1 : ij + m - 1], zc));
-        if (r) sx = acc_rn(sx, er, cen<CEN>(z[i < m - 1 ? ij + 1 : ij + 1 - m], zc));
-        if (d) sy = mul_rn(ed, cen<CEN>(z[j > 0 ? ij - m : ij + m * (n - 1)], zc));
-        if (u) sy = acc_rn(sy, eu, cen<CEN>(z[j < n - 1 ? ij + m : ij - m * (n - 1)], zc));
+        // neighbour indices wrap, so every load is in range (see GenOp::gen_sum)
+        const T zl = z[i > 0 ? ij - 1 : ij + m - 1], zr = z[i < m - 1 ? ij + 1 : ij + 1 - m];
+        const T zd = z[j > 0 ? ij - m : ij + m * (n - 1)], zu = z[j < n - 1 ? ij + m : ij - m * (n - 1)];
         diag = diag_of(i, l, r, d, u, el, er, ed, eu);
-        return add_rn(mul_rn(xxsp, sx), mul_rn(yysp, sy));
+        return mac_terms<CEN>(l, r, d, u, el, er, ed, eu, zl, zr, zd, zu, zc);
+    }
+
+    /** xxsp (el zl + er zr) + yysp (ed zd + eu zu), terms outside the grid
+     * skipped (centred: each z minus zc). */
+    template <bool CEN>
+    __device__ __forceinline__ T mac_terms(bool l, bool r, bool d, bool u, T el, T er, T ed, T eu, T zl, T zr, T zd,
+                                           T zu, T zc) const {
+        T sx = l ? mul_rn(el, cen<CEN>(zl, zc)) : T(0);
+        sx = r ? acc_rn(sx, er, cen<CEN>(zr, zc)) : sx;
+        T sy = d ? mul_rn(ed, cen<CEN>(zd, zc)) : T(0);
+        sy = u ? acc_rn(sy, eu, cen<CEN>(zu, zc)) : sy;
+        return fma_rn(xxsp, sx, mul_rn(yysp, sy));
     }
 
     /** The diagonal a_cc (mgs_mac.hh:93-97): the zero-pressure edge's ghost
@@ -115,13 +127,8 @@ struct MacOp {
                                            T &diag) const {
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         const T zc = CEN ? zs[lz] : T(0);
-        T sx = 0, sy = 0;
-        if (l) sx = mul_rn(el, cen<CEN>(zs[lz - 1], zc));
-        if (r) sx = acc_rn(sx, er, cen<CEN>(zs[lz + 1], zc));
-        if (d) sy = mul_rn(ed, cen<CEN>(zs[lz - ldz], zc));
-        if (u) sy = acc_rn(sy, eu, cen<CEN>(zs[lz + ldz], zc));
         diag = diag_of(i, l, r, d, u, el, er, ed, eu);
-        return add_rn(mul_rn(xxsp, sx), mul_rn(yysp, sy));
+        return mac_terms<CEN>(l, r, d, u, el, er, ed, eu, zs[lz - 1], zs[lz + 1], zs[lz - ldz], zs[lz + ldz], zc);
     }
 
     __device__ __forceinline__ void coef9(int i, int j, T a[9]) const {
@@ -200,12 +207,11 @@ struct FemOp {
         diag = mul_rn(fm, add_rn(add_rn(cul, cdl), add_rn(cur, cdr)));
         const T *w = zs + lz;
         // each cell's three neighbours: x-edge (hex), corner (fc), y-edge (hey)
-        auto cell = [&](T cv, int ox, int oy) {
-            const T s = add_rn(add_rn(mul_rn(cen<CEN>(w[ox], zc), hex), mul_rn(cen<CEN>(w[ox + oy], zc), fc)),
-                               mul_rn(cen<CEN>(w[oy], zc), hey));
-            return mul_rn(cv, s);
+        auto cell = [&](int ox, int oy) {
+            return fma_rn(cen<CEN>(w[oy], zc), hey,
+                          fma_rn(cen<CEN>(w[ox + oy], zc), fc, mul_rn(cen<CEN>(w[ox], zc), hex)));
         };
-        return add_rn(add_rn(add_rn(cell(cul, -1, ldz), cell(cdl, -1, -ldz)), cell(cur, 1, ldz)), cell(cdr, 1, -ldz));
+        return fma_rn(cdr, cell(1, -ldz), fma_rn(cur, cell(1, ldz), fma_rn(cdl, cell(-1, -ldz), mul_rn(cul, cell(-1, ldz)))));
     }
 
     /** offdiag_s at a node on an edge of the grid (the cells from c). */
@@ -307,24 +313,37 @@ struct GenOp {
     template <bool CEN, class C>
     static __device__ __forceinline__ T gen_sum(bool l, bool r, bool d, bool u, const C *c, long ldc, const T *w,
                                                 int dx, int dy, T zc, T &diag) {
+        // Every entry and neighbour is read unconditionally (the point's own
+        // entries, and neighbours inside the caller's array: a shared-memory
+        // tile with a halo, or a wrapped global index), so that all eighteen
+        // loads can be in flight at once; the terms outside the grid are then
+        // skipped by selection, which leaves the sum as the branches would.
+        const T k0 = c[0], k1 = c[ldc], k2 = c[2 * ldc], k3 = c[3 * ldc], k5 = c[5 * ldc], k6 = c[6 * ldc],
+                k7 = c[7 * ldc], k8 = c[8 * ldc];
+        const T z0 = w[-dy - dx], z1 = w[-dy], z2 = w[-dy + dx], z3 = w[-dx], z5 = w[dx], z6 = w[dy - dx],
+                z7 = w[dy], z8 = w[dy + dx];
+        return gen_terms<CEN>(l, r, d, u, k0, k1, k2, k3, k5, k6, k7, k8, z0, z1, z2, z3, z5, z6, z7, z8, zc, diag);
+    }
+
+    /** The off-diagonal sum from the eight entries and neighbour values
+     * (order dl,dc,dr,cl,cr,ul,uc,ur), terms outside the grid skipped. */
+    template <bool CEN>
+    static __device__ __forceinline__ T gen_terms(bool l, bool r, bool d, bool u, T k0, T k1, T k2, T k3, T k5, T k6,
+                                                  T k7, T k8, T z0, T z1, T z2, T z3, T z5, T z6, T z7, T z8, T zc,
+                                                  T &diag) {
         T t = 0, a = 0;
-        auto term = [&](int k, int off) {
-            const T ck = c[k * ldc];
-            t = acc_rn(t, ck, cen<CEN>(w[off], zc));
-            if constexpr (CEN) a = add_rn(a, ck);
+        auto term = [&](bool on, T ck, T zk) {
+            t = on ? acc_rn(t, ck, cen<CEN>(zk, zc)) : t;
+            if constexpr (CEN) a = on ? add_rn(a, ck) : a;
         };
-        if (d) {
-            if (l) term(0, -dy - dx);
-            term(1, -dy);
-            if (r) term(2, -dy + dx);
-        }
-        if (l) term(3, -dx);
-        if (r) term(5, dx);
-        if (u) {
-            if (l) term(6, dy - dx);
-            term(7, dy);
-            if (r) term(8, dy + dx);
-        }
+        term(d && l, k0, z0);
+        term(d, k1, z1);
+        term(d && r, k2, z2);
+        term(l, k3, z3);
+        term(r, k5, z5);
+        term(u && l, k6, z6);
+        term(u, k7, z7);
+        term(u && r, k8, z8);
         if constexpr (CEN) diag = sub_rn(diag, a);
         return t;
     }
@@ -337,26 +356,10 @@ struct GenOp {
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         if (!CEN) zc = T(0);
         diag = st[4 * N + ij];
-        T t = 0, a = 0;
-        auto term = [&](int k, long off) {
-            const T ck = st[k * N + ij];
-            t = acc_rn(t, ck, cen<CEN>(z[ij + off], zc));
-            if constexpr (CEN) a = add_rn(a, ck);
-        };
-        if (d) {
-            if (l) term(0, jd + il);
-            term(1, jd);
-            if (r) term(2, jd + ir);
-        }
-        if (l) term(3, il);
-        if (r) term(5, ir);
-        if (u) {
-            if (l) term(6, ju + il);
-            term(7, ju);
-            if (r) term(8, ju + ir);
-        }
-        if constexpr (CEN) diag = sub_rn(diag, a);
-        return t;
+        const T *c = st + ij;
+        const T *w = z + ij;
+        return gen_terms<CEN>(l, r, d, u, c[0], c[N], c[2 * N], c[3 * N], c[5 * N], c[6 * N], c[7 * N], c[8 * N],
+                              w[jd + il], w[jd], w[jd + ir], w[il], w[ir], w[ju + il], w[ju], w[ju + ir], zc, diag);
     }
 
     /** Row sum, stored in entry 4 of the single-precision stencils. */
@@ -373,7 +376,7 @@ __device__ __forceinline__ double gs_value(double b, double off, double diag, do
     return sub_rn(b, off) / diag;
 }
 __device__ __forceinline__ float gs_value(float b, float off, float diag, float zc, float rs) {
-    return add_rn(zc, sub_rn(sub_rn(b, off), mul_rn(rs, zc)) / diag);
+    return add_rn(zc, fma_rn(-rs, zc, sub_rn(b, off)) / diag);
 }
 
 template <class Op, class T>
@@ -411,10 +414,10 @@ __device__ __forceinline__ T residual_at(const Op &op, int i, int j, const T *z,
     const T zc = z[i + static_cast<long>(op.m) * j];
     if constexpr (sizeof(T) == 8) {
         const T off = op.offdiag(i, j, z, diag);
-        return sub_rn(sub_rn(b, off), mul_rn(diag, zc));
+        return fma_rn(-diag, zc, sub_rn(b, off));
     } else {
         const T off = op.template offdiag<true>(i, j, z, diag, zc);
-        return sub_rn(sub_rn(b, off), mul_rn(op.rowsum(i, j), zc));
+        return fma_rn(-op.rowsum(i, j), zc, sub_rn(b, off));
     }
 }
 

@@ -55,7 +55,7 @@ __global__ void k_na_apply(Op op, const double *z, double *out, int m, int n) {
     if (i >= m || j >= n) return;
     double diag;
     const double off = op.offdiag(i, j, z, diag);
-    out[i + m * j] = add_rn(off, mul_rn(diag, z[i + m * j]));
+    out[i + m * j] = fma_rn(diag, z[i + m * j], off);
 }
 
 /** Device address of the scratch on the current device; the first call on a

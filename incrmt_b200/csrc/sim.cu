@@ -66,6 +66,14 @@ struct Sim {
         long z0_n = 0;
     } learn[2];
     unsigned long long *d_lcnt = nullptr;  // [sys][applied, fallback]
+    // Warm start of the projections: 0 the previous solution (the
+    // reference's), 1 its linear extrapolation 2 z(n-1) - z(n-2) once two
+    // solutions exist; zold[sys] holds z(n-2), nsol[sys] the solves since the
+    // history was last reset.
+    int guess = 0;
+    double *zold[2] = {nullptr, nullptr};
+    long long nsol[2] = {0, 0};
+    int extrapolate_guess(int sys, double *z);
     incrmt_mg_opts mgo{1e-9, 200, INCRMT_PREC_FP64};
     double dt_reg = 0, time = 0;
     double w_scale = 3, w_force = 20, tw = 2.5, pinw = 2.5;
@@ -723,6 +731,36 @@ int Sim::update_reference_map(double dt) {
     return INCRMT_OK;
 }
 
+/** z = 2 z - zo and zo = the old z (extrap), or zo = z alone. */
+__global__ void k_extrapolate_guess(double *z, double *zo, long N, int extrap) {
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x) {
+        const double v = z[q];
+        if (extrap) z[q] = __dsub_rn(2.0 * v, zo[q]);
+        zo[q] = v;
+    }
+}
+
+/** The extrapolated warm start of a projection (guess 1): from the third
+ * solve on, z(n-1) becomes 2 z(n-1) - z(n-2), a second-order prediction of
+ * a pressure that varies smoothly in time; the solve then reaches the same
+ * relative residual from a closer start. The first two solves keep the
+ * previous solution, as the reference does always (fluid_2d.cc:1175-1236,
+ * 1297-1328 solve from the pressure left in place). */
+int Sim::extrapolate_guess(int sys, double *z) {
+    if (!guess) return INCRMT_OK;
+    const long N = sys == INCRMT_SYS_MAC ? static_cast<long>(g.m) * g.n : static_cast<long>(g.mf) * g.nf;
+    if (!zold[sys]) {
+        int r = alloc(&zold[sys], static_cast<size_t>(N));
+        if (r) return r;
+    }
+    const int nb = cdiv(N, 256) < 4 * kB200SMs ? cdiv(N, 256) : 4 * kB200SMs;
+    k_extrapolate_guess<<<nb, 256, 0, stream>>>(z, zold[sys], N, nsol[sys] >= 2 ? 1 : 0);
+    launches++;
+    INCRMT_CKL("k_extrapolate_guess");
+    return INCRMT_OK;
+}
+
 /** fluid_2d::mac_projection (fluid_2d.cc:1175-1236). */
 int Sim::mac_projection() {
     k_mac_source<<<g2(g.m, g.n), kB2, 0, stream>>>(g, f, src_mac);
@@ -737,9 +775,11 @@ int Sim::mac_projection() {
     if ((r = phase_begin(outer))) return r;
     incrmt_mg_stats st{};
     long long l0 = mac.launches;
+    if ((r = extrapolate_guess(INCRMT_SYS_MAC, z_mac))) return r;
     if ((r = learned_pre(INCRMT_SYS_MAC, src_mac, z_mac))) return r;
     r = const_rho ? mac.solve_device(src_mac, z_mac, &mgo, &st, false) : mac.solve_lagged(src_mac, z_mac, &mgo, &st, false);
     if (!r) r = learned_post(INCRMT_SYS_MAC, z_mac);
+    if (!r) nsol[INCRMT_SYS_MAC]++;
     launches += mac.launches - l0;
     vc_mac += st.vcycles;
     solves_mac++;
@@ -808,9 +848,11 @@ int Sim::fem_projection(double dt) {
     if ((r = phase_begin(outer))) return r;
     incrmt_mg_stats st{};
     long long l0 = fem.launches;
+    if ((r = extrapolate_guess(INCRMT_SYS_FEM, z_fem))) return r;
     if ((r = learned_pre(INCRMT_SYS_FEM, src_fem, z_fem))) return r;
     r = const_rho ? fem.solve_device(src_fem, z_fem, &mgo, &st, false) : fem.solve_lagged(src_fem, z_fem, &mgo, &st, false);
     if (!r) r = learned_post(INCRMT_SYS_FEM, z_fem);
+    if (!r) nsol[INCRMT_SYS_FEM]++;
     launches += fem.launches - l0;
     vc_fem += st.vcycles;
     solves_fem++;
@@ -1284,6 +1326,7 @@ int incrmt_set_field(incrmt_sim *h, int id, int k, const double *host) {
     if (int r = S.win_reset()) return r;
     S.mac.coarse_stale = true;
     S.fem.coarse_stale = true;
+    S.nsol[0] = S.nsol[1] = 0;  // the warm start's history no longer applies
     if (id == INCRMT_FIELD_STATUS) {
         if (k < 0 || k >= static_cast<int>(S.sol.size())) { set_error("bad object"); return INCRMT_ERR_BADARG; }
         std::vector<int> tmp(w * rows);
@@ -1505,6 +1548,13 @@ int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err) {
     INCRMT_CK(cudaMemcpyAsync(err, dev_err, sizeof(double) * 32, cudaMemcpyDeviceToHost, S.stream));
     INCRMT_CK(cudaFreeAsync(part, S.stream));
     INCRMT_CK(cudaStreamSynchronize(S.stream));
+    return INCRMT_OK;
+}
+
+int incrmt_sim_set_guess(incrmt_sim *h, int mode) {
+    if (!h || mode < 0 || mode > 1) { set_error("bad argument"); return INCRMT_ERR_BADARG; }
+    h->s.guess = mode;
+    h->s.nsol[0] = h->s.nsol[1] = 0;
     return INCRMT_OK;
 }
 

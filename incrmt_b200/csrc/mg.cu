@@ -197,8 +197,8 @@ __global__ void k_galerkin(Op op, int fm, int fn, int px, int py, bool kx, bool 
                     }
                 }
         }
-    const long N = static_cast<long>(cm) * cn, ij = I + static_cast<long>(cm) * J;
-    for (int e = 0; e < 9; e++) st[e * N + ij] = q[e];
+    const long N = static_cast<long>(cm) * cn;
+    for (int e = 0; e < 9; e++) st[e * N + colour_index(cm, cn, I, J)] = q[e];
 }
 
 /** k_galerkin for a 32 x 8 tile of coarse unknowns per 256-thread block,
@@ -283,9 +283,10 @@ __global__ void __launch_bounds__(256) k_galerkin_tile(Op op, int fm, int fn, in
                     }
                 }
         }
-    const long N = static_cast<long>(cm) * cn, ij = I + static_cast<long>(cm) * J;
+    const long N = static_cast<long>(cm) * cn;
+    const long qi = colour_index(cm, cn, I, J);
 #pragma unroll
-    for (int e = 0; e < 9; e++) st[e * N + ij] = q[e];
+    for (int e = 0; e < 9; e++) st[e * N + qi] = q[e];
 }
 
 /** The shared-memory limit of every k_galerkin_tile instance of Op. */
@@ -425,8 +426,9 @@ __global__ void __launch_bounds__(256) k_smooth_tile_gen(GenOp<T> op, const T *z
             const long ij = i + static_cast<long>(m) * j;
             zs[t] = zin[ij];
             bs[t] = b[ij];
+            const long q = op.at(i, j);
 #pragma unroll
-            for (int k = 0; k < 9; k++) cs[k * LA + t] = op.st[k * N + ij];
+            for (int k = 0; k < 9; k++) cs[k * LA + t] = op.st[k * N + q];
         }
     }
     __syncthreads();
@@ -677,13 +679,13 @@ __global__ void k_coarse_inverse(const double *st, int m, int n, int px, int py,
                 bool okx = true;
                 const int ii = wrap_idx(i + di, m, px, okx);
                 if (!okx) continue;
-                const double v = st[(3 * (dj + 1) + di + 1) * static_cast<long>(N) + r];
+                const double v = st[(3 * (dj + 1) + di + 1) * static_cast<long>(N) + colour_index(m, n, i, j)];
                 a[static_cast<long>(r) * W + ii + m * jj] += v;
                 rs += v;
             }
         }
         rsmax = fmax(rsmax, fabs(rs));
-        dsum += fabs(st[4 * static_cast<long>(N) + r]);
+        dsum += fabs(st[4 * static_cast<long>(N) + colour_index(m, n, i, j)]);
         a[static_cast<long>(r) * W + N + r] = 1;
     }
     // block max / sum (1024 threads = 32 warps)

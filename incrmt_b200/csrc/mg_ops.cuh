@@ -278,8 +278,22 @@ struct FemOp {
     }
 };
 
+/** Position of unknown (i,j) of an m x n level in the colour-split layout
+ * of the Galerkin stencils: the four Gauss-Seidel colours (i mod 2, j mod 2)
+ * each hold a contiguous row-major block, in the order (0,0), (1,0), (0,1),
+ * (1,1). A colour phase of the smoothers then reads its points' entries
+ * contiguously (every byte of each 32-byte sector, once per sweep) instead
+ * of every second entry of a row in each of the two phases that share the
+ * row's sectors. */
+__host__ __device__ __forceinline__ long colour_index(int m, int n, int i, int j) {
+    const int pi = i & 1, pj = j & 1;
+    const long m0 = (m + 1) >> 1, m1 = m >> 1, n0 = (n + 1) >> 1;
+    const long base = (pj ? static_cast<long>(m) * n0 : 0) + (pi ? (pj ? m0 * (n >> 1) : m0 * n0) : 0);
+    return base + static_cast<long>(j >> 1) * (pi ? m1 : m0) + (i >> 1);
+}
+
 /** A Galerkin coarse level: explicit 9-point stencil stored structure-of-
- * arrays, entry k of unknown ij at st[k*N+ij]. */
+ * arrays, entry k of unknown (i,j) at st[k*N + colour_index(m, n, i, j)]. */
 template <class T>
 struct GenOp {
     static constexpr bool kFivePoint = false;
@@ -287,10 +301,12 @@ struct GenOp {
     long N;
     const T *st;
 
+    __device__ __forceinline__ long at(int i, int j) const { return colour_index(m, n, i, j); }
+
     __device__ __forceinline__ void coef9(int i, int j, T a[9]) const {
-        const int ij = i + m * j;
+        const long q = at(i, j);
 #pragma unroll
-        for (int k = 0; k < 9; k++) a[k] = st[k * N + ij];
+        for (int k = 0; k < 9; k++) a[k] = st[k * N + q];
     }
 
     /** With CEN (the single-precision stencils, whose entry 4 holds the row
@@ -298,10 +314,10 @@ struct GenOp {
      * row sum minus the off-diagonal entries. */
     template <bool CEN = false>
     __device__ __forceinline__ T offdiag_s(int i, int j, const T *zs, int lz, int ldz, T &diag) const {
-        const int ij = i + m * j;
+        const long q = at(i, j);
         const T zc = CEN ? zs[lz] : T(0);
-        diag = st[4 * N + ij];
-        return gen_sum<CEN>(px || i > 0, px || i < m - 1, py || j > 0, py || j < n - 1, st + ij, N, zs + lz, 1, ldz,
+        diag = st[4 * N + q];
+        return gen_sum<CEN>(px || i > 0, px || i < m - 1, py || j > 0, py || j < n - 1, st + q, N, zs + lz, 1, ldz,
                             zc, diag);
     }
 
@@ -355,15 +371,15 @@ struct GenOp {
         const int jd = j > 0 ? -m : m * (n - 1), ju = j < n - 1 ? m : -m * (n - 1);
         const bool l = px || i > 0, r = px || i < m - 1, d = py || j > 0, u = py || j < n - 1;
         if (!CEN) zc = T(0);
-        diag = st[4 * N + ij];
-        const T *c = st + ij;
+        const T *c = st + at(i, j);
+        diag = c[4 * N];
         const T *w = z + ij;
         return gen_terms<CEN>(l, r, d, u, c[0], c[N], c[2 * N], c[3 * N], c[5 * N], c[6 * N], c[7 * N], c[8 * N],
                               w[jd + il], w[jd], w[jd + ir], w[il], w[ir], w[ju + il], w[ju], w[ju + ir], zc, diag);
     }
 
     /** Row sum, stored in entry 4 of the single-precision stencils. */
-    __device__ __forceinline__ T rowsum(int i, int j) const { return st[4 * N + i + static_cast<long>(m) * j]; }
+    __device__ __forceinline__ T rowsum(int i, int j) const { return st[4 * N + at(i, j)]; }
 };
 
 /** A Gauss-Seidel update of unknown (i,j) with the iterate in global memory:

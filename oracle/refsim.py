@@ -41,8 +41,12 @@ def available():
     return os.path.exists(LIB)
 
 
-def build(ref_root="/root/reference"):
-    """Builds oracle/_ref from the reference sources (needs the reference tree)."""
+def build(ref_root=None):
+    """Builds oracle/_ref from the reference sources (needs the reference
+    tree: ref_root, else $INCRMT_REFERENCE, else the build container's
+    checkout)."""
+    if ref_root is None:
+        ref_root = os.environ.get("INCRMT_REFERENCE", "/root/reference")
     subprocess.run(["make", "-C", HERE, f"REF={ref_root}", "-j8"], check=True,
                    stdout=subprocess.DEVNULL)
 

@@ -121,7 +121,9 @@ int incrmt_mg_set_coarse_refresh(incrmt_mg *h, int every);
 /** Mixed-precision solves (INCRMT_PREC_MIXED) since creation that finished
  * with FP64 V-cycles: a solve switches once an FP32 defect-correction step
  * fails to halve the FP64 residual norm, so it converges as the FP64 solve
- * would. */
+ * would. After three such solves in a row the handle runs the next 50
+ * mixed-precision requests as FP64 solves (not counted here), then tries
+ * FP32 cycles again. */
 long long incrmt_mg_mixed_fallbacks(const incrmt_mg *h);
 
 /** Galerkin hierarchy rebuilds since creation; *retries (if not null)

@@ -563,16 +563,18 @@ __global__ void k_restrict(Op op, const T *z, const T *b, int fm, int fn, int px
  * 2X0-1 .. 2(X0+31)+1 in a coarsened direction, X0 .. X0+31 otherwise) into
  * shared memory, then every coarse point sums its support's residuals with
  * the weights and in the order of k_restrict: the same values. */
-template <class Op, class T>
+template <class Op, class T, bool KX, bool KY>
 __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const T *b, int fm, int fn, int px, int py,
-                                                       bool kx, bool ky, int cm, int cn, T *bc, T *zc,
-                                                       const double *P) {
+                                                       int cm, int cn, T *bc, T *zc, const double *P) {
+    // The coarsening flags are template parameters, so the region's width
+    // (the divisor of the staging loop's index) is a constant.
+    constexpr bool kx = KX, ky = KY;
     constexpr int CTW = 32, CTH = 8, RW = 2 * CTW + 1, RH = 2 * CTH + 1;
     __shared__ T rs[RW * RH];
     __shared__ double ps[4 * RW * RH];  // the region's prolongation weights (zero outside the grid)
     const int X0 = blockIdx.x * CTW, Y0 = blockIdx.y * CTH;
     const int FX0 = kx ? 2 * X0 - 1 : X0, FY0 = ky ? 2 * Y0 - 1 : Y0;
-    const int FW = kx ? RW : CTW, FH = ky ? RH : CTH;
+    constexpr int FW = kx ? RW : CTW, FH = ky ? RH : CTH;
     // Only fine unknowns in the support of a coarse point I < cm, J < cn are
     // needed (and beyond them a periodic index could wrap past the grid).
     const int fxmax = kx ? 2 * cm - 1 : cm - 1, fymax = ky ? 2 * cn - 1 : cn - 1;
@@ -585,8 +587,10 @@ __global__ void __launch_bounds__(256) k_restrict_tile(Op op, const T *z, const 
         if (ok) {
             const int f = fx + fm * fy;
             r = residual_at(op, fx, fy, z, b[f]);
-            const double *q = P + 4 * static_cast<long>(f);
-            w0 = q[0]; w1 = q[1]; w2 = q[2]; w3 = q[3];
+            // four weights per fine point: 32-byte aligned, two 16-byte loads
+            const double2 *q = reinterpret_cast<const double2 *>(P + 4 * static_cast<long>(f));
+            const double2 q01 = q[0], q23 = q[1];
+            w0 = q01.x; w1 = q01.y; w2 = q23.x; w3 = q23.y;
         }
         rs[t] = r;
         ps[4 * t] = w0; ps[4 * t + 1] = w1; ps[4 * t + 2] = w2; ps[4 * t + 3] = w3;
@@ -619,9 +623,12 @@ __global__ void k_prolong(T *zf, int fm, int fn, int px, int py, bool kx, bool k
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= fm || j >= fn) return;
     const long f = i + static_cast<long>(fm) * j;
-    const double *q = P + 4 * f;
+    const double2 *q2 = reinterpret_cast<const double2 *>(P + 4 * f);  // 32-byte aligned
+    const double2 q01 = q2[0], q23 = q2[1];
+    const double q[4] = {q01.x, q01.y, q23.x, q23.y};
     const int bx = base_of(i, kx), by = base_of(j, ky);
     T t = 0;
+#pragma unroll
     for (int r = 0; r < 4; r++) {
         const double w = q[r];
         if (w == 0) continue;
@@ -1055,11 +1062,17 @@ int smooth(Op op, T *z, T *zalt, const T *b, int m, int n, int sweeps, cudaStrea
 template <class Op, class T>
 void restrict_launch(bool tiles, Op op, cudaStream_t s, const T *z, const T *b, int fm, int fn, int px, int py,
                      bool kx, bool ky, int cm, int cn, T *bc, T *zc, const double *we) {
-    if (tiles)
-        k_restrict_tile<<<dim3(cdiv(cm, 32), cdiv(cn, 8)), 256, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc,
-                                                                         we);
-    else
+    if (!tiles) {
         k_restrict<<<grid2(cm, cn), kBlk2, 0, s>>>(op, z, b, fm, fn, px, py, kx, ky, cm, cn, bc, zc, we);
+        return;
+    }
+    const dim3 g(cdiv(cm, 32), cdiv(cn, 8));
+    if (kx && ky)
+        k_restrict_tile<Op, T, true, true><<<g, 256, 0, s>>>(op, z, b, fm, fn, px, py, cm, cn, bc, zc, we);
+    else if (kx)
+        k_restrict_tile<Op, T, true, false><<<g, 256, 0, s>>>(op, z, b, fm, fn, px, py, cm, cn, bc, zc, we);
+    else
+        k_restrict_tile<Op, T, false, true><<<g, 256, 0, s>>>(op, z, b, fm, fn, px, py, cm, cn, bc, zc, we);
 }
 
 }  // namespace
@@ -1634,8 +1647,16 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
     if (!ready) { set_error("density not set"); return INCRMT_ERR_BADARG; }
     const double rtol = (o && o->rel_tol > 0) ? o->rel_tol : 1e-9;
     const int maxc = (o && o->max_vcycles > 0) ? o->max_vcycles : 200;
-    const int prec = o ? o->precision : INCRMT_PREC_FP64;
+    int prec = o ? o->precision : INCRMT_PREC_FP64;
     if (prec != INCRMT_PREC_FP64 && prec != INCRMT_PREC_MIXED) { set_error("bad precision %d", prec); return INCRMT_ERR_BADARG; }
+    // After kMixedStrikes consecutive mixed solves that fell back to FP64,
+    // the next kMixedRest solves run FP64 from the start (the FP32 cycle
+    // only cost time on this system), then mixed precision is tried again.
+    if (prec == INCRMT_PREC_MIXED && mixed_rest > 0) {
+        mixed_rest--;
+        mixed_rested++;
+        prec = INCRMT_PREC_FP64;
+    }
     const long N = static_cast<long>(m) * n;
     // The solve reads a residual norm back to the host after every V-cycle,
     // which a stream under capture cannot do.
@@ -1733,6 +1754,16 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
             if (use_graph && (r = capture())) return r;
         }
         rn_prev = rn;
+    }
+    if (prec == INCRMT_PREC_MIXED) {
+        if (cur != prec) {
+            if (++mixed_streak >= kMixedStrikes) {
+                mixed_streak = 0;
+                mixed_rest = kMixedRest;
+            }
+        } else {
+            mixed_streak = 0;
+        }
     }
     if (time_it) {
         INCRMT_CK(cudaEventRecord(ev1, stream));

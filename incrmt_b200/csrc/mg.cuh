@@ -67,6 +67,11 @@ public:
     long long coarse_builds = 0;
     long long coarse_retries = 0;    // solves repeated after rebuilding lagged coarse levels
     long long mixed_fallbacks = 0;   // mixed-precision solves finished with FP64 V-cycles
+    // Mixed solves that fell back in a row, the FP64 solves still to run
+    // before mixed precision is tried again, and the solves run that way.
+    static constexpr int kMixedStrikes = 3, kMixedRest = 50;
+    int mixed_streak = 0, mixed_rest = 0;
+    long long mixed_rested = 0;
     const double *lag_rho = nullptr; // density of the last set_density_lagged (read again on a retry)
     int lag_ld = 0;
     bool f32_stale = true;           // FP32 Galerkin stencils not cast since the last rebuild

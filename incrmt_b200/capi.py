@@ -463,8 +463,15 @@ class Simulation:
             return name
         return FIELDS.get(name, SFIELDS.get(name, {"phi": FIELD_PHI, "status": FIELD_STATUS}.get(name)))
 
-    def get(self, name, k=0):
-        out = np.empty(self.ml * self.nl)
+    def get(self, name, k=0, out=None):
+        """A field on the ghosted grid (incrmt_get_field). `out`, if given,
+        is a C-contiguous float64 array of nl x ml elements to fill (e.g. a
+        view of pinned host memory, which the copy then reaches at full
+        PCIe bandwidth)."""
+        if out is None:
+            out = np.empty(self.ml * self.nl)
+        elif out.dtype != np.float64 or out.size != self.ml * self.nl or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float64 array of nl x ml elements")
         check(lib().incrmt_get_field(self._h, self._fid(name), k, _dptr(out)))
         return out.reshape(self.nl, self.ml)
 

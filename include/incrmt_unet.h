@@ -145,9 +145,11 @@ int incrmt_conv_status(void);
 /** Kernel choice of incrmt_conv_bf16 (and of the networks' 3x3 layers) for
  * the whole process: 0 automatic (default), 1 one tap per pipeline stage,
  * 2 row reuse (each stage holds one column offset of the tile's rows -1..8
- * and the weights of that column's three taps). Both compute the same
- * products; the FP32 sums visit the taps in another order. No reference
- * counterpart (a check and tuning knob); INCRMT_ERR_BADARG outside 0..2. */
+ * and the weights of that column's three taps), 3 row reuse in persistent
+ * CTAs with the layer's weights resident in shared memory (layers of at most
+ * 128 outputs whose weights fit; others fall back to 2). All compute the same
+ * products; the FP32 sums visit the taps in other orders. No reference
+ * counterpart (a check and tuning knob); INCRMT_ERR_BADARG outside 0..3. */
 int incrmt_conv_set_variant(int variant);
 
 /** Kernel launches issued by this network so far. */

@@ -776,7 +776,7 @@ def conv_status():
 
 def conv_set_variant(variant):
     """3x3 kernel choice for the process (incrmt_conv_set_variant): 0
-    automatic, 1 one tap per stage, 2 row reuse."""
+    automatic, 1 one tap per stage, 2 row reuse, 3 resident weights."""
     check(_ulib().incrmt_conv_set_variant(int(variant)))
 
 

@@ -99,6 +99,10 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -286,6 +290,179 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+}
+
+constexpr int kPersistThreads = 192;  // producer warp, MMA warp, four epilogue warps
+
+/** Persistent 3x3 convolution with the layer's weights resident in shared
+ * memory (row reuse as in k_conv_tc<9, KC, true>). Each CTA loads all 9 x
+ * Cin x N weights once, then walks the 16 x 8 pixel tiles blockIdx.x,
+ * blockIdx.x + gridDim.x, ...: warp 0 (one thread) streams the tiles' input
+ * stages (one column offset and channel chunk each: 16 x 10 pixels x KC)
+ * through a ring of S buffers without draining between tiles, warp 1 (one
+ * thread) issues the three row offsets' MMAs of each stage against the
+ * resident weights into one of two tensor-memory accumulators (tile j uses
+ * accumulator j mod 2), and warps 2-5 drain the other accumulator (bias,
+ * ReLU, BF16 stores) while the next tile accumulates. Only input pixels cross
+ * from L2 per tile. Barriers: full[S], empty[S] (stage ring), wfull
+ * (weights), tfull[2] (MMA -> epilogue), tempty[2] (epilogue -> MMA, one
+ * arrival per epilogue warp), done (all MMAs complete). Every wait is
+ * bounded as in k_conv_tc. Dynamic shared memory: 1024 + W + S * A + 8 *
+ * (2S + 6) + 16, W = 9 (Cin / KC) N KC 2 bytes of weights, A = 160 KC 2. */
+template <int KC>
+__global__ void __launch_bounds__(kPersistThreads, 1)
+    k_conv_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                      const float *__restrict__ bias, bf16 *__restrict__ Y, int H, int W, int N, int tiles_x,
+                      int tiles_y, int ntiles, int nck, int flip, int relu, int S, uint32_t cols) {
+    constexpr uint32_t abytes = (kTileM + 2 * kRowsW) * KC * 2;
+    extern __shared__ __align__(1024) unsigned char conv_smem[];
+    const uint32_t raw = smem_addr(conv_smem);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    const uint32_t tbytes = static_cast<uint32_t>(N) * KC * 2;  // one (tap, chunk) block of weights
+    const uint32_t wbytes = 9u * nck * tbytes;
+    const uint32_t sW = base, sA = base + wbytes;
+    const uint32_t bar0 = sA + S * abytes;
+    // full[s] = bar0 + 8s, empty[s] = bar0 + 8(S+s), then wfull, tfull[2], tempty[2], done
+    const uint32_t wfull = bar0 + 16 * S, tfull = wfull + 8, tempty = tfull + 16, done = tempty + 16;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(conv_smem + (done + 8 - raw));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int G = gridDim.x;
+
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 2 * S; q++) mbar_init(bar0 + 8 * q, 1);
+        mbar_init(wfull, 1);
+        mbar_init(tfull, 1);
+        mbar_init(tfull + 8, 1);
+        mbar_init(tempty, 4);
+        mbar_init(tempty + 8, 4);
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(2 * cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0) {
+        // producer: the weights once, then the tiles' input stages
+        mbar_arrive_expect_tx(wfull, wbytes);
+        for (int tap = 0; tap < 9; tap++)
+            for (int ck = 0; ck < nck; ck++)
+                tma_load_3d(sW + (tap * nck + ck) * tbytes, &mapB, wfull, ck * KC, 0, flip ? 8 - tap : tap);
+        int it = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += G) {
+            int t = tile;
+            const int tx = t % tiles_x;
+            t /= tiles_x;
+            const int ty = t % tiles_y, b = t / tiles_y;
+            const int x0 = tx * kRowsW, y0 = ty * kRowsH;
+            for (int g = 0; g < 3 && ok; g++)
+                for (int ck = 0; ck < nck; ck++) {
+                    const int s = it % S;
+                    if (it >= S && !mbar_wait(bar0 + 8 * (S + s), ((it / S) - 1) & 1)) { ok = false; break; }
+                    mbar_arrive_expect_tx(bar0 + 8 * s, abytes);
+                    tma_load_4d(sA + s * abytes, &mapA, bar0 + 8 * s, ck * KC, x0 + g - 1, y0 - 1, b);
+                    it++;
+                }
+        }
+        // no copy may still be in flight when the CTA exits
+        for (int q = it > S ? it - S : 0; q < it; q++) mbar_wait(bar0 + 8 * (q % S), (q / S) & 1);
+        mbar_wait(wfull, 0);
+    } else if (threadIdx.x == 32) {
+        // MMA issuer
+        const uint32_t idesc = instr_desc(N);
+        bool ok = mbar_wait(wfull, 0);
+        int it = 0, j = 0;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += G, j++) {
+            const int a = j & 1;
+            if (j >= 2 && !mbar_wait(tempty + 8 * a, ((j >> 1) - 1) & 1)) break;
+            tc_fence_after();
+            const uint32_t acc = tmem + a * cols;
+            for (int g = 0; g < 3 && ok; g++)
+                for (int ck = 0; ck < nck; ck++) {
+                    const int s = it % S;
+                    if (!mbar_wait(bar0 + 8 * s, (it / S) & 1)) { ok = false; break; }
+                    tc_fence_after();
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        const uint64_t ad = smem_desc<KC>(sA + s * abytes + r * kRowsW * KC * 2),
+                                       bd = smem_desc<KC>(sW + ((3 * r + g) * nck + ck) * tbytes);
+#pragma unroll
+                        for (int k = 0; k < KC / 16; k++)
+                            tc_mma(acc, ad + 2 * k, bd + 2 * k, idesc, (g > 0 || ck > 0 || r > 0 || k > 0) ? 1u : 0u);
+                    }
+                    tc_commit(bar0 + 8 * (S + s));
+                    it++;
+                }
+            tc_commit(tfull + 8 * a);
+        }
+        // arrives once every MMA issued above has completed
+        tc_commit(done);
+    } else if (warp >= 2) {
+        // epilogue: warp w reads tensor-memory lanes 32 (w mod 4) .. + 31
+        const int q = warp & 3;
+        const int r = q * 32 + lane;
+        int j = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += G, j++) {
+            const int a = j & 1;
+            bool ok = mbar_wait(tfull + 8 * a, (j >> 1) & 1);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            tc_fence_after();
+            int t = tile;
+            const int tx = t % tiles_x;
+            t /= tiles_x;
+            const int ty = t % tiles_y, b = t / tiles_y;
+            const int py = ty * kRowsH + r / kRowsW, px = tx * kRowsW + r % kRowsW;
+            const bool valid = py < H && px < W;
+            bf16 *yrow = Y + ((static_cast<long>(b) * H + py) * W + px) * static_cast<long>(N);
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                uint32_t v[16];
+                tc_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + a * cols + static_cast<uint32_t>(c0), v);
+                if (!valid) continue;
+                uint32_t packed[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    float f0 = __uint_as_float(v[2 * e]), f1 = __uint_as_float(v[2 * e + 1]);
+                    if (bias) {
+                        f0 += bias[c0 + 2 * e];
+                        f1 += bias[c0 + 2 * e + 1];
+                    }
+                    if (relu) {
+                        f0 = fmaxf(f0, 0.f);
+                        f1 = fmaxf(f1, 0.f);
+                    }
+                    const __nv_bfloat162 h = __floats2bfloat162_rn(f0, f1);
+                    packed[e] = *reinterpret_cast<const uint32_t *>(&h);
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(yrow + c0);
+                dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+                dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty + 8 * a);
+        }
+    }
+    __syncwarp();
+    if (warp == 0) {
+        // every MMA done before the tensor memory is freed
+        mbar_wait(done, 0);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * cols) : "memory");
 }
 
 /** Shared-memory descriptor of an MN-major operand: atoms of KA elements
@@ -552,7 +729,78 @@ int launch_taps(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
     return launch_conv<TAPS, 16, ROWS>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
 }
 
-int g_conv_variant = 0;  // 0 automatic, 1 one tap per stage, 2 row reuse
+/** Launch of k_conv_tc_persist; INCRMT_ERR_BADARG (nothing launched) when
+ * the layer's weights and two stages do not fit in shared memory. */
+template <int KC>
+int launch_conv_persist(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, bool flip,
+                        const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
+    EncodeTiled enc = encode_tiled();
+    if (!enc) {
+        set_error("conv: cuTensorMapEncodeTiled is not available");
+        return INCRMT_ERR_CUDA;
+    }
+    const int nck = Cin / KC;
+    const size_t abytes = static_cast<size_t>(kTileM + 2 * kRowsW) * KC * 2;
+    const size_t wbytes = 9ull * nck * Cout * KC * 2;
+    const size_t fixed = 1024 + wbytes + 8 * 6 + 16;
+    if (fixed + 2 * (abytes + 16) > static_cast<size_t>(kMaxSmem)) {
+        set_error("conv: weights of %zu bytes leave no room for two stages", wbytes);
+        return INCRMT_ERR_BADARG;
+    }
+    int S = static_cast<int>((kMaxSmem - fixed) / (abytes + 16));
+    if (S > 8) S = 8;
+    const size_t smem = fixed + S * abytes + 16 * S;
+    const int tiles_x = (W + kRowsW - 1) / kRowsW, tiles_y = (H + kRowsH - 1) / kRowsH;
+    const int ntiles = B * tiles_x * tiles_y;
+    CUtensorMap mA, mB;
+    {
+        const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Cin), static_cast<cuuint64_t>(W),
+                                    static_cast<cuuint64_t>(H), static_cast<cuuint64_t>(B)};
+        const cuuint64_t strides[3] = {static_cast<cuuint64_t>(Cin) * 2, static_cast<cuuint64_t>(W) * Cin * 2,
+                                       static_cast<cuuint64_t>(H) * W * Cin * 2};
+        const cuuint32_t box[4] = {static_cast<cuuint32_t>(KC), static_cast<cuuint32_t>(kRowsW),
+                                   static_cast<cuuint32_t>(kRowsH + 2), 1};
+        const cuuint32_t es[4] = {1, 1, 1, 1};
+        CUresult r = enc(&mA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(X), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(KC), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            set_error("conv: activation tensor map rejected (%d)", static_cast<int>(r));
+            return INCRMT_ERR_CUDA;
+        }
+    }
+    {
+        const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Cin), static_cast<cuuint64_t>(Cout), 9};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(Cin) * 2, static_cast<cuuint64_t>(Cout) * Cin * 2};
+        const cuuint32_t box[3] = {static_cast<cuuint32_t>(KC), static_cast<cuuint32_t>(Cout), 1};
+        const cuuint32_t es[3] = {1, 1, 1};
+        CUresult r = enc(&mB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16 *>(wk), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(KC), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            set_error("conv: weight tensor map rejected (%d)", static_cast<int>(r));
+            return INCRMT_ERR_CUDA;
+        }
+    }
+    uint32_t cols = 32;
+    while (cols < static_cast<uint32_t>(Cout)) cols <<= 1;
+    static bool attr = false;
+    if (!attr) {
+        INCRMT_CK(cudaFuncSetAttribute(k_conv_tc_persist<KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+        attr = true;
+    }
+    int occ = 0;
+    INCRMT_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv_tc_persist<KC>, kPersistThreads, smem));
+    if (occ < 1) occ = 1;
+    while (occ > 1 && occ * 2 * cols > 512) occ--;  // two accumulators per CTA in the SM's 512 columns
+    const int grid = ntiles < kB200SMs * occ ? ntiles : kB200SMs * occ;
+    k_conv_tc_persist<KC><<<grid, kPersistThreads, smem, s>>>(mA, mB, bias, Y, H, W, Cout, tiles_x, tiles_y, ntiles,
+                                                              nck, flip ? 1 : 0, relu ? 1 : 0, S, cols);
+    INCRMT_CKL("k_conv_tc_persist");
+    return INCRMT_OK;
+}
+
+int g_conv_variant = 0;  // 0 automatic, 1 one tap per stage, 2 row reuse, 3 row reuse with resident weights
 
 /** Split of the weight gradient over the pixels: about four waves of CTAs
  * over the SMs. */
@@ -684,7 +932,18 @@ int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int tap
     // Row reuse (3x3) for up to 128 output channels per CTA, where its three
     // taps' weights per stage still leave room for two CTAs per SM; one tap
     // per stage above that.
-    const bool rows = taps == 9 && (g_conv_variant == 2 || (g_conv_variant == 0 && Cout <= 128));
+    // Resident weights (persistent CTAs) where a 3x3 layer's weights take at
+    // most 160 KB with 64 to 128 output channels, the default there. With
+    // fewer outputs each tile's MMAs are too short for one CTA's four
+    // epilogue warps to keep up, and row reuse with several CTAs per SM is
+    // faster (2048^2, 32 -> 32: 291 against 186 TFLOP/s).
+    if (taps == 9 && Cout <= 128 && 9ull * Cin * Cout * 2 <= 160 * 1024 &&
+        (g_conv_variant == 3 || (g_conv_variant == 0 && Cout >= 64))) {
+        if (Cin % 64 == 0) return launch_conv_persist<64>(X, B, H, W, Cin, wk, Cout, flip, bias, relu, Y, s);
+        if (Cin % 32 == 0) return launch_conv_persist<32>(X, B, H, W, Cin, wk, Cout, flip, bias, relu, Y, s);
+        return launch_conv_persist<16>(X, B, H, W, Cin, wk, Cout, flip, bias, relu, Y, s);
+    }
+    const bool rows = taps == 9 && (g_conv_variant == 2 || (g_conv_variant != 1 && Cout <= 128));
     // output channels per CTA: all of them up to the cap (128 with row reuse,
     // else 256), else the largest multiple of 16 below the cap dividing Cout
     const int cap = rows ? 128 : 256;
@@ -699,8 +958,8 @@ int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int tap
 }
 
 int conv_tc_set_variant(int v) {
-    if (v < 0 || v > 2) {
-        set_error("conv: variant %d not in 0..2", v);
+    if (v < 0 || v > 3) {
+        set_error("conv: variant %d not in 0..3", v);
         return INCRMT_ERR_BADARG;
     }
     g_conv_variant = v;

@@ -364,9 +364,11 @@ def cpu_reference_sim(workload, steps, warmup):
 
 
 def cpu_steps(workload):
-    """A bounded sample for the CPU reference: a few seconds to a minute."""
+    """A bounded sample for the CPU reference: about 10-30 s of host work
+    (the 2048-wide flag and sediment run at about one step per second on
+    16 threads)."""
     kind, m, n = SIM_WORKLOADS[workload]
-    return {"sspin": 40, "flag": 2, "sed": 2}[kind] if m * n > 2e6 else 40
+    return {"sspin": 40, "flag": 12, "sed": 12}[kind] if m * n > 2e6 else 40
 
 
 def run_reference(args, ws, rank):
@@ -689,8 +691,8 @@ def run_ours_sim(args, ws, rank, local, dist):
         if plain is not None and "phases" in plain:
             roof["projection_plain_fp64"] = projection_roofline(None, args.workload, capi.PREC_FP64, plain["vc_mac"],
                                                                 plain["vc_fem"], plain["phases"])
-    start = "the extrapolation 2 z(n-1) - z(n-2) of the last two solutions" if args.extrapolate else \
-        "the previous solution"
+    start = {0: "the previous solution", 1: "the extrapolation 2 z(n-1) - z(n-2) of the last two solutions",
+             2: "the extrapolation 3 z(n-1) - 3 z(n-2) + z(n-3) of the last three solutions"}[args.extrapolate]
     guess = f"learned warm start on {start}" if args.guess == "learned" else start
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws,
@@ -997,9 +999,10 @@ def main():
                     help="initial guess of each projection: the previous solution, or the learned warm start "
                          "trained first on a training run of the workload")
     ap.add_argument("--learned", action="store_true", help="same as --guess learned")
-    ap.add_argument("--extrapolate", type=int, default=1, choices=[0, 1],
-                    help="1: the projections start from 2 z(n-1) - z(n-2) (incrmt_sim_set_guess); the plain "
-                         "FP64 comparison run always starts from the previous solution")
+    ap.add_argument("--extrapolate", type=int, default=2, choices=[0, 1, 2],
+                    help="1: the projections start from 2 z(n-1) - z(n-2), 2: from 3 z(n-1) - 3 z(n-2) + "
+                         "z(n-3) (incrmt_sim_set_guess); the plain FP64 comparison run always starts from the "
+                         "previous solution")
     ap.add_argument("--coarse-refresh", type=int, default=1,
                     help="rebuild the projections' Galerkin coarse operators every K projections "
                          "(1: on every density change, as the reference)")

@@ -245,7 +245,9 @@ int incrmt_sim_set_windows(incrmt_sim *h, int on);
  * fluid_2d::mac_projection and finite_element_projection solve from the
  * pressure left in place (fluid_2d.cc:1175-1236, 1297-1328); 1 from the
  * third solve on, the linear extrapolation 2 z(n-1) - z(n-2) of the last two
- * solutions (one extra array per system). Every solve still stops at the same
+ * solutions (one extra array per system); 2 from the fourth solve on, the
+ * quadratic 3 z(n-1) - 3 z(n-2) + z(n-3) (two extra arrays per system).
+ * Every solve still stops at the same
  * relative residual; the start only changes how many V-cycles that takes. A
  * learned guess (incrmt_sim_set_learned) corrects whichever start this
  * gives. Setting the mode, and incrmt_set_field, restart the history.

@@ -582,7 +582,8 @@ class Simulation:
 
     def set_guess(self, mode):
         """Warm start of the projections (incrmt_sim_set_guess): 0 the
-        previous solution, 1 the extrapolation 2 z(n-1) - z(n-2)."""
+        previous solution, 1 the extrapolation 2 z(n-1) - z(n-2), 2 the
+        quadratic 3 z(n-1) - 3 z(n-2) + z(n-3)."""
         check(lib().incrmt_sim_set_guess(self._h, int(mode)))
 
     def set_profiling(self, on=True, smoothers=False):

@@ -157,14 +157,19 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
  * crosses from L2 3 (Ht + 2) / Ht = 3.75 times instead of 9, and each barrier
  * round trip feeds three times the tensor-core work. Otherwise a stage holds
  * one tap: 128 shifted pixels and that tap's weights. */
-template <int TAPS, int KC, bool ROWS>
+template <int TAPS, int KC, bool ROWS, int HALVES = 1>
 __global__ void __launch_bounds__(kThreads, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
               const float *__restrict__ bias, bf16 *__restrict__ Y, int H, int W, int N, int ldy, int Wt, int Ht,
               int tiles_x, int tiles_y, int nck, int flip, int relu, int S, uint32_t tmem_cols) {
     static_assert(!ROWS || TAPS == 9, "row reuse is for 3x3 convolutions");
+    static_assert(HALVES == 1 || ROWS, "two halves only with row reuse");
+    // HALVES = 2 (row reuse): the tile is 16 x 16 pixels, two 128-pixel
+    // halves stacked in y, each with its own tensor-memory accumulator of
+    // tmem_cols / 2 columns; a stage holds the 16 x 18 input pixels of both
+    // (rows -1 .. 16) and the three taps' weights, which both halves use.
     constexpr int kGroup = ROWS ? 3 : 1;                         // taps per stage
-    constexpr uint32_t abytes = (ROWS ? kTileM + 2 * kRowsW : kTileM) * KC * 2;
+    constexpr uint32_t abytes = (ROWS ? HALVES * kTileM + 2 * kRowsW : kTileM) * KC * 2;
     extern __shared__ __align__(1024) unsigned char conv_smem[];
     const uint32_t raw = smem_addr(conv_smem);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -235,14 +240,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!mbar_wait(bar0 + 8 * s, (it / S) & 1)) break;
             tc_fence_after();
 #pragma unroll
-            for (int r = 0; r < kGroup; r++) {
-                // row offset r - 1: the stage's pixels from row r on (ROWS)
-                const uint64_t ad = smem_desc<KC>(sA + s * abytes + r * kRowsW * KC * 2),
-                               bd = smem_desc<KC>(sB + s * bbytes + r * tbytes);
+            for (int h = 0; h < HALVES; h++)
 #pragma unroll
-                for (int k = 0; k < KC / 16; k++)
-                    tc_mma(tmem, ad + 2 * k, bd + 2 * k, idesc, (it > 0 || r > 0 || k > 0) ? 1u : 0u);
-            }
+                for (int r = 0; r < kGroup; r++) {
+                    // row offset r - 1: the stage's pixels from row h * 8 + r on (ROWS)
+                    const uint64_t ad = smem_desc<KC>(sA + s * abytes + (h * kRowsH + r) * kRowsW * KC * 2),
+                                   bd = smem_desc<KC>(sB + s * bbytes + r * tbytes);
+#pragma unroll
+                    for (int k = 0; k < KC / 16; k++)
+                        tc_mma(tmem + h * (tmem_cols / HALVES), ad + 2 * k, bd + 2 * k, idesc,
+                               (it > 0 || r > 0 || k > 0) ? 1u : 0u);
+                }
             tc_commit(bar0 + 8 * (S + s));
         }
         // arrives once every MMA issued above has completed
@@ -257,14 +265,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     // on whether the wait succeeded
     ok = __all_sync(0xffffffffu, ok);
     tc_fence_after();
-    if (ok) {
+    for (int h = 0; h < HALVES && ok; h++) {
         const int r = warp * 32 + lane;
-        const int py = y0 + r / Wt, px = x0 + r % Wt;
+        const int py = y0 + h * kRowsH + r / Wt, px = x0 + r % Wt;
         const bool valid = py < H && px < W;
         bf16 *yrow = Y + ((static_cast<long>(b) * H + py) * W + px) * static_cast<long>(ldy) + n0;
         for (int c0 = 0; c0 < N; c0 += 16) {
             uint32_t v[16];
-            tc_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), v);
+            tc_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + h * (tmem_cols / HALVES) +
+                        static_cast<uint32_t>(c0),
+                    v);
             if (!valid) continue;
             uint32_t packed[8];
 #pragma unroll
@@ -278,8 +288,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     f0 = fmaxf(f0, 0.f);
                     f1 = fmaxf(f1, 0.f);
                 }
-                const __nv_bfloat162 h = __floats2bfloat162_rn(f0, f1);
-                packed[j] = *reinterpret_cast<const uint32_t *>(&h);
+                const __nv_bfloat162 hv = __floats2bfloat162_rn(f0, f1);
+                packed[j] = *reinterpret_cast<const uint32_t *>(&hv);
             }
             uint4 *dst = reinterpret_cast<uint4 *>(yrow + c0);
             dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
@@ -642,7 +652,7 @@ CUtensorMapSwizzle swizzle_of(int kc) {
 
 constexpr int kMaxSmem = 227 * 1024;
 
-template <int TAPS, int KC, bool ROWS>
+template <int TAPS, int KC, bool ROWS, int HALVES = 1>
 int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, int Nt, bool flip,
                 const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
     EncodeTiled enc = encode_tiled();
@@ -650,7 +660,7 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
         set_error("conv: cuTensorMapEncodeTiled is not available");
         return INCRMT_ERR_CUDA;
     }
-    const int Wt = ROWS ? kRowsW : W >= 128 ? 128 : W >= 64 ? 64 : W >= 32 ? 32 : 16, Ht = kTileM / Wt;
+    const int Wt = ROWS ? kRowsW : W >= 128 ? 128 : W >= 64 ? 64 : W >= 32 ? 32 : 16, Ht = HALVES * kTileM / Wt;
     const int tiles_x = (W + Wt - 1) / Wt, tiles_y = (H + Ht - 1) / Ht;
     CUtensorMap mA, mB;
     {
@@ -689,7 +699,7 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
         // as many stages as the CTA has steps, within a quarter of an SM's
         // shared memory (four CTAs per SM where the stages are small), at
         // least two
-        per = static_cast<size_t>(kTileM + 2 * kRowsW + 3 * Nt) * KC * 2;
+        per = static_cast<size_t>(HALVES * kTileM + 2 * kRowsW + 3 * Nt) * KC * 2;
         const int steps = 3 * (Cin / KC);
         S = static_cast<int>((56 * 1024) / per);
         if (S > steps) S = steps;
@@ -708,25 +718,29 @@ int launch_conv(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int
     }
     uint32_t cols = 32;
     while (cols < static_cast<uint32_t>(Nt)) cols <<= 1;
+    cols *= HALVES;
     static bool attr = false;
     if (!attr) {
-        INCRMT_CK(cudaFuncSetAttribute(k_conv_tc<TAPS, KC, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        INCRMT_CK(cudaFuncSetAttribute(k_conv_tc<TAPS, KC, ROWS, HALVES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kMaxSmem));
         attr = true;
     }
     const dim3 grid(static_cast<unsigned>(B * tiles_x * tiles_y), static_cast<unsigned>(Cout / Nt));
-    k_conv_tc<TAPS, KC, ROWS><<<grid, kThreads, smem, s>>>(mA, mB, bias, Y, H, W, Nt, Cout, Wt, Ht, tiles_x,
-                                                           tiles_y, Cin / KC, flip ? 1 : 0, relu ? 1 : 0, S, cols);
+    k_conv_tc<TAPS, KC, ROWS, HALVES><<<grid, kThreads, smem, s>>>(mA, mB, bias, Y, H, W, Nt, Cout, Wt, Ht, tiles_x,
+                                                                   tiles_y, Cin / KC, flip ? 1 : 0, relu ? 1 : 0, S,
+                                                                   cols);
     INCRMT_CKL("k_conv_tc");
     return INCRMT_OK;
 }
 
-template <int TAPS, bool ROWS>
+template <int TAPS, bool ROWS, int HALVES = 1>
 int launch_taps(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int Cout, int Nt, bool flip,
                 const float *bias, bool relu, bf16 *Y, cudaStream_t s) {
-    if (Cin % 64 == 0) return launch_conv<TAPS, 64, ROWS>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
-    if (Cin % 32 == 0) return launch_conv<TAPS, 32, ROWS>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
-    return launch_conv<TAPS, 16, ROWS>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    if (Cin % 64 == 0)
+        return launch_conv<TAPS, 64, ROWS, HALVES>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    if (Cin % 32 == 0)
+        return launch_conv<TAPS, 32, ROWS, HALVES>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
+    return launch_conv<TAPS, 16, ROWS, HALVES>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
 }
 
 /** Launch of k_conv_tc_persist; INCRMT_ERR_BADARG (nothing launched) when
@@ -952,14 +966,18 @@ int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int tap
         Nt = cap;
         while (Cout % Nt) Nt -= 16;
     }
+    // Two 128-pixel halves per CTA (variant 4): the weights of each stage
+    // serve 256 pixels.
+    if (taps == 9 && g_conv_variant == 4 && Cout <= 64)
+        return launch_taps<9, true, 2>(X, B, H, W, Cin, wk, Cout, Cout, flip, bias, relu, Y, s);
     if (rows) return launch_taps<9, true>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
     if (taps == 9) return launch_taps<9, false>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
     return launch_taps<1, false>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
 }
 
 int conv_tc_set_variant(int v) {
-    if (v < 0 || v > 3) {
-        set_error("conv: variant %d not in 0..3", v);
+    if (v < 0 || v > 4) {
+        set_error("conv: variant %d not in 0..4", v);
         return INCRMT_ERR_BADARG;
     }
     g_conv_variant = v;

@@ -68,10 +68,11 @@ struct Sim {
     unsigned long long *d_lcnt = nullptr;  // [sys][applied, fallback]
     // Warm start of the projections: 0 the previous solution (the
     // reference's), 1 its linear extrapolation 2 z(n-1) - z(n-2) once two
-    // solutions exist; zold[sys] holds z(n-2), nsol[sys] the solves since the
-    // history was last reset.
+    // solutions exist, 2 the quadratic one 3 z(n-1) - 3 z(n-2) + z(n-3) once
+    // three exist; zold[sys] holds z(n-2), zold2[sys] z(n-3), nsol[sys] the
+    // solves since the history was last reset.
     int guess = 0;
-    double *zold[2] = {nullptr, nullptr};
+    double *zold[2] = {nullptr, nullptr}, *zold2[2] = {nullptr, nullptr};
     long long nsol[2] = {0, 0};
     int extrapolate_guess(int sys, double *z);
     incrmt_mg_opts mgo{1e-9, 200, INCRMT_PREC_FP64};
@@ -731,12 +732,16 @@ int Sim::update_reference_map(double dt) {
     return INCRMT_OK;
 }
 
-/** z = 2 z - zo and zo = the old z (extrap), or zo = z alone. */
-__global__ void k_extrapolate_guess(double *z, double *zo, long N, int extrap) {
+/** The extrapolated start of order `order` (0: z kept, 1: 2 z - zo,
+ * 2: 3 (z - zo) + zo2) and the history shifted: zo2 = zo (when kept, zo2
+ * not null), zo = the old z. */
+__global__ void k_extrapolate_guess(double *z, double *zo, double *zo2, long N, int order) {
     for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
          q += static_cast<long>(gridDim.x) * blockDim.x) {
-        const double v = z[q];
-        if (extrap) z[q] = __dsub_rn(2.0 * v, zo[q]);
+        const double v = z[q], o = zo[q];
+        if (order == 1) z[q] = __dsub_rn(2.0 * v, o);
+        if (order == 2) z[q] = __dadd_rn(3.0 * __dsub_rn(v, o), zo2[q]);
+        if (zo2) zo2[q] = o;
         zo[q] = v;
     }
 }
@@ -744,9 +749,11 @@ __global__ void k_extrapolate_guess(double *z, double *zo, long N, int extrap) {
 /** The extrapolated warm start of a projection (guess 1): from the third
  * solve on, z(n-1) becomes 2 z(n-1) - z(n-2), a second-order prediction of
  * a pressure that varies smoothly in time; the solve then reaches the same
- * relative residual from a closer start. The first two solves keep the
- * previous solution, as the reference does always (fluid_2d.cc:1175-1236,
- * 1297-1328 solve from the pressure left in place). */
+ * relative residual from a closer start. Guess 2 uses the quadratic
+ * 3 z(n-1) - 3 z(n-2) + z(n-3) from the fourth solve on (linear for the
+ * third). The first two solves keep the previous solution, as the reference
+ * does always (fluid_2d.cc:1175-1236, 1297-1328 solve from the pressure
+ * left in place). */
 int Sim::extrapolate_guess(int sys, double *z) {
     if (!guess) return INCRMT_OK;
     const long N = sys == INCRMT_SYS_MAC ? static_cast<long>(g.m) * g.n : static_cast<long>(g.mf) * g.nf;
@@ -754,8 +761,13 @@ int Sim::extrapolate_guess(int sys, double *z) {
         int r = alloc(&zold[sys], static_cast<size_t>(N));
         if (r) return r;
     }
+    if (guess == 2 && !zold2[sys]) {
+        int r = alloc(&zold2[sys], static_cast<size_t>(N));
+        if (r) return r;
+    }
+    const int order = guess == 2 && nsol[sys] >= 3 ? 2 : nsol[sys] >= 2 ? 1 : 0;
     const int nb = cdiv(N, 256) < 4 * kB200SMs ? cdiv(N, 256) : 4 * kB200SMs;
-    k_extrapolate_guess<<<nb, 256, 0, stream>>>(z, zold[sys], N, nsol[sys] >= 2 ? 1 : 0);
+    k_extrapolate_guess<<<nb, 256, 0, stream>>>(z, zold[sys], guess == 2 ? zold2[sys] : nullptr, N, order);
     launches++;
     INCRMT_CKL("k_extrapolate_guess");
     return INCRMT_OK;
@@ -1552,7 +1564,7 @@ int incrmt_l_comparison(incrmt_sim *h, incrmt_sim *fine, double *err) {
 }
 
 int incrmt_sim_set_guess(incrmt_sim *h, int mode) {
-    if (!h || mode < 0 || mode > 1) { set_error("bad argument"); return INCRMT_ERR_BADARG; }
+    if (!h || mode < 0 || mode > 2) { set_error("bad argument"); return INCRMT_ERR_BADARG; }
     h->s.guess = mode;
     h->s.nsol[0] = h->s.nsol[1] = 0;
     return INCRMT_OK;

@@ -12,9 +12,10 @@ high (width 128) and eight rows high (width 16), output channels split over
 two CTAs (384 = 2 x 192), the 1x1 head, bias and ReLU, and the reversed taps
 of the input-gradient convolution; every 3x3 case runs with each kernel
 choice (incrmt_conv_set_variant: automatic, one tap per stage, row reuse,
-row reuse with the weights resident in persistent CTAs; the 16 x 8 tiles of
-the last two are partial at widths 40, 56 and 8 and heights 20 and 12, and
-the persistent CTAs each take several tiles of the larger images).
+row reuse with the weights resident in persistent CTAs, row reuse with two
+128-pixel halves per CTA; the 16 x 8 and 16 x 16 tiles of the last three are
+partial at widths 40, 56 and 8 and heights 20 and 12, and the persistent CTAs
+each take several tiles of the larger images).
 """
 import numpy as np
 import pytest
@@ -37,7 +38,7 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("B,H,W,cin,cout,taps,relu,use_bias,flip", CASES)
 def test_conv_matches_torch(gpu, B, H, W, cin, cout, taps, relu, use_bias, flip, variant):
     import torch

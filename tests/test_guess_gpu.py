@@ -1,4 +1,5 @@
-"""The extrapolated warm start of the projections (incrmt_sim_set_guess 1):
+"""The extrapolated warm starts of the projections (incrmt_sim_set_guess 1,
+linear, and 2, quadratic):
 every solve stops at the same 1e-9 relative residual as with the previous
 solution as the start (the reference's), so after 40 steps of the rotor and
 of two falling bodies at 256^2 the fields agree with the default run to
@@ -28,13 +29,14 @@ def _scene(kind, guess):
 
 
 @pytest.mark.parametrize("kind", ["sspin", "bodies"])
-def test_extrapolated_guess(gpu, kind):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_extrapolated_guess(gpu, kind, mode):
     runs = {}
-    for guess in (0, 1):
+    for guess in (0, mode):
         g, dt = _scene(kind, guess)
         g.step(0.9 * dt, 40)
         runs[guess] = (g, g.stats())
-    (g0, s0), (g1, s1) = runs[0], runs[1]
+    (g0, s0), (g1, s1) = runs[0], runs[mode]
     for f in ("u", "v", "p"):
         e = _rel(g1.get(f)[2:-2, 2:-2], g0.get(f)[2:-2, 2:-2])
         assert e <= 1e-6, (f, e)
@@ -53,5 +55,5 @@ def test_bad_mode_refused(gpu):
     from incrmt_b200 import capi
     g = capi.Simulation(64, 64, ntrace=0)
     with pytest.raises(capi.IncrmtError):
-        g.set_guess(2)
+        g.set_guess(3)
     g.close()

@@ -147,9 +147,11 @@ int incrmt_conv_status(void);
  * 2 row reuse (each stage holds one column offset of the tile's rows -1..8
  * and the weights of that column's three taps), 3 row reuse in persistent
  * CTAs with the layer's weights resident in shared memory (layers of at most
- * 128 outputs whose weights fit; others fall back to 2). All compute the same
- * products; the FP32 sums visit the taps in other orders. No reference
- * counterpart (a check and tuning knob); INCRMT_ERR_BADARG outside 0..3. */
+ * 128 outputs whose weights fit; others fall back to 2), 4 row reuse with two
+ * 128-pixel halves per CTA sharing each stage's weights (up to 64 outputs;
+ * others fall back to 2). All compute the same products; the FP32 sums visit
+ * the taps in other orders. No reference counterpart (a check and tuning
+ * knob); INCRMT_ERR_BADARG outside 0..4. */
 int incrmt_conv_set_variant(int variant);
 
 /** Kernel launches issued by this network so far. */

@@ -777,7 +777,8 @@ def conv_status():
 
 def conv_set_variant(variant):
     """3x3 kernel choice for the process (incrmt_conv_set_variant): 0
-    automatic, 1 one tap per stage, 2 row reuse, 3 resident weights."""
+    automatic, 1 one tap per stage, 2 row reuse, 3 resident weights, 4 two
+    128-pixel halves per CTA."""
     check(_ulib().incrmt_conv_set_variant(int(variant)))
 
 

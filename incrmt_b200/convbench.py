@@ -6,7 +6,8 @@
 
 --shape B,H,W,Cin,Cout times one 3x3 layer (bias and ReLU); --variant pins
 the kernel (incrmt_conv_set_variant: 0 automatic, 1 one tap per pipeline
-stage, 2 row reuse, 3 row reuse with resident weights). Prints one JSON line
+stage, 2 row reuse, 3 row reuse with resident weights, 4 two 128-pixel halves
+per CTA). Prints one JSON line
 per layer or network: milliseconds per call and TFLOP/s of
 2*9*Cin*Cout*pixels (the network: the sum over its layers).
 """

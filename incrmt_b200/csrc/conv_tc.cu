@@ -814,7 +814,7 @@ int launch_conv_persist(const bf16 *X, int B, int H, int W, int Cin, const bf16 
     return INCRMT_OK;
 }
 
-int g_conv_variant = 0;  // 0 automatic, 1 one tap per stage, 2 row reuse, 3 row reuse with resident weights
+int g_conv_variant = 0;  // 0 automatic, 1 one tap per stage, 2 row reuse, 3 resident weights, 4 two halves
 
 /** Split of the weight gradient over the pixels: about four waves of CTAs
  * over the SMs. */
@@ -943,9 +943,14 @@ int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int tap
         set_error("conv: bad arguments (channels must be positive multiples of 16, taps 1 or 9)");
         return INCRMT_ERR_BADARG;
     }
-    // Row reuse (3x3) for up to 128 output channels per CTA, where its three
-    // taps' weights per stage still leave room for two CTAs per SM; one tap
-    // per stage above that.
+    // Two 128-pixel halves per CTA (variant 4): the weights of each stage
+    // serve 256 pixels. The default for up to 32 outputs, and for up to 64
+    // from at most 32 inputs (2048^2, 32 -> 32: 384 against 291 TFLOP/s;
+    // 1024^2, 32 -> 64: 379 against 336 with resident weights; 64 -> 64 is
+    // faster with resident weights, 537 against 364).
+    const bool halves = g_conv_variant == 4 || (g_conv_variant == 0 && (Cout <= 32 || (Cout <= 64 && Cin <= 32)));
+    if (taps == 9 && halves && Cout <= 64)
+        return launch_taps<9, true, 2>(X, B, H, W, Cin, wk, Cout, Cout, flip, bias, relu, Y, s);
     // Resident weights (persistent CTAs) where a 3x3 layer's weights take at
     // most 160 KB with 64 to 128 output channels, the default there. With
     // fewer outputs each tile's MMAs are too short for one CTA's four
@@ -957,6 +962,9 @@ int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int tap
         if (Cin % 32 == 0) return launch_conv_persist<32>(X, B, H, W, Cin, wk, Cout, flip, bias, relu, Y, s);
         return launch_conv_persist<16>(X, B, H, W, Cin, wk, Cout, flip, bias, relu, Y, s);
     }
+    // Row reuse (3x3) for up to 128 output channels per CTA, where its three
+    // taps' weights per stage still leave room for two CTAs per SM; one tap
+    // per stage above that.
     const bool rows = taps == 9 && (g_conv_variant == 2 || (g_conv_variant != 1 && Cout <= 128));
     // output channels per CTA: all of them up to the cap (128 with row reuse,
     // else 256), else the largest multiple of 16 below the cap dividing Cout
@@ -966,10 +974,6 @@ int conv_tc(const bf16 *X, int B, int H, int W, int Cin, const bf16 *wk, int tap
         Nt = cap;
         while (Cout % Nt) Nt -= 16;
     }
-    // Two 128-pixel halves per CTA (variant 4): the weights of each stage
-    // serve 256 pixels.
-    if (taps == 9 && g_conv_variant == 4 && Cout <= 64)
-        return launch_taps<9, true, 2>(X, B, H, W, Cin, wk, Cout, Cout, flip, bias, relu, Y, s);
     if (rows) return launch_taps<9, true>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
     if (taps == 9) return launch_taps<9, false>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);
     return launch_taps<1, false>(X, B, H, W, Cin, wk, Cout, Nt, flip, bias, relu, Y, s);

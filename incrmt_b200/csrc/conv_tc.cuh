@@ -31,10 +31,12 @@ int conv_tc_wgrad(const __nv_bfloat16 *X, const __nv_bfloat16 *dY, int B, int H,
                   float *dW, float *part, size_t part_floats, cudaStream_t s);
 size_t conv_tc_wgrad_workspace(int B, int H, int W, int Cin, int Cout, int taps);
 
-/** Kernel choice of conv_tc for 3x3 convolutions: 0 automatic (resident
- * weights where they fit with 64 to 128 outputs, else row reuse up to 128
- * output channels), 1 one tap per pipeline stage, 2 row reuse always, 3
- * resident weights where they fit (else as 2).
+/** Kernel choice of conv_tc for 3x3 convolutions: 0 automatic (two halves up
+ * to 32 outputs, or up to 64 from at most 32 inputs; resident weights where
+ * they fit with 64 to 128 outputs; else row reuse up to 128 outputs), 1 one
+ * tap per pipeline stage, 2 row reuse always, 3 resident weights where they
+ * fit (else as 2), 4 row reuse with two 128-pixel halves per CTA up to 64
+ * outputs (else as 2).
  * Both form the same products; the FP32 accumulation visits the taps in
  * another order. A check and tuning knob. */
 int conv_tc_set_variant(int v);

@@ -732,15 +732,36 @@ int Sim::update_reference_map(double dt) {
     return INCRMT_OK;
 }
 
-/** The extrapolated start of order `order` (0: z kept, 1: 2 z - zo,
- * 2: 3 (z - zo) + zo2) and the history shifted: zo2 = zo (when kept, zo2
+/** The extrapolated start of order `order` at one unknown (0: z, 1:
+ * 2 z - zo, 2: 3 (z - zo) + zo2). */
+__device__ __forceinline__ double extrapolated(int order, double v, double o, const double *zo2, long q) {
+    if (order == 1) return __dsub_rn(2.0 * v, o);
+    if (order == 2) return __dadd_rn(3.0 * __dsub_rn(v, o), zo2[q]);
+    return v;
+}
+
+/** Block sums of the extrapolation's increment (extrapolated - z). */
+__global__ void k_extrapolate_increment(const double *z, const double *zo, const double *zo2, long N, int order,
+                                        double *partial) {
+    double acc = 0;
+    for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
+         q += static_cast<long>(gridDim.x) * blockDim.x) {
+        const double v = z[q];
+        acc += __dsub_rn(extrapolated(order, v, zo[q], zo2, q), v);
+    }
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+/** The extrapolated start, less the mean of its increment when `isum` (the
+ * sum of the increments) is given, and the history shifted: zo2 = zo (zo2
  * not null), zo = the old z. */
-__global__ void k_extrapolate_guess(double *z, double *zo, double *zo2, long N, int order) {
+__global__ void k_extrapolate_guess(double *z, double *zo, double *zo2, long N, int order, const double *isum) {
+    const double shift = isum ? *isum / static_cast<double>(N) : 0.0;
     for (long q = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; q < N;
          q += static_cast<long>(gridDim.x) * blockDim.x) {
         const double v = z[q], o = zo[q];
-        if (order == 1) z[q] = __dsub_rn(2.0 * v, o);
-        if (order == 2) z[q] = __dadd_rn(3.0 * __dsub_rn(v, o), zo2[q]);
+        if (order) z[q] = __dsub_rn(extrapolated(order, v, o, zo2, q), shift);
         if (zo2) zo2[q] = o;
         zo[q] = v;
     }
@@ -767,7 +788,23 @@ int Sim::extrapolate_guess(int sys, double *z) {
     }
     const int order = guess == 2 && nsol[sys] >= 3 ? 2 : nsol[sys] >= 2 ? 1 : 0;
     const int nb = cdiv(N, 256) < 4 * kB200SMs ? cdiv(N, 256) : 4 * kB200SMs;
-    k_extrapolate_guess<<<nb, 256, 0, stream>>>(z, zold[sys], guess == 2 ? zold2[sys] : nullptr, N, order);
+    double *zo2 = guess == 2 ? zold2[sys] : nullptr;
+    // Without a Dirichlet condition (no zero-pressure column) the system is
+    // singular and its solutions differ by constants, which the solves
+    // neither fix nor use. Extrapolated, a constant drift between steps would
+    // grow without bound (quadratically for the quadratic start) until the
+    // residual drowns in the rounding of a huge constant; the increment's
+    // mean is therefore removed.
+    const double *isum = nullptr;
+    if (order && !g.zpr) {
+        // partial holds 4 x kB200SMs doubles: block sums, then their total
+        const int nbs = nb < 2 * kB200SMs ? nb : 2 * kB200SMs;
+        k_extrapolate_increment<<<nbs, 256, 0, stream>>>(z, zold[sys], zo2, N, order, partial);
+        k_reduce_partials<<<1, 256, 0, stream>>>(partial, nbs, partial + nbs);
+        launches += 2;
+        isum = partial + nbs;
+    }
+    k_extrapolate_guess<<<nb, 256, 0, stream>>>(z, zold[sys], zo2, N, order, isum);
     launches++;
     INCRMT_CKL("k_extrapolate_guess");
     return INCRMT_OK;

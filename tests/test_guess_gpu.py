@@ -57,3 +57,22 @@ def test_bad_mode_refused(gpu):
     with pytest.raises(capi.IncrmtError):
         g.set_guess(3)
     g.close()
+
+
+def test_singular_systems_do_not_drift(gpu):
+    """The rotor's walled box makes both pressure systems pure Neumann (no
+    zero-pressure column): their solutions are fixed only up to a constant.
+    The extrapolated starts remove the mean of their increment, so over many
+    steps the quadratic start does not grow that constant (which it would
+    at the square of the step count) and every solve still converges."""
+    from incrmt_b200 import capi
+    g = capi.Simulation(64, 64, ntrace=0)
+    g.add_simple_spin()
+    g.set_guess(2)
+    dt = g.initialize()
+    g.step(0.9 * dt, 400)
+    for which in (0, 1):
+        z = g.get_mg(which)
+        spread = np.abs(z - z.mean()).max()
+        assert abs(z.mean()) <= 10 * spread + 1e-12, (which, z.mean(), spread)
+    g.close()

@@ -167,6 +167,9 @@ int learned_input(Multigrid &mg, LearnedWork &w, const double *d_b, const double
  * residual rule, 1: energy rule only), optional applied/fallback counters. */
 int learned_guess(Multigrid &mg, LearnedWork &w, incrmt_unet *net, const double *d_b, double *d_z, int f, int rule,
                   unsigned long long *cnt);
+/** How many times the network's activation buffers have been (re)allocated
+ * (a captured forward pass is valid only while this stays the same). */
+long long unet_generation(const incrmt_unet *h);
 /** Block averages of znew - zold on the network grid (training targets). */
 int learned_target(Multigrid &mg, const double *znew, const double *zold, int f, int H, int W, float *tgt);
 

@@ -64,6 +64,25 @@ struct Sim {
         long long captured = 0;
         double *z0 = nullptr;  // the warm start, kept for the capture's target
         long z0_n = 0;
+        // The guess (features, network, step along its output) captured into
+        // a CUDA graph for one (net, b, z), replayed on later projections:
+        // some sixty small launches, most of them the network's layers on a
+        // 256-square grid, whose host-side launch cost was a good part of the
+        // guess's time.
+        cudaGraphExec_t gexec = nullptr;
+        const incrmt_unet *gkey_net = nullptr;
+        long long gkey_gen = -1;
+        const double *gkey_b = nullptr;
+        const double *gkey_z = nullptr;
+        long long glaunches = 0;
+        const incrmt_unet *warm_net = nullptr;  // network and allocation generation
+        long long warm_gen = -1;                // after the last direct guess
+        bool gfail = false;
+        void release_graph() {
+            if (gexec) cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+            gkey_net = nullptr;
+        }
     } learn[2];
     unsigned long long *d_lcnt = nullptr;  // [sys][applied, fallback]
     // Warm start of the projections: 0 the previous solution (the
@@ -866,7 +885,48 @@ int Sim::learned_pre(int sys, const double *b, double *z) {
         return INCRMT_OK;
     }
     if (!L.net) return INCRMT_OK;
-    return learned_guess(mg, L.w, L.net, b, z, L.factor, L.rule, d_lcnt + 2 * sys);
+    unsigned long long *cnt = d_lcnt + 2 * sys;
+    if (L.gexec && L.gkey_net == L.net && L.gkey_gen == unet_generation(L.net) && L.gkey_b == b && L.gkey_z == z) {
+        INCRMT_CK(cudaGraphLaunch(L.gexec, stream));
+        mg.launches += L.glaunches;
+        return INCRMT_OK;
+    }
+    // A guess runs directly while the network's buffers may still be
+    // (re)allocated for this grid: the first one, and the first after the
+    // network was used at another size; the next one is captured (nothing is
+    // allocated then) and replayed from then on.
+    if (L.gfail || L.warm_net != L.net || L.warm_gen != unet_generation(L.net)) {
+        const int rd = learned_guess(mg, L.w, L.net, b, z, L.factor, L.rule, cnt);
+        L.warm_net = L.net;
+        L.warm_gen = unet_generation(L.net);
+        return rd;
+    }
+    L.release_graph();
+    const long long l0 = mg.launches;
+    INCRMT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int rc = learned_guess(mg, L.w, L.net, b, z, L.factor, L.rule, cnt);
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+    if (rc == INCRMT_OK && ce == cudaSuccess) {
+        ce = cudaGraphInstantiate(&L.gexec, graph, 0);
+        if (ce != cudaSuccess) L.gexec = nullptr;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != INCRMT_OK || ce != cudaSuccess || !L.gexec) {
+        // not capturable here: run the guess directly from now on
+        cudaGetLastError();
+        L.release_graph();
+        L.gfail = true;
+        mg.launches = l0;
+        return learned_guess(mg, L.w, L.net, b, z, L.factor, L.rule, cnt);
+    }
+    L.gkey_net = L.net;
+    L.gkey_gen = unet_generation(L.net);
+    L.gkey_b = b;
+    L.gkey_z = z;
+    L.glaunches = mg.launches - l0;
+    INCRMT_CK(cudaGraphLaunch(L.gexec, stream));
+    return INCRMT_OK;
 }
 
 /** After a solve under capture: the target (block averages of the solution
@@ -1242,6 +1302,7 @@ void Sim::destroy() {
     d_remap = nullptr;
     d_lcnt = nullptr;
     for (Learned &L : learn) {
+        L.release_graph();
         L.w.release();
         cudaFree(L.z0);
         L.z0 = nullptr;
@@ -1526,6 +1587,10 @@ int incrmt_sim_set_learned(incrmt_sim *h, int sys, incrmt_unet *net, int factor,
     if (net) {
         if (int r = incrmt::learned_supported(sys == INCRMT_SYS_MAC ? S.mac : S.fem)) return r;
     }
+    if (S.stream) INCRMT_CK(cudaStreamSynchronize(S.stream));
+    S.learn[sys].release_graph();
+    S.learn[sys].warm_net = nullptr;
+    S.learn[sys].gfail = false;
     S.learn[sys].net = net;
     S.learn[sys].factor = factor;
     S.learn[sys].rule = rule;

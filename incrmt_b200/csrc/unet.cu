@@ -284,6 +284,7 @@ struct UNet {
     long long launches = 0;
     // Workspace for the current (batch, H, W).
     int wb = 0, wh = 0, ww = 0;
+    long long gen = 0;  // activation (re)allocations so far
     std::vector<Act> acts;
     std::vector<void *> work;
     float *part = nullptr;  // weight- and bias-gradient partials
@@ -380,6 +381,7 @@ struct UNet {
     int ensure(int B, int H, int W) {
         if (B == wb && H == wh && W == ww) return INCRMT_OK;
         free_work();
+        gen++;  // every pointer into the activations changes
         auto alloc = [&](int level, int Cc) -> int {
             Act a;
             a.level = level;
@@ -576,6 +578,10 @@ struct UNet {
 struct incrmt_unet {
     incrmt::UNet u;
 };
+
+namespace incrmt {
+long long unet_generation(const incrmt_unet *h) { return h->u.gen; }
+}  // namespace incrmt
 
 extern "C" {
 

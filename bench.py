@@ -562,7 +562,8 @@ def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist
         lst1 = {s: sim.learned_stats(s) for s in nets}
         nm = lambda s: "mac" if s == capi.SYS_MAC else "fem"  # noqa: E731
         out["learned"] = {nm(s): {"applied": int(lst1[s].applied - lst0[s].applied),
-                                  "fallback": int(lst1[s].fallback - lst0[s].fallback)} for s in nets}
+                                  "fallback": int(lst1[s].fallback - lst0[s].fallback),
+                                  "skipped": int(lst1[s].skipped - lst0[s].skipped)} for s in nets}
         for v in out["learned"].values():
             v["fallback_rate"] = v["fallback"] / max(1, v["applied"] + v["fallback"])
     out["snapshot"] = _snapshot(sim)

@@ -108,9 +108,12 @@ int incrmt_sim_learned_capture(incrmt_sim *h, int sys, int factor, float *d_in, 
 
 /** Counts of system sys since the simulation was created: guesses applied,
  * guesses rejected by the rule (the solve then starts from the previous
- * solution), and samples captured by the current capture. */
+ * solution), samples captured by the current capture, and projections that
+ * skipped the guess: after 8 rejected guesses in a row the next 32
+ * projections of that system start from the warm start without computing a
+ * guess (the network's cost would buy nothing), then guessing resumes. */
 typedef struct incrmt_sim_learned_stats {
-    long long applied, fallback, captured;
+    long long applied, fallback, captured, skipped;
 } incrmt_sim_learned_stats;
 int incrmt_sim_get_learned_stats(incrmt_sim *h, int sys, incrmt_sim_learned_stats *st);
 

@@ -644,7 +644,8 @@ class LearnedStats(ctypes.Structure):
 
 
 class SimLearnedStats(ctypes.Structure):
-    _fields_ = [("applied", ctypes.c_longlong), ("fallback", ctypes.c_longlong), ("captured", ctypes.c_longlong)]
+    _fields_ = [("applied", ctypes.c_longlong), ("fallback", ctypes.c_longlong), ("captured", ctypes.c_longlong),
+                ("skipped", ctypes.c_longlong)]
 
 
 def _unet_sigs(L):

@@ -24,6 +24,8 @@ const dim3 kB2(32, 8);
 inline dim3 g2(int m, int n) { return dim3(cdiv(m, 32), cdiv(n, 8)); }
 constexpr int kLsMaxSweeps = 400;       // cap of the fixed-point sweeps of one march
 constexpr int kExtrapMaxSweeps = 1000;  // cap of the extrapolation wavefront sweeps
+constexpr int kLearnedStrikes = 8;      // rejected learned guesses in a row ...
+constexpr int kLearnedRest = 32;        // ... after which this many projections skip the guess
 }  // namespace
 
 struct Sim {
@@ -78,6 +80,13 @@ struct Sim {
         const incrmt_unet *warm_net = nullptr;  // network and allocation generation
         long long warm_gen = -1;                // after the last direct guess
         bool gfail = false;
+        // Rejected guesses in a row, projections still to skip, the rejection
+        // count last read, whether this projection computed a guess, and the
+        // projections skipped so far.
+        int fb_streak = 0, skip = 0;
+        unsigned long long fb_seen = 0;
+        bool ran = false;
+        long long skipped = 0;
         void release_graph() {
             if (gexec) cudaGraphExecDestroy(gexec);
             gexec = nullptr;
@@ -885,6 +894,12 @@ int Sim::learned_pre(int sys, const double *b, double *z) {
         return INCRMT_OK;
     }
     if (!L.net) return INCRMT_OK;
+    if (L.skip > 0) {
+        L.skip--;
+        L.skipped++;
+        return INCRMT_OK;
+    }
+    L.ran = true;
     unsigned long long *cnt = d_lcnt + 2 * sys;
     if (L.gexec && L.gkey_net == L.net && L.gkey_gen == unet_generation(L.net) && L.gkey_b == b && L.gkey_z == z) {
         INCRMT_CK(cudaGraphLaunch(L.gexec, stream));
@@ -933,6 +948,23 @@ int Sim::learned_pre(int sys, const double *b, double *z) {
  * minus the warm start). */
 int Sim::learned_post(int sys, const double *z) {
     Learned &L = learn[sys];
+    if (L.ran) {
+        // the solve has synchronised the stream: reading the rejection count
+        // costs one small copy
+        L.ran = false;
+        unsigned long long fb = 0;
+        INCRMT_CK(cudaMemcpyAsync(&fb, d_lcnt + 2 * sys + 1, sizeof(fb), cudaMemcpyDeviceToHost, stream));
+        INCRMT_CK(cudaStreamSynchronize(stream));
+        if (fb > L.fb_seen) {
+            if (++L.fb_streak >= kLearnedStrikes) {
+                L.fb_streak = 0;
+                L.skip = kLearnedRest;
+            }
+        } else {
+            L.fb_streak = 0;
+        }
+        L.fb_seen = fb;
+    }
     if (!(L.cap > 0 && L.captured < L.cap)) return INCRMT_OK;
     Multigrid &mg = sys == INCRMT_SYS_MAC ? mac : fem;
     int H, W;
@@ -1591,6 +1623,8 @@ int incrmt_sim_set_learned(incrmt_sim *h, int sys, incrmt_unet *net, int factor,
     S.learn[sys].release_graph();
     S.learn[sys].warm_net = nullptr;
     S.learn[sys].gfail = false;
+    S.learn[sys].fb_streak = 0;
+    S.learn[sys].skip = 0;
     S.learn[sys].net = net;
     S.learn[sys].factor = factor;
     S.learn[sys].rule = rule;
@@ -1636,6 +1670,7 @@ int incrmt_sim_get_learned_stats(incrmt_sim *h, int sys, incrmt_sim_learned_stat
     st->applied = static_cast<long long>(c[0]);
     st->fallback = static_cast<long long>(c[1]);
     st->captured = S.learn[sys].captured;
+    st->skipped = S.learn[sys].skipped;
     return INCRMT_OK;
 }
 

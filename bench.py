@@ -645,7 +645,10 @@ def compare_workload(workload, args, ws, rank, dev, dist, clocks=None, extras=Tr
         b = sim_run(workload, rank, dev, prec, None, args.steps, args.warmup, args.coarse_refresh, dist,
                     extras=False, guess=args.extrapolate)
         a["without_learned"] = {"steps_per_s": ws * b["steps_per_s"],
-                                "vcycles_per_projection": {"mac": b["vc_mac"], "fem": b["vc_fem"]}}
+                                "vcycles_per_projection": {"mac": b["vc_mac"], "fem": b["vc_fem"]},
+                                "mixed_fallbacks": b["mixed_fallbacks"],
+                                "errors_vs_fp64": _snap_errors(b["snapshot"], plain["snapshot"])
+                                if plain is not None else None}
     return a, plain, info
 
 

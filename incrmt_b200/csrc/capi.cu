@@ -121,6 +121,10 @@ int incrmt_mg_set_tiles(incrmt_mg *h, int on) {
         cudaGraphExecDestroy(mg.gexec);
         mg.gexec = nullptr;
     }
+    if (mg.setup_exec) {  // and so does the captured rebuild
+        cudaGraphExecDestroy(mg.setup_exec);
+        mg.setup_exec = nullptr;
+    }
     return INCRMT_OK;
 }
 

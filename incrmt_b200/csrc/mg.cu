@@ -1221,6 +1221,7 @@ void Multigrid::destroy() {
 
     if (hnorm) cudaFreeHost(hnorm);
     if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+    if (setup_exec) { cudaGraphExecDestroy(setup_exec); setup_exec = nullptr; }
     for (auto e : prof_ev) cudaEventDestroy(e);
     prof_ev.clear();
     if (ev0) cudaEventDestroy(ev0);
@@ -1238,7 +1239,7 @@ int Multigrid::set_density_device(const double *d_rho, int ld) {
     }
     launches++;
     INCRMT_CKL("coefficients");
-    int r = galerkin_all();
+    int r = galerkin_graph();
     if (r == INCRMT_OK) ready = true;
     coarse_builds++;
     coarse_age = 0;
@@ -1348,6 +1349,35 @@ int Multigrid::galerkin_all() {
         launches++;
         INCRMT_CKL("k_coarse_inverse");
     }
+    return INCRMT_OK;
+}
+
+int Multigrid::galerkin_graph() {
+    // The hierarchy's arrays never move, so the whole rebuild (weights,
+    // Galerkin products, the coarsest inverse: dozens of launches, most on
+    // small levels) is captured once and replayed; profiling runs it
+    // directly.
+    if (prof) return galerkin_all();
+    if (!setup_exec) {
+        const long long l0 = launches;
+        cudaGraph_t graph = nullptr;
+        INCRMT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int rc = galerkin_all();
+        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+        if (rc == INCRMT_OK && ce == cudaSuccess) ce = cudaGraphInstantiate(&setup_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (rc != INCRMT_OK || ce != cudaSuccess) {
+            setup_exec = nullptr;
+            cudaGetLastError();
+            launches = l0;
+            return galerkin_all();
+        }
+        setup_launches = launches - l0;
+        launches = l0;
+    }
+    INCRMT_CK(cudaGraphLaunch(setup_exec, stream));
+    launches += setup_launches;
+    f32_stale = true;
     return INCRMT_OK;
 }
 

@@ -78,6 +78,8 @@ public:
     bool tiles = true;               // tile-fused smoothing where it applies
     int tail_level = -1;             // first level run by the one-block tail kernel
     cudaGraphExec_t gexec = nullptr; // captured V-cycle + norm
+    cudaGraphExec_t setup_exec = nullptr;  // captured rebuild of the coarse levels
+    long long setup_launches = 0;
     int gkey_prec = -1;
     const double *gkey_b = nullptr;
     const double *gkey_z = nullptr;
@@ -135,6 +137,8 @@ public:
 private:
     int build_hierarchy();
     int galerkin_all();
+    /** galerkin_all as a CUDA graph captured on first use and replayed. */
+    int galerkin_graph();
     /** FP32 copies of the Galerkin stencils, made on the first mixed solve
      * after a rebuild (FP64 solves never read them). */
     int cast_levels();

@@ -515,7 +515,7 @@ def projection_roofline(sim, workload, prec, vc_mac, vc_fem, phases):
 
 
 def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist, clocks=None, extras=True, guess=0,
-            e2e_steps=0, learned_rule=0):
+            e2e_steps=0, learned_rule=0, krylov=False):
     """One run of a simulation workload: warm-up, K timed steps (CUDA events
     on the simulation stream, max over ranks), end snapshot, then (extras)
     the phase breakdown and the live smoother roofline over further steps
@@ -526,6 +526,7 @@ def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist
     sim = make_sim(workload, rank, prec)
     sim.set_coarse_refresh(coarse_refresh)
     sim.set_guess(guess)
+    sim.set_krylov(krylov)
     dt = frame_dt(sim.dt_reg, frame_interval(workload))
     if nets is not None:
         for sys, net in nets.items():
@@ -556,6 +557,7 @@ def sim_run(workload, rank, dev, prec, nets, steps, warmup, coarse_refresh, dist
     out["coarse_builds_per_step"] = (st1.coarse_builds - st0.coarse_builds) / steps
     out["coarse_retries"] = int(st1.coarse_retries - st0.coarse_retries)
     out["mixed_fallbacks"] = int(st1.mixed_fallbacks - st0.mixed_fallbacks)
+    out["krylov_fallbacks"] = int(st1.krylov_fallbacks - st0.krylov_fallbacks)
     out["march_sweeps_per_step"] = (st1.march_sweeps - st0.march_sweeps) / steps
     out["extrap_sweeps_per_step"] = (st1.extrap_sweeps - st0.extrap_sweeps) / steps
     if nets:
@@ -621,7 +623,7 @@ def compare_workload(workload, args, ws, rank, dev, dist, clocks=None, extras=Tr
         nets, info = train_learned_sim(workload, rank, dev, args.extrapolate)
     a = sim_run(workload, rank, dev, prec, nets, args.steps, args.warmup, args.coarse_refresh, dist, clocks=clocks,
                 extras=extras, guess=args.extrapolate, e2e_steps=args.steps if e2e else 0,
-                learned_rule=args.learned_rule)
+                learned_rule=args.learned_rule, krylov=bool(args.krylov))
     plain = None
     if nets is not None or prec != capi.PREC_FP64 or args.extrapolate:
         plain = sim_run(workload, rank, dev, capi.PREC_FP64, None, args.steps, args.warmup, args.coarse_refresh,
@@ -632,18 +634,27 @@ def compare_workload(workload, args, ws, rank, dev, dist, clocks=None, extras=Tr
         # every 16 projections instead of on every one (the reference's
         # policy, kept for the headline)
         c = sim_run(workload, rank, dev, prec, nets, args.steps, args.warmup, 16, dist, extras=False,
-                    guess=args.extrapolate, learned_rule=args.learned_rule)
+                    guess=args.extrapolate, learned_rule=args.learned_rule, krylov=bool(args.krylov))
         a["coarse_refresh_16"] = {"steps_per_s": ws * c["steps_per_s"],
                                   "vcycles_per_projection": {"mac": c["vc_mac"], "fem": c["vc_fem"]},
                                   "errors_vs_fp64": _snap_errors(c["snapshot"], plain["snapshot"])
                                   if plain is not None else None}
+    # the timed configuration with the flexible CG around the V-cycle
+    # switched the other way (incrmt_sim_set_krylov)
+    kv = sim_run(workload, rank, dev, prec, nets, args.steps, args.warmup, args.coarse_refresh, dist,
+                 extras=False, guess=args.extrapolate, learned_rule=args.learned_rule, krylov=not args.krylov)
+    a["with_krylov" if not args.krylov else "without_krylov"] = {
+        "steps_per_s": ws * kv["steps_per_s"],
+        "vcycles_per_projection": {"mac": kv["vc_mac"], "fem": kv["vc_fem"]},
+        "krylov_fallbacks": kv["krylov_fallbacks"], "mixed_fallbacks": kv["mixed_fallbacks"],
+        "errors_vs_fp64": _snap_errors(kv["snapshot"], plain["snapshot"]) if plain is not None else None}
     if nets is not None:
         for net in nets.values():
             net.close()
         # the same configuration without the networks: what the learned
         # correction adds or costs on top of the rest
         b = sim_run(workload, rank, dev, prec, None, args.steps, args.warmup, args.coarse_refresh, dist,
-                    extras=False, guess=args.extrapolate)
+                    extras=False, guess=args.extrapolate, krylov=bool(args.krylov))
         a["without_learned"] = {"steps_per_s": ws * b["steps_per_s"],
                                 "vcycles_per_projection": {"mac": b["vc_mac"], "fem": b["vc_fem"]},
                                 "mixed_fallbacks": b["mixed_fallbacks"],
@@ -681,6 +692,9 @@ def run_ours_sim(args, ws, rank, local, dist):
             also[w]["errors_vs_fp64"] = b["errors_vs_fp64"]
         if "learned" in b:
             also[w]["learned"] = b["learned"]
+        for key in ("with_krylov", "without_krylov"):
+            if key in b:
+                also[w][key] = b[key]
     if rank != 0:
         return
     cpu = None
@@ -716,9 +730,10 @@ def run_ours_sim(args, ws, rank, local, dist):
         "data": "synthetic",
         "config": {"workload": describe(args.workload), "precision": args.precision, "initial_guess": guess,
                    "flush": "working set larger than L2", "parallelism": f"replicas x{ws}",
-                   "coarse_refresh": args.coarse_refresh},
+                   "coarse_refresh": args.coarse_refresh, "krylov": bool(args.krylov)},
         "vcycles_per_projection": {"mac": a["vc_mac"], "fem": a["vc_fem"]},
         "mixed_fallbacks": a["mixed_fallbacks"],
+        "krylov_fallbacks": a["krylov_fallbacks"],
         "coarse_builds_per_step": a["coarse_builds_per_step"],
         "phase_ms_per_step": a["phases"],
         "march_sweeps_per_step": a["march_sweeps_per_step"],
@@ -745,6 +760,9 @@ def run_ours_sim(args, ws, rank, local, dist):
         line["without_learned"] = a["without_learned"]
     if "coarse_refresh_16" in a:
         line["coarse_refresh_16"] = a["coarse_refresh_16"]
+    for key in ("with_krylov", "without_krylov"):
+        if key in a:
+            line[key] = a[key]
     if also:
         line["also"] = also
     print(json.dumps(line))
@@ -847,6 +865,8 @@ def run_ours(args, ws, rank, local, dist):
         dz, ds = z - z.mean(), zstar - zstar.mean()
         learned_info["guess_relative_error"] = float((dz - ds).norm() / ds.norm())
         learned_info["guess_alpha"] = st.alpha
+
+    s.set_krylov(bool(args.krylov))
 
     def step():
         s.set_density_device(rho.data_ptr())
@@ -963,7 +983,8 @@ def run_ours(args, ws, rank, local, dist):
         "config": {"workload": f"standalone MAC solve {m}x{m} (8 circles rho 3, 64 blobs), "
                                f"setup + V-cycles to 1e-9 from " +
                                ("the learned guess" if args.learned else "zero"), "precision": args.precision,
-                   "flush": "inputs larger than L2 (each array 134 MB)", "parallelism": f"replicas x{ws}"},
+                   "flush": "inputs larger than L2 (each array 134 MB)", "parallelism": f"replicas x{ws}",
+                   "krylov": bool(args.krylov)},
         "vcycles_per_projection": float(np.mean(vcs)),
         "roofline": _roofline("mac4096_smooth", kms, kbytes, klaunch,
                               "k_smooth_rb (fine-level red-black Gauss-Seidel, two sweeps per launch)",
@@ -981,6 +1002,11 @@ def run_ours(args, ws, rank, local, dist):
         # the whole step, which also rebuilds the coefficients and the
         # Galerkin hierarchy (the reference's setup per solve)
         bpu = 304.0 if prec == capi.PREC_FP64 else 152.0 + 68.0
+        if args.krylov:
+            # the flexible CG's FP64 vector passes per iteration (dot
+            # products, direction, A p, step: 124 B per unknown) instead of
+            # the mixed path's 68 B outer residual and update
+            bpu += 124.0 - (0.0 if prec == capi.PREC_FP64 else 68.0)
         ach = float(np.mean(vcs)) * m * m * bpu / (ms_max / args.steps / 1e3) / 1e9
         peak, kind = _peaks()
         line["roofline"]["vcycle_level"] = {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
@@ -1024,6 +1050,9 @@ def main():
                          "(1: on every density change, as the reference)")
     ap.add_argument("--also", default="sed2048",
                     help="further simulation workloads compared the same way (comma-separated; N=1 only)")
+    ap.add_argument("--krylov", type=int, default=0, choices=[0, 1],
+                    help="1: flexible conjugate gradients with the V-cycle as preconditioner in the timed "
+                         "configuration (incrmt_sim_set_krylov); the plain FP64 comparison run never uses it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned-rule", type=int, default=0, choices=[0, 1],
                     help="fallback rule of the simulation's learned warm start (0: when the guess raises the "

@@ -105,6 +105,24 @@ int incrmt_mg_set_profiling(incrmt_mg *h, int on);
  * colour everywhere; it exists to check that identity. */
 int incrmt_mg_set_tiles(incrmt_mg *h, int on);
 
+/** Flexible conjugate gradients around the V-cycle (no reference
+ * counterpart; off by default). On (1), each solve iterates FCG(1) (Notay,
+ * SIAM J. Sci. Comput. 22 (2000) 1444-1460) with one V-cycle of the
+ * requested precision as the preconditioner: the direction is the
+ * preconditioned residual made A-orthogonal to the previous direction, the
+ * step minimises the energy norm along it, and the residual is updated in
+ * FP64 (confirmed on b - A z when it reaches the tolerance). The tolerance,
+ * the statistics (vcycles counts iterations, one V-cycle each) and the
+ * result's accuracy are those of the plain solve; an iteration that fails to
+ * halve the residual hands the solve to plain FP64 V-cycles from the current
+ * iterate (counted by incrmt_mg_krylov_fallbacks). Off, the solve is the
+ * reference's plain V-cycle iteration. */
+int incrmt_mg_set_krylov(incrmt_mg *h, int on);
+
+/** Solves since creation in which the flexible CG handed over to plain FP64
+ * V-cycles. */
+long long incrmt_mg_krylov_fallbacks(const incrmt_mg *h);
+
 /** Lagged coarse operators (no reference counterpart; default 1). With
  * every > 1 a density change recomputes the fine-level coefficients, which
  * define the system solved, but rebuilds the Galerkin coarse levels only on

@@ -115,6 +115,8 @@ typedef struct incrmt_sim_stats {
                                               coarse levels, with the levels rebuilt */
     long long mixed_fallbacks;             /* mixed-precision projections finished with FP64 V-cycles
                                               (an FP32 correction did not halve the residual) */
+    long long krylov_fallbacks;            /* projections whose flexible CG handed over to plain FP64
+                                              V-cycles (incrmt_sim_set_krylov) */
 } incrmt_sim_stats;
 
 /** Creates the simulation (fluid_2d::fluid_2d, fluid_2d.cc:26-43). */
@@ -264,6 +266,11 @@ int incrmt_sim_set_guess(incrmt_sim *h, int mode);
  * benchmark use 16, which on the rotor and sediment scenes keeps the V-cycle
  * counts and removes most of the setup time. */
 int incrmt_sim_set_coarse_refresh(incrmt_sim *h, int every);
+
+/** Flexible conjugate gradients around the V-cycle in both projections
+ * (incrmt_mg_set_krylov; off by default, the reference's plain V-cycles).
+ * Every projection still reaches the same relative residual. */
+int incrmt_sim_set_krylov(incrmt_sim *h, int on);
 
 /** fluid_2d::solid_prd_bc (fluid_2d.hh:124), set before incrmt_initialize on
  * a doubly periodic domain: every object's reference map is periodic up to

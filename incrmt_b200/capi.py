@@ -80,6 +80,9 @@ def lib():
     L.incrmt_mg_set_profiling.argtypes = [P, I]
     L.incrmt_mg_set_tiles.argtypes = [P, I]
     L.incrmt_mg_set_coarse_refresh.argtypes = [P, I]
+    L.incrmt_mg_set_krylov.argtypes = [P, I]
+    L.incrmt_mg_krylov_fallbacks.argtypes = [P]
+    L.incrmt_mg_krylov_fallbacks.restype = ctypes.c_longlong
     L.incrmt_mg_coarse_builds.argtypes = [P, ctypes.POINTER(ctypes.c_longlong)]
     L.incrmt_mg_coarse_builds.restype = ctypes.c_longlong
     L.incrmt_mg_mixed_fallbacks.argtypes = [P]
@@ -191,6 +194,15 @@ class MGSolver:
         (incrmt_mg_set_coarse_refresh; 1 rebuilds on every change)."""
         check(lib().incrmt_mg_set_coarse_refresh(self._h, int(every)))
 
+    def set_krylov(self, on=True):
+        """Flexible conjugate gradients with the V-cycle as preconditioner
+        (incrmt_mg_set_krylov); off runs plain V-cycles."""
+        check(lib().incrmt_mg_set_krylov(self._h, int(on)))
+
+    def krylov_fallbacks(self):
+        """Solves whose flexible CG handed over to plain FP64 V-cycles."""
+        return int(lib().incrmt_mg_krylov_fallbacks(self._h))
+
     def mixed_fallbacks(self):
         """Mixed-precision solves that finished with FP64 V-cycles."""
         return int(lib().incrmt_mg_mixed_fallbacks(self._h))
@@ -292,7 +304,7 @@ class SimStats(ctypes.Structure):
                 ("dt_reg", ctypes.c_double), ("time", ctypes.c_double),
                 ("march_monotone", ctypes.c_longlong), ("window_points", ctypes.c_longlong),
                 ("coarse_builds", ctypes.c_longlong), ("coarse_retries", ctypes.c_longlong),
-                ("mixed_fallbacks", ctypes.c_longlong)]
+                ("mixed_fallbacks", ctypes.c_longlong), ("krylov_fallbacks", ctypes.c_longlong)]
 
 
 def _sim_sigs(L):
@@ -320,6 +332,7 @@ def _sim_sigs(L):
     L.incrmt_sim_set_windows.argtypes = [P, I]
     L.incrmt_set_solid_prd_bc.argtypes = [P, I]
     L.incrmt_sim_set_coarse_refresh.argtypes = [P, I]
+    L.incrmt_sim_set_krylov.argtypes = [P, I]
     L.incrmt_sim_set_guess.argtypes = [P, I]
     L.incrmt_set_object_tracers.argtypes = [P, dp, I, I]
     L.incrmt_l_comparison.argtypes = [P, P, dp]
@@ -579,6 +592,11 @@ class Simulation:
         """Rebuild the projections' Galerkin coarse operators every `every`
         projections (1 = every density change)."""
         check(lib().incrmt_sim_set_coarse_refresh(self._h, int(every)))
+
+    def set_krylov(self, on=True):
+        """Flexible conjugate gradients around the V-cycle in both
+        projections (incrmt_sim_set_krylov)."""
+        check(lib().incrmt_sim_set_krylov(self._h, int(on)))
 
     def set_guess(self, mode):
         """Warm start of the projections (incrmt_sim_set_guess): 0 the

@@ -125,8 +125,20 @@ int incrmt_mg_set_tiles(incrmt_mg *h, int on) {
         cudaGraphExecDestroy(mg.setup_exec);
         mg.setup_exec = nullptr;
     }
+    if (mg.kexec) {  // and the captured Krylov iteration
+        cudaGraphExecDestroy(mg.kexec);
+        mg.kexec = nullptr;
+    }
     return INCRMT_OK;
 }
+
+int incrmt_mg_set_krylov(incrmt_mg *h, int on) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    h->mg.krylov = on != 0;
+    return INCRMT_OK;
+}
+
+long long incrmt_mg_krylov_fallbacks(const incrmt_mg *h) { return h ? h->mg.krylov_fallbacks : 0; }
 
 int incrmt_mg_set_coarse_refresh(incrmt_mg *h, int every) {
     if (!h || every < 1) { set_error("bad argument"); return INCRMT_ERR_BADARG; }

@@ -1000,6 +1000,139 @@ __global__ void k_zero_column(double *b, int m, int n) {
     if (j < n) b[m - 1 + m * j] = 0;
 }
 
+// ---------------------------------------------------------------------------
+// Flexible conjugate gradients (FCG(1), Notay, SIAM J. Sci. Comput. 22 (2000)
+// 1444-1460) with one V-cycle as the preconditioner e = M r:
+//   p_k = e_k - (e_k . q_{k-1} / p_{k-1} . q_{k-1}) p_{k-1},  q_k = A p_k,
+//   alpha_k = p_k . r_k / p_k . q_k,  z += alpha_k p_k,  r -= alpha_k q_k.
+// The explicit orthogonalisation against the previous direction keeps the
+// iteration convergent although the V-cycle (the same colour order before and
+// after the coarse correction, FP32 in mixed precision) is not a symmetric
+// linear operator. The scalars live on the device (ks), so an iteration needs
+// no host round trip besides the residual norm. For the singular systems (no
+// zero-pressure edge) e is made mean-free, so every direction, and the
+// iterate's mean, stay in the range of A.
+
+/** Per-block sums of e, e.q and q (part[b], part[nb + b], part[2 nb + b]). */
+template <class Te>
+__global__ void k_cg_dots(const Te *e, const double *q, long N, double *part) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < N;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const double ev = static_cast<double>(e[i]), qv = q[i];
+        s0 += ev;
+        s1 += ev * qv;
+        s2 += qv;
+    }
+    s0 = block_sum_256(s0);
+    s1 = block_sum_256(s1);
+    s2 = block_sum_256(s2);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s0;
+        part[gridDim.x + blockIdx.x] = s1;
+        part[2 * gridDim.x + blockIdx.x] = s2;
+    }
+}
+
+/** out[k] = sum of part[k nb .. k nb + nb - 1] for k < K, in a fixed order. */
+template <int K>
+__global__ void k_reduce_n(const double *part, int nb, double *out) {
+#pragma unroll 1
+    for (int k = 0; k < K; k++) {
+        double acc = 0;
+        for (int q = threadIdx.x; q < nb; q += blockDim.x) acc += part[k * nb + q];
+        acc = block_sum_256(acc);
+        if (threadIdx.x == 0) out[k] = acc;
+    }
+}
+
+/** The new direction p = (e - mu) - beta p, mu the mean of e on a singular
+ * system (else 0), beta = (e - mu).q / p.q of the previous direction (0 for
+ * the first direction, ks[3] == 0, when p is not read). */
+template <class Te>
+__global__ void k_cg_direction(const Te *e, double *p, long N, const double *ks, int singular) {
+    const double mu = singular ? ks[0] / static_cast<double>(N) : 0.0;
+    const double pq = ks[3];
+    const double beta = pq != 0 ? (ks[1] - mu * ks[2]) / pq : 0.0;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < N;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        const double em = static_cast<double>(e[i]) - mu;
+        p[i] = beta != 0 ? em - beta * p[i] : em;
+    }
+}
+
+/** q = A p with per-block sums of p.q and p.r (part[b], part[nb + b]); rows
+ * strided over the blocks as in k_resnorm. */
+template <class Op>
+__global__ void k_cg_apply(Op op, const double *p, double *q, const double *r, int m, int n, double *part) {
+    double s0 = 0, s1 = 0;
+    for (int j = blockIdx.x; j < n; j += gridDim.x)
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const long k = i + static_cast<long>(m) * j;
+            double diag;
+            const double off = op.offdiag(i, j, p, diag);
+            const double pv = p[k], qv = fma_rn(diag, pv, off);
+            q[k] = qv;
+            s0 += pv * qv;
+            s1 += pv * r[k];
+        }
+    s0 = block_sum_256(s0);
+    s1 = block_sum_256(s1);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s0;
+        part[gridDim.x + blockIdx.x] = s1;
+    }
+}
+
+/** z += alpha p, r -= alpha q (alpha = p.r / p.q from ks[5], ks[4]), the
+ * FP32 copy of r for the next mixed cycle, per-block sums of r^2. */
+__global__ void k_cg_update(double *z, double *r, const double *p, const double *q, float *rf, long N,
+                            const double *ks, double *part) {
+    const double pq = ks[4], alpha = pq != 0 ? ks[5] / pq : 0.0;
+    double acc = 0;
+    for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < N;
+         i += static_cast<long>(gridDim.x) * blockDim.x) {
+        z[i] = fma_rn(alpha, p[i], z[i]);
+        const double rn = fma_rn(-alpha, q[i], r[i]);
+        r[i] = rn;
+        if (rf) rf[i] = static_cast<float>(rn);
+        acc += rn * rn;
+    }
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+/** ||r||^2 into *norm from the update's partials; the direction's p.q
+ * becomes the previous one for the next iteration. */
+__global__ void k_cg_finish(const double *part, int nb, double *norm, double *ks) {
+    double acc = 0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) acc += part[q];
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) {
+        *norm = acc;
+        ks[3] = ks[4];
+    }
+}
+
+/** r = b - A z in FP64 (and FP32 into rf if given), per-block sums of r^2. */
+template <class Op>
+__global__ void k_cg_residual(Op op, const double *z, const double *b, int m, int n, double *r, float *rf,
+                              double *part) {
+    double acc = 0;
+    for (int j = blockIdx.x; j < n; j += gridDim.x)
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const long k = i + static_cast<long>(m) * j;
+            double diag;
+            const double off = op.offdiag(i, j, z, diag);
+            const double rv = fma_rn(-diag, z[k], sub_rn(b[k], off));
+            r[k] = rv;
+            if (rf) rf[k] = static_cast<float>(rv);
+            acc += rv * rv;
+        }
+    acc = block_sum_256(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
 constexpr int kRedBlocks = 4 * kB200SMs;  // reduction grid: 4 x 148 blocks of 256
 
 inline dim3 grid2(int m, int n) { return dim3(cdiv(m, 32), cdiv(n, 8)); }
@@ -1222,6 +1355,9 @@ void Multigrid::destroy() {
     if (hnorm) cudaFreeHost(hnorm);
     if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
     if (setup_exec) { cudaGraphExecDestroy(setup_exec); setup_exec = nullptr; }
+    if (kexec) { cudaGraphExecDestroy(kexec); kexec = nullptr; }
+    cudaFree(kr); cudaFree(kp); cudaFree(kq); cudaFree(ke); cudaFree(kpart); cudaFree(ks);
+    kr = kp = kq = ke = kpart = ks = nullptr;
     for (auto e : prof_ev) cudaEventDestroy(e);
     prof_ev.clear();
     if (ev0) cudaEventDestroy(ev0);
@@ -1646,6 +1782,144 @@ int Multigrid::vcycle_and_norm(int prec, const double *b, double *d_z, long N) {
     return INCRMT_OK;
 }
 
+int Multigrid::krylov_alloc() {
+    if (kr) return INCRMT_OK;
+    const size_t N = static_cast<size_t>(m) * n;
+    INCRMT_CK(cudaMalloc(&kr, sizeof(double) * N));
+    INCRMT_CK(cudaMalloc(&kp, sizeof(double) * N));
+    INCRMT_CK(cudaMalloc(&kq, sizeof(double) * N));
+    INCRMT_CK(cudaMalloc(&ke, sizeof(double) * N));
+    INCRMT_CK(cudaMalloc(&kpart, sizeof(double) * 3 * kRedBlocks));
+    INCRMT_CK(cudaMalloc(&ks, sizeof(double) * 8));
+    // q enters the first iteration's dot products (whose results the first
+    // direction does not use): keep it finite
+    INCRMT_CK(cudaMemsetAsync(kq, 0, sizeof(double) * N, stream));
+    INCRMT_CK(cudaMemsetAsync(kp, 0, sizeof(double) * N, stream));
+    INCRMT_CK(cudaMemsetAsync(ks, 0, sizeof(double) * 8, stream));
+    return INCRMT_OK;
+}
+
+int Multigrid::krylov_residual(int prec, const double *b, const double *d_z) {
+    const int nb = n < kRedBlocks ? n : kRedBlocks;  // blocks over the rows
+    float *rf = prec == INCRMT_PREC_MIXED ? lev[0].bf : nullptr;
+    if (sys == INCRMT_SYS_MAC) k_cg_residual<<<nb, 256, 0, stream>>>(mac64(), d_z, b, m, n, kr, rf, kpart);
+    else k_cg_residual<<<nb, 256, 0, stream>>>(fem64(), d_z, b, m, n, kr, rf, kpart);
+    k_reduce<<<1, 256, 0, stream>>>(kpart, nb, dnorm);
+    launches += 2;
+    INCRMT_CKL("krylov residual");
+    return INCRMT_OK;
+}
+
+int Multigrid::krylov_iteration(int prec, double *d_z, long N) {
+    int r;
+    const long long l0 = launches;
+    const int nbk = cdiv(N, 256) < kRedBlocks ? cdiv(N, 256) : kRedBlocks;
+    const int nbr = n < kRedBlocks ? n : kRedBlocks;
+    const int singular = zpr ? 0 : 1;
+    if (prec == INCRMT_PREC_FP64) {
+        k_fill<double><<<nbk, 256, 0, stream>>>(ke, N, 0.0);
+        launches++;
+        if ((r = cycle64(0, kr, ke))) return r;
+        k_cg_dots<double><<<nbk, 256, 0, stream>>>(ke, kq, N, kpart);
+        k_reduce_n<3><<<1, 256, 0, stream>>>(kpart, nbk, ks);
+        k_cg_direction<double><<<nbk, 256, 0, stream>>>(ke, kp, N, ks, singular);
+    } else {
+        k_fill<float><<<nbk, 256, 0, stream>>>(lev[0].zf, N, 0.f);
+        launches++;
+        if ((r = cycle32(0))) return r;
+        k_cg_dots<float><<<nbk, 256, 0, stream>>>(lev[0].zf, kq, N, kpart);
+        k_reduce_n<3><<<1, 256, 0, stream>>>(kpart, nbk, ks);
+        k_cg_direction<float><<<nbk, 256, 0, stream>>>(lev[0].zf, kp, N, ks, singular);
+    }
+    if (sys == INCRMT_SYS_MAC) k_cg_apply<<<nbr, 256, 0, stream>>>(mac64(), kp, kq, kr, m, n, kpart);
+    else k_cg_apply<<<nbr, 256, 0, stream>>>(fem64(), kp, kq, kr, m, n, kpart);
+    k_reduce_n<2><<<1, 256, 0, stream>>>(kpart, nbr, ks + 4);
+    k_cg_update<<<nbk, 256, 0, stream>>>(d_z, kr, kp, kq, prec == INCRMT_PREC_MIXED ? lev[0].bf : nullptr, N, ks,
+                                         kpart);
+    k_cg_finish<<<1, 256, 0, stream>>>(kpart, nbk, dnorm, ks);
+    launches += 7;
+    INCRMT_CKL("krylov iteration");
+    INCRMT_CK(cudaMemcpyAsync(hnorm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    kexec_launches = launches - l0;
+    return INCRMT_OK;
+}
+
+int Multigrid::krylov_solve(int prec, const double *b, double *d_z, long N, double tol, int maxc, int &k,
+                            double &rn2, bool &conv, bool &finite, bool &fell) {
+    int r;
+    conv = false;
+    finite = true;
+    fell = false;
+    if ((r = krylov_alloc())) return r;
+    if (prec == INCRMT_PREC_MIXED && (r = cast_levels())) return r;
+    // The fixed column's rows of the FEM system with the zero-pressure edge
+    // hold the diagonal alone and a zero right-hand side: their solution is
+    // 0, set here, so that the iteration stays on the symmetric remainder.
+    if (sys == INCRMT_SYS_FEM && zpr) {
+        k_zero_column<<<cdiv(n, 256), 256, 0, stream>>>(d_z, m, n);
+        launches++;
+        INCRMT_CKL("zero column");
+    }
+    if ((r = krylov_residual(prec, b, d_z))) return r;
+    if ((r = fetch_norm(&rn2))) return r;
+    double rn_prev = std::sqrt(rn2);
+    if (!std::isfinite(rn_prev)) { finite = false; return INCRMT_OK; }
+    if (rn_prev <= tol) { conv = true; return INCRMT_OK; }
+    INCRMT_CK(cudaMemsetAsync(ks, 0, sizeof(double) * 8, stream));
+    const bool use_graph = !prof;
+    if (use_graph && (!kexec || kkey_prec != prec || kkey_b != b || kkey_z != d_z)) {
+        if (kexec) { cudaGraphExecDestroy(kexec); kexec = nullptr; }
+        cudaGraph_t graph = nullptr;
+        INCRMT_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = krylov_iteration(prec, d_z, N);
+        cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+        if (rc || ce != cudaSuccess) {
+            if (ce == cudaSuccess && graph) cudaGraphDestroy(graph);
+            if (rc) return rc;
+            return cuda_status(ce, "capture", __FILE__, __LINE__);
+        }
+        ce = cudaGraphInstantiate(&kexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) { kexec = nullptr; return cuda_status(ce, "instantiate", __FILE__, __LINE__); }
+        kkey_prec = prec; kkey_b = b; kkey_z = d_z;
+    }
+    while (k < maxc) {
+        if (use_graph) {
+            INCRMT_CK(cudaGraphLaunch(kexec, stream));
+            launches += kexec_launches;
+        } else if ((r = krylov_iteration(prec, d_z, N))) {
+            return r;
+        }
+        INCRMT_CK(cudaStreamSynchronize(stream));
+        rn2 = hnorm[0];
+        k++;
+        const double rn = std::sqrt(rn2);
+        if (!std::isfinite(rn)) { finite = false; return INCRMT_OK; }
+        if (rn <= tol) {
+            // The recurrence's residual has converged: confirm it on b - A z
+            // itself, else restart from that residual.
+            if ((r = krylov_residual(prec, b, d_z))) return r;
+            if ((r = fetch_norm(&rn2))) return r;
+            const double rt = std::sqrt(rn2);
+            if (!std::isfinite(rt)) { finite = false; return INCRMT_OK; }
+            if (rt <= tol) { conv = true; return INCRMT_OK; }
+            INCRMT_CK(cudaMemsetAsync(ks, 0, sizeof(double) * 8, stream));
+            rn_prev = rt;
+            continue;
+        }
+        // An iteration that does not halve the residual: the preconditioned
+        // iteration is not working on this system; the caller finishes with
+        // plain FP64 V-cycles from the current iterate.
+        if (rn > kMixedContraction * rn_prev) {
+            fell = true;
+            krylov_fallbacks++;
+            return INCRMT_OK;
+        }
+        rn_prev = rn;
+    }
+    return INCRMT_OK;
+}
+
 int Multigrid::vcycle64(const double *d_b, double *d_z) {
     if (!ready) { set_error("density not set"); return INCRMT_ERR_BADARG; }
     return cycle64(0, d_b, d_z);
@@ -1729,9 +2003,20 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         }
         return INCRMT_OK;
     }
-    bool conv = false, finite = true;
+    bool conv = false, finite = true, plain = true;
     double rn_prev = 0;
-    if (prec == INCRMT_PREC_MIXED) {
+    int cur = prec;
+    if (krylov) {
+        // Flexible CG around the V-cycle; plain FP64 V-cycles finish the
+        // solve only if an iteration fails to halve the residual.
+        bool fell = false;
+        if ((r = krylov_solve(prec, b, d_z, N, tol, maxc, k, rn2, conv, finite, fell))) return r;
+        plain = fell;
+        if (fell) {
+            cur = INCRMT_PREC_FP64;
+            if (prec == INCRMT_PREC_MIXED) mixed_fallbacks++;
+        }
+    } else if (prec == INCRMT_PREC_MIXED) {
         if ((r = cast_levels())) return r;
         if ((r = residual_norm(b, d_z, lev[0].bf, dnorm))) return r;
         if ((r = fetch_norm(&rn2))) return r;
@@ -1740,7 +2025,6 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
     // One V-cycle, its residual norm and the read-back of that norm, captured
     // once into a CUDA graph per (precision, b, z) and replayed per cycle.
     const bool use_graph = !prof;
-    int cur = prec;
     auto capture = [&]() -> int {
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
         cudaGraph_t graph = nullptr;
@@ -1758,8 +2042,9 @@ int Multigrid::solve_device(const double *d_b, double *d_z, const incrmt_mg_opts
         gkey_prec = cur; gkey_b = b; gkey_z = d_z;
         return INCRMT_OK;
     };
-    if (use_graph && (!gexec || gkey_prec != cur || gkey_b != b || gkey_z != d_z) && (r = capture())) return r;
-    while (k < maxc) {
+    if (plain && use_graph && (!gexec || gkey_prec != cur || gkey_b != b || gkey_z != d_z) && (r = capture()))
+        return r;
+    while (plain && k < maxc) {
         if (use_graph) {
             INCRMT_CK(cudaGraphLaunch(gexec, stream));
             launches += graph_launches;

@@ -13,6 +13,10 @@
 // residual r = b - A z and the update z += e in FP64 and solves A e = r with
 // one FP32 V-cycle per outer iteration (FP32 copies of the fine coefficients
 // and of the Galerkin stencils).
+//
+// Optionally (krylov) the outer iteration is a flexible conjugate gradient
+// method, FCG(1), with one V-cycle of either precision as its preconditioner
+// and the residual, direction and iterate in FP64.
 #pragma once
 #include <vector>
 #include "common.cuh"
@@ -84,6 +88,21 @@ public:
     const double *gkey_b = nullptr;
     const double *gkey_z = nullptr;
     long long graph_launches = 0;    // kernels in the captured graph
+    // Flexible conjugate gradients with the V-cycle as preconditioner
+    // (incrmt_mg_set_krylov; off by default). kr: FP64 residual, kp: search
+    // direction, kq: A kp, ke: FP64 preconditioned residual (FP64 cycles;
+    // mixed cycles leave it in lev[0].zf), kpart: 3 x kRedBlocks partial
+    // sums, ks: device scalars (sum e, e.q, sum q, the previous direction's
+    // p.q, p.q, p.r).
+    bool krylov = false;
+    double *kr = nullptr, *kp = nullptr, *kq = nullptr, *ke = nullptr;
+    double *kpart = nullptr, *ks = nullptr;
+    cudaGraphExec_t kexec = nullptr; // captured iteration (V-cycle, direction, step, norm)
+    int kkey_prec = -1;
+    const double *kkey_b = nullptr;
+    const double *kkey_z = nullptr;
+    long long kexec_launches = 0;
+    long long krylov_fallbacks = 0;  // solves finished with plain FP64 V-cycles
     // Optional timing of the fine-level smoothing launches (the dominant
     // kernel): CUDA events around each launch on the handle's stream.
     bool prof = false;
@@ -150,6 +169,18 @@ private:
     int norm2_rhs(const double *b, double *out_dev);
     int residual_norm(const double *b, const double *z, float *rf, double *out_dev);
     int fetch_norm(double *v);
+    int krylov_alloc();
+    /** kr = b - A z (and its FP32 copy into lev[0].bf in mixed precision),
+     * ||kr||^2 into dnorm[0]. */
+    int krylov_residual(int prec, const double *b, const double *d_z);
+    /** One flexible-CG iteration: e = V-cycle(kr), the new direction, the
+     * step along it, and ||kr||^2 into dnorm[0] and hnorm[0]. */
+    int krylov_iteration(int prec, double *d_z, long N);
+    /** Iterations of the flexible CG from d_z until the residual reaches
+     * tol (*conv), fails to halve (*fell, the caller continues with plain
+     * FP64 V-cycles) or is not finite (*finite false); *k counts them. */
+    int krylov_solve(int prec, const double *b, double *d_z, long N, double tol, int maxc, int &k, double &rn2,
+                     bool &conv, bool &finite, bool &fell);
 };
 
 /** Workspace of the learned initial guess (learned.cu), per solver. */

@@ -1602,6 +1602,7 @@ int incrmt_get_stats(const incrmt_sim *h, incrmt_sim_stats *st) {
     st->coarse_builds = S.mac.coarse_builds + S.fem.coarse_builds;
     st->coarse_retries = S.mac.coarse_retries + S.fem.coarse_retries;
     st->mixed_fallbacks = S.mac.mixed_fallbacks + S.fem.mixed_fallbacks;
+    st->krylov_fallbacks = S.mac.krylov_fallbacks + S.fem.krylov_fallbacks;
     st->launches = S.launches;
     st->dt_reg = S.dt_reg;
     st->time = S.time;
@@ -1713,6 +1714,13 @@ int incrmt_sim_set_coarse_refresh(incrmt_sim *h, int every) {
     h->s.fem.coarse_every = every;
     h->s.mac.coarse_stale = true;
     h->s.fem.coarse_stale = true;
+    return INCRMT_OK;
+}
+
+int incrmt_sim_set_krylov(incrmt_sim *h, int on) {
+    if (!h) { set_error("null handle"); return INCRMT_ERR_BADARG; }
+    h->s.mac.krylov = on != 0;
+    h->s.fem.krylov = on != 0;
     return INCRMT_OK;
 }
 

@@ -116,7 +116,8 @@ int incrmt_mg_set_tiles(incrmt_mg *h, int on);
  * result's accuracy are those of the plain solve; an iteration that fails to
  * halve the residual hands the solve to plain FP64 V-cycles from the current
  * iterate (counted by incrmt_mg_krylov_fallbacks). Off, the solve is the
- * reference's plain V-cycle iteration. */
+ * reference's plain V-cycle iteration (mg.solve_v_cycle, mgs_mac.cc:67,
+ * mgs_fem.cc:116). */
 int incrmt_mg_set_krylov(incrmt_mg *h, int on);
 
 /** Solves since creation in which the flexible CG handed over to plain FP64

@@ -227,9 +227,16 @@ __global__ void __launch_bounds__(256) k_galerkin_tile(Op op, int fm, int fn, in
     constexpr int NW = SW + 2, NH = SH + 2;
     double *As = gal_smem;          // entry k of support point t at As[k * SA + t]
     double *Ps = gal_smem + 9 * SA;  // weights of region point t at Ps[4 * t .. 4 * t + 3]
+    // Only the supports of coarse points I < cm, J < cn (fine x up to sxmax)
+    // and their stencil neighbours (one further) are read below. Beyond them
+    // the region of a level smaller than the tile would reach more than one
+    // period past a periodic grid, where one wrap does not bring an index
+    // back inside it: such points are not staged.
+    const int sxmax = kx ? 2 * cm - 1 : cm - 1, symax = ky ? 2 * cn - 1 : cn - 1;
     for (int t = threadIdx.x; t < NW * NH; t += blockDim.x) {
-        bool ok = true;
-        const int i = wrap_idx(NX0 + t % NW, fm, px, ok), j = wrap_idx(NY0 + t / NW, fn, py, ok);
+        const int xu = NX0 + t % NW, yu = NY0 + t / NW;
+        bool ok = xu <= sxmax + 1 && yu <= symax + 1;
+        const int i = wrap_idx(xu, fm, px, ok), j = wrap_idx(yu, fn, py, ok);
         double w[4] = {0, 0, 0, 0};
         if (ok) {
             const double *q = P + 4 * (static_cast<long>(i) + static_cast<long>(fm) * j);
@@ -238,9 +245,10 @@ __global__ void __launch_bounds__(256) k_galerkin_tile(Op op, int fm, int fn, in
         Ps[4 * t] = w[0]; Ps[4 * t + 1] = w[1]; Ps[4 * t + 2] = w[2]; Ps[4 * t + 3] = w[3];
     }
     for (int t = threadIdx.x; t < SA; t += blockDim.x) {
-        bool ok = true;
-        const int i = wrap_idx(SX0 + t % SW, fm, px, ok), j = wrap_idx(SY0 + t / SW, fn, py, ok);
-        if (!ok) continue;  // a point outside the grid has weight zero: never read
+        const int xu = SX0 + t % SW, yu = SY0 + t / SW;
+        bool ok = xu <= sxmax && yu <= symax;
+        const int i = wrap_idx(xu, fm, px, ok), j = wrap_idx(yu, fn, py, ok);
+        if (!ok) continue;  // outside the grid (weight zero) or no support of the tile: never read
         double a[9];
         op.coef9(i, j, a);
 #pragma unroll
@@ -735,7 +743,10 @@ __global__ void k_coarse_inverse(const double *st, int m, int n, int px, int py,
                 const int op_ = __shfl_down_sync(0xffffffffu, p, o);
                 if (ob > best || (ob == best && op_ >= 0 && (p < 0 || op_ < p))) { best = ob; p = op_; }
             }
-            if (threadIdx.x == 0) piv = p;
+            // no candidate compares (a NaN column): keep row k, so the
+            // inverse comes out NaN and the solve reports it, and no row
+            // outside the matrix is touched
+            if (threadIdx.x == 0) piv = p < 0 ? k : p;
         }
         __syncthreads();
         const int p = piv;

@@ -33,6 +33,12 @@ def test_bad_arguments_rejected_without_gpu():
     # A periodic direction needs an even number of unknowns (four-colour ordering).
     assert L.incrmt_mg_create(0, 63, 64, -1.0, 1.0, -1.0, 1.0, 1, 0, 0, ctypes.byref(h)) == capi.ERR_BADARG
     assert L.incrmt_mg_create(0, 1, 64, -1.0, 1.0, -1.0, 1.0, 0, 0, 0, ctypes.byref(h)) == capi.ERR_BADARG
+    # The solver and simulation switches refuse a null handle before touching a device.
+    assert L.incrmt_mg_set_krylov(None, 1) == capi.ERR_BADARG
+    assert L.incrmt_mg_krylov_fallbacks(None) == 0
+    assert L.incrmt_sim_set_krylov(None, 1) == capi.ERR_BADARG
+    assert L.incrmt_mg_set_coarse_refresh(None, 4) == capi.ERR_BADARG
+    assert L.incrmt_sim_set_guess(None, 1) == capi.ERR_BADARG
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):

@@ -390,7 +390,7 @@ def run_reference(args, ws, rank):
             "ms_per_step": 1e3 * dt / nref, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": describe(args.workload), "flush": "working set larger than L2",
-                       "coarse_refresh": 1},
+                       "coarse_refresh": 1, "krylov": False},
             "vcycles_per_projection": vc,
             "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": thr, "kind": "reference",
                              "sample": f"{nref} steps after {nwarm} warm-up steps (reference sources + TGMG-API "
